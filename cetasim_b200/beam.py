@@ -1,0 +1,125 @@
+"""Python host API over libcetagpu.so, mirroring the reference's MPBeam stage
+methods (include/MPBeam.h:131-177).  Each method forwards to one C-ABI call;
+all work runs in the sm_100a kernels.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from .configs import Workload
+
+
+class MPBeam:
+    """One device handle tracking a bunch train (MPBeam + its bunches + the
+    LatticeInterActionPoint ion clouds)."""
+
+    def __init__(self, wl: Workload, device: int = 0):
+        self.lib = _abi.load()
+        self.wl = wl
+        h = C.c_void_p()
+        rc = self.lib.cg_create(C.byref(wl.cfg), device, C.byref(h))
+        if rc:
+            raise _abi.CgError(rc, self.lib.cg_last_error(None).decode())
+        self.h = h
+        self._check(self.lib.cg_set_beam(h, wl.n_bunches, _abi.ptr(wl.n_macro), _abi.ptr(wl.harm),
+                                         _abi.ptr(wl.ne)))
+
+    # -- plumbing ------------------------------------------------------------
+    def _check(self, rc: int):
+        if rc:
+            raise _abi.CgError(rc, self.lib.cg_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.cg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- state in / out --------------------------------------------------------
+    def generate(self, seed: int = 99):
+        ex, ey, sz, sdp = self.wl.gen
+        self._check(self.lib.cg_generate_gaussian(self.h, ex, ey, sz, sdp, seed))
+
+    def upload(self, j: int, coords: np.ndarray, surv: np.ndarray | None = None):
+        c = [np.ascontiguousarray(coords[d], dtype=np.float64) for d in range(6)]
+        s = None if surv is None else np.ascontiguousarray(surv, dtype=np.uint8)
+        self._check(self.lib.cg_upload_bunch(self.h, j, *[_abi.ptr(a) for a in c], _abi.ptr(s)))
+
+    def download(self, j: int):
+        n = int(self.wl.n_macro[j])
+        c = np.empty((6, n))
+        s = np.empty(n, dtype=np.uint8)
+        self._check(self.lib.cg_download_bunch(self.h, j, *[_abi.ptr(c[d]) for d in range(6)],
+                                               _abi.ptr(s)))
+        return c, s
+
+    def moments(self):
+        out = (_abi.BunchMoments * self.wl.n_bunches)()
+        self._check(self.lib.cg_get_moments(self.h, out))
+        return out
+
+    # -- MPBeam stage methods ----------------------------------------------------
+    def MPBeamRMSCal(self, k: int):
+        self._check(self.lib.cg_beam_rms(self.h, k))
+
+    def SSBeamIonEffectOneInteractionPoint(self, turn: int, k: int):
+        self._check(self.lib.cg_beam_ion_ip(self.h, turn, k))
+
+    def BeamTransferPerInteractionPointDueToLatticeT(self, k: int):
+        self._check(self.lib.cg_section_map(self.h, k))
+
+    def BeamMomtumUpdateDueToRFTest(self):
+        self._check(self.lib.cg_rf_kick(self.h))
+
+    def BeamLongiPosTransferOneTurn(self):
+        self._check(self.lib.cg_longi_drift(self.h))
+
+    def BeamEnergyLossOneTurn(self):
+        self._check(self.lib.cg_energy_loss(self.h))
+
+    def BeamSynRadDamping(self, turn: int):
+        self._check(self.lib.cg_synrad(self.h, turn))
+
+    def LRWakeBeamIntaction(self):
+        self._check(self.lib.cg_lr_wake(self.h))
+
+    def SRWakeBeamIntaction(self, turn: int):
+        self._check(self.lib.cg_sr_wake(self.h, turn))
+
+    def FIRBunchByBunchFeedback(self, turn: int):
+        self._check(self.lib.cg_fir(self.h, turn))
+
+    def MarkParticleLostInBunch(self):
+        tr = np.empty(self.wl.n_bunches)
+        self._check(self.lib.cg_mark_lost(self.h, _abi.ptr(tr)))
+        return tr
+
+    def Run(self, turn0: int, n_turns: int):
+        self._check(self.lib.cg_run_turns(self.h, turn0, n_turns))
+
+    # -- ion clouds --------------------------------------------------------------
+    def ions(self, k: int, p: int = 0):
+        cap = int(self.wl.cfg.ion.max_ions) + 8
+        a = [np.empty(cap) for _ in range(4)]
+        n = C.c_int()
+        self._check(self.lib.cg_ion_download(self.h, k, p, *[_abi.ptr(x) for x in a], cap, C.byref(n)))
+        return [x[: n.value] for x in a]
+
+    def cloud_record(self, k: int):
+        out = np.empty((self.wl.n_bunches, max(1, self.wl.cfg.ion.n_species), 6))
+        self._check(self.lib.cg_ion_cloud_record(self.h, k, _abi.ptr(out)))
+        return out
+
+    def sr_bins(self, j: int):
+        zlo, dz = C.c_double(), C.c_double()
+        cnt = np.empty(int(self.wl.cfg.sr_bins), dtype=np.int32)
+        self._check(self.lib.cg_sr_bins(self.h, j, C.byref(zlo), C.byref(dz), _abi.ptr(cnt)))
+        return zlo.value, dz.value, cnt

@@ -1,0 +1,89 @@
+"""Builds libcetagpu.so (sm_100a) in-tree with nvcc.
+
+The library is a plain C-ABI shared object (include/cetasim_gpu.h); nothing in
+it depends on PyTorch.  Usage: ``python -m cetasim_b200.build`` or
+``cetasim_b200.build.build()``.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libcetagpu.so")
+
+SOURCES = ["capi.cu", "kernels.cu", "kernels_sr.cu", "faddeeva_table.cpp", "input_settings.cpp"]
+HEADERS = ["cg_common.cuh", "faddeeva.cuh", "be_field.cuh", "track_math.cuh", "cg_internal.h",
+           "kernels.cuh"]
+
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-lineinfo", "-O3", "-std=c++17",
+    "--compiler-options", "-fPIC",
+    "-Xptxas", "-O3",
+    "--expt-relaxed-constexpr",
+    "-rdc=false",
+]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
+        if cand and (os.path.isabs(cand) and os.path.exists(cand) or not os.path.isabs(cand)):
+            return cand
+    return "nvcc"
+
+
+def _stale(target: str, deps: list[str]) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = False) -> str:
+    deps = [os.path.join(CSRC, s) for s in SOURCES + HEADERS]
+    deps.append(os.path.join(ROOT, "include", "cetasim_gpu.h"))
+    if not force and not _stale(LIB, deps):
+        return LIB
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    objs = []
+    for src in SOURCES:
+        obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
+        cmd = [nvcc(), *NVCC_FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
+        if ptxas_verbose and src.endswith(".cu"):
+            cmd += ["-Xptxas", "-v"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+        objs.append(obj)
+    tmp = LIB + ".tmp"
+    cmd = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp, *objs,
+           "-lcudart_static", "-lrt", "-ldl", "-lpthread"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+def build_oracle(verbose: bool = False) -> None:
+    """Builds the CPU oracle (test infrastructure) and, when the reference
+    sources are present, its compiled w(z) under oracle/_ref."""
+    odir = os.path.join(ROOT, "oracle")
+    subprocess.run(["make", "-s", "-C", odir, "CC=gcc", "CXX=g++"], check=True,
+                   stdout=None if verbose else subprocess.DEVNULL)
+    ref_src = os.environ.get("CETASIM_REFERENCE", "/root/reference")
+    if os.path.exists(os.path.join(ref_src, "src", "Faddeeva.cpp")):
+        subprocess.run(["make", "-s", "-C", odir, "ref", f"REF={ref_src}", "CC=gcc", "CXX=g++"],
+                       check=True, stdout=None if verbose else subprocess.DEVNULL,
+                       stderr=subprocess.DEVNULL)
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True, ptxas_verbose="-v" in sys.argv)
+    build_oracle(verbose=True)
+    print(LIB)

@@ -1,0 +1,945 @@
+// C ABI of libcetagpu.so (declarations and reference citations in
+// include/cetasim_gpu.h).  Host-side orchestration: configuration, device
+// state, stage launches, the per-turn CUDA graph, status mapping.
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+#include "kernels.cuh"
+
+using namespace cg;
+
+namespace {
+
+thread_local std::string g_create_error;
+std::mutex g_table_mu;
+bool g_table_host_ready = false;
+bool g_table_dev_ready[64] = {false};
+
+int fail(Handle* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  else g_create_error = msg;
+  return code;
+}
+
+int cuda_fail(Handle* h, cudaError_t e, const char* where) {
+  return fail(h, CG_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CG_CUDA(h, call)                               \
+  do {                                                 \
+    cudaError_t _e = (call);                           \
+    if (_e != cudaSuccess) return cuda_fail(h, _e, #call); \
+  } while (0)
+
+template <class T>
+cudaError_t dalloc(T** p, size_t count) {
+  return cudaMalloc((void**)p, count * sizeof(T) > 0 ? count * sizeof(T) : 16);
+}
+
+void dfree(void* p) {
+  if (p) cudaFree(p);
+}
+
+int ensure_weideman(int device) {
+  std::lock_guard<std::mutex> lk(g_table_mu);
+  if (!g_table_host_ready) {
+    weideman_table_init(&h_weideman);
+    g_table_host_ready = true;
+  }
+  if (device >= 0 && device < 64 && !g_table_dev_ready[device]) {
+    cudaError_t e = upload_weideman_table();
+    if (e != cudaSuccess) return (int)e;
+    g_table_dev_ready[device] = true;
+  }
+  return 0;
+}
+
+// Reads the device status word and maps it to a cg_status.
+int check_status(Handle& h) {
+  cudaError_t e = cudaStreamSynchronize(h.stream);
+  if (e != cudaSuccess) return cuda_fail(&h, e, "cudaStreamSynchronize");
+  int st = 0;
+  e = cudaMemcpy(&st, h.d.status, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(&h, e, "status read");
+  if (st == 0) return CG_OK;
+  cudaMemset(h.d.status, 0, sizeof(int));
+  if (st & kStatusIonOverflow)
+    return fail(&h, CG_ERR_ION_OVERFLOW,
+                "the accumulated ions at an interaction point exceed ionCalIonMaxNumber");
+  if (st & kStatusTransmission)
+    return fail(&h, CG_ERR_TRANSMISSION, "a bunch lost more than 50% of its particles");
+  if (st & kStatusLrRange)
+    return fail(&h, CG_ERR_INVALID, "long-range wake lag outside the wake table (tau > 0)");
+  return fail(&h, CG_ERR_CUDA, "unknown device status");
+}
+
+int launch_ok(Handle& h, cudaError_t e, const char* what) {
+  if (e != cudaSuccess) return cuda_fail(&h, e, what);
+  return CG_OK;
+}
+
+void free_beam(Handle& h) {
+  DeviceBufs& d = h.d;
+  dfree(d.c); dfree(d.surv); dfree(d.tile_bunch); dfree(d.bunch); dfree(d.partials);
+  dfree(d.counters); dfree(d.mom); dfree(d.loss_count); dfree(d.scratch);
+  dfree(d.rec); dfree(d.lr_hist); dfree(d.lr_force); dfree(d.fir_hist); dfree(d.fir_kick);
+  dfree(d.sr_geom); dfree(d.sr_counts); dfree(d.sr_sumx); dfree(d.sr_sumy); dfree(d.sr_lag);
+  dfree(d.sr_pot);
+  d.c = nullptr; d.surv = nullptr; d.tile_bunch = nullptr; d.bunch = nullptr; d.partials = nullptr;
+  d.counters = nullptr; d.mom = nullptr; d.loss_count = nullptr; d.scratch = nullptr;
+  d.rec = nullptr; d.lr_hist = nullptr; d.lr_force = nullptr; d.fir_hist = nullptr;
+  d.fir_kick = nullptr; d.sr_geom = nullptr; d.sr_counts = nullptr; d.sr_sumx = nullptr;
+  d.sr_sumy = nullptr; d.sr_lag = nullptr; d.sr_pot = nullptr;
+  if (h.turn_graph) {
+    cudaGraphExecDestroy(h.turn_graph);
+    h.turn_graph = nullptr;
+  }
+  h.beam_set = false;
+}
+
+// WakeFunction::GetBBRWakeFun (WakeFunction.cpp:655-721) for the LR table.
+void bbr_wake(const cg_bbr& w, double bx, double by, double tau, double out[3]) {
+  out[0] = out[1] = out[2] = 0;
+  for (int i = 0; i < w.n; i++) {
+    double alpha = w.tx_omega[i] / 2.0 / w.tx_q[i];
+    double omegab = std::sqrt(std::pow(w.tx_omega[i], 2) - std::pow(alpha, 2));
+    double coeff = kCLight * w.tx_rs[i] * w.tx_omega[i] / w.tx_q[i] / omegab *
+                   std::exp(alpha * tau) * std::sin(omegab * tau);
+    out[0] += coeff / bx;
+    alpha = w.ty_omega[i] / 2.0 / w.ty_q[i];
+    omegab = std::sqrt(std::pow(w.ty_omega[i], 2) - std::pow(alpha, 2));
+    coeff = kCLight * w.ty_rs[i] * w.ty_omega[i] / w.ty_q[i] / omegab * std::exp(alpha * tau) *
+            std::sin(omegab * tau);
+    out[1] += coeff / by;
+  }
+  for (int i = 0; i < w.n; i++) {
+    double alpha = w.l_omega[i] / 2.0 / w.l_q[i];
+    double omegab = std::sqrt(std::pow(w.l_omega[i], 2) - std::pow(alpha, 2));
+    double coeff = 2 * alpha * w.l_rs[i] * std::exp(alpha * tau);
+    double c1 = std::cos(omegab * tau);
+    double c2 = std::sin(omegab * tau) * alpha / omegab;
+    if (tau == 0) out[2] += coeff / 2;
+    else out[2] += coeff * (c1 + c2);
+  }
+}
+
+SectionDev make_section_dev(const cg_section& s, const cg_ring& r) {
+  SectionDev d;
+  d.beta_x = s.beta_x; d.alpha_x = s.alpha_x; d.beta_y = s.beta_y; d.alpha_y = s.alpha_y;
+  d.eta_x = s.eta_x; d.etap_x = s.etap_x; d.eta_y = s.eta_y; d.etap_y = s.etap_y;
+  d.phase_adv_x = s.phase_adv_x; d.phase_adv_y = s.phase_adv_y;
+  d.weigh_x = s.phase_adv_x / (2 * kPi * r.work_qx);
+  d.weigh_y = s.phase_adv_y / (2 * kPi * r.work_qy);
+  d.aperture_x = s.aperture_x; d.aperture_y = s.aperture_y;
+  std::memcpy(d.b1h1, s.map_b1h1, sizeof d.b1h1);
+  std::memcpy(d.h1b1, s.map_h1b1, sizeof d.h1b1);
+  std::memcpy(d.h2b2, s.map_h2b2, sizeof d.h2b2);
+  return d;
+}
+
+RingDev make_ring_dev(const cg_config& c, const cg_section& s0) {
+  const cg_ring& r = c.ring;
+  RingDev d;
+  std::memset(&d, 0, sizeof d);
+  d.chrom[0] = r.chrom[0]; d.chrom[1] = r.chrom[1];
+  for (int i = 0; i < 5; ++i) { d.adtx[i] = r.adtx[i]; d.adty[i] = r.adty[i]; }
+  d.circ_ring = r.circ_ring;
+  for (int i = 0; i < 3; ++i) d.alphac[i] = r.alphac[i];
+  d.energy = r.electron_energy;
+  d.r_beta2 = std::pow(r.r_beta, 2);
+  d.u0_term = r.u0 / r.electron_energy / std::pow(r.r_beta, 2);
+  double fRF = r.f0 * r.harmonics;
+  d.n_cav = r.n_cav;
+  for (int i = 0; i < r.n_cav && i < 4; ++i) {
+    d.rf_theta_coeff[i] = 1.0 / kCLight / r.r_beta * 2. * kPi * (double)r.cav_harm[i] * fRF;
+    d.vreq_re[i] = r.cav_vreq_re[i];
+    d.vreq_im[i] = r.cav_vreq_im[i];
+  }
+  for (int i = 0; i < 3; ++i) d.lambda[i] = std::exp(-1.0 / r.synch_rad_damp_time[i]);
+  d.qe_coeff[0] = std::sqrt(1 - std::pow(d.lambda[0], 2)) * std::sqrt(r.emit_nat[0]);
+  d.qe_coeff[1] = std::sqrt(1 - std::pow(d.lambda[1], 2)) * std::sqrt(r.emit_nat[1]);
+  d.qe_coeff[2] = std::sqrt(1 - std::pow(d.lambda[2], 4)) * std::sqrt(r.emit_nat[2]);
+  d.z_loss = r.t0 * kCLight / r.harmonics / 2;
+  d.r_gamma = r.r_gamma;
+  (void)s0;
+  return d;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cg_abi_version(void) { return CG_ABI_VERSION; }
+
+// ReadInputSettings.cpp:986-1081 and CavityResonator.cpp:121-131.
+int cg_config_derive(cg_config* cfg) {
+  if (!cfg) return fail(nullptr, CG_ERR_INVALID, "cfg is NULL");
+  cg_ring* r = &cfg->ring;
+  if (r->n_cav < 1 || r->n_cav > CG_MAX_CAVITIES)
+    return fail(nullptr, CG_ERR_INVALID, "rfResNum must be in [1, 4]");
+  const double PI = 4 * std::atan(1.E0);
+  double rGamma = r->electron_energy / kElectronMassEV;
+  double eta = r->alphac[0] - 1. / std::pow(rGamma, 2);
+  double rBeta = std::sqrt(1.E0 - std::pow(rGamma, -2));
+  double t0 = r->circ_ring / kCLight / rBeta;
+  double f0 = 1 / t0;
+  double vRF = r->cav_vol[0];
+  double synPhase = PI - std::asin(r->u0 / vRF);
+  double workQz = std::sqrt(-1 * eta * r->harmonics * vRF * std::cos(synPhase) /
+                            (2 * PI * rBeta * r->electron_energy));
+  r->r_gamma = rGamma; r->r_beta = rBeta; r->t0 = t0; r->f0 = f0; r->eta = eta;
+  r->work_qz = workQz;
+  r->natural_bunch_length = eta * kCLight * r->sdelta0 / (2 * PI * workQz * f0);
+  r->emit_nat[0] = r->natural_emit / (1 + r->coupling);
+  r->emit_nat[1] = r->natural_emit / (1 + r->coupling) * r->coupling;
+  r->emit_nat[2] = r->natural_bunch_length * r->sdelta0;
+  r->beta_z = r->natural_bunch_length / r->sdelta0;
+  double ph[CG_MAX_CAVITIES];
+  for (int i = 0; i < r->n_cav; ++i) ph[i] = r->cav_phase[i];
+  if (r->n_cav == 1) ph[0] = PI - std::asin(r->u0 / r->cav_vol[0]) - PI / 2.;
+  for (int i = 0; i < r->n_cav; ++i) {
+    r->cav_vreq_re[i] = r->cav_vol[i] * std::cos(ph[i]);
+    r->cav_vreq_im[i] = r->cav_vol[i] * std::sin(ph[i]);
+  }
+  return CG_OK;
+}
+
+// gsl_blas_dgemm(NoTrans, NoTrans) order: inner index ascending, zero A
+// entries skipped, accumulation from 0.
+static void dgemm66(const double* A, const double* B, double* C) {
+  for (int i = 0; i < 36; ++i) C[i] = 0.0;
+  for (int i = 0; i < 6; ++i)
+    for (int k = 0; k < 6; ++k) {
+      double t = A[6 * i + k];
+      if (t != 0.0)
+        for (int j = 0; j < 6; ++j) C[6 * i + j] += t * B[6 * k + j];
+    }
+}
+
+// LIP.cpp:242-283 (apertures, lengths, phase advances) and LIP.cpp:326-433.
+int cg_lattice_init(const cg_ring* ring, cg_section* sec, int n) {
+  if (!ring || !sec || n < 1) return fail(nullptr, CG_ERR_INVALID, "bad lattice arguments");
+  const double PI = 4 * std::atan(1.E0);
+  for (int i = 0; i < n; ++i) {
+    if (!(ring->pipe_aperture_x > sec[i].aperture_x)) sec[i].aperture_x = ring->pipe_aperture_x;
+    if (!(ring->pipe_aperture_y > sec[i].aperture_y)) sec[i].aperture_y = ring->pipe_aperture_y;
+  }
+  for (int i = 0; i < n; ++i) {
+    if (i != n - 1) {
+      sec[i].length = sec[i + 1].s - sec[i].s;
+      sec[i].phase_adv_x = sec[i + 1].psi_x - sec[i].psi_x;
+      sec[i].phase_adv_y = sec[i + 1].psi_y - sec[i].psi_y;
+    } else {
+      sec[i].length = ring->circ_ring - sec[i].s + sec[0].s;
+      sec[i].phase_adv_x = 2 * PI * ring->work_qx - sec[i].psi_x + sec[0].psi_x;
+      sec[i].phase_adv_y = 2 * PI * ring->work_qy - sec[i].psi_y + sec[0].psi_y;
+    }
+  }
+  const double bz = ring->beta_z;
+  for (int i = 0; i < n; ++i) {
+    const cg_section& a = sec[i];
+    const cg_section& b = sec[i < n - 1 ? i + 1 : 0];
+    double H1[36] = {0}, IH1[36] = {0}, IH2[36] = {0}, B1[36] = {0}, IB1[36] = {0}, IB2[36] = {0};
+    for (int d = 0; d < 6; ++d) H1[7 * d] = IH1[7 * d] = IH2[7 * d] = 1.0;
+    auto M = [](double* A, int r, int c) -> double& { return A[6 * r + c]; };
+    M(H1, 0, 5) = -a.eta_x; M(H1, 1, 5) = -a.etap_x; M(H1, 2, 5) = -a.eta_y; M(H1, 3, 5) = -a.etap_y;
+    M(H1, 4, 0) = a.etap_x; M(H1, 4, 1) = -a.eta_x; M(H1, 4, 2) = a.etap_y; M(H1, 4, 3) = -a.eta_y;
+    M(IH1, 0, 5) = a.eta_x; M(IH1, 1, 5) = a.etap_x; M(IH1, 2, 5) = a.eta_y; M(IH1, 3, 5) = a.etap_y;
+    M(IH1, 4, 0) = -a.etap_x; M(IH1, 4, 1) = a.eta_x; M(IH1, 4, 2) = -a.etap_y; M(IH1, 4, 3) = a.eta_y;
+    M(IH2, 0, 5) = b.eta_x; M(IH2, 1, 5) = b.etap_x; M(IH2, 2, 5) = b.eta_y; M(IH2, 3, 5) = b.etap_y;
+    M(IH2, 4, 0) = -b.etap_x; M(IH2, 4, 1) = b.eta_x; M(IH2, 4, 2) = -b.etap_y; M(IH2, 4, 3) = b.eta_y;
+    M(B1, 0, 0) = 1 / std::sqrt(a.beta_x); M(B1, 1, 0) = a.alpha_x / std::sqrt(a.beta_x);
+    M(B1, 1, 1) = std::sqrt(a.beta_x);
+    M(B1, 2, 2) = 1 / std::sqrt(a.beta_y); M(B1, 3, 2) = a.alpha_y / std::sqrt(a.beta_y);
+    M(B1, 3, 3) = std::sqrt(a.beta_y);
+    M(B1, 4, 4) = 1 / std::sqrt(bz); M(B1, 5, 5) = std::sqrt(bz);
+    M(IB1, 0, 0) = std::sqrt(a.beta_x); M(IB1, 1, 0) = -a.alpha_x / std::sqrt(a.beta_x);
+    M(IB1, 1, 1) = 1 / std::sqrt(a.beta_x);
+    M(IB1, 2, 2) = std::sqrt(a.beta_y); M(IB1, 3, 2) = -a.alpha_y / std::sqrt(a.beta_y);
+    M(IB1, 3, 3) = 1 / std::sqrt(a.beta_y);
+    M(IB1, 4, 4) = std::sqrt(bz); M(IB1, 5, 5) = 1 / std::sqrt(bz);
+    M(IB2, 0, 0) = std::sqrt(b.beta_x); M(IB2, 1, 0) = -b.alpha_x / std::sqrt(b.beta_x);
+    M(IB2, 1, 1) = 1 / std::sqrt(b.beta_x);
+    M(IB2, 2, 2) = std::sqrt(b.beta_y); M(IB2, 3, 2) = -b.alpha_y / std::sqrt(b.beta_y);
+    M(IB2, 3, 3) = 1 / std::sqrt(b.beta_y);
+    M(IB2, 4, 4) = std::sqrt(bz); M(IB2, 5, 5) = 1 / std::sqrt(bz);
+    dgemm66(B1, H1, sec[i].map_b1h1);
+    dgemm66(IH1, IB1, sec[i].map_h1b1);
+    dgemm66(IH2, IB2, sec[i].map_h2b2);
+  }
+  return CG_OK;
+}
+
+int cg_create(const cg_config* cfg, int device, cg_handle** out) {
+  if (!cfg || !out) return fail(nullptr, CG_ERR_INVALID, "NULL argument");
+  *out = nullptr;
+  if (cfg->n_sections < 1 || !cfg->sections)
+    return fail(nullptr, CG_ERR_INVALID, "ringSectNum must be >= 1 with sections");
+  if (cfg->ring.skew_quad_k != 0.0)
+    return fail(nullptr, CG_ERR_UNSUPPORTED, "ringskewQuadK != 0 is not supported");
+  if (cfg->ring.n_cav < 1 || cfg->ring.n_cav > CG_MAX_CAVITIES)
+    return fail(nullptr, CG_ERR_INVALID, "rfResNum must be in [1, 4]");
+  if (cfg->flag_beam_ion &&
+      (cfg->ion.n_species < 1 || cfg->ion.n_species > CG_MAX_SPECIES || cfg->ion.max_ions < 1 ||
+       cfg->ion.macro_ions_per_ip < 1))
+    return fail(nullptr, CG_ERR_INVALID, "bad ion settings");
+  if (cfg->flag_sr_wake && (cfg->sr_bins < 1 || cfg->sr_bins > 2048 || cfg->sr_bbr.n < 1))
+    return fail(nullptr, CG_ERR_INVALID, "SRWBunchBinNum must be in [1, 2048] with resonators");
+  if (cfg->flag_lr_wake && (cfg->lr_turns < 2 || cfg->lr_bbr.n < 1))
+    return fail(nullptr, CG_ERR_INVALID, "LR wake needs >= 1 truncation turn and resonators");
+  if (cfg->flag_fir && cfg->fir.mode != 0 &&
+      (cfg->fir.delay + cfg->fir.taps < 1 || cfg->fir.delay + cfg->fir.taps > CG_MAX_FIR))
+    return fail(nullptr, CG_ERR_INVALID, "fbDelay + fbTaps must be in [1, 64]");
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0)
+    return fail(nullptr, CG_ERR_CUDA, "no CUDA device available (the library has no CPU path)");
+  if (device < 0 || device >= ndev) return fail(nullptr, CG_ERR_INVALID, "bad device index");
+  e = cudaSetDevice(device);
+  if (e != cudaSuccess) return fail(nullptr, CG_ERR_CUDA, cudaGetErrorString(e));
+  if (ensure_weideman(device)) return fail(nullptr, CG_ERR_CUDA, "Weideman table upload failed");
+
+  cg_handle* H = new cg_handle();
+  Handle& h = H->h;
+  h.cfg = *cfg;
+  h.device = device;
+  h.K = cfg->n_sections;
+  h.P = cfg->ion.n_species > 0 ? cfg->ion.n_species : 1;
+  h.sections.assign(cfg->sections, cfg->sections + h.K);
+  h.cfg.sections = h.sections.data();
+  for (int k = 0; k < h.K; ++k) h.sec_dev_host.push_back(make_section_dev(h.sections[k], cfg->ring));
+  h.ring = make_ring_dev(*cfg, h.sections[0]);
+  ChainParams& cp = h.chain;
+  std::memset(&cp, 0, sizeof cp);
+  for (int p = 0; p < h.P && p < CG_MAX_SPECIES; ++p) {
+    cp.cross_section[p] = cfg->ion.cross_section[p];
+    cp.gas_percent[p] = cfg->ion.gas_percent[p];
+    cp.mass_number[p] = cfg->ion.mass_number[p];
+  }
+  cp.loss_boundary = cfg->ion.loss_boundary;
+  cp.circ_ring = cfg->ring.circ_ring;
+  cp.harmonics = cfg->ring.harmonics;
+  cp.r_gamma = cfg->ring.r_gamma;
+  cp.n_species = h.P;
+  cp.macro_per_ip = cfg->ion.macro_ions_per_ip;
+  cp.max_ions = cfg->ion.max_ions;
+  cp.seed = cfg->seed;
+
+  auto bail = [&](int code, const std::string& msg) {
+    g_create_error = msg;
+    cg_destroy(H);
+    return code;
+  };
+  if ((e = cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking)) != cudaSuccess)
+    return bail(CG_ERR_CUDA, cudaGetErrorString(e));
+  if ((e = dalloc(&h.sec_dev, h.K)) != cudaSuccess) return bail(CG_ERR_OOM, "sections");
+  cudaMemcpy(h.sec_dev, h.sec_dev_host.data(), sizeof(SectionDev) * h.K, cudaMemcpyHostToDevice);
+  if ((e = dalloc(&h.d.status, 4)) != cudaSuccess) return bail(CG_ERR_OOM, "status");
+  cudaMemset(h.d.status, 0, 4 * sizeof(int));
+  if ((e = dalloc(&h.d.turn, 1)) != cudaSuccess) return bail(CG_ERR_OOM, "turn");
+  cudaMemset(h.d.turn, 0, sizeof(int));
+
+  // ion clouds: ping-pong buffers per (IP, species)
+  if (cfg->flag_beam_ion) {
+    h.ion_cap = cfg->ion.max_ions + cfg->ion.macro_ions_per_ip + 1;
+    std::vector<CloudDev> cl(h.K * h.P);
+    for (auto& c : cl) {
+      c.cap = h.ion_cap;
+      for (int b = 0; b < 2; ++b) {
+        if (dalloc(&c.x[b], h.ion_cap) || dalloc(&c.y[b], h.ion_cap) ||
+            dalloc(&c.vx[b], h.ion_cap) || dalloc(&c.vy[b], h.ion_cap))
+          return bail(CG_ERR_OOM, "ion cloud buffers");
+      }
+    }
+    if (dalloc(&h.d.clouds, cl.size())) return bail(CG_ERR_OOM, "clouds");
+    cudaMemcpy(h.d.clouds, cl.data(), sizeof(CloudDev) * cl.size(), cudaMemcpyHostToDevice);
+    if (dalloc(&h.d.cloud_state, cl.size())) return bail(CG_ERR_OOM, "cloud state");
+    cudaMemset(h.d.cloud_state, 0, sizeof(CloudState) * cl.size());
+  }
+  // long-range wake table (WakeFunction::InitialLRWake, WakeFunction.cpp:49-202)
+  if (cfg->flag_lr_wake) {
+    int turns = cfg->lr_turns;
+    double trf = cfg->ring.t0 / cfg->ring.harmonics;
+    double dt = trf / 2;
+    int np = int(turns * cfg->ring.harmonics * trf / dt) + 2;
+    std::vector<double> tab(3 * (size_t)np);
+    for (int i = 0; i < np; ++i) {
+      double w[3];
+      bbr_wake(cfg->lr_bbr, h.sections[0].beta_x, h.sections[0].beta_y, -i * dt, w);
+      for (int d = 0; d < 3; ++d) tab[(size_t)d * np + i] = w[d];
+    }
+    h.lr_np = np;
+    h.lr_dt = (1 * dt) - (0 * dt);
+    if (dalloc(&h.d.lr_tab, tab.size())) return bail(CG_ERR_OOM, "LR table");
+    cudaMemcpy(h.d.lr_tab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice);
+    if (dalloc(&h.d.lr_head, 1)) return bail(CG_ERR_OOM, "LR head");
+    cudaMemset(h.d.lr_head, 0, sizeof(int));
+  }
+  if (cfg->flag_fir) {
+    const cg_fir_params& f = cfg->fir;
+    h.fir_order = f.mode == 0 ? 1 : f.delay + f.taps;
+    h.fir_limit = std::sqrt(2 * f.power_limit * f.kicker_imped) / cfg->ring.electron_energy;
+    std::vector<double> co(3 * (size_t)h.fir_order, 0.0);
+    for (int q = 0; q < h.fir_order && f.mode != 0; ++q) {
+      co[q] = f.coeff_x[q];
+      co[h.fir_order + q] = f.coeff_y[q];
+      co[2 * h.fir_order + q] = f.coeff_z[q];
+    }
+    if (dalloc(&h.d.fir_coeff, co.size())) return bail(CG_ERR_OOM, "FIR");
+    cudaMemcpy(h.d.fir_coeff, co.data(), sizeof(double) * co.size(), cudaMemcpyHostToDevice);
+    if (dalloc(&h.d.fir_head, 1)) return bail(CG_ERR_OOM, "FIR head");
+    cudaMemset(h.d.fir_head, 0, sizeof(int));
+  }
+  // short-range wake: per-resonator constants and u-independent factors
+  // (GetBBRPusdoWakeFun, WakeFunction.cpp:573-601)
+  if (cfg->flag_sr_wake) {
+    const int NZ = 1000;
+    const cg_bbr& w = cfg->sr_bbr;
+    std::vector<double> buf(3 * CG_MAX_RESONATORS + (size_t)w.n * NZ, 0.0);
+    const double PI = 4 * std::atan(1.E0);
+    double sigmat = 1.e-3 / kCLight;
+    double sigmaz = sigmat * kCLight;
+    for (int r = 0; r < w.n; ++r) {
+      double q = w.l_q[r];
+      double vz = w.l_omega[r] * sigmaz / kCLight;
+      double zMax = 3 * vz / (2 * q);
+      double dz = zMax / NZ;
+      buf[3 * r + 0] = dz;
+      buf[3 * r + 1] = 2 * q / vz;
+      buf[3 * r + 2] = std::sqrt(2. / PI) * w.l_rs[r] * kCLight / sigmaz;
+      double a = std::sqrt(4 * q * q - 1);
+      for (int j = 0; j < NZ; ++j) {
+        double z = j * dz;
+        buf[3 * CG_MAX_RESONATORS + (size_t)r * NZ + j] = std::cos(z * a) - std::sin(z * a) / a;
+      }
+    }
+    if (dalloc(&h.d.sr_green, buf.size())) return bail(CG_ERR_OOM, "SR green");
+    cudaMemcpy(h.d.sr_green, buf.data(), sizeof(double) * buf.size(), cudaMemcpyHostToDevice);
+  }
+  if ((e = cudaDeviceSynchronize()) != cudaSuccess) return bail(CG_ERR_CUDA, cudaGetErrorString(e));
+  *out = H;
+  return CG_OK;
+}
+
+int cg_destroy(cg_handle* H) {
+  if (!H) return CG_OK;
+  Handle& h = H->h;
+  cudaSetDevice(h.device);
+  free_beam(h);
+  dfree(h.sec_dev); dfree(h.d.status); dfree(h.d.turn);
+  if (h.d.clouds) {
+    std::vector<CloudDev> cl(h.K * h.P);
+    cudaMemcpy(cl.data(), h.d.clouds, sizeof(CloudDev) * cl.size(), cudaMemcpyDeviceToHost);
+    for (auto& c : cl)
+      for (int b = 0; b < 2; ++b) { dfree(c.x[b]); dfree(c.y[b]); dfree(c.vx[b]); dfree(c.vy[b]); }
+    dfree(h.d.clouds);
+  }
+  dfree(h.d.cloud_state); dfree(h.d.lr_tab); dfree(h.d.lr_head); dfree(h.d.fir_coeff);
+  dfree(h.d.fir_head); dfree(h.d.sr_green);
+  if (h.stream) cudaStreamDestroy(h.stream);
+  delete H;
+  return CG_OK;
+}
+
+const char* cg_last_error(const cg_handle* H) {
+  if (!H) return g_create_error.c_str();
+  return H->h.err.c_str();
+}
+
+// MPBeam::Initial (MPBeam.cpp:64-188): layout, gaps, charges.
+int cg_set_beam(cg_handle* H, int M, const int* n_macro, const int* harm, const double* ne) {
+  if (!H || M < 1 || !n_macro || !harm || !ne) return fail(H ? &H->h : nullptr, CG_ERR_INVALID, "bad beam arguments");
+  Handle& h = H->h;
+  cudaSetDevice(h.device);
+  free_beam(h);
+  const int Hh = h.cfg.ring.harmonics;
+  for (int j = 0; j < M; ++j) {
+    if (n_macro[j] < 1) return fail(&h, CG_ERR_INVALID, "each bunch needs >= 1 macroparticle");
+    if (harm[j] < 0 || harm[j] >= Hh) return fail(&h, CG_ERR_INVALID, "bunch harmonic number out of range");
+    if (j > 0 && harm[j] <= harm[j - 1]) return fail(&h, CG_ERR_INVALID, "bunch harmonic numbers must increase");
+  }
+  h.M = M;
+  h.n_macro.assign(n_macro, n_macro + M);
+  h.harm.assign(harm, harm + M);
+  h.ne.assign(ne, ne + M);
+  h.gap.assign(M, 0);
+  for (int j = 0; j < M - 1; ++j) h.gap[j] = harm[j + 1] - harm[j];
+  h.gap[M - 1] = Hh - harm[M - 1];
+  std::vector<BunchDev> bd(M);
+  std::vector<int> tb;
+  h.tile_off.assign(M + 1, 0);
+  int tiles = 0;
+  for (int j = 0; j < M; ++j) {
+    int nt = (n_macro[j] + kTile - 1) / kTile;
+    bd[j].n = n_macro[j];
+    bd[j].tile_off = tiles;
+    bd[j].n_tiles = nt;
+    bd[j].harm = harm[j];
+    bd[j].gap = h.gap[j];
+    bd[j].pad = 0;
+    bd[j].ne = ne[j];
+    bd[j].q_macro = ne[j] / n_macro[j];
+    h.tile_off[j] = tiles;
+    for (int t = 0; t < nt; ++t) tb.push_back(j);
+    tiles += nt;
+  }
+  h.tile_off[M] = tiles;
+  h.n_tiles = tiles;
+  h.npad = (int64_t)tiles * kTile;
+  DeviceBufs& d = h.d;
+  if (dalloc(&d.c, 6 * (size_t)h.npad) || dalloc(&d.surv, (size_t)h.npad) ||
+      dalloc(&d.tile_bunch, tiles) || dalloc(&d.bunch, M) || dalloc(&d.partials, tiles) ||
+      dalloc(&d.counters, M + 1) || dalloc(&d.mom, M) || dalloc(&d.loss_count, M + 1)) {
+    free_beam(h);
+    return fail(&h, CG_ERR_OOM, "beam allocation failed");
+  }
+  d.scratch_bytes = sizeof(double) * std::max<size_t>(2 * (size_t)tiles, 1024);
+  if (cudaMalloc((void**)&d.scratch, d.scratch_bytes) != cudaSuccess) {
+    free_beam(h);
+    return fail(&h, CG_ERR_OOM, "scratch allocation failed");
+  }
+  cudaMemset(d.c, 0, sizeof(double) * 6 * h.npad);
+  cudaMemset(d.surv, 0xFF, h.npad);
+  cudaMemcpy(d.tile_bunch, tb.data(), sizeof(int) * tiles, cudaMemcpyHostToDevice);
+  cudaMemcpy(d.bunch, bd.data(), sizeof(BunchDev) * M, cudaMemcpyHostToDevice);
+  cudaMemset(d.counters, 0, sizeof(unsigned) * (M + 1));
+  cudaMemset(d.loss_count, 0, sizeof(int) * (M + 1));
+  std::vector<BunchMomDev> m0(M);
+  std::memset(m0.data(), 0, sizeof(BunchMomDev) * M);
+  for (auto& m : m0) m.transmission = 1.0;
+  cudaMemcpy(d.mom, m0.data(), sizeof(BunchMomDev) * M, cudaMemcpyHostToDevice);
+  if (h.cfg.flag_beam_ion) {
+    if (dalloc(&d.rec, (size_t)h.K * M * h.P)) { free_beam(h); return fail(&h, CG_ERR_OOM, "ion records"); }
+    cudaMemset(d.rec, 0, sizeof(CloudRec) * h.K * M * h.P);
+  }
+  if (h.cfg.flag_lr_wake) {
+    if (dalloc(&d.lr_hist, (size_t)h.cfg.lr_turns * 3 * M) || dalloc(&d.lr_force, 3 * (size_t)M)) {
+      free_beam(h);
+      return fail(&h, CG_ERR_OOM, "LR history");
+    }
+    cudaMemset(d.lr_hist, 0, sizeof(double) * h.cfg.lr_turns * 3 * M);
+    cudaMemset(d.lr_force, 0, sizeof(double) * 3 * M);
+    cudaMemset(d.lr_head, 0, sizeof(int));
+  } else {
+    if (dalloc(&d.lr_force, 3 * (size_t)M)) { free_beam(h); return fail(&h, CG_ERR_OOM, "LR force"); }
+    cudaMemset(d.lr_force, 0, sizeof(double) * 3 * M);
+  }
+  if (dalloc(&d.fir_kick, 3 * (size_t)M)) { free_beam(h); return fail(&h, CG_ERR_OOM, "FIR kick"); }
+  cudaMemset(d.fir_kick, 0, sizeof(double) * 3 * M);
+  if (h.cfg.flag_fir) {
+    if (dalloc(&d.fir_hist, (size_t)h.fir_order * 3 * M)) { free_beam(h); return fail(&h, CG_ERR_OOM, "FIR history"); }
+    cudaMemset(d.fir_hist, 0, sizeof(double) * h.fir_order * 3 * M);
+    cudaMemset(h.d.fir_head, 0, sizeof(int));
+  }
+  if (h.cfg.flag_sr_wake) {
+    int B = h.cfg.sr_bins;
+    if (dalloc(&d.sr_geom, 2 * (size_t)M) || dalloc(&d.sr_counts, (size_t)M * B) ||
+        dalloc(&d.sr_sumx, (size_t)M * B) || dalloc(&d.sr_sumy, (size_t)M * B) ||
+        dalloc(&d.sr_lag, (size_t)M * (2 * B - 1)) || dalloc(&d.sr_pot, (size_t)M * B)) {
+      free_beam(h);
+      return fail(&h, CG_ERR_OOM, "SR buffers");
+    }
+    cudaMemset(d.sr_pot, 0, sizeof(double) * M * B);
+  }
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return cuda_fail(&h, e, "cg_set_beam");
+  h.beam_set = true;
+  return CG_OK;
+}
+
+int cg_upload_bunch(cg_handle* H, int j, const double* x, const double* px, const double* y,
+                    const double* py, const double* z, const double* dp, const uint8_t* surv) {
+  if (!H) return CG_ERR_INVALID;
+  Handle& h = H->h;
+  if (!h.beam_set) return fail(&h, CG_ERR_NOT_READY, "cg_set_beam first");
+  if (j < 0 || j >= h.M) return fail(&h, CG_ERR_INVALID, "bunch index out of range");
+  cudaSetDevice(h.device);
+  const double* src[6] = {x, px, y, py, z, dp};
+  int64_t off = (int64_t)h.tile_off[j] * kTile;
+  size_t n = h.n_macro[j];
+  for (int d = 0; d < 6; ++d) {
+    if (!src[d]) return fail(&h, CG_ERR_INVALID, "NULL coordinate array");
+    CG_CUDA(&h, cudaMemcpyAsync(h.d.c + d * h.npad + off, src[d], n * sizeof(double),
+                                cudaMemcpyHostToDevice, h.stream));
+  }
+  if (surv) CG_CUDA(&h, cudaMemcpyAsync(h.d.surv + off, surv, n, cudaMemcpyHostToDevice, h.stream));
+  else CG_CUDA(&h, cudaMemsetAsync(h.d.surv + off, 0, n, h.stream));
+  CG_CUDA(&h, cudaStreamSynchronize(h.stream));
+  return CG_OK;
+}
+
+int cg_download_bunch(cg_handle* H, int j, double* x, double* px, double* y, double* py,
+                      double* z, double* dp, uint8_t* surv) {
+  if (!H) return CG_ERR_INVALID;
+  Handle& h = H->h;
+  if (!h.beam_set) return fail(&h, CG_ERR_NOT_READY, "cg_set_beam first");
+  if (j < 0 || j >= h.M) return fail(&h, CG_ERR_INVALID, "bunch index out of range");
+  cudaSetDevice(h.device);
+  double* dst[6] = {x, px, y, py, z, dp};
+  int64_t off = (int64_t)h.tile_off[j] * kTile;
+  size_t n = h.n_macro[j];
+  for (int d = 0; d < 6; ++d)
+    if (dst[d])
+      CG_CUDA(&h, cudaMemcpyAsync(dst[d], h.d.c + d * h.npad + off, n * sizeof(double),
+                                  cudaMemcpyDeviceToHost, h.stream));
+  if (surv) CG_CUDA(&h, cudaMemcpyAsync(surv, h.d.surv + off, n, cudaMemcpyDeviceToHost, h.stream));
+  CG_CUDA(&h, cudaStreamSynchronize(h.stream));
+  return CG_OK;
+}
+
+int cg_generate_gaussian(cg_handle* H, double emit_x, double emit_y, double sigma_z,
+                         double sigma_dp, uint64_t seed) {
+  if (!H) return CG_ERR_INVALID;
+  Handle& h = H->h;
+  if (!h.beam_set) return fail(&h, CG_ERR_NOT_READY, "cg_set_beam first");
+  cudaSetDevice(h.device);
+  int st = launch_ok(h, launch_gaussian(h, emit_x, emit_y, sigma_z, sigma_dp, seed), "gaussian");
+  if (st) return st;
+  return check_status(h);
+}
+
+#define STAGE_PROLOGUE                                                              \
+  if (!H) return CG_ERR_INVALID;                                                    \
+  Handle& h = H->h;                                                                 \
+  if (!h.beam_set) return fail(&h, CG_ERR_NOT_READY, "cg_set_beam first");          \
+  cudaSetDevice(h.device);
+
+int cg_beam_rms(cg_handle* H, int k) {
+  STAGE_PROLOGUE
+  if (k < 0 || k >= h.K) return fail(&h, CG_ERR_INVALID, "section index out of range");
+  int st = launch_ok(h, launch_moments(h, k), "moments");
+  return st ? st : check_status(h);
+}
+
+int cg_get_moments(cg_handle* H, cg_bunch_moments* out) {
+  STAGE_PROLOGUE
+  std::vector<BunchMomDev> m(h.M);
+  CG_CUDA(&h, cudaStreamSynchronize(h.stream));
+  CG_CUDA(&h, cudaMemcpy(m.data(), h.d.mom, sizeof(BunchMomDev) * h.M, cudaMemcpyDeviceToHost));
+  for (int j = 0; j < h.M; ++j) {
+    cg_bunch_moments& o = out[j];
+    const BunchMomDev& s = m[j];
+    o.n_alive = (int)s.n_alive;
+    o.n_macro = h.n_macro[j];
+    for (int d = 0; d < 6; ++d) o.mean[d] = s.mean[d];
+    for (int d = 0; d < 3; ++d) { o.emit[d] = s.emit[d]; o.eff_emit[d] = s.eff_emit[d]; }
+    o.rms_x = s.rms_x; o.rms_y = s.rms_y; o.eff_rms_x = s.eff_rms_x; o.eff_rms_y = s.eff_rms_y;
+    o.bunch_length = s.bunch_length; o.energy_spread = s.energy_spread;
+    o.z_min = s.z_min; o.z_max = s.z_max; o.transmission = s.transmission;
+  }
+  return CG_OK;
+}
+
+static int set_turn(Handle& h, int turn) {
+  return cudaMemcpyAsync(h.d.turn, &turn, sizeof(int), cudaMemcpyHostToDevice, h.stream) == cudaSuccess
+             ? CG_OK : fail(&h, CG_ERR_CUDA, "turn upload");
+}
+
+int cg_beam_ion_ip(cg_handle* H, int turn, int k) {
+  STAGE_PROLOGUE
+  if (!h.cfg.flag_beam_ion) return fail(&h, CG_ERR_NOT_READY, "runBeamIonFlag is off");
+  if (k < 0 || k >= h.K) return fail(&h, CG_ERR_INVALID, "section index out of range");
+  int st = set_turn(h, turn);
+  if (st) return st;
+  CG_CUDA(&h, cudaStreamSynchronize(h.stream));
+  if ((st = launch_ok(h, launch_ion_chain(h, k), "ion chain"))) return st;
+  if ((st = check_status(h))) return st;
+  if ((st = launch_ok(h, launch_ion_kick(h, k), "ion kick"))) return st;
+  return check_status(h);
+}
+
+int cg_section_map(cg_handle* H, int k) {
+  STAGE_PROLOGUE
+  if (k < 0 || k >= h.K) return fail(&h, CG_ERR_INVALID, "section index out of range");
+  int st = launch_ok(h, launch_map(h, k), "map");
+  return st ? st : check_status(h);
+}
+
+int cg_rf_kick(cg_handle* H) {
+  STAGE_PROLOGUE
+  int st = launch_ok(h, launch_long(h, kLongRF), "rf");
+  return st ? st : check_status(h);
+}
+int cg_longi_drift(cg_handle* H) {
+  STAGE_PROLOGUE
+  int st = launch_ok(h, launch_long(h, kLongDrift), "drift");
+  return st ? st : check_status(h);
+}
+int cg_energy_loss(cg_handle* H) {
+  STAGE_PROLOGUE
+  int st = launch_ok(h, launch_long(h, kLongLoss), "loss");
+  return st ? st : check_status(h);
+}
+int cg_synrad(cg_handle* H, int turn) {
+  STAGE_PROLOGUE
+  int st = set_turn(h, turn);
+  if (st) return st;
+  st = launch_ok(h, launch_long(h, kLongSynrad), "synrad");
+  return st ? st : check_status(h);
+}
+int cg_lr_wake(cg_handle* H) {
+  STAGE_PROLOGUE
+  if (!h.cfg.flag_lr_wake) return fail(&h, CG_ERR_NOT_READY, "runLongRangeWake is off");
+  int st = launch_ok(h, launch_lr_compute(h), "lr");
+  if (!st) st = launch_ok(h, launch_lr_kick(h), "lr kick");
+  return st ? st : check_status(h);
+}
+int cg_sr_wake(cg_handle* H, int turn) {
+  STAGE_PROLOGUE
+  (void)turn;
+  if (!h.cfg.flag_sr_wake) return fail(&h, CG_ERR_NOT_READY, "runShortRangeWake is off");
+  int st = launch_ok(h, launch_sr_wake(h), "sr");
+  return st ? st : check_status(h);
+}
+int cg_sr_bins(cg_handle* H, int j, double* zlo, double* dz, int* counts) {
+  STAGE_PROLOGUE
+  if (!h.cfg.flag_sr_wake) return fail(&h, CG_ERR_NOT_READY, "runShortRangeWake is off");
+  if (j < 0 || j >= h.M) return fail(&h, CG_ERR_INVALID, "bunch index out of range");
+  CG_CUDA(&h, cudaStreamSynchronize(h.stream));
+  double g[2];
+  CG_CUDA(&h, cudaMemcpy(g, h.d.sr_geom + 2 * j, sizeof g, cudaMemcpyDeviceToHost));
+  if (zlo) *zlo = g[0];
+  if (dz) *dz = g[1];
+  if (counts)
+    CG_CUDA(&h, cudaMemcpy(counts, h.d.sr_counts + (size_t)j * h.cfg.sr_bins,
+                           sizeof(int) * h.cfg.sr_bins, cudaMemcpyDeviceToHost));
+  return CG_OK;
+}
+
+int cg_fir(cg_handle* H, int turn) {
+  STAGE_PROLOGUE
+  if (!h.cfg.flag_fir) return fail(&h, CG_ERR_NOT_READY, "runFIRBunchByBunchFeedbackFlag is off");
+  int st = set_turn(h, turn);
+  if (st) return st;
+  st = launch_ok(h, launch_fir_compute(h), "fir");
+  if (st) return st;
+  // kick every particle of each bunch (no loss marking in this call)
+  st = launch_ok(h, launch_mark_lost(h, true, false), "fir kick");
+  return st ? st : check_status(h);
+}
+int cg_mark_lost(cg_handle* H, double* trans) {
+  STAGE_PROLOGUE
+  int st = launch_ok(h, launch_mark_lost(h, false, true), "mark lost");
+  int s2 = check_status(h);
+  if (!st) st = s2;
+  if (trans) {
+    std::vector<BunchMomDev> m(h.M);
+    cudaMemcpy(m.data(), h.d.mom, sizeof(BunchMomDev) * h.M, cudaMemcpyDeviceToHost);
+    for (int j = 0; j < h.M; ++j) trans[j] = m[j].transmission;
+  }
+  return st;
+}
+
+// One turn of MPBeam::Run (MPBeam.cpp:1010-1102) as a kernel sequence on
+// h.stream.  The turn-start and post-map moment calls whose results no stage
+// reads are skipped (the per-turn output writer is not part of this path).
+static cudaError_t enqueue_turn(Handle& h) {
+  const cg_config& c = h.cfg;
+  cudaError_t e;
+  for (int k = 0; k < h.K; ++k) {
+    if (c.flag_beam_ion) {
+      if ((e = launch_moments(h, k))) return e;
+      if ((e = launch_ion_chain(h, k))) return e;
+      if ((e = launch_ion_kick(h, k))) return e;
+    }
+    if ((e = launch_map(h, k))) return e;
+  }
+  if (c.flag_lr_wake || c.flag_sr_wake) {
+    if ((e = launch_moments(h, h.K - 1))) return e;
+  }
+  if (c.flag_lr_wake && (e = launch_lr_compute(h))) return e;
+  unsigned fl = kLongRF | kLongDrift | kLongLoss;
+  if (c.flag_synrad) fl |= kLongSynrad;
+  if (c.flag_lr_wake) fl |= kLongLR;
+  if ((e = launch_long(h, fl))) return e;
+  if (c.flag_sr_wake && (e = launch_sr_wake(h))) return e;
+  if (c.flag_fir) {
+    if ((e = launch_moments(h, 0))) return e;
+    if ((e = launch_fir_compute(h))) return e;
+  }
+  if ((e = launch_mark_lost(h, c.flag_fir != 0, true))) return e;
+  return launch_turn_advance(h);
+}
+
+int cg_run_turns(cg_handle* H, int turn0, int n_turns) {
+  STAGE_PROLOGUE
+  if (n_turns < 0) return fail(&h, CG_ERR_INVALID, "n_turns < 0");
+  int st = set_turn(h, turn0);
+  if (st) return st;
+  if (!h.turn_graph) {
+    cudaGraph_t g;
+    CG_CUDA(&h, cudaStreamBeginCapture(h.stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = enqueue_turn(h);
+    cudaError_t e2 = cudaStreamEndCapture(h.stream, &g);
+    if (e != cudaSuccess) return cuda_fail(&h, e, "turn capture");
+    if (e2 != cudaSuccess) return cuda_fail(&h, e2, "end capture");
+    e = cudaGraphInstantiate(&h.turn_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(&h, e, "graph instantiate");
+  }
+  for (int n = 0; n < n_turns; ++n) {
+    CG_CUDA(&h, cudaGraphLaunch(h.turn_graph, h.stream));
+    // status is polled every 64 turns (and at the end) to keep the GPU fed
+    if (((n + 1) & 63) == 0 || n + 1 == n_turns) {
+      if ((st = check_status(h))) return st;
+    }
+  }
+  return check_status(h);
+}
+
+// ---- ion clouds ----
+
+static int cloud_index(Handle& h, int k, int p) { return k * h.P + p; }
+
+int cg_ion_count(cg_handle* H, int k, int p, int* count) {
+  if (!H || !count) return CG_ERR_INVALID;
+  Handle& h = H->h;
+  if (!h.cfg.flag_beam_ion) return fail(&h, CG_ERR_NOT_READY, "runBeamIonFlag is off");
+  if (k < 0 || k >= h.K || p < 0 || p >= h.P) return fail(&h, CG_ERR_INVALID, "bad IP/species");
+  cudaSetDevice(h.device);
+  CloudState s;
+  CG_CUDA(&h, cudaStreamSynchronize(h.stream));
+  CG_CUDA(&h, cudaMemcpy(&s, h.d.cloud_state + cloud_index(h, k, p), sizeof s, cudaMemcpyDeviceToHost));
+  *count = s.n;
+  return CG_OK;
+}
+
+int cg_ion_download(cg_handle* H, int k, int p, double* x, double* y, double* vx, double* vy,
+                    int capacity, int* count) {
+  if (!H || !count) return CG_ERR_INVALID;
+  Handle& h = H->h;
+  if (!h.cfg.flag_beam_ion) return fail(&h, CG_ERR_NOT_READY, "runBeamIonFlag is off");
+  if (k < 0 || k >= h.K || p < 0 || p >= h.P) return fail(&h, CG_ERR_INVALID, "bad IP/species");
+  cudaSetDevice(h.device);
+  CG_CUDA(&h, cudaStreamSynchronize(h.stream));
+  CloudState s;
+  CloudDev cd;
+  int ci = cloud_index(h, k, p);
+  CG_CUDA(&h, cudaMemcpy(&s, h.d.cloud_state + ci, sizeof s, cudaMemcpyDeviceToHost));
+  CG_CUDA(&h, cudaMemcpy(&cd, h.d.clouds + ci, sizeof cd, cudaMemcpyDeviceToHost));
+  *count = s.n;
+  int n = s.n < capacity ? s.n : capacity;
+  if (n > 0) {
+    if (x) CG_CUDA(&h, cudaMemcpy(x, cd.x[s.cur], n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (y) CG_CUDA(&h, cudaMemcpy(y, cd.y[s.cur], n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (vx) CG_CUDA(&h, cudaMemcpy(vx, cd.vx[s.cur], n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (vy) CG_CUDA(&h, cudaMemcpy(vy, cd.vy[s.cur], n * sizeof(double), cudaMemcpyDeviceToHost));
+  }
+  return CG_OK;
+}
+
+int cg_ion_upload(cg_handle* H, int k, int p, const double* x, const double* y, const double* vx,
+                  const double* vy, int count) {
+  if (!H) return CG_ERR_INVALID;
+  Handle& h = H->h;
+  if (!h.cfg.flag_beam_ion) return fail(&h, CG_ERR_NOT_READY, "runBeamIonFlag is off");
+  if (k < 0 || k >= h.K || p < 0 || p >= h.P) return fail(&h, CG_ERR_INVALID, "bad IP/species");
+  if (count < 0 || count > h.cfg.ion.max_ions) return fail(&h, CG_ERR_INVALID, "ion count out of range");
+  cudaSetDevice(h.device);
+  CG_CUDA(&h, cudaStreamSynchronize(h.stream));
+  int ci = cloud_index(h, k, p);
+  CloudState s;
+  CloudDev cd;
+  CG_CUDA(&h, cudaMemcpy(&s, h.d.cloud_state + ci, sizeof s, cudaMemcpyDeviceToHost));
+  CG_CUDA(&h, cudaMemcpy(&cd, h.d.clouds + ci, sizeof cd, cudaMemcpyDeviceToHost));
+  if (count > 0) {
+    CG_CUDA(&h, cudaMemcpy(cd.x[s.cur], x, count * sizeof(double), cudaMemcpyHostToDevice));
+    CG_CUDA(&h, cudaMemcpy(cd.y[s.cur], y, count * sizeof(double), cudaMemcpyHostToDevice));
+    CG_CUDA(&h, cudaMemcpy(cd.vx[s.cur], vx, count * sizeof(double), cudaMemcpyHostToDevice));
+    CG_CUDA(&h, cudaMemcpy(cd.vy[s.cur], vy, count * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  s.n = count;
+  CG_CUDA(&h, cudaMemcpy(h.d.cloud_state + ci, &s, sizeof s, cudaMemcpyHostToDevice));
+  return CG_OK;
+}
+
+int cg_ion_cloud_record(cg_handle* H, int k, double* out) {
+  if (!H || !out) return CG_ERR_INVALID;
+  Handle& h = H->h;
+  if (!h.cfg.flag_beam_ion || !h.beam_set) return fail(&h, CG_ERR_NOT_READY, "no ion records");
+  if (k < 0 || k >= h.K) return fail(&h, CG_ERR_INVALID, "bad IP");
+  cudaSetDevice(h.device);
+  CG_CUDA(&h, cudaStreamSynchronize(h.stream));
+  std::vector<CloudRec> r((size_t)h.M * h.P);
+  CG_CUDA(&h, cudaMemcpy(r.data(), h.d.rec + (size_t)k * h.M * h.P, sizeof(CloudRec) * r.size(),
+                         cudaMemcpyDeviceToHost));
+  for (size_t i = 0; i < r.size(); ++i) {
+    out[6 * i + 0] = r[i].coeff; out[6 * i + 1] = r[i].rms_x; out[6 * i + 2] = r[i].rms_y;
+    out[6 * i + 3] = r[i].aver_x; out[6 * i + 4] = r[i].aver_y; out[6 * i + 5] = r[i].count;
+  }
+  return CG_OK;
+}
+
+int cg_ion_totals(cg_handle* H, double* tot_charge, int* tot_macro) {
+  if (!H) return CG_ERR_INVALID;
+  Handle& h = H->h;
+  if (!h.cfg.flag_beam_ion) return fail(&h, CG_ERR_NOT_READY, "runBeamIonFlag is off");
+  cudaSetDevice(h.device);
+  CG_CUDA(&h, cudaStreamSynchronize(h.stream));
+  std::vector<CloudState> s((size_t)h.K * h.P);
+  CG_CUDA(&h, cudaMemcpy(s.data(), h.d.cloud_state, sizeof(CloudState) * s.size(), cudaMemcpyDeviceToHost));
+  double q = 0;
+  int n = 0;
+  for (auto& c : s) {
+    q += c.n * c.macro_charge;
+    n += c.n;
+  }
+  if (tot_charge) *tot_charge = q;
+  if (tot_macro) *tot_macro = n;
+  return CG_OK;
+}
+
+// ---- stateless evaluators ----
+
+static int eval_arrays(int nin, const double* const* in, int nout, double* const* outp, int64_t n,
+                       int kind) {
+  if (n < 0) return fail(nullptr, CG_ERR_INVALID, "n < 0");
+  if (n == 0) return CG_OK;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(nullptr, CG_ERR_CUDA, "no CUDA device available (the library has no CPU path)");
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (ensure_weideman(dev)) return fail(nullptr, CG_ERR_CUDA, "Weideman table upload failed");
+  std::vector<double*> d(nin + nout, nullptr);
+  int st = CG_OK;
+  for (auto& p : d)
+    if (cudaMalloc((void**)&p, n * sizeof(double)) != cudaSuccess) st = CG_ERR_OOM;
+  if (!st) {
+    for (int i = 0; i < nin; ++i) cudaMemcpy(d[i], in[i], n * sizeof(double), cudaMemcpyHostToDevice);
+    cudaError_t e;
+    if (kind == 2)
+      e = launch_field(d[0], d[1], d[2], d[3], d[4], d[5], n, 0);
+    else
+      e = launch_faddeeva(d[0], d[1], d[2], d[3], n, kind == 0, 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) st = fail(nullptr, CG_ERR_CUDA, cudaGetErrorString(e));
+    for (int i = 0; i < nout && !st; ++i)
+      cudaMemcpy(outp[i], d[nin + i], n * sizeof(double), cudaMemcpyDeviceToHost);
+  }
+  for (auto p : d) dfree(p);
+  return st;
+}
+
+int cg_faddeeva_w(const double* zr, const double* zi, double* wr, double* wi, int64_t n) {
+  const double* in[2] = {zr, zi};
+  double* out[2] = {wr, wi};
+  return eval_arrays(2, in, 2, out, n, 0);
+}
+int cg_faddeeva_w_q1(const double* zr, const double* zi, double* wr, double* wi, int64_t n) {
+  const double* in[2] = {zr, zi};
+  double* out[2] = {wr, wi};
+  return eval_arrays(2, in, 2, out, n, 1);
+}
+int cg_gaussian_field(const double* x, const double* y, const double* sx, const double* sy,
+                      double* fx, double* fy, int64_t n) {
+  const double* in[4] = {x, y, sx, sy};
+  double* out[2] = {fx, fy};
+  return eval_arrays(4, in, 2, out, n, 2);
+}
+
+}  // extern "C"

@@ -1,0 +1,116 @@
+// Internal (host) definitions of libcetagpu: the handle and its device state.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+#include "../../include/cetasim_gpu.h"
+#include "track_math.cuh"
+
+namespace cg {
+
+constexpr int kTile = 256;            // particles per tile == threads per CTA
+constexpr int kChainThreads = 128;    // ion-chain CTA size
+
+struct BunchDev {
+  int n, tile_off, n_tiles, harm, gap;
+  int pad;
+  double ne, q_macro;
+};
+
+// Ion cloud of one (IP, species): ping-pong buffers of capacity `cap`.
+struct CloudDev {
+  double* x[2];
+  double* y[2];
+  double* vx[2];
+  double* vy[2];
+  int cap;
+};
+
+// Device-side per-(IP, species) ion state that persists across launches.
+struct CloudState {
+  int n;         // ionAccumuNumber
+  int cur;       // which ping-pong buffer holds the cloud
+  double aver_x, aver_y, rms_x, rms_y;  // IonRMSCal (stale when n <= 1)
+  double macro_charge;
+};
+
+// Parameters of the ion chain kernel that do not change between launches.
+struct ChainParams {
+  double cross_section[CG_MAX_SPECIES], gas_percent[CG_MAX_SPECIES], mass_number[CG_MAX_SPECIES];
+  double loss_boundary;
+  double circ_ring, harmonics;  // ion drift over a gap: v C/h gap/c (LIP.cpp:1172-1173)
+  double r_gamma;
+  int n_species, macro_per_ip, max_ions, n_bunches;
+  uint64_t seed;
+};
+
+struct DeviceBufs {
+  double* c = nullptr;          // 6 x npad SoA
+  uint8_t* surv = nullptr;      // npad
+  int* tile_bunch = nullptr;    // n_tiles
+  BunchDev* bunch = nullptr;    // M
+  MomPartial* partials = nullptr;  // n_tiles
+  unsigned* counters = nullptr;    // M (+ spare)
+  BunchMomDev* mom = nullptr;      // M
+  int* loss_count = nullptr;       // M
+  int* status = nullptr;           // device status word(s)
+  int* turn = nullptr;             // device turn counter (graph replays)
+  // ion clouds
+  CloudDev* clouds = nullptr;      // K x P (device array of buffer pointers)
+  CloudState* cloud_state = nullptr;  // K x P
+  CloudRec* rec = nullptr;         // K x M x P
+  double* ion_totals = nullptr;    // K (charge), used by cg_ion_totals
+  // long-range wake
+  double* lr_tab = nullptr;        // 3 x np
+  double* lr_hist = nullptr;       // turns x 3 x M ring buffer
+  int* lr_head = nullptr;
+  double* lr_force = nullptr;      // M x 3
+  // FIR
+  double* fir_hist = nullptr;      // order x 3 x M ring buffer
+  int* fir_head = nullptr;
+  double* fir_kick = nullptr;      // M x 3
+  double* fir_coeff = nullptr;     // 3 x order
+  // short-range wake
+  double* sr_geom = nullptr;       // M x 2 (zlo, dz)
+  int* sr_counts = nullptr;        // M x B
+  double* sr_sumx = nullptr;       // M x B
+  double* sr_sumy = nullptr;       // M x B
+  double* sr_lag = nullptr;        // M x (2B-1)
+  double* sr_pot = nullptr;        // M x B (z plane, persistent)
+  double* sr_green = nullptr;      // resonators x 1000 (u-independent factors)
+  // scratch
+  double* scratch = nullptr;
+  size_t scratch_bytes = 0;
+};
+
+struct Handle {
+  cg_config cfg;
+  std::vector<cg_section> sections;
+  std::vector<SectionDev> sec_dev_host;
+  SectionDev* sec_dev = nullptr;  // device copy (K)
+  RingDev ring;
+  ChainParams chain;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int K = 0, M = 0, P = 1;
+  int n_tiles = 0;
+  int64_t npad = 0;
+  std::vector<int> n_macro, harm, gap, tile_off;
+  std::vector<double> ne;
+  DeviceBufs d;
+  int lr_np = 0;
+  double lr_dt = 0;
+  int fir_order = 0;
+  double fir_limit = 0;
+  bool beam_set = false;
+  int ion_cap = 0;
+  cudaGraphExec_t turn_graph = nullptr;
+  std::string err;
+};
+
+}  // namespace cg
+
+struct cg_handle {
+  cg::Handle h;
+};

@@ -1,0 +1,860 @@
+// sm_100a kernels of the MP tracking path.
+//
+// Data layout in HBM: six FP64 structure-of-arrays coordinate vectors
+// (x, px, y, py, z, dp), each of `npad` doubles, plus one survival byte per
+// particle.  Bunch j occupies tiles [tile_off[j], tile_off[j] + n_tiles[j]);
+// every bunch segment starts on a 256-particle tile boundary (2 KiB), so
+// loads of one CTA are fully coalesced 128-byte lines and a tile never spans
+// two bunches.  Bunches of uneven size (ragged trains) are just different
+// tile counts; fill-pattern gaps hold no tiles at all.
+#include <cuda_runtime.h>
+#include "kernels.cuh"
+
+namespace cg {
+
+#define FULL_MASK 0xffffffffu
+
+// ---------------------------------------------------------------------------
+// Block reductions with a fixed combination tree (deterministic results).
+
+template <int N>
+__device__ __forceinline__ void warp_sum(double (&v)[N]) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+    for (int k = 0; k < N; ++k) v[k] += __shfl_xor_sync(FULL_MASK, v[k], o);
+}
+
+// Sum N values over a CTA of NT threads; every thread receives the totals.
+// smem must hold N * 32 doubles.
+template <int N, int NT>
+__device__ __forceinline__ void block_sum(double (&v)[N], double* smem) {
+  constexpr int NW = NT / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  warp_sum<N>(v);
+  if (NW == 1) return;
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < N; ++k) smem[k * 32 + warp] = v[k];
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int k = 0; k < N; ++k) v[k] = (lane < NW) ? smem[k * 32 + lane] : 0.0;
+    warp_sum<N>(v);
+    if (lane == 0)
+#pragma unroll
+      for (int k = 0; k < N; ++k) smem[k * 32] = v[k];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < N; ++k) v[k] = smem[k * 32];
+  __syncthreads();
+}
+
+template <int NT>
+__device__ __forceinline__ void block_minmax(double& mn, double& mx, double* smem) {
+  constexpr int NW = NT / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    mn = fmin(mn, __shfl_xor_sync(FULL_MASK, mn, o));
+    mx = fmax(mx, __shfl_xor_sync(FULL_MASK, mx, o));
+  }
+  if (NW == 1) return;
+  if (lane == 0) {
+    smem[warp] = mn;
+    smem[32 + warp] = mx;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    mn = lane < NW ? smem[lane] : INFINITY;
+    mx = lane < NW ? smem[32 + lane] : -INFINITY;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      mn = fmin(mn, __shfl_xor_sync(FULL_MASK, mn, o));
+      mx = fmax(mx, __shfl_xor_sync(FULL_MASK, mx, o));
+    }
+    if (lane == 0) {
+      smem[0] = mn;
+      smem[32] = mx;
+    }
+  }
+  __syncthreads();
+  mn = smem[0];
+  mx = smem[32];
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// Tile addressing
+
+struct TileIdx {
+  int b;       // bunch
+  int i;       // index within the bunch
+  int64_t g;   // global index into the SoA arrays
+  bool valid;  // i < n_b
+};
+
+__device__ __forceinline__ TileIdx tile_index(const int* tile_bunch, const BunchDev* bunch) {
+  TileIdx t;
+  t.b = tile_bunch[blockIdx.x];
+  const BunchDev& B = bunch[t.b];
+  t.i = (blockIdx.x - B.tile_off) * kTile + threadIdx.x;
+  t.g = (int64_t)blockIdx.x * kTile + threadIdx.x;
+  t.valid = t.i < B.n;
+  return t;
+}
+
+__device__ __forceinline__ void load6(const double* __restrict__ c, int64_t npad, int64_t g,
+                                      double v[6]) {
+#pragma unroll
+  for (int d = 0; d < 6; ++d) v[d] = c[d * npad + g];
+}
+__device__ __forceinline__ void store6(double* __restrict__ c, int64_t npad, int64_t g,
+                                       const double v[6]) {
+#pragma unroll
+  for (int d = 0; d < 6; ++d) c[d * npad + g] = v[d];
+}
+
+// ---------------------------------------------------------------------------
+// Moments (MPBunch::GetMPBunchRMS, MPBunch.cpp:342-498): per tile a two-pass
+// partial (mean, centred co-moments) over alive particles, then the last CTA
+// of each bunch merges the bunch's partials in tile order.
+
+__device__ void tile_moment_partial(const double v[6], bool alive, double* smem,
+                                    MomPartial* out) {
+  double s[7];
+#pragma unroll
+  for (int d = 0; d < 6; ++d) s[d] = alive ? v[d] : 0.0;
+  s[6] = alive ? 1.0 : 0.0;
+  block_sum<7, kTile>(s, smem);
+  const double n = s[6];
+  double mean[6];
+#pragma unroll
+  for (int d = 0; d < 6; ++d) mean[d] = n > 0 ? s[d] / n : 0.0;
+  double q[9];
+  double dv[6];
+#pragma unroll
+  for (int d = 0; d < 6; ++d) dv[d] = alive ? v[d] - mean[d] : 0.0;
+#pragma unroll
+  for (int d = 0; d < 6; ++d) q[d] = dv[d] * dv[d];
+  q[6] = dv[0] * dv[1];
+  q[7] = dv[2] * dv[3];
+  q[8] = dv[4] * dv[5];
+  block_sum<9, kTile>(q, smem);
+  double mn = alive ? v[4] : INFINITY, mx = alive ? v[4] : -INFINITY;
+  block_minmax<kTile>(mn, mx, smem);
+  if (threadIdx.x == 0) {
+    MomPartial p;
+    p.n = n;
+#pragma unroll
+    for (int d = 0; d < 6; ++d) p.mean[d] = mean[d];
+#pragma unroll
+    for (int d = 0; d < 9; ++d) p.c[d] = q[d];
+    p.zmin = mn;
+    p.zmax = mx;
+    *out = p;
+  }
+}
+
+// Called by all threads of every CTA after its partial is stored: the last
+// CTA of bunch b merges the partials (fixed pairwise tree) and finalises.
+__device__ void bunch_moment_finish(int b, const BunchDev& B, const MomPartial* partials,
+                                    unsigned* counters, BunchMomDev* mom, double beta_x,
+                                    double beta_y, const double* z, MomPartial* sp) {
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned prev = atomicAdd(&counters[b], 1u);
+    last = (prev == (unsigned)(B.n_tiles - 1));
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  // level 0: thread t merges partials t, t + kTile, ... sequentially
+  MomPartial acc;
+  mom_clear(acc);
+  for (int t = threadIdx.x; t < B.n_tiles; t += kTile) {
+    // partials written by other CTAs: read through L2 (no stale L1 lines)
+    const double* src = reinterpret_cast<const double*>(partials + B.tile_off + t);
+    MomPartial q;
+    double* dst = reinterpret_cast<double*>(&q);
+#pragma unroll
+    for (int e = 0; e < (int)(sizeof(MomPartial) / sizeof(double)); ++e) dst[e] = __ldcg(src + e);
+    mom_merge(acc, q);
+  }
+  sp[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = 1; s < kTile; s <<= 1) {
+    if ((threadIdx.x % (2 * s)) == 0 && threadIdx.x + s < kTile) mom_merge(sp[threadIdx.x], sp[threadIdx.x + s]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    BunchMomDev m = mom[b];
+    double tr = m.transmission;
+    double z0 = z[(int64_t)B.tile_off * kTile];
+    mom_finalize(sp[0], beta_x, beta_y, z0, m);
+    m.transmission = tr;
+    mom[b] = m;
+    counters[b] = 0;
+  }
+}
+
+__global__ void __launch_bounds__(kTile) k_moments(const double* __restrict__ c, int64_t npad,
+                                                   const uint8_t* __restrict__ surv,
+                                                   const int* __restrict__ tile_bunch,
+                                                   const BunchDev* __restrict__ bunch,
+                                                   MomPartial* partials, unsigned* counters,
+                                                   BunchMomDev* mom, double beta_x, double beta_y) {
+  __shared__ double smem[9 * 32];
+  __shared__ MomPartial sp[kTile];
+  TileIdx t = tile_index(tile_bunch, bunch);
+  double v[6] = {0, 0, 0, 0, 0, 0};
+  bool alive = false;
+  if (t.valid) {
+    alive = surv[t.g] == kAlive;
+    load6(c, npad, t.g, v);
+  }
+  tile_moment_partial(v, alive, smem, &partials[blockIdx.x]);
+  bunch_moment_finish(t.b, bunch[t.b], partials, counters, mom, beta_x, beta_y, c + 4 * npad, sp);
+}
+
+cudaError_t launch_moments(Handle& h, int k) {
+  const SectionDev& s = h.sec_dev_host[k];
+  k_moments<<<h.n_tiles, kTile, 0, h.stream>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch, h.d.bunch,
+                                               h.d.partials, h.d.counters, h.d.mom, s.beta_x,
+                                               s.beta_y);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Section map (Bunch::BunchTransferDueToLatticeTSymplectic).
+
+__global__ void __launch_bounds__(kTile) k_map(double* __restrict__ c, int64_t npad,
+                                               const uint8_t* __restrict__ surv,
+                                               const int* __restrict__ tile_bunch,
+                                               const BunchDev* __restrict__ bunch,
+                                               const SectionDev* __restrict__ secp, RingDev r) {
+  TileIdx t = tile_index(tile_bunch, bunch);
+  if (!t.valid || surv[t.g] != kAlive) return;
+  double v[6];
+  load6(c, npad, t.g, v);
+  section_map_particle(*secp, r, v);
+  store6(c, npad, t.g, v);
+}
+
+cudaError_t launch_map(Handle& h, int k) {
+  k_map<<<h.n_tiles, kTile, 0, h.stream>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch, h.d.bunch,
+                                           h.sec_dev + k, h.ring);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Electron-side ion kick (MPBunch.cpp:1164-1206 + Bunch.cpp:213-220) with the
+// cloud Gaussians the chain kernel recorded for each bunch at this IP.
+
+__global__ void __launch_bounds__(kTile) k_ion_kick(double* __restrict__ c, int64_t npad,
+                                                    const uint8_t* __restrict__ surv,
+                                                    const int* __restrict__ tile_bunch,
+                                                    const BunchDev* __restrict__ bunch,
+                                                    const CloudRec* __restrict__ rec, int P) {
+  TileIdx t = tile_index(tile_bunch, bunch);
+  if (!t.valid || surv[t.g] != kAlive) return;
+  const CloudRec* rb = rec + (size_t)t.b * P;
+  double x = c[0 * npad + t.g], y = c[2 * npad + t.g];
+  double dpx, dpy;
+  ion_kick_particle(rb, P, x, y, &dpx, &dpy);
+  c[1 * npad + t.g] += dpx;
+  c[3 * npad + t.g] += dpy;
+}
+
+cudaError_t launch_ion_kick(Handle& h, int k) {
+  k_ion_kick<<<h.n_tiles, kTile, 0, h.stream>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch,
+                                                h.d.bunch, h.d.rec + (size_t)k * h.M * h.P, h.P);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Ion chain of one interaction point (MPBeam::SSBeamIonEffectOneInteraction
+// Point, MPBeam.cpp:2585-2611): one CTA walks the bunches in order because
+// bunch j meets the cloud left behind by bunch j-1.
+
+__device__ __forceinline__ int block_excl_scan(int v, int* smem_i, int* total) {
+  // NT = kChainThreads
+  constexpr int NW = kChainThreads / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(FULL_MASK, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) smem_i[warp] = x;
+  __syncthreads();
+  int wpre = 0, tot = 0;
+#pragma unroll
+  for (int w = 0; w < NW; ++w) {
+    int s = smem_i[w];
+    if (w < warp) wpre += s;
+    tot += s;
+  }
+  __syncthreads();
+  *total = tot;
+  return wpre + x - v;
+}
+
+struct ChainSection {
+  double pressure, temperature, length, aperture_x, aperture_y;
+};
+
+__global__ void __launch_bounds__(kChainThreads) k_ion_chain(
+    ChainParams cp, ChainSection cs, const BunchDev* __restrict__ bunch,
+    const BunchMomDev* __restrict__ mom, CloudDev* clouds, CloudState* cst, CloudRec* rec,
+    int* status, const int* __restrict__ d_turn, int k) {
+  __shared__ double smem[4 * 32];
+  __shared__ int smem_i[32];
+  __shared__ double s_bx, s_by;
+  const int tid = threadIdx.x;
+  const int M = cp.n_bunches, P = cp.n_species;
+  const uint32_t turn = (uint32_t)(*d_turn);
+  // MPGetBeamInfo: bunchSizeXMax / YMax over all bunches (MPBeam.cpp:2175-2186)
+  if (tid == 0) {
+    double mx = mom[0].rms_x, my = mom[0].rms_y;
+    for (int j = 1; j < M; ++j) {
+      if (mom[j].rms_x > mx) mx = mom[j].rms_x;
+      if (mom[j].rms_y > my) my = mom[j].rms_y;
+    }
+    double lbx = cp.loss_boundary * mx, lby = cp.loss_boundary * my;
+    s_bx = cs.aperture_x > lbx ? lbx : cs.aperture_x;
+    s_by = cs.aperture_y > lby ? lby : cs.aperture_y;
+  }
+  __syncthreads();
+  const double bx = s_bx, by = s_by;
+  const uint32_t k0 = (uint32_t)cp.seed, k1 = (uint32_t)(cp.seed >> 32) ^ kStreamIonBirth;
+
+  for (int j = 0; j < M; ++j) {
+    const BunchDev B = bunch[j];
+    const double mx = mom[j].mean[0], my = mom[j].mean[2];
+    const double sx = mom[j].rms_x, sy = mom[j].rms_y;
+    for (int p = 0; p < P; ++p) {
+      CloudDev cd = clouds[p];
+      CloudState st = cst[p];
+      // LIP::GetIonNumberPerInterAction (LIP.cpp:974-982)
+      double press_p = cp.gas_percent[p] * cs.pressure;
+      double line_density = cp.cross_section[p] * press_p / cs.temperature / kBoltzmann * B.ne;
+      double ion_number = line_density * cs.length;
+      st.macro_charge = ion_number / cp.macro_per_ip;
+      // LIP::IonGenerator (LIP.cpp:985-1019): N(mean, rms) births, rejected
+      // when ((x-mean)/rms)^2 + ((y-mean)/rms)^2 > 4; attempt a of bunch j
+      // is Philox counter {a, j, turn, k*CG_MAX_SPECIES+p}.
+      if (st.n + cp.macro_per_ip > cd.cap) {
+        if (tid == 0) atomicOr(status, kStatusIonOverflow);
+        return;
+      }
+      if (tid < 32) {
+        int need = cp.macro_per_ip;
+        uint32_t base = 0;
+        int wpos = st.n;
+        double* X = cd.x[st.cur];
+        double* Y = cd.y[st.cur];
+        double* VX = cd.vx[st.cur];
+        double* VY = cd.vy[st.cur];
+        while (need > 0) {
+          u32x4 ctr = {{base + (uint32_t)tid, (uint32_t)j, turn, (uint32_t)(k * CG_MAX_SPECIES + p)}};
+          double g0, g1;
+          normal2(philox4x32_10(ctr, k0, k1), &g0, &g1);
+          double tx = mx + sx * g0, ty = my + sy * g1;
+          double ax = (tx - mx) / sx, ay = (ty - my) / sy;
+          bool ok = !(ax * ax + ay * ay > 4.E0);
+          unsigned bal = __ballot_sync(FULL_MASK, ok);
+          int rank = __popc(bal & ((1u << tid) - 1u));
+          if (ok && rank < need) {
+            X[wpos + rank] = tx;
+            Y[wpos + rank] = ty;
+            VX[wpos + rank] = 0.0;
+            VY[wpos + rank] = 0.0;
+          }
+          int got = min(__popc(bal), need);
+          need -= got;
+          wpos += got;
+          base += 32;
+        }
+      }
+      st.n += cp.macro_per_ip;
+      __syncthreads();
+      if (st.n > cp.max_ions) {
+        if (tid == 0) atomicOr(status, kStatusIonOverflow);
+        return;
+      }
+      // LIP::IonRMSCal(k, p) (LIP.cpp:1113-1155)
+      const double* X = cd.x[st.cur];
+      const double* Y = cd.y[st.cur];
+      if (st.n == 1) {
+        st.rms_x = fabs(X[0]);
+        st.rms_y = fabs(Y[0]);
+      } else if (st.n > 1) {
+        double s2[2] = {0.0, 0.0};
+        for (int i = tid; i < st.n; i += kChainThreads) {
+          s2[0] += X[i];
+          s2[1] += Y[i];
+        }
+        block_sum<2, kChainThreads>(s2, smem);
+        st.aver_x = s2[0] / st.n;
+        st.aver_y = s2[1] / st.n;
+        double q[2] = {0.0, 0.0};
+        for (int i = tid; i < st.n; i += kChainThreads) {
+          double dx = X[i] - st.aver_x, dy = Y[i] - st.aver_y;
+          q[0] = fma(dx, dx, q[0]);
+          q[1] = fma(dy, dy, q[1]);
+        }
+        block_sum<2, kChainThreads>(q, smem);
+        st.rms_x = sqrt(q[0] / st.n);
+        st.rms_y = sqrt(q[1] / st.n);
+      } else {
+        st.rms_x = 0;
+        st.rms_y = 0;
+      }
+      if (tid == 0) {
+        CloudRec r;
+        r.coeff = 2.0 * (st.macro_charge * st.n) * kElecClassicRadius / cp.r_gamma;
+        r.rms_x = st.rms_x;
+        r.rms_y = st.rms_y;
+        r.aver_x = st.aver_x;
+        r.aver_y = st.aver_y;
+        r.count = st.n;
+        rec[(size_t)j * P + p] = r;
+      }
+      // ion side (MPBunch.cpp:1111-1157) fused with LIP::IonTransferDueToBunch
+      // (LIP.cpp:1158-1211): v += F, x += v C/h gap/c, stable removal of ions
+      // beyond the loss boundary into the other ping-pong buffer.
+      const double coeffI = 2.0 * B.ne * kElecClassicRadius * kElectronMassEV / kIonMassEV /
+                            cp.mass_number[p] * kCLight;
+      const double* VX = cd.vx[st.cur];
+      const double* VY = cd.vy[st.cur];
+      double* X2 = cd.x[st.cur ^ 1];
+      double* Y2 = cd.y[st.cur ^ 1];
+      double* VX2 = cd.vx[st.cur ^ 1];
+      double* VY2 = cd.vy[st.cur ^ 1];
+      int out_base = 0;
+      for (int c0 = 0; c0 < st.n; c0 += kChainThreads) {
+        int i = c0 + tid;
+        bool keep = false;
+        double x = 0, y = 0, vx = 0, vy = 0;
+        if (i < st.n) {
+          x = X[i];
+          y = Y[i];
+          vx = VX[i];
+          vy = VY[i];
+          double fx, fy;
+          gaussian_field(x - mx, y - my, sx, sy, &fx, &fy);
+          vx += coeffI * fx;
+          vy += coeffI * fy;
+          x += vx * cp.circ_ring / cp.harmonics * B.gap / kCLight;
+          y += vy * cp.circ_ring / cp.harmonics * B.gap / kCLight;
+          keep = !(fabs(x) > bx || fabs(y) > by);
+        }
+        int tot;
+        int pos = block_excl_scan(keep ? 1 : 0, smem_i, &tot);
+        if (keep) {
+          X2[out_base + pos] = x;
+          Y2[out_base + pos] = y;
+          VX2[out_base + pos] = vx;
+          VY2[out_base + pos] = vy;
+        }
+        out_base += tot;
+      }
+      __syncthreads();
+      st.n = out_base;
+      st.cur ^= 1;
+      if (tid == 0) cst[p] = st;
+      __syncthreads();
+    }
+  }
+}
+
+cudaError_t launch_ion_chain(Handle& h, int k) {
+  ChainSection cs;
+  const cg_section& s = h.sections[k];
+  cs.pressure = s.pressure;
+  cs.temperature = s.temperature;
+  cs.length = s.length;
+  cs.aperture_x = s.aperture_x;
+  cs.aperture_y = s.aperture_y;
+  k_ion_chain<<<1, kChainThreads, 0, h.stream>>>(
+      h.chain, cs, h.d.bunch, h.d.mom, h.d.clouds + (size_t)k * h.P, h.d.cloud_state + (size_t)k * h.P,
+      h.d.rec + (size_t)k * h.M * h.P, h.d.status, h.d.turn, k);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Turn tail: RF kick, drift, energy loss (all particles), synchrotron
+// radiation (alive), long-range wake kick (all particles).
+
+__global__ void __launch_bounds__(kTile) k_long(double* __restrict__ c, int64_t npad,
+                                                const uint8_t* __restrict__ surv,
+                                                const int* __restrict__ tile_bunch,
+                                                const BunchDev* __restrict__ bunch,
+                                                const SectionDev* __restrict__ sec0, RingDev r,
+                                                unsigned flags, uint64_t seed,
+                                                const int* __restrict__ d_turn,
+                                                const double* __restrict__ lr_force) {
+  TileIdx t = tile_index(tile_bunch, bunch);
+  if (!t.valid) return;
+  double v[6];
+  load6(c, npad, t.g, v);
+  if (flags & kLongRF) v[5] = rf_kick_dp(r, v[4], v[5]);
+  if (flags & kLongDrift) v[4] = drift_z(r, v[4], v[5]);
+  if (flags & kLongLoss) v[5] -= r.u0_term;
+  if ((flags & kLongSynrad) && surv[t.g] == kAlive) {
+    double g[6];
+    synrad_normals(seed, (uint32_t)t.i, (uint32_t)t.b, (uint32_t)(*d_turn), g);
+    synrad_particle(*sec0, r, v, g, bunch[t.b].n != 1);
+  }
+  if (flags & kLongLR) {
+    const double* f = lr_force + 3 * t.b;
+    v[1] += f[0];
+    v[3] += f[1];
+    v[5] += f[2];
+  }
+  store6(c, npad, t.g, v);
+}
+
+cudaError_t launch_long(Handle& h, unsigned flags) {
+  k_long<<<h.n_tiles, kTile, 0, h.stream>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch, h.d.bunch,
+                                            h.sec_dev, h.ring, flags, h.cfg.seed, h.d.turn,
+                                            h.d.lr_force);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Long-range wake (MPBeam::LRWakeBeamIntaction, MPBeam.cpp:3232-3349).
+// k_lr_push stores this turn's centroids in the history ring; k_lr_force
+// sums the tabulated wake over (turn n, source bunch i) for each bunch j.
+
+__global__ void k_lr_push(const BunchMomDev* __restrict__ mom, double* hist, int* head, int T,
+                          int M) {
+  __shared__ int h;
+  if (threadIdx.x == 0) {
+    h = (*head + 1) % T;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < M; i += blockDim.x) {
+    double* slot = hist + (size_t)h * 3 * M;
+    slot[i] = mom[i].mean[0];
+    slot[M + i] = mom[i].mean[2];
+    slot[2 * M + i] = mom[i].mean[4];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *head = h;
+}
+
+__global__ void k_lr_force(const BunchMomDev* __restrict__ mom, const BunchDev* __restrict__ bunch,
+                           const double* __restrict__ hist, const int* __restrict__ head,
+                           const double* __restrict__ tab, int np, double dt, double tRF,
+                           double scale, int T, int M, int H, double inv_c_beta,
+                           double* lr_force, int* status) {
+  __shared__ double smem[3 * 32];
+  const int j = blockIdx.x;
+  const int hd = *head;
+  const int hj = bunch[j].harm;
+  const double zj = mom[j].mean[4];
+  double f[3] = {0.0, 0.0, 0.0};
+  // enumerate (n, i) pairs of the reference's loop: n = 0 -> i < j;
+  // n = T-1 -> i >= j; otherwise all i.
+  const int64_t total = (int64_t)T * M;
+  for (int64_t q = threadIdx.x; q < total; q += blockDim.x) {
+    int n = (int)(q / M), i = (int)(q % M);
+    if (n == 0 && i >= j) continue;
+    if (n == T - 1 && i < j) continue;
+    const double* hs = hist + (size_t)((hd - n + T) % T) * 3 * M;
+    int nT = bunch[i].harm - hj - n * H;
+    double tau = nT * tRF + (zj - hs[2 * M + i]) * inv_c_beta;
+    double a = -tau / dt;
+    int idx = (int)floor(a);
+    if (tau > 0 || idx < 0 || idx + 1 >= np) {
+      atomicOr(status, kStatusLrRange);
+      continue;
+    }
+    double v1 = a - idx, v0 = 1 - v1;
+    double ne = bunch[i].ne;
+    double w0 = tab[idx] * v0 + tab[idx + 1] * v1;
+    double w1 = tab[np + idx] * v0 + tab[np + idx + 1] * v1;
+    double w2 = tab[2 * np + idx] * v0 + tab[2 * np + idx + 1] * v1;
+    f[0] -= w0 * ne * hs[i];
+    f[1] -= w1 * ne * hs[M + i];
+    f[2] -= w2 * ne;
+  }
+  block_sum<3, 256>(f, smem);
+  if (threadIdx.x == 0) {
+    lr_force[3 * j + 0] = f[0] * scale;
+    lr_force[3 * j + 1] = f[1] * scale;
+    lr_force[3 * j + 2] = f[2] * scale;
+  }
+}
+
+cudaError_t launch_lr_compute(Handle& h) {
+  const cg_ring& r = h.cfg.ring;
+  int T = h.cfg.lr_turns;
+  k_lr_push<<<1, 256, 0, h.stream>>>(h.d.mom, h.d.lr_hist, h.d.lr_head, T, h.M);
+  double tRF = r.t0 / (double)r.harmonics;
+  double scale = kElectronCharge / r.electron_energy / (r.r_beta * r.r_beta);
+  double inv_c_beta = 1.0 / kCLight / r.r_beta;
+  k_lr_force<<<h.M, 256, 0, h.stream>>>(h.d.mom, h.d.bunch, h.d.lr_hist, h.d.lr_head, h.d.lr_tab,
+                                        h.lr_np, h.lr_dt, tRF, scale, T, h.M, r.harmonics,
+                                        inv_c_beta, h.d.lr_force, h.d.status);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lr_kick(Handle& h) { return launch_long(h, kLongLR); }
+
+// ---------------------------------------------------------------------------
+// FIR bunch-by-bunch feedback (MPBeam::FIRBunchByBunchFeedback,
+// MPBeam.cpp:2978-3090): history push + kick per bunch.
+
+__global__ void k_fir_compute(const BunchMomDev* __restrict__ mom, double* hist, int* head,
+                              const double* __restrict__ coeff, int order, int M, int mode,
+                              double gain, double kx, double ky, double kf, double limit,
+                              const int* __restrict__ d_turn, int n_sec, int4 se0, int4 se1,
+                              int4 se2, int4 se3, double* kick) {
+  const int turn = *d_turn;
+  int starts[8] = {se0.x, se0.z, se1.x, se1.z, se2.x, se2.z, se3.x, se3.z};
+  int ends[8] = {se0.y, se0.w, se1.y, se1.w, se2.y, se2.w, se3.y, se3.w};
+  bool on = false;
+  for (int q = 0; q < n_sec && q < 8; ++q)
+    if (turn > starts[q] && turn < ends[q]) on = true;
+  if (mode == 0) {
+    for (int j = threadIdx.x; j < M; j += blockDim.x) {
+      kick[3 * j + 0] = on ? -mom[j].mean[1] : 0.0;
+      kick[3 * j + 1] = on ? -mom[j].mean[3] : 0.0;
+      kick[3 * j + 2] = on ? -mom[j].mean[5] : 0.0;
+    }
+    return;
+  }
+  __shared__ int hd;
+  if (threadIdx.x == 0) hd = (*head + 1) % order;
+  __syncthreads();
+  for (int j = threadIdx.x; j < M; j += blockDim.x) {
+    double* slot = hist + (size_t)hd * 3 * M;
+    slot[j] = mom[j].mean[0];
+    slot[M + j] = mom[j].mean[2];
+    slot[2 * M + j] = mom[j].mean[4];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *head = hd;
+  for (int j = threadIdx.x; j < M; j += blockDim.x) {
+    double a = 0, b = 0, cz = 0;
+    if (on) {
+      // q = 0 is the oldest sample (reference posxData[0])
+      for (int q = 0; q < order; ++q) {
+        const double* hs = hist + (size_t)((hd + 1 + q) % order) * 3 * M;
+        a += coeff[order - q - 1] * hs[j];
+        b += coeff[order + order - q - 1] * hs[M + j];
+        cz += coeff[2 * order + order - q - 1] * hs[2 * M + j];
+      }
+      a = a * gain * kx;
+      b = b * gain * ky;
+      cz = cz * gain * kf;
+      if (a > limit) a = limit;
+      if (b > limit) b = limit;
+      if (cz > limit) cz = limit;
+    }
+    kick[3 * j + 0] = a;
+    kick[3 * j + 1] = b;
+    kick[3 * j + 2] = cz;  // divided by beta^2 when applied
+  }
+}
+
+cudaError_t launch_fir_compute(Handle& h) {
+  const cg_fir_params& f = h.cfg.fir;
+  int st[8] = {0}, en[8] = {0};
+  for (int q = 0; q < f.n_sections && q < 8; ++q) {
+    st[q] = f.start[q];
+    en[q] = f.end[q];
+  }
+  int4 a = {st[0], en[0], st[1], en[1]}, b = {st[2], en[2], st[3], en[3]};
+  int4 c = {st[4], en[4], st[5], en[5]}, d = {st[6], en[6], st[7], en[7]};
+  k_fir_compute<<<1, 256, 0, h.stream>>>(h.d.mom, h.d.fir_hist, h.d.fir_head, h.d.fir_coeff,
+                                         h.fir_order, h.M, f.mode, f.gain, f.kick_strength[0],
+                                         f.kick_strength[1], f.kick_strength[2], h.fir_limit,
+                                         h.d.turn, f.n_sections, a, b, c, d, h.d.fir_kick);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// FIR kick (all particles) + Bunch::MarkLostParticle (Bunch.cpp:172-200).
+
+__global__ void __launch_bounds__(kTile) k_mark_lost(double* __restrict__ c, int64_t npad,
+                                                     uint8_t* __restrict__ surv,
+                                                     const int* __restrict__ tile_bunch,
+                                                     const BunchDev* __restrict__ bunch, RingDev r,
+                                                     double ax, double ay, int mode,
+                                                     const double* __restrict__ fir_kick,
+                                                     double inv_beta2, int* loss_count,
+                                                     unsigned* counters, BunchMomDev* mom,
+                                                     int* status, bool mark) {
+  __shared__ double smem[32];
+  __shared__ bool last;
+  TileIdx t = tile_index(tile_bunch, bunch);
+  double cnt[1] = {0.0};
+  if (t.valid && mode > 0) {
+    const double* k = fir_kick + 3 * t.b;
+    c[1 * npad + t.g] += k[0];
+    c[3 * npad + t.g] += k[1];
+    if (mode == 1) c[5 * npad + t.g] += k[2] * inv_beta2;
+    else c[5 * npad + t.g] += k[2];
+  }
+  if (!mark) return;
+  if (t.valid) {
+    double x = c[t.g], y = c[2 * npad + t.g], z = c[4 * npad + t.g];
+    uint8_t s = surv[t.g];
+    cnt[0] = (double)mark_lost_particle(r, ax, ay, x, y, z, &s);
+    surv[t.g] = s;
+  }
+  block_sum<1, kTile>(cnt, smem);
+  const BunchDev& B = bunch[t.b];
+  if (threadIdx.x == 0) atomicAdd(&loss_count[t.b], (int)cnt[0]);
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned prev = atomicAdd(&counters[t.b], 1u);
+    last = (prev == (unsigned)(B.n_tiles - 1));
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    int count = atomicAdd(&loss_count[t.b], 0);
+    double tr = (B.n - count) / (double)B.n;
+    mom[t.b].transmission = tr;
+    if (tr < 0.5) atomicOr(status, kStatusTransmission);
+    loss_count[t.b] = 0;
+    counters[t.b] = 0;
+  }
+}
+
+cudaError_t launch_mark_lost(Handle& h, bool fir_kick, bool mark) {
+  int mode = 0;
+  if (fir_kick) mode = (h.cfg.fir.mode == 0) ? 2 : 1;
+  double inv_beta2 = 1.0 / (h.cfg.ring.r_beta * h.cfg.ring.r_beta);
+  k_mark_lost<<<h.n_tiles, kTile, 0, h.stream>>>(
+      h.d.c, h.npad, h.d.surv, h.d.tile_bunch, h.d.bunch, h.ring, h.sections[0].aperture_x,
+      h.sections[0].aperture_y, mode, h.d.fir_kick, inv_beta2, h.d.loss_count, h.d.counters,
+      h.d.mom, h.d.status, mark);
+  return cudaGetLastError();
+}
+
+__global__ void k_turn_advance(int* turn) { *turn += 1; }
+cudaError_t launch_turn_advance(Handle& h) {
+  k_turn_advance<<<1, 1, 0, h.stream>>>(h.d.turn);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Seeded initial distribution: MPBunch::DistriGenerator type 3
+// (MPBunch.cpp:134-277) with counter-based draws: (z, dp) Gaussian cut at
+// 3 sigma jointly, transverse Gaussian in action-angle cut at 3 sigma in
+// (x/rX)^2 + (y/rY)^2, plus dispersion (MPBunch.cpp:268-277).
+
+__global__ void __launch_bounds__(kTile) k_gaussian(double* __restrict__ c, int64_t npad,
+                                                    uint8_t* __restrict__ surv,
+                                                    const int* __restrict__ tile_bunch,
+                                                    const BunchDev* __restrict__ bunch,
+                                                    const SectionDev* __restrict__ sec0,
+                                                    double emit_x, double emit_y, double sz,
+                                                    double sdp, double r_beta2, uint64_t seed) {
+  TileIdx t = tile_index(tile_bunch, bunch);
+  if (!t.valid) {
+    surv[t.g] = 0xFF;  // padding slot: never alive
+#pragma unroll
+    for (int d = 0; d < 6; ++d) c[d * npad + t.g] = 0.0;
+    return;
+  }
+  const SectionDev& s = *sec0;
+  const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32) ^ kStreamInitDist;
+  double z = 0, dp = 0;
+  for (uint32_t a = 0;; ++a) {
+    u32x4 ctr = {{(uint32_t)t.i, (uint32_t)t.b, a, 0u}};
+    double g0, g1;
+    normal2(philox4x32_10(ctr, k0, k1), &g0, &g1);
+    if (g0 * g0 + g1 * g1 < 9.0) {
+      z = sz * g0;
+      dp = sdp * g1 / r_beta2;
+      break;
+    }
+  }
+  double rx = sqrt(emit_x * s.beta_x), ry = sqrt(emit_y * s.beta_y);
+  double x = 0, px = 0, y = 0, py = 0;
+  for (uint32_t a = 0;; ++a) {
+    u32x4 ctr = {{(uint32_t)t.i, (uint32_t)t.b, a, 1u}};
+    double g0, g1, g2, g3;
+    normal2(philox4x32_10(ctr, k0, k1), &g0, &g1);
+    ctr.v[3] = 2u;
+    normal2(philox4x32_10(ctr, k0, k1), &g2, &g3);
+    // normalised phase space (u, u') ~ N(0, emit) per plane
+    double ux = sqrt(emit_x) * g0, upx = sqrt(emit_x) * g1;
+    double uy = sqrt(emit_y) * g2, upy = sqrt(emit_y) * g3;
+    x = sqrt(s.beta_x) * ux;
+    px = (upx - s.alpha_x * ux) / sqrt(s.beta_x);
+    y = sqrt(s.beta_y) * uy;
+    py = (upy - s.alpha_y * uy) / sqrt(s.beta_y);
+    if ((x / rx) * (x / rx) + (y / ry) * (y / ry) <= 9.0) break;
+  }
+  x += s.eta_x * dp;
+  y += s.eta_y * dp;
+  px += s.etap_x * dp;
+  py += s.etap_y * dp;
+  double v[6] = {x, px, y, py, z, dp};
+  store6(c, npad, t.g, v);
+  surv[t.g] = kAlive;
+}
+
+cudaError_t launch_gaussian(Handle& h, double emit_x, double emit_y, double sigma_z,
+                            double sigma_dp, uint64_t seed) {
+  double rb2 = h.cfg.ring.r_beta * h.cfg.ring.r_beta;
+  k_gaussian<<<h.n_tiles, kTile, 0, h.stream>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch,
+                                                h.d.bunch, h.sec_dev, emit_x, emit_y, sigma_z,
+                                                sigma_dp, rb2, seed);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Stateless evaluators.
+
+__global__ void k_faddeeva(const double* __restrict__ zr, const double* __restrict__ zi,
+                           double* wr, double* wi, int64_t n, bool general) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  cplx w = general ? w_general(zr[i], zi[i]) : w_quadrant1(zr[i], zi[i]);
+  wr[i] = w.re;
+  wi[i] = w.im;
+}
+
+cudaError_t launch_faddeeva(const double* zr, const double* zi, double* wr, double* wi, int64_t n,
+                            bool general, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  int64_t blocks = (n + 255) / 256;
+  k_faddeeva<<<(unsigned)blocks, 256, 0, s>>>(zr, zi, wr, wi, n, general);
+  return cudaGetLastError();
+}
+
+__global__ void k_field(const double* __restrict__ x, const double* __restrict__ y,
+                        const double* __restrict__ sx, const double* __restrict__ sy, double* fx,
+                        double* fy, int64_t n) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  gaussian_field(x[i], y[i], sx[i], sy[i], &fx[i], &fy[i]);
+}
+
+cudaError_t launch_field(const double* x, const double* y, const double* sx, const double* sy,
+                         double* fx, double* fy, int64_t n, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  int64_t blocks = (n + 255) / 256;
+  k_field<<<(unsigned)blocks, 256, 0, s>>>(x, y, sx, sy, fx, fy, n);
+  return cudaGetLastError();
+}
+
+cudaError_t upload_weideman_table() {
+  return cudaMemcpyToSymbol(c_weideman, &h_weideman, sizeof(WeidemanTable));
+}
+
+}  // namespace cg

@@ -1,0 +1,40 @@
+// Kernel launchers of libcetagpu (host-callable, implemented in kernels.cu).
+#pragma once
+#include "cg_internal.h"
+
+namespace cg {
+
+// status word bits (DeviceBufs::status[0])
+enum : int {
+  kStatusIonOverflow = 1,
+  kStatusTransmission = 2,
+  kStatusLrRange = 4,
+};
+
+cudaError_t launch_moments(Handle& h, int k);
+cudaError_t launch_map(Handle& h, int k);
+cudaError_t launch_ion_chain(Handle& h, int k);
+cudaError_t launch_ion_kick(Handle& h, int k);
+enum LongFlags : unsigned {
+  kLongRF = 1,
+  kLongDrift = 2,
+  kLongLoss = 4,
+  kLongSynrad = 8,
+  kLongLR = 16,
+};
+cudaError_t launch_long(Handle& h, unsigned flags);
+cudaError_t launch_lr_compute(Handle& h);
+cudaError_t launch_lr_kick(Handle& h);
+cudaError_t launch_fir_compute(Handle& h);
+cudaError_t launch_mark_lost(Handle& h, bool fir_kick, bool mark);
+cudaError_t launch_sr_wake(Handle& h);
+cudaError_t launch_turn_advance(Handle& h);
+cudaError_t launch_gaussian(Handle& h, double emit_x, double emit_y, double sigma_z,
+                            double sigma_dp, uint64_t seed);
+cudaError_t launch_faddeeva(const double* zr, const double* zi, double* wr, double* wi, int64_t n,
+                            bool general, cudaStream_t s);
+cudaError_t launch_field(const double* x, const double* y, const double* sx, const double* sy,
+                         double* fx, double* fy, int64_t n, cudaStream_t s);
+cudaError_t upload_weideman_table();
+
+}  // namespace cg

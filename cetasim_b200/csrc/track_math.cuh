@@ -1,0 +1,258 @@
+// Per-particle and per-bunch arithmetic of the tracking stages, written once
+// as __host__ __device__ functions so that the sm_100a kernels and the CPU
+// self-check build (tests compile this header with g++) run the same code.
+#pragma once
+#include "cg_common.cuh"
+#include "be_field.cuh"
+
+namespace cg {
+
+// ---------------------------------------------------------------------------
+// Device-resident parameter blocks (plain structs, copied to __constant__ or
+// global memory by the host).
+
+struct SectionDev {
+  double beta_x, alpha_x, beta_y, alpha_y;
+  double eta_x, etap_x, eta_y, etap_y;
+  double phase_adv_x, phase_adv_y;
+  double weigh_x, weigh_y;           // phaseAdv / (2 pi nu), Bunch.cpp:662-663
+  double aperture_x, aperture_y;
+  double b1h1[36], h1b1[36], h2b2[36];
+};
+
+struct RingDev {
+  double chrom[2];
+  double adtx[5], adty[5];
+  double circ_ring, alphac[3];
+  double energy, r_beta2, u0_term;   // u0 / E / beta^2 (Bunch.cpp:490)
+  double rf_theta_coeff[4];          // 2 pi h_c f_RF / (c beta), Bunch.cpp:468
+  double vreq_re[4], vreq_im[4];
+  int n_cav;
+  double lambda[3], qe_coeff[3];     // synrad (Bunch.cpp:973-980)
+  double z_loss;                     // t0 c / h / 2 (Bunch.cpp:181)
+  double r_gamma;
+};
+
+// y = A v with the inner index ascending (the order of GSL's dgemm loop).
+CG_HD void matvec6(const double* A, const double v[6], double out[6]) {
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    double acc = A[6 * i] * v[0];
+#pragma unroll
+    for (int k = 1; k < 6; ++k) acc = fma(A[6 * i + k], v[k], acc);
+    out[i] = acc;
+  }
+}
+
+// Bunch::BunchTransferDueToLatticeTSymplectic for one alive particle
+// (Bunch.cpp:664-740): dispersion removed for the amplitude, tune shift from
+// chromaticity and amplitude-dependent detuning, then
+// v <- H2B2 . R(phi_x, phi_y) . B1H1 . v.
+CG_HD void section_map_particle(const SectionDev& s, const RingDev& r, double v[6]) {
+  const double dp = v[5];
+  double x = v[0] - s.eta_x * dp;
+  double px = v[1] - s.etap_x * dp;
+  double y = v[2] - s.eta_y * dp;
+  double py = v[3] - s.etap_y * dp;
+  double ux = fma(s.alpha_x, x, s.beta_x * px);
+  double uy = fma(s.alpha_y, y, s.beta_y * py);
+  double ampX = fma(x, x, ux * ux) / s.beta_x;
+  double ampY = fma(y, y, uy * uy) / s.beta_y;
+  double ax2 = ampX * ampX, ay2 = ampY * ampY, axy = ampX * ampY;
+  double dnux = r.chrom[0] * dp + r.adtx[0] * ampX + r.adtx[1] * ampY + r.adtx[2] * ax2 / 2 +
+                r.adtx[3] * ay2 / 2 + r.adtx[4] * axy;
+  double dnuy = r.chrom[1] * dp + r.adty[0] * ampX + r.adty[1] * ampY + r.adty[2] * ax2 / 2 +
+                r.adty[3] * ay2 / 2 + r.adty[4] * axy;
+  dnux *= s.weigh_x;
+  dnuy *= s.weigh_y;
+  double phiX = s.phase_adv_x + 2 * kPi * dnux;
+  double phiY = s.phase_adv_y + 2 * kPi * dnuy;
+  double sx, cx, sy, cy;
+  sincos(phiX, &sx, &cx);
+  sincos(phiY, &sy, &cy);
+  double v1[6];
+  matvec6(s.b1h1, v, v1);
+  double v2[6];
+  v2[0] = fma(cx, v1[0], sx * v1[1]);
+  v2[1] = fma(-sx, v1[0], cx * v1[1]);
+  v2[2] = fma(cy, v1[2], sy * v1[3]);
+  v2[3] = fma(-sy, v1[2], cy * v1[3]);
+  v2[4] = v1[4];
+  v2[5] = v1[5];
+  matvec6(s.h2b2, v2, v);
+}
+
+// Bunch::BunchMomentumUpdateDueToRFCA (Bunch.cpp:466-472), every particle.
+CG_HD double rf_kick_dp(const RingDev& r, double z, double dp) {
+  for (int c = 0; c < r.n_cav; ++c) {
+    double th = z * r.rf_theta_coeff[c];
+    double s, co;
+    sincos(th, &s, &co);
+    // Re(V e^{-i th}) = Vr cos th + Vi sin th
+    double re = fma(r.vreq_re[c], co, r.vreq_im[c] * s);
+    dp += re / r.energy / r.r_beta2;
+  }
+  return dp;
+}
+
+// Bunch::BunchLongPosTransferOneTurn (Bunch.cpp:499-500).
+CG_HD double drift_z(const RingDev& r, double z, double dp) {
+  double poly = fma(r.alphac[2], dp * dp * dp, fma(r.alphac[1], dp * dp, r.alphac[0] * dp));
+  return z - r.circ_ring * poly;
+}
+
+// Bunch::BunchSynRadDamping for one alive particle (Bunch.cpp:995-1040) with
+// the standard normals g[0..5] (g[4] is drawn but unused, as in the reference).
+CG_HD void synrad_particle(const SectionDev& s0, const RingDev& r, double v[6],
+                           const double g[6], bool excite) {
+  double X[6];
+  matvec6(s0.b1h1, v, X);
+  X[0] *= r.lambda[0];
+  X[1] *= r.lambda[0];
+  X[2] *= r.lambda[1];
+  X[3] *= r.lambda[1];
+  X[5] *= r.lambda[2] * r.lambda[2];
+  if (excite) {
+    X[0] = fma(r.qe_coeff[0], g[0], X[0]);
+    X[1] = fma(r.qe_coeff[0], g[1], X[1]);
+    X[2] = fma(r.qe_coeff[1], g[2], X[2]);
+    X[3] = fma(r.qe_coeff[1], g[3], X[3]);
+    X[5] = fma(r.qe_coeff[2], g[5], X[5]);
+  }
+  matvec6(s0.h1b1, X, v);
+}
+
+// Six synrad normals of particle i of bunch j at turn `turn`.
+CG_HD void synrad_normals(uint64_t seed, uint32_t i, uint32_t j, uint32_t turn, double g[6]) {
+  const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32) ^ kStreamSynrad;
+#pragma unroll
+  for (uint32_t q = 0; q < 3; ++q) {
+    u32x4 c = {{i, j, turn, q}};
+    normal2(philox4x32_10(c, k0, k1), &g[2 * q], &g[2 * q + 1]);
+  }
+}
+
+// Bunch::MarkLostParticle per particle (Bunch.cpp:179-191): returns the
+// number of loss conditions met (0, 1 or 2; the reference counts both) and
+// updates the survival code.
+CG_HD int mark_lost_particle(const RingDev& r, double ax, double ay, double x, double y, double z,
+                             uint8_t* surv) {
+  int count = 0;
+  if (fabs(z) > r.z_loss) {
+    *surv = 2;
+    count++;
+  }
+  double tx = x / ax, ty = y / ay;
+  if (fma(tx, tx, ty * ty) > 1) {
+    *surv = 1;
+    count++;
+  }
+  return count;
+}
+
+// ---------------------------------------------------------------------------
+// Moments: per-tile partials merged with Chan, Golub & LeVeque's pairwise
+// update, in a fixed order, so the result is deterministic and two-pass
+// accurate (the reference makes two passes, MPBunch.cpp:355-455).
+
+struct MomPartial {
+  double n;
+  double mean[6];
+  double c[9];        // centred co-moments: xx pxpx yy pypy zz pzpz xpx ypy zpz
+  double zmin, zmax;  // alive only
+};
+
+CG_HD void mom_clear(MomPartial& p) {
+  p.n = 0;
+  for (int d = 0; d < 6; ++d) p.mean[d] = 0;
+  for (int d = 0; d < 9; ++d) p.c[d] = 0;
+  p.zmin = INFINITY;
+  p.zmax = -INFINITY;
+}
+
+// a <- a (+) b
+CG_HD void mom_merge(MomPartial& a, const MomPartial& b) {
+  if (b.n == 0) return;
+  if (a.n == 0) {
+    a = b;
+    return;
+  }
+  double n = a.n + b.n;
+  double f = b.n / n;
+  double w = a.n * b.n / n;
+  double d[6];
+  for (int k = 0; k < 6; ++k) d[k] = b.mean[k] - a.mean[k];
+  const int ia[9] = {0, 1, 2, 3, 4, 5, 0, 2, 4};
+  const int ib[9] = {0, 1, 2, 3, 4, 5, 1, 3, 5};
+  for (int k = 0; k < 9; ++k) a.c[k] = a.c[k] + b.c[k] + d[ia[k]] * d[ib[k]] * w;
+  for (int k = 0; k < 6; ++k) a.mean[k] = fma(d[k], f, a.mean[k]);
+  a.n = n;
+  a.zmin = fmin(a.zmin, b.zmin);
+  a.zmax = fmax(a.zmax, b.zmax);
+}
+
+// Bunch-level outputs of MPBunch::GetMPBunchRMS (MPBunch.cpp:390-497) from
+// the merged partial.  beta_x/beta_y are the twiss betas of the section k
+// the call names; z0 is particle 0's z (GetZMinMax seeds with it).
+struct BunchMomDev {
+  double n_alive;
+  double mean[6];
+  double emit[3], eff_emit[3];
+  double rms_x, rms_y, eff_rms_x, eff_rms_y;
+  double bunch_length, energy_spread;
+  double z_min, z_max;
+  double transmission;
+  double pad;
+};
+
+CG_HD void mom_finalize(const MomPartial& p, double beta_x, double beta_y, double z0,
+                        BunchMomDev& m) {
+  double n = p.n;
+  m.n_alive = n;
+  for (int k = 0; k < 6; ++k) m.mean[k] = p.mean[k];
+  double x2 = p.c[0] / n, px2 = p.c[1] / n, y2 = p.c[2] / n, py2 = p.c[3] / n;
+  double z2 = p.c[4] / n, pz2 = p.c[5] / n, xpx = p.c[6] / n, ypy = p.c[7] / n, zpz = p.c[8] / n;
+  m.emit[0] = sqrt(x2 * px2 - xpx * xpx);
+  m.emit[1] = sqrt(y2 * py2 - ypy * ypy);
+  m.emit[2] = sqrt(z2 * pz2 - zpz * zpz);
+  m.rms_x = sqrt(m.emit[0] * beta_x);
+  m.rms_y = sqrt(m.emit[1] * beta_y);
+  m.bunch_length = sqrt(z2);
+  m.energy_spread = sqrt(pz2);
+  // uncentred second moments <u^2> = centred + mean^2 ("effective" emittance)
+  const double* a = p.mean;
+  double rx2 = x2 + a[0] * a[0], rpx2 = px2 + a[1] * a[1], rxpx = xpx + a[0] * a[1];
+  double ry2 = y2 + a[2] * a[2], rpy2 = py2 + a[3] * a[3], rypy = ypy + a[2] * a[3];
+  double rz2 = z2 + a[4] * a[4], rpz2 = pz2 + a[5] * a[5], rzpz = zpz + a[4] * a[5];
+  m.eff_emit[0] = sqrt(rx2 * rpx2 - rxpx * rxpx);
+  m.eff_emit[1] = sqrt(ry2 * rpy2 - rypy * rypy);
+  m.eff_emit[2] = sqrt(rz2 * rpz2 - rzpz * rzpz);
+  m.eff_rms_x = sqrt(m.eff_emit[0] * beta_x);
+  m.eff_rms_y = sqrt(m.eff_emit[1] * beta_y);
+  double zmin = fmin(z0, p.zmin), zmax = fmax(z0, p.zmax);
+  m.z_min = zmin - 1.e-6;
+  m.z_max = zmax + 1.e-6;
+}
+
+// ---------------------------------------------------------------------------
+// Ion-cloud Gaussian seen by the electrons of one bunch (MPBunch.cpp:
+// 1170-1206): coeffE = 2 N_ion r_e / gamma, rms, centroid.
+struct CloudRec {
+  double coeff, rms_x, rms_y, aver_x, aver_y, count;
+};
+
+// Electron-side kick of one particle from all species (MPBunch.cpp:1166-1206).
+CG_HD void ion_kick_particle(const CloudRec* rec, int n_species, double x, double y, double* dpx,
+                             double* dpy) {
+  double fx = 0, fy = 0;
+  for (int p = 0; p < n_species; ++p) {
+    double ex, ey;
+    gaussian_field(x - rec[p].aver_x, y - rec[p].aver_y, rec[p].rms_x, rec[p].rms_y, &ex, &ey);
+    fx = fma(rec[p].coeff, ex, fx);
+    fy = fma(rec[p].coeff, ey, fy);
+  }
+  *dpx = fx;
+  *dpy = fy;
+}
+
+}  // namespace cg

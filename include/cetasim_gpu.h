@@ -1,0 +1,311 @@
+/*
+ * cetasim_gpu.h -- C ABI of libcetagpu.so, the sm_100a implementation of the
+ * CETASim multi-particle (MP) tracking path.
+ *
+ * The reference has no plugin or FFI layer: its boundary is the C++ method
+ * surface of MPBeam (include/MPBeam.h:131-177), the per-bunch state of
+ * MPBunch/Bunch (include/Bunch.h:43-105, include/MPBunch.h:43-77), the ion
+ * state of LatticeInterActionPoint (include/LatticeInterActionPoint.h:75-120)
+ * and the input.dat keyword set (src/ReadInputSettings.cpp:81-920).  Each
+ * entry point below names the reference method it replaces.  All arguments
+ * are plain C types and host pointers; device memory is owned by the handle.
+ *
+ * Conventions
+ *   - Every function returns a cg_status (0 = CG_OK).  Nothing in the library
+ *     calls exit(); where the reference exits (ion overflow LIP.cpp:1043-1048,
+ *     transmission < 0.5 Bunch.cpp:194-197, bad fill pattern Train.cpp:79-86)
+ *     the call returns a status and cg_last_error() holds the message.
+ *   - A handle is bound to one CUDA device and one stream; it is not
+ *     thread-safe.  Calls are host-synchronous unless stated otherwise.
+ *   - Coordinates follow the reference: x [m], px [rad], y [m], py [rad],
+ *     z [m] (head positive), dp = momentum deviation.
+ */
+#ifndef CETASIM_GPU_H
+#define CETASIM_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CG_ABI_VERSION 1
+#define CG_MAX_SPECIES 8
+#define CG_MAX_CAVITIES 4
+#define CG_MAX_RESONATORS 16
+#define CG_MAX_FIR 64
+#define CG_MAX_FB_SECTIONS 8
+
+typedef enum cg_status {
+  CG_OK = 0,
+  CG_ERR_INVALID = 1,        /* bad argument or configuration */
+  CG_ERR_OOM = 2,            /* device allocation failed */
+  CG_ERR_CUDA = 3,           /* CUDA runtime error */
+  CG_ERR_ION_OVERFLOW = 4,   /* accumulated ions > ionCalIonMaxNumber (LIP.cpp:1043-1048) */
+  CG_ERR_TRANSMISSION = 5,   /* a bunch lost more than half its particles (Bunch.cpp:194-197) */
+  CG_ERR_TIMEOUT = 6,        /* a bounded device wait gave up */
+  CG_ERR_NOT_READY = 7,      /* call order violated (e.g. no beam set) */
+  CG_ERR_UNSUPPORTED = 8     /* option not built */
+} cg_status;
+
+/* Ring constants after ReadInputSettings::ParamRead's derivations
+ * (src/ReadInputSettings.cpp:986-1081).  cg_config_derive() fills the derived
+ * fields from the raw ones exactly as the reference does. */
+typedef struct cg_ring {
+  /* raw input.dat values */
+  double circ_ring;            /* ringCircRing [m] */
+  double work_qx, work_qy;     /* ringWorkQ (the third value is recomputed) */
+  double chrom[2];             /* ringChrom */
+  double alphac[3];            /* ringAlphac */
+  double adtx[5], adty[5];     /* ringADTX / ringADTY */
+  double synch_rad_damp_time[3]; /* ringSynchRadDampTime [turns] */
+  double pipe_aperture_x, pipe_aperture_y; /* ringPipeAperatureX/Y [m] */
+  double electron_energy;      /* ringElectronBeamEnergy [eV] */
+  double sdelta0;              /* ringSdelta0 */
+  double natural_emit;         /* ringNaturalEmit [m rad] */
+  double coupling;             /* ringCoupling */
+  double u0;                   /* ringU0 [eV] */
+  double skew_quad_k;          /* ringskewQuadK [1/m] */
+  int harmonics;               /* rfRingHarm */
+  int n_cav;                   /* rfResNum (RFCA cavities; rfMode 0) */
+  int cav_harm[CG_MAX_CAVITIES];   /* rfResHarm */
+  double cav_vol[CG_MAX_CAVITIES]; /* rfResVol [V] */
+  double cav_phase[CG_MAX_CAVITIES]; /* rfResPhase [rad] (overridden for one cavity) */
+  /* derived (cg_config_derive) */
+  double r_gamma, r_beta, t0, f0, eta, work_qz;
+  double natural_bunch_length, beta_z;
+  double emit_nat[3];
+  double cav_vreq_re[CG_MAX_CAVITIES], cav_vreq_im[CG_MAX_CAVITIES];
+} cg_ring;
+
+/* One lattice section / interaction point k (LatticeInterActionPoint.h:41-90;
+ * twiss file columns LIP.cpp:222-240). */
+typedef struct cg_section {
+  double s;                      /* elemPos [m] */
+  double beta_x, alpha_x, psi_x, eta_x, etap_x, aperture_x;
+  double beta_y, alpha_y, psi_y, eta_y, etap_y, aperture_y;
+  double length;                 /* interactionLength [m] (recomputed) */
+  double pressure;               /* vacuumPressure [Pa] */
+  double temperature;            /* [K] */
+  /* derived by cg_lattice_init (LIP.cpp:257-433) */
+  double phase_adv_x, phase_adv_y; /* phaseAdvX12[k], phaseAdvY12[k] */
+  double map_b1h1[36];           /* symplecticMapB1H1[k], row-major */
+  double map_h1b1[36];           /* symplecticMapInvH1InvB1[k] */
+  double map_h2b2[36];           /* symplecticMapInvH2InvB2[k] */
+} cg_section;
+
+/* Ion species and cloud limits (ReadInputSettings.h RingIonEffPara). */
+typedef struct cg_ion_params {
+  int n_species;                           /* ionCalGasSpec */
+  double mass_number[CG_MAX_SPECIES];      /* ionCalIonMassNumber */
+  double cross_section[CG_MAX_SPECIES];    /* ionCalCorssSectionEI [m^2] (x1e-22 applied) */
+  double gas_percent[CG_MAX_SPECIES];      /* ionCalIongasPercent */
+  double loss_boundary;                    /* ionCalIonlossboundary */
+  int max_ions;                            /* ionCalIonMaxNumber */
+  int macro_ions_per_ip;                   /* ionCalMacroIonNumberGeneratedPerIP */
+} cg_ion_params;
+
+/* Broadband resonators (BBR input file, WakeFunction.cpp:251-290); omegas are
+ * angular frequencies (file value x 2 pi). */
+typedef struct cg_bbr {
+  int n;
+  double l_rs[CG_MAX_RESONATORS], l_q[CG_MAX_RESONATORS], l_omega[CG_MAX_RESONATORS];
+  double tx_rs[CG_MAX_RESONATORS], tx_q[CG_MAX_RESONATORS], tx_omega[CG_MAX_RESONATORS];
+  double ty_rs[CG_MAX_RESONATORS], ty_q[CG_MAX_RESONATORS], ty_omega[CG_MAX_RESONATORS];
+} cg_bbr;
+
+typedef struct cg_fir_params {
+  int mode;                      /* fbMode: 0 ideal, 1 FIR */
+  int delay, taps;               /* fbDelay, fbTaps */
+  double gain;                   /* fbGain */
+  double kick_strength[3];       /* fbKickStrengthKx/Ky/F */
+  double power_limit;            /* fbFIRBunchByBunchFeedbackPowerLimit [W] */
+  double kicker_imped;           /* fbFIRBunchByBunchFeedbackKickerImped [Ohm] */
+  double coeff_x[CG_MAX_FIR], coeff_y[CG_MAX_FIR], coeff_z[CG_MAX_FIR]; /* length delay+taps, zeros first */
+  int n_sections;                /* fbnumberofSections */
+  int start[CG_MAX_FB_SECTIONS], end[CG_MAX_FB_SECTIONS];
+} cg_fir_params;
+
+typedef struct cg_config {
+  cg_ring ring;
+  int n_sections;                /* ringSectNum */
+  const cg_section* sections;    /* borrowed during cg_create; copied */
+  cg_ion_params ion;
+  cg_bbr sr_bbr;                 /* SRWBBRInput resonators */
+  int sr_bins;                   /* SRWBunchBinNum */
+  cg_bbr lr_bbr;                 /* LRWBBRInput resonators */
+  int lr_turns;                  /* LRWNTurnsWakeTrunction + 1 (as stored by the parser) */
+  cg_fir_params fir;
+  int flag_synrad;               /* runSynRadDampingFlag */
+  int flag_beam_ion;             /* runBeamIonFlag */
+  int flag_lr_wake;              /* runLongRangeWake */
+  int flag_sr_wake;              /* runShortRangeWake */
+  int flag_fir;                  /* runFIRBunchByBunchFeedbackFlag */
+  uint64_t seed;                 /* Philox key for every random draw */
+  /* run and initial-bunch settings (read by cg_config_from_input; the
+     library's stage calls do not use them) */
+  int n_turns;                   /* runNTurns */
+  int bunch_info_print_interval; /* runBunchInfoPrintInterval */
+  double bunch_emit_x, bunch_emit_y; /* bunchEmittance/(1+kappa), x kappa (ReadInputSettings.cpp:1012-1016) */
+  double bunch_sigma_z;          /* bunchRmsBunchLength */
+  double bunch_sigma_dp;         /* bunchRmsEnergySpread */
+} cg_config;
+
+/* Per-bunch moments, the fields MPBunch::GetMPBunchRMS sets
+ * (MPBunch.cpp:342-498). */
+typedef struct cg_bunch_moments {
+  int n_alive;                   /* macroEleNumSurivePerBunch */
+  int n_macro;
+  double mean[6];                /* xAver pxAver yAver pyAver zAver pzAver */
+  double emit[3];                /* emittanceX/Y/Z */
+  double eff_emit[3];            /* rmsEffectiveRingEmitX/Y/Z */
+  double rms_x, rms_y;           /* rmsRx, rmsRy */
+  double eff_rms_x, eff_rms_y;   /* rmsEffectiveRx/Ry */
+  double bunch_length;           /* rmsBunchLength */
+  double energy_spread;          /* rmsEnergySpread */
+  double z_min, z_max;           /* zMinCurrentTurn, zMaxCurrentTurn */
+  double transmission;
+} cg_bunch_moments;
+
+typedef struct cg_handle cg_handle;
+
+/* ---- configuration (host only, no device needed) ---- */
+
+/* Version of this ABI (CG_ABI_VERSION). */
+int cg_abi_version(void);
+
+/* Fills cfg->ring derived fields (ReadInputSettings.cpp:986-1081 and
+ * CavityResonator::Initial, CavityResonator.cpp:121-131). */
+int cg_config_derive(cg_config* cfg);
+
+/* Recomputes section lengths/phase advances and builds the symplectic maps
+ * (LatticeInterActionPoint::InitialLattice LIP.cpp:257-283 and
+ * InitialLatticeSympMat LIP.cpp:326-433). */
+int cg_lattice_init(const cg_ring* ring, cg_section* sections, int n_sections);
+
+/* Parses an input.dat (ReadInputSettings::ParamRead, ReadInputSettings.cpp:
+ * 46-1085) plus the twiss file (LIP::InitialLattice, LIP.cpp:181-290) and the
+ * BBR files (WakeFunction::BBRWakeParaReadIn, WakeFunction.cpp:251-290) it
+ * names, relative paths resolved against the input file's directory first.
+ * Fills cfg (derived fields and lattice maps included) and the bunch train
+ * (Train::Initial, Train.cpp:38-104; MPBeam::Initial, MPBeam.cpp:64-106):
+ * per-bunch macroparticle counts, harmonic numbers and electrons per bunch.
+ * The arrays and cfg->sections are allocated by the library; release them
+ * with cg_config_free.  Keys outside the MP tracking path are accepted and
+ * ignored, except settings this library does not implement (rfMode 1,
+ * runBBIFlag, runSpaceCharge, ionCalSCMethod 2, driveModeOn, runRamping),
+ * which return CG_ERR_UNSUPPORTED.  Optional keys beyond the reference:
+ * bunchMacroEleNumPerBunchList (one count per bunch) and runRandomSeed. */
+int cg_config_from_input(const char* path, cg_config* cfg, int* n_bunches, int** n_macro,
+                         int** bunch_harm, double** bunch_ne);
+void cg_config_free(cg_config* cfg, int* n_macro, int* bunch_harm, double* bunch_ne);
+/* Message of the last failing cg_config_from_input on the calling thread
+ * (the reference prints these and exits, ReadInputSettings.cpp:62-66). */
+const char* cg_parse_error(void);
+
+/* ---- handle ---- */
+
+/* Creates a handle on CUDA device `device` (ReadInputSettings/LIP/Train/
+ * WakeFunction/FIRFeedBack initialisation). */
+int cg_create(const cg_config* cfg, int device, cg_handle** out);
+int cg_destroy(cg_handle* h);
+/* Message of the last failing call on h (or of cg_create when h is NULL). */
+const char* cg_last_error(const cg_handle* h);
+
+/* Bunch layout (MPBeam::Initial MPBeam.cpp:64-188): M bunches, macroparticles
+ * per bunch (may differ: the reference uses one global count, Bunch.cpp:57),
+ * harmonic numbers, electrons per bunch.  Gaps follow MPBeam.cpp:132-136. */
+int cg_set_beam(cg_handle* h, int n_bunches, const int* n_macro,
+                const int* bunch_harm, const double* n_electrons);
+
+/* Copies one bunch's coordinates and survival flags in / out
+ * (Bunch::ePosition{X,Y,Z}, eMomentum{X,Y,Z}, eSurive). */
+int cg_upload_bunch(cg_handle* h, int j, const double* x, const double* px,
+                    const double* y, const double* py, const double* z,
+                    const double* dp, const uint8_t* surv);
+int cg_download_bunch(cg_handle* h, int j, double* x, double* px, double* y,
+                      double* py, double* z, double* dp, uint8_t* surv);
+
+/* Seeded 6-D Gaussian generation on the device, the distribution type 3 of
+ * MPBunch::DistriGenerator (MPBunch.cpp:98-298) with Philox draws. */
+int cg_generate_gaussian(cg_handle* h, double emit_x, double emit_y,
+                         double sigma_z, double sigma_dp, uint64_t seed);
+
+/* ---- MPBeam stage methods ---- */
+
+/* MPBeam::MPBeamRMSCal(lip, k) + MPGetBeamInfo (MPBeam.cpp:2125-2317). */
+int cg_beam_rms(cg_handle* h, int k);
+int cg_get_moments(cg_handle* h, cg_bunch_moments* out /* [n_bunches] */);
+
+/* MPBeam::SSBeamIonEffectOneInteractionPoint (MPBeam.cpp:2585-2611), with
+ * the bunch moments of the last cg_beam_rms(h, k). */
+int cg_beam_ion_ip(cg_handle* h, int turn, int k);
+
+/* MPBeam::BeamTransferPerInteractionPointDueToLatticeT (MPBeam.cpp:2613-2621
+ * -> Bunch::BunchTransferDueToLatticeTSymplectic, Bunch.cpp:625-755). */
+int cg_section_map(cg_handle* h, int k);
+
+/* MPBeam::BeamMomtumUpdateDueToRFTest for RFCA cavities (MPBeam.cpp:2624-2706
+ * -> Bunch::BunchMomentumUpdateDueToRFCA, Bunch.cpp:453-481). */
+int cg_rf_kick(cg_handle* h);
+/* MPBeam::BeamLongiPosTransferOneTurn (Bunch.cpp:494-501). */
+int cg_longi_drift(cg_handle* h);
+/* MPBeam::BeamEnergyLossOneTurn (Bunch.cpp:483-491). */
+int cg_energy_loss(cg_handle* h);
+/* MPBeam::BeamSynRadDamping (Bunch.cpp:940-1044); the noise of turn `turn`
+ * is Philox(seed, turn, particle). */
+int cg_synrad(cg_handle* h, int turn);
+/* MPBeam::LRWakeBeamIntaction (MPBeam.cpp:3232-3349). */
+int cg_lr_wake(cg_handle* h);
+/* MPBeam::SRWakeBeamIntaction (MPBeam.cpp:2117-2123 ->
+ * MPBunch::BunchTransferDueToSRWake, MPBunch.cpp:1887-2025). */
+int cg_sr_wake(cg_handle* h, int turn);
+/* Bin geometry and counts of the last cg_sr_wake for bunch j: the bin range
+ * start zlo, the bin width dz and the B per-bin particle counts
+ * (MPBunch.cpp:1900-1919: histoParIndex[i].size()). */
+int cg_sr_bins(cg_handle* h, int j, double* zlo, double* dz, int* counts /* [SRWBunchBinNum] */);
+/* MPBeam::FIRBunchByBunchFeedback (MPBeam.cpp:2978-3090). */
+int cg_fir(cg_handle* h, int turn);
+/* MPBeam::MarkParticleLostInBunch (MPBeam.cpp:1358-1364 -> Bunch.cpp:172-200);
+ * transmissions may be NULL. */
+int cg_mark_lost(cg_handle* h, double* transmissions /* [n_bunches] */);
+
+/* The whole turn loop body of MPBeam::Run (MPBeam.cpp:1010-1102) for turns
+ * [turn0, turn0 + n_turns), as one CUDA graph per turn, without host
+ * round trips. */
+int cg_run_turns(cg_handle* h, int turn0, int n_turns);
+
+/* ---- ion clouds (LatticeInterActionPoint ion state) ---- */
+
+/* Number of accumulated macro-ions at IP k for species p
+ * (ionAccumuNumber[k][p]). */
+int cg_ion_count(cg_handle* h, int k, int p, int* count);
+/* ionAccumuPosition{X,Y}, ionAccumuVelocity{X,Y} of IP k, species p. */
+int cg_ion_download(cg_handle* h, int k, int p, double* x, double* y,
+                    double* vx, double* vy, int capacity, int* count);
+int cg_ion_upload(cg_handle* h, int k, int p, const double* x, const double* y,
+                  const double* vx, const double* vy, int count);
+/* Recorded per-bunch ion-cloud Gaussians of the last cg_beam_ion_ip at IP k
+ * (the moments the electron-side kick used: MPBunch.cpp:1164-1206), as
+ * [n_bunches][n_species][6] = {coeffE, rmsX, rmsY, averX, averY, count}. */
+int cg_ion_cloud_record(cg_handle* h, int k, double* out);
+/* Whole-ring totals (LIP::GetTotIonCharge, LIP.cpp:1213-1229). */
+int cg_ion_totals(cg_handle* h, double* tot_charge, int* tot_macro_ions);
+
+/* ---- stateless evaluators (host buffers in/out) ---- */
+
+/* w(z) for n points (Faddeeva::w, Faddeeva.cpp:682-974); general complex z. */
+int cg_faddeeva_w(const double* zr, const double* zi, double* wr, double* wi,
+                  int64_t n);
+/* The first-quadrant kernel path used by the field kicks. */
+int cg_faddeeva_w_q1(const double* zr, const double* zi, double* wr, double* wi,
+                     int64_t n);
+/* Gaussian-beam field with the reference's dispatch (Bunch.cpp:119-211,
+ * MPBunch.cpp:1128-1146): per point (x, y, sigma_x, sigma_y) -> (Fx, Fy) [1/m]. */
+int cg_gaussian_field(const double* x, const double* y, const double* sx,
+                      const double* sy, double* fx, double* fy, int64_t n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CETASIM_GPU_H */

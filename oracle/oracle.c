@@ -1,0 +1,992 @@
+/*
+ * ORACLE (test infrastructure only; never part of the product path).
+ *
+ * Plain-C restatement of the reference's multi-particle tracking path
+ * (CETASim, MPBeam/MPBunch/Bunch/LatticeInterActionPoint/WakeFunction/
+ * FIRFeedBack).  Each function names the reference lines it follows.  Loops
+ * run in the reference's order and with its expression order, compiled
+ * without FMA contraction (see Makefile), so that rounding follows the
+ * reference's plain C++.  Random draws use the same counter-based Philox
+ * streams as the device code, so stochastic stages can be compared draw for
+ * draw (the reference itself seeds std::mt19937 from std::random_device, so
+ * it is only reproducible statistically).
+ *
+ * Parity unpinned: the reference's tracking sources need GSL and FFTW and do
+ * not build here; only w(z) (faddeeva_q.c) is pinned against the reference.
+ */
+#include "oracle.h"
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* include/Global.h:26-40 */
+#define C_LIGHT 299792458.0
+#define E_CHARGE 1.602017733e-19
+#define E_MASS_EV 0.51099906e6
+#define ION_MASS_EV 931.49432e6
+#define RE_CLASSIC 2.81794092e-15
+#define BOLTZMANN 1.3806505E-23
+static double PI_REF(void) { return 4 * atan(1.E0); }
+
+/* ------------------------------------------------------------------------ */
+/* Philox4x32-10 (Salmon et al., SC'11) and Box-Muller, identical to the     */
+/* device code's stream definitions.                                         */
+static void philox(uint32_t c[4], uint32_t k0, uint32_t k1) {
+  for (int r = 0; r < 10; ++r) {
+    uint64_t p0 = (uint64_t)0xD2511F53u * c[0];
+    uint64_t p1 = (uint64_t)0xCD9E8D57u * c[2];
+    uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+    uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+    uint32_t o0 = hi1 ^ c[1] ^ k0, o1 = lo1, o2 = hi0 ^ c[3] ^ k1, o3 = lo0;
+    c[0] = o0; c[1] = o1; c[2] = o2; c[3] = o3;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+}
+void or_philox_normals(uint64_t seed, uint32_t stream, uint32_t c0, uint32_t c1, uint32_t c2,
+                       uint32_t c3, double* out2) {
+  uint32_t c[4] = {c0, c1, c2, c3};
+  philox(c, (uint32_t)seed, (uint32_t)(seed >> 32) ^ stream);
+  uint64_t m1 = ((uint64_t)(c[0] >> 6) << 27) | (uint64_t)(c[1] >> 5);
+  uint64_t m2 = ((uint64_t)(c[2] >> 6) << 27) | (uint64_t)(c[3] >> 5);
+  double u1 = ((double)m1 + 1.0) * (1.0 / 9007199254740992.0);
+  double u2 = (double)m2 * (1.0 / 9007199254740992.0);
+  double rad = sqrt(-2.0 * log(u1));
+  const double pi = 3.141592653589793115997963468544185161590576171875;
+  out2[0] = rad * cos(2.0 * pi * u2);
+  out2[1] = rad * sin(2.0 * pi * u2);
+}
+#define STREAM_SYNRAD 0x5359u
+#define STREAM_IONBIRTH 0x494Fu
+
+/* ------------------------------------------------------------------------ */
+/* Gaussian field: Bunch::BassettiErskine1 (Bunch.cpp:119-170),              */
+/* Bunch::GaussianField (Bunch.cpp:202-211), dispatch MPBunch.cpp:1128-1146. */
+static void be1(double posx, double posy, double sx, double sy, double* fx, double* fy) {
+  double ax = fabs(posx), ay = fabs(posy);
+  double sigma = sqrt(2 * pow(sx, 2) - 2 * pow(sy, 2));
+  double r = sy / sx;
+  double coeff = -1 * sqrt(PI_REF()) / sigma;
+  double wr[2], wi[2];
+  or_w_fast(ax / sigma, ay / sigma, &wr[0], &wi[0]);
+  or_w_fast(r * ax / sigma, ay / sigma / r, &wr[1], &wi[1]);
+  double z3 = -pow(ax / sx, 2) / 2 - pow(ay / sy, 2) / 2;
+  double w3 = -exp(z3);
+  double re = coeff * (wr[0] + w3 * wr[1]);
+  double im = coeff * (wi[0] + w3 * wi[1]);
+  *fx = im;
+  *fy = re;
+  if (posx <= 0) *fx = -*fx;
+  if (posy <= 0) *fy = -*fy;
+}
+static void round_field(double posx, double posy, double sx, double* fx, double* fy) {
+  double r2 = pow(posx, 2) + pow(posy, 2);
+  double s2 = sx * sx;
+  *fx = -posx / r2 * (1 - exp(-r2 / 2 / s2));
+  *fy = -posy / r2 * (1 - exp(-r2 / 2 / s2));
+}
+static void field(double posx, double posy, double sx, double sy, double* fx, double* fy) {
+  if (fabs(posx / sx) + fabs(posy / sy) < 1.0E-5) {
+    *fx = 0; *fy = 0;
+  } else if ((sx - sy) / sy > 1.e-4) {
+    be1(posx, posy, sx, sy, fx, fy);
+  } else if ((sx - sy) / sy < -1.e-4) {
+    be1(posy, posx, sy, sx, fy, fx);
+  } else {
+    round_field(posx, posy, sx, fx, fy);
+  }
+}
+void or_gaussian_field(const double* x, const double* y, const double* sx, const double* sy,
+                       double* fx, double* fy, int64_t n) {
+  for (int64_t i = 0; i < n; ++i) field(x[i], y[i], sx[i], sy[i], &fx[i], &fy[i]);
+}
+
+/* ------------------------------------------------------------------------ */
+/* ReadInputSettings::ParamRead derived quantities (ReadInputSettings.cpp:   */
+/* 986-1081) and CavityResonator::Initial (CavityResonator.cpp:121-131).      */
+int or_config_derive(cg_config* cfg) {
+  cg_ring* r = &cfg->ring;
+  double PI = PI_REF();
+  double rGamma = r->electron_energy / E_MASS_EV;
+  double eta = r->alphac[0] - 1. / pow(rGamma, 2);
+  double rBeta = sqrt(1.E0 - pow(rGamma, -2));
+  double t0 = r->circ_ring / C_LIGHT / rBeta;
+  double f0 = 1 / t0;
+  double vRF = r->cav_vol[0];
+  double synPhase = PI - asin(r->u0 / vRF);
+  double workQz = sqrt(-1 * eta * r->harmonics * vRF * cos(synPhase) /
+                       (2 * PI * rBeta * r->electron_energy));
+  r->r_gamma = rGamma; r->r_beta = rBeta; r->t0 = t0; r->f0 = f0; r->eta = eta;
+  r->work_qz = workQz;
+  r->natural_bunch_length = eta * C_LIGHT * r->sdelta0 / (2 * PI * workQz * f0);
+  r->emit_nat[0] = r->natural_emit / (1 + r->coupling);
+  r->emit_nat[1] = r->natural_emit / (1 + r->coupling) * r->coupling;
+  r->emit_nat[2] = r->natural_bunch_length * r->sdelta0;
+  r->beta_z = r->natural_bunch_length / r->sdelta0; /* LIP.cpp:242 */
+  double ph[CG_MAX_CAVITIES];
+  for (int i = 0; i < r->n_cav; ++i) ph[i] = r->cav_phase[i];
+  if (r->n_cav == 1) ph[0] = PI - asin(r->u0 / r->cav_vol[0]) - PI / 2.;
+  for (int i = 0; i < r->n_cav; ++i) {
+    r->cav_vreq_re[i] = r->cav_vol[i] * cos(ph[i]);
+    r->cav_vreq_im[i] = r->cav_vol[i] * sin(ph[i]);
+  }
+  return 0;
+}
+
+/* gsl_blas_dgemm(NoTrans, NoTrans, 1, A, B, 0, C) for 6x6 x 6xn: C starts  */
+/* at 0 and accumulates over the inner index in ascending order, skipping   */
+/* zero A entries (GSL's CBLAS loop order).                                  */
+static void dgemm6(const double* A, const double* B, int ncol, double* C) {
+  for (int i = 0; i < 6 * ncol; ++i) C[i] = 0.0;
+  for (int i = 0; i < 6; ++i)
+    for (int k = 0; k < 6; ++k) {
+      double t = A[6 * i + k];
+      if (t != 0.0)
+        for (int j = 0; j < ncol; ++j) C[ncol * i + j] += t * B[ncol * k + j];
+    }
+}
+
+/* LatticeInterActionPoint::InitialLattice (LIP.cpp:242-283) and            */
+/* InitialLatticeSympMat (LIP.cpp:326-433).                                   */
+int or_lattice_init(const cg_ring* ring, cg_section* sec, int n) {
+  double PI = PI_REF();
+  for (int i = 0; i < n; ++i) {
+    if (!(ring->pipe_aperture_x > sec[i].aperture_x)) sec[i].aperture_x = ring->pipe_aperture_x;
+    if (!(ring->pipe_aperture_y > sec[i].aperture_y)) sec[i].aperture_y = ring->pipe_aperture_y;
+  }
+  for (int i = 0; i < n; ++i) {
+    if (i != n - 1) {
+      sec[i].length = sec[i + 1].s - sec[i].s;
+      sec[i].phase_adv_x = sec[i + 1].psi_x - sec[i].psi_x;
+      sec[i].phase_adv_y = sec[i + 1].psi_y - sec[i].psi_y;
+    } else {
+      sec[i].length = ring->circ_ring - sec[i].s + sec[0].s;
+      sec[i].phase_adv_x = 2 * PI * ring->work_qx - sec[i].psi_x + sec[0].psi_x;
+      sec[i].phase_adv_y = 2 * PI * ring->work_qy - sec[i].psi_y + sec[0].psi_y;
+    }
+  }
+  double bz = ring->beta_z;
+  for (int i = 0; i < n; ++i) {
+    const cg_section* a = &sec[i];
+    const cg_section* b = &sec[i < n - 1 ? i + 1 : 0];
+    double H1[36] = {0}, IH1[36] = {0}, IH2[36] = {0}, B1[36] = {0}, IB1[36] = {0}, IB2[36] = {0};
+    for (int d = 0; d < 6; ++d) H1[7 * d] = IH1[7 * d] = IH2[7 * d] = 1.0;
+#define M(A, r, c) A[6 * (r) + (c)]
+    M(H1, 0, 5) = -a->eta_x; M(H1, 1, 5) = -a->etap_x; M(H1, 2, 5) = -a->eta_y; M(H1, 3, 5) = -a->etap_y;
+    M(H1, 4, 0) = a->etap_x; M(H1, 4, 1) = -a->eta_x; M(H1, 4, 2) = a->etap_y; M(H1, 4, 3) = -a->eta_y;
+    M(IH1, 0, 5) = a->eta_x; M(IH1, 1, 5) = a->etap_x; M(IH1, 2, 5) = a->eta_y; M(IH1, 3, 5) = a->etap_y;
+    M(IH1, 4, 0) = -a->etap_x; M(IH1, 4, 1) = a->eta_x; M(IH1, 4, 2) = -a->etap_y; M(IH1, 4, 3) = a->eta_y;
+    M(IH2, 0, 5) = b->eta_x; M(IH2, 1, 5) = b->etap_x; M(IH2, 2, 5) = b->eta_y; M(IH2, 3, 5) = b->etap_y;
+    M(IH2, 4, 0) = -b->etap_x; M(IH2, 4, 1) = b->eta_x; M(IH2, 4, 2) = -b->etap_y; M(IH2, 4, 3) = b->eta_y;
+    M(B1, 0, 0) = 1 / sqrt(a->beta_x); M(B1, 1, 0) = a->alpha_x / sqrt(a->beta_x); M(B1, 1, 1) = sqrt(a->beta_x);
+    M(B1, 2, 2) = 1 / sqrt(a->beta_y); M(B1, 3, 2) = a->alpha_y / sqrt(a->beta_y); M(B1, 3, 3) = sqrt(a->beta_y);
+    M(B1, 4, 4) = 1 / sqrt(bz); M(B1, 5, 5) = sqrt(bz);
+    M(IB1, 0, 0) = sqrt(a->beta_x); M(IB1, 1, 0) = -a->alpha_x / sqrt(a->beta_x); M(IB1, 1, 1) = 1 / sqrt(a->beta_x);
+    M(IB1, 2, 2) = sqrt(a->beta_y); M(IB1, 3, 2) = -a->alpha_y / sqrt(a->beta_y); M(IB1, 3, 3) = 1 / sqrt(a->beta_y);
+    M(IB1, 4, 4) = sqrt(bz); M(IB1, 5, 5) = 1 / sqrt(bz);
+    M(IB2, 0, 0) = sqrt(b->beta_x); M(IB2, 1, 0) = -b->alpha_x / sqrt(b->beta_x); M(IB2, 1, 1) = 1 / sqrt(b->beta_x);
+    M(IB2, 2, 2) = sqrt(b->beta_y); M(IB2, 3, 2) = -b->alpha_y / sqrt(b->beta_y); M(IB2, 3, 3) = 1 / sqrt(b->beta_y);
+    M(IB2, 4, 4) = sqrt(bz); M(IB2, 5, 5) = 1 / sqrt(bz);
+#undef M
+    dgemm6(B1, H1, 6, sec[i].map_b1h1);
+    dgemm6(IH1, IB1, 6, sec[i].map_h1b1);
+    dgemm6(IH2, IB2, 6, sec[i].map_h2b2);
+  }
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* State                                                                     */
+typedef struct {
+  int n, cap;
+  double *x, *y, *vx, *vy, *fx, *fy;
+  double aver_x, aver_y, rms_x, rms_y; /* ionAccumuAver/RMS (stale when n <= 1) */
+  double macro_charge;                 /* macroIonCharge[k][p] */
+} or_cloud;
+
+typedef struct {
+  int n;
+  double *c[6];
+  uint8_t* surv;
+  double *efx, *efy; /* eFxDueToIon (kept per particle, as the reference) */
+  double harm, gap, ne, q_macro;
+  int harm_i, gap_i;
+  cg_bunch_moments m;
+  double sr_pot[3 * 4096]; /* srWakePoten, kept between turns (MPBunch.cpp:1894-1897) */
+  double lr_force[3];
+  double sr_zlo, sr_dz;
+  int sr_counts[4096];
+} or_bunch;
+
+struct or_state {
+  cg_config cfg;
+  cg_section* sec;
+  int K, M, P;
+  or_bunch* b;
+  or_cloud* cloud; /* [K][P] */
+  double* rec;     /* [K][M][P][6] */
+  double size_x_max, size_y_max;
+  /* LR wake */
+  int lr_np;
+  double* lr_tab; /* [3][np] */
+  double lr_dt;
+  double *lr_hist; /* [turns][3][M] (oldest first) */
+  /* FIR */
+  double* fir_hist; /* [order][3][M] */
+  double fir_limit;
+  char err[256];
+};
+
+const char* or_last_error(or_state* s) { return s->err; }
+
+/* WakeFunction::GetBBRWakeFun (WakeFunction.cpp:655-721) */
+static void bbr_wake(const cg_bbr* w, double beta_ip_x, double beta_ip_y, double tau, double out[3]) {
+  out[0] = out[1] = out[2] = 0;
+  for (int i = 0; i < w->n; i++) {
+    double alpha = w->tx_omega[i] / 2.0 / w->tx_q[i];
+    double omegab = sqrt(pow(w->tx_omega[i], 2) - pow(alpha, 2));
+    double coeff = C_LIGHT * w->tx_rs[i] * w->tx_omega[i] / w->tx_q[i] / omegab * exp(alpha * tau) * sin(omegab * tau);
+    out[0] += coeff / beta_ip_x;
+    alpha = w->ty_omega[i] / 2.0 / w->ty_q[i];
+    omegab = sqrt(pow(w->ty_omega[i], 2) - pow(alpha, 2));
+    coeff = C_LIGHT * w->ty_rs[i] * w->ty_omega[i] / w->ty_q[i] / omegab * exp(alpha * tau) * sin(omegab * tau);
+    out[1] += coeff / beta_ip_y;
+  }
+  for (int i = 0; i < w->n; i++) {
+    double alpha = w->l_omega[i] / 2.0 / w->l_q[i];
+    double omegab = sqrt(pow(w->l_omega[i], 2) - pow(alpha, 2));
+    double coeff = 2 * alpha * w->l_rs[i] * exp(alpha * tau);
+    double coeff1 = cos(omegab * tau);
+    double coeff2 = sin(omegab * tau) * alpha / omegab;
+    if (tau == 0) out[2] += coeff / 2;
+    else out[2] += coeff * (coeff1 + coeff2);
+  }
+}
+
+or_state* or_create(const cg_config* cfg, int M, const int* n_macro, const int* harm,
+                    const double* ne) {
+  or_state* s = (or_state*)calloc(1, sizeof(or_state));
+  s->cfg = *cfg;
+  s->K = cfg->n_sections;
+  s->sec = (cg_section*)malloc(sizeof(cg_section) * s->K);
+  memcpy(s->sec, cfg->sections, sizeof(cg_section) * s->K);
+  s->cfg.sections = s->sec;
+  s->M = M;
+  s->P = cfg->ion.n_species > 0 ? cfg->ion.n_species : 1;
+  s->b = (or_bunch*)calloc(M, sizeof(or_bunch));
+  int H = cfg->ring.harmonics;
+  for (int j = 0; j < M; ++j) {
+    or_bunch* b = &s->b[j];
+    b->n = n_macro[j];
+    for (int d = 0; d < 6; ++d) b->c[d] = (double*)calloc(b->n, sizeof(double));
+    b->surv = (uint8_t*)calloc(b->n, 1);
+    b->efx = (double*)calloc(b->n, sizeof(double));
+    b->efy = (double*)calloc(b->n, sizeof(double));
+    b->harm_i = harm[j];
+    b->ne = ne[j];
+    b->q_macro = ne[j] / b->n; /* Bunch.cpp:76-77 */
+  }
+  /* MPBeam.cpp:132-136 */
+  for (int j = 0; j < M - 1; ++j) s->b[j].gap_i = s->b[j + 1].harm_i - s->b[j].harm_i;
+  s->b[M - 1].gap_i = H - s->b[M - 1].harm_i;
+  s->cloud = (or_cloud*)calloc(s->K * s->P, sizeof(or_cloud));
+  for (int i = 0; i < s->K * s->P; ++i) {
+    or_cloud* c = &s->cloud[i];
+    c->cap = cfg->ion.max_ions + cfg->ion.macro_ions_per_ip + 1;
+    c->x = (double*)calloc(c->cap, sizeof(double)); c->y = (double*)calloc(c->cap, sizeof(double));
+    c->vx = (double*)calloc(c->cap, sizeof(double)); c->vy = (double*)calloc(c->cap, sizeof(double));
+    c->fx = (double*)calloc(c->cap, sizeof(double)); c->fy = (double*)calloc(c->cap, sizeof(double));
+  }
+  s->rec = (double*)calloc((size_t)s->K * M * s->P * 6, sizeof(double));
+  /* WakeFunction::InitialLRWake (WakeFunction.cpp:49-202) */
+  if (cfg->flag_lr_wake) {
+    int turns = cfg->lr_turns;
+    double trf = cfg->ring.t0 / cfg->ring.harmonics;
+    double dt = trf / 2;
+    int np = (int)(turns * cfg->ring.harmonics * trf / dt) + 2;
+    s->lr_np = np;
+    s->lr_tab = (double*)calloc(3 * (size_t)np, sizeof(double));
+    for (int i = 0; i < np; ++i) {
+      double t = -i * dt, w[3];
+      bbr_wake(&cfg->lr_bbr, s->sec[0].beta_x, s->sec[0].beta_y, t, w);
+      for (int d = 0; d < 3; ++d) s->lr_tab[(size_t)d * np + i] = w[d];
+    }
+    s->lr_dt = (1 * dt) - (0 * dt); /* lwaketime[1] - lwaketime[0] after negation */
+    s->lr_hist = (double*)calloc((size_t)turns * 3 * M, sizeof(double));
+  }
+  if (cfg->flag_fir) {
+    int order = cfg->fir.delay + cfg->fir.taps;
+    s->fir_hist = (double*)calloc((size_t)order * 3 * M, sizeof(double));
+    /* FIRFeedBack.cpp:56 */
+    s->fir_limit = sqrt(2 * cfg->fir.power_limit * cfg->fir.kicker_imped) / cfg->ring.electron_energy;
+  }
+  return s;
+}
+
+void or_destroy(or_state* s) {
+  if (!s) return;
+  for (int j = 0; j < s->M; ++j) {
+    for (int d = 0; d < 6; ++d) free(s->b[j].c[d]);
+    free(s->b[j].surv); free(s->b[j].efx); free(s->b[j].efy);
+  }
+  for (int i = 0; i < s->K * s->P; ++i) {
+    or_cloud* c = &s->cloud[i];
+    free(c->x); free(c->y); free(c->vx); free(c->vy); free(c->fx); free(c->fy);
+  }
+  free(s->cloud); free(s->b); free(s->sec); free(s->rec); free(s->lr_tab); free(s->lr_hist);
+  free(s->fir_hist);
+  free(s);
+}
+
+int or_set_bunch(or_state* s, int j, const double* x, const double* px, const double* y,
+                 const double* py, const double* z, const double* dp, const uint8_t* surv) {
+  or_bunch* b = &s->b[j];
+  const double* src[6] = {x, px, y, py, z, dp};
+  for (int d = 0; d < 6; ++d) memcpy(b->c[d], src[d], sizeof(double) * b->n);
+  if (surv) memcpy(b->surv, surv, b->n); else memset(b->surv, 0, b->n);
+  return 0;
+}
+int or_get_bunch(or_state* s, int j, double* x, double* px, double* y, double* py, double* z,
+                 double* dp, uint8_t* surv) {
+  or_bunch* b = &s->b[j];
+  double* dst[6] = {x, px, y, py, z, dp};
+  for (int d = 0; d < 6; ++d) if (dst[d]) memcpy(dst[d], b->c[d], sizeof(double) * b->n);
+  if (surv) memcpy(surv, b->surv, b->n);
+  return 0;
+}
+
+/* MPBunch::GetZMinMax (MPBunch.cpp:1860-1884) */
+static void zminmax(or_bunch* b) {
+  double* z = b->c[4];
+  double zmin = z[0], zmax = z[0];
+  for (int i = 0; i < b->n; i++) {
+    if (b->surv[i] != 0) continue;
+    if (zmin > z[i]) zmin = z[i];
+    if (zmax < z[i]) zmax = z[i];
+  }
+  b->m.z_min = zmin - 1.e-6;
+  b->m.z_max = zmax + 1.e-6;
+}
+
+/* MPBunch::GetMPBunchRMS (MPBunch.cpp:342-498) */
+static void bunch_rms(or_state* s, or_bunch* b, int k) {
+  double* X = b->c[0]; double* PX = b->c[1]; double* Y = b->c[2];
+  double* PY = b->c[3]; double* Z = b->c[4]; double* PZ = b->c[5];
+  double a[6] = {0, 0, 0, 0, 0, 0};
+  int n = 0;
+  for (int i = 0; i < b->n; i++) {
+    if (b->surv[i] != 0) continue;
+    a[0] += X[i]; a[2] += Y[i]; a[4] += Z[i]; a[1] += PX[i]; a[3] += PY[i]; a[5] += PZ[i];
+    n++;
+  }
+  for (int d = 0; d < 6; ++d) a[d] /= n;
+  double x2 = 0, y2 = 0, z2 = 0, px2 = 0, py2 = 0, pz2 = 0, xpx = 0, ypy = 0, zpz = 0;
+  for (int i = 0; i < b->n; i++) {
+    if (b->surv[i] != 0) continue;
+    x2 += pow(X[i], 2); y2 += pow(Y[i], 2); z2 += pow(Z[i], 2);
+    px2 += pow(PX[i], 2); py2 += pow(PY[i], 2); pz2 += pow(PZ[i], 2);
+    xpx += X[i] * PX[i]; ypy += Y[i] * PY[i]; zpz += Z[i] * PZ[i];
+  }
+  x2 /= n; y2 /= n; z2 /= n; px2 /= n; py2 /= n; pz2 /= n; xpx /= n; ypy /= n; zpz /= n;
+  b->m.eff_emit[0] = sqrt(x2 * px2 - pow(xpx, 2));
+  b->m.eff_emit[1] = sqrt(y2 * py2 - pow(ypy, 2));
+  b->m.eff_emit[2] = sqrt(z2 * pz2 - pow(zpz, 2));
+  b->m.eff_rms_x = sqrt(b->m.eff_emit[0] * s->sec[k].beta_x);
+  b->m.eff_rms_y = sqrt(b->m.eff_emit[1] * s->sec[k].beta_y);
+  x2 = y2 = z2 = px2 = py2 = pz2 = xpx = ypy = zpz = 0;
+  for (int i = 0; i < b->n; i++) {
+    if (b->surv[i] != 0) continue;
+    x2 += pow(X[i] - a[0], 2); y2 += pow(Y[i] - a[2], 2); z2 += pow(Z[i] - a[4], 2);
+    px2 += pow(PX[i] - a[1], 2); py2 += pow(PY[i] - a[3], 2); pz2 += pow(PZ[i] - a[5], 2);
+    xpx += (X[i] - a[0]) * (PX[i] - a[1]);
+    ypy += (Y[i] - a[2]) * (PY[i] - a[3]);
+    zpz += (Z[i] - a[4]) * (PZ[i] - a[5]);
+  }
+  x2 /= n; y2 /= n; z2 /= n; px2 /= n; py2 /= n; pz2 /= n; xpx /= n; ypy /= n; zpz /= n;
+  b->m.emit[0] = sqrt(x2 * px2 - pow(xpx, 2));
+  b->m.emit[1] = sqrt(y2 * py2 - pow(ypy, 2));
+  b->m.emit[2] = sqrt(z2 * pz2 - pow(zpz, 2));
+  b->m.rms_x = sqrt(b->m.emit[0] * s->sec[k].beta_x);
+  b->m.rms_y = sqrt(b->m.emit[1] * s->sec[k].beta_y);
+  b->m.bunch_length = sqrt(z2);
+  b->m.energy_spread = sqrt(pz2);
+  for (int d = 0; d < 6; ++d) b->m.mean[d] = a[d];
+  b->m.n_alive = n;
+  b->m.n_macro = b->n;
+  zminmax(b);
+}
+
+/* MPBeam::MPBeamRMSCal + MPGetBeamInfo (MPBeam.cpp:2125-2260): the max rms */
+/* size over bunches bounds the ion loss region.                             */
+int or_beam_rms(or_state* s, int k) {
+  for (int j = 0; j < s->M; ++j) bunch_rms(s, &s->b[j], k);
+  double mx = s->b[0].m.rms_x, my = s->b[0].m.rms_y;
+  for (int j = 1; j < s->M; ++j) {
+    if (s->b[j].m.rms_x > mx) mx = s->b[j].m.rms_x;
+    if (s->b[j].m.rms_y > my) my = s->b[j].m.rms_y;
+  }
+  s->size_x_max = mx;
+  s->size_y_max = my;
+  return 0;
+}
+int or_get_moments(or_state* s, cg_bunch_moments* out) {
+  for (int j = 0; j < s->M; ++j) out[j] = s->b[j].m;
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Ion chain of one interaction point: MPBeam::SSBeamIonEffectOneInteraction */
+/* Point (MPBeam.cpp:2585-2611) with LIP::GetIonNumberPerInterAction         */
+/* (LIP.cpp:974-982), IonGenerator (:985-1019), IonsUpdate (:1021-1051),     */
+/* IonRMSCal (:1113-1155), MPBunch::SSIonBunchInteraction (MPBunch.cpp:      */
+/* 1094-1211), Bunch::BunchTransferDueToIon (Bunch.cpp:213-220) and          */
+/* LIP::IonTransferDueToBunch (LIP.cpp:1158-1211).                           */
+int or_beam_ion_ip(or_state* s, int turn, int k) {
+  const cg_config* cfg = &s->cfg;
+  const cg_section* sec = &s->sec[k];
+  int P = s->P;
+  for (int j = 0; j < s->M; ++j) {
+    or_bunch* b = &s->b[j];
+    for (int p = 0; p < P; ++p) {
+      or_cloud* c = &s->cloud[k * P + p];
+      /* GetIonNumberPerInterAction */
+      double pressure_p = cfg->ion.gas_percent[p] * sec->pressure;
+      double line_density = cfg->ion.cross_section[p] * pressure_p / sec->temperature / BOLTZMANN * b->ne;
+      double ion_number = line_density * sec->length;
+      /* IonGenerator: births N(aver, rms) rejected outside 2 sigma (r^2 > 4) */
+      int nmacro = cfg->ion.macro_ions_per_ip;
+      c->macro_charge = ion_number / nmacro;
+      int got = 0;
+      for (uint32_t att = 0; got < nmacro; ++att) {
+        double g[2];
+        or_philox_normals(cfg->seed, STREAM_IONBIRTH, att, (uint32_t)j, (uint32_t)turn,
+                          (uint32_t)(k * CG_MAX_SPECIES + p), g);
+        double tx = b->m.mean[0] + b->m.rms_x * g[0];
+        double ty = b->m.mean[2] + b->m.rms_y * g[1];
+        if (pow((tx - b->m.mean[0]) / b->m.rms_x, 2) + pow((ty - b->m.mean[2]) / b->m.rms_y, 2) > 4.E0)
+          continue;
+        /* IonsUpdate: append */
+        if (c->n >= c->cap) { snprintf(s->err, sizeof s->err, "ion capacity"); return CG_ERR_ION_OVERFLOW; }
+        c->x[c->n] = tx; c->y[c->n] = ty; c->vx[c->n] = 0; c->vy[c->n] = 0;
+        c->fx[c->n] = 0; c->fy[c->n] = 0;
+        c->n++;
+        got++;
+      }
+      if (c->n > cfg->ion.max_ions) {
+        snprintf(s->err, sizeof s->err,
+                 "the accumulated ions at %dth interaction point is larger than limit %d", p,
+                 cfg->ion.max_ions);
+        return CG_ERR_ION_OVERFLOW;
+      }
+      /* IonRMSCal(k, p) */
+      double x2 = 0, y2 = 0;
+      if (c->n == 0) {
+        x2 = 0; y2 = 0;
+      } else if (c->n == 1) {
+        x2 = pow(c->x[0], 2); y2 = pow(c->y[0], 2);
+      } else {
+        double sx = 0.0, sy = 0.0;
+        for (int i = 0; i < c->n; ++i) sx += c->x[i];
+        for (int i = 0; i < c->n; ++i) sy += c->y[i];
+        c->aver_x = sx / c->n;
+        c->aver_y = sy / c->n;
+        for (int i = 0; i < c->n; i++) {
+          x2 += pow(c->x[i] - c->aver_x, 2);
+          y2 += pow(c->y[i] - c->aver_y, 2);
+        }
+      }
+      if (c->n != 0) {
+        x2 = x2 / c->n; y2 = y2 / c->n;
+        c->rms_x = sqrt(x2); c->rms_y = sqrt(y2);
+      } else {
+        c->rms_x = 0; c->rms_y = 0;
+      }
+    }
+    /* SSIonBunchInteraction (1): ion side, field of bunch j at each ion */
+    double nE0 = b->ne;
+    for (int p = 0; p < P; ++p) {
+      or_cloud* c = &s->cloud[k * P + p];
+      double A = cfg->ion.mass_number[p];
+      double coeffI = 2.0 * nE0 * RE_CLASSIC * E_MASS_EV / ION_MASS_EV / A * C_LIGHT;
+      for (int i = 0; i < c->n; i++) {
+        double fx, fy;
+        field(c->x[i] - b->m.mean[0], c->y[i] - b->m.mean[2], b->m.rms_x, b->m.rms_y, &fx, &fy);
+        c->fx[i] = coeffI * fx;
+        c->fy[i] = coeffI * fy;
+      }
+    }
+    /* record the cloud Gaussians the electron side sees */
+    for (int p = 0; p < P; ++p) {
+      or_cloud* c = &s->cloud[k * P + p];
+      double* r = &s->rec[(((size_t)k * s->M + j) * P + p) * 6];
+      r[0] = 2.0 * (c->macro_charge * c->n) * RE_CLASSIC / cfg->ring.r_gamma;
+      r[1] = c->rms_x; r[2] = c->rms_y; r[3] = c->aver_x; r[4] = c->aver_y; r[5] = c->n;
+    }
+    /* SSIonBunchInteraction (2) + BunchTransferDueToIon: electron side */
+    for (int i = 0; i < b->n; i++) {
+      if (b->surv[i] != 0) continue;
+      b->efx[i] = 0; b->efy[i] = 0;
+      for (int p = 0; p < P; ++p) {
+        double* r = &s->rec[(((size_t)k * s->M + j) * P + p) * 6];
+        double fx, fy;
+        field(b->c[0][i] - r[3], b->c[2][i] - r[4], r[1], r[2], &fx, &fy);
+        b->efx[i] += r[0] * fx;
+        b->efy[i] += r[0] * fy;
+      }
+    }
+    for (int i = 0; i < b->n; i++) {
+      /* the reference applies the stored kick to every particle (lost ones
+         keep their last kick); only alive particles are compared */
+      b->c[1][i] += b->efx[i];
+      b->c[3][i] += b->efy[i];
+    }
+    /* IonTransferDueToBunch: kick, drift over the gap, remove lost ions */
+    for (int p = 0; p < P; ++p) {
+      or_cloud* c = &s->cloud[k * P + p];
+      for (int i = 0; i < c->n; i++) {
+        c->vx[i] += c->fx[i];
+        c->vy[i] += c->fy[i];
+        c->x[i] += c->vx[i] * cfg->ring.circ_ring / cfg->ring.harmonics * b->gap_i / C_LIGHT;
+        c->y[i] += c->vy[i] * cfg->ring.circ_ring / cfg->ring.harmonics * b->gap_i / C_LIGHT;
+      }
+      double bx = sec->aperture_x > cfg->ion.loss_boundary * s->size_x_max
+                      ? cfg->ion.loss_boundary * s->size_x_max : sec->aperture_x;
+      double by = sec->aperture_y > cfg->ion.loss_boundary * s->size_y_max
+                      ? cfg->ion.loss_boundary * s->size_y_max : sec->aperture_y;
+      int w = 0;
+      for (int i = 0; i < c->n; i++) {
+        if (fabs(c->x[i]) > bx || fabs(c->y[i]) > by) continue;
+        c->x[w] = c->x[i]; c->y[w] = c->y[i]; c->vx[w] = c->vx[i]; c->vy[w] = c->vy[i];
+        c->fx[w] = c->fx[i]; c->fy[w] = c->fy[i];
+        w++;
+      }
+      c->n = w;
+    }
+  }
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Bunch::BunchTransferDueToLatticeTSymplectic (Bunch.cpp:625-755)           */
+int or_section_map(or_state* s, int k) {
+  const cg_ring* r = &s->cfg.ring;
+  const cg_section* sc = &s->sec[k];
+  double PI = PI_REF();
+  double betax = sc->beta_x, betay = sc->beta_y, alphax = sc->alpha_x, alphay = sc->alpha_y;
+  double weighX = sc->phase_adv_x / (2 * PI * r->work_qx);
+  double weighY = sc->phase_adv_y / (2 * PI * r->work_qy);
+  for (int j = 0; j < s->M; ++j) {
+    or_bunch* b = &s->b[j];
+    for (int i = 0; i < b->n; i++) {
+      if (b->surv[i] != 0) continue;
+      double v[6], v1[6], v2[6];
+      for (int d = 0; d < 6; ++d) v[d] = b->c[d][i];
+      double x = v[0] - sc->eta_x * v[5];
+      double px = v[1] - sc->etap_x * v[5];
+      double y = v[2] - sc->eta_y * v[5];
+      double py = v[3] - sc->etap_y * v[5];
+      double ampX = (pow(x, 2) + pow(alphax * x + betax * px, 2)) / betax;
+      double ampY = (pow(y, 2) + pow(alphay * y + betay * py, 2)) / betay;
+      double dnux = (r->chrom[0] * v[5] + r->adtx[0] * ampX + r->adtx[1] * ampY + r->adtx[2] * pow(ampX, 2) / 2 +
+                     r->adtx[3] * pow(ampY, 2) / 2 + r->adtx[4] * ampX * ampY) * weighX;
+      double dnuy = (r->chrom[1] * v[5] + r->adty[0] * ampX + r->adty[1] * ampY + r->adty[2] * pow(ampX, 2) / 2 +
+                     r->adty[3] * pow(ampY, 2) / 2 + r->adty[4] * ampX * ampY) * weighY;
+      double phiX = sc->phase_adv_x + 2 * PI * dnux;
+      double phiY = sc->phase_adv_y + 2 * PI * dnuy;
+      double R[36] = {0};
+      R[0] = cos(phiX); R[1] = sin(phiX); R[6] = -sin(phiX); R[7] = cos(phiX);
+      R[14] = cos(phiY); R[15] = sin(phiY); R[20] = -sin(phiY); R[21] = cos(phiY);
+      R[28] = 1; R[35] = 1;
+      dgemm6(sc->map_b1h1, v, 1, v1);
+      dgemm6(R, v1, 1, v2);
+      dgemm6(sc->map_h2b2, v2, 1, v1);
+      for (int d = 0; d < 6; ++d) b->c[d][i] = v1[d];
+    }
+  }
+  return 0;
+}
+
+/* MPBeam::BeamMomtumUpdateDueToRFTest, RFCA branch (MPBeam.cpp:2624-2652) -> */
+/* Bunch::BunchMomentumUpdateDueToRFCA (Bunch.cpp:453-481), all particles.    */
+int or_rf_kick(or_state* s) {
+  const cg_ring* r = &s->cfg.ring;
+  double PI = PI_REF();
+  double fRF = r->f0 * r->harmonics;
+  for (int c = 0; c < r->n_cav; ++c) {
+    for (int j = 0; j < s->M; ++j) {
+      or_bunch* b = &s->b[j];
+      for (int i = 0; i < b->n; i++) {
+        double th = b->c[4][i] / C_LIGHT / r->r_beta * 2. * PI * (double)r->cav_harm[c] * fRF;
+        /* Re(V exp(-i th)) as std::complex multiplies it: a c - b d, d = -sin */
+        double re = r->cav_vreq_re[c] * cos(-th) - r->cav_vreq_im[c] * sin(-th);
+        b->c[5][i] += re / r->electron_energy / pow(r->r_beta, 2);
+      }
+    }
+  }
+  return 0;
+}
+/* Bunch::BunchLongPosTransferOneTurn (Bunch.cpp:494-501) */
+int or_longi_drift(or_state* s) {
+  const cg_ring* r = &s->cfg.ring;
+  for (int j = 0; j < s->M; ++j) {
+    or_bunch* b = &s->b[j];
+    for (int i = 0; i < b->n; i++) {
+      double d = b->c[5][i];
+      b->c[4][i] -= r->circ_ring * (r->alphac[0] * d + r->alphac[1] * pow(d, 2) + r->alphac[2] * pow(d, 3));
+    }
+  }
+  return 0;
+}
+/* Bunch::BunchEnergyLossOneTurn (Bunch.cpp:483-491) */
+int or_energy_loss(or_state* s) {
+  const cg_ring* r = &s->cfg.ring;
+  for (int j = 0; j < s->M; ++j) {
+    or_bunch* b = &s->b[j];
+    for (int i = 0; i < b->n; i++) b->c[5][i] -= r->u0 / r->electron_energy / pow(r->r_beta, 2);
+  }
+  return 0;
+}
+/* Bunch::BunchSynRadDamping (Bunch.cpp:940-1044), with Philox normals       */
+int or_synrad(or_state* s, int turn) {
+  const cg_ring* r = &s->cfg.ring;
+  const cg_section* sc = &s->sec[0];
+  double lambda[3], coeff[3];
+  for (int i = 0; i < 3; i++) lambda[i] = exp(-1.0 / r->synch_rad_damp_time[i]);
+  coeff[0] = sqrt(1 - pow(lambda[0], 2)) * sqrt(r->emit_nat[0]);
+  coeff[1] = sqrt(1 - pow(lambda[1], 2)) * sqrt(r->emit_nat[1]);
+  coeff[2] = sqrt(1 - pow(lambda[2], 4)) * sqrt(r->emit_nat[2]);
+  for (int j = 0; j < s->M; ++j) {
+    or_bunch* b = &s->b[j];
+    for (int i = 0; i < b->n; i++) {
+      if (b->surv[i] != 0) continue;
+      double v[6], X[6];
+      for (int d = 0; d < 6; ++d) v[d] = b->c[d][i];
+      dgemm6(sc->map_b1h1, v, 1, X);
+      X[0] *= lambda[0]; X[1] *= lambda[0]; X[2] *= lambda[1]; X[3] *= lambda[1];
+      X[5] *= lambda[2] * lambda[2];
+      if (b->n != 1) {
+        double g[6];
+        for (int q = 0; q < 3; ++q)
+          or_philox_normals(s->cfg.seed, STREAM_SYNRAD, (uint32_t)i, (uint32_t)j, (uint32_t)turn,
+                            (uint32_t)q, &g[2 * q]);
+        X[0] += coeff[0] * g[0]; X[1] += coeff[0] * g[1];
+        X[2] += coeff[1] * g[2]; X[3] += coeff[1] * g[3];
+        X[5] += coeff[2] * g[5];
+      }
+      dgemm6(sc->map_h1b1, X, 1, v);
+      for (int d = 0; d < 6; ++d) b->c[d][i] = v[d];
+    }
+  }
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Long-range wake: MPBeam::LRWakeBeamIntaction (MPBeam.cpp:3232-3349) with  */
+/* WakeFunction::GetTotLRWakeLinearFit (WakeFunction.cpp:204-230) and        */
+/* Bunch::BunchTransferDueToWake (Bunch.cpp:1091-1103).                      */
+int or_lr_table(or_state* s, double* out, int capacity, int* np) {
+  *np = s->lr_np;
+  if (out) for (int i = 0; i < 3 * s->lr_np && i < capacity; ++i) out[i] = s->lr_tab[i];
+  return 0;
+}
+int or_lr_wake(or_state* s) {
+  int T = s->cfg.lr_turns, M = s->M, H = s->cfg.ring.harmonics;
+  const cg_ring* r = &s->cfg.ring;
+  double tRF = r->t0 / (double)H;
+  /* shift history: [0..T-1] holds turns -T+1..0 */
+  memmove(s->lr_hist, s->lr_hist + 3 * M, sizeof(double) * 3 * M * (T - 1));
+  double* cur = s->lr_hist + (size_t)(T - 1) * 3 * M;
+  for (int i = 0; i < M; ++i) {
+    cur[i] = s->b[i].m.mean[0]; cur[M + i] = s->b[i].m.mean[2]; cur[2 * M + i] = s->b[i].m.mean[4];
+  }
+  int np = s->lr_np;
+  for (int j = 0; j < M; ++j) {
+    double f[3] = {0, 0, 0};
+    for (int n = 0; n < T; n++) {
+      int i0, i1;
+      if (n == 0) { i0 = 0; i1 = j - 1; }
+      else if (n == T - 1) { i0 = j; i1 = M - 1; }
+      else { i0 = 0; i1 = M - 1; }
+      const double* h = s->lr_hist + (size_t)(T - 1 - n) * 3 * M;
+      for (int i = i0; i <= i1; i++) {
+        int nT = s->b[i].harm_i - s->b[j].harm_i - n * H;
+        double ts = nT * tRF;
+        double dT = (s->b[j].m.mean[4] - h[2 * M + i]) / C_LIGHT / r->r_beta;
+        double tau = ts + dT;
+        if (tau > 0) { snprintf(s->err, sizeof s->err, "LR wake tau > 0"); return CG_ERR_INVALID; }
+        int idx = (int)floor(-tau / s->lr_dt);
+        double v1 = -tau / s->lr_dt - idx, v0 = 1 - v1;
+        if (idx + 1 >= np) { snprintf(s->err, sizeof s->err, "LR table"); return CG_ERR_INVALID; }
+        double w[3];
+        for (int d = 0; d < 3; ++d) w[d] = s->lr_tab[(size_t)d * np + idx] * v0 + s->lr_tab[(size_t)d * np + idx + 1] * v1;
+        f[0] -= w[0] * s->b[i].ne * h[i];
+        f[1] -= w[1] * s->b[i].ne * h[M + i];
+        f[2] -= w[2] * s->b[i].ne;
+      }
+    }
+    for (int d = 0; d < 3; ++d) s->b[j].lr_force[d] = f[d] * E_CHARGE / r->electron_energy / pow(r->r_beta, 2);
+  }
+  for (int j = 0; j < M; ++j) {
+    or_bunch* b = &s->b[j];
+    for (int i = 0; i < b->n; i++) {
+      b->c[1][i] += b->lr_force[0];
+      b->c[3][i] += b->lr_force[1];
+      b->c[5][i] += b->lr_force[2];
+    }
+  }
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Short-range wake: MPBunch::BunchTransferDueToSRWake (MPBunch.cpp:         */
+/* 1887-2025) with WakeFunction::GetBBRWakeFun1 (:635-653) and                */
+/* GetBBRPusdoWakeFun (:558-633).                                             */
+static void bbr_pseudo(const cg_bbr* w, double tau, double out[3]) {
+  double PI = PI_REF();
+  double sigmat = 1.e-3 / C_LIGHT;
+  out[0] = out[1] = out[2] = 0;
+  for (int i = 0; i < w->n; i++) {
+    double u = tau / sigmat;
+    double sigmaz = sigmat * C_LIGHT;
+    int nz = 1000;
+    double q = w->l_q[i];
+    double vz = w->l_omega[i] * sigmaz / C_LIGHT;
+    double zMax = 3 * vz / (2 * q), dz = zMax / nz, sum = 0;
+    for (int j = 0; j < nz; j++) {
+      double z = j * dz;
+      double t0 = -1 / 2.0 * pow(u + 2 * q / vz * z, 2) - z;
+      double t1 = cos(z * sqrt(4 * q * q - 1));
+      double t2 = sin(z * sqrt(4 * q * q - 1)) / sqrt(4 * q * q - 1);
+      sum += exp(t0) * (t1 - t2) * dz;
+    }
+    double wz = sqrt(2. / PI) * w->l_rs[i] * C_LIGHT / sigmaz * sum;
+    q = w->tx_q[i];
+    vz = w->tx_omega[i] * sigmaz / C_LIGHT;
+    zMax = 3 * vz / (2 * q); dz = zMax / nz; sum = 0;
+    for (int j = 0; j < nz; j++) {
+      double z = j * dz;
+      double t0 = -1 / 2.0 * pow(u + 2 * q / vz * z, 2) - z;
+      double t2 = sin(z * sqrt(4 * q * q - 1)) / sqrt(4 * q * q - 1);
+      sum += 2 * q / vz * exp(t0) * t2 * dz;
+    }
+    double wx = sum * (sqrt(2. / PI) * w->tx_rs[i] * C_LIGHT);
+    q = w->ty_q[i];
+    vz = w->ty_omega[i] * sigmaz / C_LIGHT;
+    zMax = 3 * vz / (2 * q); dz = zMax / nz; sum = 0;
+    for (int j = 0; j < nz; j++) {
+      double z = j * dz;
+      double t0 = -1 / 2.0 * pow(u + 2 * q / vz * z, 2) - z;
+      double t2 = sin(z * sqrt(4 * q * q - 1)) / sqrt(4 * q * q - 1);
+      sum += 2 * q / vz * exp(t0) * t2 * dz;
+    }
+    double wy = sum * (sqrt(2. / PI) * w->ty_rs[i] * C_LIGHT);
+    out[0] += wx; out[1] += wy; out[2] += wz;
+  }
+}
+int or_sr_wake(or_state* s, int turn) {
+  (void)turn;
+  int B = s->cfg.sr_bins;
+  if (B > 4096) return CG_ERR_INVALID;
+  for (int j = 0; j < s->M; ++j) {
+    or_bunch* b = &s->b[j];
+    zminmax(b);
+    double poszMin = b->m.z_min - 2 * b->m.bunch_length;
+    double poszMax = b->m.z_max + 2 * b->m.bunch_length;
+    double dzBin = (poszMax - poszMin) / B;
+    double dtBin = dzBin / C_LIGHT;
+    b->sr_zlo = poszMin; b->sr_dz = dzBin;
+    int* cnt = b->sr_counts;
+    double* ax = (double*)calloc(B, sizeof(double));
+    double* ay = (double*)calloc(B, sizeof(double));
+    int* bin = (int*)malloc(sizeof(int) * b->n);
+    for (int i = 0; i < B; ++i) cnt[i] = 0;
+    for (int i = 0; i < b->n; i++) {
+      int idx = (int)((b->c[4][i] - poszMin) / dzBin);
+      /* the reference indexes out of range for particles outside [zlo, zhi)
+         (only lost ones can be); they are left out of the histogram here */
+      bin[i] = (idx >= 0 && idx < B) ? idx : -1;
+      if (bin[i] >= 0) cnt[idx]++;
+    }
+    for (int i = 0; i < b->n; i++) {
+      if (bin[i] < 0 || b->surv[i] != 0) continue;
+      ax[bin[i]] += b->c[0][i];
+      ay[bin[i]] += b->c[2][i];
+    }
+    for (int i = 0; i < B; ++i) {
+      if (cnt[i] == 0) { ax[i] = 0; ay[i] = 0; }
+      else { ax[i] /= cnt[i]; ay[i] /= cnt[i]; }
+    }
+    double* pot = b->sr_pot;
+    for (int i = 0; i < B; i++) {
+      for (int jj = 0; jj < B; jj++) {
+        double tau = (i - jj) * dtBin;
+        double w[3];
+        bbr_pseudo(&s->cfg.sr_bbr, tau, w);
+        pot[i] += w[0] * cnt[jj] * ax[jj];
+        pot[B + i] += w[1] * cnt[jj] * ax[jj];
+        pot[2 * B + i] += w[2] * cnt[jj];
+      }
+      pot[i] *= (-1) * E_CHARGE * b->q_macro / s->cfg.ring.electron_energy;
+      pot[B + i] *= (-1) * E_CHARGE * b->q_macro / s->cfg.ring.electron_energy;
+      pot[2 * B + i] *= (-1) * E_CHARGE * b->q_macro / s->cfg.ring.electron_energy;
+    }
+    for (int i = 0; i < b->n; i++) {
+      if (bin[i] < 0 || b->surv[i] != 0) continue;
+      b->c[5][i] += pot[2 * B + bin[i]];
+    }
+    free(ax); free(ay); free(bin);
+  }
+  return 0;
+}
+int or_sr_bins(or_state* s, int j, double* zlo, double* dz, int* counts) {
+  *zlo = s->b[j].sr_zlo; *dz = s->b[j].sr_dz;
+  if (counts) memcpy(counts, s->b[j].sr_counts, sizeof(int) * s->cfg.sr_bins);
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* MPBeam::FIRBunchByBunchFeedback (MPBeam.cpp:2978-3090)                     */
+int or_fir(or_state* s, int turn) {
+  const cg_fir_params* f = &s->cfg.fir;
+  int M = s->M;
+  int on = 0;
+  for (int i = 0; i < f->n_sections; i++)
+    if (turn > f->start[i] && turn < f->end[i]) on = 1;
+  if (f->mode == 0) {
+    if (on)
+      for (int j = 0; j < M; ++j) {
+        or_bunch* b = &s->b[j];
+        for (int i = 0; i < b->n; i++) {
+          b->c[1][i] -= b->m.mean[1];
+          b->c[3][i] -= b->m.mean[3];
+          b->c[5][i] -= b->m.mean[5];
+        }
+      }
+    return 0;
+  }
+  int order = f->delay + f->taps;
+  memmove(s->fir_hist, s->fir_hist + 3 * M, sizeof(double) * 3 * M * (order - 1));
+  double* cur = s->fir_hist + (size_t)(order - 1) * 3 * M;
+  for (int i = 0; i < M; ++i) {
+    cur[i] = s->b[i].m.mean[0]; cur[M + i] = s->b[i].m.mean[2]; cur[2 * M + i] = s->b[i].m.mean[4];
+  }
+  if (!on) return 0;
+  double rb2 = pow(s->cfg.ring.r_beta, 2);
+  for (int j = 0; j < M; ++j) {
+    double kx = 0, ky = 0, kz = 0;
+    for (int q = 0; q < order; q++) {
+      const double* h = s->fir_hist + (size_t)q * 3 * M;
+      kx += f->coeff_x[order - q - 1] * h[j];
+      ky += f->coeff_y[order - q - 1] * h[M + j];
+      kz += f->coeff_z[order - q - 1] * h[2 * M + j];
+    }
+    kx = kx * f->gain * f->kick_strength[0];
+    ky = ky * f->gain * f->kick_strength[1];
+    kz = kz * f->gain * f->kick_strength[2];
+    if (kx > s->fir_limit) kx = s->fir_limit;
+    if (ky > s->fir_limit) ky = s->fir_limit;
+    if (kz > s->fir_limit) kz = s->fir_limit;
+    or_bunch* b = &s->b[j];
+    for (int i = 0; i < b->n; i++) {
+      b->c[1][i] = b->c[1][i] + kx;
+      b->c[3][i] = b->c[3][i] + ky;
+      b->c[5][i] = b->c[5][i] + kz / rb2;
+    }
+  }
+  return 0;
+}
+
+/* Bunch::MarkLostParticle (Bunch.cpp:172-200), aperture of section 0        */
+int or_mark_lost(or_state* s, double* trans) {
+  const cg_ring* r = &s->cfg.ring;
+  int status = 0;
+  for (int j = 0; j < s->M; ++j) {
+    or_bunch* b = &s->b[j];
+    int count = 0;
+    for (int i = 0; i < b->n; i++) {
+      if (fabs(b->c[4][i]) > r->t0 * C_LIGHT / r->harmonics / 2) {
+        b->surv[i] = 2;
+        count++;
+      }
+      double lt = pow(b->c[0][i] / s->sec[0].aperture_x, 2) + pow(b->c[2][i] / s->sec[0].aperture_y, 2);
+      if (lt > 1) {
+        b->surv[i] = 1;
+        count++;
+      }
+    }
+    b->m.transmission = (b->n - count) / (double)b->n;
+    if (trans) trans[j] = b->m.transmission;
+    if (b->m.transmission < 0.5) {
+      snprintf(s->err, sizeof s->err,
+               "bunch at harmoinc %d, more than 50%% particles are lost", b->harm_i);
+      status = CG_ERR_TRANSMISSION;
+    }
+  }
+  return status;
+}
+
+/* MPBeam::Run turn loop (MPBeam.cpp:1010-1102), output writers excluded.   */
+int or_run_turns(or_state* s, int turn0, int n_turns) {
+  const cg_config* c = &s->cfg;
+  int st;
+  for (int n = turn0; n < turn0 + n_turns; ++n) {
+    or_beam_rms(s, 0);
+    for (int k = 0; k < s->K; ++k) {
+      or_beam_rms(s, k);
+      if (c->flag_beam_ion && (st = or_beam_ion_ip(s, n, k))) return st;
+      or_section_map(s, k);
+      or_beam_rms(s, k);
+    }
+    or_rf_kick(s);
+    or_longi_drift(s);
+    or_energy_loss(s);
+    if (c->flag_synrad) or_synrad(s, n);
+    if (c->flag_lr_wake && (st = or_lr_wake(s))) return st;
+    if (c->flag_sr_wake) or_sr_wake(s, n);
+    or_beam_rms(s, 0);
+    if (c->flag_fir) or_fir(s, n);
+    if ((st = or_mark_lost(s, NULL))) return st;
+    or_beam_rms(s, 0);
+  }
+  return 0;
+}
+
+/* accessors for the ion clouds */
+int or_ion_count(or_state* s, int k, int p, int* count) {
+  *count = s->cloud[k * s->P + p].n;
+  return 0;
+}
+int or_ion_download(or_state* s, int k, int p, double* x, double* y, double* vx, double* vy,
+                    int capacity, int* count) {
+  or_cloud* c = &s->cloud[k * s->P + p];
+  *count = c->n;
+  int n = c->n < capacity ? c->n : capacity;
+  memcpy(x, c->x, n * sizeof(double)); memcpy(y, c->y, n * sizeof(double));
+  memcpy(vx, c->vx, n * sizeof(double)); memcpy(vy, c->vy, n * sizeof(double));
+  return 0;
+}
+int or_ion_upload(or_state* s, int k, int p, const double* x, const double* y,
+                  const double* vx, const double* vy, int count) {
+  or_cloud* c = &s->cloud[k * s->P + p];
+  if (count > c->cap) return CG_ERR_INVALID;
+  c->n = count;
+  memcpy(c->x, x, count * sizeof(double)); memcpy(c->y, y, count * sizeof(double));
+  memcpy(c->vx, vx, count * sizeof(double)); memcpy(c->vy, vy, count * sizeof(double));
+  return 0;
+}
+int or_ion_cloud_record(or_state* s, int k, double* out) {
+  memcpy(out, &s->rec[(size_t)k * s->M * s->P * 6], sizeof(double) * s->M * s->P * 6);
+  return 0;
+}
+
+/* struct sizes as this compiler lays out include/cetasim_gpu.h (test helper) */
+void or_struct_sizes(int64_t* out) {
+  out[0] = sizeof(cg_config);
+  out[1] = sizeof(cg_ring);
+  out[2] = sizeof(cg_section);
+  out[3] = sizeof(cg_bunch_moments);
+  out[4] = sizeof(cg_ion_params);
+  out[5] = sizeof(cg_bbr);
+  out[6] = sizeof(cg_fir_params);
+}

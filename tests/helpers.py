@@ -1,0 +1,86 @@
+"""Shared helpers of the GPU parity tests: small seeded workloads with the
+benchmark shapes, identical initial particles for the GPU and the oracle, and
+error metrics."""
+import ctypes as C
+
+import numpy as np
+
+import oracle
+from cetasim_b200 import configs
+
+
+def small(name, n_scale, qe=True, seed=1234, **over):
+    wl = configs.make(name, n_scale=n_scale, seed=seed)
+    if not qe:
+        for i in range(3):
+            wl.cfg.ring.emit_nat[i] = 0.0
+    for k, v in over.items():
+        if k == "sections":
+            continue
+        setattr(wl.cfg, k, v)
+    return wl
+
+
+def particles(wl, seed=7, spread=1.0, sigma_scale=1.0):
+    """Seeded 6-D Gaussian particles per bunch (host side)."""
+    rng = np.random.default_rng(seed)
+    ex, ey, sz, sdp = wl.gen
+    out = []
+    for j in range(wl.n_bunches):
+        n = int(wl.n_macro[j])
+        s = wl.sections[0]
+        c = np.empty((6, n))
+        c[0] = rng.normal(0, np.sqrt(ex * s.beta_x), n) * sigma_scale + 2e-6 * spread * rng.normal()
+        c[1] = rng.normal(0, np.sqrt(ex / s.beta_x), n) * sigma_scale
+        c[2] = rng.normal(0, np.sqrt(ey * s.beta_y), n) * sigma_scale + 1e-6 * spread * rng.normal()
+        c[3] = rng.normal(0, np.sqrt(ey / s.beta_y), n) * sigma_scale
+        c[4] = rng.normal(0, sz, n) * sigma_scale
+        c[5] = rng.normal(0, sdp, n) * sigma_scale
+        out.append(c)
+    return out
+
+
+def pair(wl, parts, surv=None):
+    from cetasim_b200.beam import MPBeam
+    g = MPBeam(wl)
+    o = oracle.OracleBeam(wl)
+    for j, c in enumerate(parts):
+        s = None if surv is None else surv[j]
+        g.upload(j, c, s)
+        o.upload(j, c, s)
+    return g, o
+
+
+def coord_err(g, o, wl, alive_only=True):
+    """max |gpu - oracle| / rms(oracle) per coordinate, over all bunches."""
+    worst = np.zeros(6)
+    for j in range(wl.n_bunches):
+        cg_, sg = g.download(j)
+        co, so = o.download(j)
+        assert np.array_equal(sg, so), "survival flags differ"
+        m = (so == 0) if alive_only else np.ones_like(so, dtype=bool)
+        for d in range(6):
+            scale = np.sqrt(np.mean(co[d][m] ** 2)) + 1e-300
+            worst[d] = max(worst[d], np.max(np.abs(cg_[d][m] - co[d][m])) / scale)
+    return worst
+
+
+def moments_close(mg, mo, rtol):
+    fields = ["mean", "emit", "eff_emit", "rms_x", "rms_y", "eff_rms_x", "eff_rms_y",
+              "bunch_length", "energy_spread", "z_min", "z_max"]
+    bad = []
+    for j in range(len(mg)):
+        a, b = mg[j], mo[j]
+        assert a.n_alive == b.n_alive
+        for f in fields:
+            va, vb = np.array(getattr(a, f), ndmin=1), np.array(getattr(b, f), ndmin=1)
+            scale = np.maximum(np.abs(vb), 1e-300)
+            if f == "mean":
+                # centroids can be ~0: compare against the bunch size scale
+                scale = np.array([np.sqrt(b.emit[0] * 10), np.sqrt(b.emit[0] / 10),
+                                  np.sqrt(b.emit[1] * 10), np.sqrt(b.emit[1] / 10),
+                                  b.bunch_length, b.energy_spread])
+            e = np.max(np.abs(va - vb) / scale)
+            if not e <= rtol:
+                bad.append((j, f, e))
+    return bad

@@ -1,0 +1,81 @@
+"""GPU w(z) and Gaussian-field kernels against the reference's known answers,
+the reference's own outputs (golden) and the oracle."""
+import numpy as np
+import pytest
+
+import oracle
+from cetasim_b200 import _abi
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_w(lib, z, q1=False):
+    zr = np.ascontiguousarray(z.real, dtype=np.float64)
+    zi = np.ascontiguousarray(z.imag, dtype=np.float64)
+    wr, wi = np.empty_like(zr), np.empty_like(zr)
+    fn = lib.cg_faddeeva_w_q1 if q1 else lib.cg_faddeeva_w
+    assert fn(_abi.ptr(zr), _abi.ptr(zi), _abi.ptr(wr), _abi.ptr(wi), len(zr)) == 0
+    return wr + 1j * wi
+
+
+def relerr(a, b):
+    """The reference self-test's relerr (Faddeeva.cpp:1905-1915): NaN/Inf
+    that match count as zero error."""
+    with np.errstate(all="ignore"):
+        e = np.abs((b - a) / a)
+    both_nan = np.isnan(a) & np.isnan(b)
+    same_inf = np.isinf(a) & np.isinf(b) & (np.sign(a) == np.sign(b))
+    e = np.where(a == b, 0.0, e)
+    e = np.where(both_nan | same_inf, 0.0, e)
+    e = np.where((a == 0) & (b != 0), np.inf, e)
+    return e
+
+
+def test_kat_all_57_points(lib, golden):
+    # tolerance of the reference's own self-test: 1e-13 per component
+    z, w = golden["kat_z"], golden["kat_w"]
+    got = gpu_w(lib, z)
+    e = np.maximum(relerr(w.real, got.real), relerr(w.imag, got.imag))
+    assert e.max() <= 1e-13, [(z[i], got[i], w[i], e[i]) for i in np.where(e > 1e-13)[0]]
+
+
+def test_grid_vs_reference_outputs(lib, golden):
+    z, ref = golden["grid_z"], golden["grid_ref"]
+    got = gpu_w(lib, z)
+    e = np.abs(got - ref) / np.abs(ref)
+    assert e.max() <= 2e-14, e.max()
+
+
+def test_kernel_path_first_quadrant(lib):
+    rng = np.random.default_rng(3)
+    z = np.concatenate([rng.uniform(0, 12, 200000) + 1j * rng.uniform(0, 12, 200000),
+                        10 ** rng.uniform(-8, 1.1, 50000) + 1j * 10 ** rng.uniform(-8, 1.1, 50000)])
+    got = gpu_w(lib, z, q1=True)
+    ref = oracle.faddeeva_w(z)
+    e = np.abs(got - ref) / np.abs(ref)
+    # stated bound of the kick path: 4e-15 relative to |w|
+    assert e.max() <= 4e-15, (e.max(), z[e.argmax()])
+
+
+def test_gaussian_field_vs_oracle(lib):
+    rng = np.random.default_rng(11)
+    n = 100000
+    sx = 10 ** rng.uniform(-6, -4, n)
+    ratio = np.concatenate([rng.uniform(0.05, 1.0, n // 2), rng.uniform(1.0, 20.0, n - n // 2)])
+    ratio[:1000] = 1.0 + rng.uniform(-5e-5, 5e-5, 1000)  # round-beam branch
+    sy = sx * ratio
+    x = rng.normal(0, 3, n) * sx
+    y = rng.normal(0, 3, n) * sy
+    x[:10] = 0.0
+    a = [np.ascontiguousarray(v) for v in (x, y, sx, sy)]
+    fx, fy = np.empty(n), np.empty(n)
+    assert lib.cg_gaussian_field(*[_abi.ptr(v) for v in a], _abi.ptr(fx), _abi.ptr(fy), n) == 0
+    ox, oy = oracle.gaussian_field(x, y, sx, sy)
+    # field scale 1/sigma_max: errors of w(z) (absolute ~1e-15) are amplified by
+    # the cancellation of w1 - exp() w2 near the beam centre
+    scale = 1.0 / np.maximum(sx, sy)
+    e = np.maximum(np.abs(fx - ox), np.abs(fy - oy)) / scale
+    assert e.max() <= 1e-12, e.max()
+    big = np.hypot(ox, oy) > 0.1 * scale
+    rel = np.hypot(fx - ox, fy - oy)[big] / np.hypot(ox, oy)[big]
+    assert rel.max() <= 1e-13, rel.max()

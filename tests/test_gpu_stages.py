@@ -1,0 +1,146 @@
+"""Each MPBeam stage on the GPU (through the C ABI) against the oracle on the
+same seeded particles.  Tolerances are relative to the rms of each
+coordinate (or to the kick's own scale) and are stated per test."""
+import numpy as np
+import pytest
+
+from helpers import coord_err, moments_close, pair, particles, small
+
+pytestmark = pytest.mark.gpu
+
+
+def test_moments_all_fields():
+    wl = small("fast_ion", 0.02)  # 80 bunches x 400
+    g, o = pair(wl, particles(wl))
+    for k in (0, 7):
+        g.MPBeamRMSCal(k)
+        o.MPBeamRMSCal(k)
+        assert not moments_close(g.moments(), o.moments(), 1e-13)
+
+
+def test_moments_ragged_bunches_with_losses():
+    wl = small("batched_uneven", 0.01)  # 900 bunches of 50..500
+    wl_parts = particles(wl, seed=3)
+    rng = np.random.default_rng(5)
+    surv = [(rng.random(len(c[0])) < 0.1).astype(np.uint8) for c in wl_parts]
+    g, o = pair(wl, wl_parts, surv)
+    g.MPBeamRMSCal(3)
+    o.MPBeamRMSCal(3)
+    assert not moments_close(g.moments(), o.moments(), 1e-13)
+
+
+def test_section_maps_one_turn():
+    wl = small("fast_ion", 0.05)
+    g, o = pair(wl, particles(wl))
+    for k in range(wl.cfg.n_sections):
+        g.BeamTransferPerInteractionPointDueToLatticeT(k)
+        o.BeamTransferPerInteractionPointDueToLatticeT(k)
+    assert coord_err(g, o, wl).max() <= 1e-13
+
+
+def test_lost_particles_are_not_mapped():
+    wl = small("plain_single", 0.01)
+    parts = particles(wl)
+    surv = [np.zeros(len(parts[0][0]), dtype=np.uint8)]
+    surv[0][::7] = 1
+    g, o = pair(wl, parts, surv)
+    g.BeamTransferPerInteractionPointDueToLatticeT(0)
+    cg_, _ = g.download(0)
+    assert np.array_equal(cg_[:, ::7], parts[0][:, ::7])
+
+
+def test_longitudinal_stages():
+    wl = small("plain_single", 0.02)
+    parts = particles(wl)
+    surv = [np.zeros(len(parts[0][0]), dtype=np.uint8)]
+    surv[0][::11] = 2  # lost particles still get RF, drift and energy loss
+    g, o = pair(wl, parts, surv)
+    for st in ("BeamMomtumUpdateDueToRFTest", "BeamLongiPosTransferOneTurn", "BeamEnergyLossOneTurn"):
+        getattr(g, st)()
+        getattr(o, st)()
+        assert coord_err(g, o, wl, alive_only=False).max() <= 1e-14, st
+
+
+@pytest.mark.parametrize("qe", [False, True])
+def test_synrad_same_philox_draws(qe):
+    wl = small("plain_single", 0.02, qe=qe)
+    g, o = pair(wl, particles(wl))
+    for turn in (0, 1, 12345):
+        g.BeamSynRadDamping(turn)
+        o.BeamSynRadDamping(turn)
+    assert coord_err(g, o, wl).max() <= 1e-13
+
+
+def test_mark_lost_flags_and_transmission():
+    wl = small("fast_ion", 0.01)
+    parts = particles(wl)
+    rng = np.random.default_rng(2)
+    for c in parts:
+        idx = rng.choice(len(c[0]), 20, replace=False)
+        c[0][idx[:8]] = 0.2   # beyond the 0.1 m aperture
+        c[4][idx[5:14]] = 0.5  # beyond C/(2h)
+    g, o = pair(wl, parts)
+    tg = g.MarkParticleLostInBunch()
+    to = o.MarkParticleLostInBunch()
+    assert np.array_equal(tg, to)
+    for j in range(wl.n_bunches):
+        assert np.array_equal(g.download(j)[1], o.download(j)[1])
+
+
+def test_sr_wake_bins_bit_exact_and_kick():
+    wl = small("plain_single", 0.05)  # 5000 particles, 100 bins
+    g, o = pair(wl, particles(wl))
+    g.MPBeamRMSCal(0)
+    o.MPBeamRMSCal(0)
+    dp0 = g.download(0)[0][5].copy()
+    z = g.download(0)[0][4]
+    for turn in range(3):
+        g.SRWakeBeamIntaction(turn)
+        o.SRWakeBeamIntaction(turn)
+        zlo_g, dz_g, cnt_g = g.sr_bins(0)
+        zlo_o, dz_o, cnt_o = o.sr_bins(0)
+        assert abs(zlo_g - zlo_o) <= 1e-14 * abs(zlo_o) and abs(dz_g - dz_o) <= 1e-14 * dz_o
+        # counts are integers: bit-exact given the geometry
+        idx = ((z - zlo_g) / dz_g).astype(np.int64)
+        idx = idx[(idx >= 0) & (idx < wl.cfg.sr_bins)]
+        assert np.array_equal(cnt_g, np.bincount(idx, minlength=wl.cfg.sr_bins))
+        if zlo_g == zlo_o and dz_g == dz_o:
+            assert np.array_equal(cnt_g, cnt_o)
+    kick_g = g.download(0)[0][5] - dp0
+    kick_o = o.download(0)[0][5] - dp0
+    assert np.max(np.abs(kick_g - kick_o)) <= 1e-11 * np.max(np.abs(kick_o))
+
+
+def test_lr_wake_and_fir_over_turns():
+    wl = small("batched_uneven", 0.004)  # 900 bunches x 20..200
+    g, o = pair(wl, particles(wl, seed=9, spread=5.0))
+    for turn in range(4):
+        g.MPBeamRMSCal(wl.cfg.n_sections - 1)
+        o.MPBeamRMSCal(wl.cfg.n_sections - 1)
+        g.LRWakeBeamIntaction()
+        o.LRWakeBeamIntaction()
+        g.MPBeamRMSCal(0)
+        o.MPBeamRMSCal(0)
+        g.FIRBunchByBunchFeedback(turn + 1)
+        o.FIRBunchByBunchFeedback(turn + 1)
+    assert coord_err(g, o, wl, alive_only=False).max() <= 1e-11
+
+
+def test_ion_chain_one_interaction_point():
+    wl = small("fast_ion", 0.02)  # 80 bunches x 400
+    g, o = pair(wl, particles(wl, seed=4, spread=3.0))
+    for turn in range(2):
+        for k in (0, 1):
+            g.MPBeamRMSCal(k)
+            o.MPBeamRMSCal(k)
+            g.SSBeamIonEffectOneInteractionPoint(turn, k)
+            o.SSBeamIonEffectOneInteractionPoint(turn, k)
+            rg, ro = g.cloud_record(k), o.cloud_record(k)
+            assert np.array_equal(rg[..., 5], ro[..., 5])  # ion counts
+            assert np.allclose(rg[..., :5], ro[..., :5], rtol=1e-12, atol=0)
+            ig, io = g.ions(k), o.ions(k)
+            assert len(ig[0]) == len(io[0])
+            for a, b in zip(ig, io):
+                if len(b):
+                    assert np.allclose(a, b, rtol=1e-11, atol=1e-11 * np.max(np.abs(b)))
+    assert coord_err(g, o, wl).max() <= 1e-12
