@@ -66,12 +66,15 @@ int check_status(Handle& h) {
   e = cudaMemcpy(&st, h.d.status, sizeof(int), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return cuda_fail(&h, e, "status read");
   if (st == 0) return CG_OK;
-  cudaMemset(h.d.status, 0, sizeof(int));
+  cudaMemsetAsync(h.d.status, 0, sizeof(int), h.stream);
+  cudaStreamSynchronize(h.stream);
   if (st & kStatusIonOverflow)
     return fail(&h, CG_ERR_ION_OVERFLOW,
                 "the accumulated ions at an interaction point exceed ionCalIonMaxNumber");
   if (st & kStatusTransmission)
     return fail(&h, CG_ERR_TRANSMISSION, "a bunch lost more than 50% of its particles");
+  if (st & kStatusIonBirth)
+    return fail(&h, CG_ERR_INVALID, "ion births rejected 2^20 times (degenerate bunch size)");
   if (st & kStatusLrRange)
     return fail(&h, CG_ERR_INVALID, "long-range wake lag outside the wake table (tau > 0)");
   return fail(&h, CG_ERR_CUDA, "unknown device status");

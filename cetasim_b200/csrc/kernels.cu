@@ -315,6 +315,7 @@ __global__ void __launch_bounds__(kChainThreads) k_ion_chain(
   __shared__ double smem[4 * 32];
   __shared__ int smem_i[32];
   __shared__ double s_bx, s_by;
+  __shared__ int s_abort;
   const int tid = threadIdx.x;
   const int M = cp.n_bunches, P = cp.n_species;
   const uint32_t turn = (uint32_t)(*d_turn);
@@ -328,6 +329,7 @@ __global__ void __launch_bounds__(kChainThreads) k_ion_chain(
     double lbx = cp.loss_boundary * mx, lby = cp.loss_boundary * my;
     s_bx = cs.aperture_x > lbx ? lbx : cs.aperture_x;
     s_by = cs.aperture_y > lby ? lby : cs.aperture_y;
+    s_abort = 0;
   }
   __syncthreads();
   const double bx = s_bx, by = s_by;
@@ -360,7 +362,16 @@ __global__ void __launch_bounds__(kChainThreads) k_ion_chain(
         double* Y = cd.y[st.cur];
         double* VX = cd.vx[st.cur];
         double* VY = cd.vy[st.cur];
+        // rejection keeps ~86% of draws; a degenerate (infinite) bunch size
+        // would reject forever, so the attempts are capped and flagged
         while (need > 0) {
+          if (base >= (1u << 20)) {
+            if (tid == 0) {
+              atomicOr(status, kStatusIonBirth);
+              s_abort = 1;
+            }
+            break;
+          }
           u32x4 ctr = {{base + (uint32_t)tid, (uint32_t)j, turn, (uint32_t)(k * CG_MAX_SPECIES + p)}};
           double g0, g1;
           normal2(philox4x32_10(ctr, k0, k1), &g0, &g1);
@@ -383,6 +394,7 @@ __global__ void __launch_bounds__(kChainThreads) k_ion_chain(
       }
       st.n += cp.macro_per_ip;
       __syncthreads();
+      if (s_abort) return;
       if (st.n > cp.max_ions) {
         if (tid == 0) atomicOr(status, kStatusIonOverflow);
         return;
@@ -771,20 +783,19 @@ __global__ void __launch_bounds__(kTile) k_gaussian(double* __restrict__ c, int6
   }
   const SectionDev& s = *sec0;
   const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32) ^ kStreamInitDist;
+  // both cuts keep ~99% of draws; at most 64 attempts (the last one is kept)
   double z = 0, dp = 0;
-  for (uint32_t a = 0;; ++a) {
+  for (uint32_t a = 0; a < 64; ++a) {
     u32x4 ctr = {{(uint32_t)t.i, (uint32_t)t.b, a, 0u}};
     double g0, g1;
     normal2(philox4x32_10(ctr, k0, k1), &g0, &g1);
-    if (g0 * g0 + g1 * g1 < 9.0) {
-      z = sz * g0;
-      dp = sdp * g1 / r_beta2;
-      break;
-    }
+    z = sz * g0;
+    dp = sdp * g1 / r_beta2;
+    if (g0 * g0 + g1 * g1 < 9.0) break;
   }
   double rx = sqrt(emit_x * s.beta_x), ry = sqrt(emit_y * s.beta_y);
   double x = 0, px = 0, y = 0, py = 0;
-  for (uint32_t a = 0;; ++a) {
+  for (uint32_t a = 0; a < 64; ++a) {
     u32x4 ctr = {{(uint32_t)t.i, (uint32_t)t.b, a, 1u}};
     double g0, g1, g2, g3;
     normal2(philox4x32_10(ctr, k0, k1), &g0, &g1);

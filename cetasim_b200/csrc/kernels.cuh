@@ -9,6 +9,7 @@ enum : int {
   kStatusIonOverflow = 1,
   kStatusTransmission = 2,
   kStatusLrRange = 4,
+  kStatusIonBirth = 8,
 };
 
 cudaError_t launch_moments(Handle& h, int k);
