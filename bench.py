@@ -1,0 +1,311 @@
+"""Benchmark: fast-ion multi-particle tracking turns on B200.
+
+Workload (one step = one full turn of MPBeam::Run order, MPBeam.cpp:1010-1102):
+80 bunches x 2e4 FP64 macroparticles in consecutive 2 ns buckets, 20
+interaction points (beta = 10 m), CO ions at 1e-9 Pa with one macro-ion per
+bunch passage per IP, exact Bassetti-Erskine kicks both ways through the
+FP64 Faddeeva kernel, synchrotron radiation with quantum excitation.
+
+  value  macroparticle-turns/s with the beam resident in HBM (device time of
+         K turns by CUDA events on the library's stream, L2 flushed between
+         turns: the 77 MB state would otherwise stay in the 126 MB L2)
+  e2e    the same through the C ABI with the beam uploaded from pinned host
+         memory and the per-bunch moments read back every turn
+  roofline  the electron-side field-kick kernel (the largest FP64 kernel of
+         the turn) against the FP64 FMA throughput measured on this GPU
+  cpu_baseline  the CPU oracle (OpenMP over particles) on a bounded sample
+
+--impl reference times the reference algorithm on the host cores (the oracle
+restatement; the reference's own tracking sources do not build here).
+Multi-GPU: one process per GPU (torchrun), each an independent replica of the
+workload (weak scaling); timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD_DESC = ("fast_ion: 80 bunches x 2e4 FP64 macroparticles, 2 ns spacing, 20 IPs, "
+                 "CO at 1e-9 Pa, 1 macro-ion/bunch/IP, exact Bassetti-Erskine both ways, "
+                 "synchrotron radiation with quantum excitation")
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True,
+                                     text=True, timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([s.strip() for s in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4)
+                          if len(s) > 5 + i and s[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def cpu_sample(turns: int = 1, n_scale: float = 0.025, threads: int | None = None):
+    """Oracle timing on a bounded sample of the workload: 80 bunches x 500
+    macroparticles, all 20 IPs, `turns` turns.  Returns (value, seconds, n)."""
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads or os.cpu_count() or 1))
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle
+    from helpers import particles, small
+    wl = small("fast_ion", n_scale)
+    o = oracle.OracleBeam(wl)
+    for j, c in enumerate(particles(wl, seed=3, spread=2.0)):
+        o.upload(j, c)
+    t = time.perf_counter()
+    o.Run(0, turns)
+    dt = time.perf_counter() - t
+    return wl.n_particles * turns / dt, dt, wl.n_particles
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    from cetasim_b200 import build
+    build.build_oracle()
+    vals = []
+    n = 0
+    for s in range(args.warmup + args.steps):
+        v, dt, n = cpu_sample(turns=1)
+        if s >= args.warmup:
+            vals.append(dt)
+    tot = sum(vals)
+    value = n * len(vals) / tot
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    sample = (f"80 bunches x {n // 80} macroparticles (of 2e4), 20 IPs, 1 turn per step; "
+              "oracle restatement in C with OpenMP over particles")
+    line = {"impl": "reference", "metric": "macroparticle-turns/s", "value": value,
+            "unit": "macroparticle-turns/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(vals), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD_DESC, "sample": sample},
+            "cpu_baseline": {"value": value, "unit": "macroparticle-turns/s", "cores": cores,
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "macroparticle-turns/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n-scale", type=float, default=1.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        return run_reference(args, rank)
+
+    import torch
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    from cetasim_b200 import _abi, configs
+    from cetasim_b200.beam import MPBeam
+
+    lib = _abi.load()
+    wl = configs.make("fast_ion", n_scale=args.n_scale, seed=1234 + rank)
+    beam = MPBeam(wl, device=local)
+    beam.generate(seed=99 + rank)
+    stream = torch.cuda.ExternalStream(lib.cg_stream(beam.h))
+    launches = C.c_int()
+    lib.cg_turn_launches(beam.h, C.byref(launches))
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def barrier():
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    # warm-up turns (the first one instantiates the turn graph)
+    beam.Run(0, args.warmup)
+    barrier()
+    times = []
+    with ClockSampler(local) as clk:
+        for s in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()  # evict the (L2-resident) beam between turns
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            beam.Run(args.warmup + s, 1)
+            e1.record(stream)
+            times.append((e0, e1))
+        torch.cuda.synchronize()
+    barrier()
+    ms = [a.elapsed_time(b) for a, b in times]
+    tot_ms = float(sum(ms))
+    if pg:
+        t = torch.tensor([tot_ms], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        tot_ms = float(t.item())
+    n_part = wl.n_particles
+    value = world * n_part * args.steps / (tot_ms * 1e-3)
+    ion_kicks_turn = n_part * wl.cfg.n_sections  # electron-side kicks (dominant)
+
+    # e2e through the C ABI: pinned host beam uploaded every turn, moments read back
+    hbufs = []
+    for j in range(wl.n_bunches):
+        n = int(wl.n_macro[j])
+        p = lib.cg_host_alloc(6 * 8 * n)
+        arr = np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_double)), shape=(6, n))
+        c, _ = beam.download(j)
+        arr[:] = c
+        hbufs.append((p, arr))
+    mom = (_abi.BunchMoments * wl.n_bunches)()
+    e2e_steps = max(3, args.steps // 2)
+    barrier()
+    ev = []
+    for s in range(e2e_steps + 1):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for j, (p, arr) in enumerate(hbufs):
+            beam._check(lib.cg_upload_bunch(beam.h, j, *[_abi.ptr(arr[d]) for d in range(6)], None))
+        beam.Run(args.warmup + args.steps + s, 1)
+        beam._check(lib.cg_beam_rms(beam.h, 0))
+        beam._check(lib.cg_get_moments(beam.h, mom))
+        e1.record(stream)
+        if s > 0:
+            ev.append((e0, e1))
+    torch.cuda.synchronize()
+    e2e_ms = float(sum(a.elapsed_time(b) for a, b in ev))
+    if pg:
+        t = torch.tensor([e2e_ms], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * n_part * len(ev) / (e2e_ms * 1e-3)
+    h2d = n_part * 48
+    d2h = wl.n_bunches * C.sizeof(_abi.BunchMoments)
+    for p, _ in hbufs:
+        lib.cg_host_free(p)
+
+    # dominant FP64 kernel: electron-side ion kick at IP 0, timed alone
+    beam.MPBeamRMSCal(0)
+    beam.SSBeamIonEffectOneInteractionPoint(10**6, 0)
+    kick_ms = C.c_double()
+    beam._check(lib.cg_time_stage(beam.h, 1, 0, 20, C.byref(kick_ms)))
+    map_ms = C.c_double()
+    beam._check(lib.cg_time_stage(beam.h, 0, 0, 20, C.byref(map_ms)))
+    chain_ms = C.c_double()
+    beam._check(lib.cg_time_stage(beam.h, 2, 0, 5, C.byref(chain_ms)))
+    peak = C.c_double()
+    lib.cg_fp64_peak(C.byref(peak))
+    flops_per_kick = FLOPS_PER_KICK
+    achieved = n_part * flops_per_kick / (kick_ms.value * 1e-3)
+
+    result = None
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu and world == 1:
+            try:
+                v, dt, n = cpu_sample(turns=1)
+                cpu = {"value": v, "unit": "macroparticle-turns/s",
+                       "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)),
+                       "kind": "port",
+                       "sample": f"80 bunches x {n // 80} macroparticles, 20 IPs, 1 turn "
+                                 f"({dt:.1f} s); C oracle, OpenMP over particles"}
+            except Exception as e:  # the baseline is reported, never required
+                cpu = {"value": None, "unit": "macroparticle-turns/s", "cores": 0, "kind": "port",
+                       "sample": f"failed: {e}"}
+        result = {
+            "metric": "macroparticle-turns/s", "value": value, "unit": "macroparticle-turns/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": tot_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD_DESC, "bunches": wl.n_bunches,
+                       "macroparticles": n_part, "interaction_points": wl.cfg.n_sections,
+                       "turns_per_step": 1, "l2": "flushed between turns (512 MB write)",
+                       "parallelism": f"replica x{world}"},
+            "ion_kicks_per_s": world * ion_kicks_turn * args.steps / (tot_ms * 1e-3),
+            "kernels_ms": {"ion_field_kick": kick_ms.value, "section_map": map_ms.value,
+                           "ion_chain": chain_ms.value},
+            "roofline": {"bound": "fp64", "kernel": "k_ion_kick (electron-side Bassetti-Erskine)",
+                         "achieved": achieved / 1e12, "peak": peak.value / 1e12, "unit": "TFLOP/s",
+                         "frac": achieved / peak.value if peak.value else None,
+                         "peak_source": "measured FP64 FMA throughput (cg_fp64_peak)",
+                         "algorithmic_flops_per_kick": flops_per_kick, "traffic": None},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "macroparticle-turns/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches.value * args.steps,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(result), flush=True)
+    beam.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return result
+
+
+# FP64 operations of one electron-side kick (two w(z) through the Weideman
+# series, the exp of the Gaussian factor counted as one operation, and the
+# field algebra), counted from be_field.cuh / faddeeva.cuh: 2 x 307 + 32.
+FLOPS_PER_KICK = 646
+
+if __name__ == "__main__":
+    main()

@@ -127,6 +127,12 @@ EXPORTS = [
     ("cg_fir", I, [C.c_void_p, I]),
     ("cg_mark_lost", I, [C.c_void_p, PD]),
     ("cg_run_turns", I, [C.c_void_p, I, I]),
+    ("cg_host_alloc", C.c_void_p, [C.c_size_t]),
+    ("cg_host_free", None, [C.c_void_p]),
+    ("cg_stream", C.c_void_p, [C.c_void_p]),
+    ("cg_turn_launches", I, [C.c_void_p, PI]),
+    ("cg_time_stage", I, [C.c_void_p, I, I, I, PD]),
+    ("cg_fp64_peak", I, [PD]),
     ("cg_ion_count", I, [C.c_void_p, I, I, PI]),
     ("cg_ion_download", I, [C.c_void_p, I, I, PD, PD, PD, PD, I, PI]),
     ("cg_ion_upload", I, [C.c_void_p, I, I, PD, PD, PD, PD, I]),

@@ -70,6 +70,27 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
     return LIB
 
 
+CLI = os.path.join(HERE, "cetasim_mp")
+HOST_SOURCES = ["mpbeam.cpp", "cetasim_mp.cpp"]
+
+
+def build_host(force: bool = False, verbose: bool = False) -> str:
+    """The C++ host layer (MPBeam-named wrapper) and the cetasim_mp driver,
+    linked against the in-tree libcetagpu.so."""
+    hdir = os.path.join(HERE, "host")
+    deps = [os.path.join(hdir, s) for s in HOST_SOURCES + ["mpbeam.hpp"]] + [LIB]
+    if not force and not _stale(CLI, deps):
+        return CLI
+    cmd = ["g++", "-O2", "-std=c++17", "-o", CLI + ".tmp",
+           *[os.path.join(hdir, s) for s in HOST_SOURCES], "-L" + HERE, "-lcetagpu",
+           "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    os.replace(CLI + ".tmp", CLI)
+    return CLI
+
+
 def build_oracle(verbose: bool = False) -> None:
     """Builds the CPU oracle (test infrastructure) and, when the reference
     sources are present, its compiled w(z) under oracle/_ref."""
@@ -85,5 +106,6 @@ def build_oracle(verbose: bool = False) -> None:
 
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose=True, ptxas_verbose="-v" in sys.argv)
+    build_host(force="--force" in sys.argv, verbose=True)
     build_oracle(verbose=True)
     print(LIB)

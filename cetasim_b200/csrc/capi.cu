@@ -466,6 +466,7 @@ int cg_set_beam(cg_handle* H, int M, const int* n_macro, const int* harm, const 
     if (j > 0 && harm[j] <= harm[j - 1]) return fail(&h, CG_ERR_INVALID, "bunch harmonic numbers must increase");
   }
   h.M = M;
+  h.chain.n_bunches = M;
   h.n_macro.assign(n_macro, n_macro + M);
   h.harm.assign(harm, harm + M);
   h.ne.assign(ne, ne + M);
@@ -792,6 +793,81 @@ int cg_run_turns(cg_handle* H, int turn0, int n_turns) {
     }
   }
   return check_status(h);
+}
+
+// ---- measurement and host memory ----
+
+void* cg_host_alloc(size_t bytes) {
+  void* p = nullptr;
+  if (cudaMallocHost(&p, bytes ? bytes : 16) != cudaSuccess) return nullptr;
+  return p;
+}
+
+void cg_host_free(void* p) {
+  if (p) cudaFreeHost(p);
+}
+
+void* cg_stream(cg_handle* H) { return H ? (void*)H->h.stream : nullptr; }
+
+static int count_turn_launches(Handle& h) {
+  const cg_config& c = h.cfg;
+  int n = h.K;                                   // maps
+  if (c.flag_beam_ion) n += 3 * h.K;             // moments + chain + kick per IP
+  if (c.flag_lr_wake || c.flag_sr_wake) n += 1;  // post-map moments
+  if (c.flag_lr_wake) n += 2;                    // push + forces
+  n += 1;                                        // longitudinal tail
+  if (c.flag_sr_wake) n += 5;
+  if (c.flag_fir) n += 2;
+  n += 2;                                        // mark lost + turn counter
+  return n;
+}
+
+int cg_turn_launches(cg_handle* H, int* launches) {
+  if (!H || !launches) return CG_ERR_INVALID;
+  *launches = count_turn_launches(H->h);
+  return CG_OK;
+}
+
+int cg_time_stage(cg_handle* H, int stage, int k, int reps, double* ms) {
+  STAGE_PROLOGUE
+  if (k < 0 || k >= h.K || reps < 1 || !ms) return fail(&h, CG_ERR_INVALID, "bad arguments");
+  if ((stage == 1 || stage == 2) && !h.cfg.flag_beam_ion)
+    return fail(&h, CG_ERR_NOT_READY, "runBeamIonFlag is off");
+  cudaEvent_t e0, e1;
+  CG_CUDA(&h, cudaEventCreate(&e0));
+  CG_CUDA(&h, cudaEventCreate(&e1));
+  CG_CUDA(&h, cudaEventRecord(e0, h.stream));
+  cudaError_t e = cudaSuccess;
+  for (int r = 0; r < reps && e == cudaSuccess; ++r) {
+    switch (stage) {
+      case 0: e = launch_map(h, k); break;
+      case 1: e = launch_ion_kick(h, k); break;
+      case 2: e = launch_ion_chain(h, k); break;
+      case 3: e = launch_moments(h, k); break;
+      default: e = launch_long(h, kLongRF | kLongDrift | kLongLoss | (h.cfg.flag_synrad ? kLongSynrad : 0));
+    }
+  }
+  CG_CUDA(&h, cudaEventRecord(e1, h.stream));
+  CG_CUDA(&h, cudaEventSynchronize(e1));
+  float t = 0;
+  cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (e != cudaSuccess) return cuda_fail(&h, e, "cg_time_stage");
+  *ms = (double)t / reps;
+  return check_status(h);
+}
+
+int cg_fp64_peak(double* flops) {
+  if (!flops) return CG_ERR_INVALID;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(nullptr, CG_ERR_CUDA, "no CUDA device available");
+  double f = 0;
+  cudaError_t e = measure_fp64_peak(&f);
+  if (e != cudaSuccess) return fail(nullptr, CG_ERR_CUDA, cudaGetErrorString(e));
+  *flops = f;
+  return CG_OK;
 }
 
 // ---- ion clouds ----

@@ -228,7 +228,8 @@ CG_HD cplx w_upper_right(double x, double y) {
 
 // General w(z) for any complex z (NaN in -> NaN out).
 CG_HD cplx w_general(double x, double y) {
-  if (isnan(x) || isnan(y)) return {NAN, NAN};
+  // NaN in gives NaN out, except that w(iy) stays real for x = 0
+  if (isnan(x) || isnan(y)) return {NAN, x == 0.0 ? 0.0 : NAN};
   if (y >= 0.0) {
     if (x >= 0.0) return w_upper_right(x, y);
     cplx w = w_upper_right(-x, y);  // w(-conj z) = conj w(z)

@@ -864,6 +864,47 @@ cudaError_t launch_field(const double* x, const double* y, const double* sx, con
   return cudaGetLastError();
 }
 
+// FP64 FMA throughput probe: 8 independent register FMA chains per thread.
+__global__ void __launch_bounds__(256) k_fp64_peak(double* out, int iters, double a, double b) {
+  double r[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) r[q] = threadIdx.x * 1e-3 + q;
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) r[q] = fma(r[q], a, b);
+  }
+  double s = 0;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) s += r[q];
+  if (s == 123.456) out[0] = s;  // keeps the chains live
+}
+
+cudaError_t measure_fp64_peak(double* flops) {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  double* out = nullptr;
+  cudaError_t e = cudaMalloc(&out, sizeof(double));
+  if (e != cudaSuccess) return e;
+  const int blocks = sms * 8, threads = 256, iters = 4096;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  k_fp64_peak<<<blocks, threads>>>(out, 64, 0.999999, 1e-7);  // warm-up
+  cudaEventRecord(e0);
+  k_fp64_peak<<<blocks, threads>>>(out, iters, 0.999999, 1e-7);
+  cudaEventRecord(e1);
+  e = cudaEventSynchronize(e1);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  if (e != cudaSuccess) return e;
+  *flops = 2.0 * 8.0 * iters * (double)blocks * threads / (ms * 1e-3);
+  return cudaGetLastError();
+}
+
 cudaError_t upload_weideman_table() {
   return cudaMemcpyToSymbol(c_weideman, &h_weideman, sizeof(WeidemanTable));
 }

@@ -37,5 +37,6 @@ cudaError_t launch_faddeeva(const double* zr, const double* zi, double* wr, doub
 cudaError_t launch_field(const double* x, const double* y, const double* sx, const double* sy,
                          double* fx, double* fy, int64_t n, cudaStream_t s);
 cudaError_t upload_weideman_table();
+cudaError_t measure_fp64_peak(double* flops);
 
 }  // namespace cg

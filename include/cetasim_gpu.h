@@ -23,6 +23,7 @@
 #ifndef CETASIM_GPU_H
 #define CETASIM_GPU_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -274,6 +275,26 @@ int cg_mark_lost(cg_handle* h, double* transmissions /* [n_bunches] */);
  * [turn0, turn0 + n_turns), as one CUDA graph per turn, without host
  * round trips. */
 int cg_run_turns(cg_handle* h, int turn0, int n_turns);
+
+/* ---- measurement and host memory (no reference counterpart: the reference
+ * only times the whole run with gettimeofday, main.cpp:53-99) ---- */
+
+/* Page-locked host buffer for fast uploads/downloads (cudaMallocHost). */
+void* cg_host_alloc(size_t bytes);
+void cg_host_free(void* p);
+/* The CUDA stream (cudaStream_t) all kernels of h run on. */
+void* cg_stream(cg_handle* h);
+/* Kernel launches one cg_run_turns turn issues. */
+int cg_turn_launches(cg_handle* h, int* launches);
+/* Times `reps` back-to-back launches of one stage kernel with CUDA events on
+ * h's stream; *ms = average per launch.  stage: 0 section map (k), 1 ion
+ * field kick (k, uses the records of the last cg_beam_ion_ip at k), 2 ion
+ * chain (k), 3 moments (k), 4 longitudinal turn tail. The beam state is
+ * advanced by these launches. */
+int cg_time_stage(cg_handle* h, int stage, int k, int reps, double* ms);
+/* FP64 FMA throughput of this device measured by a register-resident FMA
+ * chain kernel, in FLOP/s (2 per FMA). */
+int cg_fp64_peak(double* flops);
 
 /* ---- ion clouds (LatticeInterActionPoint ion state) ---- */
 

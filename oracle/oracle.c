@@ -524,6 +524,7 @@ int or_beam_ion_ip(or_state* s, int turn, int k) {
       r[1] = c->rms_x; r[2] = c->rms_y; r[3] = c->aver_x; r[4] = c->aver_y; r[5] = c->n;
     }
     /* SSIonBunchInteraction (2) + BunchTransferDueToIon: electron side */
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < b->n; i++) {
       if (b->surv[i] != 0) continue;
       b->efx[i] = 0; b->efy[i] = 0;
@@ -578,6 +579,7 @@ int or_section_map(or_state* s, int k) {
   double weighY = sc->phase_adv_y / (2 * PI * r->work_qy);
   for (int j = 0; j < s->M; ++j) {
     or_bunch* b = &s->b[j];
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < b->n; i++) {
       if (b->surv[i] != 0) continue;
       double v[6], v1[6], v2[6];
@@ -616,6 +618,7 @@ int or_rf_kick(or_state* s) {
   for (int c = 0; c < r->n_cav; ++c) {
     for (int j = 0; j < s->M; ++j) {
       or_bunch* b = &s->b[j];
+#pragma omp parallel for schedule(static)
       for (int i = 0; i < b->n; i++) {
         double th = b->c[4][i] / C_LIGHT / r->r_beta * 2. * PI * (double)r->cav_harm[c] * fRF;
         /* Re(V exp(-i th)) as std::complex multiplies it: a c - b d, d = -sin */
@@ -631,6 +634,7 @@ int or_longi_drift(or_state* s) {
   const cg_ring* r = &s->cfg.ring;
   for (int j = 0; j < s->M; ++j) {
     or_bunch* b = &s->b[j];
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < b->n; i++) {
       double d = b->c[5][i];
       b->c[4][i] -= r->circ_ring * (r->alphac[0] * d + r->alphac[1] * pow(d, 2) + r->alphac[2] * pow(d, 3));
@@ -658,6 +662,7 @@ int or_synrad(or_state* s, int turn) {
   coeff[2] = sqrt(1 - pow(lambda[2], 4)) * sqrt(r->emit_nat[2]);
   for (int j = 0; j < s->M; ++j) {
     or_bunch* b = &s->b[j];
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < b->n; i++) {
       if (b->surv[i] != 0) continue;
       double v[6], X[6];
@@ -818,6 +823,7 @@ int or_sr_wake(or_state* s, int turn) {
       else { ax[i] /= cnt[i]; ay[i] /= cnt[i]; }
     }
     double* pot = b->sr_pot;
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < B; i++) {
       for (int jj = 0; jj < B; jj++) {
         double tau = (i - jj) * dtBin;

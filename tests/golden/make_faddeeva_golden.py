@@ -38,7 +38,16 @@ def kat_points():
     z = block("cmplx z[NTST] = {")
     w = block("cmplx w[NTST] = {")
     assert len(z) == len(w) == 57, (len(z), len(w))
-    return np.array([a + 1j * b for a, b in z]), np.array([a + 1j * b for a, b in w])
+    return cplx(z), cplx(w)
+
+
+def cplx(pairs):
+    # set real and imaginary parts separately: a + 1j * b would turn
+    # 0 + 1j * inf into nan + inf j
+    out = np.empty(len(pairs), dtype=np.complex128)
+    out.real = [a for a, _ in pairs]
+    out.imag = [b for _, b in pairs]
+    return out
 
 
 def ref_w(z):
@@ -49,7 +58,7 @@ def ref_w(z):
     wr, wi = np.empty_like(zr), np.empty_like(zr)
     lib.ref_faddeeva_w(zr.ctypes.data_as(P), zi.ctypes.data_as(P), wr.ctypes.data_as(P),
                        wi.ctypes.data_as(P), ctypes.c_int64(len(zr)))
-    return wr + 1j * wi
+    return cplx(list(zip(wr, wi)))
 
 
 def main():
