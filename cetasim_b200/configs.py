@@ -115,7 +115,7 @@ class Workload:
 
 
 def make(name: str, n_scale: float = 1.0, turns_lr: int = 10, lib=None, seed: int = 1234,
-         derive=None, lattice_init=None) -> Workload:
+         derive=None, lattice_init=None, bunch_current: float | None = None) -> Workload:
     """Builds a workload.  `n_scale` scales macroparticle counts (tests use
     small values); `derive`/`lattice_init` default to the library's own
     cg_config_derive / cg_lattice_init (tests may pass the oracle's)."""
@@ -186,6 +186,8 @@ def make(name: str, n_scale: float = 1.0, turns_lr: int = 10, lib=None, seed: in
     # the regime where CO ions are trapped inside the train: critical mass
     # number ~23 < 28 for 2 ns spacing)
     current = 1e-3 if name == "plain_single" else 0.125e-3
+    if bunch_current is not None:
+        current = bunch_current
     ne = [current / f0 / E_CHARGE] * M
     eps_x = cfg.ring.natural_emit / (1 + cfg.ring.coupling)
     eps_y = eps_x * cfg.ring.coupling

@@ -18,14 +18,16 @@ namespace cg {
 
 // BassettiErskine1 for sx > sy.  posx/posy signs are restored at the end as
 // in Bunch.cpp:161-169 (note: "<= 0" flips, so x = 0 gives -0 * F).
+template <bool LowLat = false>
 CG_HD void bassetti_erskine(double posx, double posy, double sx, double sy,
                             double* fx, double* fy) {
   double ax = fabs(posx), ay = fabs(posy);
   double sigma = sqrt(2.0 * (sx * sx) - 2.0 * (sy * sy));
   double r = sy / sx;
   double coeff = -1.0 * sqrt(kPi) / sigma;
-  cplx w1 = w_quadrant1(ax / sigma, ay / sigma);
-  cplx w2 = w_quadrant1(r * ax / sigma, ay / sigma / r);
+  cplx w1 = LowLat ? w_quadrant1_lowlat(ax / sigma, ay / sigma) : w_quadrant1(ax / sigma, ay / sigma);
+  cplx w2 = LowLat ? w_quadrant1_lowlat(r * ax / sigma, ay / sigma / r)
+                   : w_quadrant1(r * ax / sigma, ay / sigma / r);
   double tx = ax / sx, ty = ay / sy;
   double z3 = -(tx * tx) / 2.0 - (ty * ty) / 2.0;
   double w3 = -exp(z3);
@@ -48,16 +50,18 @@ CG_HD void gaussian_round_field(double posx, double posy, double sx, double* fx,
   *fy = -posy / r2 * g;
 }
 
-// The dispatch of MPBunch.cpp:1128-1146 / 1179-1197.
+// The dispatch of MPBunch.cpp:1128-1146 / 1179-1197.  LowLat selects the
+// latency-optimised w(z) (Estrin form) for the sequential ion chain.
+template <bool LowLat = false>
 CG_HD void gaussian_field(double posx, double posy, double sx, double sy,
                           double* fx, double* fy) {
   if (fabs(posx / sx) + fabs(posy / sy) < 1.0e-5) {
     *fx = 0.0;
     *fy = 0.0;
   } else if ((sx - sy) / sy > 1.e-4) {
-    bassetti_erskine(posx, posy, sx, sy, fx, fy);
+    bassetti_erskine<LowLat>(posx, posy, sx, sy, fx, fy);
   } else if ((sx - sy) / sy < -1.e-4) {
-    bassetti_erskine(posy, posx, sy, sx, fy, fx);
+    bassetti_erskine<LowLat>(posy, posx, sy, sx, fy, fx);
   } else {
     gaussian_round_field(posx, posy, sx, fx, fy);
   }

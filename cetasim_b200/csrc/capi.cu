@@ -519,6 +519,8 @@ int cg_set_beam(cg_handle* H, int M, const int* n_macro, const int* harm, const 
   if (h.cfg.flag_beam_ion) {
     if (dalloc(&d.rec, (size_t)h.K * M * h.P)) { free_beam(h); return fail(&h, CG_ERR_OOM, "ion records"); }
     cudaMemset(d.rec, 0, sizeof(CloudRec) * h.K * M * h.P);
+    cudaError_t pe = prepare_ion_chain(h);
+    if (pe != cudaSuccess) { free_beam(h); return cuda_fail(&h, pe, "ion chain shared memory"); }
   }
   if (h.cfg.flag_lr_wake) {
     if (dalloc(&d.lr_hist, (size_t)h.cfg.lr_turns * 3 * M) || dalloc(&d.lr_force, 3 * (size_t)M)) {

@@ -170,35 +170,41 @@ __device__ void bunch_moment_finish(int b, const BunchDev& B, const MomPartial* 
     last = (prev == (unsigned)(B.n_tiles - 1));
   }
   __syncthreads();
-  if (!last) return;
+  if (!last || threadIdx.x >= 32) return;
   __threadfence();
-  // level 0: thread t merges partials t, t + kTile, ... sequentially
+  // warp 0: lane l merges partials l, l + 32, ... in order, then a fixed
+  // shuffle tree (lane i absorbs lane i + o) leaves the bunch total in lane 0
+  constexpr int ND = (int)(sizeof(MomPartial) / sizeof(double));
+  const int lane = threadIdx.x;
   MomPartial acc;
   mom_clear(acc);
-  for (int t = threadIdx.x; t < B.n_tiles; t += kTile) {
+  for (int t = lane; t < B.n_tiles; t += 32) {
     // partials written by other CTAs: read through L2 (no stale L1 lines)
     const double* src = reinterpret_cast<const double*>(partials + B.tile_off + t);
     MomPartial q;
     double* dst = reinterpret_cast<double*>(&q);
 #pragma unroll
-    for (int e = 0; e < (int)(sizeof(MomPartial) / sizeof(double)); ++e) dst[e] = __ldcg(src + e);
+    for (int e = 0; e < ND; ++e) dst[e] = __ldcg(src + e);
     mom_merge(acc, q);
   }
-  sp[threadIdx.x] = acc;
-  __syncthreads();
-  for (int s = 1; s < kTile; s <<= 1) {
-    if ((threadIdx.x % (2 * s)) == 0 && threadIdx.x + s < kTile) mom_merge(sp[threadIdx.x], sp[threadIdx.x + s]);
-    __syncthreads();
+  for (int o = 16; o > 0; o >>= 1) {
+    MomPartial q;
+    double* dq = reinterpret_cast<double*>(&q);
+    const double* da = reinterpret_cast<const double*>(&acc);
+#pragma unroll
+    for (int e = 0; e < ND; ++e) dq[e] = __shfl_down_sync(FULL_MASK, da[e], o);
+    if (lane < o) mom_merge(acc, q);
   }
-  if (threadIdx.x == 0) {
+  if (lane == 0) {
     BunchMomDev m = mom[b];
     double tr = m.transmission;
     double z0 = z[(int64_t)B.tile_off * kTile];
-    mom_finalize(sp[0], beta_x, beta_y, z0, m);
+    mom_finalize(acc, beta_x, beta_y, z0, m);
     m.transmission = tr;
     mom[b] = m;
     counters[b] = 0;
   }
+  (void)sp;
 }
 
 __global__ void __launch_bounds__(kTile) k_moments(const double* __restrict__ c, int64_t npad,
@@ -208,7 +214,7 @@ __global__ void __launch_bounds__(kTile) k_moments(const double* __restrict__ c,
                                                    MomPartial* partials, unsigned* counters,
                                                    BunchMomDev* mom, double beta_x, double beta_y) {
   __shared__ double smem[9 * 32];
-  __shared__ MomPartial sp[kTile];
+  MomPartial* sp = nullptr;
   TileIdx t = tile_index(tile_bunch, bunch);
   double v[6] = {0, 0, 0, 0, 0, 0};
   bool alive = false;
@@ -308,10 +314,53 @@ struct ChainSection {
   double pressure, temperature, length, aperture_x, aperture_y;
 };
 
+// Shared-memory layout of the chain kernel: per-bunch inputs, then per
+// species the cloud arrays (x, y, vx, vy) when they fit.
+struct ChainSmem {
+  int m_bytes;       // bytes of per-bunch data
+  int cap;           // ions per species that fit in shared memory
+};
+
+__device__ __forceinline__ void chain_bunch_load(const BunchDev* __restrict__ bunch,
+                                                 const BunchMomDev* __restrict__ mom, int j,
+                                                 const double* sb, int M, bool sb_ok, double& mx,
+                                                 double& my, double& sx, double& sy, double& ne,
+                                                 int& gap) {
+  if (sb_ok) {
+    mx = sb[j];
+    my = sb[M + j];
+    sx = sb[2 * M + j];
+    sy = sb[3 * M + j];
+    ne = sb[4 * M + j];
+    gap = (int)sb[5 * M + j];
+  } else {
+    mx = mom[j].mean[0];
+    my = mom[j].mean[2];
+    sx = mom[j].rms_x;
+    sy = mom[j].rms_y;
+    ne = bunch[j].ne;
+    gap = bunch[j].gap;
+  }
+}
+
+// Ion chain of one interaction point (MPBeam::SSBeamIonEffectOneInteraction
+// Point, MPBeam.cpp:2585-2611): one CTA walks the bunches in order, because
+// bunch j meets the cloud left behind by bunch j-1.  The walk is latency
+// bound, so the cloud and the bunch inputs live in shared memory for the
+// whole walk (global memory when they do not fit), removal of lost ions is an
+// in-place stable compaction, and the ion-side field uses the Estrin form of
+// w(z).  Per bunch j and species p:
+//   LIP::GetIonNumberPerInterAction (LIP.cpp:974-982), IonGenerator
+//   (LIP.cpp:985-1019) with Philox counters {attempt, j, turn, k*8+p},
+//   IonsUpdate (LIP.cpp:1021-1051), IonRMSCal (LIP.cpp:1113-1155), the record
+//   of the cloud Gaussian for the electron kick (MPBunch.cpp:1164-1206), the
+//   ion-side kick (MPBunch.cpp:1111-1157) and LIP::IonTransferDueToBunch
+//   (LIP.cpp:1158-1211).
 __global__ void __launch_bounds__(kChainThreads) k_ion_chain(
     ChainParams cp, ChainSection cs, const BunchDev* __restrict__ bunch,
     const BunchMomDev* __restrict__ mom, CloudDev* clouds, CloudState* cst, CloudRec* rec,
-    int* status, const int* __restrict__ d_turn, int k) {
+    int* status, const int* __restrict__ d_turn, int k, int smem_cap, int sb_ok) {
+  extern __shared__ double dsm[];
   __shared__ double smem[4 * 32];
   __shared__ int smem_i[32];
   __shared__ double s_bx, s_by;
@@ -319,8 +368,10 @@ __global__ void __launch_bounds__(kChainThreads) k_ion_chain(
   const int tid = threadIdx.x;
   const int M = cp.n_bunches, P = cp.n_species;
   const uint32_t turn = (uint32_t)(*d_turn);
-  // MPGetBeamInfo: bunchSizeXMax / YMax over all bunches (MPBeam.cpp:2175-2186)
+  double* sb = dsm;                                 // 6 x M
+  double* scl = dsm + (sb_ok ? 6 * (size_t)M : 0);  // P x 4 x smem_cap
   if (tid == 0) {
+    // MPGetBeamInfo: bunchSizeXMax / YMax over all bunches (MPBeam.cpp:2175-2186)
     double mx = mom[0].rms_x, my = mom[0].rms_y;
     for (int j = 1; j < M; ++j) {
       if (mom[j].rms_x > mx) mx = mom[j].rms_x;
@@ -331,39 +382,77 @@ __global__ void __launch_bounds__(kChainThreads) k_ion_chain(
     s_by = cs.aperture_y > lby ? lby : cs.aperture_y;
     s_abort = 0;
   }
+  if (sb_ok)
+    for (int j = tid; j < M; j += kChainThreads) {
+      sb[j] = mom[j].mean[0];
+      sb[M + j] = mom[j].mean[2];
+      sb[2 * M + j] = mom[j].rms_x;
+      sb[3 * M + j] = mom[j].rms_y;
+      sb[4 * M + j] = bunch[j].ne;
+      sb[5 * M + j] = (double)bunch[j].gap;
+    }
+  // per species: where the cloud lives for this walk
+  double* AX[CG_MAX_SPECIES];
+  double* AY[CG_MAX_SPECIES];
+  double* AVX[CG_MAX_SPECIES];
+  double* AVY[CG_MAX_SPECIES];
+  int cap[CG_MAX_SPECIES];
+  bool in_smem[CG_MAX_SPECIES];
+  for (int p = 0; p < P; ++p) {
+    CloudDev cd = clouds[p];
+    int n0 = cst[p].n;
+    in_smem[p] = (long long)n0 + (long long)M * cp.macro_per_ip <= smem_cap;
+    if (in_smem[p]) {
+      double* base = scl + (size_t)p * 4 * smem_cap;
+      AX[p] = base;
+      AY[p] = base + smem_cap;
+      AVX[p] = base + 2 * smem_cap;
+      AVY[p] = base + 3 * smem_cap;
+      cap[p] = smem_cap;
+      for (int i = tid; i < n0; i += kChainThreads) {
+        AX[p][i] = cd.x[0][i];
+        AY[p][i] = cd.y[0][i];
+        AVX[p][i] = cd.vx[0][i];
+        AVY[p][i] = cd.vy[0][i];
+      }
+    } else {
+      AX[p] = cd.x[0];
+      AY[p] = cd.y[0];
+      AVX[p] = cd.vx[0];
+      AVY[p] = cd.vy[0];
+      cap[p] = cd.cap;
+    }
+  }
   __syncthreads();
   const double bx = s_bx, by = s_by;
   const uint32_t k0 = (uint32_t)cp.seed, k1 = (uint32_t)(cp.seed >> 32) ^ kStreamIonBirth;
+  CloudState stv[CG_MAX_SPECIES];
+  for (int p = 0; p < P; ++p) stv[p] = cst[p];
 
   for (int j = 0; j < M; ++j) {
-    const BunchDev B = bunch[j];
-    const double mx = mom[j].mean[0], my = mom[j].mean[2];
-    const double sx = mom[j].rms_x, sy = mom[j].rms_y;
+    double mx, my, sx, sy, ne;
+    int gap;
+    chain_bunch_load(bunch, mom, j, sb, M, sb_ok != 0, mx, my, sx, sy, ne, gap);
     for (int p = 0; p < P; ++p) {
-      CloudDev cd = clouds[p];
-      CloudState st = cst[p];
-      // LIP::GetIonNumberPerInterAction (LIP.cpp:974-982)
+      CloudState& st = stv[p];
+      double* X = AX[p];
+      double* Y = AY[p];
+      double* VX = AVX[p];
+      double* VY = AVY[p];
       double press_p = cp.gas_percent[p] * cs.pressure;
-      double line_density = cp.cross_section[p] * press_p / cs.temperature / kBoltzmann * B.ne;
+      double line_density = cp.cross_section[p] * press_p / cs.temperature / kBoltzmann * ne;
       double ion_number = line_density * cs.length;
       st.macro_charge = ion_number / cp.macro_per_ip;
-      // LIP::IonGenerator (LIP.cpp:985-1019): N(mean, rms) births, rejected
-      // when ((x-mean)/rms)^2 + ((y-mean)/rms)^2 > 4; attempt a of bunch j
-      // is Philox counter {a, j, turn, k*CG_MAX_SPECIES+p}.
-      if (st.n + cp.macro_per_ip > cd.cap) {
+      if (st.n + cp.macro_per_ip > cap[p]) {
         if (tid == 0) atomicOr(status, kStatusIonOverflow);
         return;
       }
       if (tid < 32) {
+        // rejection keeps ~86% of draws; a degenerate (infinite) bunch size
+        // would reject forever, so the attempts are capped and flagged
         int need = cp.macro_per_ip;
         uint32_t base = 0;
         int wpos = st.n;
-        double* X = cd.x[st.cur];
-        double* Y = cd.y[st.cur];
-        double* VX = cd.vx[st.cur];
-        double* VY = cd.vy[st.cur];
-        // rejection keeps ~86% of draws; a degenerate (infinite) bunch size
-        // would reject forever, so the attempts are capped and flagged
         while (need > 0) {
           if (base >= (1u << 20)) {
             if (tid == 0) {
@@ -399,9 +488,7 @@ __global__ void __launch_bounds__(kChainThreads) k_ion_chain(
         if (tid == 0) atomicOr(status, kStatusIonOverflow);
         return;
       }
-      // LIP::IonRMSCal(k, p) (LIP.cpp:1113-1155)
-      const double* X = cd.x[st.cur];
-      const double* Y = cd.y[st.cur];
+      // LIP::IonRMSCal(k, p): count 1 keeps the stale centroid (LIP.cpp:1125-1129)
       if (st.n == 1) {
         st.rms_x = fabs(X[0]);
         st.rms_y = fabs(Y[0]);
@@ -437,17 +524,10 @@ __global__ void __launch_bounds__(kChainThreads) k_ion_chain(
         r.count = st.n;
         rec[(size_t)j * P + p] = r;
       }
-      // ion side (MPBunch.cpp:1111-1157) fused with LIP::IonTransferDueToBunch
-      // (LIP.cpp:1158-1211): v += F, x += v C/h gap/c, stable removal of ions
-      // beyond the loss boundary into the other ping-pong buffer.
-      const double coeffI = 2.0 * B.ne * kElecClassicRadius * kElectronMassEV / kIonMassEV /
+      // ion side: v += F, x += v C/h gap/c, then stable in-place removal of
+      // ions beyond the loss boundary (writes never pass the read position)
+      const double coeffI = 2.0 * ne * kElecClassicRadius * kElectronMassEV / kIonMassEV /
                             cp.mass_number[p] * kCLight;
-      const double* VX = cd.vx[st.cur];
-      const double* VY = cd.vy[st.cur];
-      double* X2 = cd.x[st.cur ^ 1];
-      double* Y2 = cd.y[st.cur ^ 1];
-      double* VX2 = cd.vx[st.cur ^ 1];
-      double* VY2 = cd.vy[st.cur ^ 1];
       int out_base = 0;
       for (int c0 = 0; c0 < st.n; c0 += kChainThreads) {
         int i = c0 + tid;
@@ -459,30 +539,66 @@ __global__ void __launch_bounds__(kChainThreads) k_ion_chain(
           vx = VX[i];
           vy = VY[i];
           double fx, fy;
-          gaussian_field(x - mx, y - my, sx, sy, &fx, &fy);
+          gaussian_field<true>(x - mx, y - my, sx, sy, &fx, &fy);
           vx += coeffI * fx;
           vy += coeffI * fy;
-          x += vx * cp.circ_ring / cp.harmonics * B.gap / kCLight;
-          y += vy * cp.circ_ring / cp.harmonics * B.gap / kCLight;
+          x += vx * cp.circ_ring / cp.harmonics * gap / kCLight;
+          y += vy * cp.circ_ring / cp.harmonics * gap / kCLight;
           keep = !(fabs(x) > bx || fabs(y) > by);
         }
         int tot;
-        int pos = block_excl_scan(keep ? 1 : 0, smem_i, &tot);
+        int pos = block_excl_scan(keep ? 1 : 0, smem_i, &tot);  // syncs: all reads done
         if (keep) {
-          X2[out_base + pos] = x;
-          Y2[out_base + pos] = y;
-          VX2[out_base + pos] = vx;
-          VY2[out_base + pos] = vy;
+          X[out_base + pos] = x;
+          Y[out_base + pos] = y;
+          VX[out_base + pos] = vx;
+          VY[out_base + pos] = vy;
         }
         out_base += tot;
+        __syncthreads();
       }
-      __syncthreads();
       st.n = out_base;
-      st.cur ^= 1;
-      if (tid == 0) cst[p] = st;
-      __syncthreads();
     }
   }
+  // write the clouds back
+  for (int p = 0; p < P; ++p) {
+    if (in_smem[p]) {
+      CloudDev cd = clouds[p];
+      for (int i = tid; i < stv[p].n; i += kChainThreads) {
+        cd.x[0][i] = AX[p][i];
+        cd.y[0][i] = AY[p][i];
+        cd.vx[0][i] = AVX[p][i];
+        cd.vy[0][i] = AVY[p][i];
+      }
+    }
+    if (tid == 0) {
+      stv[p].cur = 0;
+      cst[p] = stv[p];
+    }
+  }
+}
+
+// Shared memory of the chain kernel: per-bunch inputs (6 doubles per bunch)
+// when at most 2048 bunches, plus as many ions per species as fit in the
+// remaining opt-in shared memory.
+void chain_smem_plan(const Handle& h, int* sb_ok, int* cap, size_t* bytes) {
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  size_t budget = (size_t)optin - 4096;  // static shared memory of the kernel
+  size_t sb = h.M <= 2048 ? 6 * sizeof(double) * (size_t)h.M : 0;
+  *sb_ok = sb > 0;
+  size_t rest = budget > sb ? budget - sb : 0;
+  *cap = (int)(rest / (4 * sizeof(double) * (size_t)h.P));
+  *bytes = sb + (size_t)(*cap) * 4 * sizeof(double) * h.P;
+}
+
+// Opt-in shared memory of the chain kernel (set outside any graph capture).
+cudaError_t prepare_ion_chain(Handle& h) {
+  int sb_ok = 0, cap = 0;
+  size_t bytes = 0;
+  chain_smem_plan(h, &sb_ok, &cap, &bytes);
+  return cudaFuncSetAttribute(k_ion_chain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
 cudaError_t launch_ion_chain(Handle& h, int k) {
@@ -493,9 +609,12 @@ cudaError_t launch_ion_chain(Handle& h, int k) {
   cs.length = s.length;
   cs.aperture_x = s.aperture_x;
   cs.aperture_y = s.aperture_y;
-  k_ion_chain<<<1, kChainThreads, 0, h.stream>>>(
+  int sb_ok = 0, cap = 0;
+  size_t bytes = 0;
+  chain_smem_plan(h, &sb_ok, &cap, &bytes);
+  k_ion_chain<<<1, kChainThreads, bytes, h.stream>>>(
       h.chain, cs, h.d.bunch, h.d.mom, h.d.clouds + (size_t)k * h.P, h.d.cloud_state + (size_t)k * h.P,
-      h.d.rec + (size_t)k * h.M * h.P, h.d.status, h.d.turn, k);
+      h.d.rec + (size_t)k * h.M * h.P, h.d.status, h.d.turn, k, cap, sb_ok);
   return cudaGetLastError();
 }
 

@@ -15,6 +15,7 @@ enum : int {
 cudaError_t launch_moments(Handle& h, int k);
 cudaError_t launch_map(Handle& h, int k);
 cudaError_t launch_ion_chain(Handle& h, int k);
+cudaError_t prepare_ion_chain(Handle& h);
 cudaError_t launch_ion_kick(Handle& h, int k);
 enum LongFlags : unsigned {
   kLongRF = 1,

@@ -3,7 +3,7 @@ oracle's turn loop, and the fused graph path against the staged calls."""
 import numpy as np
 import pytest
 
-from helpers import coord_err, moments_close, pair, particles, small
+from helpers import TRAPPED, coord_err, moments_close, pair, particles, small
 
 pytestmark = pytest.mark.gpu
 
@@ -30,7 +30,7 @@ def test_turns_with_sr_wake_and_quantum_excitation():
 
 
 def test_fast_ion_turns():
-    wl = small("fast_ion", 0.01)  # 80 bunches x 200, 20 IPs
+    wl = small("fast_ion", 0.01, bunch_current=TRAPPED)  # 80 bunches x 200, 20 IPs
     g, o = pair(wl, particles(wl, seed=21, spread=2.0))
     g.Run(0, 5)
     o.Run(0, 5)
@@ -43,7 +43,7 @@ def test_fast_ion_turns():
 
 
 def test_batched_train_turns():
-    wl = small("batched_uneven", 0.002)
+    wl = small("batched_uneven", 0.002, bunch_current=TRAPPED)
     g, o = pair(wl, particles(wl, seed=8, spread=3.0))
     g.Run(0, 2)
     o.Run(0, 2)

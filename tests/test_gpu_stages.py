@@ -4,7 +4,7 @@ coordinate (or to the kick's own scale) and are stated per test."""
 import numpy as np
 import pytest
 
-from helpers import coord_err, moments_close, pair, particles, small
+from helpers import TRAPPED, coord_err, moments_close, pair, particles, small
 
 pytestmark = pytest.mark.gpu
 
@@ -127,7 +127,7 @@ def test_lr_wake_and_fir_over_turns():
 
 
 def test_ion_chain_one_interaction_point():
-    wl = small("fast_ion", 0.02)  # 80 bunches x 400
+    wl = small("fast_ion", 0.02, bunch_current=TRAPPED)  # 80 bunches x 400
     g, o = pair(wl, particles(wl, seed=4, spread=3.0))
     for turn in range(2):
         for k in (0, 1):
@@ -144,3 +144,22 @@ def test_ion_chain_one_interaction_point():
                 if len(b):
                     assert np.allclose(a, b, rtol=1e-11, atol=1e-11 * np.max(np.abs(b)))
     assert coord_err(g, o, wl).max() <= 1e-12
+
+
+def test_ion_chain_near_threshold_statistics():
+    """At the benchmark current (ions near their trapping threshold) the ion
+    motion is chaotic: counts agree exactly and the cloud Gaussians seen by
+    the electrons agree statistically."""
+    wl = small("fast_ion", 0.02)
+    g, o = pair(wl, particles(wl, seed=4, spread=3.0))
+    g.MPBeamRMSCal(0)
+    o.MPBeamRMSCal(0)
+    g.SSBeamIonEffectOneInteractionPoint(0, 0)
+    o.SSBeamIonEffectOneInteractionPoint(0, 0)
+    rg, ro = g.cloud_record(0), o.cloud_record(0)
+    assert np.array_equal(rg[..., 5], ro[..., 5])
+    # the first bunches see clouds of a few ions, identical to rounding
+    assert np.allclose(rg[:5, :, :5], ro[:5, :, :5], rtol=1e-9)
+    # over the train, rms sizes agree on average within 1 %
+    for q in (1, 2):
+        assert abs(rg[:, 0, q].mean() / ro[:, 0, q].mean() - 1) < 1e-2
