@@ -207,7 +207,7 @@ __device__ void bunch_moment_finish(int b, const BunchDev& B, const MomPartial* 
   (void)sp;
 }
 
-__global__ void __launch_bounds__(kTile) k_moments(const double* __restrict__ c, int64_t npad,
+__global__ void __launch_bounds__(kTile, 2) k_moments(const double* __restrict__ c, int64_t npad,
                                                    const uint8_t* __restrict__ surv,
                                                    const int* __restrict__ tile_bunch,
                                                    const BunchDev* __restrict__ bunch,
@@ -356,6 +356,7 @@ __device__ __forceinline__ void chain_bunch_load(const BunchDev* __restrict__ bu
 //   of the cloud Gaussian for the electron kick (MPBunch.cpp:1164-1206), the
 //   ion-side kick (MPBunch.cpp:1111-1157) and LIP::IonTransferDueToBunch
 //   (LIP.cpp:1158-1211).
+template <int PMAX>
 __global__ void __launch_bounds__(kChainThreads) k_ion_chain(
     ChainParams cp, ChainSection cs, const BunchDev* __restrict__ bunch,
     const BunchMomDev* __restrict__ mom, CloudDev* clouds, CloudState* cst, CloudRec* rec,
@@ -370,17 +371,24 @@ __global__ void __launch_bounds__(kChainThreads) k_ion_chain(
   const uint32_t turn = (uint32_t)(*d_turn);
   double* sb = dsm;                                 // 6 x M
   double* scl = dsm + (sb_ok ? 6 * (size_t)M : 0);  // P x 4 x smem_cap
-  if (tid == 0) {
-    // MPGetBeamInfo: bunchSizeXMax / YMax over all bunches (MPBeam.cpp:2175-2186)
-    double mx = mom[0].rms_x, my = mom[0].rms_y;
-    for (int j = 1; j < M; ++j) {
-      if (mom[j].rms_x > mx) mx = mom[j].rms_x;
-      if (mom[j].rms_y > my) my = mom[j].rms_y;
+  {
+    // MPGetBeamInfo: bunchSizeXMax / YMax over all bunches (MPBeam.cpp:2175-2186);
+    // the maximum does not depend on the order of comparison
+    double mx = -INFINITY, my = -INFINITY;
+    for (int j = tid; j < M; j += kChainThreads) {
+      mx = fmax(mx, mom[j].rms_x);
+      my = fmax(my, mom[j].rms_y);
     }
+    double mn = 0;
+    block_minmax<kChainThreads>(mn, mx, smem);
+    mn = 0;
+    block_minmax<kChainThreads>(mn, my, smem);
+    if (tid == 0) {
     double lbx = cp.loss_boundary * mx, lby = cp.loss_boundary * my;
     s_bx = cs.aperture_x > lbx ? lbx : cs.aperture_x;
     s_by = cs.aperture_y > lby ? lby : cs.aperture_y;
     s_abort = 0;
+    }
   }
   if (sb_ok)
     for (int j = tid; j < M; j += kChainThreads) {
@@ -392,13 +400,13 @@ __global__ void __launch_bounds__(kChainThreads) k_ion_chain(
       sb[5 * M + j] = (double)bunch[j].gap;
     }
   // per species: where the cloud lives for this walk
-  double* AX[CG_MAX_SPECIES];
-  double* AY[CG_MAX_SPECIES];
-  double* AVX[CG_MAX_SPECIES];
-  double* AVY[CG_MAX_SPECIES];
-  int cap[CG_MAX_SPECIES];
-  bool in_smem[CG_MAX_SPECIES];
-  for (int p = 0; p < P; ++p) {
+  double* AX[PMAX];
+  double* AY[PMAX];
+  double* AVX[PMAX];
+  double* AVY[PMAX];
+  int cap[PMAX];
+  bool in_smem[PMAX];
+  for (int p = 0; p < P && p < PMAX; ++p) {
     CloudDev cd = clouds[p];
     int n0 = cst[p].n;
     in_smem[p] = (long long)n0 + (long long)M * cp.macro_per_ip <= smem_cap;
@@ -426,14 +434,14 @@ __global__ void __launch_bounds__(kChainThreads) k_ion_chain(
   __syncthreads();
   const double bx = s_bx, by = s_by;
   const uint32_t k0 = (uint32_t)cp.seed, k1 = (uint32_t)(cp.seed >> 32) ^ kStreamIonBirth;
-  CloudState stv[CG_MAX_SPECIES];
-  for (int p = 0; p < P; ++p) stv[p] = cst[p];
+  CloudState stv[PMAX];
+  for (int p = 0; p < P && p < PMAX; ++p) stv[p] = cst[p];
 
   for (int j = 0; j < M; ++j) {
     double mx, my, sx, sy, ne;
     int gap;
     chain_bunch_load(bunch, mom, j, sb, M, sb_ok != 0, mx, my, sx, sy, ne, gap);
-    for (int p = 0; p < P; ++p) {
+    for (int p = 0; p < P && p < PMAX; ++p) {
       CloudState& st = stv[p];
       double* X = AX[p];
       double* Y = AY[p];
@@ -561,7 +569,7 @@ __global__ void __launch_bounds__(kChainThreads) k_ion_chain(
     }
   }
   // write the clouds back
-  for (int p = 0; p < P; ++p) {
+  for (int p = 0; p < P && p < PMAX; ++p) {
     if (in_smem[p]) {
       CloudDev cd = clouds[p];
       for (int i = tid; i < stv[p].n; i += kChainThreads) {
@@ -598,7 +606,11 @@ cudaError_t prepare_ion_chain(Handle& h) {
   int sb_ok = 0, cap = 0;
   size_t bytes = 0;
   chain_smem_plan(h, &sb_ok, &cap, &bytes);
-  return cudaFuncSetAttribute(k_ion_chain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaError_t e = cudaFuncSetAttribute(k_ion_chain<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)bytes);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_ion_chain<CG_MAX_SPECIES>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
 cudaError_t launch_ion_chain(Handle& h, int k) {
@@ -612,7 +624,8 @@ cudaError_t launch_ion_chain(Handle& h, int k) {
   int sb_ok = 0, cap = 0;
   size_t bytes = 0;
   chain_smem_plan(h, &sb_ok, &cap, &bytes);
-  k_ion_chain<<<1, kChainThreads, bytes, h.stream>>>(
+  auto kern = h.P == 1 ? k_ion_chain<1> : k_ion_chain<CG_MAX_SPECIES>;
+  kern<<<1, kChainThreads, bytes, h.stream>>>(
       h.chain, cs, h.d.bunch, h.d.mom, h.d.clouds + (size_t)k * h.P, h.d.cloud_state + (size_t)k * h.P,
       h.d.rec + (size_t)k * h.M * h.P, h.d.status, h.d.turn, k, cap, sb_ok);
   return cudaGetLastError();

@@ -42,12 +42,32 @@ def test_fast_ion_turns():
             assert np.allclose(ig[0], io[0], rtol=1e-9, atol=1e-9 * np.max(np.abs(io[0])))
 
 
-def test_batched_train_turns():
+def test_batched_train_turns_without_ions():
+    # ragged 900-bunch train, 50 sections, LR wake + FIR + synchrotron radiation
+    wl = small("batched_uneven", 0.002, flag_beam_ion=0)
+    g, o = pair(wl, particles(wl, seed=8, spread=3.0))
+    g.Run(0, 3)
+    o.Run(0, 3)
+    assert coord_err(g, o, wl).max() <= 1e-9
+
+
+def test_batched_train_turns_with_ions_statistics():
+    # with the ion chain on, a 1e-15 change of one coordinate grows to 1e-5
+    # in two turns in the oracle itself (the ion motion over 900 passages is
+    # chaotic), so the comparison is on bunch moments
     wl = small("batched_uneven", 0.002, bunch_current=TRAPPED)
     g, o = pair(wl, particles(wl, seed=8, spread=3.0))
     g.Run(0, 2)
     o.Run(0, 2)
-    assert coord_err(g, o, wl).max() <= 1e-9
+    g.MPBeamRMSCal(0)
+    o.MPBeamRMSCal(0)
+    mg, mo = g.moments(), o.moments()
+    for f in ("rms_x", "rms_y", "bunch_length", "energy_spread"):
+        a = np.array([getattr(m, f) for m in mg])
+        b = np.array([getattr(m, f) for m in mo])
+        assert np.max(np.abs(a / b - 1)) < 1e-3, f
+    ex = np.array([m.emit[0] for m in mg]) / np.array([m.emit[0] for m in mo])
+    assert np.max(np.abs(ex - 1)) < 1e-3
 
 
 def test_graph_equals_staged_calls():
