@@ -8,6 +8,7 @@
 // two bunches.  Bunches of uneven size (ragged trains) are just different
 // tile counts; fill-pattern gaps hold no tiles at all.
 #include <cuda_runtime.h>
+#include <algorithm>
 #include "kernels.cuh"
 
 namespace cg {
@@ -360,7 +361,7 @@ template <int PMAX>
 __global__ void __launch_bounds__(kChainThreads) k_ion_chain(
     ChainParams cp, ChainSection cs, const BunchDev* __restrict__ bunch,
     const BunchMomDev* __restrict__ mom, CloudDev* clouds, CloudState* cst, CloudRec* rec,
-    int* status, const int* __restrict__ d_turn, int k, int smem_cap, int sb_ok) {
+    int* status, const int* __restrict__ d_turn, int k, int smem_cap, int sb_ok, int births_ok) {
   extern __shared__ double dsm[];
   __shared__ double smem[4 * 32];
   __shared__ int smem_i[32];
@@ -370,7 +371,8 @@ __global__ void __launch_bounds__(kChainThreads) k_ion_chain(
   const int M = cp.n_bunches, P = cp.n_species;
   const uint32_t turn = (uint32_t)(*d_turn);
   double* sb = dsm;                                 // 6 x M
-  double* scl = dsm + (sb_ok ? 6 * (size_t)M : 0);  // P x 4 x smem_cap
+  double* scl = dsm + (sb_ok ? 6 * (size_t)M : 0) +                  // P x 4 x smem_cap
+                (births_ok ? 2 * (size_t)M * cp.macro_per_ip : 0);  // after the births
   {
     // MPGetBeamInfo: bunchSizeXMax / YMax over all bunches (MPBeam.cpp:2175-2186);
     // the maximum does not depend on the order of comparison
@@ -436,6 +438,157 @@ __global__ void __launch_bounds__(kChainThreads) k_ion_chain(
   const uint32_t k0 = (uint32_t)cp.seed, k1 = (uint32_t)(cp.seed >> 32) ^ kStreamIonBirth;
   CloudState stv[PMAX];
   for (int p = 0; p < P && p < PMAX; ++p) stv[p] = cst[p];
+
+  // Single-species walk with precomputed births: the birth positions of bunch
+  // j depend only on its moments and Philox counters, so all of them are
+  // drawn in parallel first (attempts in order per bunch, exactly as the
+  // sequential draw).  A cloud that stays within 128 ions is then walked by
+  // one warp: shuffle reductions, ballot compaction, no block barriers, and up
+  // to four ions per lane in flight.
+  if (PMAX == 1 && births_ok && in_smem[0]) {
+    double* BXn = dsm + (sb_ok ? 6 * (size_t)M : 0);
+    double* BYn = BXn + (size_t)M * cp.macro_per_ip;
+    for (int j = tid; j < M; j += kChainThreads) {
+      double mx, my, sx, sy, ne;
+      int gap;
+      chain_bunch_load(bunch, mom, j, sb, M, sb_ok != 0, mx, my, sx, sy, ne, gap);
+      int got = 0;
+      for (uint32_t a = 0; got < cp.macro_per_ip; ++a) {
+        if (a >= (1u << 20)) {
+          atomicOr(status, kStatusIonBirth);
+          s_abort = 1;
+          break;
+        }
+        u32x4 ctr = {{a, (uint32_t)j, turn, (uint32_t)(k * CG_MAX_SPECIES)}};
+        double g0, g1;
+        normal2(philox4x32_10(ctr, k0, k1), &g0, &g1);
+        double tx = mx + sx * g0, ty = my + sy * g1;
+        double ax = (tx - mx) / sx, ay = (ty - my) / sy;
+        if (ax * ax + ay * ay > 4.E0) continue;
+        BXn[(size_t)j * cp.macro_per_ip + got] = tx;
+        BYn[(size_t)j * cp.macro_per_ip + got] = ty;
+        got++;
+      }
+    }
+    __syncthreads();
+    if (s_abort) return;
+    const long long worst = (long long)stv[0].n + (long long)M * cp.macro_per_ip;
+    if (worst <= 128) {
+      if (tid >= 32) return;
+      const int lane = tid;
+      CloudState st = stv[0];
+      double* X = AX[0];
+      double* Y = AY[0];
+      double* VX = AVX[0];
+      double* VY = AVY[0];
+      for (int j = 0; j < M; ++j) {
+        double mx, my, sx, sy, ne;
+        int gap;
+        chain_bunch_load(bunch, mom, j, sb, M, sb_ok != 0, mx, my, sx, sy, ne, gap);
+        double press_p = cp.gas_percent[0] * cs.pressure;
+        double line_density = cp.cross_section[0] * press_p / cs.temperature / kBoltzmann * ne;
+        double ion_number = line_density * cs.length;
+        st.macro_charge = ion_number / cp.macro_per_ip;
+        if (lane < cp.macro_per_ip) {
+          X[st.n + lane] = BXn[(size_t)j * cp.macro_per_ip + lane];
+          Y[st.n + lane] = BYn[(size_t)j * cp.macro_per_ip + lane];
+          VX[st.n + lane] = 0.0;
+          VY[st.n + lane] = 0.0;
+        }
+        st.n += cp.macro_per_ip;
+        __syncwarp();
+        if (st.n > cp.max_ions) {
+          if (lane == 0) atomicOr(status, kStatusIonOverflow);
+          return;
+        }
+        // LIP::IonRMSCal(k, p): count 1 keeps the stale centroid (LIP.cpp:1125-1129)
+        if (st.n == 1) {
+          st.rms_x = fabs(X[0]);
+          st.rms_y = fabs(Y[0]);
+        } else {
+          double s2[2] = {0.0, 0.0};
+          for (int i = lane; i < st.n; i += 32) {
+            s2[0] += X[i];
+            s2[1] += Y[i];
+          }
+          warp_sum<2>(s2);
+          st.aver_x = s2[0] / st.n;
+          st.aver_y = s2[1] / st.n;
+          double q[2] = {0.0, 0.0};
+          for (int i = lane; i < st.n; i += 32) {
+            double dx = X[i] - st.aver_x, dy = Y[i] - st.aver_y;
+            q[0] = fma(dx, dx, q[0]);
+            q[1] = fma(dy, dy, q[1]);
+          }
+          warp_sum<2>(q);
+          st.rms_x = sqrt(q[0] / st.n);
+          st.rms_y = sqrt(q[1] / st.n);
+        }
+        if (lane == 0) {
+          CloudRec r;
+          r.coeff = 2.0 * (st.macro_charge * st.n) * kElecClassicRadius / cp.r_gamma;
+          r.rms_x = st.rms_x;
+          r.rms_y = st.rms_y;
+          r.aver_x = st.aver_x;
+          r.aver_y = st.aver_y;
+          r.count = st.n;
+          rec[j] = r;
+        }
+        const double coeffI = 2.0 * ne * kElecClassicRadius * kElectronMassEV / kIonMassEV /
+                              cp.mass_number[0] * kCLight;
+        double px[4], py[4], pvx[4], pvy[4];
+        bool keep[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          int i = lane + 32 * q;
+          keep[q] = false;
+          px[q] = py[q] = pvx[q] = pvy[q] = 0.0;
+          if (i < st.n) {
+            double x = X[i], y = Y[i], vx = VX[i], vy = VY[i];
+            double fx, fy;
+            gaussian_field<true>(x - mx, y - my, sx, sy, &fx, &fy);
+            vx += coeffI * fx;
+            vy += coeffI * fy;
+            x += vx * cp.circ_ring / cp.harmonics * gap / kCLight;
+            y += vy * cp.circ_ring / cp.harmonics * gap / kCLight;
+            keep[q] = !(fabs(x) > bx || fabs(y) > by);
+            px[q] = x;
+            py[q] = y;
+            pvx[q] = vx;
+            pvy[q] = vy;
+          }
+        }
+        __syncwarp();
+        int base = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          unsigned bal = __ballot_sync(FULL_MASK, keep[q]);
+          int pos = base + __popc(bal & ((1u << lane) - 1u));
+          if (keep[q]) {
+            X[pos] = px[q];
+            Y[pos] = py[q];
+            VX[pos] = pvx[q];
+            VY[pos] = pvy[q];
+          }
+          base += __popc(bal);
+        }
+        st.n = base;
+        __syncwarp();
+      }
+      CloudDev cd = clouds[0];
+      for (int i = lane; i < st.n; i += 32) {
+        cd.x[0][i] = X[i];
+        cd.y[0][i] = Y[i];
+        cd.vx[0][i] = VX[i];
+        cd.vy[0][i] = VY[i];
+      }
+      if (lane == 0) {
+        st.cur = 0;
+        cst[0] = st;
+      }
+      return;
+    }
+  }
 
   for (int j = 0; j < M; ++j) {
     double mx, my, sx, sy, ne;
@@ -589,23 +742,26 @@ __global__ void __launch_bounds__(kChainThreads) k_ion_chain(
 // Shared memory of the chain kernel: per-bunch inputs (6 doubles per bunch)
 // when at most 2048 bunches, plus as many ions per species as fit in the
 // remaining opt-in shared memory.
-void chain_smem_plan(const Handle& h, int* sb_ok, int* cap, size_t* bytes) {
+void chain_smem_plan(const Handle& h, int* sb_ok, int* births_ok, int* cap, size_t* bytes) {
   int dev = 0, optin = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   size_t budget = (size_t)optin - 4096;  // static shared memory of the kernel
   size_t sb = h.M <= 2048 ? 6 * sizeof(double) * (size_t)h.M : 0;
   *sb_ok = sb > 0;
-  size_t rest = budget > sb ? budget - sb : 0;
+  size_t br = 2 * sizeof(double) * (size_t)h.M * (size_t)std::max(1, h.cfg.ion.macro_ions_per_ip);
+  *births_ok = (h.P == 1 && sb + br <= budget / 2) ? 1 : 0;
+  if (!*births_ok) br = 0;
+  size_t rest = budget > sb + br ? budget - sb - br : 0;
   *cap = (int)(rest / (4 * sizeof(double) * (size_t)h.P));
-  *bytes = sb + (size_t)(*cap) * 4 * sizeof(double) * h.P;
+  *bytes = sb + br + (size_t)(*cap) * 4 * sizeof(double) * h.P;
 }
 
 // Opt-in shared memory of the chain kernel (set outside any graph capture).
 cudaError_t prepare_ion_chain(Handle& h) {
-  int sb_ok = 0, cap = 0;
+  int sb_ok = 0, births_ok = 0, cap = 0;
   size_t bytes = 0;
-  chain_smem_plan(h, &sb_ok, &cap, &bytes);
+  chain_smem_plan(h, &sb_ok, &births_ok, &cap, &bytes);
   cudaError_t e = cudaFuncSetAttribute(k_ion_chain<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)bytes);
   if (e != cudaSuccess) return e;
@@ -621,13 +777,13 @@ cudaError_t launch_ion_chain(Handle& h, int k) {
   cs.length = s.length;
   cs.aperture_x = s.aperture_x;
   cs.aperture_y = s.aperture_y;
-  int sb_ok = 0, cap = 0;
+  int sb_ok = 0, births_ok = 0, cap = 0;
   size_t bytes = 0;
-  chain_smem_plan(h, &sb_ok, &cap, &bytes);
+  chain_smem_plan(h, &sb_ok, &births_ok, &cap, &bytes);
   auto kern = h.P == 1 ? k_ion_chain<1> : k_ion_chain<CG_MAX_SPECIES>;
   kern<<<1, kChainThreads, bytes, h.stream>>>(
       h.chain, cs, h.d.bunch, h.d.mom, h.d.clouds + (size_t)k * h.P, h.d.cloud_state + (size_t)k * h.P,
-      h.d.rec + (size_t)k * h.M * h.P, h.d.status, h.d.turn, k, cap, sb_ok);
+      h.d.rec + (size_t)k * h.M * h.P, h.d.status, h.d.turn, k, cap, sb_ok, births_ok);
   return cudaGetLastError();
 }
 
