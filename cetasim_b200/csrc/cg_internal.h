@@ -10,7 +10,7 @@
 namespace cg {
 
 constexpr int kTile = 256;            // particles per tile == threads per CTA
-constexpr int kChainThreads = 128;    // ion-chain CTA size
+constexpr int kChainThreads = 256;    // ion-chain CTA size (two lanes per ion)
 
 struct BunchDev {
   int n, tile_off, n_tiles, harm, gap;
@@ -60,6 +60,7 @@ struct DeviceBufs {
   CloudDev* clouds = nullptr;      // K x P (device array of buffer pointers)
   CloudState* cloud_state = nullptr;  // K x P
   CloudRec* rec = nullptr;         // K x M x P
+  FieldPrep* prep = nullptr;       // K x M x P: field constants of each record
   double* ion_totals = nullptr;    // K (charge), used by cg_ion_totals
   // long-range wake
   double* lr_tab = nullptr;        // 3 x np

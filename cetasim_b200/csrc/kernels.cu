@@ -265,20 +265,23 @@ __global__ void __launch_bounds__(kTile) k_ion_kick(double* __restrict__ c, int6
                                                     const uint8_t* __restrict__ surv,
                                                     const int* __restrict__ tile_bunch,
                                                     const BunchDev* __restrict__ bunch,
-                                                    const CloudRec* __restrict__ rec, int P) {
+                                                    const CloudRec* __restrict__ rec,
+                                                    const FieldPrep* __restrict__ prep, int P) {
   TileIdx t = tile_index(tile_bunch, bunch);
   if (!t.valid || surv[t.g] != kAlive) return;
   const CloudRec* rb = rec + (size_t)t.b * P;
+  const FieldPrep* pb = prep + (size_t)t.b * P;
   double x = c[0 * npad + t.g], y = c[2 * npad + t.g];
   double dpx, dpy;
-  ion_kick_particle(rb, P, x, y, &dpx, &dpy);
+  ion_kick_particle_prep(rb, pb, P, x, y, &dpx, &dpy);
   c[1 * npad + t.g] += dpx;
   c[3 * npad + t.g] += dpy;
 }
 
 cudaError_t launch_ion_kick(Handle& h, int k) {
   k_ion_kick<<<h.n_tiles, kTile, 0, h.stream>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch,
-                                                h.d.bunch, h.d.rec + (size_t)k * h.M * h.P, h.P);
+                                                h.d.bunch, h.d.rec + (size_t)k * h.M * h.P,
+                                                h.d.prep + (size_t)k * h.M * h.P, h.P);
   return cudaGetLastError();
 }
 
@@ -361,7 +364,8 @@ template <int PMAX>
 __global__ void __launch_bounds__(kChainThreads) k_ion_chain(
     ChainParams cp, ChainSection cs, const BunchDev* __restrict__ bunch,
     const BunchMomDev* __restrict__ mom, CloudDev* clouds, CloudState* cst, CloudRec* rec,
-    int* status, const int* __restrict__ d_turn, int k, int smem_cap, int sb_ok, int births_ok) {
+    FieldPrep* prep, int* status, const int* __restrict__ d_turn, int k, int smem_cap, int sb_ok,
+    int births_ok) {
   extern __shared__ double dsm[];
   __shared__ double smem[4 * 32];
   __shared__ int smem_i[32];
@@ -472,122 +476,6 @@ __global__ void __launch_bounds__(kChainThreads) k_ion_chain(
     }
     __syncthreads();
     if (s_abort) return;
-    const long long worst = (long long)stv[0].n + (long long)M * cp.macro_per_ip;
-    if (worst <= 128) {
-      if (tid >= 32) return;
-      const int lane = tid;
-      CloudState st = stv[0];
-      double* X = AX[0];
-      double* Y = AY[0];
-      double* VX = AVX[0];
-      double* VY = AVY[0];
-      for (int j = 0; j < M; ++j) {
-        double mx, my, sx, sy, ne;
-        int gap;
-        chain_bunch_load(bunch, mom, j, sb, M, sb_ok != 0, mx, my, sx, sy, ne, gap);
-        double press_p = cp.gas_percent[0] * cs.pressure;
-        double line_density = cp.cross_section[0] * press_p / cs.temperature / kBoltzmann * ne;
-        double ion_number = line_density * cs.length;
-        st.macro_charge = ion_number / cp.macro_per_ip;
-        if (lane < cp.macro_per_ip) {
-          X[st.n + lane] = BXn[(size_t)j * cp.macro_per_ip + lane];
-          Y[st.n + lane] = BYn[(size_t)j * cp.macro_per_ip + lane];
-          VX[st.n + lane] = 0.0;
-          VY[st.n + lane] = 0.0;
-        }
-        st.n += cp.macro_per_ip;
-        __syncwarp();
-        if (st.n > cp.max_ions) {
-          if (lane == 0) atomicOr(status, kStatusIonOverflow);
-          return;
-        }
-        // LIP::IonRMSCal(k, p): count 1 keeps the stale centroid (LIP.cpp:1125-1129)
-        if (st.n == 1) {
-          st.rms_x = fabs(X[0]);
-          st.rms_y = fabs(Y[0]);
-        } else {
-          double s2[2] = {0.0, 0.0};
-          for (int i = lane; i < st.n; i += 32) {
-            s2[0] += X[i];
-            s2[1] += Y[i];
-          }
-          warp_sum<2>(s2);
-          st.aver_x = s2[0] / st.n;
-          st.aver_y = s2[1] / st.n;
-          double q[2] = {0.0, 0.0};
-          for (int i = lane; i < st.n; i += 32) {
-            double dx = X[i] - st.aver_x, dy = Y[i] - st.aver_y;
-            q[0] = fma(dx, dx, q[0]);
-            q[1] = fma(dy, dy, q[1]);
-          }
-          warp_sum<2>(q);
-          st.rms_x = sqrt(q[0] / st.n);
-          st.rms_y = sqrt(q[1] / st.n);
-        }
-        if (lane == 0) {
-          CloudRec r;
-          r.coeff = 2.0 * (st.macro_charge * st.n) * kElecClassicRadius / cp.r_gamma;
-          r.rms_x = st.rms_x;
-          r.rms_y = st.rms_y;
-          r.aver_x = st.aver_x;
-          r.aver_y = st.aver_y;
-          r.count = st.n;
-          rec[j] = r;
-        }
-        const double coeffI = 2.0 * ne * kElecClassicRadius * kElectronMassEV / kIonMassEV /
-                              cp.mass_number[0] * kCLight;
-        double px[4], py[4], pvx[4], pvy[4];
-        bool keep[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          int i = lane + 32 * q;
-          keep[q] = false;
-          px[q] = py[q] = pvx[q] = pvy[q] = 0.0;
-          if (i < st.n) {
-            double x = X[i], y = Y[i], vx = VX[i], vy = VY[i];
-            double fx, fy;
-            gaussian_field<true>(x - mx, y - my, sx, sy, &fx, &fy);
-            vx += coeffI * fx;
-            vy += coeffI * fy;
-            x += vx * cp.circ_ring / cp.harmonics * gap / kCLight;
-            y += vy * cp.circ_ring / cp.harmonics * gap / kCLight;
-            keep[q] = !(fabs(x) > bx || fabs(y) > by);
-            px[q] = x;
-            py[q] = y;
-            pvx[q] = vx;
-            pvy[q] = vy;
-          }
-        }
-        __syncwarp();
-        int base = 0;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          unsigned bal = __ballot_sync(FULL_MASK, keep[q]);
-          int pos = base + __popc(bal & ((1u << lane) - 1u));
-          if (keep[q]) {
-            X[pos] = px[q];
-            Y[pos] = py[q];
-            VX[pos] = pvx[q];
-            VY[pos] = pvy[q];
-          }
-          base += __popc(bal);
-        }
-        st.n = base;
-        __syncwarp();
-      }
-      CloudDev cd = clouds[0];
-      for (int i = lane; i < st.n; i += 32) {
-        cd.x[0][i] = X[i];
-        cd.y[0][i] = Y[i];
-        cd.vx[0][i] = VX[i];
-        cd.vy[0][i] = VY[i];
-      }
-      if (lane == 0) {
-        st.cur = 0;
-        cst[0] = st;
-      }
-      return;
-    }
   }
 
   for (int j = 0; j < M; ++j) {
@@ -684,28 +572,38 @@ __global__ void __launch_bounds__(kChainThreads) k_ion_chain(
         r.aver_y = st.aver_y;
         r.count = st.n;
         rec[(size_t)j * P + p] = r;
+        prep[(size_t)j * P + p] = field_prep(st.rms_x, st.rms_y);
       }
       // ion side: v += F, x += v C/h gap/c, then stable in-place removal of
       // ions beyond the loss boundary (writes never pass the read position)
       const double coeffI = 2.0 * ne * kElecClassicRadius * kElectronMassEV / kIonMassEV /
                             cp.mass_number[p] * kCLight;
+      // two lanes per ion: the even lane evaluates w(z1), the odd lane w(z2)
+      const FieldPrep fp = field_prep(sx, sy);
+      const int half = tid & 1;
       int out_base = 0;
-      for (int c0 = 0; c0 < st.n; c0 += kChainThreads) {
-        int i = c0 + tid;
+      for (int c0 = 0; c0 < st.n; c0 += kChainThreads / 2) {
+        int i = c0 + (tid >> 1);
         bool keep = false;
         double x = 0, y = 0, vx = 0, vy = 0;
+        double z1r = 0, z1i = 0, z2r = 0, z2i = 0;
         if (i < st.n) {
           x = X[i];
           y = Y[i];
           vx = VX[i];
           vy = VY[i];
+          field_zargs(fp, x - mx, y - my, &z1r, &z1i, &z2r, &z2i);
+        }
+        cplx wm = half ? w_quadrant1_lowlat(z2r, z2i) : w_quadrant1_lowlat(z1r, z1i);
+        cplx wo = {__shfl_xor_sync(FULL_MASK, wm.re, 1), __shfl_xor_sync(FULL_MASK, wm.im, 1)};
+        if (i < st.n) {
           double fx, fy;
-          gaussian_field<true>(x - mx, y - my, sx, sy, &fx, &fy);
+          field_finish(fp, x - mx, y - my, half ? wo : wm, half ? wm : wo, &fx, &fy);
           vx += coeffI * fx;
           vy += coeffI * fy;
           x += vx * cp.circ_ring / cp.harmonics * gap / kCLight;
           y += vy * cp.circ_ring / cp.harmonics * gap / kCLight;
-          keep = !(fabs(x) > bx || fabs(y) > by);
+          keep = !(fabs(x) > bx || fabs(y) > by) && half == 0;
         }
         int tot;
         int pos = block_excl_scan(keep ? 1 : 0, smem_i, &tot);  // syncs: all reads done
@@ -783,7 +681,8 @@ cudaError_t launch_ion_chain(Handle& h, int k) {
   auto kern = h.P == 1 ? k_ion_chain<1> : k_ion_chain<CG_MAX_SPECIES>;
   kern<<<1, kChainThreads, bytes, h.stream>>>(
       h.chain, cs, h.d.bunch, h.d.mom, h.d.clouds + (size_t)k * h.P, h.d.cloud_state + (size_t)k * h.P,
-      h.d.rec + (size_t)k * h.M * h.P, h.d.status, h.d.turn, k, cap, sb_ok, births_ok);
+      h.d.rec + (size_t)k * h.M * h.P, h.d.prep + (size_t)k * h.M * h.P, h.d.status, h.d.turn, k,
+      cap, sb_ok, births_ok);
   return cudaGetLastError();
 }
 

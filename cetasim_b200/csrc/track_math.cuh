@@ -255,4 +255,18 @@ CG_HD void ion_kick_particle(const CloudRec* rec, int n_species, double x, doubl
   *dpy = fy;
 }
 
+// The same with the per-record field constants prepared by the ion chain.
+CG_HD void ion_kick_particle_prep(const CloudRec* rec, const FieldPrep* prep, int n_species,
+                                  double x, double y, double* dpx, double* dpy) {
+  double fx = 0, fy = 0;
+  for (int p = 0; p < n_species; ++p) {
+    double ex, ey;
+    gaussian_field_prep<false>(prep[p], x - rec[p].aver_x, y - rec[p].aver_y, &ex, &ey);
+    fx = fma(rec[p].coeff, ex, fx);
+    fy = fma(rec[p].coeff, ey, fy);
+  }
+  *dpx = fx;
+  *dpy = fy;
+}
+
 }  // namespace cg
