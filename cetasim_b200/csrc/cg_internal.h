@@ -60,7 +60,6 @@ struct DeviceBufs {
   CloudDev* clouds = nullptr;      // K x P (device array of buffer pointers)
   CloudState* cloud_state = nullptr;  // K x P
   CloudRec* rec = nullptr;         // K x M x P
-  FieldPrep* prep = nullptr;       // K x M x P: field constants of each record
   double* ion_totals = nullptr;    // K (charge), used by cg_ion_totals
   // long-range wake
   double* lr_tab = nullptr;        // 3 x np

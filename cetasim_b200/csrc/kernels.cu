@@ -265,23 +265,25 @@ __global__ void __launch_bounds__(kTile) k_ion_kick(double* __restrict__ c, int6
                                                     const uint8_t* __restrict__ surv,
                                                     const int* __restrict__ tile_bunch,
                                                     const BunchDev* __restrict__ bunch,
-                                                    const CloudRec* __restrict__ rec,
-                                                    const FieldPrep* __restrict__ prep, int P) {
+                                                    const CloudRec* __restrict__ rec, int P) {
+  // the field constants of the bunch's records, once per CTA (a tile holds
+  // particles of one bunch)
+  __shared__ FieldPrep s_prep[CG_MAX_SPECIES];
   TileIdx t = tile_index(tile_bunch, bunch);
-  if (!t.valid || surv[t.g] != kAlive) return;
   const CloudRec* rb = rec + (size_t)t.b * P;
-  const FieldPrep* pb = prep + (size_t)t.b * P;
+  if ((int)threadIdx.x < P) s_prep[threadIdx.x] = field_prep(rb[threadIdx.x].rms_x, rb[threadIdx.x].rms_y);
+  __syncthreads();
+  if (!t.valid || surv[t.g] != kAlive) return;
   double x = c[0 * npad + t.g], y = c[2 * npad + t.g];
   double dpx, dpy;
-  ion_kick_particle_prep(rb, pb, P, x, y, &dpx, &dpy);
+  ion_kick_particle_prep(rb, s_prep, P, x, y, &dpx, &dpy);
   c[1 * npad + t.g] += dpx;
   c[3 * npad + t.g] += dpy;
 }
 
 cudaError_t launch_ion_kick(Handle& h, int k) {
   k_ion_kick<<<h.n_tiles, kTile, 0, h.stream>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch,
-                                                h.d.bunch, h.d.rec + (size_t)k * h.M * h.P,
-                                                h.d.prep + (size_t)k * h.M * h.P, h.P);
+                                                h.d.bunch, h.d.rec + (size_t)k * h.M * h.P, h.P);
   return cudaGetLastError();
 }
 
@@ -364,7 +366,7 @@ template <int PMAX>
 __global__ void __launch_bounds__(kChainThreads) k_ion_chain(
     ChainParams cp, ChainSection cs, const BunchDev* __restrict__ bunch,
     const BunchMomDev* __restrict__ mom, CloudDev* clouds, CloudState* cst, CloudRec* rec,
-    FieldPrep* prep, int* status, const int* __restrict__ d_turn, int k, int smem_cap, int sb_ok,
+    int* status, const int* __restrict__ d_turn, int k, int smem_cap, int sb_ok,
     int births_ok) {
   extern __shared__ double dsm[];
   __shared__ double smem[4 * 32];
@@ -572,7 +574,6 @@ __global__ void __launch_bounds__(kChainThreads) k_ion_chain(
         r.aver_y = st.aver_y;
         r.count = st.n;
         rec[(size_t)j * P + p] = r;
-        prep[(size_t)j * P + p] = field_prep(st.rms_x, st.rms_y);
       }
       // ion side: v += F, x += v C/h gap/c, then stable in-place removal of
       // ions beyond the loss boundary (writes never pass the read position)
@@ -637,34 +638,302 @@ __global__ void __launch_bounds__(kChainThreads) k_ion_chain(
   }
 }
 
-// Shared memory of the chain kernel: per-bunch inputs (6 doubles per bunch)
-// when at most 2048 bunches, plus as many ions per species as fit in the
-// remaining opt-in shared memory.
-void chain_smem_plan(const Handle& h, int* sb_ok, int* births_ok, int* cap, size_t* bytes) {
+// Block-wide exclusive scan of `keep` fused with the sums of four values over
+// the kept entries (fixed tree: deterministic).  Two barriers.
+__device__ __forceinline__ int scan_keep_sums(bool keep, const double v[4], int* s_cnt,
+                                              double* s_sum, int* total, double tot[4]) {
+  constexpr int NW = kChainThreads / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned bal = __ballot_sync(FULL_MASK, keep);
+  int pre = __popc(bal & ((1u << lane) - 1u));
+  double w[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) w[q] = keep ? v[q] : 0.0;
+  warp_sum<4>(w);
+  if (lane == 0) {
+    s_cnt[warp] = __popc(bal);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) s_sum[q * NW + warp] = w[q];
+  }
+  __syncthreads();
+  int wpre = 0, t = 0;
+#pragma unroll
+  for (int u = 0; u < NW; ++u) {
+    int c = s_cnt[u];
+    wpre += (u < warp) ? c : 0;
+    t += c;
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    double acc = 0.0;
+#pragma unroll
+    for (int u = 0; u < NW; ++u) acc += s_sum[q * NW + u];
+    tot[q] = acc;
+  }
+  __syncthreads();
+  *total = t;
+  return wpre + pre;
+}
+
+// Single-species ion chain (the common case).  Everything that does not depend
+// on the cloud is computed for all bunches before the walk and kept in shared
+// memory: the birth positions (Philox attempts in order per bunch, as the
+// sequential draw), the bunch centroid/size/charge/gap and the prepared field
+// constants.  The walk keeps the cloud sums (sum x, y, x^2, y^2) up to date
+// from the compaction pass, so a bunch step is: append births, cloud rms from
+// the sums, record, one field-kick/drift/compaction pass with two lanes per
+// ion.  Three block barriers per bunch.
+__global__ void __launch_bounds__(kChainThreads) k_ion_chain1(
+    ChainParams cp, ChainSection cs, const BunchDev* __restrict__ bunch,
+    const BunchMomDev* __restrict__ mom, CloudDev* clouds, CloudState* cst, CloudRec* rec,
+    int* status, const int* __restrict__ d_turn, int k, int smem_cap) {
+  extern __shared__ double dsm[];
+  __shared__ double smem[4 * 32];
+  __shared__ int s_cnt[kChainThreads / 32];
+  __shared__ double s_sum[4 * (kChainThreads / 32)];
+  __shared__ double s_bx, s_by;
+  __shared__ int s_abort;
+  const int tid = threadIdx.x;
+  const int M = cp.n_bunches, NM = cp.macro_per_ip;
+  const uint32_t turn = (uint32_t)(*d_turn);
+  // shared layout: bunch data 6M | births 2 M NM | field constants | cloud 4 cap
+  double* sb = dsm;
+  double* BXn = sb + 6 * (size_t)M;
+  double* BYn = BXn + (size_t)M * NM;
+  FieldPrep* FP = reinterpret_cast<FieldPrep*>(BYn + (size_t)M * NM);
+  double* scl = reinterpret_cast<double*>(FP + M);
+  {
+    double mx = -INFINITY, my = -INFINITY;
+    for (int j = tid; j < M; j += kChainThreads) {
+      mx = fmax(mx, mom[j].rms_x);
+      my = fmax(my, mom[j].rms_y);
+    }
+    double mn = 0;
+    block_minmax<kChainThreads>(mn, mx, smem);
+    mn = 0;
+    block_minmax<kChainThreads>(mn, my, smem);
+    if (tid == 0) {
+      double lbx = cp.loss_boundary * mx, lby = cp.loss_boundary * my;
+      s_bx = cs.aperture_x > lbx ? lbx : cs.aperture_x;
+      s_by = cs.aperture_y > lby ? lby : cs.aperture_y;
+      s_abort = 0;
+    }
+  }
+  const uint32_t k0 = (uint32_t)cp.seed, k1 = (uint32_t)(cp.seed >> 32) ^ kStreamIonBirth;
+  for (int j = tid; j < M; j += kChainThreads) {
+    const double mx = mom[j].mean[0], my = mom[j].mean[2];
+    const double sx = mom[j].rms_x, sy = mom[j].rms_y;
+    sb[j] = mx;
+    sb[M + j] = my;
+    sb[2 * M + j] = sx;
+    sb[3 * M + j] = sy;
+    sb[4 * M + j] = bunch[j].ne;
+    sb[5 * M + j] = (double)bunch[j].gap;
+    FP[j] = field_prep(sx, sy);
+    int got = 0;
+    for (uint32_t a = 0; got < NM; ++a) {
+      if (a >= (1u << 20)) {
+        atomicOr(status, kStatusIonBirth);
+        s_abort = 1;
+        break;
+      }
+      u32x4 ctr = {{a, (uint32_t)j, turn, (uint32_t)(k * CG_MAX_SPECIES)}};
+      double g0, g1;
+      normal2(philox4x32_10(ctr, k0, k1), &g0, &g1);
+      double tx = mx + sx * g0, ty = my + sy * g1;
+      double ax = (tx - mx) / sx, ay = (ty - my) / sy;
+      if (ax * ax + ay * ay > 4.E0) continue;
+      BXn[(size_t)j * NM + got] = tx;
+      BYn[(size_t)j * NM + got] = ty;
+      got++;
+    }
+  }
+  CloudDev cd = clouds[0];
+  CloudState st = cst[0];
+  const bool in_smem = (long long)st.n + (long long)M * NM <= smem_cap;
+  double* X = in_smem ? scl : cd.x[0];
+  double* Y = in_smem ? scl + smem_cap : cd.y[0];
+  double* VX = in_smem ? scl + 2 * (size_t)smem_cap : cd.vx[0];
+  double* VY = in_smem ? scl + 3 * (size_t)smem_cap : cd.vy[0];
+  const int cap = in_smem ? smem_cap : cd.cap;
+  double S[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int i = tid; i < st.n; i += kChainThreads) {
+    double x = cd.x[0][i], y = cd.y[0][i];
+    if (in_smem) {
+      X[i] = x;
+      Y[i] = y;
+      VX[i] = cd.vx[0][i];
+      VY[i] = cd.vy[0][i];
+    }
+    S[0] += x;
+    S[1] += y;
+    S[2] = fma(x, x, S[2]);
+    S[3] = fma(y, y, S[3]);
+  }
+  block_sum<4, kChainThreads>(S, smem);  // also publishes the prologue's shared writes
+  if (s_abort) return;
+  const double bx = s_bx, by = s_by;
+  const double pressure = cp.gas_percent[0] * cs.pressure;
+  const int half = tid & 1;
+  const double drift = cp.circ_ring / cp.harmonics;
+
+  for (int j = 0; j < M; ++j) {
+    const double mx = sb[j], my = sb[M + j], ne = sb[4 * M + j];
+    const int gap = (int)sb[5 * M + j];
+    // LIP::GetIonNumberPerInterAction + IonGenerator charge (LIP.cpp:974-995)
+    const double line_density = cp.cross_section[0] * pressure / cs.temperature / kBoltzmann * ne;
+    st.macro_charge = line_density * cs.length / NM;
+    if (st.n + NM > cap) {
+      if (tid == 0) atomicOr(status, kStatusIonOverflow);
+      return;
+    }
+    // IonsUpdate: append the births (LIP.cpp:1021-1051)
+    for (int q = 0; q < NM; ++q) {
+      const double x = BXn[(size_t)j * NM + q], y = BYn[(size_t)j * NM + q];
+      if (tid == q % kChainThreads) {
+        X[st.n + q] = x;
+        Y[st.n + q] = y;
+        VX[st.n + q] = 0.0;
+        VY[st.n + q] = 0.0;
+      }
+      S[0] += x;
+      S[1] += y;
+      S[2] = fma(x, x, S[2]);
+      S[3] = fma(y, y, S[3]);
+    }
+    st.n += NM;
+    if (st.n > cp.max_ions) {
+      if (tid == 0) atomicOr(status, kStatusIonOverflow);
+      return;
+    }
+    __syncthreads();
+    // IonRMSCal (LIP.cpp:1113-1155); one ion keeps the stale centroid
+    if (st.n == 1) {
+      st.rms_x = fabs(X[0]);
+      st.rms_y = fabs(Y[0]);
+    } else {
+      st.aver_x = S[0] / st.n;
+      st.aver_y = S[1] / st.n;
+      st.rms_x = sqrt(fmax(S[2] / st.n - st.aver_x * st.aver_x, 0.0));
+      st.rms_y = sqrt(fmax(S[3] / st.n - st.aver_y * st.aver_y, 0.0));
+    }
+    if (tid == 0) {
+      CloudRec r;
+      r.coeff = 2.0 * (st.macro_charge * st.n) * kElecClassicRadius / cp.r_gamma;
+      r.rms_x = st.rms_x;
+      r.rms_y = st.rms_y;
+      r.aver_x = st.aver_x;
+      r.aver_y = st.aver_y;
+      r.count = st.n;
+      rec[j] = r;
+    }
+    // ion side and IonTransferDueToBunch, two lanes per ion
+    const double coeffI =
+        2.0 * ne * kElecClassicRadius * kElectronMassEV / kIonMassEV / cp.mass_number[0] * kCLight;
+    const FieldPrep& fp = FP[j];
+    int out_base = 0;
+    double Sn[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int c0 = 0; c0 < st.n; c0 += kChainThreads / 2) {
+      const int i = c0 + (tid >> 1);
+      bool keep = false;
+      double x = 0, y = 0, vx = 0, vy = 0;
+      double z1r = 0, z1i = 0, z2r = 0, z2i = 0;
+      if (i < st.n) {
+        x = X[i];
+        y = Y[i];
+        vx = VX[i];
+        vy = VY[i];
+        field_zargs(fp, x - mx, y - my, &z1r, &z1i, &z2r, &z2i);
+      }
+      cplx wm = half ? w_quadrant1_lowlat(z2r, z2i) : w_quadrant1_lowlat(z1r, z1i);
+      cplx wo = {__shfl_xor_sync(FULL_MASK, wm.re, 1), __shfl_xor_sync(FULL_MASK, wm.im, 1)};
+      if (i < st.n) {
+        double fx, fy;
+        field_finish(fp, x - mx, y - my, half ? wo : wm, half ? wm : wo, &fx, &fy);
+        vx += coeffI * fx;
+        vy += coeffI * fy;
+        x += vx * drift * gap / kCLight;
+        y += vy * drift * gap / kCLight;
+        keep = !(fabs(x) > bx || fabs(y) > by) && half == 0;
+      }
+      const double v4[4] = {x, y, x * x, y * y};
+      int tot;
+      double ts[4];
+      const int pos = scan_keep_sums(keep, v4, s_cnt, s_sum, &tot, ts);  // all reads done
+      if (keep) {
+        X[out_base + pos] = x;
+        Y[out_base + pos] = y;
+        VX[out_base + pos] = vx;
+        VY[out_base + pos] = vy;
+      }
+      out_base += tot;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) Sn[q] += ts[q];
+    }
+    st.n = out_base;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) S[q] = Sn[q];
+  }
+  __syncthreads();
+  if (in_smem)
+    for (int i = tid; i < st.n; i += kChainThreads) {
+      cd.x[0][i] = X[i];
+      cd.y[0][i] = Y[i];
+      cd.vx[0][i] = VX[i];
+      cd.vy[0][i] = VY[i];
+    }
+  if (tid == 0) {
+    st.cur = 0;
+    cst[0] = st;
+  }
+}
+
+// Shared memory of the chain kernels.  Single species, when the fixed part
+// fits in half the opt-in shared memory: per-bunch inputs (6 doubles), the
+// births (2 x macro ions per IP doubles) and the field constants of every
+// bunch, then the cloud (4 doubles per ion) in the rest.  Otherwise the
+// generic kernel: per-bunch inputs when at most 2048 bunches, plus as many
+// ions per species as fit in the remaining opt-in shared memory.
+struct ChainPlan {
+  int single;  // k_ion_chain1
+  int sb_ok, births_ok, cap;
+  size_t bytes;
+};
+
+static ChainPlan chain_smem_plan(const Handle& h) {
+  ChainPlan pl{};
   int dev = 0, optin = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  size_t budget = (size_t)optin - 4096;  // static shared memory of the kernel
-  size_t sb = h.M <= 2048 ? 6 * sizeof(double) * (size_t)h.M : 0;
-  *sb_ok = sb > 0;
-  size_t br = 2 * sizeof(double) * (size_t)h.M * (size_t)std::max(1, h.cfg.ion.macro_ions_per_ip);
-  *births_ok = (h.P == 1 && sb + br <= budget / 2) ? 1 : 0;
-  if (!*births_ok) br = 0;
+  const size_t budget = (size_t)optin - 4096;  // static shared memory of the kernels
+  const size_t M = (size_t)h.M, NM = (size_t)std::max(1, h.cfg.ion.macro_ions_per_ip);
+  const size_t fixed1 = 6 * sizeof(double) * M + 2 * sizeof(double) * M * NM + sizeof(FieldPrep) * M;
+  if (h.P == 1 && fixed1 <= budget / 2) {
+    pl.single = 1;
+    pl.sb_ok = pl.births_ok = 1;
+    pl.cap = (int)((budget - fixed1) / (4 * sizeof(double)));
+    pl.bytes = fixed1 + (size_t)pl.cap * 4 * sizeof(double);
+    return pl;
+  }
+  size_t sb = h.M <= 2048 ? 6 * sizeof(double) * M : 0;
+  pl.sb_ok = sb > 0;
+  size_t br = 2 * sizeof(double) * M * NM;
+  pl.births_ok = (h.P == 1 && sb + br <= budget / 2) ? 1 : 0;
+  if (!pl.births_ok) br = 0;
   size_t rest = budget > sb + br ? budget - sb - br : 0;
-  *cap = (int)(rest / (4 * sizeof(double) * (size_t)h.P));
-  *bytes = sb + br + (size_t)(*cap) * 4 * sizeof(double) * h.P;
+  pl.cap = (int)(rest / (4 * sizeof(double) * (size_t)h.P));
+  pl.bytes = sb + br + (size_t)pl.cap * 4 * sizeof(double) * h.P;
+  return pl;
 }
 
-// Opt-in shared memory of the chain kernel (set outside any graph capture).
+// Opt-in shared memory of the chain kernels (set outside any graph capture).
 cudaError_t prepare_ion_chain(Handle& h) {
-  int sb_ok = 0, births_ok = 0, cap = 0;
-  size_t bytes = 0;
-  chain_smem_plan(h, &sb_ok, &births_ok, &cap, &bytes);
-  cudaError_t e = cudaFuncSetAttribute(k_ion_chain<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)bytes);
+  const ChainPlan pl = chain_smem_plan(h);
+  cudaError_t e = cudaFuncSetAttribute(pl.single ? (const void*)k_ion_chain1 : (const void*)k_ion_chain<1>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.bytes);
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(k_ion_chain<CG_MAX_SPECIES>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.bytes);
 }
 
 cudaError_t launch_ion_chain(Handle& h, int k) {
@@ -675,14 +944,17 @@ cudaError_t launch_ion_chain(Handle& h, int k) {
   cs.length = s.length;
   cs.aperture_x = s.aperture_x;
   cs.aperture_y = s.aperture_y;
-  int sb_ok = 0, births_ok = 0, cap = 0;
-  size_t bytes = 0;
-  chain_smem_plan(h, &sb_ok, &births_ok, &cap, &bytes);
+  const ChainPlan pl = chain_smem_plan(h);
+  if (pl.single) {
+    k_ion_chain1<<<1, kChainThreads, pl.bytes, h.stream>>>(
+        h.chain, cs, h.d.bunch, h.d.mom, h.d.clouds + k, h.d.cloud_state + k,
+        h.d.rec + (size_t)k * h.M, h.d.status, h.d.turn, k, pl.cap);
+    return cudaGetLastError();
+  }
   auto kern = h.P == 1 ? k_ion_chain<1> : k_ion_chain<CG_MAX_SPECIES>;
-  kern<<<1, kChainThreads, bytes, h.stream>>>(
+  kern<<<1, kChainThreads, pl.bytes, h.stream>>>(
       h.chain, cs, h.d.bunch, h.d.mom, h.d.clouds + (size_t)k * h.P, h.d.cloud_state + (size_t)k * h.P,
-      h.d.rec + (size_t)k * h.M * h.P, h.d.prep + (size_t)k * h.M * h.P, h.d.status, h.d.turn, k,
-      cap, sb_ok, births_ok);
+      h.d.rec + (size_t)k * h.M * h.P, h.d.status, h.d.turn, k, pl.cap, pl.sb_ok, pl.births_ok);
   return cudaGetLastError();
 }
 
