@@ -141,6 +141,8 @@ EXPORTS = [
     ("cg_faddeeva_w", I, [PD, PD, PD, PD, C.c_int64]),
     ("cg_faddeeva_w_q1", I, [PD, PD, PD, PD, C.c_int64]),
     ("cg_gaussian_field", I, [PD, PD, PD, PD, PD, PD, C.c_int64]),
+    ("cg_bunch_moments_noalloc", I, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, D, D,
+                                     C.c_void_p, C.c_void_p]),
 ]
 
 _lib = None

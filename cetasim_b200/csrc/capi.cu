@@ -1026,4 +1026,47 @@ int cg_gaussian_field(const double* x, const double* y, const double* sx, const 
   return eval_arrays(4, in, 2, out, n, 2);
 }
 
+// ---- device buffers in/out, no allocation ----
+
+static_assert((long long)kNoAllocMaxTiles * kTile == CG_NOALLOC_MAX_PARTICLES,
+              "static moments scratch size");
+
+static std::mutex g_noalloc_mu;
+static double* g_noalloc_ptr[64] = {nullptr};
+
+int cg_bunch_moments_noalloc(const double* d_coords, int64_t stride, const uint8_t* d_surv,
+                             int64_t n, double beta_x, double beta_y, cg_bunch_moments* d_out,
+                             void* stream) {
+  if (!d_coords || !d_surv || !d_out) return fail(nullptr, CG_ERR_INVALID, "null device pointer");
+  if (((uintptr_t)d_coords | (uintptr_t)d_out) % alignof(double) != 0)
+    return fail(nullptr, CG_ERR_INVALID, "d_coords and d_out must be 8-byte aligned");
+  if (n < 1) return fail(nullptr, CG_ERR_INVALID, "n must be at least 1");
+  if (n > CG_NOALLOC_MAX_PARTICLES)
+    return fail(nullptr, CG_ERR_INVALID,
+                "n = " + std::to_string(n) +
+                    " exceeds the static scratch of cg_bunch_moments_noalloc (at most " +
+                    std::to_string(CG_NOALLOC_MAX_PARTICLES) + " particles per call)");
+  if (stride < n) return fail(nullptr, CG_ERR_INVALID, "stride must be at least n");
+  if (!(beta_x > 0) || !(beta_y > 0)) return fail(nullptr, CG_ERR_INVALID, "beta must be > 0");
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaGetDevice");
+  if (dev < 0 || dev >= 64) return fail(nullptr, CG_ERR_UNSUPPORTED, "device index above 63");
+  double* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+      e = noalloc_scratch_address(&g_noalloc_ptr[dev]);
+      if (e != cudaSuccess) {
+        g_noalloc_ptr[dev] = nullptr;
+        return cuda_fail(nullptr, e, "static moments scratch");
+      }
+    }
+    scratch = g_noalloc_ptr[dev];
+  }
+  e = launch_moments_noalloc(d_coords, stride, d_surv, (int)n, beta_x, beta_y, scratch, d_out,
+                             (cudaStream_t)stream);
+  return e == cudaSuccess ? CG_OK : cuda_fail(nullptr, e, "moments (no allocation)");
+}
+
 }  // extern "C"

@@ -1368,4 +1368,96 @@ cudaError_t upload_weideman_table() {
   return cudaMemcpyToSymbol(c_weideman, &h_weideman, sizeof(WeidemanTable));
 }
 
+// ---------------------------------------------------------------------------
+// Moments of one bunch in the caller's device buffers without any device
+// allocation.  A caller that owns the particle arrays and calls once per turn
+// (another code's tracking loop, a PyTorch program whose caching allocator owns
+// the device memory) cannot afford a cudaMalloc/cudaFree pair per call: both
+// synchronise the device and stall the caller's other streams.  The per-tile
+// partials, the finished moments and the completion counter therefore live in
+// one file-scope device array of fixed size.
+//
+// Layout of the array (doubles): kNoAllocMaxTiles partials, then one
+// BunchMomDev slot (32 doubles), then the completion counter (32 doubles).
+// Only the counter must read zero when a call starts: it is zero at module
+// load, zeroed again when the address is first resolved on a device, and the
+// last CTA of every call puts it back to zero.  The partials and the moments
+// slot are written before they are read in every call.  Two calls that overlap
+// on one device (different streams, or different host threads without
+// ordering) share this array and race.
+constexpr int kNoAllocPartialDoubles = (int)(sizeof(MomPartial) / sizeof(double));
+constexpr size_t kNoAllocMomOff = (size_t)kNoAllocMaxTiles * kNoAllocPartialDoubles;
+constexpr size_t kNoAllocCounterOff = kNoAllocMomOff + 32;
+constexpr size_t kNoAllocDoubles = kNoAllocCounterOff + 32;
+static_assert(sizeof(MomPartial) % sizeof(double) == 0, "partial is a whole number of doubles");
+static_assert(sizeof(BunchMomDev) <= 32 * sizeof(double), "moments slot holds a BunchMomDev");
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+
+cudaError_t noalloc_scratch_address(double** ptr) {
+  cudaError_t e = cudaGetSymbolAddress((void**)ptr, g_noalloc_scratch);
+  if (e != cudaSuccess) return e;
+  return cudaMemset(*ptr + kNoAllocCounterOff, 0, 32 * sizeof(double));
+}
+
+__global__ void __launch_bounds__(kTile, 2) k_moments_noalloc(const double* __restrict__ c,
+                                                           int64_t stride,
+                                                           const uint8_t* __restrict__ surv, int n,
+                                                           double beta_x, double beta_y,
+                                                           double* scratch) {
+  __shared__ double smem[9 * 32];
+  MomPartial* partials = reinterpret_cast<MomPartial*>(scratch);
+  BunchMomDev* mom = reinterpret_cast<BunchMomDev*>(scratch + kNoAllocMomOff);
+  unsigned* counter = reinterpret_cast<unsigned*>(scratch + kNoAllocCounterOff);
+  const int i = blockIdx.x * kTile + threadIdx.x;
+  double v[6] = {0, 0, 0, 0, 0, 0};
+  bool alive = false;
+  if (i < n) {
+    alive = surv[i] == kAlive;
+#pragma unroll
+    for (int d = 0; d < 6; ++d) v[d] = c[d * stride + i];
+  }
+  tile_moment_partial(v, alive, smem, &partials[blockIdx.x]);
+  BunchDev B{};
+  B.n = n;
+  B.tile_off = 0;
+  B.n_tiles = (int)gridDim.x;
+  bunch_moment_finish(0, B, partials, counter, mom, beta_x, beta_y, c + 4 * stride, nullptr);
+}
+
+// Converts the finished moments into the public record (one thread; the
+// transmission of a record made this way is n_alive / n).
+__global__ void k_moments_noalloc_out(const double* __restrict__ scratch, int n,
+                                      cg_bunch_moments* out) {
+  const BunchMomDev s = *reinterpret_cast<const BunchMomDev*>(scratch + kNoAllocMomOff);
+  cg_bunch_moments o;
+  o.n_alive = (int)s.n_alive;
+  o.n_macro = n;
+  for (int d = 0; d < 6; ++d) o.mean[d] = s.mean[d];
+  for (int d = 0; d < 3; ++d) {
+    o.emit[d] = s.emit[d];
+    o.eff_emit[d] = s.eff_emit[d];
+  }
+  o.rms_x = s.rms_x;
+  o.rms_y = s.rms_y;
+  o.eff_rms_x = s.eff_rms_x;
+  o.eff_rms_y = s.eff_rms_y;
+  o.bunch_length = s.bunch_length;
+  o.energy_spread = s.energy_spread;
+  o.z_min = s.z_min;
+  o.z_max = s.z_max;
+  o.transmission = s.n_alive / (double)n;
+  *out = o;
+}
+
+cudaError_t launch_moments_noalloc(const double* c, int64_t stride, const uint8_t* surv, int n,
+                                   double beta_x, double beta_y, double* scratch,
+                                   cg_bunch_moments* out, cudaStream_t s) {
+  const int tiles = (n + kTile - 1) / kTile;
+  k_moments_noalloc<<<tiles, kTile, 0, s>>>(c, stride, surv, n, beta_x, beta_y, scratch);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_moments_noalloc_out<<<1, 1, 0, s>>>(scratch, n, out);
+  return cudaGetLastError();
+}
+
 }  // namespace cg

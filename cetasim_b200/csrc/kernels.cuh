@@ -38,6 +38,15 @@ cudaError_t launch_faddeeva(const double* zr, const double* zi, double* wr, doub
 cudaError_t launch_field(const double* x, const double* y, const double* sx, const double* sy,
                          double* fx, double* fy, int64_t n, cudaStream_t s);
 cudaError_t upload_weideman_table();
+
+// Moments of one bunch held in the caller's device buffers, with the partials
+// in a fixed file-scope device array (no allocation).  At most
+// kNoAllocMaxTiles tiles of kTile particles per call.
+constexpr int kNoAllocMaxTiles = 4096;
+cudaError_t noalloc_scratch_address(double** ptr);
+cudaError_t launch_moments_noalloc(const double* c, int64_t stride, const uint8_t* surv, int n,
+                                   double beta_x, double beta_y, double* scratch,
+                                   cg_bunch_moments* out, cudaStream_t s);
 cudaError_t measure_fp64_peak(double* flops);
 
 }  // namespace cg

@@ -326,6 +326,33 @@ int cg_faddeeva_w_q1(const double* zr, const double* zi, double* wr, double* wi,
 int cg_gaussian_field(const double* x, const double* y, const double* sx,
                       const double* sy, double* fx, double* fy, int64_t n);
 
+/* ---- device buffers in/out, no allocation ---- */
+
+/* Largest n of one cg_bunch_moments_noalloc call (4096 tiles of 256). */
+#define CG_NOALLOC_MAX_PARTICLES 1048576
+
+/* No counterpart in the reference.  The moments MPBunch::GetMPBunchRMS sets
+ * (MPBunch.cpp:342-498; the same kernels and merge order as cg_beam_rms) for
+ * one bunch whose particles sit in the caller's DEVICE memory: d_coords holds
+ * x, px, y, py, z, dp as six rows of `stride` doubles, d_surv one flag per
+ * particle (0 = alive), and the result is written to *d_out in device memory
+ * (n_macro = n, transmission = n_alive / n).  Work is enqueued on `stream`
+ * (a cudaStream_t; NULL = legacy default stream) of the current device and
+ * the call returns without waiting.
+ *
+ * It never allocates: the partials live in a fixed static device array of
+ * CG_NOALLOC_MAX_PARTICLES / 256 tiles (about 577 KB per device), and
+ * n > CG_NOALLOC_MAX_PARTICLES is rejected with CG_ERR_INVALID.  The first
+ * call on each device resolves that array's address and zeroes its
+ * completion counter with a synchronous memset, so make it before any stream
+ * capture.  Calls on one device share the array: two calls that overlap in
+ * time (different streams, or host threads without ordering between them)
+ * race and both results are undefined. */
+int cg_bunch_moments_noalloc(const double* d_coords, int64_t stride,
+                             const uint8_t* d_surv, int64_t n, double beta_x,
+                             double beta_y, cg_bunch_moments* d_out,
+                             void* stream);
+
 #ifdef __cplusplus
 }
 #endif
