@@ -87,12 +87,18 @@ int launch_ok(Handle& h, cudaError_t e, const char* what) {
 
 void free_beam(Handle& h) {
   DeviceBufs& d = h.d;
-  dfree(d.c); dfree(d.surv); dfree(d.tile_bunch); dfree(d.bunch); dfree(d.partials);
+  dfree(d.c); dfree(d.surv); dfree(d.tile_bunch); dfree(d.chunk_bunch); dfree(d.bunch);
+  dfree(d.partials);
   dfree(d.counters); dfree(d.mom); dfree(d.loss_count); dfree(d.scratch);
   dfree(d.rec); dfree(d.lr_hist); dfree(d.lr_force); dfree(d.fir_hist); dfree(d.fir_kick);
   dfree(d.sr_geom); dfree(d.sr_counts); dfree(d.sr_sumx); dfree(d.sr_sumy); dfree(d.sr_lag);
   dfree(d.sr_pot);
-  d.c = nullptr; d.surv = nullptr; d.tile_bunch = nullptr; d.bunch = nullptr; d.partials = nullptr;
+  IonWalk& w = d.iw;
+  dfree(w.births); dfree(w.prep); dfree(w.bunch); dfree(w.spec); dfree(w.bound); dfree(w.part);
+  dfree(w.traj); dfree(w.alive);
+  w = IonWalk();
+  d.c = nullptr; d.surv = nullptr; d.tile_bunch = nullptr; d.chunk_bunch = nullptr;
+  d.bunch = nullptr; d.partials = nullptr;
   d.counters = nullptr; d.mom = nullptr; d.loss_count = nullptr; d.scratch = nullptr;
   d.rec = nullptr; d.lr_hist = nullptr; d.lr_force = nullptr; d.fir_hist = nullptr;
   d.fir_kick = nullptr; d.sr_geom = nullptr; d.sr_counts = nullptr; d.sr_sumx = nullptr;
@@ -474,29 +480,35 @@ int cg_set_beam(cg_handle* H, int M, const int* n_macro, const int* harm, const 
   for (int j = 0; j < M - 1; ++j) h.gap[j] = harm[j + 1] - harm[j];
   h.gap[M - 1] = Hh - harm[M - 1];
   std::vector<BunchDev> bd(M);
-  std::vector<int> tb;
+  std::vector<int> tb, cb;
   h.tile_off.assign(M + 1, 0);
-  int tiles = 0;
+  int tiles = 0, chunks = 0;
   for (int j = 0; j < M; ++j) {
     int nt = (n_macro[j] + kTile - 1) / kTile;
+    int nc = (nt + kMomChunkTiles - 1) / kMomChunkTiles;
     bd[j].n = n_macro[j];
     bd[j].tile_off = tiles;
     bd[j].n_tiles = nt;
     bd[j].harm = harm[j];
     bd[j].gap = h.gap[j];
-    bd[j].pad = 0;
+    bd[j].chunk_off = chunks;
+    bd[j].n_chunks = nc;
     bd[j].ne = ne[j];
     bd[j].q_macro = ne[j] / n_macro[j];
     h.tile_off[j] = tiles;
     for (int t = 0; t < nt; ++t) tb.push_back(j);
+    for (int t = 0; t < nc; ++t) cb.push_back(j);
     tiles += nt;
+    chunks += nc;
   }
   h.tile_off[M] = tiles;
   h.n_tiles = tiles;
+  h.n_chunks = chunks;
   h.npad = (int64_t)tiles * kTile;
   DeviceBufs& d = h.d;
   if (dalloc(&d.c, 6 * (size_t)h.npad) || dalloc(&d.surv, (size_t)h.npad) ||
-      dalloc(&d.tile_bunch, tiles) || dalloc(&d.bunch, M) || dalloc(&d.partials, tiles) ||
+      dalloc(&d.tile_bunch, tiles) || dalloc(&d.chunk_bunch, chunks) || dalloc(&d.bunch, M) ||
+      dalloc(&d.partials, chunks) ||
       dalloc(&d.counters, M + 1) || dalloc(&d.mom, M) || dalloc(&d.loss_count, M + 1)) {
     free_beam(h);
     return fail(&h, CG_ERR_OOM, "beam allocation failed");
@@ -509,6 +521,7 @@ int cg_set_beam(cg_handle* H, int M, const int* n_macro, const int* harm, const 
   cudaMemset(d.c, 0, sizeof(double) * 6 * h.npad);
   cudaMemset(d.surv, 0xFF, h.npad);
   cudaMemcpy(d.tile_bunch, tb.data(), sizeof(int) * tiles, cudaMemcpyHostToDevice);
+  cudaMemcpy(d.chunk_bunch, cb.data(), sizeof(int) * chunks, cudaMemcpyHostToDevice);
   cudaMemcpy(d.bunch, bd.data(), sizeof(BunchDev) * M, cudaMemcpyHostToDevice);
   cudaMemset(d.counters, 0, sizeof(unsigned) * (M + 1));
   cudaMemset(d.loss_count, 0, sizeof(int) * (M + 1));
@@ -522,8 +535,18 @@ int cg_set_beam(cg_handle* H, int M, const int* n_macro, const int* harm, const 
       return fail(&h, CG_ERR_OOM, "ion records");
     }
     cudaMemset(d.rec, 0, sizeof(CloudRec) * h.K * M * h.P);
-    cudaError_t pe = prepare_ion_chain(h);
-    if (pe != cudaSuccess) { free_beam(h); return cuda_fail(&h, pe, "ion chain shared memory"); }
+    // ion-chain scratch: trajectories = the cloud's capacity + the births of one walk
+    IonWalk& w = d.iw;
+    const size_t NM = (size_t)h.cfg.ion.macro_ions_per_ip, P = (size_t)h.P;
+    w.tcap = (int64_t)h.ion_cap + (int64_t)M * (int64_t)NM;
+    w.grid = ion_walk_grid(w.tcap);
+    if (dalloc(&w.births, P * M * NM * 2) || dalloc(&w.prep, (size_t)M) ||
+        dalloc(&w.bunch, 3 * (size_t)M) || dalloc(&w.spec, P * M * 2) || dalloc(&w.bound, 2) ||
+        dalloc(&w.part, P * M * (size_t)w.grid * 5) || dalloc(&w.traj, P * 4 * (size_t)w.tcap) ||
+        dalloc(&w.alive, P * (size_t)w.tcap)) {
+      free_beam(h);
+      return fail(&h, CG_ERR_OOM, "ion chain scratch");
+    }
   }
   if (h.cfg.flag_lr_wake) {
     if (dalloc(&d.lr_hist, (size_t)h.cfg.lr_turns * 3 * M) || dalloc(&d.lr_force, 3 * (size_t)M)) {

@@ -10,11 +10,12 @@
 namespace cg {
 
 constexpr int kTile = 256;            // particles per tile == threads per CTA
-constexpr int kChainThreads = 256;    // ion-chain CTA size (two lanes per ion)
+
+constexpr int kMomChunkTiles = 4;     // tiles per CTA of the moments kernel
 
 struct BunchDev {
   int n, tile_off, n_tiles, harm, gap;
-  int pad;
+  int chunk_off, n_chunks;  // moments chunks of kMomChunkTiles tiles
   double ne, q_macro;
 };
 
@@ -45,12 +46,34 @@ struct ChainParams {
   uint64_t seed;
 };
 
+// Section data the ion chain of one IP needs.
+struct ChainSection {
+  double pressure, temperature, length, aperture_x, aperture_y;
+};
+
+// Scratch of the ion chain (one IP at a time, reused across IPs): per-bunch
+// constants and births from k_ion_prep, per-step partial sums and trajectory
+// end states from k_ion_walk.
+struct IonWalk {
+  double* births = nullptr;   // P x M x NM x (x, y)
+  FieldPrep* prep = nullptr;  // M: field constants of each bunch
+  double* bunch = nullptr;    // M x (mean x, mean y, drift time to the next bunch)
+  double* spec = nullptr;     // P x M x (macro-ion charge, ion-side coefficient)
+  double* bound = nullptr;    // loss bounds (x, y)
+  double* part = nullptr;     // P x M x grid x (count, sum x, sum y, sum x^2, sum y^2)
+  double* traj = nullptr;     // P x 4 x tcap: x, y, vx, vy after the walk
+  uint8_t* alive = nullptr;   // P x tcap
+  int64_t tcap = 0;           // trajectories per species: cloud capacity + M x NM
+  int grid = 0;               // CTAs of k_ion_walk per species
+};
+
 struct DeviceBufs {
   double* c = nullptr;          // 6 x npad SoA
   uint8_t* surv = nullptr;      // npad
   int* tile_bunch = nullptr;    // n_tiles
+  int* chunk_bunch = nullptr;   // n_chunks: bunch of each moments chunk
   BunchDev* bunch = nullptr;    // M
-  MomPartial* partials = nullptr;  // n_tiles
+  MomPartial* partials = nullptr;  // n_chunks
   unsigned* counters = nullptr;    // M (+ spare)
   BunchMomDev* mom = nullptr;      // M
   int* loss_count = nullptr;       // M
@@ -61,6 +84,7 @@ struct DeviceBufs {
   CloudState* cloud_state = nullptr;  // K x P
   CloudRec* rec = nullptr;         // K x M x P
   double* ion_totals = nullptr;    // K (charge), used by cg_ion_totals
+  IonWalk iw;
   // long-range wake
   double* lr_tab = nullptr;        // 3 x np
   double* lr_hist = nullptr;       // turns x 3 x M ring buffer
@@ -95,6 +119,7 @@ struct Handle {
   cudaStream_t stream = nullptr;
   int K = 0, M = 0, P = 1;
   int n_tiles = 0;
+  int n_chunks = 0;
   int64_t npad = 0;
   std::vector<int> n_macro, harm, gap, tile_off;
   std::vector<double> ne;

@@ -118,32 +118,47 @@ __device__ __forceinline__ void store6(double* __restrict__ c, int64_t npad, int
 }
 
 // ---------------------------------------------------------------------------
-// Moments (MPBunch::GetMPBunchRMS, MPBunch.cpp:342-498): per tile a two-pass
-// partial (mean, centred co-moments) over alive particles, then the last CTA
-// of each bunch merges the bunch's partials in tile order.
+// Moments (MPBunch::GetMPBunchRMS, MPBunch.cpp:342-498): a CTA takes a chunk
+// of up to kMomChunkTiles tiles of one bunch, holds its particles in
+// registers and makes a two-pass partial (mean, then centred co-moments) over
+// the alive ones; the last CTA of each bunch merges the bunch's partials in
+// chunk order (Chan et al. pairwise update: deterministic, and as accurate as
+// the reference's two passes over the whole bunch).
 
-__device__ void tile_moment_partial(const double v[6], bool alive, double* smem,
-                                    MomPartial* out) {
-  double s[7];
+// v[u][d]: coordinate d of this thread's particle in tile u of the chunk.
+__device__ void chunk_moment_partial(const double (&v)[kMomChunkTiles][6],
+                                     const bool (&alive)[kMomChunkTiles], double* smem,
+                                     MomPartial* out) {
+  double s[7] = {0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
-  for (int d = 0; d < 6; ++d) s[d] = alive ? v[d] : 0.0;
-  s[6] = alive ? 1.0 : 0.0;
+  for (int u = 0; u < kMomChunkTiles; ++u) {
+#pragma unroll
+    for (int d = 0; d < 6; ++d) s[d] += alive[u] ? v[u][d] : 0.0;
+    s[6] += alive[u] ? 1.0 : 0.0;
+  }
   block_sum<7, kTile>(s, smem);
   const double n = s[6];
   double mean[6];
 #pragma unroll
   for (int d = 0; d < 6; ++d) mean[d] = n > 0 ? s[d] / n : 0.0;
-  double q[9];
-  double dv[6];
+  double q[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  double mn = INFINITY, mx = -INFINITY;
 #pragma unroll
-  for (int d = 0; d < 6; ++d) dv[d] = alive ? v[d] - mean[d] : 0.0;
+  for (int u = 0; u < kMomChunkTiles; ++u) {
+    double dv[6];
 #pragma unroll
-  for (int d = 0; d < 6; ++d) q[d] = dv[d] * dv[d];
-  q[6] = dv[0] * dv[1];
-  q[7] = dv[2] * dv[3];
-  q[8] = dv[4] * dv[5];
+    for (int d = 0; d < 6; ++d) dv[d] = alive[u] ? v[u][d] - mean[d] : 0.0;
+#pragma unroll
+    for (int d = 0; d < 6; ++d) q[d] = fma(dv[d], dv[d], q[d]);
+    q[6] = fma(dv[0], dv[1], q[6]);
+    q[7] = fma(dv[2], dv[3], q[7]);
+    q[8] = fma(dv[4], dv[5], q[8]);
+    if (alive[u]) {
+      mn = fmin(mn, v[u][4]);
+      mx = fmax(mx, v[u][4]);
+    }
+  }
   block_sum<9, kTile>(q, smem);
-  double mn = alive ? v[4] : INFINITY, mx = alive ? v[4] : -INFINITY;
   block_minmax<kTile>(mn, mx, smem);
   if (threadIdx.x == 0) {
     MomPartial p;
@@ -158,17 +173,19 @@ __device__ void tile_moment_partial(const double v[6], bool alive, double* smem,
   }
 }
 
-// Called by all threads of every CTA after its partial is stored: the last
-// CTA of bunch b merges the partials (fixed pairwise tree) and finalises.
-__device__ void bunch_moment_finish(int b, const BunchDev& B, const MomPartial* partials,
+// Called by all threads of every CTA after its partial is stored: the last of
+// the n_parts CTAs of bunch b merges partials [part_off, part_off + n_parts)
+// and finalises.  z0 = z of the bunch's first particle (GetZMinMax seeds the
+// range with it, MPBunch.cpp:1862-1863).
+__device__ __noinline__ void bunch_moment_finish(int b, int part_off, int n_parts, const MomPartial* partials,
                                     unsigned* counters, BunchMomDev* mom, double beta_x,
-                                    double beta_y, const double* z, MomPartial* sp) {
+                                    double beta_y, const double* z0) {
   __shared__ bool last;
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) {
     unsigned prev = atomicAdd(&counters[b], 1u);
-    last = (prev == (unsigned)(B.n_tiles - 1));
+    last = (prev == (unsigned)(n_parts - 1));
   }
   __syncthreads();
   if (!last || threadIdx.x >= 32) return;
@@ -179,9 +196,9 @@ __device__ void bunch_moment_finish(int b, const BunchDev& B, const MomPartial* 
   const int lane = threadIdx.x;
   MomPartial acc;
   mom_clear(acc);
-  for (int t = lane; t < B.n_tiles; t += 32) {
+  for (int t = lane; t < n_parts; t += 32) {
     // partials written by other CTAs: read through L2 (no stale L1 lines)
-    const double* src = reinterpret_cast<const double*>(partials + B.tile_off + t);
+    const double* src = reinterpret_cast<const double*>(partials + part_off + t);
     MomPartial q;
     double* dst = reinterpret_cast<double*>(&q);
 #pragma unroll
@@ -199,39 +216,44 @@ __device__ void bunch_moment_finish(int b, const BunchDev& B, const MomPartial* 
   if (lane == 0) {
     BunchMomDev m = mom[b];
     double tr = m.transmission;
-    double z0 = z[(int64_t)B.tile_off * kTile];
-    mom_finalize(acc, beta_x, beta_y, z0, m);
+    mom_finalize(acc, beta_x, beta_y, *z0, m);
     m.transmission = tr;
     mom[b] = m;
     counters[b] = 0;
   }
-  (void)sp;
 }
 
 __global__ void __launch_bounds__(kTile, 2) k_moments(const double* __restrict__ c, int64_t npad,
                                                    const uint8_t* __restrict__ surv,
-                                                   const int* __restrict__ tile_bunch,
+                                                   const int* __restrict__ chunk_bunch,
                                                    const BunchDev* __restrict__ bunch,
                                                    MomPartial* partials, unsigned* counters,
                                                    BunchMomDev* mom, double beta_x, double beta_y) {
   __shared__ double smem[9 * 32];
-  MomPartial* sp = nullptr;
-  TileIdx t = tile_index(tile_bunch, bunch);
-  double v[6] = {0, 0, 0, 0, 0, 0};
-  bool alive = false;
-  if (t.valid) {
-    alive = surv[t.g] == kAlive;
-    load6(c, npad, t.g, v);
+  const int b = chunk_bunch[blockIdx.x];
+  const BunchDev B = bunch[b];
+  const int tile0 = B.tile_off + (blockIdx.x - B.chunk_off) * kMomChunkTiles;
+  const int i0 = (tile0 - B.tile_off) * kTile + threadIdx.x;
+  double v[kMomChunkTiles][6];
+  bool alive[kMomChunkTiles];
+#pragma unroll
+  for (int u = 0; u < kMomChunkTiles; ++u) {
+    const int64_t g = (int64_t)(tile0 + u) * kTile + threadIdx.x;
+    const bool valid = i0 + u * kTile < B.n;
+    alive[u] = valid && surv[g] == kAlive;
+#pragma unroll
+    for (int d = 0; d < 6; ++d) v[u][d] = valid ? c[d * npad + g] : 0.0;
   }
-  tile_moment_partial(v, alive, smem, &partials[blockIdx.x]);
-  bunch_moment_finish(t.b, bunch[t.b], partials, counters, mom, beta_x, beta_y, c + 4 * npad, sp);
+  chunk_moment_partial(v, alive, smem, &partials[blockIdx.x]);
+  bunch_moment_finish(b, B.chunk_off, B.n_chunks, partials, counters, mom, beta_x, beta_y,
+                      c + 4 * npad + (int64_t)B.tile_off * kTile);
 }
 
 cudaError_t launch_moments(Handle& h, int k) {
   const SectionDev& s = h.sec_dev_host[k];
-  k_moments<<<h.n_tiles, kTile, 0, h.stream>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch, h.d.bunch,
-                                               h.d.partials, h.d.counters, h.d.mom, s.beta_x,
-                                               s.beta_y);
+  k_moments<<<h.n_chunks, kTile, 0, h.stream>>>(h.d.c, h.npad, h.d.surv, h.d.chunk_bunch, h.d.bunch,
+                                                h.d.partials, h.d.counters, h.d.mom, s.beta_x,
+                                                s.beta_y);
   return cudaGetLastError();
 }
 
@@ -284,677 +306,6 @@ __global__ void __launch_bounds__(kTile) k_ion_kick(double* __restrict__ c, int6
 cudaError_t launch_ion_kick(Handle& h, int k) {
   k_ion_kick<<<h.n_tiles, kTile, 0, h.stream>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch,
                                                 h.d.bunch, h.d.rec + (size_t)k * h.M * h.P, h.P);
-  return cudaGetLastError();
-}
-
-// ---------------------------------------------------------------------------
-// Ion chain of one interaction point (MPBeam::SSBeamIonEffectOneInteraction
-// Point, MPBeam.cpp:2585-2611): one CTA walks the bunches in order because
-// bunch j meets the cloud left behind by bunch j-1.
-
-__device__ __forceinline__ int block_excl_scan(int v, int* smem_i, int* total) {
-  // NT = kChainThreads
-  constexpr int NW = kChainThreads / 32;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int x = v;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    int y = __shfl_up_sync(FULL_MASK, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) smem_i[warp] = x;
-  __syncthreads();
-  int wpre = 0, tot = 0;
-#pragma unroll
-  for (int w = 0; w < NW; ++w) {
-    int s = smem_i[w];
-    if (w < warp) wpre += s;
-    tot += s;
-  }
-  __syncthreads();
-  *total = tot;
-  return wpre + x - v;
-}
-
-struct ChainSection {
-  double pressure, temperature, length, aperture_x, aperture_y;
-};
-
-// Shared-memory layout of the chain kernel: per-bunch inputs, then per
-// species the cloud arrays (x, y, vx, vy) when they fit.
-struct ChainSmem {
-  int m_bytes;       // bytes of per-bunch data
-  int cap;           // ions per species that fit in shared memory
-};
-
-__device__ __forceinline__ void chain_bunch_load(const BunchDev* __restrict__ bunch,
-                                                 const BunchMomDev* __restrict__ mom, int j,
-                                                 const double* sb, int M, bool sb_ok, double& mx,
-                                                 double& my, double& sx, double& sy, double& ne,
-                                                 int& gap) {
-  if (sb_ok) {
-    mx = sb[j];
-    my = sb[M + j];
-    sx = sb[2 * M + j];
-    sy = sb[3 * M + j];
-    ne = sb[4 * M + j];
-    gap = (int)sb[5 * M + j];
-  } else {
-    mx = mom[j].mean[0];
-    my = mom[j].mean[2];
-    sx = mom[j].rms_x;
-    sy = mom[j].rms_y;
-    ne = bunch[j].ne;
-    gap = bunch[j].gap;
-  }
-}
-
-// Ion chain of one interaction point (MPBeam::SSBeamIonEffectOneInteraction
-// Point, MPBeam.cpp:2585-2611): one CTA walks the bunches in order, because
-// bunch j meets the cloud left behind by bunch j-1.  The walk is latency
-// bound, so the cloud and the bunch inputs live in shared memory for the
-// whole walk (global memory when they do not fit), removal of lost ions is an
-// in-place stable compaction, and the ion-side field uses the Estrin form of
-// w(z).  Per bunch j and species p:
-//   LIP::GetIonNumberPerInterAction (LIP.cpp:974-982), IonGenerator
-//   (LIP.cpp:985-1019) with Philox counters {attempt, j, turn, k*8+p},
-//   IonsUpdate (LIP.cpp:1021-1051), IonRMSCal (LIP.cpp:1113-1155), the record
-//   of the cloud Gaussian for the electron kick (MPBunch.cpp:1164-1206), the
-//   ion-side kick (MPBunch.cpp:1111-1157) and LIP::IonTransferDueToBunch
-//   (LIP.cpp:1158-1211).
-template <int PMAX>
-__global__ void __launch_bounds__(kChainThreads) k_ion_chain(
-    ChainParams cp, ChainSection cs, const BunchDev* __restrict__ bunch,
-    const BunchMomDev* __restrict__ mom, CloudDev* clouds, CloudState* cst, CloudRec* rec,
-    int* status, const int* __restrict__ d_turn, int k, int smem_cap, int sb_ok,
-    int births_ok) {
-  extern __shared__ double dsm[];
-  __shared__ double smem[4 * 32];
-  __shared__ int smem_i[32];
-  __shared__ double s_bx, s_by;
-  __shared__ int s_abort;
-  const int tid = threadIdx.x;
-  const int M = cp.n_bunches, P = cp.n_species;
-  const uint32_t turn = (uint32_t)(*d_turn);
-  double* sb = dsm;                                 // 6 x M
-  double* scl = dsm + (sb_ok ? 6 * (size_t)M : 0) +                  // P x 4 x smem_cap
-                (births_ok ? 2 * (size_t)M * cp.macro_per_ip : 0);  // after the births
-  {
-    // MPGetBeamInfo: bunchSizeXMax / YMax over all bunches (MPBeam.cpp:2175-2186);
-    // the maximum does not depend on the order of comparison
-    double mx = -INFINITY, my = -INFINITY;
-    for (int j = tid; j < M; j += kChainThreads) {
-      mx = fmax(mx, mom[j].rms_x);
-      my = fmax(my, mom[j].rms_y);
-    }
-    double mn = 0;
-    block_minmax<kChainThreads>(mn, mx, smem);
-    mn = 0;
-    block_minmax<kChainThreads>(mn, my, smem);
-    if (tid == 0) {
-    double lbx = cp.loss_boundary * mx, lby = cp.loss_boundary * my;
-    s_bx = cs.aperture_x > lbx ? lbx : cs.aperture_x;
-    s_by = cs.aperture_y > lby ? lby : cs.aperture_y;
-    s_abort = 0;
-    }
-  }
-  if (sb_ok)
-    for (int j = tid; j < M; j += kChainThreads) {
-      sb[j] = mom[j].mean[0];
-      sb[M + j] = mom[j].mean[2];
-      sb[2 * M + j] = mom[j].rms_x;
-      sb[3 * M + j] = mom[j].rms_y;
-      sb[4 * M + j] = bunch[j].ne;
-      sb[5 * M + j] = (double)bunch[j].gap;
-    }
-  // per species: where the cloud lives for this walk
-  double* AX[PMAX];
-  double* AY[PMAX];
-  double* AVX[PMAX];
-  double* AVY[PMAX];
-  int cap[PMAX];
-  bool in_smem[PMAX];
-  for (int p = 0; p < P && p < PMAX; ++p) {
-    CloudDev cd = clouds[p];
-    int n0 = cst[p].n;
-    in_smem[p] = (long long)n0 + (long long)M * cp.macro_per_ip <= smem_cap;
-    if (in_smem[p]) {
-      double* base = scl + (size_t)p * 4 * smem_cap;
-      AX[p] = base;
-      AY[p] = base + smem_cap;
-      AVX[p] = base + 2 * smem_cap;
-      AVY[p] = base + 3 * smem_cap;
-      cap[p] = smem_cap;
-      for (int i = tid; i < n0; i += kChainThreads) {
-        AX[p][i] = cd.x[0][i];
-        AY[p][i] = cd.y[0][i];
-        AVX[p][i] = cd.vx[0][i];
-        AVY[p][i] = cd.vy[0][i];
-      }
-    } else {
-      AX[p] = cd.x[0];
-      AY[p] = cd.y[0];
-      AVX[p] = cd.vx[0];
-      AVY[p] = cd.vy[0];
-      cap[p] = cd.cap;
-    }
-  }
-  __syncthreads();
-  const double bx = s_bx, by = s_by;
-  const uint32_t k0 = (uint32_t)cp.seed, k1 = (uint32_t)(cp.seed >> 32) ^ kStreamIonBirth;
-  CloudState stv[PMAX];
-  for (int p = 0; p < P && p < PMAX; ++p) stv[p] = cst[p];
-
-  // Single-species walk with precomputed births: the birth positions of bunch
-  // j depend only on its moments and Philox counters, so all of them are
-  // drawn in parallel first (attempts in order per bunch, exactly as the
-  // sequential draw).  A cloud that stays within 128 ions is then walked by
-  // one warp: shuffle reductions, ballot compaction, no block barriers, and up
-  // to four ions per lane in flight.
-  if (PMAX == 1 && births_ok && in_smem[0]) {
-    double* BXn = dsm + (sb_ok ? 6 * (size_t)M : 0);
-    double* BYn = BXn + (size_t)M * cp.macro_per_ip;
-    for (int j = tid; j < M; j += kChainThreads) {
-      double mx, my, sx, sy, ne;
-      int gap;
-      chain_bunch_load(bunch, mom, j, sb, M, sb_ok != 0, mx, my, sx, sy, ne, gap);
-      int got = 0;
-      for (uint32_t a = 0; got < cp.macro_per_ip; ++a) {
-        if (a >= (1u << 20)) {
-          atomicOr(status, kStatusIonBirth);
-          s_abort = 1;
-          break;
-        }
-        u32x4 ctr = {{a, (uint32_t)j, turn, (uint32_t)(k * CG_MAX_SPECIES)}};
-        double g0, g1;
-        normal2(philox4x32_10(ctr, k0, k1), &g0, &g1);
-        double tx = mx + sx * g0, ty = my + sy * g1;
-        double ax = (tx - mx) / sx, ay = (ty - my) / sy;
-        if (ax * ax + ay * ay > 4.E0) continue;
-        BXn[(size_t)j * cp.macro_per_ip + got] = tx;
-        BYn[(size_t)j * cp.macro_per_ip + got] = ty;
-        got++;
-      }
-    }
-    __syncthreads();
-    if (s_abort) return;
-  }
-
-  for (int j = 0; j < M; ++j) {
-    double mx, my, sx, sy, ne;
-    int gap;
-    chain_bunch_load(bunch, mom, j, sb, M, sb_ok != 0, mx, my, sx, sy, ne, gap);
-    for (int p = 0; p < P && p < PMAX; ++p) {
-      CloudState& st = stv[p];
-      double* X = AX[p];
-      double* Y = AY[p];
-      double* VX = AVX[p];
-      double* VY = AVY[p];
-      double press_p = cp.gas_percent[p] * cs.pressure;
-      double line_density = cp.cross_section[p] * press_p / cs.temperature / kBoltzmann * ne;
-      double ion_number = line_density * cs.length;
-      st.macro_charge = ion_number / cp.macro_per_ip;
-      if (st.n + cp.macro_per_ip > cap[p]) {
-        if (tid == 0) atomicOr(status, kStatusIonOverflow);
-        return;
-      }
-      if (tid < 32) {
-        // rejection keeps ~86% of draws; a degenerate (infinite) bunch size
-        // would reject forever, so the attempts are capped and flagged
-        int need = cp.macro_per_ip;
-        uint32_t base = 0;
-        int wpos = st.n;
-        while (need > 0) {
-          if (base >= (1u << 20)) {
-            if (tid == 0) {
-              atomicOr(status, kStatusIonBirth);
-              s_abort = 1;
-            }
-            break;
-          }
-          u32x4 ctr = {{base + (uint32_t)tid, (uint32_t)j, turn, (uint32_t)(k * CG_MAX_SPECIES + p)}};
-          double g0, g1;
-          normal2(philox4x32_10(ctr, k0, k1), &g0, &g1);
-          double tx = mx + sx * g0, ty = my + sy * g1;
-          double ax = (tx - mx) / sx, ay = (ty - my) / sy;
-          bool ok = !(ax * ax + ay * ay > 4.E0);
-          unsigned bal = __ballot_sync(FULL_MASK, ok);
-          int rank = __popc(bal & ((1u << tid) - 1u));
-          if (ok && rank < need) {
-            X[wpos + rank] = tx;
-            Y[wpos + rank] = ty;
-            VX[wpos + rank] = 0.0;
-            VY[wpos + rank] = 0.0;
-          }
-          int got = min(__popc(bal), need);
-          need -= got;
-          wpos += got;
-          base += 32;
-        }
-      }
-      st.n += cp.macro_per_ip;
-      __syncthreads();
-      if (s_abort) return;
-      if (st.n > cp.max_ions) {
-        if (tid == 0) atomicOr(status, kStatusIonOverflow);
-        return;
-      }
-      // LIP::IonRMSCal(k, p): count 1 keeps the stale centroid (LIP.cpp:1125-1129)
-      if (st.n == 1) {
-        st.rms_x = fabs(X[0]);
-        st.rms_y = fabs(Y[0]);
-      } else if (st.n > 1) {
-        double s2[2] = {0.0, 0.0};
-        for (int i = tid; i < st.n; i += kChainThreads) {
-          s2[0] += X[i];
-          s2[1] += Y[i];
-        }
-        block_sum<2, kChainThreads>(s2, smem);
-        st.aver_x = s2[0] / st.n;
-        st.aver_y = s2[1] / st.n;
-        double q[2] = {0.0, 0.0};
-        for (int i = tid; i < st.n; i += kChainThreads) {
-          double dx = X[i] - st.aver_x, dy = Y[i] - st.aver_y;
-          q[0] = fma(dx, dx, q[0]);
-          q[1] = fma(dy, dy, q[1]);
-        }
-        block_sum<2, kChainThreads>(q, smem);
-        st.rms_x = sqrt(q[0] / st.n);
-        st.rms_y = sqrt(q[1] / st.n);
-      } else {
-        st.rms_x = 0;
-        st.rms_y = 0;
-      }
-      if (tid == 0) {
-        CloudRec r;
-        r.coeff = 2.0 * (st.macro_charge * st.n) * kElecClassicRadius / cp.r_gamma;
-        r.rms_x = st.rms_x;
-        r.rms_y = st.rms_y;
-        r.aver_x = st.aver_x;
-        r.aver_y = st.aver_y;
-        r.count = st.n;
-        rec[(size_t)j * P + p] = r;
-      }
-      // ion side: v += F, x += v C/h gap/c, then stable in-place removal of
-      // ions beyond the loss boundary (writes never pass the read position)
-      const double coeffI = 2.0 * ne * kElecClassicRadius * kElectronMassEV / kIonMassEV /
-                            cp.mass_number[p] * kCLight;
-      // two lanes per ion: the even lane evaluates w(z1), the odd lane w(z2)
-      const FieldPrep fp = field_prep(sx, sy);
-      const int half = tid & 1;
-      int out_base = 0;
-      for (int c0 = 0; c0 < st.n; c0 += kChainThreads / 2) {
-        int i = c0 + (tid >> 1);
-        bool keep = false;
-        double x = 0, y = 0, vx = 0, vy = 0;
-        double z1r = 0, z1i = 0, z2r = 0, z2i = 0;
-        if (i < st.n) {
-          x = X[i];
-          y = Y[i];
-          vx = VX[i];
-          vy = VY[i];
-          field_zargs(fp, x - mx, y - my, &z1r, &z1i, &z2r, &z2i);
-        }
-        cplx wm = half ? w_quadrant1_lowlat(z2r, z2i) : w_quadrant1_lowlat(z1r, z1i);
-        cplx wo = {__shfl_xor_sync(FULL_MASK, wm.re, 1), __shfl_xor_sync(FULL_MASK, wm.im, 1)};
-        if (i < st.n) {
-          double fx, fy;
-          field_finish(fp, x - mx, y - my, half ? wo : wm, half ? wm : wo, &fx, &fy);
-          vx += coeffI * fx;
-          vy += coeffI * fy;
-          x += vx * cp.circ_ring / cp.harmonics * gap / kCLight;
-          y += vy * cp.circ_ring / cp.harmonics * gap / kCLight;
-          keep = !(fabs(x) > bx || fabs(y) > by) && half == 0;
-        }
-        int tot;
-        int pos = block_excl_scan(keep ? 1 : 0, smem_i, &tot);  // syncs: all reads done
-        if (keep) {
-          X[out_base + pos] = x;
-          Y[out_base + pos] = y;
-          VX[out_base + pos] = vx;
-          VY[out_base + pos] = vy;
-        }
-        out_base += tot;
-        __syncthreads();
-      }
-      st.n = out_base;
-    }
-  }
-  // write the clouds back
-  for (int p = 0; p < P && p < PMAX; ++p) {
-    if (in_smem[p]) {
-      CloudDev cd = clouds[p];
-      for (int i = tid; i < stv[p].n; i += kChainThreads) {
-        cd.x[0][i] = AX[p][i];
-        cd.y[0][i] = AY[p][i];
-        cd.vx[0][i] = AVX[p][i];
-        cd.vy[0][i] = AVY[p][i];
-      }
-    }
-    if (tid == 0) {
-      stv[p].cur = 0;
-      cst[p] = stv[p];
-    }
-  }
-}
-
-// Block-wide exclusive scan of `keep` fused with the sums of four values over
-// the kept entries (fixed tree: deterministic).  Two barriers.
-__device__ __forceinline__ int scan_keep_sums(bool keep, const double v[4], int* s_cnt,
-                                              double* s_sum, int* total, double tot[4]) {
-  constexpr int NW = kChainThreads / 32;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  unsigned bal = __ballot_sync(FULL_MASK, keep);
-  int pre = __popc(bal & ((1u << lane) - 1u));
-  double w[4];
-#pragma unroll
-  for (int q = 0; q < 4; ++q) w[q] = keep ? v[q] : 0.0;
-  warp_sum<4>(w);
-  if (lane == 0) {
-    s_cnt[warp] = __popc(bal);
-#pragma unroll
-    for (int q = 0; q < 4; ++q) s_sum[q * NW + warp] = w[q];
-  }
-  __syncthreads();
-  int wpre = 0, t = 0;
-#pragma unroll
-  for (int u = 0; u < NW; ++u) {
-    int c = s_cnt[u];
-    wpre += (u < warp) ? c : 0;
-    t += c;
-  }
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    double acc = 0.0;
-#pragma unroll
-    for (int u = 0; u < NW; ++u) acc += s_sum[q * NW + u];
-    tot[q] = acc;
-  }
-  __syncthreads();
-  *total = t;
-  return wpre + pre;
-}
-
-// Single-species ion chain (the common case).  Everything that does not depend
-// on the cloud is computed for all bunches before the walk and kept in shared
-// memory: the birth positions (Philox attempts in order per bunch, as the
-// sequential draw), the bunch centroid/size/charge/gap and the prepared field
-// constants.  The walk keeps the cloud sums (sum x, y, x^2, y^2) up to date
-// from the compaction pass, so a bunch step is: append births, cloud rms from
-// the sums, record, one field-kick/drift/compaction pass with two lanes per
-// ion.  Three block barriers per bunch.
-__global__ void __launch_bounds__(kChainThreads) k_ion_chain1(
-    ChainParams cp, ChainSection cs, const BunchDev* __restrict__ bunch,
-    const BunchMomDev* __restrict__ mom, CloudDev* clouds, CloudState* cst, CloudRec* rec,
-    int* status, const int* __restrict__ d_turn, int k, int smem_cap) {
-  extern __shared__ double dsm[];
-  __shared__ double smem[4 * 32];
-  __shared__ int s_cnt[kChainThreads / 32];
-  __shared__ double s_sum[4 * (kChainThreads / 32)];
-  __shared__ double s_bx, s_by;
-  __shared__ int s_abort;
-  const int tid = threadIdx.x;
-  const int M = cp.n_bunches, NM = cp.macro_per_ip;
-  const uint32_t turn = (uint32_t)(*d_turn);
-  // shared layout: bunch data 6M | births 2 M NM | field constants | cloud 4 cap
-  double* sb = dsm;
-  double* BXn = sb + 6 * (size_t)M;
-  double* BYn = BXn + (size_t)M * NM;
-  FieldPrep* FP = reinterpret_cast<FieldPrep*>(BYn + (size_t)M * NM);
-  double* scl = reinterpret_cast<double*>(FP + M);
-  {
-    double mx = -INFINITY, my = -INFINITY;
-    for (int j = tid; j < M; j += kChainThreads) {
-      mx = fmax(mx, mom[j].rms_x);
-      my = fmax(my, mom[j].rms_y);
-    }
-    double mn = 0;
-    block_minmax<kChainThreads>(mn, mx, smem);
-    mn = 0;
-    block_minmax<kChainThreads>(mn, my, smem);
-    if (tid == 0) {
-      double lbx = cp.loss_boundary * mx, lby = cp.loss_boundary * my;
-      s_bx = cs.aperture_x > lbx ? lbx : cs.aperture_x;
-      s_by = cs.aperture_y > lby ? lby : cs.aperture_y;
-      s_abort = 0;
-    }
-  }
-  const uint32_t k0 = (uint32_t)cp.seed, k1 = (uint32_t)(cp.seed >> 32) ^ kStreamIonBirth;
-  for (int j = tid; j < M; j += kChainThreads) {
-    const double mx = mom[j].mean[0], my = mom[j].mean[2];
-    const double sx = mom[j].rms_x, sy = mom[j].rms_y;
-    sb[j] = mx;
-    sb[M + j] = my;
-    sb[2 * M + j] = sx;
-    sb[3 * M + j] = sy;
-    sb[4 * M + j] = bunch[j].ne;
-    sb[5 * M + j] = (double)bunch[j].gap;
-    FP[j] = field_prep(sx, sy);
-    int got = 0;
-    for (uint32_t a = 0; got < NM; ++a) {
-      if (a >= (1u << 20)) {
-        atomicOr(status, kStatusIonBirth);
-        s_abort = 1;
-        break;
-      }
-      u32x4 ctr = {{a, (uint32_t)j, turn, (uint32_t)(k * CG_MAX_SPECIES)}};
-      double g0, g1;
-      normal2(philox4x32_10(ctr, k0, k1), &g0, &g1);
-      double tx = mx + sx * g0, ty = my + sy * g1;
-      double ax = (tx - mx) / sx, ay = (ty - my) / sy;
-      if (ax * ax + ay * ay > 4.E0) continue;
-      BXn[(size_t)j * NM + got] = tx;
-      BYn[(size_t)j * NM + got] = ty;
-      got++;
-    }
-  }
-  CloudDev cd = clouds[0];
-  CloudState st = cst[0];
-  const bool in_smem = (long long)st.n + (long long)M * NM <= smem_cap;
-  double* X = in_smem ? scl : cd.x[0];
-  double* Y = in_smem ? scl + smem_cap : cd.y[0];
-  double* VX = in_smem ? scl + 2 * (size_t)smem_cap : cd.vx[0];
-  double* VY = in_smem ? scl + 3 * (size_t)smem_cap : cd.vy[0];
-  const int cap = in_smem ? smem_cap : cd.cap;
-  double S[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int i = tid; i < st.n; i += kChainThreads) {
-    double x = cd.x[0][i], y = cd.y[0][i];
-    if (in_smem) {
-      X[i] = x;
-      Y[i] = y;
-      VX[i] = cd.vx[0][i];
-      VY[i] = cd.vy[0][i];
-    }
-    S[0] += x;
-    S[1] += y;
-    S[2] = fma(x, x, S[2]);
-    S[3] = fma(y, y, S[3]);
-  }
-  block_sum<4, kChainThreads>(S, smem);  // also publishes the prologue's shared writes
-  if (s_abort) return;
-  const double bx = s_bx, by = s_by;
-  const double pressure = cp.gas_percent[0] * cs.pressure;
-  const int half = tid & 1;
-  const double drift = cp.circ_ring / cp.harmonics;
-
-  for (int j = 0; j < M; ++j) {
-    const double mx = sb[j], my = sb[M + j], ne = sb[4 * M + j];
-    const int gap = (int)sb[5 * M + j];
-    // LIP::GetIonNumberPerInterAction + IonGenerator charge (LIP.cpp:974-995)
-    const double line_density = cp.cross_section[0] * pressure / cs.temperature / kBoltzmann * ne;
-    st.macro_charge = line_density * cs.length / NM;
-    if (st.n + NM > cap) {
-      if (tid == 0) atomicOr(status, kStatusIonOverflow);
-      return;
-    }
-    // IonsUpdate: append the births (LIP.cpp:1021-1051)
-    for (int q = 0; q < NM; ++q) {
-      const double x = BXn[(size_t)j * NM + q], y = BYn[(size_t)j * NM + q];
-      if (tid == q % kChainThreads) {
-        X[st.n + q] = x;
-        Y[st.n + q] = y;
-        VX[st.n + q] = 0.0;
-        VY[st.n + q] = 0.0;
-      }
-      S[0] += x;
-      S[1] += y;
-      S[2] = fma(x, x, S[2]);
-      S[3] = fma(y, y, S[3]);
-    }
-    st.n += NM;
-    if (st.n > cp.max_ions) {
-      if (tid == 0) atomicOr(status, kStatusIonOverflow);
-      return;
-    }
-    __syncthreads();
-    // IonRMSCal (LIP.cpp:1113-1155); one ion keeps the stale centroid
-    if (st.n == 1) {
-      st.rms_x = fabs(X[0]);
-      st.rms_y = fabs(Y[0]);
-    } else {
-      st.aver_x = S[0] / st.n;
-      st.aver_y = S[1] / st.n;
-      st.rms_x = sqrt(fmax(S[2] / st.n - st.aver_x * st.aver_x, 0.0));
-      st.rms_y = sqrt(fmax(S[3] / st.n - st.aver_y * st.aver_y, 0.0));
-    }
-    if (tid == 0) {
-      CloudRec r;
-      r.coeff = 2.0 * (st.macro_charge * st.n) * kElecClassicRadius / cp.r_gamma;
-      r.rms_x = st.rms_x;
-      r.rms_y = st.rms_y;
-      r.aver_x = st.aver_x;
-      r.aver_y = st.aver_y;
-      r.count = st.n;
-      rec[j] = r;
-    }
-    // ion side and IonTransferDueToBunch, two lanes per ion
-    const double coeffI =
-        2.0 * ne * kElecClassicRadius * kElectronMassEV / kIonMassEV / cp.mass_number[0] * kCLight;
-    const FieldPrep& fp = FP[j];
-    int out_base = 0;
-    double Sn[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int c0 = 0; c0 < st.n; c0 += kChainThreads / 2) {
-      const int i = c0 + (tid >> 1);
-      bool keep = false;
-      double x = 0, y = 0, vx = 0, vy = 0;
-      double z1r = 0, z1i = 0, z2r = 0, z2i = 0;
-      if (i < st.n) {
-        x = X[i];
-        y = Y[i];
-        vx = VX[i];
-        vy = VY[i];
-        field_zargs(fp, x - mx, y - my, &z1r, &z1i, &z2r, &z2i);
-      }
-      cplx wm = half ? w_quadrant1_lowlat(z2r, z2i) : w_quadrant1_lowlat(z1r, z1i);
-      cplx wo = {__shfl_xor_sync(FULL_MASK, wm.re, 1), __shfl_xor_sync(FULL_MASK, wm.im, 1)};
-      if (i < st.n) {
-        double fx, fy;
-        field_finish(fp, x - mx, y - my, half ? wo : wm, half ? wm : wo, &fx, &fy);
-        vx += coeffI * fx;
-        vy += coeffI * fy;
-        x += vx * drift * gap / kCLight;
-        y += vy * drift * gap / kCLight;
-        keep = !(fabs(x) > bx || fabs(y) > by) && half == 0;
-      }
-      const double v4[4] = {x, y, x * x, y * y};
-      int tot;
-      double ts[4];
-      const int pos = scan_keep_sums(keep, v4, s_cnt, s_sum, &tot, ts);  // all reads done
-      if (keep) {
-        X[out_base + pos] = x;
-        Y[out_base + pos] = y;
-        VX[out_base + pos] = vx;
-        VY[out_base + pos] = vy;
-      }
-      out_base += tot;
-#pragma unroll
-      for (int q = 0; q < 4; ++q) Sn[q] += ts[q];
-    }
-    st.n = out_base;
-#pragma unroll
-    for (int q = 0; q < 4; ++q) S[q] = Sn[q];
-  }
-  __syncthreads();
-  if (in_smem)
-    for (int i = tid; i < st.n; i += kChainThreads) {
-      cd.x[0][i] = X[i];
-      cd.y[0][i] = Y[i];
-      cd.vx[0][i] = VX[i];
-      cd.vy[0][i] = VY[i];
-    }
-  if (tid == 0) {
-    st.cur = 0;
-    cst[0] = st;
-  }
-}
-
-// Shared memory of the chain kernels.  Single species, when the fixed part
-// fits in half the opt-in shared memory: per-bunch inputs (6 doubles), the
-// births (2 x macro ions per IP doubles) and the field constants of every
-// bunch, then the cloud (4 doubles per ion) in the rest.  Otherwise the
-// generic kernel: per-bunch inputs when at most 2048 bunches, plus as many
-// ions per species as fit in the remaining opt-in shared memory.
-struct ChainPlan {
-  int single;  // k_ion_chain1
-  int sb_ok, births_ok, cap;
-  size_t bytes;
-};
-
-static ChainPlan chain_smem_plan(const Handle& h) {
-  ChainPlan pl{};
-  int dev = 0, optin = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  const size_t budget = (size_t)optin - 4096;  // static shared memory of the kernels
-  const size_t M = (size_t)h.M, NM = (size_t)std::max(1, h.cfg.ion.macro_ions_per_ip);
-  const size_t fixed1 = 6 * sizeof(double) * M + 2 * sizeof(double) * M * NM + sizeof(FieldPrep) * M;
-  if (h.P == 1 && fixed1 <= budget / 2) {
-    pl.single = 1;
-    pl.sb_ok = pl.births_ok = 1;
-    pl.cap = (int)((budget - fixed1) / (4 * sizeof(double)));
-    pl.bytes = fixed1 + (size_t)pl.cap * 4 * sizeof(double);
-    return pl;
-  }
-  size_t sb = h.M <= 2048 ? 6 * sizeof(double) * M : 0;
-  pl.sb_ok = sb > 0;
-  size_t br = 2 * sizeof(double) * M * NM;
-  pl.births_ok = (h.P == 1 && sb + br <= budget / 2) ? 1 : 0;
-  if (!pl.births_ok) br = 0;
-  size_t rest = budget > sb + br ? budget - sb - br : 0;
-  pl.cap = (int)(rest / (4 * sizeof(double) * (size_t)h.P));
-  pl.bytes = sb + br + (size_t)pl.cap * 4 * sizeof(double) * h.P;
-  return pl;
-}
-
-// Opt-in shared memory of the chain kernels (set outside any graph capture).
-cudaError_t prepare_ion_chain(Handle& h) {
-  const ChainPlan pl = chain_smem_plan(h);
-  cudaError_t e = cudaFuncSetAttribute(pl.single ? (const void*)k_ion_chain1 : (const void*)k_ion_chain<1>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.bytes);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_ion_chain<CG_MAX_SPECIES>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.bytes);
-}
-
-cudaError_t launch_ion_chain(Handle& h, int k) {
-  ChainSection cs;
-  const cg_section& s = h.sections[k];
-  cs.pressure = s.pressure;
-  cs.temperature = s.temperature;
-  cs.length = s.length;
-  cs.aperture_x = s.aperture_x;
-  cs.aperture_y = s.aperture_y;
-  const ChainPlan pl = chain_smem_plan(h);
-  if (pl.single) {
-    k_ion_chain1<<<1, kChainThreads, pl.bytes, h.stream>>>(
-        h.chain, cs, h.d.bunch, h.d.mom, h.d.clouds + k, h.d.cloud_state + k,
-        h.d.rec + (size_t)k * h.M, h.d.status, h.d.turn, k, pl.cap);
-    return cudaGetLastError();
-  }
-  auto kern = h.P == 1 ? k_ion_chain<1> : k_ion_chain<CG_MAX_SPECIES>;
-  kern<<<1, kChainThreads, pl.bytes, h.stream>>>(
-      h.chain, cs, h.d.bunch, h.d.mom, h.d.clouds + (size_t)k * h.P, h.d.cloud_state + (size_t)k * h.P,
-      h.d.rec + (size_t)k * h.M * h.P, h.d.status, h.d.turn, k, pl.cap, pl.sb_ok, pl.births_ok);
   return cudaGetLastError();
 }
 
@@ -1365,7 +716,8 @@ cudaError_t measure_fp64_peak(double* flops) {
 }
 
 cudaError_t upload_weideman_table() {
-  return cudaMemcpyToSymbol(c_weideman, &h_weideman, sizeof(WeidemanTable));
+  cudaError_t e = cudaMemcpyToSymbol(c_weideman, &h_weideman, sizeof(WeidemanTable));
+  return e != cudaSuccess ? e : upload_weideman_table_ion();
 }
 
 // ---------------------------------------------------------------------------
@@ -1408,20 +760,18 @@ __global__ void __launch_bounds__(kTile, 2) k_moments_noalloc(const double* __re
   MomPartial* partials = reinterpret_cast<MomPartial*>(scratch);
   BunchMomDev* mom = reinterpret_cast<BunchMomDev*>(scratch + kNoAllocMomOff);
   unsigned* counter = reinterpret_cast<unsigned*>(scratch + kNoAllocCounterOff);
-  const int i = blockIdx.x * kTile + threadIdx.x;
-  double v[6] = {0, 0, 0, 0, 0, 0};
-  bool alive = false;
-  if (i < n) {
-    alive = surv[i] == kAlive;
+  double v[kMomChunkTiles][6];
+  bool alive[kMomChunkTiles];
 #pragma unroll
-    for (int d = 0; d < 6; ++d) v[d] = c[d * stride + i];
+  for (int u = 0; u < kMomChunkTiles; ++u) {
+    const int i = (blockIdx.x * kMomChunkTiles + u) * kTile + threadIdx.x;
+    const bool valid = i < n;
+    alive[u] = valid && surv[i] == kAlive;
+#pragma unroll
+    for (int d = 0; d < 6; ++d) v[u][d] = valid ? c[d * stride + i] : 0.0;
   }
-  tile_moment_partial(v, alive, smem, &partials[blockIdx.x]);
-  BunchDev B{};
-  B.n = n;
-  B.tile_off = 0;
-  B.n_tiles = (int)gridDim.x;
-  bunch_moment_finish(0, B, partials, counter, mom, beta_x, beta_y, c + 4 * stride, nullptr);
+  chunk_moment_partial(v, alive, smem, &partials[blockIdx.x]);
+  bunch_moment_finish(0, 0, (int)gridDim.x, partials, counter, mom, beta_x, beta_y, c + 4 * stride);
 }
 
 // Converts the finished moments into the public record (one thread; the
@@ -1452,8 +802,8 @@ __global__ void k_moments_noalloc_out(const double* __restrict__ scratch, int n,
 cudaError_t launch_moments_noalloc(const double* c, int64_t stride, const uint8_t* surv, int n,
                                    double beta_x, double beta_y, double* scratch,
                                    cg_bunch_moments* out, cudaStream_t s) {
-  const int tiles = (n + kTile - 1) / kTile;
-  k_moments_noalloc<<<tiles, kTile, 0, s>>>(c, stride, surv, n, beta_x, beta_y, scratch);
+  const int chunks = (n + kTile * kMomChunkTiles - 1) / (kTile * kMomChunkTiles);
+  k_moments_noalloc<<<chunks, kTile, 0, s>>>(c, stride, surv, n, beta_x, beta_y, scratch);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   k_moments_noalloc_out<<<1, 1, 0, s>>>(scratch, n, out);

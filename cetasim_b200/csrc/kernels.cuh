@@ -15,7 +15,7 @@ enum : int {
 cudaError_t launch_moments(Handle& h, int k);
 cudaError_t launch_map(Handle& h, int k);
 cudaError_t launch_ion_chain(Handle& h, int k);
-cudaError_t prepare_ion_chain(Handle& h);
+int ion_walk_grid(int64_t tcap);
 cudaError_t launch_ion_kick(Handle& h, int k);
 enum LongFlags : unsigned {
   kLongRF = 1,
@@ -37,7 +37,8 @@ cudaError_t launch_faddeeva(const double* zr, const double* zi, double* wr, doub
                             bool general, cudaStream_t s);
 cudaError_t launch_field(const double* x, const double* y, const double* sx, const double* sy,
                          double* fx, double* fy, int64_t n, cudaStream_t s);
-cudaError_t upload_weideman_table();
+cudaError_t upload_weideman_table();      // every translation unit that evaluates w(z)
+cudaError_t upload_weideman_table_ion();
 
 // Moments of one bunch held in the caller's device buffers, with the partials
 // in a fixed file-scope device array (no allocation).  At most

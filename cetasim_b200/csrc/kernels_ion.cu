@@ -1,0 +1,411 @@
+// Ion chain of one interaction point (MPBeam::SSBeamIonEffectOneInteraction
+// Point, MPBeam.cpp:2585-2611) as independent ion trajectories.
+//
+// In the reference, bunch j of the train meets the cloud the previous bunches
+// left behind: macro-ions are born (LIP::IonGenerator, LIP.cpp:985-1019) and
+// appended (IonsUpdate, :1021-1051), the cloud's moments are taken
+// (IonRMSCal, :1113-1155) for the electron-side kick, every ion is kicked by
+// the field of bunch j (MPBunch.cpp:1111-1157), drifts over the gap to the
+// next bunch and is erased beyond the loss bound (IonTransferDueToBunch,
+// LIP.cpp:1158-1211).  The ions never act on one another: an ion's motion
+// depends only on the bunches it meets, whose centroids and sizes are fixed
+// for the call, and the loss bound min(aperture, boundary * max sigma) is
+// fixed for the call too (MPBeam.cpp:2257).  So the chain is a set of
+// independent trajectories - the ions already in the cloud, then the ions
+// born at bunch j, in the reference's order - and the only quantities that
+// couple them are the cloud moments each bunch sees, which are per-step sums
+// over the ions alive at that step.
+//
+// Three kernels per IP:
+//   k_ion_prep    per bunch: loss bounds, birth positions (Philox, attempts in
+//                 order), field constants, coefficients;
+//   k_ion_walk    each CTA walks 128 trajectories (two lanes per ion: the even
+//                 lane evaluates w(z1), the odd one w(z2)) through all bunches
+//                 without a barrier per bunch, and writes per-step partial
+//                 sums (count, sum x, y, x^2, y^2) every kWin bunches;
+//   k_ion_finish  per step: sums in CTA order -> cloud centroid and rms ->
+//                 the record the electron kick reads; stable compaction of the
+//                 survivors into the cloud (birth order, as the reference's
+//                 erase keeps it).
+// The critical path is one field evaluation per bunch passage of the longest
+// trajectory, instead of a block-synchronised cloud pass per bunch.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include "kernels.cuh"
+
+namespace cg {
+
+#define FULL_MASK 0xffffffffu
+
+constexpr int kWalkIons = 128;                 // trajectories per CTA block
+constexpr int kWalkThreads = 2 * kWalkIons;    // two lanes per ion
+constexpr int kWin = 16;                       // steps per shared-memory window
+constexpr int kGroups = kWalkThreads / kWin;   // ion groups summed per step
+constexpr int kGroupIons = kWalkIons / kGroups;
+static_assert(kGroups * kGroupIons == kWalkIons, "ion groups tile the block");
+constexpr int kPrepThreads = 128;
+constexpr int kFinishThreads = 1024;
+constexpr int kFinishChunk = 2048;             // steps per shared-memory chunk
+
+__device__ __forceinline__ void warp_max2(double& a, double& b) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a = fmax(a, __shfl_xor_sync(FULL_MASK, a, o));
+    b = fmax(b, __shfl_xor_sync(FULL_MASK, b, o));
+  }
+}
+
+// Loss bounds, births and per-bunch constants for one IP.
+__global__ void __launch_bounds__(kPrepThreads) k_ion_prep(ChainParams cp, ChainSection cs,
+                                                         const BunchDev* __restrict__ bunch,
+                                                         const BunchMomDev* __restrict__ mom,
+                                                         IonWalk w, int* status,
+                                                         const int* __restrict__ d_turn, int k) {
+  __shared__ double s_mx[kPrepThreads / 32], s_my[kPrepThreads / 32];
+  const int tid = threadIdx.x, M = cp.n_bunches, NM = cp.macro_per_ip, P = cp.n_species;
+  if (blockIdx.x == 0) {
+    // MPGetBeamInfo: bunchSizeXMax / YMax (MPBeam.cpp:2175-2186); the maximum
+    // does not depend on the order of comparison
+    double mx = -INFINITY, my = -INFINITY;
+    for (int j = tid; j < M; j += kPrepThreads) {
+      mx = fmax(mx, mom[j].rms_x);
+      my = fmax(my, mom[j].rms_y);
+    }
+    warp_max2(mx, my);
+    if ((tid & 31) == 0) {
+      s_mx[tid >> 5] = mx;
+      s_my[tid >> 5] = my;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      for (int u = 1; u < kPrepThreads / 32; ++u) {
+        mx = fmax(mx, s_mx[u]);
+        my = fmax(my, s_my[u]);
+      }
+      const double lbx = cp.loss_boundary * mx, lby = cp.loss_boundary * my;
+      w.bound[0] = cs.aperture_x > lbx ? lbx : cs.aperture_x;  // LIP.cpp:1172-1181
+      w.bound[1] = cs.aperture_y > lby ? lby : cs.aperture_y;
+    }
+  }
+  const int j = blockIdx.x * kPrepThreads + tid;
+  if (j >= M) return;
+  const double mx = mom[j].mean[0], my = mom[j].mean[2];
+  const double sx = mom[j].rms_x, sy = mom[j].rms_y;
+  const double ne = bunch[j].ne;
+  w.prep[j] = field_prep(sx, sy);
+  w.bunch[3 * j + 0] = mx;
+  w.bunch[3 * j + 1] = my;
+  // drift time to the next bunch: gap * C/h / c (LIP.cpp:1172-1173)
+  w.bunch[3 * j + 2] = cp.circ_ring / cp.harmonics * bunch[j].gap / kCLight;
+  const uint32_t turn = (uint32_t)(*d_turn);
+  const uint32_t k0 = (uint32_t)cp.seed, k1 = (uint32_t)(cp.seed >> 32) ^ kStreamIonBirth;
+  for (int p = 0; p < P; ++p) {
+    // LIP::GetIonNumberPerInterAction (LIP.cpp:974-982) and the macro-ion
+    // charge of IonGenerator (LIP.cpp:985-995)
+    const double press_p = cp.gas_percent[p] * cs.pressure;
+    const double line_density = cp.cross_section[p] * press_p / cs.temperature / kBoltzmann * ne;
+    const double ion_number = line_density * cs.length;
+    w.spec[2 * ((size_t)p * M + j) + 0] = ion_number / NM;
+    // ion-side coefficient 2 N_e r_e (m_e / m_ion A) c (MPBunch.cpp:1117)
+    w.spec[2 * ((size_t)p * M + j) + 1] =
+        2.0 * ne * kElecClassicRadius * kElectronMassEV / kIonMassEV / cp.mass_number[p] * kCLight;
+    // births: Gaussian around the bunch centroid with the bunch sizes,
+    // rejected beyond r^2 > 4 (LIP.cpp:1000-1016); attempt a of bunch j, IP k,
+    // species p draws Philox({a, j, turn, 8k + p})
+    double* out = w.births + 2 * ((size_t)p * M + j) * NM;
+    int got = 0;
+    for (uint32_t a = 0; got < NM; ++a) {
+      if (a >= (1u << 20)) {  // a degenerate bunch size would reject forever
+        atomicOr(status, kStatusIonBirth);
+        for (; got < NM; ++got) out[2 * got] = out[2 * got + 1] = 0.0;
+        break;
+      }
+      u32x4 ctr = {{a, (uint32_t)j, turn, (uint32_t)(k * CG_MAX_SPECIES + p)}};
+      double g0, g1;
+      normal2(philox4x32_10(ctr, k0, k1), &g0, &g1);
+      const double tx = mx + sx * g0, ty = my + sy * g1;
+      const double ax = (tx - mx) / sx, ay = (ty - my) / sy;
+      if (ax * ax + ay * ay > 4.E0) continue;
+      out[2 * got] = tx;
+      out[2 * got + 1] = ty;
+      got++;
+    }
+  }
+}
+
+// One CTA block = 128 trajectories: index t < n0 is ion t of the cloud the
+// previous call left, t >= n0 the ion born as number (t - n0) % NM at bunch
+// (t - n0) / NM.  blockIdx.y = species.  The step loop has no block barrier:
+// each ion's position at each step goes to a shared-memory window of kWin
+// steps, and after each window the CTA sums it per step in a fixed order
+// (groups of 8 ions, then the 16 groups) into the per-step partials.
+__global__ void __launch_bounds__(kWalkThreads, 1) k_ion_walk(ChainParams cp, IonWalk w,
+                                                         const CloudDev* __restrict__ clouds,
+                                                         const CloudState* __restrict__ cst) {
+  __shared__ double s_x[kWin][kWalkIons], s_y[kWin][kWalkIons];
+  __shared__ uint8_t s_act[kWin][kWalkIons];
+  __shared__ double s_grp[kWin][kGroups][5];
+  const int p = blockIdx.y, G = gridDim.x, c = blockIdx.x;
+  const int M = cp.n_bunches, NM = cp.macro_per_ip;
+  const int n0 = cst[p].n;
+  const int64_t T = (int64_t)n0 + (int64_t)M * NM;
+  const int nblk = (int)((T + kWalkIons - 1) / kWalkIons);
+  if (c >= nblk) return;
+  const int tid = threadIdx.x, half = tid & 1, slot = tid >> 1;
+  const CloudDev cd = clouds[p];
+  const double bx = w.bound[0], by = w.bound[1];
+  const double* births = w.births + 2 * (size_t)p * M * NM;
+  const double* spec = w.spec + 2 * (size_t)p * M;
+  double* part = w.part + (size_t)p * M * G * 5;
+  double* traj = w.traj + (size_t)p * 4 * w.tcap;
+  uint8_t* alive_out = w.alive + (size_t)p * w.tcap;
+  bool first = true;
+  for (int blk = c; blk < nblk; blk += G, first = false) {
+    const int64_t t = (int64_t)blk * kWalkIons + slot;
+    const int64_t tb = (int64_t)blk * kWalkIons;
+    const int jfirst = tb < n0 ? 0 : (int)((tb - n0) / NM);
+    if (first && tid < 5)
+      for (int j = 0; j < jfirst; ++j) part[((size_t)j * G + c) * 5 + tid] = 0.0;
+    bool alive = t < T;
+    int j0 = 0;
+    double x = 0, y = 0, vx = 0, vy = 0;
+    if (alive) {
+      if (t < n0) {
+        x = cd.x[0][t];
+        y = cd.y[0][t];
+        vx = cd.vx[0][t];
+        vy = cd.vy[0][t];
+      } else {
+        const int64_t b = t - n0;
+        j0 = (int)(b / NM);
+        x = births[2 * b];
+        y = births[2 * b + 1];
+      }
+    }
+    for (int jw = jfirst; jw < M; jw += kWin) {
+      const int nw = min(kWin, M - jw);
+      for (int s = 0; s < nw; ++s) {
+        const int j = jw + s;
+        const bool active = alive && j >= j0;
+        // the cloud bunch j sees: ions alive after the births of bunch j
+        if (half == 0) {
+          s_x[s][slot] = x;
+          s_y[s][slot] = y;
+          s_act[s][slot] = active ? 1 : 0;
+        }
+        // ion side of MPBunch::SSIonBunchInteraction and the drift/loss of
+        // LIP::IonTransferDueToBunch
+        if (__any_sync(FULL_MASK, active)) {
+          const FieldPrep fp = w.prep[j];
+          const double mx = w.bunch[3 * j], my = w.bunch[3 * j + 1], dt = w.bunch[3 * j + 2];
+          const double coeffI = spec[2 * j + 1];
+          double z1r = 0, z1i = 0, z2r = 0, z2i = 0;
+          if (active) field_zargs(fp, x - mx, y - my, &z1r, &z1i, &z2r, &z2i);
+          const cplx wm = half ? w_quadrant1_lowlat(z2r, z2i) : w_quadrant1_lowlat(z1r, z1i);
+          const cplx wo = {__shfl_xor_sync(FULL_MASK, wm.re, 1),
+                           __shfl_xor_sync(FULL_MASK, wm.im, 1)};
+          if (active) {
+            double fx, fy;
+            field_finish(fp, x - mx, y - my, half ? wo : wm, half ? wm : wo, &fx, &fy);
+            vx += coeffI * fx;
+            vy += coeffI * fy;
+            x += vx * dt;
+            y += vy * dt;
+            alive = !(fabs(x) > bx || fabs(y) > by);
+          }
+        }
+      }
+      __syncthreads();
+      {  // per step and group of 8 ions: (count, sum x, sum y, sum x^2, sum y^2)
+        const int s = tid / kGroups, g = tid % kGroups;
+        if (s < nw) {
+          double a[5] = {0, 0, 0, 0, 0};
+          for (int i = g * kGroupIons; i < (g + 1) * kGroupIons; ++i) {
+            if (!s_act[s][i]) continue;
+            const double xi = s_x[s][i], yi = s_y[s][i];
+            a[0] += 1.0;
+            a[1] += xi;
+            a[2] += yi;
+            a[3] += xi * xi;
+            a[4] += yi * yi;
+          }
+#pragma unroll
+          for (int q = 0; q < 5; ++q) s_grp[s][g][q] = a[q];
+        }
+      }
+      __syncthreads();
+      if (tid < 5 * nw) {
+        const int s = tid / 5, q = tid % 5;
+        double a = 0.0;
+#pragma unroll
+        for (int g = 0; g < kGroups; ++g) a += s_grp[s][g][q];
+        double* dst = part + ((size_t)(jw + s) * G + c) * 5 + q;
+        *dst = first ? a : *dst + a;
+      }
+    }
+    if (t < T && half == 0) {
+      traj[t] = x;
+      traj[w.tcap + t] = y;
+      traj[2 * w.tcap + t] = vx;
+      traj[3 * w.tcap + t] = vy;
+      alive_out[t] = alive ? 1 : 0;
+    }
+    __syncthreads();  // shared windows reused by the next block of this CTA
+  }
+}
+
+// Records and cloud update, one CTA per species.
+__global__ void __launch_bounds__(kFinishThreads) k_ion_finish(ChainParams cp, IonWalk w,
+                                                             CloudDev* clouds, CloudState* cst,
+                                                             CloudRec* rec, int* status, int G) {
+  __shared__ double s_ax[kFinishChunk], s_ay[kFinishChunk];
+  __shared__ int s_n[kFinishChunk];
+  __shared__ int s_wsum[kFinishThreads / 32];
+  __shared__ double s_carry[2];
+  __shared__ int s_base;
+  const int p = blockIdx.x, P = cp.n_species, tid = threadIdx.x;
+  const int M = cp.n_bunches, NM = cp.macro_per_ip;
+  const CloudState st0 = cst[p];
+  const int64_t T = (int64_t)st0.n + (int64_t)M * NM;
+  const int nblk = (int)((T + kWalkIons - 1) / kWalkIons);
+  const int nwork = nblk < G ? nblk : G;
+  const double* part = w.part + (size_t)p * M * G * 5;
+  const double* spec = w.spec + 2 * (size_t)p * M;
+  if (tid == 0) {
+    s_carry[0] = st0.aver_x;
+    s_carry[1] = st0.aver_y;
+  }
+  double last_rms_x = st0.rms_x, last_rms_y = st0.rms_y;
+  for (int j0 = 0; j0 < M; j0 += kFinishChunk) {
+    const int nj = min(kFinishChunk, M - j0);
+    __syncthreads();
+    for (int jj = tid; jj < nj; jj += kFinishThreads) {
+      const int j = j0 + jj;
+      double s[5] = {0, 0, 0, 0, 0};
+      for (int cc = 0; cc < nwork; ++cc)
+#pragma unroll
+        for (int q = 0; q < 5; ++q) s[q] += part[((size_t)j * G + cc) * 5 + q];
+      const int n = (int)s[0];
+      double ax = 0, ay = 0, rx, ry;
+      if (n == 1) {  // one ion: rms = |x| and the centroid stays (LIP.cpp:1125-1129)
+        rx = fabs(s[1]);
+        ry = fabs(s[2]);
+      } else {
+        const double inv_n = 1.0 / n;
+        ax = s[1] * inv_n;
+        ay = s[2] * inv_n;
+        rx = sqrt(fmax(s[3] * inv_n - ax * ax, 0.0));
+        ry = sqrt(fmax(s[4] * inv_n - ay * ay, 0.0));
+      }
+      if (n > cp.max_ions) atomicOr(status, kStatusIonOverflow);  // LIP.cpp:1043-1048
+      s_n[jj] = n;
+      s_ax[jj] = ax;
+      s_ay[jj] = ay;
+      CloudRec r;
+      r.coeff = 2.0 * (spec[2 * j] * n) * kElecClassicRadius / cp.r_gamma;
+      r.rms_x = rx;
+      r.rms_y = ry;
+      r.count = n;
+      rec[(size_t)j * P + p] = r;  // centroid filled below
+    }
+    __syncthreads();
+    if (tid == 0) {  // the stale-centroid carry is sequential
+      double cx = s_carry[0], cy = s_carry[1];
+      for (int jj = 0; jj < nj; ++jj) {
+        if (s_n[jj] == 1) {
+          s_ax[jj] = cx;
+          s_ay[jj] = cy;
+        } else {
+          cx = s_ax[jj];
+          cy = s_ay[jj];
+        }
+      }
+      s_carry[0] = cx;
+      s_carry[1] = cy;
+    }
+    __syncthreads();
+    for (int jj = tid; jj < nj; jj += kFinishThreads) {
+      CloudRec* r = rec + (size_t)(j0 + jj) * P + p;
+      r->aver_x = s_ax[jj];
+      r->aver_y = s_ay[jj];
+    }
+    if (j0 + nj == M) {
+      const CloudRec* r = rec + (size_t)(M - 1) * P + p;
+      __syncthreads();
+      last_rms_x = r->rms_x;
+      last_rms_y = r->rms_y;
+    }
+  }
+  // survivors in trajectory order -> cloud buffer 0
+  CloudDev cd = clouds[p];
+  const double* traj = w.traj + (size_t)p * 4 * w.tcap;
+  const uint8_t* al = w.alive + (size_t)p * w.tcap;
+  if (tid == 0) s_base = 0;
+  __syncthreads();
+  const int lane = tid & 31, warp = tid >> 5;
+  for (int64_t t0 = 0; t0 < T; t0 += kFinishThreads) {
+    const int64_t t = t0 + tid;
+    const bool keep = t < T && al[t];
+    const unsigned bal = __ballot_sync(FULL_MASK, keep);
+    if (lane == 0) s_wsum[warp] = __popc(bal);
+    __syncthreads();
+    int pre = s_base, tot = 0;
+    for (int u = 0; u < kFinishThreads / 32; ++u) {
+      pre += u < warp ? s_wsum[u] : 0;
+      tot += s_wsum[u];
+    }
+    pre += __popc(bal & ((1u << lane) - 1u));
+    if (keep && pre < cd.cap) {
+      cd.x[0][pre] = traj[t];
+      cd.y[0][pre] = traj[w.tcap + t];
+      cd.vx[0][pre] = traj[2 * w.tcap + t];
+      cd.vy[0][pre] = traj[3 * w.tcap + t];
+    }
+    __syncthreads();
+    if (tid == 0) s_base += tot;
+    __syncthreads();
+  }
+  if (tid == 0) {
+    CloudState st;
+    st.n = s_base < cd.cap ? s_base : cd.cap;
+    if (s_base > cd.cap) atomicOr(status, kStatusIonOverflow);
+    st.cur = 0;
+    st.aver_x = s_carry[0];
+    st.aver_y = s_carry[1];
+    st.rms_x = last_rms_x;
+    st.rms_y = last_rms_y;
+    st.macro_charge = spec[2 * (M - 1)];
+    cst[p] = st;
+  }
+}
+
+cudaError_t launch_ion_chain(Handle& h, int k) {
+  ChainSection cs;
+  const cg_section& s = h.sections[k];
+  cs.pressure = s.pressure;
+  cs.temperature = s.temperature;
+  cs.length = s.length;
+  cs.aperture_x = s.aperture_x;
+  cs.aperture_y = s.aperture_y;
+  const int M = h.M;
+  k_ion_prep<<<(M + kPrepThreads - 1) / kPrepThreads, kPrepThreads, 0, h.stream>>>(
+      h.chain, cs, h.d.bunch, h.d.mom, h.d.iw, h.d.status, h.d.turn, k);
+  dim3 grid(h.d.iw.grid, h.P);
+  k_ion_walk<<<grid, kWalkThreads, 0, h.stream>>>(h.chain, h.d.iw, h.d.clouds + (size_t)k * h.P,
+                                                  h.d.cloud_state + (size_t)k * h.P);
+  k_ion_finish<<<h.P, kFinishThreads, 0, h.stream>>>(
+      h.chain, h.d.iw, h.d.clouds + (size_t)k * h.P, h.d.cloud_state + (size_t)k * h.P,
+      h.d.rec + (size_t)k * h.M * h.P, h.d.status, h.d.iw.grid);
+  return cudaGetLastError();
+}
+
+cudaError_t upload_weideman_table_ion() {
+  return cudaMemcpyToSymbol(c_weideman, &h_weideman, sizeof(WeidemanTable));
+}
+
+int ion_walk_grid(int64_t tcap) {
+  const int64_t blocks = (tcap + kWalkIons - 1) / kWalkIons;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(blocks, 148 * 4));
+}
+
+}  // namespace cg
