@@ -252,6 +252,12 @@ def main():
     beam._check(lib.cg_time_stage(beam.h, 0, 0, 20, C.byref(map_ms)))
     chain_ms = C.c_double()
     beam._check(lib.cg_time_stage(beam.h, 2, 0, 5, C.byref(chain_ms)))
+    mom_ms = C.c_double()
+    beam._check(lib.cg_time_stage(beam.h, 3, 0, 20, C.byref(mom_ms)))
+    pass_ms = C.c_double()
+    beam._check(lib.cg_time_stage(beam.h, 5, 0, 20, C.byref(pass_ms)))
+    tail_ms = C.c_double()
+    beam._check(lib.cg_time_stage(beam.h, 4, 0, 5, C.byref(tail_ms)))
     peak = C.c_double()
     lib.cg_fp64_peak(C.byref(peak))
     flops_per_kick = FLOPS_PER_KICK
@@ -282,7 +288,9 @@ def main():
                        "parallelism": f"replica x{world}"},
             "ion_kicks_per_s": world * ion_kicks_turn * args.steps / (tot_ms * 1e-3),
             "kernels_ms": {"ion_field_kick": kick_ms.value, "section_map": map_ms.value,
-                           "ion_chain": chain_ms.value},
+                           "moments": mom_ms.value, "ion_chain": chain_ms.value,
+                           "map_moments_pass": pass_ms.value,
+                           "longitudinal_tail": tail_ms.value},
             "roofline": {"bound": "fp64", "kernel": "k_ion_kick (electron-side Bassetti-Erskine)",
                          "achieved": achieved / 1e12, "peak": peak.value / 1e12, "unit": "TFLOP/s",
                          "frac": achieved / peak.value if peak.value else None,

@@ -145,6 +145,16 @@ CG_HD void field_finish(const FieldPrep& p, double posx, double posy, cplx w1, c
   }
 }
 
+// The same with the kick kernels' w(z) (w_quadrant1_wide).
+CG_HD void gaussian_field_kick(const FieldPrep& p, double posx, double posy, double* fx,
+                               double* fy) {
+  double z1r, z1i, z2r, z2i;
+  field_zargs(p, posx, posy, &z1r, &z1i, &z2r, &z2i);
+  cplx w1 = w_quadrant1_wide(z1r, z1i);
+  cplx w2 = w_quadrant1_wide(z2r, z2i);
+  field_finish(p, posx, posy, w1, w2, fx, fy);
+}
+
 template <bool LowLat = false>
 CG_HD void gaussian_field_prep(const FieldPrep& p, double posx, double posy, double* fx,
                                double* fy) {

@@ -143,6 +143,9 @@ SectionDev make_section_dev(const cg_section& s, const cg_ring& r) {
   d.phase_adv_x = s.phase_adv_x; d.phase_adv_y = s.phase_adv_y;
   d.weigh_x = s.phase_adv_x / (2 * kPi * r.work_qx);
   d.weigh_y = s.phase_adv_y / (2 * kPi * r.work_qy);
+  d.cos_x = std::cos(s.phase_adv_x); d.sin_x = std::sin(s.phase_adv_x);
+  d.cos_y = std::cos(s.phase_adv_y); d.sin_y = std::sin(s.phase_adv_y);
+  d.inv_beta_x = 1.0 / s.beta_x; d.inv_beta_y = 1.0 / s.beta_y;
   d.aperture_x = s.aperture_x; d.aperture_y = s.aperture_y;
   std::memcpy(d.b1h1, s.map_b1h1, sizeof d.b1h1);
   std::memcpy(d.h1b1, s.map_h1b1, sizeof d.h1b1);
@@ -522,6 +525,10 @@ int cg_set_beam(cg_handle* H, int M, const int* n_macro, const int* harm, const 
   cudaMemset(d.surv, 0xFF, h.npad);
   cudaMemcpy(d.tile_bunch, tb.data(), sizeof(int) * tiles, cudaMemcpyHostToDevice);
   cudaMemcpy(d.chunk_bunch, cb.data(), sizeof(int) * chunks, cudaMemcpyHostToDevice);
+  if (cudaError_t pe = prepare_ip_pass()) {
+    free_beam(h);
+    return cuda_fail(&h, pe, "particle pass shared memory");
+  }
   cudaMemcpy(d.bunch, bd.data(), sizeof(BunchDev) * M, cudaMemcpyHostToDevice);
   cudaMemset(d.counters, 0, sizeof(unsigned) * (M + 1));
   cudaMemset(d.loss_count, 0, sizeof(int) * (M + 1));
@@ -772,16 +779,20 @@ int cg_mark_lost(cg_handle* H, double* trans) {
 static cudaError_t enqueue_turn(Handle& h) {
   const cg_config& c = h.cfg;
   cudaError_t e;
+  // per IP: ion chain, electron-side kick, then one particle pass with the map
+  // and the moments the next stage reads (those of IP k+1 for its ion chain;
+  // after the last IP those of section K-1 for the wakes, MPBeam.cpp:1069)
+  const bool post = c.flag_lr_wake || c.flag_sr_wake;
+  if (c.flag_beam_ion && (e = launch_moments(h, 0))) return e;
   for (int k = 0; k < h.K; ++k) {
     if (c.flag_beam_ion) {
-      if ((e = launch_moments(h, k))) return e;
       if ((e = launch_ion_chain(h, k))) return e;
       if ((e = launch_ion_kick(h, k))) return e;
     }
-    if ((e = launch_map(h, k))) return e;
-  }
-  if (c.flag_lr_wake || c.flag_sr_wake) {
-    if ((e = launch_moments(h, h.K - 1))) return e;
+    int mom = -1;
+    if (k + 1 < h.K) mom = c.flag_beam_ion ? k + 1 : -1;
+    else mom = post ? h.K - 1 : -1;
+    if ((e = launch_ip_pass(h, k, false, mom))) return e;
   }
   if (c.flag_lr_wake && (e = launch_lr_compute(h))) return e;
   unsigned fl = kLongRF | kLongDrift | kLongLoss;
@@ -839,9 +850,8 @@ void* cg_stream(cg_handle* H) { return H ? (void*)H->h.stream : nullptr; }
 
 static int count_turn_launches(Handle& h) {
   const cg_config& c = h.cfg;
-  int n = h.K;                                   // maps
-  if (c.flag_beam_ion) n += 3 * h.K;             // moments + chain + kick per IP
-  if (c.flag_lr_wake || c.flag_sr_wake) n += 1;  // post-map moments
+  int n = h.K;                                   // map + moments passes
+  if (c.flag_beam_ion) n += 1 + 4 * h.K;         // moments at IP 0 + prep/walk/finish/kick per IP
   if (c.flag_lr_wake) n += 2;                    // push + forces
   n += 1;                                        // longitudinal tail
   if (c.flag_sr_wake) n += 5;
@@ -859,7 +869,7 @@ int cg_turn_launches(cg_handle* H, int* launches) {
 int cg_time_stage(cg_handle* H, int stage, int k, int reps, double* ms) {
   STAGE_PROLOGUE
   if (k < 0 || k >= h.K || reps < 1 || !ms) return fail(&h, CG_ERR_INVALID, "bad arguments");
-  if ((stage == 1 || stage == 2) && !h.cfg.flag_beam_ion)
+  if ((stage == 1 || stage == 2 || stage == 5) && !h.cfg.flag_beam_ion)
     return fail(&h, CG_ERR_NOT_READY, "runBeamIonFlag is off");
   cudaEvent_t e0, e1;
   CG_CUDA(&h, cudaEventCreate(&e0));
@@ -872,6 +882,7 @@ int cg_time_stage(cg_handle* H, int stage, int k, int reps, double* ms) {
       case 1: e = launch_ion_kick(h, k); break;
       case 2: e = launch_ion_chain(h, k); break;
       case 3: e = launch_moments(h, k); break;
+      case 5: e = launch_ip_pass(h, k, false, k); break;
       default: e = launch_long(h, kLongRF | kLongDrift | kLongLoss | (h.cfg.flag_synrad ? kLongSynrad : 0));
     }
   }

@@ -201,6 +201,22 @@ CG_HD cplx w_quadrant1_lowlat(double x, double y) {
   return w;
 }
 
+// The kick kernels' first-quadrant path: Weideman's expansion up to |z| = 30,
+// where it stays within 3e-14 of w relative to |w| (the real-axis region
+// included), the continued fraction beyond.  Beam particles and ions sit
+// within a few tens of sigma of the other beam, so every lane of a warp takes
+// the same branch and the two w(z) of a kick do not diverge.
+CG_HD cplx w_quadrant1_wide(double x, double y) {
+  double r2 = fma(x, x, y * y);
+  if (r2 < 900.0) return w_weideman(x, y);
+  return w_cfrac<8>(x, y);
+}
+CG_HD cplx w_quadrant1_wide_lowlat(double x, double y) {
+  double r2 = fma(x, x, y * y);
+  if (r2 < 900.0) return w_weideman_estrin(x, y);
+  return w_cfrac<8>(x, y);
+}
+
 // Near-real-axis strip (0 <= y < 0.5): shifted trapezoidal rule for
 // (i/pi) Int exp(-t^2)/(z - t) dt plus the residue of the pole at t = z
 // (Chiarella & Reichel 1968; Matta & Reichel 1971).  Every term of the real

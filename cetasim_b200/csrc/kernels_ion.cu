@@ -145,6 +145,8 @@ __global__ void __launch_bounds__(kWalkThreads, 1) k_ion_walk(ChainParams cp, Io
   __shared__ double s_x[kWin][kWalkIons], s_y[kWin][kWalkIons];
   __shared__ uint8_t s_act[kWin][kWalkIons];
   __shared__ double s_grp[kWin][kGroups][5];
+  __shared__ FieldPrep s_fp[kWin];
+  __shared__ double s_bc[kWin][4];  // mean x, mean y, drift time, ion coefficient
   const int p = blockIdx.y, G = gridDim.x, c = blockIdx.x;
   const int M = cp.n_bunches, NM = cp.macro_per_ip;
   const int n0 = cst[p].n;
@@ -184,6 +186,17 @@ __global__ void __launch_bounds__(kWalkThreads, 1) k_ion_walk(ChainParams cp, Io
     }
     for (int jw = jfirst; jw < M; jw += kWin) {
       const int nw = min(kWin, M - jw);
+      // the window's bunch constants in shared memory (global loads would sit
+      // on the latency chain of every step)
+      if (tid < nw) {
+        const int j = jw + tid;
+        s_fp[tid] = w.prep[j];
+        s_bc[tid][0] = w.bunch[3 * j];
+        s_bc[tid][1] = w.bunch[3 * j + 1];
+        s_bc[tid][2] = w.bunch[3 * j + 2];
+        s_bc[tid][3] = spec[2 * j + 1];
+      }
+      __syncthreads();
       for (int s = 0; s < nw; ++s) {
         const int j = jw + s;
         const bool active = alive && j >= j0;
@@ -196,12 +209,11 @@ __global__ void __launch_bounds__(kWalkThreads, 1) k_ion_walk(ChainParams cp, Io
         // ion side of MPBunch::SSIonBunchInteraction and the drift/loss of
         // LIP::IonTransferDueToBunch
         if (__any_sync(FULL_MASK, active)) {
-          const FieldPrep fp = w.prep[j];
-          const double mx = w.bunch[3 * j], my = w.bunch[3 * j + 1], dt = w.bunch[3 * j + 2];
-          const double coeffI = spec[2 * j + 1];
+          const FieldPrep& fp = s_fp[s];
+          const double mx = s_bc[s][0], my = s_bc[s][1], dt = s_bc[s][2], coeffI = s_bc[s][3];
           double z1r = 0, z1i = 0, z2r = 0, z2i = 0;
           if (active) field_zargs(fp, x - mx, y - my, &z1r, &z1i, &z2r, &z2i);
-          const cplx wm = half ? w_quadrant1_lowlat(z2r, z2i) : w_quadrant1_lowlat(z1r, z1i);
+          const cplx wm = half ? w_quadrant1_wide_lowlat(z2r, z2i) : w_quadrant1_wide_lowlat(z1r, z1i);
           const cplx wo = {__shfl_xor_sync(FULL_MASK, wm.re, 1),
                            __shfl_xor_sync(FULL_MASK, wm.im, 1)};
           if (active) {

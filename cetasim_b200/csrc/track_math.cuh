@@ -16,6 +16,8 @@ struct SectionDev {
   double eta_x, etap_x, eta_y, etap_y;
   double phase_adv_x, phase_adv_y;
   double weigh_x, weigh_y;           // phaseAdv / (2 pi nu), Bunch.cpp:662-663
+  double cos_x, sin_x, cos_y, sin_y; // of phaseAdv (angle addition in the map)
+  double inv_beta_x, inv_beta_y;
   double aperture_x, aperture_y;
   double b1h1[36], h1b1[36], h2b2[36];
 };
@@ -44,10 +46,34 @@ CG_HD void matvec6(const double* A, const double v[6], double out[6]) {
   }
 }
 
+// sin and cos of phi0 + d from those of phi0 and a Taylor series of d
+// (|d| <= 1/16: the first omitted terms are below 1e-20 relative); larger d
+// takes sincos of the sum.  The chromatic and amplitude tune shifts of a
+// section are ~1e-3 rad, so the series is the path taken: it costs a dozen
+// FMAs instead of two argument reductions.
+CG_HD void sincos_shifted(double phi0, double c0, double s0, double d, double* sn, double* cs) {
+  if (fabs(d) <= 0.0625) {
+    const double d2 = d * d;
+    const double sd =
+        d * fma(d2, fma(d2, fma(d2, fma(d2, fma(d2, -1.0 / 39916800.0, 1.0 / 362880.0),
+                                            -1.0 / 5040.0), 1.0 / 120.0), -1.0 / 6.0), 1.0);
+    const double cd =
+        fma(d2, fma(d2, fma(d2, fma(d2, fma(d2, -1.0 / 3628800.0, 1.0 / 40320.0), -1.0 / 720.0),
+                            1.0 / 24.0), -0.5), 1.0);
+    *sn = fma(s0, cd, c0 * sd);
+    *cs = fma(c0, cd, -(s0 * sd));
+  } else {
+    sincos(phi0 + d, sn, cs);
+  }
+}
+
 // Bunch::BunchTransferDueToLatticeTSymplectic for one alive particle
 // (Bunch.cpp:664-740): dispersion removed for the amplitude, tune shift from
 // chromaticity and amplitude-dependent detuning, then
-// v <- H2B2 . R(phi_x, phi_y) . B1H1 . v.
+// v <- H2B2 . R(phi_x, phi_y) . B1H1 . v.  The phase phi = phaseAdv + 2 pi dnu
+// is rounded as in the reference and applied by angle addition
+// (sincos_shifted); the amplitude uses 1/beta.  Both differ from the
+// reference's direct forms by an ulp or so.
 CG_HD void section_map_particle(const SectionDev& s, const RingDev& r, double v[6]) {
   const double dp = v[5];
   double x = v[0] - s.eta_x * dp;
@@ -56,8 +82,8 @@ CG_HD void section_map_particle(const SectionDev& s, const RingDev& r, double v[
   double py = v[3] - s.etap_y * dp;
   double ux = fma(s.alpha_x, x, s.beta_x * px);
   double uy = fma(s.alpha_y, y, s.beta_y * py);
-  double ampX = fma(x, x, ux * ux) / s.beta_x;
-  double ampY = fma(y, y, uy * uy) / s.beta_y;
+  double ampX = fma(x, x, ux * ux) * s.inv_beta_x;
+  double ampY = fma(y, y, uy * uy) * s.inv_beta_y;
   double ax2 = ampX * ampX, ay2 = ampY * ampY, axy = ampX * ampY;
   double dnux = r.chrom[0] * dp + r.adtx[0] * ampX + r.adtx[1] * ampY + r.adtx[2] * ax2 / 2 +
                 r.adtx[3] * ay2 / 2 + r.adtx[4] * axy;
@@ -65,11 +91,13 @@ CG_HD void section_map_particle(const SectionDev& s, const RingDev& r, double v[
                 r.adty[3] * ay2 / 2 + r.adty[4] * axy;
   dnux *= s.weigh_x;
   dnuy *= s.weigh_y;
-  double phiX = s.phase_adv_x + 2 * kPi * dnux;
-  double phiY = s.phase_adv_y + 2 * kPi * dnuy;
+  // the reference's rounded phase phi = phaseAdv + 2 pi dnu; phi - phaseAdv is
+  // exact (Sterbenz), so the angle addition applies the same phase
+  const double phiX = s.phase_adv_x + 2 * kPi * dnux;
+  const double phiY = s.phase_adv_y + 2 * kPi * dnuy;
   double sx, cx, sy, cy;
-  sincos(phiX, &sx, &cx);
-  sincos(phiY, &sy, &cy);
+  sincos_shifted(s.phase_adv_x, s.cos_x, s.sin_x, phiX - s.phase_adv_x, &sx, &cx);
+  sincos_shifted(s.phase_adv_y, s.cos_y, s.sin_y, phiY - s.phase_adv_y, &sy, &cy);
   double v1[6];
   matvec6(s.b1h1, v, v1);
   double v2[6];
@@ -261,7 +289,7 @@ CG_HD void ion_kick_particle_prep(const CloudRec* rec, const FieldPrep* prep, in
   double fx = 0, fy = 0;
   for (int p = 0; p < n_species; ++p) {
     double ex, ey;
-    gaussian_field_prep<false>(prep[p], x - rec[p].aver_x, y - rec[p].aver_y, &ex, &ey);
+    gaussian_field_kick(prep[p], x - rec[p].aver_x, y - rec[p].aver_y, &ex, &ey);
     fx = fma(rec[p].coeff, ex, fx);
     fy = fma(rec[p].coeff, ey, fy);
   }
