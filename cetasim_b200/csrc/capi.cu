@@ -525,10 +525,6 @@ int cg_set_beam(cg_handle* H, int M, const int* n_macro, const int* harm, const 
   cudaMemset(d.surv, 0xFF, h.npad);
   cudaMemcpy(d.tile_bunch, tb.data(), sizeof(int) * tiles, cudaMemcpyHostToDevice);
   cudaMemcpy(d.chunk_bunch, cb.data(), sizeof(int) * chunks, cudaMemcpyHostToDevice);
-  if (cudaError_t pe = prepare_ip_pass()) {
-    free_beam(h);
-    return cuda_fail(&h, pe, "particle pass shared memory");
-  }
   cudaMemcpy(d.bunch, bd.data(), sizeof(BunchDev) * M, cudaMemcpyHostToDevice);
   cudaMemset(d.counters, 0, sizeof(unsigned) * (M + 1));
   cudaMemset(d.loss_count, 0, sizeof(int) * (M + 1));
@@ -792,7 +788,7 @@ static cudaError_t enqueue_turn(Handle& h) {
     int mom = -1;
     if (k + 1 < h.K) mom = c.flag_beam_ion ? k + 1 : -1;
     else mom = post ? h.K - 1 : -1;
-    if ((e = launch_ip_pass(h, k, false, mom))) return e;
+    if ((e = launch_map_pass(h, k, mom))) return e;
   }
   if (c.flag_lr_wake && (e = launch_lr_compute(h))) return e;
   unsigned fl = kLongRF | kLongDrift | kLongLoss;
@@ -882,7 +878,7 @@ int cg_time_stage(cg_handle* H, int stage, int k, int reps, double* ms) {
       case 1: e = launch_ion_kick(h, k); break;
       case 2: e = launch_ion_chain(h, k); break;
       case 3: e = launch_moments(h, k); break;
-      case 5: e = launch_ip_pass(h, k, false, k); break;
+      case 5: e = launch_map_pass(h, k, k); break;
       default: e = launch_long(h, kLongRF | kLongDrift | kLongLoss | (h.cfg.flag_synrad ? kLongSynrad : 0));
     }
   }

@@ -264,18 +264,19 @@ __global__ void __launch_bounds__(kTile) k_map(double* __restrict__ c, int64_t n
                                                const uint8_t* __restrict__ surv,
                                                const int* __restrict__ tile_bunch,
                                                const BunchDev* __restrict__ bunch,
-                                               const SectionDev* __restrict__ secp, RingDev r) {
+                                               const __grid_constant__ SectionDev sec,
+                                               const __grid_constant__ RingDev r) {
   TileIdx t = tile_index(tile_bunch, bunch);
   if (!t.valid || surv[t.g] != kAlive) return;
   double v[6];
   load6(c, npad, t.g, v);
-  section_map_particle(*secp, r, v);
+  section_map_particle(sec, r, v);
   store6(c, npad, t.g, v);
 }
 
 cudaError_t launch_map(Handle& h, int k) {
   k_map<<<h.n_tiles, kTile, 0, h.stream>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch, h.d.bunch,
-                                           h.sec_dev + k, h.ring);
+                                           h.sec_dev_host[k], h.ring);
   return cudaGetLastError();
 }
 
@@ -303,95 +304,57 @@ __global__ void __launch_bounds__(kTile, 3) k_ion_kick(double* __restrict__ c, i
   c[3 * npad + t.g] += dpy;
 }
 
-// One pass per interaction point inside the turn graph: the electron-side ion
-// kick of IP k (KICK), the section map k, and the moments the next stage
-// reads (MOM: at the twiss of section `mom_section`, MPBeam.cpp:1061/1069),
-// over chunks of kMomChunkTiles tiles of one bunch.  Per particle the order is
-// that of the separate stages (kick, then map), so results equal the staged
-// calls; the particle is read and written once instead of three times.
-template <bool KICK, bool MOM>
-__global__ void __launch_bounds__(kTile, KICK ? 1 : 2) k_ip_pass(double* __restrict__ c, int64_t npad,
-                                                   const uint8_t* __restrict__ surv,
-                                                   const int* __restrict__ chunk_bunch,
-                                                   const BunchDev* __restrict__ bunch,
-                                                   const CloudRec* __restrict__ rec, int P,
-                                                   const SectionDev* __restrict__ secp, RingDev r,
-                                                   MomPartial* partials, unsigned* counters,
-                                                   BunchMomDev* mom, double beta_x, double beta_y) {
-  extern __shared__ double s_v[];  // MOM: mapped coordinates [6][kMomChunkTiles * kTile]
+// The map of section k with the moments the next stage reads (MOM: at the
+// twiss of section `mom_section`, MPBeam.cpp:1061/1069) in one pass over
+// chunks of kMomChunkTiles tiles of one bunch: all loads of a chunk are issued
+// first, the mapped particles stay in registers for the moments, and each
+// particle is read and written once.  Results equal k_map followed by
+// k_moments.
+template <bool MOM>
+__global__ void __launch_bounds__(kTile, 2) k_map_pass(double* __restrict__ c, int64_t npad,
+                                                    const uint8_t* __restrict__ surv,
+                                                    const int* __restrict__ chunk_bunch,
+                                                    const BunchDev* __restrict__ bunch,
+                                                    const __grid_constant__ SectionDev sec,
+                                                    const __grid_constant__ RingDev r,
+                                                    MomPartial* partials, unsigned* counters,
+                                                    BunchMomDev* mom, double beta_x, double beta_y) {
   __shared__ double smem[9 * 32];
-  __shared__ FieldPrep s_prep[CG_MAX_SPECIES];
   const int b = chunk_bunch[blockIdx.x];
   const BunchDev B = bunch[b];
-  const CloudRec* rb = rec + (size_t)b * P;
-  if (KICK) {
-    if ((int)threadIdx.x < P)
-      s_prep[threadIdx.x] = field_prep(rb[threadIdx.x].rms_x, rb[threadIdx.x].rms_y);
-    __syncthreads();
-  }
-  const SectionDev& sec = *secp;
   const int tile0 = B.tile_off + (blockIdx.x - B.chunk_off) * kMomChunkTiles;
   const int i0 = (tile0 - B.tile_off) * kTile + threadIdx.x;
-  unsigned amask = 0;
-#pragma unroll 1
+  double v[kMomChunkTiles][6];
+  bool alive[kMomChunkTiles];
+#pragma unroll
   for (int u = 0; u < kMomChunkTiles; ++u) {
     const int64_t g = (int64_t)(tile0 + u) * kTile + threadIdx.x;
     const bool valid = i0 + u * kTile < B.n;
-    const bool alive = valid && surv[g] == kAlive;
-    double v[6] = {0, 0, 0, 0, 0, 0};
-    if (alive) {
-      amask |= 1u << u;
-      load6(c, npad, g, v);
-      if (KICK) {
-        double dpx, dpy;
-        ion_kick_particle_prep(rb, s_prep, P, v[0], v[2], &dpx, &dpy);
-        v[1] += dpx;
-        v[3] += dpy;
-      }
-      section_map_particle(sec, r, v);
-      store6(c, npad, g, v);
-    }
-    if (MOM)
+    alive[u] = valid && surv[g] == kAlive;
 #pragma unroll
-      for (int d = 0; d < 6; ++d) s_v[(d * kMomChunkTiles + u) * kTile + threadIdx.x] = v[d];
+    for (int d = 0; d < 6; ++d) v[u][d] = valid ? c[d * npad + g] : 0.0;
+  }
+#pragma unroll
+  for (int u = 0; u < kMomChunkTiles; ++u) {
+    if (!alive[u]) continue;
+    section_map_particle(sec, r, v[u]);
+    store6(c, npad, (int64_t)(tile0 + u) * kTile + threadIdx.x, v[u]);
   }
   if (MOM) {
-    // each thread reads back only its own entries: no barrier needed
-    double v[kMomChunkTiles][6];
-    bool alive[kMomChunkTiles];
-#pragma unroll
-    for (int u = 0; u < kMomChunkTiles; ++u) {
-      alive[u] = (amask >> u) & 1u;
-#pragma unroll
-      for (int d = 0; d < 6; ++d) v[u][d] = s_v[(d * kMomChunkTiles + u) * kTile + threadIdx.x];
-    }
     chunk_moment_partial(v, alive, smem, &partials[blockIdx.x]);
     bunch_moment_finish(b, B.chunk_off, B.n_chunks, partials, counters, mom, beta_x, beta_y,
                         c + 4 * npad + (int64_t)B.tile_off * kTile);
   }
 }
 
-constexpr size_t kIpPassSmem = 6 * kMomChunkTiles * kTile * sizeof(double);
-
-// Opt-in shared memory of the moments variants (outside any graph capture).
-cudaError_t prepare_ip_pass() {
-  cudaError_t e = cudaFuncSetAttribute(k_ip_pass<true, true>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kIpPassSmem);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_ip_pass<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)kIpPassSmem);
-}
-
-cudaError_t launch_ip_pass(Handle& h, int k, bool kick, int mom_section) {
+cudaError_t launch_map_pass(Handle& h, int k, int mom_section) {
   const bool m = mom_section >= 0;
   const double bx = m ? h.sec_dev_host[mom_section].beta_x : 0.0;
   const double by = m ? h.sec_dev_host[mom_section].beta_y : 0.0;
-  const CloudRec* rec = kick ? h.d.rec + (size_t)k * h.M * h.P : nullptr;
-  auto kern = kick ? (m ? k_ip_pass<true, true> : k_ip_pass<true, false>)
-                   : (m ? k_ip_pass<false, true> : k_ip_pass<false, false>);
-  kern<<<h.n_chunks, kTile, m ? kIpPassSmem : 0, h.stream>>>(
-      h.d.c, h.npad, h.d.surv, h.d.chunk_bunch, h.d.bunch, rec, h.P, h.sec_dev + k, h.ring,
-      h.d.partials, h.d.counters, h.d.mom, bx, by);
+  auto kern = m ? k_map_pass<true> : k_map_pass<false>;
+  kern<<<h.n_chunks, kTile, 0, h.stream>>>(h.d.c, h.npad, h.d.surv, h.d.chunk_bunch, h.d.bunch,
+                                           h.sec_dev_host[k], h.ring, h.d.partials,
+                                           h.d.counters, h.d.mom, bx, by);
   return cudaGetLastError();
 }
 
@@ -409,7 +372,8 @@ __global__ void __launch_bounds__(kTile) k_long(double* __restrict__ c, int64_t 
                                                 const uint8_t* __restrict__ surv,
                                                 const int* __restrict__ tile_bunch,
                                                 const BunchDev* __restrict__ bunch,
-                                                const SectionDev* __restrict__ sec0, RingDev r,
+                                                const __grid_constant__ SectionDev sec0,
+                                                const __grid_constant__ RingDev r,
                                                 unsigned flags, uint64_t seed,
                                                 const int* __restrict__ d_turn,
                                                 const double* __restrict__ lr_force) {
@@ -423,7 +387,7 @@ __global__ void __launch_bounds__(kTile) k_long(double* __restrict__ c, int64_t 
   if ((flags & kLongSynrad) && surv[t.g] == kAlive) {
     double g[6];
     synrad_normals(seed, (uint32_t)t.i, (uint32_t)t.b, (uint32_t)(*d_turn), g);
-    synrad_particle(*sec0, r, v, g, bunch[t.b].n != 1);
+    synrad_particle(sec0, r, v, g, bunch[t.b].n != 1);
   }
   if (flags & kLongLR) {
     const double* f = lr_force + 3 * t.b;
@@ -436,7 +400,7 @@ __global__ void __launch_bounds__(kTile) k_long(double* __restrict__ c, int64_t 
 
 cudaError_t launch_long(Handle& h, unsigned flags) {
   k_long<<<h.n_tiles, kTile, 0, h.stream>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch, h.d.bunch,
-                                            h.sec_dev, h.ring, flags, h.cfg.seed, h.d.turn,
+                                            h.sec_dev_host[0], h.ring, flags, h.cfg.seed, h.d.turn,
                                             h.d.lr_force);
   return cudaGetLastError();
 }

@@ -17,9 +17,8 @@ cudaError_t launch_map(Handle& h, int k);
 cudaError_t launch_ion_chain(Handle& h, int k);
 int ion_walk_grid(int64_t tcap);
 cudaError_t launch_ion_kick(Handle& h, int k);
-// kick (if `kick`) + map of section k + moments at section `mom_section` (if >= 0)
-cudaError_t launch_ip_pass(Handle& h, int k, bool kick, int mom_section);
-cudaError_t prepare_ip_pass();
+// map of section k + moments at section `mom_section` (if >= 0)
+cudaError_t launch_map_pass(Handle& h, int k, int mom_section);
 enum LongFlags : unsigned {
   kLongRF = 1,
   kLongDrift = 2,
