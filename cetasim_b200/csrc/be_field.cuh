@@ -116,9 +116,17 @@ CG_HD void field_zargs(const FieldPrep& p, double posx, double posy, double* z1r
   *z2i = ay * p.ir;
 }
 
-// Field from the prepared constants and the two w values.
-CG_HD void field_finish(const FieldPrep& p, double posx, double posy, cplx w1, cplx w2,
-                        double* fx, double* fy) {
+// The Gaussian factor exp(-x^2/2 sx^2 - y^2/2 sy^2) of the BE formula (modes
+// 0 and 1), separate so that a caller can evaluate it alongside w(z).
+CG_HD double field_gauss(const FieldPrep& p, double posx, double posy) {
+  double a = p.mode == 1 ? posy : posx, b = p.mode == 1 ? posx : posy;
+  double tx = fabs(a) * p.ia, ty = fabs(b) * p.ib;
+  return exp(-(tx * tx) / 2.0 - (ty * ty) / 2.0);
+}
+
+// Field from the prepared constants, the two w values and the Gaussian factor.
+CG_HD void field_finish_g(const FieldPrep& p, double posx, double posy, cplx w1, cplx w2,
+                          double g, double* fx, double* fy) {
   if (fabs(posx * p.isx) + fabs(posy * p.isy) < 1.0e-5) {
     *fx = 0.0;
     *fy = 0.0;
@@ -129,8 +137,7 @@ CG_HD void field_finish(const FieldPrep& p, double posx, double posy, cplx w1, c
     return;
   }
   double a = p.mode == 1 ? posy : posx, b = p.mode == 1 ? posx : posy;
-  double tx = fabs(a) * p.ia, ty = fabs(b) * p.ib;
-  double w3 = -exp(-(tx * tx) / 2.0 - (ty * ty) / 2.0);
+  double w3 = -g;
   double re = p.coeff * fma(w3, w2.re, w1.re);
   double im = p.coeff * fma(w3, w2.im, w1.im);
   double Fa = im, Fb = re;
@@ -143,6 +150,13 @@ CG_HD void field_finish(const FieldPrep& p, double posx, double posy, cplx w1, c
     *fx = Fa;
     *fy = Fb;
   }
+}
+
+// Field from the prepared constants and the two w values.
+CG_HD void field_finish(const FieldPrep& p, double posx, double posy, cplx w1, cplx w2,
+                        double* fx, double* fy) {
+  const double g = p.mode == 2 ? 0.0 : field_gauss(p, posx, posy);
+  field_finish_g(p, posx, posy, w1, w2, g, fx, fy);
 }
 
 // The same with the kick kernels' w(z) (w_quadrant1_wide).

@@ -201,6 +201,63 @@ CG_HD cplx w_quadrant1_lowlat(double x, double y) {
   return w;
 }
 
+// 1/d for 0 < d < 3e38 by Newton-Raphson refinement of a single-precision
+// seed (two steps, r <- r + r (1 - d r): 2^-23 -> 2^-46 -> rounding level,
+// within about an ulp of the correctly rounded quotient).
+CG_HD double recip_newton(double d) {
+#if defined(__CUDA_ARCH__)
+  double r = (double)__frcp_rn((float)d);
+#else
+  double r = (double)(1.0f / (float)d);
+#endif
+  double e = fma(-d, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-d, r, 1.0);
+  return fma(r, e, r);
+}
+
+// Half of Weideman's series for a w(z) split over two lanes: with the
+// coefficients c_m = a[39 - m] of Z^m, the lower lane (upper = false) returns
+// sum_{m<20} c_m Z^m and the upper lane Z^20 sum_{m<20} c_{m+20} Z^m, both in
+// Estrin's form (5 levels); their sum p gives w = 2 p / (L - iz)^2 +
+// 1 / (sqrt(pi) (L - iz)).  *rden = 1/(L - iz).  For 0 <= |z| < 30 in the
+// first quadrant (the reciprocal assumes |L - iz|^2 well inside float range).
+CG_HD cplx weideman_half(double x, double y, double L, const double* a, bool upper, cplx* rden) {
+  cplx den = {L + y, -x};
+  cplx num = {L - y, x};
+  const double inv = recip_newton(fma(den.re, den.re, den.im * den.im));
+  cplx Z = {fma(num.re, den.re, num.im * den.im) * inv,
+            fma(num.im, den.re, -num.re * den.im) * inv};
+  cplx Z2 = cmul(Z, Z);
+  cplx Z4 = cmul(Z2, Z2);
+  cplx Z8 = cmul(Z4, Z4);
+  cplx Z16 = cmul(Z8, Z8);
+  const int base = upper ? 20 : 0;
+  cplx q[10];
+#pragma unroll
+  for (int i = 0; i < 10; ++i) {
+    const double c0 = a[kWeidemanN - 1 - base - 2 * i], c1 = a[kWeidemanN - 2 - base - 2 * i];
+    q[i] = {fma(c1, Z.re, c0), c1 * Z.im};
+  }
+  cplx r[5];
+#pragma unroll
+  for (int i = 0; i < 5; ++i) r[i] = cmuladd(q[2 * i], q[2 * i + 1], Z2);
+  cplx s0 = cmuladd(r[0], r[1], Z4);  // Z^0 .. Z^7
+  cplx s1 = cmuladd(r[2], r[3], Z4);  // Z^8 .. Z^15 (over Z^8)
+  cplx t = cmuladd(s0, s1, Z8);       // Z^0 .. Z^15
+  cplx p = cmuladd(t, r[4], Z16);     // + Z^16 .. Z^19
+  if (upper) p = cmul(p, cmul(Z16, Z4));
+  *rden = {den.re * inv, -den.im * inv};
+  return p;
+}
+
+// w(z) from the summed halves of weideman_half.
+CG_HD cplx weideman_from_sum(cplx p, cplx rden) {
+  cplx rden2 = cmul(rden, rden);
+  cplx t = cmul(p, rden2);
+  return {fma(2.0, t.re, kInvSqrtPi * rden.re), fma(2.0, t.im, kInvSqrtPi * rden.im)};
+}
+
 // The kick kernels' first-quadrant path: Weideman's expansion up to |z| = 30,
 // where it stays within 3e-14 of w relative to |w| (the real-axis region
 // included), the continued fraction beyond.  Beam particles and ions sit

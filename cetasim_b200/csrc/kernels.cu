@@ -126,23 +126,62 @@ __device__ __forceinline__ void store6(double* __restrict__ c, int64_t npad, int
 // the reference's two passes over the whole bunch).
 
 // v[u][d]: coordinate d of this thread's particle in tile u of the chunk.
+// Two block reductions with fixed trees: (sums, count, z min, z max), whose
+// totals every thread needs for the centred pass, then the centred
+// co-moments, whose totals only thread 0 needs.  Three barriers.
 __device__ void chunk_moment_partial(const double (&v)[kMomChunkTiles][6],
                                      const bool (&alive)[kMomChunkTiles], double* smem,
                                      MomPartial* out) {
+  constexpr int NW = kTile / 32;
+  double* sa = smem;            // 9 x 32: sums (7), min z, max z
+  double* sb = smem + 9 * 32;   // 9 x 32: centred co-moments
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   double s[7] = {0, 0, 0, 0, 0, 0, 0};
+  double mn = INFINITY, mx = -INFINITY;
 #pragma unroll
   for (int u = 0; u < kMomChunkTiles; ++u) {
 #pragma unroll
     for (int d = 0; d < 6; ++d) s[d] += alive[u] ? v[u][d] : 0.0;
     s[6] += alive[u] ? 1.0 : 0.0;
+    if (alive[u]) {
+      mn = fmin(mn, v[u][4]);
+      mx = fmax(mx, v[u][4]);
+    }
   }
-  block_sum<7, kTile>(s, smem);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+    for (int k = 0; k < 7; ++k) s[k] += __shfl_xor_sync(FULL_MASK, s[k], o);
+    mn = fmin(mn, __shfl_xor_sync(FULL_MASK, mn, o));
+    mx = fmax(mx, __shfl_xor_sync(FULL_MASK, mx, o));
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < 7; ++k) sa[k * 32 + warp] = s[k];
+    sa[7 * 32 + warp] = mn;
+    sa[8 * 32 + warp] = mx;
+  }
+  __syncthreads();
+  // every thread combines the NW warp totals in the same order
+#pragma unroll
+  for (int k = 0; k < 7; ++k) {
+    double a = sa[k * 32];
+#pragma unroll
+    for (int w = 1; w < NW; ++w) a += sa[k * 32 + w];
+    s[k] = a;
+  }
+  mn = sa[7 * 32];
+  mx = sa[8 * 32];
+#pragma unroll
+  for (int w = 1; w < NW; ++w) {
+    mn = fmin(mn, sa[7 * 32 + w]);
+    mx = fmax(mx, sa[8 * 32 + w]);
+  }
   const double n = s[6];
   double mean[6];
 #pragma unroll
   for (int d = 0; d < 6; ++d) mean[d] = n > 0 ? s[d] / n : 0.0;
   double q[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  double mn = INFINITY, mx = -INFINITY;
 #pragma unroll
   for (int u = 0; u < kMomChunkTiles; ++u) {
     double dv[6];
@@ -153,20 +192,24 @@ __device__ void chunk_moment_partial(const double (&v)[kMomChunkTiles][6],
     q[6] = fma(dv[0], dv[1], q[6]);
     q[7] = fma(dv[2], dv[3], q[7]);
     q[8] = fma(dv[4], dv[5], q[8]);
-    if (alive[u]) {
-      mn = fmin(mn, v[u][4]);
-      mx = fmax(mx, v[u][4]);
-    }
   }
-  block_sum<9, kTile>(q, smem);
-  block_minmax<kTile>(mn, mx, smem);
+  warp_sum<9>(q);
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < 9; ++k) sb[k * 32 + warp] = q[k];
+  __syncthreads();
   if (threadIdx.x == 0) {
     MomPartial p;
     p.n = n;
 #pragma unroll
     for (int d = 0; d < 6; ++d) p.mean[d] = mean[d];
 #pragma unroll
-    for (int d = 0; d < 9; ++d) p.c[d] = q[d];
+    for (int k = 0; k < 9; ++k) {
+      double a = sb[k * 32];
+#pragma unroll
+      for (int w = 1; w < NW; ++w) a += sb[k * 32 + w];
+      p.c[k] = a;
+    }
     p.zmin = mn;
     p.zmax = mx;
     *out = p;
@@ -229,7 +272,7 @@ __global__ void __launch_bounds__(kTile, 2) k_moments(const double* __restrict__
                                                    const BunchDev* __restrict__ bunch,
                                                    MomPartial* partials, unsigned* counters,
                                                    BunchMomDev* mom, double beta_x, double beta_y) {
-  __shared__ double smem[9 * 32];
+  __shared__ double smem[18 * 32];
   const int b = chunk_bunch[blockIdx.x];
   const BunchDev B = bunch[b];
   const int tile0 = B.tile_off + (blockIdx.x - B.chunk_off) * kMomChunkTiles;
@@ -319,7 +362,7 @@ __global__ void __launch_bounds__(kTile, 2) k_map_pass(double* __restrict__ c, i
                                                     const __grid_constant__ RingDev r,
                                                     MomPartial* partials, unsigned* counters,
                                                     BunchMomDev* mom, double beta_x, double beta_y) {
-  __shared__ double smem[9 * 32];
+  __shared__ double smem[18 * 32];
   const int b = chunk_bunch[blockIdx.x];
   const BunchDev B = bunch[b];
   const int tile0 = B.tile_off + (blockIdx.x - B.chunk_off) * kMomChunkTiles;
@@ -812,7 +855,7 @@ __global__ void __launch_bounds__(kTile, 2) k_moments_noalloc(const double* __re
                                                            const uint8_t* __restrict__ surv, int n,
                                                            double beta_x, double beta_y,
                                                            double* scratch) {
-  __shared__ double smem[9 * 32];
+  __shared__ double smem[18 * 32];
   MomPartial* partials = reinterpret_cast<MomPartial*>(scratch);
   BunchMomDev* mom = reinterpret_cast<BunchMomDev*>(scratch + kNoAllocMomOff);
   unsigned* counter = reinterpret_cast<unsigned*>(scratch + kNoAllocCounterOff);

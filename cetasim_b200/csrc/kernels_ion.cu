@@ -19,8 +19,8 @@
 // Three kernels per IP:
 //   k_ion_prep    per bunch: loss bounds, birth positions (Philox, attempts in
 //                 order), field constants, coefficients;
-//   k_ion_walk    each CTA walks 128 trajectories (two lanes per ion: the even
-//                 lane evaluates w(z1), the odd one w(z2)) through all bunches
+//   k_ion_walk    each CTA walks 64 trajectories (four lanes per ion: w(z1)
+//                 and w(z2) each split into halves of the series) through all bunches
 //                 without a barrier per bunch, and writes per-step partial
 //                 sums (count, sum x, y, x^2, y^2) every kWin bunches;
 //   k_ion_finish  per step: sums in CTA order -> cloud centroid and rms ->
@@ -37,8 +37,8 @@ namespace cg {
 
 #define FULL_MASK 0xffffffffu
 
-constexpr int kWalkIons = 128;                 // trajectories per CTA block
-constexpr int kWalkThreads = 2 * kWalkIons;    // two lanes per ion
+constexpr int kWalkIons = 64;                  // trajectories per CTA block
+constexpr int kWalkThreads = 4 * kWalkIons;    // four lanes per ion
 constexpr int kWin = 16;                       // steps per shared-memory window
 constexpr int kGroups = kWalkThreads / kWin;   // ion groups summed per step
 constexpr int kGroupIons = kWalkIons / kGroups;
@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(kPrepThreads) k_ion_prep(ChainParams cp, Chain
   }
 }
 
-// One CTA block = 128 trajectories: index t < n0 is ion t of the cloud the
+// One CTA block = 64 trajectories: index t < n0 is ion t of the cloud the
 // previous call left, t >= n0 the ion born as number (t - n0) % NM at bunch
 // (t - n0) / NM.  blockIdx.y = species.  The step loop has no block barrier:
 // each ion's position at each step goes to a shared-memory window of kWin
@@ -147,13 +147,17 @@ __global__ void __launch_bounds__(kWalkThreads, 1) k_ion_walk(ChainParams cp, Io
   __shared__ double s_grp[kWin][kGroups][5];
   __shared__ FieldPrep s_fp[kWin];
   __shared__ double s_bc[kWin][4];  // mean x, mean y, drift time, ion coefficient
+  __shared__ double s_a[kWeidemanN];  // Weideman coefficients (lanes read different ones)
   const int p = blockIdx.y, G = gridDim.x, c = blockIdx.x;
   const int M = cp.n_bunches, NM = cp.macro_per_ip;
   const int n0 = cst[p].n;
   const int64_t T = (int64_t)n0 + (int64_t)M * NM;
   const int nblk = (int)((T + kWalkIons - 1) / kWalkIons);
   if (c >= nblk) return;
-  const int tid = threadIdx.x, half = tid & 1, slot = tid >> 1;
+  const int tid = threadIdx.x, slot = tid >> 2, sub = tid & 3;
+  const bool second = (sub >> 1) != 0, upper = (sub & 1) != 0;
+  if (tid < kWeidemanN) s_a[tid] = weideman_table().a[tid];
+  const double L = weideman_table().L;
   const CloudDev cd = clouds[p];
   const double bx = w.bound[0], by = w.bound[1];
   const double* births = w.births + 2 * (size_t)p * M * NM;
@@ -201,7 +205,7 @@ __global__ void __launch_bounds__(kWalkThreads, 1) k_ion_walk(ChainParams cp, Io
         const int j = jw + s;
         const bool active = alive && j >= j0;
         // the cloud bunch j sees: ions alive after the births of bunch j
-        if (half == 0) {
+        if (sub == 0) {
           s_x[s][slot] = x;
           s_y[s][slot] = y;
           s_act[s][slot] = active ? 1 : 0;
@@ -211,14 +215,32 @@ __global__ void __launch_bounds__(kWalkThreads, 1) k_ion_walk(ChainParams cp, Io
         if (__any_sync(FULL_MASK, active)) {
           const FieldPrep& fp = s_fp[s];
           const double mx = s_bc[s][0], my = s_bc[s][1], dt = s_bc[s][2], coeffI = s_bc[s][3];
+          const double dx = x - mx, dy = y - my;
           double z1r = 0, z1i = 0, z2r = 0, z2i = 0;
-          if (active) field_zargs(fp, x - mx, y - my, &z1r, &z1i, &z2r, &z2i);
-          const cplx wm = half ? w_quadrant1_wide_lowlat(z2r, z2i) : w_quadrant1_wide_lowlat(z1r, z1i);
-          const cplx wo = {__shfl_xor_sync(FULL_MASK, wm.re, 1),
-                           __shfl_xor_sync(FULL_MASK, wm.im, 1)};
+          if (active) field_zargs(fp, dx, dy, &z1r, &z1i, &z2r, &z2i);
+          // lanes 0, 1 of the quad: w(z1); lanes 2, 3: w(z2), which also
+          // evaluate the Gaussian factor alongside the series
+          const double zr = second ? z2r : z1r, zi = second ? z2i : z1i;
+          const double g = (active && second && fp.mode != 2) ? field_gauss(fp, dx, dy) : 0.0;
+          cplx wv;
+          if (__all_sync(FULL_MASK, fp.mode == 2 || fma(zr, zr, zi * zi) < 900.0)) {
+            // each w(z) over two lanes: lower and upper halves of the series
+            cplx rden;
+            const cplx ph = weideman_half(zr, zi, L, s_a, upper, &rden);
+            const cplx po = {__shfl_xor_sync(FULL_MASK, ph.re, 1),
+                             __shfl_xor_sync(FULL_MASK, ph.im, 1)};
+            const cplx lo = upper ? po : ph, hi = upper ? ph : po;
+            wv = weideman_from_sum({lo.re + hi.re, lo.im + hi.im}, rden);
+          } else {
+            wv = w_quadrant1_wide_lowlat(zr, zi);
+          }
+          const cplx wo = {__shfl_xor_sync(FULL_MASK, wv.re, 2),
+                           __shfl_xor_sync(FULL_MASK, wv.im, 2)};
+          const double go = __shfl_xor_sync(FULL_MASK, g, 2);
           if (active) {
             double fx, fy;
-            field_finish(fp, x - mx, y - my, half ? wo : wm, half ? wm : wo, &fx, &fy);
+            field_finish_g(fp, dx, dy, second ? wo : wv, second ? wv : wo, second ? g : go, &fx,
+                           &fy);
             vx += coeffI * fx;
             vy += coeffI * fy;
             x += vx * dt;
@@ -252,10 +274,11 @@ __global__ void __launch_bounds__(kWalkThreads, 1) k_ion_walk(ChainParams cp, Io
 #pragma unroll
         for (int g = 0; g < kGroups; ++g) a += s_grp[s][g][q];
         double* dst = part + ((size_t)(jw + s) * G + c) * 5 + q;
-        *dst = first ? a : *dst + a;
+        if (first) *dst = a;
+        else *dst += a;
       }
     }
-    if (t < T && half == 0) {
+    if (t < T && sub == 0) {
       traj[t] = x;
       traj[w.tcap + t] = y;
       traj[2 * w.tcap + t] = vx;
