@@ -262,6 +262,7 @@ def main():
     lib.cg_fp64_peak(C.byref(peak))
     flops_per_kick = FLOPS_PER_KICK
     achieved = n_part * flops_per_kick / (kick_ms.value * 1e-3)
+    traffic = kick_traffic()
 
     result = None
     if rank == 0:
@@ -295,7 +296,11 @@ def main():
                          "achieved": achieved / 1e12, "peak": peak.value / 1e12, "unit": "TFLOP/s",
                          "frac": achieved / peak.value if peak.value else None,
                          "peak_source": "measured FP64 FMA throughput (cg_fp64_peak)",
-                         "algorithmic_flops_per_kick": flops_per_kick, "traffic": None},
+                         "algorithmic_flops_per_kick": flops_per_kick, "traffic": traffic,
+                         "traffic_source": "profiles/k_ion_kick_fast_ion.md (ncu, one launch)"},
+            "ion_chain": {"us_per_ip": 1e3 * chain_ms.value,
+                          "us_per_bunch_step": 1e3 * chain_ms.value / wl.n_bunches,
+                          "bound": "latency (one field evaluation per bunch step)"},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "macroparticle-turns/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
@@ -314,6 +319,17 @@ def main():
 # series, the exp of the Gaussian factor counted as one operation, and the
 # field algebra), counted from be_field.cuh / faddeeva.cuh: 2 x 307 + 32.
 FLOPS_PER_KICK = 646
+
+
+def kick_traffic():
+    """DRAM bytes per k_ion_kick launch from the committed ncu summary."""
+    import re
+    try:
+        txt = open(os.path.join(ROOT, "profiles", "k_ion_kick_fast_ion.md")).read()
+    except OSError:
+        return None
+    m = re.search(r"dram bytes read / written per launch \| ([\d.]+) MB / ([\d.]+) MB", txt)
+    return (float(m.group(1)) + float(m.group(2))) * 1e6 if m else None
 
 if __name__ == "__main__":
     main()
