@@ -94,8 +94,14 @@ class BunchMoments(C.Structure):
 
 
 PD = C.POINTER(C.c_double)
+PF = C.POINTER(C.c_float)
 PU8 = C.POINTER(C.c_uint8)
 PI = C.POINTER(C.c_int)
+
+class SurTrainParams(C.Structure):
+    _fields_ = [("seed", C.c_uint64), ("n_train", C.c_int64), ("n_holdout", C.c_int64),
+                ("epochs", C.c_int), ("batch", C.c_int), ("lr", C.c_double)]
+
 
 # (name, restype, argtypes) of every export declared in include/cetasim_gpu.h
 EXPORTS = [
@@ -141,6 +147,13 @@ EXPORTS = [
     ("cg_faddeeva_w", I, [PD, PD, PD, PD, C.c_int64]),
     ("cg_faddeeva_w_q1", I, [PD, PD, PD, PD, C.c_int64]),
     ("cg_gaussian_field", I, [PD, PD, PD, PD, PD, PD, C.c_int64]),
+    ("cg_surrogate_dataset", I, [C.c_uint64, C.c_int64, PF, PF]),
+    ("cg_surrogate_eval", I, [PF, PF, C.c_int64, PF]),
+    ("cg_surrogate_grad", I, [PF, PF, PF, I, PF, PD]),
+    ("cg_surrogate_train", I, [C.POINTER(SurTrainParams), PF, PD]),
+    ("cg_set_surrogate", I, [C.c_void_p, PF, I]),
+    ("cg_surrogate_audit", I, [C.c_void_p, I, PD]),
+    ("cg_surrogate_audit_stats", I, [C.c_void_p, PI, PD, PD]),
     ("cg_bunch_moments_noalloc", I, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, D, D,
                                      C.c_void_p, C.c_void_p]),
 ]
@@ -181,6 +194,8 @@ def ptr(a):
         return None
     if a.dtype == np.float64:
         return a.ctypes.data_as(PD)
+    if a.dtype == np.float32:
+        return a.ctypes.data_as(PF)
     if a.dtype == np.int32:
         return a.ctypes.data_as(PI)
     if a.dtype == np.uint8:

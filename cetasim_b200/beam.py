@@ -105,6 +105,26 @@ class MPBeam:
     def Run(self, turn0: int, n_turns: int):
         self._check(self.lib.cg_run_turns(self.h, turn0, n_turns))
 
+    # -- field surrogate (no reference counterpart) -------------------------------
+    def set_surrogate(self, weights, audit_interval: int = 0):
+        """Electron-side ion kicks from the trained surrogate (None: exact)."""
+        w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float32)
+        self._check(self.lib.cg_set_surrogate(self.h, _abi.ptr(w), audit_interval))
+        self._sur_w = w
+
+    def surrogate_audit(self, k: int):
+        """(max |F_sur - F_exact|, max |F_exact|) at IP k on the current beam."""
+        out = np.zeros(2)
+        self._check(self.lib.cg_surrogate_audit(self.h, k, _abi.ptr(out)))
+        return out
+
+    def surrogate_audit_stats(self):
+        n = C.c_int()
+        last, worst = C.c_double(), C.c_double()
+        self._check(self.lib.cg_surrogate_audit_stats(self.h, C.byref(n), C.byref(last),
+                                                      C.byref(worst)))
+        return n.value, last.value, worst.value
+
     # -- ion clouds --------------------------------------------------------------
     def ions(self, k: int, p: int = 0):
         cap = int(self.wl.cfg.ion.max_ions) + 8

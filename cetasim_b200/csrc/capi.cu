@@ -9,6 +9,7 @@
 #include <string>
 #include <vector>
 #include "kernels.cuh"
+#include "surrogate.cuh"
 
 using namespace cg;
 
@@ -75,6 +76,8 @@ int check_status(Handle& h) {
     return fail(&h, CG_ERR_TRANSMISSION, "a bunch lost more than 50% of its particles");
   if (st & kStatusIonBirth)
     return fail(&h, CG_ERR_INVALID, "ion births rejected 2^20 times (degenerate bunch size)");
+  if (st & kStatusSurrogateWait)
+    return fail(&h, CG_ERR_TIMEOUT, "a tensor-core completion wait of the field surrogate gave up");
   if (st & kStatusLrRange)
     return fail(&h, CG_ERR_INVALID, "long-range wake lag outside the wake table (tau > 0)");
   return fail(&h, CG_ERR_CUDA, "unknown device status");
@@ -443,6 +446,7 @@ int cg_destroy(cg_handle* H) {
   cudaSetDevice(h.device);
   free_beam(h);
   dfree(h.sec_dev); dfree(h.d.status); dfree(h.d.turn);
+  dfree(h.d.sur_w); dfree(h.d.sur_audit);
   if (h.d.clouds) {
     std::vector<CloudDev> cl(h.K * h.P);
     cudaMemcpy(cl.data(), h.d.clouds, sizeof(CloudDev) * cl.size(), cudaMemcpyDeviceToHost);
@@ -683,7 +687,8 @@ int cg_beam_ion_ip(cg_handle* H, int turn, int k) {
   CG_CUDA(&h, cudaStreamSynchronize(h.stream));
   if ((st = launch_ok(h, launch_ion_chain(h, k), "ion chain"))) return st;
   if ((st = check_status(h))) return st;
-  if ((st = launch_ok(h, launch_ion_kick(h, k), "ion kick"))) return st;
+  cudaError_t ke = h.d.sur_w ? launch_ion_kick_sur(h, k) : launch_ion_kick(h, k);
+  if ((st = launch_ok(h, ke, "ion kick"))) return st;
   return check_status(h);
 }
 
@@ -783,7 +788,7 @@ static cudaError_t enqueue_turn(Handle& h) {
   for (int k = 0; k < h.K; ++k) {
     if (c.flag_beam_ion) {
       if ((e = launch_ion_chain(h, k))) return e;
-      if ((e = launch_ion_kick(h, k))) return e;
+      if ((e = h.d.sur_w ? launch_ion_kick_sur(h, k) : launch_ion_kick(h, k))) return e;
     }
     int mom = -1;
     if (k + 1 < h.K) mom = c.flag_beam_ion ? k + 1 : -1;
@@ -822,6 +827,14 @@ int cg_run_turns(cg_handle* H, int turn0, int n_turns) {
   }
   for (int n = 0; n < n_turns; ++n) {
     CG_CUDA(&h, cudaGraphLaunch(h.turn_graph, h.stream));
+    if (h.d.sur_w && h.sur_audit_every > 0 && h.cfg.flag_beam_ion &&
+        ((turn0 + n + 1) % h.sur_audit_every) == 0) {
+      double a[2];
+      if ((st = cg_surrogate_audit(H, h.K - 1, a))) return st;
+      h.sur_audit_last = a[1] > 0 ? a[0] / a[1] : 0.0;
+      h.sur_audit_worst = std::max(h.sur_audit_worst, h.sur_audit_last);
+      h.sur_audits++;
+    }
     // status is polled every 64 turns (and at the end) to keep the GPU fed
     if (((n + 1) & 63) == 0 || n + 1 == n_turns) {
       if ((st = check_status(h))) return st;
@@ -1054,6 +1067,289 @@ int cg_gaussian_field(const double* x, const double* y, const double* sx, const 
   const double* in[4] = {x, y, sx, sy};
   double* out[2] = {fx, fy};
   return eval_arrays(4, in, 2, out, n, 2);
+}
+
+// ---- field surrogate ----
+
+}  // extern "C"
+
+namespace {
+
+// Device buffers of one surrogate call, freed on every exit path.
+struct DevBufs {
+  std::vector<void*> p;
+  ~DevBufs() {
+    for (void* q : p) dfree(q);
+  }
+  template <class T>
+  T* get(size_t count) {
+    void* q = nullptr;
+    if (cudaMalloc(&q, std::max<size_t>(count * sizeof(T), 16)) != cudaSuccess) return nullptr;
+    p.push_back(q);
+    return static_cast<T*>(q);
+  }
+};
+
+int sur_device_ready() {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(nullptr, CG_ERR_CUDA, "no CUDA device available (the library has no CPU path)");
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (ensure_weideman(dev)) return fail(nullptr, CG_ERR_CUDA, "Weideman table upload failed");
+  cudaError_t e = prepare_surrogate();
+  if (e != cudaSuccess) return cuda_fail(nullptr, e, "surrogate kernel attributes");
+  return CG_OK;
+}
+
+int sur_status(int* d_status) {
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return cuda_fail(nullptr, e, "surrogate kernels");
+  int st = 0;
+  cudaMemcpy(&st, d_status, sizeof(int), cudaMemcpyDeviceToHost);
+  if (st & kStatusSurrogateWait)
+    return fail(nullptr, CG_ERR_TIMEOUT, "a tensor-core completion wait gave up");
+  return st ? fail(nullptr, CG_ERR_CUDA, "unexpected device status") : CG_OK;
+}
+
+// splitmix64 (Steele, Lea and Flood 2014): the host's seeded stream for the
+// initial weights and the per-epoch sample order.
+uint64_t splitmix64(uint64_t& s) {
+  uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+}  // namespace
+
+extern "C" {
+
+int cg_surrogate_dataset(uint64_t seed, int64_t n, float* inputs, float* targets) {
+  if (n < 0 || (n > 0 && (!inputs || !targets))) return fail(nullptr, CG_ERR_INVALID, "bad arguments");
+  if (n == 0) return CG_OK;
+  int st = sur_device_ready();
+  if (st) return st;
+  DevBufs b;
+  float* x = b.get<float>(3 * (size_t)n);
+  float* t = b.get<float>(2 * (size_t)n);
+  if (!x || !t) return fail(nullptr, CG_ERR_OOM, "surrogate dataset");
+  cudaError_t e = launch_sur_data(seed, n, x, t, 0);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return cuda_fail(nullptr, e, "surrogate dataset");
+  cudaMemcpy(inputs, x, 3 * n * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaMemcpy(targets, t, 2 * n * sizeof(float), cudaMemcpyDeviceToHost);
+  return CG_OK;
+}
+
+int cg_surrogate_eval(const float* weights, const float* inputs, int64_t n, float* outputs) {
+  if (!weights || n < 0 || (n > 0 && (!inputs || !outputs)))
+    return fail(nullptr, CG_ERR_INVALID, "bad arguments");
+  if (n == 0) return CG_OK;
+  int st = sur_device_ready();
+  if (st) return st;
+  DevBufs b;
+  float* w = b.get<float>(CG_SUR_PARAMS);
+  float* x = b.get<float>(3 * (size_t)n);
+  float* o = b.get<float>(2 * (size_t)n);
+  int* s = b.get<int>(1);
+  if (!w || !x || !o || !s) return fail(nullptr, CG_ERR_OOM, "surrogate eval");
+  cudaMemcpy(w, weights, CG_SUR_PARAMS * sizeof(float), cudaMemcpyHostToDevice);
+  cudaMemcpy(x, inputs, 3 * n * sizeof(float), cudaMemcpyHostToDevice);
+  cudaMemset(s, 0, sizeof(int));
+  cudaError_t e = launch_sur_eval(w, x, n, o, s, 0);
+  if (e != cudaSuccess) return cuda_fail(nullptr, e, "surrogate eval launch");
+  if ((st = sur_status(s))) return st;
+  cudaMemcpy(outputs, o, 2 * n * sizeof(float), cudaMemcpyDeviceToHost);
+  return CG_OK;
+}
+
+int cg_surrogate_grad(const float* weights, const float* inputs, const float* targets, int n,
+                      float* grads, double* loss) {
+  if (!weights || !inputs || !targets || !grads || n <= 0 || n % 128 != 0 || n > 65536)
+    return fail(nullptr, CG_ERR_INVALID, "n must be a positive multiple of 128, at most 65536");
+  int st = sur_device_ready();
+  if (st) return st;
+  DevBufs b;
+  const int ncta = n / 128;
+  float* w = b.get<float>(CG_SUR_PARAMS);
+  float* x = b.get<float>(3 * (size_t)n);
+  float* t = b.get<float>(2 * (size_t)n);
+  float* part = b.get<float>((size_t)ncta * (CG_SUR_PARAMS + 1));
+  float* g = b.get<float>(CG_SUR_PARAMS);
+  double* l = b.get<double>(1);
+  int* s = b.get<int>(1);
+  if (!w || !x || !t || !part || !g || !l || !s) return fail(nullptr, CG_ERR_OOM, "surrogate grad");
+  cudaMemcpy(w, weights, CG_SUR_PARAMS * sizeof(float), cudaMemcpyHostToDevice);
+  cudaMemcpy(x, inputs, 3 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice);
+  cudaMemcpy(t, targets, 2 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice);
+  cudaMemset(l, 0, sizeof(double));
+  cudaMemset(s, 0, sizeof(int));
+  cudaError_t e = launch_sur_step(w, x, t, n, 0, n, 1, 0, part, nullptr, nullptr, nullptr, 0.0f,
+                                  1.0f, 1.0f, l, g, s, 0);
+  if (e != cudaSuccess) return cuda_fail(nullptr, e, "surrogate grad launch");
+  if ((st = sur_status(s))) return st;
+  cudaMemcpy(grads, g, CG_SUR_PARAMS * sizeof(float), cudaMemcpyDeviceToHost);
+  if (loss) {
+    double lh = 0;
+    cudaMemcpy(&lh, l, sizeof(double), cudaMemcpyDeviceToHost);
+    *loss = lh / (2.0 * n);
+  }
+  return CG_OK;
+}
+
+int cg_surrogate_train(const cg_sur_train_params* p, float* weights, double* stats) {
+  if (!p || !weights || p->batch <= 0 || p->batch % 128 != 0 || p->n_train < p->batch ||
+      p->n_train % p->batch != 0 || p->n_holdout < 1 || p->epochs < 1 || !(p->lr > 0))
+    return fail(nullptr, CG_ERR_INVALID, "bad training parameters");
+  int st = sur_device_ready();
+  if (st) return st;
+  const int64_t n = p->n_train, nh = p->n_holdout;
+  const int ncta = p->batch / 128;
+  DevBufs b;
+  float* x = b.get<float>(3 * (size_t)n);
+  float* t = b.get<float>(2 * (size_t)n);
+  float* xh = b.get<float>(3 * (size_t)nh);
+  float* th = b.get<float>(2 * (size_t)nh);
+  float* oh = b.get<float>(2 * (size_t)nh);
+  float* w = b.get<float>(CG_SUR_PARAMS);
+  float* m = b.get<float>(CG_SUR_PARAMS);
+  float* v = b.get<float>(CG_SUR_PARAMS);
+  float* part = b.get<float>((size_t)ncta * (CG_SUR_PARAMS + 1));
+  double* l = b.get<double>(1);
+  int* s = b.get<int>(1);
+  if (!x || !t || !xh || !th || !oh || !w || !m || !v || !part || !l || !s)
+    return fail(nullptr, CG_ERR_OOM, "surrogate training buffers");
+  // initial weights: uniform in +-1/sqrt(fan_in) (the common default of
+  // linear layers), from the seeded host stream
+  std::vector<float> w0(CG_SUR_PARAMS);
+  uint64_t rs = p->seed ^ 0x5357u;
+  auto fill = [&](int off, int count, int fan_in) {
+    const double bound = 1.0 / std::sqrt((double)fan_in);
+    for (int i = 0; i < count; ++i) {
+      const double u = (double)(splitmix64(rs) >> 11) * (1.0 / 9007199254740992.0);
+      w0[off + i] = (float)((2.0 * u - 1.0) * bound);
+    }
+  };
+  fill(kSurW1, 192, 3); fill(kSurB1, 64, 3);
+  fill(kSurW2, 4096, 64); fill(kSurB2, 64, 64);
+  fill(kSurW3, 4096, 64); fill(kSurB3, 64, 64);
+  fill(kSurW4, 128, 64); fill(kSurB4, 2, 64);
+  cudaMemcpy(w, w0.data(), CG_SUR_PARAMS * sizeof(float), cudaMemcpyHostToDevice);
+  cudaMemset(m, 0, CG_SUR_PARAMS * sizeof(float));
+  cudaMemset(v, 0, CG_SUR_PARAMS * sizeof(float));
+  cudaMemset(s, 0, sizeof(int));
+  cudaError_t e = launch_sur_data(p->seed, n, x, t, 0);
+  if (e == cudaSuccess) e = launch_sur_data(p->seed + 1, nh, xh, th, 0);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return cuda_fail(nullptr, e, "surrogate dataset");
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, 0);
+  const int64_t steps_per_epoch = n / p->batch;
+  const int64_t total = steps_per_epoch * p->epochs;
+  const int64_t warm = std::max<int64_t>(1, (int64_t)(0.3 * total));
+  int64_t step = 0;
+  for (int ep = 0; ep < p->epochs && e == cudaSuccess; ++ep) {
+    // sample order of the epoch: j -> (mul j + add) mod n, mul odd and
+    // coprime to n when n is a power of two (any n: the map is still a
+    // bijection when gcd(mul, n) = 1, which the loop below enforces)
+    uint64_t mul = splitmix64(rs) | 1u, add = splitmix64(rs) % (uint64_t)n;
+    auto gcd = [](uint64_t a, uint64_t c) { while (c) { uint64_t r = a % c; a = c; c = r; } return a; };
+    mul %= (uint64_t)n;
+    while (gcd(mul, (uint64_t)n) != 1) mul = (mul + 2) % (uint64_t)n;
+    if (ep == p->epochs - 1) cudaMemsetAsync(l, 0, sizeof(double), 0);
+    for (int64_t q = 0; q < steps_per_epoch && e == cudaSuccess; ++q, ++step) {
+      double lr = step < warm ? p->lr * (double)(step + 1) / warm
+                              : p->lr * 0.5 * (1.0 + std::cos(3.14159265358979323846 *
+                                                               (double)(step - warm) / (total - warm)));
+      const float bc1 = (float)(1.0 - std::pow(0.9, (double)(step + 1)));
+      const float bc2 = (float)(1.0 - std::pow(0.999, (double)(step + 1)));
+      e = launch_sur_step(w, x, t, n, q * p->batch, p->batch, mul, add, part, m, v, w, (float)lr,
+                          bc1, bc2, ep == p->epochs - 1 ? l : nullptr, nullptr, s, 0);
+    }
+  }
+  cudaEventRecord(e1, 0);
+  if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (e != cudaSuccess) return cuda_fail(nullptr, e, "surrogate training");
+  if ((st = sur_status(s))) return st;
+  if ((e = launch_sur_eval(w, xh, nh, oh, s, 0)) != cudaSuccess)
+    return cuda_fail(nullptr, e, "surrogate hold-out");
+  if ((st = sur_status(s))) return st;
+  std::vector<float> ph(2 * nh), tt(2 * nh);
+  cudaMemcpy(ph.data(), oh, 2 * nh * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaMemcpy(tt.data(), th, 2 * nh * sizeof(float), cudaMemcpyDeviceToHost);
+  double peak = 0, se = 0, emax = 0;
+  for (int64_t i = 0; i < 2 * nh; ++i) peak = std::max(peak, (double)std::fabs(tt[i]));
+  for (int64_t i = 0; i < 2 * nh; ++i) {
+    const double d = (double)ph[i] - (double)tt[i];
+    se += d * d;
+    emax = std::max(emax, std::fabs(d));
+  }
+  double lh = 0;
+  cudaMemcpy(&lh, l, sizeof(double), cudaMemcpyDeviceToHost);
+  cudaMemcpy(weights, w, CG_SUR_PARAMS * sizeof(float), cudaMemcpyDeviceToHost);
+  if (stats) {
+    stats[0] = lh / (2.0 * (double)n);
+    stats[1] = std::sqrt(se / (2.0 * (double)nh)) / peak;
+    stats[2] = emax / peak;
+    stats[3] = ms * 1e-3;
+  }
+  return CG_OK;
+}
+
+int cg_set_surrogate(cg_handle* H, const float* weights, int audit_interval) {
+  STAGE_PROLOGUE
+  if (audit_interval < 0) return fail(&h, CG_ERR_INVALID, "audit_interval < 0");
+  if (h.turn_graph) {
+    cudaGraphExecDestroy(h.turn_graph);
+    h.turn_graph = nullptr;
+  }
+  if (!weights) {
+    dfree(h.d.sur_w);
+    h.d.sur_w = nullptr;
+    h.sur_audit_every = 0;
+    return CG_OK;
+  }
+  cudaError_t e = prepare_surrogate();
+  if (e != cudaSuccess) return cuda_fail(&h, e, "surrogate kernel attributes");
+  if (!h.d.sur_w && dalloc(&h.d.sur_w, CG_SUR_PARAMS)) return fail(&h, CG_ERR_OOM, "surrogate weights");
+  if (!h.d.sur_audit && dalloc(&h.d.sur_audit, 2)) return fail(&h, CG_ERR_OOM, "surrogate audit");
+  CG_CUDA(&h, cudaMemcpy(h.d.sur_w, weights, CG_SUR_PARAMS * sizeof(float), cudaMemcpyHostToDevice));
+  h.sur_audit_every = audit_interval;
+  h.sur_audits = 0;
+  h.sur_audit_last = h.sur_audit_worst = 0;
+  return CG_OK;
+}
+
+int cg_surrogate_audit(cg_handle* H, int k, double* out) {
+  STAGE_PROLOGUE
+  if (!out) return fail(&h, CG_ERR_INVALID, "out is NULL");
+  if (!h.d.sur_w) return fail(&h, CG_ERR_NOT_READY, "no surrogate set (cg_set_surrogate)");
+  if (!h.cfg.flag_beam_ion) return fail(&h, CG_ERR_NOT_READY, "runBeamIonFlag is off");
+  if (k < 0 || k >= h.K) return fail(&h, CG_ERR_INVALID, "section index out of range");
+  CG_CUDA(&h, cudaMemsetAsync(h.d.sur_audit, 0, 2 * sizeof(unsigned long long), h.stream));
+  int st = launch_ok(h, launch_sur_audit(h, k, h.d.sur_audit), "surrogate audit");
+  if (st || (st = check_status(h))) return st;
+  unsigned long long bits[2];
+  CG_CUDA(&h, cudaMemcpy(bits, h.d.sur_audit, sizeof bits, cudaMemcpyDeviceToHost));
+  std::memcpy(&out[0], &bits[0], sizeof(double));
+  std::memcpy(&out[1], &bits[1], sizeof(double));
+  return CG_OK;
+}
+
+int cg_surrogate_audit_stats(cg_handle* H, int* count, double* last, double* worst) {
+  if (!H) return CG_ERR_INVALID;
+  Handle& h = H->h;
+  if (count) *count = h.sur_audits;
+  if (last) *last = h.sur_audit_last;
+  if (worst) *worst = h.sur_audit_worst;
+  return CG_OK;
 }
 
 // ---- device buffers in/out, no allocation ----

@@ -97,6 +97,7 @@ enum : uint32_t {
   kStreamSynrad = 0x5359u,    // quantum excitation noise
   kStreamIonBirth = 0x494Fu,  // macro-ion birth positions
   kStreamInitDist = 0x4449u,  // initial distribution
+  kStreamSurrogate = 0x5347u, // surrogate training samples
 };
 
 }  // namespace cg

@@ -85,6 +85,9 @@ struct DeviceBufs {
   CloudRec* rec = nullptr;         // K x M x P
   double* ion_totals = nullptr;    // K (charge), used by cg_ion_totals
   IonWalk iw;
+  // field surrogate
+  float* sur_w = nullptr;                 // FP32 parameters (null: exact kicks)
+  unsigned long long* sur_audit = nullptr;  // audit maxima (double bit patterns)
   // long-range wake
   double* lr_tab = nullptr;        // 3 x np
   double* lr_hist = nullptr;       // turns x 3 x M ring buffer
@@ -131,6 +134,9 @@ struct Handle {
   bool beam_set = false;
   int ion_cap = 0;
   cudaGraphExec_t turn_graph = nullptr;
+  int sur_audit_every = 0;     // turns between exact audits of the surrogate (0: none)
+  int sur_audits = 0;
+  double sur_audit_last = 0, sur_audit_worst = 0;
   std::string err;
 };
 

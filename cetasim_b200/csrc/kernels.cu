@@ -816,7 +816,8 @@ cudaError_t measure_fp64_peak(double* flops) {
 
 cudaError_t upload_weideman_table() {
   cudaError_t e = cudaMemcpyToSymbol(c_weideman, &h_weideman, sizeof(WeidemanTable));
-  return e != cudaSuccess ? e : upload_weideman_table_ion();
+  if (e == cudaSuccess) e = upload_weideman_table_ion();
+  return e != cudaSuccess ? e : upload_weideman_table_sur();
 }
 
 // ---------------------------------------------------------------------------

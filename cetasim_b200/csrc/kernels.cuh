@@ -10,6 +10,7 @@ enum : int {
   kStatusTransmission = 2,
   kStatusLrRange = 4,
   kStatusIonBirth = 8,
+  kStatusSurrogateWait = 16,  // a tensor-core completion wait gave up
 };
 
 cudaError_t launch_moments(Handle& h, int k);
@@ -39,6 +40,19 @@ cudaError_t launch_faddeeva(const double* zr, const double* zi, double* wr, doub
                             bool general, cudaStream_t s);
 cudaError_t launch_field(const double* x, const double* y, const double* sx, const double* sy,
                          double* fx, double* fy, int64_t n, cudaStream_t s);
+// field surrogate (surrogate.cu)
+cudaError_t prepare_surrogate();
+cudaError_t launch_sur_data(uint64_t seed, int64_t n, float* xin, float* tout, cudaStream_t s);
+cudaError_t launch_sur_eval(const float* w, const float* xin, int64_t n, float* out, int* status,
+                            cudaStream_t s);
+cudaError_t launch_sur_step(const float* w, const float* xin, const float* tin, int64_t n,
+                            int64_t row0, int batch, uint64_t mul, uint64_t add, float* part,
+                            float* m, float* v, float* wmut, float lr, float bc1, float bc2,
+                            double* loss, float* grad_out, int* status, cudaStream_t s);
+cudaError_t launch_ion_kick_sur(Handle& h, int k);
+cudaError_t launch_sur_audit(Handle& h, int k, unsigned long long* out);
+cudaError_t upload_weideman_table_sur();
+
 cudaError_t upload_weideman_table();      // every translation unit that evaluates w(z)
 cudaError_t upload_weideman_table_ion();
 

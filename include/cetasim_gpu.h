@@ -327,6 +327,54 @@ int cg_faddeeva_w_q1(const double* zr, const double* zi, double* wr, double* wi,
 int cg_gaussian_field(const double* x, const double* y, const double* sx,
                       const double* sy, double* fx, double* fy, int64_t n);
 
+/* ---- field surrogate (no counterpart in the reference) ---- */
+
+/* A 3 -> 64 -> 64 -> 64 -> 2 MLP (SiLU, BF16 weights, FP32 accumulation) for
+ * the normalised Gaussian-beam field of Bunch::BassettiErskine1 /
+ * GaussianField (Bunch.cpp:119-211).  Inputs a = |x|/(8 sigma_x),
+ * b = |y|/(8 sigma_y) in [0, 1] and r = sigma_y/sigma_x in [0.05, 1]
+ * (sigma_x >= sigma_y); outputs G = -sigma_x (F_x, F_y) at (|x|, |y|).
+ * Parameters (CG_SUR_PARAMS floats): W1[64][3] b1[64] W2[64][64] b2[64]
+ * W3[64][64] b3[64] W4[2][64] b4[2]; weights are used rounded to BF16. */
+#define CG_SUR_PARAMS 8706
+
+typedef struct cg_sur_train_params {
+  uint64_t seed;       /* training set, hold-out set (seed + 1) and initial weights */
+  int64_t n_train;     /* training samples, a multiple of batch */
+  int64_t n_holdout;   /* hold-out samples */
+  int epochs;
+  int batch;           /* a multiple of 128 */
+  double lr;           /* peak Adam learning rate (30 % linear warm-up, cosine decay) */
+} cg_sur_train_params;
+
+/* n samples (a, b, r) of the exact FP64 field (Philox-seeded) -> inputs
+ * [n][3], targets G [n][2] (host buffers). */
+int cg_surrogate_dataset(uint64_t seed, int64_t n, float* inputs, float* targets);
+/* Network outputs for n inputs (a, b, r) on the tensor cores (host buffers). */
+int cg_surrogate_eval(const float* weights, const float* inputs, int64_t n,
+                      float* outputs);
+/* Gradient of L = sum (out - target)^2 / (2n) for n samples (a multiple of
+ * 128, at most 65536) from the training kernels; *loss = L. */
+int cg_surrogate_grad(const float* weights, const float* inputs, const float* targets,
+                      int n, float* grads, double* loss);
+/* Trains from seeded initial weights on seeded exact-field samples, all on the
+ * GPU; weights (CG_SUR_PARAMS) out.  stats[0] = final training loss per
+ * output, stats[1] = hold-out RMS error of G relative to the hold-out peak
+ * |G|, stats[2] = hold-out maximum error relative to that peak, stats[3] =
+ * training time [s]. */
+int cg_surrogate_train(const cg_sur_train_params* p, float* weights, double* stats);
+/* Electron-side ion kicks of h from the surrogate (NULL weights: the exact
+ * path again); points outside the domain take the exact path.  Every
+ * audit_interval turns of cg_run_turns (0: never) the exact path judges the
+ * surrogate on the current beam (cg_surrogate_audit at the last IP). */
+int cg_set_surrogate(cg_handle* h, const float* weights, int audit_interval);
+/* At IP k, over the alive particles inside the domain: out[0] = max |F_sur -
+ * F_exact|, out[1] = max |F_exact| (1/m, both components, the cloud records
+ * of the last ion pass at k). */
+int cg_surrogate_audit(cg_handle* h, int k, double* out);
+/* Audits made by cg_run_turns: count, last and worst ratio out[0]/out[1]. */
+int cg_surrogate_audit_stats(cg_handle* h, int* count, double* last, double* worst);
+
 /* ---- device buffers in/out, no allocation ---- */
 
 /* Largest n of one cg_bunch_moments_noalloc call (4096 tiles of 256). */
