@@ -36,6 +36,9 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+BATCHED_DESC = ("batched_uneven: 900 of 1000 buckets filled, 5e3-5e4 FP64 macroparticles "
+                "per bunch (log-uniform), 50 IPs, CO ions, exact Bassetti-Erskine both ways, "
+                "long-range HOM wake, 9-tap FIR, synchrotron radiation with quantum excitation")
 WORKLOAD_DESC = ("fast_ion: 80 bunches x 2e4 FP64 macroparticles, 2 ns spacing, 20 IPs, "
                  "CO at 1e-9 Pa, 1 macro-ion/bunch/IP, exact Bassetti-Erskine both ways, "
                  "synchrotron radiation with quantum excitation")
@@ -149,6 +152,10 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n-scale", type=float, default=1.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-surrogate", action="store_true",
+                    help="skip the surrogate measurement (training + surrogate turns)")
+    ap.add_argument("--workload", default="fast_ion", choices=["fast_ion", "batched_uneven"],
+                    help="batched_uneven: 900 bunches of 5e3-5e4, 50 IPs, LR wake + FIR")
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.impl == "reference":
@@ -166,7 +173,7 @@ def main():
     from cetasim_b200.beam import MPBeam
 
     lib = _abi.load()
-    wl = configs.make("fast_ion", n_scale=args.n_scale, seed=1234 + rank)
+    wl = configs.make(args.workload, n_scale=args.n_scale, seed=1234 + rank)
     beam = MPBeam(wl, device=local)
     beam.generate(seed=99 + rank)
     stream = torch.cuda.ExternalStream(lib.cg_stream(beam.h))
@@ -262,12 +269,15 @@ def main():
     lib.cg_fp64_peak(C.byref(peak))
     flops_per_kick = FLOPS_PER_KICK
     achieved = n_part * flops_per_kick / (kick_ms.value * 1e-3)
-    traffic = kick_traffic()
+    traffic = kick_traffic() if args.workload == "fast_ion" else None
+    sur = None
+    if world == 1 and not args.no_surrogate:
+        sur = surrogate_leg(args, beam, lib, stream, flush, kick_ms.value, tot_ms / args.steps)
 
     result = None
     if rank == 0:
         cpu = None
-        if not args.no_cpu and world == 1:
+        if not args.no_cpu and world == 1 and args.workload == "fast_ion":
             try:
                 v, dt, n = cpu_sample(turns=1)
                 cpu = {"value": v, "unit": "macroparticle-turns/s",
@@ -283,7 +293,8 @@ def main():
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": tot_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD_DESC, "bunches": wl.n_bunches,
+            "config": {"workload": WORKLOAD_DESC if args.workload == "fast_ion" else
+                       BATCHED_DESC, "bunches": wl.n_bunches,
                        "macroparticles": n_part, "interaction_points": wl.cfg.n_sections,
                        "turns_per_step": 1, "l2": "flushed between turns (512 MB write)",
                        "parallelism": f"replica x{world}"},
@@ -302,6 +313,7 @@ def main():
                           "us_per_bunch_step": 1e3 * chain_ms.value / wl.n_bunches,
                           "bound": "latency (one field evaluation per bunch step)"},
             "cpu_baseline": cpu,
+            "surrogate": sur,
             "e2e": {"value": e2e_value, "unit": "macroparticle-turns/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches.value * args.steps,
@@ -319,6 +331,43 @@ def main():
 # series, the exp of the Gaussian factor counted as one operation, and the
 # field algebra), counted from be_field.cuh / faddeeva.cuh: 2 x 307 + 32.
 FLOPS_PER_KICK = 646
+
+
+def surrogate_leg(args, beam, lib, stream, flush, exact_kick_ms, exact_turn_ms):
+    """The learned field in place of the exact one: trains the surrogate on the
+    GPU (2^20 exact-field samples), then times its kick kernel and whole turns
+    with it, the same way as the exact path."""
+    import torch
+    from cetasim_b200 import surrogate as S
+    w, st = S.train()
+    beam.set_surrogate(w)
+    k_ms = C.c_double()
+    beam._check(lib.cg_time_stage(beam.h, 6, 0, 20, C.byref(k_ms)))
+    t0 = 10 ** 6
+    beam.Run(t0, 2)
+    ev = []
+    for s in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        beam.Run(t0 + 2 + s, 1)
+        e1.record(stream)
+        ev.append((e0, e1))
+    torch.cuda.synchronize()
+    turn_ms = sum(a.elapsed_time(b) for a, b in ev) / len(ev)
+    audit = beam.surrogate_audit(beam.wl.cfg.n_sections - 1)
+    beam.set_surrogate(None)
+    n = beam.wl.n_particles
+    return {"network": "3-64-64-64-2 SiLU, BF16 weights, FP32 accumulation, tcgen05",
+            "holdout_rms_rel": st[1], "holdout_max_rel": st[2], "train_s": st[3],
+            "kick_ms": k_ms.value, "exact_kick_ms": exact_kick_ms,
+            "kick_speedup": exact_kick_ms / k_ms.value,
+            "ion_kicks_per_s_kernel": n / (k_ms.value * 1e-3),
+            "ms_per_turn": turn_ms, "exact_ms_per_turn": exact_turn_ms,
+            "turn_speedup": exact_turn_ms / turn_ms,
+            "audit_max_field_err_rel": audit[0] / audit[1] if audit[1] else None}
 
 
 def kick_traffic():

@@ -878,7 +878,7 @@ int cg_turn_launches(cg_handle* H, int* launches) {
 int cg_time_stage(cg_handle* H, int stage, int k, int reps, double* ms) {
   STAGE_PROLOGUE
   if (k < 0 || k >= h.K || reps < 1 || !ms) return fail(&h, CG_ERR_INVALID, "bad arguments");
-  if ((stage == 1 || stage == 2 || stage == 5) && !h.cfg.flag_beam_ion)
+  if ((stage == 1 || stage == 2 || stage == 6) && !h.cfg.flag_beam_ion)
     return fail(&h, CG_ERR_NOT_READY, "runBeamIonFlag is off");
   cudaEvent_t e0, e1;
   CG_CUDA(&h, cudaEventCreate(&e0));
@@ -892,6 +892,9 @@ int cg_time_stage(cg_handle* H, int stage, int k, int reps, double* ms) {
       case 2: e = launch_ion_chain(h, k); break;
       case 3: e = launch_moments(h, k); break;
       case 5: e = launch_map_pass(h, k, k); break;
+      case 6:
+        e = h.d.sur_w ? launch_ion_kick_sur(h, k) : cudaErrorInvalidValue;
+        break;
       default: e = launch_long(h, kLongRF | kLongDrift | kLongLoss | (h.cfg.flag_synrad ? kLongSynrad : 0));
     }
   }

@@ -41,7 +41,10 @@ struct SurSmall {
 };
 
 __device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
+// SiLU with the hardware exponential and reciprocal (a few ulp in FP32, far
+// below the BF16 weight rounding of the model); for z < -87 the exponential
+// overflows and the quotient is -0, the limit.
+__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
 __device__ __forceinline__ float dsilu(float z) {
   const float s = 1.0f / (1.0f + __expf(-z));
   return s * fmaf(z, 1.0f - s, 1.0f);
@@ -449,6 +452,13 @@ __device__ __forceinline__ void sur_frame(const CloudRec& rc, double x, double y
   *s_large = sl;
 }
 
+// The exact path for points outside the network's domain, out of line so that
+// its registers do not add to the network's.
+__device__ __noinline__ void exact_field_fallback(const CloudRec& rc, double x, double y,
+                                                  double* fx, double* fy) {
+  gaussian_field_kick(field_prep(rc.rms_x, rc.rms_y), x - rc.aver_x, y - rc.aver_y, fx, fy);
+}
+
 // Field (1/m, the reference's tempFx/tempFy) from the network outputs G.
 __device__ __forceinline__ void sur_field(const float (&o)[2], bool swap, double u, double v,
                                           double sl, double* fx, double* fy) {
@@ -458,7 +468,7 @@ __device__ __forceinline__ void sur_field(const float (&o)[2], bool swap, double
   *fy = swap ? fu : fv;
 }
 
-__global__ void __launch_bounds__(kSurRows, 2) k_ion_kick_sur(double* __restrict__ c, int64_t npad,
+__global__ void __launch_bounds__(kSurRows, 3) k_ion_kick_sur(double* __restrict__ c, int64_t npad,
                                                            const uint8_t* __restrict__ surv,
                                                            const int* __restrict__ tile_bunch,
                                                            const BunchDev* __restrict__ bunch,
@@ -494,7 +504,7 @@ __global__ void __launch_bounds__(kSurRows, 2) k_ion_kick_sur(double* __restrict
       if (dom) {
         sur_field(o, sw, u, v, sl, &fx, &fy);
       } else {
-        gaussian_field_kick(field_prep(rc.rms_x, rc.rms_y), x - rc.aver_x, y - rc.aver_y, &fx, &fy);
+        exact_field_fallback(rc, x, y, &fx, &fy);
       }
       dpx = fma(rc.coeff, fx, dpx);
       dpy = fma(rc.coeff, fy, dpy);
@@ -567,7 +577,7 @@ static int sur_grid(int64_t tiles) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  return (int)std::max<int64_t>(1, std::min<int64_t>(tiles, 2 * (int64_t)sms));
+  return (int)std::max<int64_t>(1, std::min<int64_t>(tiles, 4 * (int64_t)sms));
 }
 
 cudaError_t prepare_surrogate() {

@@ -290,8 +290,8 @@ int cg_turn_launches(cg_handle* h, int* launches);
  * h's stream; *ms = average per launch.  stage: 0 section map (k), 1 ion
  * field kick (k, uses the records of the last cg_beam_ion_ip at k), 2 ion
  * chain (k), 3 moments (k), 4 longitudinal turn tail, 5 the map + moments
- * pass of the turn graph (section k). The beam state is advanced by these
- * launches. */
+ * pass of the turn graph (section k), 6 the surrogate field kick (k, after
+ * cg_set_surrogate). The beam state is advanced by these launches. */
 int cg_time_stage(cg_handle* h, int stage, int k, int reps, double* ms);
 /* FP64 FMA throughput of this device measured by a register-resident FMA
  * chain kernel, in FLOP/s (2 per FMA). */
