@@ -147,6 +147,9 @@ EXPORTS = [
     ("cg_faddeeva_w", I, [PD, PD, PD, PD, C.c_int64]),
     ("cg_faddeeva_w_q1", I, [PD, PD, PD, PD, C.c_int64]),
     ("cg_gaussian_field", I, [PD, PD, PD, PD, PD, PD, C.c_int64]),
+    ("cg_checkpoint_size", I, [C.c_void_p, C.POINTER(C.c_size_t)]),
+    ("cg_checkpoint_save", I, [C.c_void_p, C.c_void_p, C.c_size_t]),
+    ("cg_checkpoint_load", I, [C.c_void_p, C.c_void_p, C.c_size_t]),
     ("cg_surrogate_dataset", I, [C.c_uint64, C.c_int64, PF, PF]),
     ("cg_surrogate_eval", I, [PF, PF, C.c_int64, PF]),
     ("cg_surrogate_grad", I, [PF, PF, PF, I, PF, PD]),

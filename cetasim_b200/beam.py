@@ -105,6 +105,18 @@ class MPBeam:
     def Run(self, turn0: int, n_turns: int):
         self._check(self.lib.cg_run_turns(self.h, turn0, n_turns))
 
+    # -- checkpoint / resume ------------------------------------------------------
+    def checkpoint(self) -> bytes:
+        n = C.c_size_t()
+        self._check(self.lib.cg_checkpoint_size(self.h, C.byref(n)))
+        buf = C.create_string_buffer(n.value)
+        self._check(self.lib.cg_checkpoint_save(self.h, buf, n.value))
+        return buf.raw
+
+    def restore(self, blob: bytes):
+        buf = C.create_string_buffer(blob, len(blob))
+        self._check(self.lib.cg_checkpoint_load(self.h, buf, len(blob)))
+
     # -- field surrogate (no reference counterpart) -------------------------------
     def set_surrogate(self, weights, audit_interval: int = 0):
         """Electron-side ion kicks from the trained surrogate (None: exact)."""

@@ -1072,6 +1072,174 @@ int cg_gaussian_field(const double* x, const double* y, const double* sx, const 
   return eval_arrays(4, in, 2, out, n, 2);
 }
 
+// ---- checkpoint / resume ----
+
+}  // extern "C"
+
+namespace {
+
+constexpr uint64_t kCkptMagic = 0x43474B5043545331ull;  // "CGKPCTS1"
+
+struct CkptHeader {
+  uint64_t magic;
+  int32_t version, M, K, P;
+  int64_t npad;
+  int32_t ion_cap, lr_turns, fir_order, sr_bins;
+  int32_t flags;  // beam_ion | lr << 1 | fir << 2 | sr << 3
+  int32_t pad;
+  uint64_t cloud_ions;  // sum of the saved cloud counts
+};
+
+// The pieces of device state a checkpoint holds, in order; `op` is applied
+// to (device pointer, bytes) of each fixed piece.  Ion clouds are handled
+// separately (only their first n entries are stored).
+template <class Op>
+int ckpt_fixed(Handle& h, Op op) {
+  const size_t M = (size_t)h.M;
+  int st;
+  if ((st = op(h.d.c, 6 * (size_t)h.npad * sizeof(double)))) return st;
+  if ((st = op(h.d.surv, (size_t)h.npad))) return st;
+  if ((st = op(h.d.mom, M * sizeof(BunchMomDev)))) return st;
+  if (h.cfg.flag_lr_wake) {
+    if ((st = op(h.d.lr_hist, (size_t)h.cfg.lr_turns * 3 * M * sizeof(double)))) return st;
+    if ((st = op(h.d.lr_head, sizeof(int)))) return st;
+  }
+  if (h.cfg.flag_fir) {
+    if ((st = op(h.d.fir_hist, (size_t)h.fir_order * 3 * M * sizeof(double)))) return st;
+    if ((st = op(h.d.fir_head, sizeof(int)))) return st;
+  }
+  if (h.cfg.flag_sr_wake && (st = op(h.d.sr_pot, M * (size_t)h.cfg.sr_bins * sizeof(double))))
+    return st;
+  return CG_OK;
+}
+
+CkptHeader ckpt_header(const Handle& h) {
+  CkptHeader c{};
+  c.magic = kCkptMagic;
+  c.version = 1;
+  c.M = h.M;
+  c.K = h.K;
+  c.P = h.P;
+  c.npad = h.npad;
+  c.ion_cap = h.ion_cap;
+  c.lr_turns = h.cfg.flag_lr_wake ? h.cfg.lr_turns : 0;
+  c.fir_order = h.cfg.flag_fir ? h.fir_order : 0;
+  c.sr_bins = h.cfg.flag_sr_wake ? h.cfg.sr_bins : 0;
+  c.flags = (h.cfg.flag_beam_ion ? 1 : 0) | (h.cfg.flag_lr_wake ? 2 : 0) |
+            (h.cfg.flag_fir ? 4 : 0) | (h.cfg.flag_sr_wake ? 8 : 0);
+  return c;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cg_checkpoint_size(cg_handle* H, size_t* bytes) {
+  STAGE_PROLOGUE
+  if (!bytes) return fail(&h, CG_ERR_INVALID, "bytes is NULL");
+  CG_CUDA(&h, cudaStreamSynchronize(h.stream));
+  size_t n = sizeof(CkptHeader);
+  ckpt_fixed(h, [&](void*, size_t b) { n += b; return CG_OK; });
+  if (h.cfg.flag_beam_ion) {
+    std::vector<CloudState> s((size_t)h.K * h.P);
+    CG_CUDA(&h, cudaMemcpy(s.data(), h.d.cloud_state, sizeof(CloudState) * s.size(),
+                           cudaMemcpyDeviceToHost));
+    for (auto& c : s) n += sizeof(CloudState) + 4 * sizeof(double) * (size_t)c.n;
+  }
+  *bytes = n;
+  return CG_OK;
+}
+
+int cg_checkpoint_save(cg_handle* H, void* buf, size_t bytes) {
+  STAGE_PROLOGUE
+  size_t need = 0;
+  int st = cg_checkpoint_size(H, &need);
+  if (st) return st;
+  if (!buf || bytes < need) return fail(&h, CG_ERR_INVALID, "checkpoint buffer too small");
+  char* p = static_cast<char*>(buf);
+  CkptHeader hd = ckpt_header(h);
+  char* hp = p;
+  p += sizeof hd;
+  st = ckpt_fixed(h, [&](void* d, size_t b) {
+    if (cudaMemcpy(p, d, b, cudaMemcpyDeviceToHost) != cudaSuccess)
+      return fail(&h, CG_ERR_CUDA, "checkpoint read");
+    p += b;
+    return (int)CG_OK;
+  });
+  if (st) return st;
+  if (h.cfg.flag_beam_ion) {
+    std::vector<CloudState> s((size_t)h.K * h.P);
+    std::vector<CloudDev> cl((size_t)h.K * h.P);
+    CG_CUDA(&h, cudaMemcpy(s.data(), h.d.cloud_state, sizeof(CloudState) * s.size(),
+                           cudaMemcpyDeviceToHost));
+    CG_CUDA(&h, cudaMemcpy(cl.data(), h.d.clouds, sizeof(CloudDev) * cl.size(),
+                           cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < s.size(); ++i) {
+      std::memcpy(p, &s[i], sizeof(CloudState));
+      p += sizeof(CloudState);
+      const size_t b = sizeof(double) * (size_t)s[i].n;
+      const double* src[4] = {cl[i].x[s[i].cur], cl[i].y[s[i].cur], cl[i].vx[s[i].cur],
+                              cl[i].vy[s[i].cur]};
+      for (int q = 0; q < 4; ++q) {
+        if (b) CG_CUDA(&h, cudaMemcpy(p, src[q], b, cudaMemcpyDeviceToHost));
+        p += b;
+      }
+      hd.cloud_ions += (uint64_t)s[i].n;
+    }
+  }
+  std::memcpy(hp, &hd, sizeof hd);
+  return CG_OK;
+}
+
+int cg_checkpoint_load(cg_handle* H, const void* buf, size_t bytes) {
+  STAGE_PROLOGUE
+  if (!buf || bytes < sizeof(CkptHeader)) return fail(&h, CG_ERR_INVALID, "checkpoint too short");
+  const char* p = static_cast<const char*>(buf);
+  const char* end = p + bytes;
+  CkptHeader hd;
+  std::memcpy(&hd, p, sizeof hd);
+  p += sizeof hd;
+  CkptHeader me = ckpt_header(h);
+  if (hd.magic != kCkptMagic || hd.version != 1)
+    return fail(&h, CG_ERR_INVALID, "not a checkpoint of this library version");
+  if (hd.M != me.M || hd.K != me.K || hd.P != me.P || hd.npad != me.npad ||
+      hd.ion_cap != me.ion_cap || hd.lr_turns != me.lr_turns || hd.fir_order != me.fir_order ||
+      hd.sr_bins != me.sr_bins || hd.flags != me.flags)
+    return fail(&h, CG_ERR_INVALID, "checkpoint of a different configuration or beam layout");
+  int st = ckpt_fixed(h, [&](void* d, size_t b) {
+    if ((size_t)(end - p) < b) return fail(&h, CG_ERR_INVALID, "checkpoint truncated");
+    if (cudaMemcpy(d, p, b, cudaMemcpyHostToDevice) != cudaSuccess)
+      return fail(&h, CG_ERR_CUDA, "checkpoint write");
+    p += b;
+    return (int)CG_OK;
+  });
+  if (st) return st;
+  if (h.cfg.flag_beam_ion) {
+    std::vector<CloudDev> cl((size_t)h.K * h.P);
+    CG_CUDA(&h, cudaMemcpy(cl.data(), h.d.clouds, sizeof(CloudDev) * cl.size(),
+                           cudaMemcpyDeviceToHost));
+    std::vector<CloudState> s(cl.size());
+    for (size_t i = 0; i < cl.size(); ++i) {
+      if ((size_t)(end - p) < sizeof(CloudState)) return fail(&h, CG_ERR_INVALID, "checkpoint truncated");
+      std::memcpy(&s[i], p, sizeof(CloudState));
+      p += sizeof(CloudState);
+      if (s[i].n < 0 || s[i].n > cl[i].cap) return fail(&h, CG_ERR_INVALID, "checkpoint cloud size");
+      const size_t b = sizeof(double) * (size_t)s[i].n;
+      if ((size_t)(end - p) < 4 * b) return fail(&h, CG_ERR_INVALID, "checkpoint truncated");
+      double* dst[4] = {cl[i].x[0], cl[i].y[0], cl[i].vx[0], cl[i].vy[0]};
+      for (int q = 0; q < 4; ++q) {
+        if (b) CG_CUDA(&h, cudaMemcpy(dst[q], p, b, cudaMemcpyHostToDevice));
+        p += b;
+      }
+      s[i].cur = 0;
+    }
+    CG_CUDA(&h, cudaMemcpy(h.d.cloud_state, s.data(), sizeof(CloudState) * s.size(),
+                           cudaMemcpyHostToDevice));
+  }
+  CG_CUDA(&h, cudaDeviceSynchronize());
+  return CG_OK;
+}
+
 // ---- field surrogate ----
 
 }  // extern "C"

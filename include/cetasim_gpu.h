@@ -327,6 +327,20 @@ int cg_faddeeva_w_q1(const double* zr, const double* zi, double* wr, double* wi,
 int cg_gaussian_field(const double* x, const double* y, const double* sx,
                       const double* sy, double* fx, double* fy, int64_t n);
 
+/* ---- checkpoint / resume (no counterpart in the reference, which only
+ * writes outputs) ---- */
+
+/* Bytes of a checkpoint of h's beam state now: coordinates and survival
+ * flags, bunch moments (with transmission), ion clouds, long-range wake and
+ * FIR histories, short-range wake potentials.  Random draws are counters of
+ * (seed, turn, ...), so a run resumed with cg_run_turns(h, turn, ...) from a
+ * checkpoint taken at `turn` repeats the uninterrupted run bit for bit. */
+int cg_checkpoint_size(cg_handle* h, size_t* bytes);
+int cg_checkpoint_save(cg_handle* h, void* buf, size_t bytes);
+/* Into a handle with the same configuration and beam layout (cg_set_beam with
+ * the same bunches); CG_ERR_INVALID otherwise. */
+int cg_checkpoint_load(cg_handle* h, const void* buf, size_t bytes);
+
 /* ---- field surrogate (no counterpart in the reference) ---- */
 
 /* A 3 -> 64 -> 64 -> 64 -> 2 MLP (SiLU, BF16 weights, FP32 accumulation) for

@@ -166,3 +166,30 @@ def test_ion_chain_near_threshold_statistics():
     # over the train, rms sizes agree on average within 1 %
     for q in (1, 2):
         assert abs(rg[:, 0, q].mean() / ro[:, 0, q].mean() - 1) < 1e-2
+
+
+def test_ion_chain_two_species():
+    """CO and CO2 clouds at the same IP (one trajectory set per species): the
+    records of both species and the clouds against the oracle, both species
+    trapped (H2 would sit below the critical mass at this current, where the
+    ion motion is chaotic)."""
+    wl = small("fast_ion", 0.02, bunch_current=TRAPPED)
+    ion = wl.cfg.ion
+    ion.n_species = 2
+    ion.mass_number[1] = 44.0
+    ion.cross_section[1] = 2.5e-22
+    ion.gas_percent[0], ion.gas_percent[1] = 0.8, 0.2
+    g, o = pair(wl, particles(wl, seed=8, spread=3.0))
+    for k in (0, 1):
+        g.MPBeamRMSCal(k)
+        o.MPBeamRMSCal(k)
+        g.SSBeamIonEffectOneInteractionPoint(0, k)
+        o.SSBeamIonEffectOneInteractionPoint(0, k)
+        rg, ro = g.cloud_record(k), o.cloud_record(k)
+        assert rg.shape == ro.shape == (wl.n_bunches, 2, 6)
+        assert np.array_equal(rg[..., 5], ro[..., 5])
+        assert np.allclose(rg[..., :3], ro[..., :3], rtol=1e-11, atol=0)
+        for p in (0, 1):
+            ig, io = g.ions(k, p), o.ions(k, p)
+            assert len(ig[0]) == len(io[0])
+    assert coord_err(g, o, wl).max() <= 1e-12
