@@ -147,6 +147,10 @@ EXPORTS = [
     ("cg_faddeeva_w", I, [PD, PD, PD, PD, C.c_int64]),
     ("cg_faddeeva_w_q1", I, [PD, PD, PD, PD, C.c_int64]),
     ("cg_gaussian_field", I, [PD, PD, PD, PD, PD, PD, C.c_int64]),
+    ("cg_shard_plan", I, [PI, I, I, PI, PI]),
+    ("cg_nccl_unique_id", I, [C.c_void_p]),
+    ("cg_set_shard", I, [C.c_void_p, I, I, C.c_void_p]),
+    ("cg_shard_range", I, [C.c_void_p, PI, PI]),
     ("cg_checkpoint_size", I, [C.c_void_p, C.POINTER(C.c_size_t)]),
     ("cg_checkpoint_save", I, [C.c_void_p, C.c_void_p, C.c_size_t]),
     ("cg_checkpoint_load", I, [C.c_void_p, C.c_void_p, C.c_size_t]),

@@ -12,11 +12,20 @@ from . import _abi
 from .configs import Workload
 
 
+def _load_torch_nccl():
+    """The library opens whichever NCCL the process already holds, else the
+    system's; PyTorch needs its own (newer) one, and two cannot share the
+    soname, so PyTorch is imported first."""
+    import torch  # noqa: F401
+
+
 class MPBeam:
     """One device handle tracking a bunch train (MPBeam + its bunches + the
     LatticeInterActionPoint ion clouds)."""
 
-    def __init__(self, wl: Workload, device: int = 0):
+    def __init__(self, wl: Workload, device: int = 0, shard=None):
+        """shard = (rank, world, nccl_id bytes): bunch-sharded run over
+        `world` processes (see cg_set_shard)."""
         self.lib = _abi.load()
         self.wl = wl
         h = C.c_void_p()
@@ -24,8 +33,26 @@ class MPBeam:
         if rc:
             raise _abi.CgError(rc, self.lib.cg_last_error(None).decode())
         self.h = h
+        if shard is not None:
+            _load_torch_nccl()
+            rank, world, nid = shard
+            idbuf = None if nid is None else C.create_string_buffer(bytes(nid), 128)
+            self._check(self.lib.cg_set_shard(h, rank, world, idbuf))
         self._check(self.lib.cg_set_beam(h, wl.n_bunches, _abi.ptr(wl.n_macro), _abi.ptr(wl.harm),
                                          _abi.ptr(wl.ne)))
+        j0, j1 = C.c_int(), C.c_int()
+        self._check(self.lib.cg_shard_range(h, C.byref(j0), C.byref(j1)))
+        self.local = range(j0.value, j1.value)
+
+    @staticmethod
+    def nccl_unique_id() -> bytes:
+        _load_torch_nccl()
+        lib = _abi.load()
+        buf = C.create_string_buffer(128)
+        rc = lib.cg_nccl_unique_id(buf)
+        if rc:
+            raise _abi.CgError(rc, lib.cg_last_error(None).decode())
+        return buf.raw
 
     # -- plumbing ------------------------------------------------------------
     def _check(self, rc: int):

@@ -96,6 +96,8 @@ void free_beam(Handle& h) {
   dfree(d.rec); dfree(d.lr_hist); dfree(d.lr_force); dfree(d.fir_hist); dfree(d.fir_kick);
   dfree(d.sr_geom); dfree(d.sr_counts); dfree(d.sr_sumx); dfree(d.sr_sumy); dfree(d.sr_lag);
   dfree(d.sr_pot);
+  dfree(d.mom_send); dfree(d.mom_all); dfree(d.sh_off); dfree(d.sh_cnt);
+  d.mom_send = nullptr; d.mom_all = nullptr; d.sh_off = nullptr; d.sh_cnt = nullptr;
   IonWalk& w = d.iw;
   dfree(w.births); dfree(w.prep); dfree(w.bunch); dfree(w.spec); dfree(w.bound); dfree(w.part);
   dfree(w.traj); dfree(w.alive);
@@ -444,7 +446,9 @@ int cg_destroy(cg_handle* H) {
   if (!H) return CG_OK;
   Handle& h = H->h;
   cudaSetDevice(h.device);
-  free_beam(h);
+  free_beam(h);  // the turn graph (which may hold NCCL calls) goes first
+  nccl_comm_destroy(h.nccl_comm);
+  h.nccl_comm = nullptr;
   dfree(h.sec_dev); dfree(h.d.status); dfree(h.d.turn);
   dfree(h.d.sur_w); dfree(h.d.sur_audit);
   if (h.d.clouds) {
@@ -490,10 +494,18 @@ int cg_set_beam(cg_handle* H, int M, const int* n_macro, const int* harm, const 
   std::vector<int> tb, cb;
   h.tile_off.assign(M + 1, 0);
   int tiles = 0, chunks = 0;
+  // bunch sharding: this rank tracks the particles of bunches [j0, j1)
+  std::vector<int> sj0(h.sh_world, 0), sj1(h.sh_world, M);
+  if (h.sh_world > 1) shard_plan(n_macro, M, h.sh_world, sj0.data(), sj1.data());
+  h.sh_j0 = sj0[h.sh_rank];
+  h.sh_j1 = sj1[h.sh_rank];
+  h.sh_maxlocal = 0;
+  for (int r = 0; r < h.sh_world; ++r) h.sh_maxlocal = std::max(h.sh_maxlocal, sj1[r] - sj0[r]);
   for (int j = 0; j < M; ++j) {
-    int nt = (n_macro[j] + kTile - 1) / kTile;
+    const bool local = j >= h.sh_j0 && j < h.sh_j1;
+    int nt = local ? (n_macro[j] + kTile - 1) / kTile : 0;
     int nc = (nt + kMomChunkTiles - 1) / kMomChunkTiles;
-    bd[j].n = n_macro[j];
+    bd[j].n = local ? n_macro[j] : 0;
     bd[j].tile_off = tiles;
     bd[j].n_tiles = nt;
     bd[j].harm = harm[j];
@@ -529,6 +541,19 @@ int cg_set_beam(cg_handle* H, int M, const int* n_macro, const int* harm, const 
   cudaMemset(d.surv, 0xFF, h.npad);
   cudaMemcpy(d.tile_bunch, tb.data(), sizeof(int) * tiles, cudaMemcpyHostToDevice);
   cudaMemcpy(d.chunk_bunch, cb.data(), sizeof(int) * chunks, cudaMemcpyHostToDevice);
+  if (h.nccl_comm) {
+    const int W = h.sh_world, ml = std::max(1, h.sh_maxlocal);
+    if (dalloc(&d.mom_send, (size_t)ml) || dalloc(&d.mom_all, (size_t)W * ml) ||
+        dalloc(&d.sh_off, (size_t)W) || dalloc(&d.sh_cnt, (size_t)W)) {
+      free_beam(h);
+      return fail(&h, CG_ERR_OOM, "shard exchange buffers");
+    }
+    std::vector<int> cnt(W);
+    for (int r = 0; r < W; ++r) cnt[r] = sj1[r] - sj0[r];
+    cudaMemcpy(d.sh_off, sj0.data(), sizeof(int) * W, cudaMemcpyHostToDevice);
+    cudaMemcpy(d.sh_cnt, cnt.data(), sizeof(int) * W, cudaMemcpyHostToDevice);
+    cudaMemset(d.mom_send, 0, sizeof(BunchMomDev) * ml);
+  }
   cudaMemcpy(d.bunch, bd.data(), sizeof(BunchDev) * M, cudaMemcpyHostToDevice);
   cudaMemset(d.counters, 0, sizeof(unsigned) * (M + 1));
   cudaMemset(d.loss_count, 0, sizeof(int) * (M + 1));
@@ -596,6 +621,7 @@ int cg_upload_bunch(cg_handle* H, int j, const double* x, const double* px, cons
   Handle& h = H->h;
   if (!h.beam_set) return fail(&h, CG_ERR_NOT_READY, "cg_set_beam first");
   if (j < 0 || j >= h.M) return fail(&h, CG_ERR_INVALID, "bunch index out of range");
+  if (j < h.sh_j0 || j >= h.sh_j1) return fail(&h, CG_ERR_INVALID, "bunch held by another rank");
   cudaSetDevice(h.device);
   const double* src[6] = {x, px, y, py, z, dp};
   int64_t off = (int64_t)h.tile_off[j] * kTile;
@@ -617,6 +643,7 @@ int cg_download_bunch(cg_handle* H, int j, double* x, double* px, double* y, dou
   Handle& h = H->h;
   if (!h.beam_set) return fail(&h, CG_ERR_NOT_READY, "cg_set_beam first");
   if (j < 0 || j >= h.M) return fail(&h, CG_ERR_INVALID, "bunch index out of range");
+  if (j < h.sh_j0 || j >= h.sh_j1) return fail(&h, CG_ERR_INVALID, "bunch held by another rank");
   cudaSetDevice(h.device);
   double* dst[6] = {x, px, y, py, z, dp};
   int64_t off = (int64_t)h.tile_off[j] * kTile;
@@ -651,6 +678,7 @@ int cg_beam_rms(cg_handle* H, int k) {
   STAGE_PROLOGUE
   if (k < 0 || k >= h.K) return fail(&h, CG_ERR_INVALID, "section index out of range");
   int st = launch_ok(h, launch_moments(h, k), "moments");
+  if (!st) st = launch_ok(h, exchange_moments(h), "moments exchange");
   return st ? st : check_status(h);
 }
 
@@ -784,7 +812,7 @@ static cudaError_t enqueue_turn(Handle& h) {
   // and the moments the next stage reads (those of IP k+1 for its ion chain;
   // after the last IP those of section K-1 for the wakes, MPBeam.cpp:1069)
   const bool post = c.flag_lr_wake || c.flag_sr_wake;
-  if (c.flag_beam_ion && (e = launch_moments(h, 0))) return e;
+  if (c.flag_beam_ion && ((e = launch_moments(h, 0)) || (e = exchange_moments(h)))) return e;
   for (int k = 0; k < h.K; ++k) {
     if (c.flag_beam_ion) {
       if ((e = launch_ion_chain(h, k))) return e;
@@ -794,6 +822,7 @@ static cudaError_t enqueue_turn(Handle& h) {
     if (k + 1 < h.K) mom = c.flag_beam_ion ? k + 1 : -1;
     else mom = post ? h.K - 1 : -1;
     if ((e = launch_map_pass(h, k, mom))) return e;
+    if (mom >= 0 && (e = exchange_moments(h))) return e;
   }
   if (c.flag_lr_wake && (e = launch_lr_compute(h))) return e;
   unsigned fl = kLongRF | kLongDrift | kLongLoss;
@@ -803,6 +832,7 @@ static cudaError_t enqueue_turn(Handle& h) {
   if (c.flag_sr_wake && (e = launch_sr_wake(h))) return e;
   if (c.flag_fir) {
     if ((e = launch_moments(h, 0))) return e;
+    if ((e = exchange_moments(h))) return e;
     if ((e = launch_fir_compute(h))) return e;
   }
   if ((e = launch_mark_lost(h, c.flag_fir != 0, true))) return e;
@@ -866,6 +896,13 @@ static int count_turn_launches(Handle& h) {
   if (c.flag_sr_wake) n += 5;
   if (c.flag_fir) n += 2;
   n += 2;                                        // mark lost + turn counter
+  if (h.nccl_comm) {                             // moments scatter after each exchange
+    int ex = 0;
+    for (int k = 0; k < h.K; ++k)
+      if (k + 1 < h.K ? c.flag_beam_ion : (c.flag_lr_wake || c.flag_sr_wake)) ++ex;
+    ex += (c.flag_beam_ion ? 1 : 0) + (c.flag_fir ? 1 : 0);
+    n += ex;
+  }
   return n;
 }
 
@@ -1070,6 +1107,52 @@ int cg_gaussian_field(const double* x, const double* y, const double* sx, const 
   const double* in[4] = {x, y, sx, sy};
   double* out[2] = {fx, fy};
   return eval_arrays(4, in, 2, out, n, 2);
+}
+
+// ---- bunch sharding over ranks ----
+
+int cg_shard_plan(const int* n_macro, int M, int world, int* j0, int* j1) {
+  if (!n_macro || !j0 || !j1 || M < 1 || world < 1)
+    return fail(nullptr, CG_ERR_INVALID, "bad shard plan arguments");
+  shard_plan(n_macro, M, world, j0, j1);
+  return CG_OK;
+}
+
+int cg_nccl_unique_id(void* id) {
+  if (!id) return fail(nullptr, CG_ERR_INVALID, "id is NULL");
+  const int r = nccl_unique_id(id);
+  if (r < 0) return fail(nullptr, CG_ERR_UNSUPPORTED, "NCCL (libnccl.so.2) could not be loaded");
+  return r ? fail(nullptr, CG_ERR_CUDA, "ncclGetUniqueId: " + nccl_error(r)) : CG_OK;
+}
+
+int cg_set_shard(cg_handle* H, int rank, int world, const void* id) {
+  if (!H) return CG_ERR_INVALID;
+  Handle& h = H->h;
+  if (h.beam_set) return fail(&h, CG_ERR_NOT_READY, "cg_set_shard must precede cg_set_beam");
+  if (world < 1 || rank < 0 || rank >= world) return fail(&h, CG_ERR_INVALID, "bad rank/world");
+  if (h.nccl_comm) return fail(&h, CG_ERR_NOT_READY, "the handle already has a communicator");
+  if (world > 1 && !id) return fail(&h, CG_ERR_INVALID, "an NCCL unique id is needed for world > 1");
+  h.sh_rank = rank;
+  h.sh_world = world;
+  if (!id) return CG_OK;  // one rank without exchanges
+  cudaSetDevice(h.device);
+  const int r = nccl_comm_init(&h.nccl_comm, world, id, rank);
+  if (r < 0) return fail(&h, CG_ERR_UNSUPPORTED, "NCCL (libnccl.so.2) could not be loaded");
+  if (r) {
+    h.sh_rank = 0;
+    h.sh_world = 1;
+    return fail(&h, CG_ERR_CUDA, "ncclCommInitRank: " + nccl_error(r));
+  }
+  return CG_OK;
+}
+
+int cg_shard_range(cg_handle* H, int* j0, int* j1) {
+  if (!H) return CG_ERR_INVALID;
+  Handle& h = H->h;
+  if (!h.beam_set) return fail(&h, CG_ERR_NOT_READY, "cg_set_beam first");
+  if (j0) *j0 = h.sh_j0;
+  if (j1) *j1 = h.sh_j1;
+  return CG_OK;
 }
 
 // ---- checkpoint / resume ----

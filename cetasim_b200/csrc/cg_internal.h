@@ -85,6 +85,11 @@ struct DeviceBufs {
   CloudRec* rec = nullptr;         // K x M x P
   double* ion_totals = nullptr;    // K (charge), used by cg_ion_totals
   IonWalk iw;
+  // bunch-sharded runs: moments of the local bunches out, of all bunches in
+  BunchMomDev* mom_send = nullptr;  // max local bunches
+  BunchMomDev* mom_all = nullptr;   // ranks x max local bunches
+  int* sh_off = nullptr;            // ranks: first bunch of each rank
+  int* sh_cnt = nullptr;            // ranks: bunches of each rank
   // field surrogate
   float* sur_w = nullptr;                 // FP32 parameters (null: exact kicks)
   unsigned long long* sur_audit = nullptr;  // audit maxima (double bit patterns)
@@ -134,6 +139,9 @@ struct Handle {
   bool beam_set = false;
   int ion_cap = 0;
   cudaGraphExec_t turn_graph = nullptr;
+  int sh_rank = 0, sh_world = 1;  // bunch sharding over ranks (cg_set_shard)
+  int sh_j0 = 0, sh_j1 = 0, sh_maxlocal = 0;
+  void* nccl_comm = nullptr;
   int sur_audit_every = 0;     // turns between exact audits of the surrogate (0: none)
   int sur_audits = 0;
   double sur_audit_last = 0, sur_audit_worst = 0;

@@ -40,6 +40,15 @@ cudaError_t launch_faddeeva(const double* zr, const double* zi, double* wr, doub
                             bool general, cudaStream_t s);
 cudaError_t launch_field(const double* x, const double* y, const double* sx, const double* sy,
                          double* fx, double* fy, int64_t n, cudaStream_t s);
+// bunch sharding (shard.cu)
+void shard_plan(const int* n_macro, int M, int world, int* j0, int* j1);
+cudaError_t exchange_moments(Handle& h);
+int nccl_unique_id(void* out);
+int nccl_comm_init(void** comm, int world, const void* id, int rank);
+void nccl_comm_destroy(void* comm);
+std::string nccl_error(int r);
+bool nccl_available();
+
 // field surrogate (surrogate.cu)
 cudaError_t prepare_surrogate();
 cudaError_t launch_sur_data(uint64_t seed, int64_t n, float* xin, float* tout, cudaStream_t s);

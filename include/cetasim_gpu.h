@@ -327,6 +327,27 @@ int cg_faddeeva_w_q1(const double* zr, const double* zi, double* wr, double* wi,
 int cg_gaussian_field(const double* x, const double* y, const double* sx,
                       const double* sy, double* fx, double* fy, int64_t n);
 
+/* ---- bunch-sharded runs over several GPUs (no counterpart in the reference,
+ * which is single-threaded) ---- */
+
+/* Contiguous bunch ranges [j0[r], j1[r]) of `world` ranks, balanced by
+ * macroparticle count (host only). */
+int cg_shard_plan(const int* n_macro, int M, int world, int* j0, int* j1);
+/* An NCCL unique id (128 bytes) for cg_set_shard; rank 0 makes it, the
+ * caller broadcasts it (e.g. with torch.distributed). */
+int cg_nccl_unique_id(void* id);
+/* Before cg_set_beam: this handle is rank `rank` of `world` (one process per
+ * GPU).  cg_set_beam then keeps the particles of this rank's bunches only
+ * (cg_shard_plan); after every moments pass the ranks all-gather the bunch
+ * moments over NCCL, so every rank runs the same ion chain and wakes on all
+ * bunches and kicks its own.  Upload, download and generation address local
+ * bunches only.  Every rank must make the same calls in the same order.
+ * world = 1 with an id runs the exchange path on one GPU (a one-rank NCCL
+ * communicator); world = 1 without one is the default single-GPU mode. */
+int cg_set_shard(cg_handle* h, int rank, int world, const void* id);
+/* The bunch range [*j0, *j1) this rank holds (after cg_set_beam). */
+int cg_shard_range(cg_handle* h, int* j0, int* j1);
+
 /* ---- checkpoint / resume (no counterpart in the reference, which only
  * writes outputs) ---- */
 
