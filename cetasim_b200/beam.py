@@ -132,6 +132,19 @@ class MPBeam:
     def Run(self, turn0: int, n_turns: int):
         self._check(self.lib.cg_run_turns(self.h, turn0, n_turns))
 
+    # -- autotuning ---------------------------------------------------------------
+    def autotune(self, k: int = 0, reps: int = 10):
+        """Times the kick shapes on this beam at IP k; returns (choice, ms)."""
+        n = C.c_int()
+        self._check(self.lib.cg_kick_variants(C.byref(n)))
+        ms = np.zeros(n.value)
+        choice = C.c_int()
+        self._check(self.lib.cg_autotune(self.h, k, reps, C.byref(choice), _abi.ptr(ms)))
+        return choice.value, ms
+
+    def set_kick_variant(self, v: int):
+        self._check(self.lib.cg_set_kick_variant(self.h, v))
+
     # -- checkpoint / resume ------------------------------------------------------
     def checkpoint(self) -> bytes:
         n = C.c_size_t()

@@ -1109,6 +1109,71 @@ int cg_gaussian_field(const double* x, const double* y, const double* sx, const 
   return eval_arrays(4, in, 2, out, n, 2);
 }
 
+// ---- autotuning ----
+
+int cg_kick_variants(int* n) {
+  if (!n) return CG_ERR_INVALID;
+  *n = kick_variants();
+  return CG_OK;
+}
+
+int cg_set_kick_variant(cg_handle* H, int v) {
+  if (!H) return CG_ERR_INVALID;
+  Handle& h = H->h;
+  if (v < 0 || v >= kick_variants()) return fail(&h, CG_ERR_INVALID, "no such kick variant");
+  if (h.kick_variant != v && h.turn_graph) {
+    cudaGraphExecDestroy(h.turn_graph);
+    h.turn_graph = nullptr;
+  }
+  h.kick_variant = v;
+  return CG_OK;
+}
+
+int cg_autotune(cg_handle* H, int k, int reps, int* choice, double* ms) {
+  STAGE_PROLOGUE
+  if (!h.cfg.flag_beam_ion) return fail(&h, CG_ERR_NOT_READY, "runBeamIonFlag is off");
+  if (k < 0 || k >= h.K || reps < 1) return fail(&h, CG_ERR_INVALID, "bad arguments");
+  // the kicks under test change px and py: keep them and put them back
+  double* keep = nullptr;
+  if (dalloc(&keep, 2 * (size_t)h.npad)) return fail(&h, CG_ERR_OOM, "autotune buffer");
+  const size_t row = sizeof(double) * (size_t)h.npad;
+  cudaError_t e = cudaMemcpyAsync(keep, h.d.c + h.npad, row, cudaMemcpyDeviceToDevice, h.stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(keep + h.npad, h.d.c + 3 * h.npad, row, cudaMemcpyDeviceToDevice, h.stream);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  int best = 0;
+  double best_ms = 0;
+  for (int v = 0; v < kick_variants() && e == cudaSuccess; ++v) {
+    e = launch_ion_kick_variant(h, k, v);  // warm-up
+    if (e == cudaSuccess) e = cudaEventRecord(e0, h.stream);
+    for (int r = 0; r < reps && e == cudaSuccess; ++r) e = launch_ion_kick_variant(h, k, v);
+    if (e == cudaSuccess) e = cudaEventRecord(e1, h.stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    float t = 0;
+    cudaEventElapsedTime(&t, e0, e1);
+    const double per = (double)t / reps;
+    if (ms) ms[v] = per;
+    if (v == 0 || per < best_ms) {
+      best = v;
+      best_ms = per;
+    }
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(h.d.c + h.npad, keep, row, cudaMemcpyDeviceToDevice, h.stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(h.d.c + 3 * h.npad, keep + h.npad, row, cudaMemcpyDeviceToDevice,
+                          h.stream);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h.stream);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  dfree(keep);
+  if (e != cudaSuccess) return cuda_fail(&h, e, "autotune");
+  if (choice) *choice = best;
+  return cg_set_kick_variant(H, best);
+}
+
 // ---- bunch sharding over ranks ----
 
 int cg_shard_plan(const int* n_macro, int M, int world, int* j0, int* j1) {

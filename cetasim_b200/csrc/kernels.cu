@@ -52,6 +52,37 @@ __device__ __forceinline__ void block_sum(double (&v)[N], double* smem) {
   __syncthreads();
 }
 
+// Warp sums of 8 values with the transposed butterfly: at the shuffles by 16,
+// 8 and 4 each lane passes half of its remaining values to its partner and
+// keeps the other half, then the last value is summed by 2 and 1.  18
+// shuffles of a double instead of 40; afterwards lane l holds the warp total
+// of value ((l >> 4) & 1) * 4 + ((l >> 3) & 1) * 2 + ((l >> 2) & 1).  Fixed
+// tree: deterministic.
+__device__ __forceinline__ double warp_sum8_t(const double (&v)[8]) {
+  const int lane = threadIdx.x & 31;
+  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+  double k4[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const double keep = b4 ? v[i + 4] : v[i], send = b4 ? v[i] : v[i + 4];
+    k4[i] = keep + __shfl_xor_sync(FULL_MASK, send, 16);
+  }
+  double k2[2];
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const double keep = b3 ? k4[i + 2] : k4[i], send = b3 ? k4[i] : k4[i + 2];
+    k2[i] = keep + __shfl_xor_sync(FULL_MASK, send, 8);
+  }
+  const double keep = b2 ? k2[1] : k2[0], send = b2 ? k2[0] : k2[1];
+  double t = keep + __shfl_xor_sync(FULL_MASK, send, 4);
+  t += __shfl_xor_sync(FULL_MASK, t, 2);
+  t += __shfl_xor_sync(FULL_MASK, t, 1);
+  return t;
+}
+__device__ __forceinline__ int warp_sum8_index(int lane) {
+  return ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
+}
+
 template <int NT>
 __device__ __forceinline__ void block_minmax(double& mn, double& mx, double* smem) {
   constexpr int NW = NT / 32;
@@ -128,7 +159,8 @@ __device__ __forceinline__ void store6(double* __restrict__ c, int64_t npad, int
 // v[u][d]: coordinate d of this thread's particle in tile u of the chunk.
 // Two block reductions with fixed trees: (sums, count, z min, z max), whose
 // totals every thread needs for the centred pass, then the centred
-// co-moments, whose totals only thread 0 needs.  Three barriers.
+// co-moments, whose totals only thread 0 needs.  Three barriers; the warp
+// stage of the sums uses the transposed butterfly (warp_sum8_t).
 __device__ void chunk_moment_partial(const double (&v)[kMomChunkTiles][6],
                                      const bool (&alive)[kMomChunkTiles], double* smem,
                                      MomPartial* out) {
@@ -148,16 +180,18 @@ __device__ void chunk_moment_partial(const double (&v)[kMomChunkTiles][6],
       mx = fmax(mx, v[u][4]);
     }
   }
+  {
+    const double s8[8] = {s[0], s[1], s[2], s[3], s[4], s[5], s[6], 0.0};
+    const double t = warp_sum8_t(s8);
+    const int idx = warp_sum8_index(lane);
+    if ((lane & 3) == 0 && idx < 7) sa[idx * 32 + warp] = t;
+  }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
-#pragma unroll
-    for (int k = 0; k < 7; ++k) s[k] += __shfl_xor_sync(FULL_MASK, s[k], o);
     mn = fmin(mn, __shfl_xor_sync(FULL_MASK, mn, o));
     mx = fmax(mx, __shfl_xor_sync(FULL_MASK, mx, o));
   }
   if (lane == 0) {
-#pragma unroll
-    for (int k = 0; k < 7; ++k) sa[k * 32 + warp] = s[k];
     sa[7 * 32 + warp] = mn;
     sa[8 * 32 + warp] = mx;
   }
@@ -193,10 +227,15 @@ __device__ void chunk_moment_partial(const double (&v)[kMomChunkTiles][6],
     q[7] = fma(dv[2], dv[3], q[7]);
     q[8] = fma(dv[4], dv[5], q[8]);
   }
-  warp_sum<9>(q);
-  if (lane == 0)
+  {
+    const double q8[8] = {q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7]};
+    const double t = warp_sum8_t(q8);
+    if ((lane & 3) == 0) sb[warp_sum8_index(lane) * 32 + warp] = t;
+    double q9 = q[8];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) sb[k * 32 + warp] = q[k];
+    for (int o = 16; o > 0; o >>= 1) q9 += __shfl_xor_sync(FULL_MASK, q9, o);
+    if (lane == 0) sb[8 * 32 + warp] = q9;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
     MomPartial p;
@@ -327,24 +366,65 @@ cudaError_t launch_map(Handle& h, int k) {
 // Electron-side ion kick (MPBunch.cpp:1164-1206 + Bunch.cpp:213-220) with the
 // cloud Gaussians the chain kernel recorded for each bunch at this IP.
 
-__global__ void __launch_bounds__(kTile, 3) k_ion_kick(double* __restrict__ c, int64_t npad,
-                                                    const uint8_t* __restrict__ surv,
-                                                    const int* __restrict__ tile_bunch,
-                                                    const BunchDev* __restrict__ bunch,
-                                                    const CloudRec* __restrict__ rec, int P) {
+// NT threads per CTA (a CTA covers NT particles of one tile) and at least
+// MINB CTAs per SM (the register budget): the shapes the autotuner picks from.
+template <int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_ion_kick(double* __restrict__ c, int64_t npad,
+                                                      const uint8_t* __restrict__ surv,
+                                                      const int* __restrict__ tile_bunch,
+                                                      const BunchDev* __restrict__ bunch,
+                                                      const CloudRec* __restrict__ rec, int P) {
   // the field constants of the bunch's records, once per CTA (a tile holds
   // particles of one bunch)
   __shared__ FieldPrep s_prep[CG_MAX_SPECIES];
-  TileIdx t = tile_index(tile_bunch, bunch);
-  const CloudRec* rb = rec + (size_t)t.b * P;
+  constexpr int kSub = kTile / NT;
+  const int tile = blockIdx.x / kSub;
+  const int b = tile_bunch[tile];
+  const BunchDev& B = bunch[b];
+  const int lane = (blockIdx.x % kSub) * NT + threadIdx.x;
+  const int i = (tile - B.tile_off) * kTile + lane;
+  const int64_t g = (int64_t)tile * kTile + lane;
+  const CloudRec* rb = rec + (size_t)b * P;
   if ((int)threadIdx.x < P) s_prep[threadIdx.x] = field_prep(rb[threadIdx.x].rms_x, rb[threadIdx.x].rms_y);
   __syncthreads();
-  if (!t.valid || surv[t.g] != kAlive) return;
-  double x = c[0 * npad + t.g], y = c[2 * npad + t.g];
+  if (i >= B.n || surv[g] != kAlive) return;
+  double x = c[0 * npad + g], y = c[2 * npad + g];
   double dpx, dpy;
   ion_kick_particle_prep(rb, s_prep, P, x, y, &dpx, &dpy);
-  c[1 * npad + t.g] += dpx;
-  c[3 * npad + t.g] += dpy;
+  c[1 * npad + g] += dpx;
+  c[3 * npad + g] += dpy;
+}
+
+// The kick shapes (threads per CTA, minimum CTAs per SM) of autotune choice v.
+static const int kKickShapes[][2] = {{256, 3}, {256, 4}, {128, 4}, {128, 6}};
+constexpr int kKickVariants = 4;
+
+cudaError_t launch_ion_kick_variant(Handle& h, int k, int v) {
+  const CloudRec* rec = h.d.rec + (size_t)k * h.M * h.P;
+  switch (v) {
+    case 1:
+      k_ion_kick<256, 4><<<h.n_tiles, 256, 0, h.stream>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch,
+                                                          h.d.bunch, rec, h.P);
+      break;
+    case 2:
+      k_ion_kick<128, 4><<<2 * h.n_tiles, 128, 0, h.stream>>>(h.d.c, h.npad, h.d.surv,
+                                                              h.d.tile_bunch, h.d.bunch, rec, h.P);
+      break;
+    case 3:
+      k_ion_kick<128, 6><<<2 * h.n_tiles, 128, 0, h.stream>>>(h.d.c, h.npad, h.d.surv,
+                                                              h.d.tile_bunch, h.d.bunch, rec, h.P);
+      break;
+    default:
+      k_ion_kick<256, 3><<<h.n_tiles, 256, 0, h.stream>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch,
+                                                          h.d.bunch, rec, h.P);
+  }
+  return cudaGetLastError();
+}
+
+int kick_variants() { return kKickVariants; }
+void kick_variant_shape(int v, int* threads, int* min_ctas) {
+  *threads = kKickShapes[v][0];
+  *min_ctas = kKickShapes[v][1];
 }
 
 // The map of section k with the moments the next stage reads (MOM: at the
@@ -401,11 +481,7 @@ cudaError_t launch_map_pass(Handle& h, int k, int mom_section) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_ion_kick(Handle& h, int k) {
-  k_ion_kick<<<h.n_tiles, kTile, 0, h.stream>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch,
-                                                h.d.bunch, h.d.rec + (size_t)k * h.M * h.P, h.P);
-  return cudaGetLastError();
-}
+cudaError_t launch_ion_kick(Handle& h, int k) { return launch_ion_kick_variant(h, k, h.kick_variant); }
 
 // ---------------------------------------------------------------------------
 // Turn tail: RF kick, drift, energy loss (all particles), synchrotron

@@ -18,6 +18,9 @@ cudaError_t launch_map(Handle& h, int k);
 cudaError_t launch_ion_chain(Handle& h, int k);
 int ion_walk_grid(int64_t tcap);
 cudaError_t launch_ion_kick(Handle& h, int k);
+cudaError_t launch_ion_kick_variant(Handle& h, int k, int v);
+int kick_variants();
+void kick_variant_shape(int v, int* threads, int* min_ctas);
 // map of section k + moments at section `mom_section` (if >= 0)
 cudaError_t launch_map_pass(Handle& h, int k, int mom_section);
 enum LongFlags : unsigned {

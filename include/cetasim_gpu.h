@@ -327,6 +327,17 @@ int cg_faddeeva_w_q1(const double* zr, const double* zi, double* wr, double* wi,
 int cg_gaussian_field(const double* x, const double* y, const double* sx,
                       const double* sy, double* fx, double* fy, int64_t n);
 
+/* ---- autotuning (no counterpart in the reference) ---- */
+
+/* Number of shapes (threads per CTA, register budget) of the field-kick kernel. */
+int cg_kick_variants(int* n);
+/* Use shape v for the field kick of h (the turn graph is rebuilt). */
+int cg_set_kick_variant(cg_handle* h, int v);
+/* Times every kick shape on h's own beam at IP k (reps launches each, after
+ * a warm-up; the records of the last ion pass at k), leaves px and py as
+ * they were, and selects the fastest: *choice, ms[v] per launch. */
+int cg_autotune(cg_handle* h, int k, int reps, int* choice, double* ms);
+
 /* ---- bunch-sharded runs over several GPUs (no counterpart in the reference,
  * which is single-threaded) ---- */
 

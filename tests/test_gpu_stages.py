@@ -193,3 +193,31 @@ def test_ion_chain_two_species():
             ig, io = g.ions(k, p), o.ions(k, p)
             assert len(ig[0]) == len(io[0])
     assert coord_err(g, o, wl).max() <= 1e-12
+
+
+def test_kick_autotuner_keeps_the_beam_and_shapes_agree():
+    """The autotuner times the kick shapes on the live beam and puts px, py
+    back; every shape computes the same kicks bit for bit."""
+    import ctypes as C
+    wl = small("fast_ion", 0.02, bunch_current=TRAPPED)
+    parts = particles(wl, seed=6, spread=3.0)
+    g, _ = pair(wl, parts)
+    g.MPBeamRMSCal(0)
+    g.SSBeamIonEffectOneInteractionPoint(0, 0)
+    before = [g.download(j) for j in range(wl.n_bunches)]
+    choice, ms = g.autotune(0, reps=3)
+    assert 0 <= choice < len(ms) and np.all(ms > 0) and ms[choice] == ms.min()
+    after = [g.download(j) for j in range(wl.n_bunches)]
+    for (a, s), (b, t) in zip(before, after):
+        assert np.array_equal(a, b) and np.array_equal(s, t)
+    kicked = []
+    for v in range(len(ms)):
+        for j, (c, s) in enumerate(before):
+            g.upload(j, c, s)
+        g.set_kick_variant(v)
+        t = C.c_double()
+        g._check(g.lib.cg_time_stage(g.h, 1, 0, 1, C.byref(t)))
+        kicked.append([g.download(j)[0] for j in range(wl.n_bunches)])
+    for other in kicked[1:]:
+        for a, b in zip(kicked[0], other):
+            assert np.array_equal(a, b)
