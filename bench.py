@@ -332,8 +332,11 @@ def main():
                           "us_per_bunch_step": 1e3 * chain_ms.value / wl.n_bunches,
                           "bound": "latency (one field evaluation per bunch step)"},
             "cpu_baseline": cpu,
-            "autotune": {"kick_shapes_ms": [round(float(x), 5) for x in tune[1]],
-                         "chosen": int(tune[0]),
+            "autotune": {"kick_shapes_ms": [round(float(x), 5) for x in tune[1][:-2]],
+                         "map_pass_ms": round(float(tune[1][-2]), 5),
+                         "map_pass_with_kick_ms": round(float(tune[1][-1]), 5),
+                         "chosen_shape": int(tune[0]) % (len(tune[1]) - 2),
+                         "kick_in_map_pass": bool(tune[0] >= len(tune[1]) - 2),
                          "shapes": ["256 thr x3/SM", "256 thr x4/SM", "128 thr x4/SM",
                                     "128 thr x6/SM"]},
             "surrogate": sur,

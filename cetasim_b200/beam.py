@@ -137,7 +137,7 @@ class MPBeam:
         """Times the kick shapes on this beam at IP k; returns (choice, ms)."""
         n = C.c_int()
         self._check(self.lib.cg_kick_variants(C.byref(n)))
-        ms = np.zeros(n.value)
+        ms = np.zeros(n.value + 2)
         choice = C.c_int()
         self._check(self.lib.cg_autotune(self.h, k, reps, C.byref(choice), _abi.ptr(ms)))
         return choice.value, ms

@@ -814,14 +814,15 @@ static cudaError_t enqueue_turn(Handle& h) {
   const bool post = c.flag_lr_wake || c.flag_sr_wake;
   if (c.flag_beam_ion && ((e = launch_moments(h, 0)) || (e = exchange_moments(h)))) return e;
   for (int k = 0; k < h.K; ++k) {
+    const bool fused = c.flag_beam_ion && !h.d.sur_w && h.fuse_kick;
     if (c.flag_beam_ion) {
       if ((e = launch_ion_chain(h, k))) return e;
-      if ((e = h.d.sur_w ? launch_ion_kick_sur(h, k) : launch_ion_kick(h, k))) return e;
+      if (!fused && (e = h.d.sur_w ? launch_ion_kick_sur(h, k) : launch_ion_kick(h, k))) return e;
     }
     int mom = -1;
     if (k + 1 < h.K) mom = c.flag_beam_ion ? k + 1 : -1;
     else mom = post ? h.K - 1 : -1;
-    if ((e = launch_map_pass(h, k, mom))) return e;
+    if ((e = launch_map_pass(h, k, mom, fused))) return e;
     if (mom >= 0 && (e = exchange_moments(h))) return e;
   }
   if (c.flag_lr_wake && (e = launch_lr_compute(h))) return e;
@@ -929,6 +930,9 @@ int cg_time_stage(cg_handle* H, int stage, int k, int reps, double* ms) {
       case 2: e = launch_ion_chain(h, k); break;
       case 3: e = launch_moments(h, k); break;
       case 5: e = launch_map_pass(h, k, k); break;
+      case 7:
+        e = h.cfg.flag_beam_ion ? launch_map_pass(h, k, k, true) : cudaErrorInvalidValue;
+        break;
       case 6:
         e = h.d.sur_w ? launch_ion_kick_sur(h, k) : cudaErrorInvalidValue;
         break;
@@ -1120,6 +1124,20 @@ int cg_kick_variants(int* n) {
 int cg_set_kick_variant(cg_handle* H, int v) {
   if (!H) return CG_ERR_INVALID;
   Handle& h = H->h;
+  if (v >= kick_variants() && v < 2 * kick_variants()) {  // the kick inside the map pass
+    if (!h.fuse_kick && h.turn_graph) {
+      cudaGraphExecDestroy(h.turn_graph);
+      h.turn_graph = nullptr;
+    }
+    h.fuse_kick = true;
+    v -= kick_variants();
+  } else if (h.fuse_kick && v >= 0 && v < kick_variants()) {
+    if (h.turn_graph) {
+      cudaGraphExecDestroy(h.turn_graph);
+      h.turn_graph = nullptr;
+    }
+    h.fuse_kick = false;
+  }
   if (v < 0 || v >= kick_variants()) return fail(&h, CG_ERR_INVALID, "no such kick variant");
   if (h.kick_variant != v && h.turn_graph) {
     cudaGraphExecDestroy(h.turn_graph);
@@ -1133,45 +1151,74 @@ int cg_autotune(cg_handle* H, int k, int reps, int* choice, double* ms) {
   STAGE_PROLOGUE
   if (!h.cfg.flag_beam_ion) return fail(&h, CG_ERR_NOT_READY, "runBeamIonFlag is off");
   if (k < 0 || k >= h.K || reps < 1) return fail(&h, CG_ERR_INVALID, "bad arguments");
-  // the kicks under test change px and py: keep them and put them back
+  // the passes under test change the coordinates and the bunch moments: keep
+  // them and put them back after every trial
   double* keep = nullptr;
-  if (dalloc(&keep, 2 * (size_t)h.npad)) return fail(&h, CG_ERR_OOM, "autotune buffer");
-  const size_t row = sizeof(double) * (size_t)h.npad;
-  cudaError_t e = cudaMemcpyAsync(keep, h.d.c + h.npad, row, cudaMemcpyDeviceToDevice, h.stream);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(keep + h.npad, h.d.c + 3 * h.npad, row, cudaMemcpyDeviceToDevice, h.stream);
+  BunchMomDev* keep_mom = nullptr;
+  if (dalloc(&keep, 6 * (size_t)h.npad) || dalloc(&keep_mom, (size_t)h.M)) {
+    dfree(keep);
+    return fail(&h, CG_ERR_OOM, "autotune buffer");
+  }
+  const size_t all = 6 * sizeof(double) * (size_t)h.npad, mb = sizeof(BunchMomDev) * (size_t)h.M;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  int best = 0;
-  double best_ms = 0;
-  for (int v = 0; v < kick_variants() && e == cudaSuccess; ++v) {
-    e = launch_ion_kick_variant(h, k, v);  // warm-up
-    if (e == cudaSuccess) e = cudaEventRecord(e0, h.stream);
-    for (int r = 0; r < reps && e == cudaSuccess; ++r) e = launch_ion_kick_variant(h, k, v);
-    if (e == cudaSuccess) e = cudaEventRecord(e1, h.stream);
-    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+  cudaError_t e = cudaMemcpyAsync(keep, h.d.c, all, cudaMemcpyDeviceToDevice, h.stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(keep_mom, h.d.mom, mb, cudaMemcpyDeviceToDevice, h.stream);
+  auto restore = [&]() {
+    cudaError_t r = cudaMemcpyAsync(h.d.c, keep, all, cudaMemcpyDeviceToDevice, h.stream);
+    if (r == cudaSuccess) r = cudaMemcpyAsync(h.d.mom, keep_mom, mb, cudaMemcpyDeviceToDevice, h.stream);
+    return r;
+  };
+  auto time_it = [&](auto launch, double* out) {
+    cudaError_t r = launch();  // warm-up
+    if (r == cudaSuccess) r = restore();
+    if (r == cudaSuccess) r = cudaEventRecord(e0, h.stream);
+    for (int q = 0; q < reps && r == cudaSuccess; ++q) r = launch();
+    if (r == cudaSuccess) r = cudaEventRecord(e1, h.stream);
+    if (r == cudaSuccess) r = cudaEventSynchronize(e1);
     float t = 0;
     cudaEventElapsedTime(&t, e0, e1);
-    const double per = (double)t / reps;
+    *out = (double)t / reps;
+    if (r == cudaSuccess) r = restore();
+    return r;
+  };
+  int best = 0;
+  double best_ms = 0;
+  const int nv = kick_variants();
+  for (int v = 0; v < nv && e == cudaSuccess; ++v) {
+    double per = 0;
+    e = time_it([&]() { return launch_ion_kick_variant(h, k, v); }, &per);
     if (ms) ms[v] = per;
     if (v == 0 || per < best_ms) {
       best = v;
       best_ms = per;
     }
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(h.d.c + h.npad, keep, row, cudaMemcpyDeviceToDevice, h.stream);
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(h.d.c + 3 * h.npad, keep + h.npad, row, cudaMemcpyDeviceToDevice,
-                          h.stream);
+  }
+  // the separate kick + map pass against the kick inside the map pass
+  const int mom = k + 1 < h.K ? k + 1 : k;
+  double map_ms = 0, fused_ms = 0;
+  if (e == cudaSuccess) e = time_it([&]() { return launch_map_pass(h, k, mom, false); }, &map_ms);
+  if (e == cudaSuccess) e = time_it([&]() { return launch_map_pass(h, k, mom, true); }, &fused_ms);
+  if (ms) {
+    ms[nv] = map_ms;
+    ms[nv + 1] = fused_ms;
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(h.stream);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   dfree(keep);
+  dfree(keep_mom);
   if (e != cudaSuccess) return cuda_fail(&h, e, "autotune");
-  if (choice) *choice = best;
-  return cg_set_kick_variant(H, best);
+  const bool fuse = fused_ms < best_ms + map_ms;
+  if (choice) *choice = best + (fuse ? nv : 0);
+  int st = cg_set_kick_variant(H, best);
+  if (h.fuse_kick != fuse && h.turn_graph) {
+    cudaGraphExecDestroy(h.turn_graph);
+    h.turn_graph = nullptr;
+  }
+  h.fuse_kick = fuse;
+  return st;
 }
 
 // ---- bunch sharding over ranks ----

@@ -140,6 +140,7 @@ struct Handle {
   int ion_cap = 0;
   cudaGraphExec_t turn_graph = nullptr;
   int kick_variant = 0;         // autotuned shape of the kick kernel
+  bool fuse_kick = false;       // autotuned: kick inside the map pass
   int sh_rank = 0, sh_world = 1;  // bunch sharding over ranks (cg_set_shard)
   int sh_j0 = 0, sh_j1 = 0, sh_maxlocal = 0;
   void* nccl_comm = nullptr;

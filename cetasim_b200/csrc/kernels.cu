@@ -433,7 +433,7 @@ void kick_variant_shape(int v, int* threads, int* min_ctas) {
 // first, the mapped particles stay in registers for the moments, and each
 // particle is read and written once.  Results equal k_map followed by
 // k_moments.
-template <bool MOM>
+template <bool MOM, bool KICK>
 __global__ void __launch_bounds__(kTile, 2) k_map_pass(double* __restrict__ c, int64_t npad,
                                                     const uint8_t* __restrict__ surv,
                                                     const int* __restrict__ chunk_bunch,
@@ -441,10 +441,18 @@ __global__ void __launch_bounds__(kTile, 2) k_map_pass(double* __restrict__ c, i
                                                     const __grid_constant__ SectionDev sec,
                                                     const __grid_constant__ RingDev r,
                                                     MomPartial* partials, unsigned* counters,
-                                                    BunchMomDev* mom, double beta_x, double beta_y) {
+                                                    BunchMomDev* mom, double beta_x, double beta_y,
+                                                    const CloudRec* __restrict__ rec, int P) {
   __shared__ double smem[18 * 32];
+  __shared__ FieldPrep s_prep[CG_MAX_SPECIES];
   const int b = chunk_bunch[blockIdx.x];
   const BunchDev B = bunch[b];
+  const CloudRec* rb = rec + (size_t)b * P;
+  if (KICK) {
+    if ((int)threadIdx.x < P)
+      s_prep[threadIdx.x] = field_prep(rb[threadIdx.x].rms_x, rb[threadIdx.x].rms_y);
+    __syncthreads();
+  }
   const int tile0 = B.tile_off + (blockIdx.x - B.chunk_off) * kMomChunkTiles;
   const int i0 = (tile0 - B.tile_off) * kTile + threadIdx.x;
   double v[kMomChunkTiles][6];
@@ -460,6 +468,12 @@ __global__ void __launch_bounds__(kTile, 2) k_map_pass(double* __restrict__ c, i
 #pragma unroll
   for (int u = 0; u < kMomChunkTiles; ++u) {
     if (!alive[u]) continue;
+    if (KICK) {
+      double dpx, dpy;
+      ion_kick_particle_prep(rb, s_prep, P, v[u][0], v[u][2], &dpx, &dpy);
+      v[u][1] += dpx;
+      v[u][3] += dpy;
+    }
     section_map_particle(sec, r, v[u]);
     store6(c, npad, (int64_t)(tile0 + u) * kTile + threadIdx.x, v[u]);
   }
@@ -470,14 +484,16 @@ __global__ void __launch_bounds__(kTile, 2) k_map_pass(double* __restrict__ c, i
   }
 }
 
-cudaError_t launch_map_pass(Handle& h, int k, int mom_section) {
+cudaError_t launch_map_pass(Handle& h, int k, int mom_section, bool kick) {
   const bool m = mom_section >= 0;
   const double bx = m ? h.sec_dev_host[mom_section].beta_x : 0.0;
   const double by = m ? h.sec_dev_host[mom_section].beta_y : 0.0;
-  auto kern = m ? k_map_pass<true> : k_map_pass<false>;
+  const CloudRec* rec = kick ? h.d.rec + (size_t)k * h.M * h.P : nullptr;
+  auto kern = m ? (kick ? k_map_pass<true, true> : k_map_pass<true, false>)
+                : (kick ? k_map_pass<false, true> : k_map_pass<false, false>);
   kern<<<h.n_chunks, kTile, 0, h.stream>>>(h.d.c, h.npad, h.d.surv, h.d.chunk_bunch, h.d.bunch,
                                            h.sec_dev_host[k], h.ring, h.d.partials,
-                                           h.d.counters, h.d.mom, bx, by);
+                                           h.d.counters, h.d.mom, bx, by, rec, h.P);
   return cudaGetLastError();
 }
 

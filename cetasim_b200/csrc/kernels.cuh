@@ -21,8 +21,9 @@ cudaError_t launch_ion_kick(Handle& h, int k);
 cudaError_t launch_ion_kick_variant(Handle& h, int k, int v);
 int kick_variants();
 void kick_variant_shape(int v, int* threads, int* min_ctas);
-// map of section k + moments at section `mom_section` (if >= 0)
-cudaError_t launch_map_pass(Handle& h, int k, int mom_section);
+// (ion kick of IP k if `kick`) + map of section k + moments at section
+// `mom_section` (if >= 0)
+cudaError_t launch_map_pass(Handle& h, int k, int mom_section, bool kick = false);
 enum LongFlags : unsigned {
   kLongRF = 1,
   kLongDrift = 2,

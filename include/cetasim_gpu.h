@@ -329,13 +329,19 @@ int cg_gaussian_field(const double* x, const double* y, const double* sx,
 
 /* ---- autotuning (no counterpart in the reference) ---- */
 
-/* Number of shapes (threads per CTA, register budget) of the field-kick kernel. */
+/* Number n of shapes (threads per CTA, register budget) of the field-kick
+ * kernel.  Choices 0 .. n-1 run the kick as its own kernel with that shape;
+ * n .. 2n-1 the same shape for the staged calls and, in the turn graph, the
+ * kick inside the map pass (one particle pass for kick, map and moments). */
 int cg_kick_variants(int* n);
-/* Use shape v for the field kick of h (the turn graph is rebuilt). */
+/* Use choice v for h (the turn graph is rebuilt). */
 int cg_set_kick_variant(cg_handle* h, int v);
 /* Times every kick shape on h's own beam at IP k (reps launches each, after
- * a warm-up; the records of the last ion pass at k), leaves px and py as
- * they were, and selects the fastest: *choice, ms[v] per launch. */
+ * a warm-up; the records of the last ion pass at k), then the map pass with
+ * and without the kick inside; restores the beam after every trial and
+ * selects the fastest combination: *choice (as cg_set_kick_variant takes it),
+ * ms[0 .. n-1] per kick launch, ms[n] the map pass, ms[n+1] the map pass with
+ * the kick (ms holds n + 2 values). */
 int cg_autotune(cg_handle* h, int k, int reps, int* choice, double* ms);
 
 /* ---- bunch-sharded runs over several GPUs (no counterpart in the reference,
