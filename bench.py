@@ -205,6 +205,9 @@ def main():
     beam.Run(0, 1)
     tune = beam.autotune(0, reps=10)
     t_first = 1
+    # pipeline shape (walk segments x walk CTA size) over whole turns; the
+    # beam is restored after each trial
+    pipe = beam.autotune_pipeline(t_first, reps=3) if wl.cfg.flag_beam_ion else None
     beam.Run(t_first, args.warmup)
     barrier()
     times = []
@@ -338,7 +341,12 @@ def main():
                          "chosen_shape": int(tune[0]) % (len(tune[1]) - 2),
                          "kick_in_map_pass": bool(tune[0] >= len(tune[1]) - 2),
                          "shapes": ["256 thr x3/SM", "256 thr x4/SM", "128 thr x4/SM",
-                                    "128 thr x6/SM"]},
+                                    "128 thr x6/SM"],
+                         "pipeline": None if pipe is None else {
+                             "segments": pipe[0][0], "walk_ions": pipe[0][1],
+                             "turn_ms": {f"{g}x{w}": round(float(m), 4) for (g, w), m in zip(
+                                 [(1, 64), (2, 64), (3, 64), (4, 64), (6, 64),
+                                  (1, 16), (2, 16), (3, 16), (4, 16), (6, 16)], pipe[1])}}},
             "surrogate": sur,
             "e2e": {"value": e2e_value, "unit": "macroparticle-turns/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},

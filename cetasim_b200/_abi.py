@@ -148,6 +148,8 @@ EXPORTS = [
     ("cg_faddeeva_w_q1", I, [PD, PD, PD, PD, C.c_int64]),
     ("cg_gaussian_field", I, [PD, PD, PD, PD, PD, PD, C.c_int64]),
     ("cg_kick_variants", I, [PI]),
+    ("cg_set_pipeline", I, [C.c_void_p, I, I]),
+    ("cg_autotune_pipeline", I, [C.c_void_p, I, I, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p]),
     ("cg_set_kick_variant", I, [C.c_void_p, I]),
     ("cg_autotune", I, [C.c_void_p, I, I, PI, PD]),
     ("cg_shard_plan", I, [PI, I, I, PI, PI]),

@@ -145,6 +145,18 @@ class MPBeam:
     def set_kick_variant(self, v: int):
         self._check(self.lib.cg_set_kick_variant(self.h, v))
 
+    def set_pipeline(self, groups: int, walk_ions: int = 0):
+        self._check(self.lib.cg_set_pipeline(self.h, groups, walk_ions))
+
+    def autotune_pipeline(self, turn0: int, reps: int = 5):
+        """Times whole turns with each pipeline shape, restores the beam and
+        keeps the fastest; returns ((groups, walk_ions), ms per shape)."""
+        ms = np.zeros(10)
+        g, w = C.c_int(), C.c_int()
+        self._check(self.lib.cg_autotune_pipeline(self.h, turn0, reps, C.byref(g), C.byref(w),
+                                                  _abi.ptr(ms)))
+        return (g.value, w.value), ms
+
     # -- checkpoint / resume ------------------------------------------------------
     def checkpoint(self) -> bytes:
         n = C.c_size_t()

@@ -80,6 +80,8 @@ int check_status(Handle& h) {
     return fail(&h, CG_ERR_TIMEOUT, "a tensor-core completion wait of the field surrogate gave up");
   if (st & kStatusLrRange)
     return fail(&h, CG_ERR_INVALID, "long-range wake lag outside the wake table (tau > 0)");
+  if (st & kStatusCopyWait)
+    return fail(&h, CG_ERR_TIMEOUT, "a bulk-copy completion wait of the map pass gave up");
   return fail(&h, CG_ERR_CUDA, "unknown device status");
 }
 
@@ -100,7 +102,7 @@ void free_beam(Handle& h) {
   d.mom_send = nullptr; d.mom_all = nullptr; d.sh_off = nullptr; d.sh_cnt = nullptr;
   IonWalk& w = d.iw;
   dfree(w.births); dfree(w.prep); dfree(w.bunch); dfree(w.spec); dfree(w.bound); dfree(w.part);
-  dfree(w.traj); dfree(w.alive);
+  dfree(w.traj); dfree(w.alive); dfree(w.carry);
   w = IonWalk();
   d.c = nullptr; d.surv = nullptr; d.tile_bunch = nullptr; d.chunk_bunch = nullptr;
   d.bunch = nullptr; d.partials = nullptr;
@@ -351,6 +353,16 @@ int cg_create(const cg_config* cfg, int device, cg_handle** out) {
     cg_destroy(H);
     return code;
   };
+  if ((e = cudaStreamCreateWithFlags(&h.side, cudaStreamNonBlocking)) != cudaSuccess)
+    return bail(CG_ERR_CUDA, cudaGetErrorString(e));
+  if ((e = cudaStreamCreateWithFlags(&h.side2, cudaStreamNonBlocking)) != cudaSuccess)
+    return bail(CG_ERR_CUDA, cudaGetErrorString(e));
+  h.pipe_ev.assign(kMaxPipeGroups + 1, nullptr);
+  h.kick_ev.assign(kMaxPipeGroups + 1, nullptr);
+  for (auto* evs : {&h.pipe_ev, &h.kick_ev})
+    for (auto& ev : *evs)
+      if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess)
+        return bail(CG_ERR_CUDA, cudaGetErrorString(e));
   if ((e = cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking)) != cudaSuccess)
     return bail(CG_ERR_CUDA, cudaGetErrorString(e));
   if ((e = dalloc(&h.sec_dev, h.K)) != cudaSuccess) return bail(CG_ERR_OOM, "sections");
@@ -461,6 +473,11 @@ int cg_destroy(cg_handle* H) {
   dfree(h.d.cloud_state); dfree(h.d.lr_tab); dfree(h.d.lr_head); dfree(h.d.fir_coeff);
   dfree(h.d.fir_head); dfree(h.d.sr_green);
   if (h.stream) cudaStreamDestroy(h.stream);
+  if (h.side) cudaStreamDestroy(h.side);
+  if (h.side2) cudaStreamDestroy(h.side2);
+  for (auto* evs : {&h.pipe_ev, &h.kick_ev})
+    for (auto ev : *evs)
+      if (ev) cudaEventDestroy(ev);
   delete H;
   return CG_OK;
 }
@@ -521,6 +538,9 @@ int cg_set_beam(cg_handle* H, int M, const int* n_macro, const int* harm, const 
     chunks += nc;
   }
   h.tile_off[M] = tiles;
+  h.chunk_off.assign(M + 1, 0);
+  for (int j = 0; j < M; ++j) h.chunk_off[j] = bd[j].chunk_off;
+  h.chunk_off[M] = chunks;
   h.n_tiles = tiles;
   h.n_chunks = chunks;
   h.npad = (int64_t)tiles * kTile;
@@ -571,11 +591,11 @@ int cg_set_beam(cg_handle* H, int M, const int* n_macro, const int* harm, const 
     IonWalk& w = d.iw;
     const size_t NM = (size_t)h.cfg.ion.macro_ions_per_ip, P = (size_t)h.P;
     w.tcap = (int64_t)h.ion_cap + (int64_t)M * (int64_t)NM;
-    w.grid = ion_walk_grid(w.tcap);
+    w.grid = ion_walk_grid(w.tcap, 16);  // the most walk CTAs of any shape
     if (dalloc(&w.births, P * M * NM * 2) || dalloc(&w.prep, (size_t)M) ||
         dalloc(&w.bunch, 3 * (size_t)M) || dalloc(&w.spec, P * M * 2) || dalloc(&w.bound, 2) ||
         dalloc(&w.part, P * M * (size_t)w.grid * 5) || dalloc(&w.traj, P * 4 * (size_t)w.tcap) ||
-        dalloc(&w.alive, P * (size_t)w.tcap)) {
+        dalloc(&w.alive, P * (size_t)w.tcap) || dalloc(&w.carry, 4 * P)) {
       free_beam(h);
       return fail(&h, CG_ERR_OOM, "ion chain scratch");
     }
@@ -813,16 +833,52 @@ static cudaError_t enqueue_turn(Handle& h) {
   // after the last IP those of section K-1 for the wakes, MPBeam.cpp:1069)
   const bool post = c.flag_lr_wake || c.flag_sr_wake;
   if (c.flag_beam_ion && ((e = launch_moments(h, 0)) || (e = exchange_moments(h)))) return e;
+  const int G = std::max(1, std::min(h.pipe_groups, h.M));
   for (int k = 0; k < h.K; ++k) {
     const bool fused = c.flag_beam_ion && !h.d.sur_w && h.fuse_kick;
-    if (c.flag_beam_ion) {
-      if ((e = launch_ion_chain(h, k))) return e;
-      if (!fused && (e = h.d.sur_w ? launch_ion_kick_sur(h, k) : launch_ion_kick(h, k))) return e;
-    }
     int mom = -1;
     if (k + 1 < h.K) mom = c.flag_beam_ion ? k + 1 : -1;
     else mom = post ? h.K - 1 : -1;
-    if ((e = launch_map_pass(h, k, mom, fused))) return e;
+    if (c.flag_beam_ion && G > 1) {
+      // the walk in G segments of bunches on the main stream; as soon as a
+      // segment is walked, its records and kick on `side` and its map (with
+      // the next IP's moments) on `side2`, so that the walk of segment g + 1,
+      // the kick of g + 1 and the map of g run at the same time
+      if ((e = launch_ion_prep(h, k))) return e;
+      for (int g = 0; g < G; ++g) {
+        const int ja = (int)((int64_t)h.M * g / G), jb = (int)((int64_t)h.M * (g + 1) / G);
+        if ((e = launch_ion_walk(h, k, ja, jb, h.stream))) return e;
+        if ((e = cudaEventRecord(h.pipe_ev[g], h.stream))) return e;
+        if ((e = cudaStreamWaitEvent(h.side, h.pipe_ev[g], 0))) return e;
+        if ((e = launch_ion_records(h, k, ja, jb, h.side))) return e;
+        const int ta = h.tile_off[ja], tb = h.tile_off[jb];
+        const int ca = h.chunk_off[ja], cb = h.chunk_off[jb];
+        if (fused) {
+          if ((e = launch_map_pass(h, k, mom, true, ca, cb, h.side))) return e;
+          continue;
+        }
+        e = h.d.sur_w ? launch_ion_kick_sur(h, k, ta, tb, h.side)
+                      : launch_ion_kick_variant(h, k, h.kick_variant, ta, tb, h.side);
+        if (e) return e;
+        if ((e = cudaEventRecord(h.kick_ev[g], h.side))) return e;
+        if ((e = cudaStreamWaitEvent(h.side2, h.kick_ev[g], 0))) return e;
+        if ((e = launch_map_pass(h, k, mom, false, ca, cb, h.side2))) return e;
+      }
+      if ((e = launch_ion_compact(h, k, h.side))) return e;
+      if ((e = cudaEventRecord(h.pipe_ev[kMaxPipeGroups], h.side))) return e;
+      if ((e = cudaStreamWaitEvent(h.stream, h.pipe_ev[kMaxPipeGroups], 0))) return e;
+      if (!fused) {
+        if ((e = cudaEventRecord(h.kick_ev[kMaxPipeGroups], h.side2))) return e;
+        if ((e = cudaStreamWaitEvent(h.stream, h.kick_ev[kMaxPipeGroups], 0))) return e;
+      }
+    } else {
+      if (c.flag_beam_ion) {
+        if ((e = launch_ion_chain(h, k))) return e;
+        if (!fused && (e = h.d.sur_w ? launch_ion_kick_sur(h, k) : launch_ion_kick(h, k)))
+          return e;
+      }
+      if ((e = launch_map_pass(h, k, mom, fused))) return e;
+    }
     if (mom >= 0 && (e = exchange_moments(h))) return e;
   }
   if (c.flag_lr_wake && (e = launch_lr_compute(h))) return e;
@@ -891,7 +947,13 @@ void* cg_stream(cg_handle* H) { return H ? (void*)H->h.stream : nullptr; }
 static int count_turn_launches(Handle& h) {
   const cg_config& c = h.cfg;
   int n = h.K;                                   // map + moments passes
-  if (c.flag_beam_ion) n += 1 + 4 * h.K;         // moments at IP 0 + prep/walk/finish/kick per IP
+  const int G = std::max(1, std::min(h.pipe_groups, h.M));
+  if (c.flag_beam_ion) {                         // moments at IP 0, then per IP:
+    if (G > 1) n += 1 + h.K * (2 + 3 * G + (G - 1));  // prep, compact, G x (walk, records,
+                                                       // kick), G - 1 more map passes
+    else n += 1 + 5 * h.K;                       // prep, walk, records, compact, kick
+    if (h.fuse_kick && !h.d.sur_w) n -= h.K * G;  // kicks inside the map passes
+  }
   if (c.flag_lr_wake) n += 2;                    // push + forces
   n += 1;                                        // longitudinal tail
   if (c.flag_sr_wake) n += 5;
@@ -932,6 +994,10 @@ int cg_time_stage(cg_handle* H, int stage, int k, int reps, double* ms) {
       case 5: e = launch_map_pass(h, k, k); break;
       case 7:
         e = h.cfg.flag_beam_ion ? launch_map_pass(h, k, k, true) : cudaErrorInvalidValue;
+        break;
+      case 8: e = launch_map_stream(h, k, k); break;
+      case 9:
+        e = h.cfg.flag_beam_ion ? launch_map_stream(h, k, k, true) : cudaErrorInvalidValue;
         break;
       case 6:
         e = h.d.sur_w ? launch_ion_kick_sur(h, k) : cudaErrorInvalidValue;
@@ -1221,6 +1287,23 @@ int cg_autotune(cg_handle* H, int k, int reps, int* choice, double* ms) {
   return st;
 }
 
+int cg_set_pipeline(cg_handle* H, int groups, int walk_ions) {
+  if (!H) return CG_ERR_INVALID;
+  Handle& h = H->h;
+  if (groups < 1 || groups > kMaxPipeGroups)
+    return fail(&h, CG_ERR_INVALID, "pipeline groups must be 1 .. 16");
+  if (walk_ions == 0) walk_ions = h.walk_ions;
+  if (walk_ions != 16 && walk_ions != 32 && walk_ions != 64)
+    return fail(&h, CG_ERR_INVALID, "walk_ions must be 16, 32 or 64 (0: keep)");
+  if ((h.pipe_groups != groups || h.walk_ions != walk_ions) && h.turn_graph) {
+    cudaGraphExecDestroy(h.turn_graph);
+    h.turn_graph = nullptr;
+  }
+  h.pipe_groups = groups;
+  h.walk_ions = walk_ions;
+  return CG_OK;
+}
+
 // ---- bunch sharding over ranks ----
 
 int cg_shard_plan(const int* n_macro, int M, int world, int* j0, int* j1) {
@@ -1433,6 +1516,52 @@ int cg_checkpoint_load(cg_handle* H, const void* buf, size_t bytes) {
   }
   CG_CUDA(&h, cudaDeviceSynchronize());
   return CG_OK;
+}
+
+// The pipeline shapes cg_autotune_pipeline tries, in order: (segments, walk ions).
+static const int kPipeShapes[CG_PIPE_SHAPES][2] = {{1, 64}, {2, 64}, {3, 64}, {4, 64}, {6, 64},
+                                                   {1, 16}, {2, 16}, {3, 16}, {4, 16}, {6, 16}};
+
+int cg_autotune_pipeline(cg_handle* H, int turn0, int reps, int* groups, int* walk_ions,
+                         double* ms) {
+  STAGE_PROLOGUE
+  if (!h.cfg.flag_beam_ion) return fail(&h, CG_ERR_NOT_READY, "runBeamIonFlag is off");
+  if (reps < 1 || turn0 < 0) return fail(&h, CG_ERR_INVALID, "bad arguments");
+  // whole turns change the beam and the clouds: a checkpoint in host memory
+  // puts them back after every trial
+  size_t n = 0;
+  int st = cg_checkpoint_size(H, &n);
+  if (st) return st;
+  std::vector<char> keep(n);
+  if ((st = cg_checkpoint_save(H, keep.data(), n))) return st;
+  cudaEvent_t e0, e1;
+  CG_CUDA(&h, cudaEventCreate(&e0));
+  CG_CUDA(&h, cudaEventCreate(&e1));
+  int best = -1;
+  double best_ms = 0;
+  for (int v = 0; v < CG_PIPE_SHAPES && !st; ++v) {
+    if ((st = cg_set_pipeline(H, kPipeShapes[v][0], kPipeShapes[v][1]))) break;
+    if ((st = cg_run_turns(H, turn0, 1))) break;  // captures the turn graph
+    cudaEventRecord(e0, h.stream);
+    if ((st = cg_run_turns(H, turn0 + 1, reps))) break;
+    cudaEventRecord(e1, h.stream);
+    cudaEventSynchronize(e1);
+    float t = 0;
+    cudaEventElapsedTime(&t, e0, e1);
+    const double per = (double)t / reps;
+    if (ms) ms[v] = per;
+    if (best < 0 || per < best_ms) {
+      best = v;
+      best_ms = per;
+    }
+    st = cg_checkpoint_load(H, keep.data(), n);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st) return st;
+  if (groups) *groups = kPipeShapes[best][0];
+  if (walk_ions) *walk_ions = kPipeShapes[best][1];
+  return cg_set_pipeline(H, kPipeShapes[best][0], kPipeShapes[best][1]);
 }
 
 // ---- field surrogate ----

@@ -12,6 +12,7 @@ namespace cg {
 constexpr int kTile = 256;            // particles per tile == threads per CTA
 
 constexpr int kMomChunkTiles = 4;     // tiles per CTA of the moments kernel
+constexpr int kMaxPipeGroups = 16;    // segments of the pipelined ion pass
 
 struct BunchDev {
   int n, tile_off, n_tiles, harm, gap;
@@ -63,6 +64,7 @@ struct IonWalk {
   double* part = nullptr;     // P x M x grid x (count, sum x, sum y, sum x^2, sum y^2)
   double* traj = nullptr;     // P x 4 x tcap: x, y, vx, vy after the walk
   uint8_t* alive = nullptr;   // P x tcap
+  double* carry = nullptr;    // P x (centroid x, y carried between steps, last rms x, y)
   int64_t tcap = 0;           // trajectories per species: cloud capacity + M x NM
   int grid = 0;               // CTAs of k_ion_walk per species
 };
@@ -129,7 +131,18 @@ struct Handle {
   int n_tiles = 0;
   int n_chunks = 0;
   int64_t npad = 0;
-  std::vector<int> n_macro, harm, gap, tile_off;
+  std::vector<int> n_macro, harm, gap, tile_off, chunk_off;
+  // pipelined turn: the ion walk of an IP in `pipe_groups` segments of bunches;
+  // records, kicks and maps of a segment run on `side` while the next segment
+  // walks
+  int pipe_groups = 4;
+  // trajectories per walk CTA (16, 32, 64): a smaller CTA finds room on an
+  // SM sooner while the kicks and maps of earlier segments fill the GPU
+  int walk_ions = 64;
+  cudaStream_t side = nullptr;   // records and kicks of the segments
+  cudaStream_t side2 = nullptr;  // maps of the segments (kick g + 1 overlaps map g)
+  std::vector<cudaEvent_t> pipe_ev;  // kMaxPipeGroups + 1: walked segments, then the join
+  std::vector<cudaEvent_t> kick_ev;  // kMaxPipeGroups + 1: kicked segments, then the join
   std::vector<double> ne;
   DeviceBufs d;
   int lr_np = 0;

@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 #include <algorithm>
 #include "kernels.cuh"
+#include "bulk.cuh"
 
 namespace cg {
 
@@ -161,25 +162,18 @@ __device__ __forceinline__ void store6(double* __restrict__ c, int64_t npad, int
 // totals every thread needs for the centred pass, then the centred
 // co-moments, whose totals only thread 0 needs.  Three barriers; the warp
 // stage of the sums uses the transposed butterfly (warp_sum8_t).
-__device__ void chunk_moment_partial(const double (&v)[kMomChunkTiles][6],
-                                     const bool (&alive)[kMomChunkTiles], double* smem,
-                                     MomPartial* out) {
+// The reductions of a chunk partial from this thread's sums over its alive
+// particles (s: six coordinates then the count; mn, mx: the z range), with
+// get(u, d) = coordinate d of the thread's particle in tile u, read again for
+// the centred pass (only where alive[u]).
+template <class Get>
+__device__ __forceinline__ void chunk_moment_reduce(double (&s)[7], double mn, double mx,
+                                                    const bool (&alive)[kMomChunkTiles], Get get,
+                                                    double* smem, MomPartial* out) {
   constexpr int NW = kTile / 32;
   double* sa = smem;            // 9 x 32: sums (7), min z, max z
   double* sb = smem + 9 * 32;   // 9 x 32: centred co-moments
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  double s[7] = {0, 0, 0, 0, 0, 0, 0};
-  double mn = INFINITY, mx = -INFINITY;
-#pragma unroll
-  for (int u = 0; u < kMomChunkTiles; ++u) {
-#pragma unroll
-    for (int d = 0; d < 6; ++d) s[d] += alive[u] ? v[u][d] : 0.0;
-    s[6] += alive[u] ? 1.0 : 0.0;
-    if (alive[u]) {
-      mn = fmin(mn, v[u][4]);
-      mx = fmax(mx, v[u][4]);
-    }
-  }
   {
     const double s8[8] = {s[0], s[1], s[2], s[3], s[4], s[5], s[6], 0.0};
     const double t = warp_sum8_t(s8);
@@ -220,7 +214,7 @@ __device__ void chunk_moment_partial(const double (&v)[kMomChunkTiles][6],
   for (int u = 0; u < kMomChunkTiles; ++u) {
     double dv[6];
 #pragma unroll
-    for (int d = 0; d < 6; ++d) dv[d] = alive[u] ? v[u][d] - mean[d] : 0.0;
+    for (int d = 0; d < 6; ++d) dv[d] = alive[u] ? get(u, d) - mean[d] : 0.0;
 #pragma unroll
     for (int d = 0; d < 6; ++d) q[d] = fma(dv[d], dv[d], q[d]);
     q[6] = fma(dv[0], dv[1], q[6]);
@@ -253,6 +247,28 @@ __device__ void chunk_moment_partial(const double (&v)[kMomChunkTiles][6],
     p.zmax = mx;
     *out = p;
   }
+}
+
+// The thread's sums over its alive particles in tile order, as the reductions
+// take them.
+__device__ __forceinline__ void chunk_sums_add(const double (&v)[6], double (&s)[7], double& mn,
+                                               double& mx) {
+#pragma unroll
+  for (int d = 0; d < 6; ++d) s[d] += v[d];
+  s[6] += 1.0;
+  mn = fmin(mn, v[4]);
+  mx = fmax(mx, v[4]);
+}
+
+__device__ void chunk_moment_partial(const double (&v)[kMomChunkTiles][6],
+                                     const bool (&alive)[kMomChunkTiles], double* smem,
+                                     MomPartial* out) {
+  double s[7] = {0, 0, 0, 0, 0, 0, 0};
+  double mn = INFINITY, mx = -INFINITY;
+#pragma unroll
+  for (int u = 0; u < kMomChunkTiles; ++u)
+    if (alive[u]) chunk_sums_add(v[u], s, mn, mx);
+  chunk_moment_reduce(s, mn, mx, alive, [&](int u, int d) { return v[u][d]; }, smem, out);
 }
 
 // Called by all threads of every CTA after its partial is stored: the last of
@@ -373,12 +389,13 @@ __global__ void __launch_bounds__(NT, MINB) k_ion_kick(double* __restrict__ c, i
                                                       const uint8_t* __restrict__ surv,
                                                       const int* __restrict__ tile_bunch,
                                                       const BunchDev* __restrict__ bunch,
-                                                      const CloudRec* __restrict__ rec, int P) {
+                                                      const CloudRec* __restrict__ rec, int P,
+                                                      int tile_base) {
   // the field constants of the bunch's records, once per CTA (a tile holds
   // particles of one bunch)
   __shared__ FieldPrep s_prep[CG_MAX_SPECIES];
   constexpr int kSub = kTile / NT;
-  const int tile = blockIdx.x / kSub;
+  const int tile = tile_base + (int)(blockIdx.x / kSub);
   const int b = tile_bunch[tile];
   const BunchDev& B = bunch[b];
   const int lane = (blockIdx.x % kSub) * NT + threadIdx.x;
@@ -399,24 +416,29 @@ __global__ void __launch_bounds__(NT, MINB) k_ion_kick(double* __restrict__ c, i
 static const int kKickShapes[][2] = {{256, 3}, {256, 4}, {128, 4}, {128, 6}};
 constexpr int kKickVariants = 4;
 
-cudaError_t launch_ion_kick_variant(Handle& h, int k, int v) {
+cudaError_t launch_ion_kick_variant(Handle& h, int k, int v, int tile_a, int tile_b,
+                                    cudaStream_t s) {
   const CloudRec* rec = h.d.rec + (size_t)k * h.M * h.P;
+  if (tile_b < 0) tile_b = h.n_tiles;
+  if (!s) s = h.stream;
+  const int nt = tile_b - tile_a;
+  if (nt <= 0) return cudaSuccess;
   switch (v) {
     case 1:
-      k_ion_kick<256, 4><<<h.n_tiles, 256, 0, h.stream>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch,
-                                                          h.d.bunch, rec, h.P);
+      k_ion_kick<256, 4><<<nt, 256, 0, s>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch, h.d.bunch,
+                                            rec, h.P, tile_a);
       break;
     case 2:
-      k_ion_kick<128, 4><<<2 * h.n_tiles, 128, 0, h.stream>>>(h.d.c, h.npad, h.d.surv,
-                                                              h.d.tile_bunch, h.d.bunch, rec, h.P);
+      k_ion_kick<128, 4><<<2 * nt, 128, 0, s>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch,
+                                                h.d.bunch, rec, h.P, tile_a);
       break;
     case 3:
-      k_ion_kick<128, 6><<<2 * h.n_tiles, 128, 0, h.stream>>>(h.d.c, h.npad, h.d.surv,
-                                                              h.d.tile_bunch, h.d.bunch, rec, h.P);
+      k_ion_kick<128, 6><<<2 * nt, 128, 0, s>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch,
+                                                h.d.bunch, rec, h.P, tile_a);
       break;
     default:
-      k_ion_kick<256, 3><<<h.n_tiles, 256, 0, h.stream>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch,
-                                                          h.d.bunch, rec, h.P);
+      k_ion_kick<256, 3><<<nt, 256, 0, s>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch, h.d.bunch,
+                                            rec, h.P, tile_a);
   }
   return cudaGetLastError();
 }
@@ -442,10 +464,12 @@ __global__ void __launch_bounds__(kTile, 2) k_map_pass(double* __restrict__ c, i
                                                     const __grid_constant__ RingDev r,
                                                     MomPartial* partials, unsigned* counters,
                                                     BunchMomDev* mom, double beta_x, double beta_y,
-                                                    const CloudRec* __restrict__ rec, int P) {
+                                                    const CloudRec* __restrict__ rec, int P,
+                                                    int chunk_base) {
   __shared__ double smem[18 * 32];
   __shared__ FieldPrep s_prep[CG_MAX_SPECIES];
-  const int b = chunk_bunch[blockIdx.x];
+  const int chunk = chunk_base + (int)blockIdx.x;
+  const int b = chunk_bunch[chunk];
   const BunchDev B = bunch[b];
   const CloudRec* rb = rec + (size_t)b * P;
   if (KICK) {
@@ -453,7 +477,7 @@ __global__ void __launch_bounds__(kTile, 2) k_map_pass(double* __restrict__ c, i
       s_prep[threadIdx.x] = field_prep(rb[threadIdx.x].rms_x, rb[threadIdx.x].rms_y);
     __syncthreads();
   }
-  const int tile0 = B.tile_off + (blockIdx.x - B.chunk_off) * kMomChunkTiles;
+  const int tile0 = B.tile_off + (chunk - B.chunk_off) * kMomChunkTiles;
   const int i0 = (tile0 - B.tile_off) * kTile + threadIdx.x;
   double v[kMomChunkTiles][6];
   bool alive[kMomChunkTiles];
@@ -478,23 +502,198 @@ __global__ void __launch_bounds__(kTile, 2) k_map_pass(double* __restrict__ c, i
     store6(c, npad, (int64_t)(tile0 + u) * kTile + threadIdx.x, v[u]);
   }
   if (MOM) {
-    chunk_moment_partial(v, alive, smem, &partials[blockIdx.x]);
+    chunk_moment_partial(v, alive, smem, &partials[chunk]);
     bunch_moment_finish(b, B.chunk_off, B.n_chunks, partials, counters, mom, beta_x, beta_y,
                         c + 4 * npad + (int64_t)B.tile_off * kTile);
   }
 }
 
-cudaError_t launch_map_pass(Handle& h, int k, int mom_section, bool kick) {
+cudaError_t launch_map_pass(Handle& h, int k, int mom_section, bool kick, int chunk_a,
+                            int chunk_b, cudaStream_t s) {
   const bool m = mom_section >= 0;
   const double bx = m ? h.sec_dev_host[mom_section].beta_x : 0.0;
   const double by = m ? h.sec_dev_host[mom_section].beta_y : 0.0;
   const CloudRec* rec = kick ? h.d.rec + (size_t)k * h.M * h.P : nullptr;
+  if (chunk_b < 0) chunk_b = h.n_chunks;
+  if (!s) s = h.stream;
+  if (chunk_b <= chunk_a) return cudaSuccess;
   auto kern = m ? (kick ? k_map_pass<true, true> : k_map_pass<true, false>)
                 : (kick ? k_map_pass<false, true> : k_map_pass<false, false>);
-  kern<<<h.n_chunks, kTile, 0, h.stream>>>(h.d.c, h.npad, h.d.surv, h.d.chunk_bunch, h.d.bunch,
+  kern<<<chunk_b - chunk_a, kTile, 0, s>>>(h.d.c, h.npad, h.d.surv, h.d.chunk_bunch, h.d.bunch,
                                            h.sec_dev_host[k], h.ring, h.d.partials,
-                                           h.d.counters, h.d.mom, bx, by, rec, h.P);
+                                           h.d.counters, h.d.mom, bx, by, rec, h.P, chunk_a);
   return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// The map pass with the chunks streamed through shared memory.  The register
+// pass above issues a chunk's loads, then computes and reduces with nothing in
+// flight, so DRAM idles while a CTA works.  Here a persistent grid of two CTAs
+// per SM walks the chunks [chunk_a, chunk_b) with stride gridDim.x; each CTA
+// has two chunk buffers, and one thread refills a buffer with the chunk two
+// ahead (seven bulk copies: six coordinate rows and the survival bytes of up
+// to kMomChunkTiles tiles, 2 KiB-aligned) as soon as the CTA has moved the
+// chunk into registers.  The arithmetic and the reductions are those of
+// k_map_pass, so the results are bitwise the same.
+
+constexpr int kStreamStages = 2;
+constexpr int kChunkParticles = kMomChunkTiles * kTile;
+constexpr uint32_t kCopyWaitLimit = 1u << 26;  // mbarrier polls before giving up
+struct StreamBuf {
+  double v[6][kChunkParticles];
+  uint8_t s[kChunkParticles];
+};
+static_assert(sizeof(StreamBuf) % 16 == 0, "buffers stay 16-byte aligned");
+constexpr size_t kStreamSmem = kStreamStages * sizeof(StreamBuf);
+
+struct ChunkLoc {
+  int b, tile0, nt;
+};
+__device__ __forceinline__ ChunkLoc chunk_loc(int chunk, const int* chunk_bunch,
+                                              const BunchDev* bunch) {
+  ChunkLoc l;
+  l.b = chunk_bunch[chunk];
+  const BunchDev& B = bunch[l.b];
+  const int q = chunk - B.chunk_off;
+  l.tile0 = B.tile_off + q * kMomChunkTiles;
+  l.nt = min(kMomChunkTiles, B.n_tiles - q * kMomChunkTiles);
+  return l;
+}
+
+template <bool MOM, bool KICK>
+__global__ void __launch_bounds__(kTile, 2) k_map_stream(double* __restrict__ c, int64_t npad,
+                                                      const uint8_t* __restrict__ surv,
+                                                      const int* __restrict__ chunk_bunch,
+                                                      const BunchDev* __restrict__ bunch,
+                                                      const __grid_constant__ SectionDev sec,
+                                                      const __grid_constant__ RingDev r,
+                                                      MomPartial* partials, unsigned* counters,
+                                                      BunchMomDev* mom, double beta_x,
+                                                      double beta_y,
+                                                      const CloudRec* __restrict__ rec, int P,
+                                                      int chunk_a, int chunk_b, int* status) {
+  extern __shared__ __align__(128) unsigned char dyn_smem[];
+  StreamBuf* buf = reinterpret_cast<StreamBuf*>(dyn_smem);
+  __shared__ __align__(8) uint64_t s_bar[kStreamStages];
+  __shared__ double smem[18 * 32];
+  __shared__ FieldPrep s_prep[CG_MAX_SPECIES];
+  const int tid = threadIdx.x;
+  const int nmine = (chunk_b - chunk_a - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+  if (nmine <= 0) return;
+  if (tid == 0) {
+    for (int st = 0; st < kStreamStages; ++st) umma::mbar_init(umma::smem_addr(&s_bar[st]), 1);
+    bulk::fence_mbar_init();
+  }
+  __syncthreads();
+  // thread 0: chunk number `it` of this CTA into buffer it % kStreamStages
+  auto issue = [&](int it) {
+    const ChunkLoc l = chunk_loc(chunk_a + (int)blockIdx.x + it * (int)gridDim.x, chunk_bunch, bunch);
+    StreamBuf& sb = buf[it % kStreamStages];
+    const uint32_t bar = umma::smem_addr(&s_bar[it % kStreamStages]);
+    const uint32_t bc = (uint32_t)l.nt * kTile * sizeof(double), bs = (uint32_t)l.nt * kTile;
+    bulk::arrive_expect(bar, 6 * bc + bs);
+    const int64_t g0 = (int64_t)l.tile0 * kTile;
+#pragma unroll
+    for (int d = 0; d < 6; ++d) bulk::load(umma::smem_addr(&sb.v[d][0]), c + d * npad + g0, bc, bar);
+    bulk::load(umma::smem_addr(&sb.s[0]), surv + g0, bs, bar);
+  };
+  if (tid == 0)
+    for (int it = 0; it < kStreamStages && it < nmine; ++it) issue(it);
+  for (int it = 0; it < nmine; ++it) {
+    const int chunk = chunk_a + (int)blockIdx.x + it * (int)gridDim.x;
+    const ChunkLoc l = chunk_loc(chunk, chunk_bunch, bunch);
+    const BunchDev B = bunch[l.b];
+    const CloudRec* rb = rec + (size_t)l.b * P;
+    if (KICK && tid < P) s_prep[tid] = field_prep(rb[tid].rms_x, rb[tid].rms_y);
+    const int st = it % kStreamStages;
+    const bool ok = umma::mbar_wait(umma::smem_addr(&s_bar[st]), (uint32_t)(it / kStreamStages) & 1u,
+                                    kCopyWaitLimit);
+    if (__syncthreads_or(!ok)) {
+      // give up: record it, let the copies in flight land, leave
+      if (tid == 0) {
+        atomicOr(status, kStatusCopyWait);
+        for (int j = it; j < it + kStreamStages && j < nmine; ++j)
+          umma::mbar_wait(umma::smem_addr(&s_bar[j % kStreamStages]),
+                          (uint32_t)(j / kStreamStages) & 1u, kCopyWaitLimit);
+      }
+      return;
+    }
+    StreamBuf& sb = buf[st];
+    const int i0 = (l.tile0 - B.tile_off) * kTile + tid;
+    double v[kMomChunkTiles][6];
+    bool alive[kMomChunkTiles];
+#pragma unroll
+    for (int u = 0; u < kMomChunkTiles; ++u) {
+      const int idx = u * kTile + tid;
+      const bool valid = i0 + u * kTile < B.n;
+      alive[u] = valid && sb.s[idx] == kAlive;
+#pragma unroll
+      for (int d = 0; d < 6; ++d) v[u][d] = valid ? sb.v[d][idx] : 0.0;
+    }
+    // buffer st is read: the copy two chunks ahead may refill it
+    __syncthreads();
+    if (tid == 0 && it + kStreamStages < nmine) issue(it + kStreamStages);
+#pragma unroll
+    for (int u = 0; u < kMomChunkTiles; ++u) {
+      if (!alive[u]) continue;
+      if (KICK) {
+        double dpx, dpy;
+        ion_kick_particle_prep(rb, s_prep, P, v[u][0], v[u][2], &dpx, &dpy);
+        v[u][1] += dpx;
+        v[u][3] += dpy;
+      }
+      section_map_particle(sec, r, v[u]);
+      store6(c, npad, (int64_t)(l.tile0 + u) * kTile + tid, v[u]);
+    }
+    if (MOM) {
+      chunk_moment_partial(v, alive, smem, &partials[chunk]);
+      bunch_moment_finish(l.b, B.chunk_off, B.n_chunks, partials, counters, mom, beta_x, beta_y,
+                          c + 4 * npad + (int64_t)B.tile_off * kTile);
+    } else if (KICK) {
+      __syncthreads();  // s_prep is rewritten for the next chunk
+    }
+  }
+}
+
+template <bool MOM, bool KICK>
+static cudaError_t map_stream_kernel(int grid, cudaStream_t s, Handle& h, int k, double bx,
+                                     double by, const CloudRec* rec, int chunk_a, int chunk_b) {
+  static bool attr = false;  // once per instantiation
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(k_map_stream<MOM, KICK>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kStreamSmem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  k_map_stream<MOM, KICK><<<grid, kTile, kStreamSmem, s>>>(
+      h.d.c, h.npad, h.d.surv, h.d.chunk_bunch, h.d.bunch, h.sec_dev_host[k], h.ring,
+      h.d.partials, h.d.counters, h.d.mom, bx, by, rec, h.P, chunk_a, chunk_b, h.d.status);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_map_stream(Handle& h, int k, int mom_section, bool kick, int chunk_a,
+                              int chunk_b, cudaStream_t s) {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms < 1) sms = 1;
+  }
+  const bool m = mom_section >= 0;
+  const double bx = m ? h.sec_dev_host[mom_section].beta_x : 0.0;
+  const double by = m ? h.sec_dev_host[mom_section].beta_y : 0.0;
+  const CloudRec* rec = kick ? h.d.rec + (size_t)k * h.M * h.P : nullptr;
+  if (chunk_b < 0) chunk_b = h.n_chunks;
+  if (!s) s = h.stream;
+  if (chunk_b <= chunk_a) return cudaSuccess;
+  const int grid = std::min(chunk_b - chunk_a, 2 * sms);
+  if (m)
+    return kick ? map_stream_kernel<true, true>(grid, s, h, k, bx, by, rec, chunk_a, chunk_b)
+                : map_stream_kernel<true, false>(grid, s, h, k, bx, by, rec, chunk_a, chunk_b);
+  return kick ? map_stream_kernel<false, true>(grid, s, h, k, bx, by, rec, chunk_a, chunk_b)
+              : map_stream_kernel<false, false>(grid, s, h, k, bx, by, rec, chunk_a, chunk_b);
 }
 
 cudaError_t launch_ion_kick(Handle& h, int k) { return launch_ion_kick_variant(h, k, h.kick_variant); }

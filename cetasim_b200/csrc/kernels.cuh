@@ -11,19 +11,36 @@ enum : int {
   kStatusLrRange = 4,
   kStatusIonBirth = 8,
   kStatusSurrogateWait = 16,  // a tensor-core completion wait gave up
+  kStatusCopyWait = 32,       // a bulk-copy completion wait gave up
 };
 
 cudaError_t launch_moments(Handle& h, int k);
 cudaError_t launch_map(Handle& h, int k);
 cudaError_t launch_ion_chain(Handle& h, int k);
-int ion_walk_grid(int64_t tcap);
+// the chain in pieces (the pipelined turn): prep, walk / records of the bunch
+// steps [ja, jb), compaction
+cudaError_t launch_ion_prep(Handle& h, int k);
+cudaError_t launch_ion_walk(Handle& h, int k, int ja, int jb, cudaStream_t s);
+cudaError_t launch_ion_records(Handle& h, int k, int ja, int jb, cudaStream_t s);
+cudaError_t launch_ion_compact(Handle& h, int k, cudaStream_t s);
+// walk CTAs for `tcap` trajectory slots at `ions` trajectories per CTA
+int ion_walk_grid(int64_t tcap, int ions);
 cudaError_t launch_ion_kick(Handle& h, int k);
-cudaError_t launch_ion_kick_variant(Handle& h, int k, int v);
+// the kick of the tiles [tile_a, tile_b) (tile_b < 0: all) on stream s (null: h.stream)
+cudaError_t launch_ion_kick_variant(Handle& h, int k, int v, int tile_a = 0, int tile_b = -1,
+                                    cudaStream_t s = nullptr);
 int kick_variants();
 void kick_variant_shape(int v, int* threads, int* min_ctas);
 // (ion kick of IP k if `kick`) + map of section k + moments at section
-// `mom_section` (if >= 0)
-cudaError_t launch_map_pass(Handle& h, int k, int mom_section, bool kick = false);
+// `mom_section` (if >= 0), over the moments chunks [chunk_a, chunk_b)
+// (chunk_b < 0: all) on stream s (null: h.stream)
+cudaError_t launch_map_pass(Handle& h, int k, int mom_section, bool kick = false, int chunk_a = 0,
+                            int chunk_b = -1, cudaStream_t s = nullptr);
+// The same pass with the chunks streamed through shared memory: a persistent
+// grid (two CTAs per SM), each CTA with two chunk buffers filled by bulk
+// asynchronous copies while it maps and reduces the previous chunk.
+cudaError_t launch_map_stream(Handle& h, int k, int mom_section, bool kick = false,
+                              int chunk_a = 0, int chunk_b = -1, cudaStream_t s = nullptr);
 enum LongFlags : unsigned {
   kLongRF = 1,
   kLongDrift = 2,
@@ -62,7 +79,8 @@ cudaError_t launch_sur_step(const float* w, const float* xin, const float* tin, 
                             int64_t row0, int batch, uint64_t mul, uint64_t add, float* part,
                             float* m, float* v, float* wmut, float lr, float bc1, float bc2,
                             double* loss, float* grad_out, int* status, cudaStream_t s);
-cudaError_t launch_ion_kick_sur(Handle& h, int k);
+cudaError_t launch_ion_kick_sur(Handle& h, int k, int tile_a = 0, int tile_b = -1,
+                                cudaStream_t s = nullptr);
 cudaError_t launch_sur_audit(Handle& h, int k, unsigned long long* out);
 cudaError_t upload_weideman_table_sur();
 

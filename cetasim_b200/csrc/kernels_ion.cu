@@ -19,14 +19,15 @@
 // Three kernels per IP:
 //   k_ion_prep    per bunch: loss bounds, birth positions (Philox, attempts in
 //                 order), field constants, coefficients;
-//   k_ion_walk    each CTA walks 64 trajectories (four lanes per ion: w(z1)
+//   k_ion_walk    each CTA walks 16 to 64 trajectories (four lanes per ion: w(z1)
 //                 and w(z2) each split into halves of the series) through all bunches
 //                 without a barrier per bunch, and writes per-step partial
 //                 sums (count, sum x, y, x^2, y^2) every kWin bunches;
-//   k_ion_finish  per step: sums in CTA order -> cloud centroid and rms ->
-//                 the record the electron kick reads; stable compaction of the
-//                 survivors into the cloud (birth order, as the reference's
-//                 erase keeps it).
+//   k_ion_records per step: sums in CTA order -> cloud centroid and rms ->
+//                 the record the electron kick reads;
+//   k_ion_compact stable compaction of the survivors into the cloud (birth
+//                 order, as the reference's erase keeps it) and the cloud state.
+// The walk and the records also run as consecutive segments of bunch steps.
 // The critical path is one field evaluation per bunch passage of the longest
 // trajectory, instead of a block-synchronised cloud pass per bunch.
 #include <cuda_runtime.h>
@@ -37,12 +38,11 @@ namespace cg {
 
 #define FULL_MASK 0xffffffffu
 
-constexpr int kWalkIons = 64;                  // trajectories per CTA block
-constexpr int kWalkThreads = 4 * kWalkIons;    // four lanes per ion
+// The walk's CTA shape: IONS trajectories per block (16, 32 or 64), four
+// lanes per ion; per step the block's ions are summed in groups of 4 (in
+// trajectory order), then the groups in order.
 constexpr int kWin = 16;                       // steps per shared-memory window
-constexpr int kGroups = kWalkThreads / kWin;   // ion groups summed per step
-constexpr int kGroupIons = kWalkIons / kGroups;
-static_assert(kGroups * kGroupIons == kWalkIons, "ion groups tile the block");
+constexpr int kGroupIons = 4;
 constexpr int kPrepThreads = 128;
 constexpr int kFinishThreads = 1024;
 constexpr int kFinishChunk = 2048;             // steps per shared-memory chunk
@@ -133,15 +133,25 @@ __global__ void __launch_bounds__(kPrepThreads) k_ion_prep(ChainParams cp, Chain
   }
 }
 
-// One CTA block = 64 trajectories: index t < n0 is ion t of the cloud the
+// One CTA block = IONS trajectories: index t < n0 is ion t of the cloud the
 // previous call left, t >= n0 the ion born as number (t - n0) % NM at bunch
 // (t - n0) / NM.  blockIdx.y = species.  The step loop has no block barrier:
 // each ion's position at each step goes to a shared-memory window of kWin
 // steps, and after each window the CTA sums it per step in a fixed order
-// (groups of 8 ions, then the 16 groups) into the per-step partials.
-__global__ void __launch_bounds__(kWalkThreads, 1) k_ion_walk(ChainParams cp, IonWalk w,
-                                                         const CloudDev* __restrict__ clouds,
-                                                         const CloudState* __restrict__ cst) {
+// (groups of 4 ions, then the IONS / 4 groups) into the per-step partials.
+// A launch walks the bunch steps [ja, jb): trajectories that started before
+// ja resume from the state the previous segment stored, so the walk can run
+// as consecutive segments (the turn graph kicks the bunches of one segment
+// while the next segment walks).
+template <int IONS>
+__global__ void __launch_bounds__(4 * IONS, 1) k_ion_walk(ChainParams cp, IonWalk w,
+                                                      const CloudDev* __restrict__ clouds,
+                                                      const CloudState* __restrict__ cst,
+                                                      int ja, int jb) {
+  constexpr int kWalkIons = IONS;
+  constexpr int kWalkThreads = 4 * IONS;
+  constexpr int kGroups = IONS / kGroupIons;   // ion groups summed per step
+  static_assert(kGroups * kWin == kWalkThreads, "the group sums of a window cover the block");
   __shared__ double s_x[kWin][kWalkIons], s_y[kWin][kWalkIons];
   __shared__ uint8_t s_act[kWin][kWalkIons];
   __shared__ double s_grp[kWin][kGroups][5];
@@ -156,7 +166,7 @@ __global__ void __launch_bounds__(kWalkThreads, 1) k_ion_walk(ChainParams cp, Io
   if (c >= nblk) return;
   const int tid = threadIdx.x, slot = tid >> 2, sub = tid & 3;
   const bool second = (sub >> 1) != 0, upper = (sub & 1) != 0;
-  if (tid < kWeidemanN) s_a[tid] = weideman_table().a[tid];
+  for (int i = tid; i < kWeidemanN; i += kWalkThreads) s_a[i] = weideman_table().a[i];
   const double L = weideman_table().L;
   const CloudDev cd = clouds[p];
   const double bx = w.bound[0], by = w.bound[1];
@@ -170,26 +180,34 @@ __global__ void __launch_bounds__(kWalkThreads, 1) k_ion_walk(ChainParams cp, Io
     const int64_t t = (int64_t)blk * kWalkIons + slot;
     const int64_t tb = (int64_t)blk * kWalkIons;
     const int jfirst = tb < n0 ? 0 : (int)((tb - n0) / NM);
+    const int js = max(jfirst, ja);
     if (first && tid < 5)
-      for (int j = 0; j < jfirst; ++j) part[((size_t)j * G + c) * 5 + tid] = 0.0;
+      for (int j = ja; j < min(js, jb); ++j) part[((size_t)j * G + c) * 5 + tid] = 0.0;
     bool alive = t < T;
     int j0 = 0;
     double x = 0, y = 0, vx = 0, vy = 0;
     if (alive) {
-      if (t < n0) {
+      const int start = t < n0 ? 0 : (int)((t - n0) / NM);
+      if (t >= n0) j0 = start;
+      if (start < ja) {  // walked by an earlier segment
+        x = traj[t];
+        y = traj[w.tcap + t];
+        vx = traj[2 * w.tcap + t];
+        vy = traj[3 * w.tcap + t];
+        alive = alive_out[t] != 0;
+      } else if (t < n0) {
         x = cd.x[0][t];
         y = cd.y[0][t];
         vx = cd.vx[0][t];
         vy = cd.vy[0][t];
       } else {
         const int64_t b = t - n0;
-        j0 = (int)(b / NM);
         x = births[2 * b];
         y = births[2 * b + 1];
       }
     }
-    for (int jw = jfirst; jw < M; jw += kWin) {
-      const int nw = min(kWin, M - jw);
+    for (int jw = js; jw < jb; jw += kWin) {
+      const int nw = min(kWin, jb - jw);
       // the window's bunch constants in shared memory (global loads would sit
       // on the latency chain of every step)
       if (tid < nw) {
@@ -268,8 +286,8 @@ __global__ void __launch_bounds__(kWalkThreads, 1) k_ion_walk(ChainParams cp, Io
         }
       }
       __syncthreads();
-      if (tid < 5 * nw) {
-        const int s = tid / 5, q = tid % 5;
+      for (int e = tid; e < 5 * nw; e += kWalkThreads) {
+        const int s = e / 5, q = e % 5;
         double a = 0.0;
 #pragma unroll
         for (int g = 0; g < kGroups; ++g) a += s_grp[s][g][q];
@@ -289,30 +307,34 @@ __global__ void __launch_bounds__(kWalkThreads, 1) k_ion_walk(ChainParams cp, Io
   }
 }
 
-// Records and cloud update, one CTA per species.
-__global__ void __launch_bounds__(kFinishThreads) k_ion_finish(ChainParams cp, IonWalk w,
-                                                             CloudDev* clouds, CloudState* cst,
-                                                             CloudRec* rec, int* status, int G) {
+// Records of the bunch steps [ja, jb), one CTA per species: per step the
+// partial sums in CTA order -> cloud centroid and rms -> the record the
+// electron kick reads.  The one-ion quirk keeps the previous centroid, so the
+// centroid is carried from step to step and, across launches, in w.carry
+// (initialised from the cloud state at ja = 0); at jb = M the last rms is
+// kept there too, for the cloud state.
+__global__ void __launch_bounds__(kFinishThreads) k_ion_records(ChainParams cp, IonWalk w,
+                                                              const CloudState* __restrict__ cst,
+                                                              CloudRec* rec, int* status, int G,
+                                                              int ions, int ja, int jb) {
   __shared__ double s_ax[kFinishChunk], s_ay[kFinishChunk];
   __shared__ int s_n[kFinishChunk];
-  __shared__ int s_wsum[kFinishThreads / 32];
   __shared__ double s_carry[2];
-  __shared__ int s_base;
   const int p = blockIdx.x, P = cp.n_species, tid = threadIdx.x;
   const int M = cp.n_bunches, NM = cp.macro_per_ip;
   const CloudState st0 = cst[p];
   const int64_t T = (int64_t)st0.n + (int64_t)M * NM;
-  const int nblk = (int)((T + kWalkIons - 1) / kWalkIons);
+  const int nblk = (int)((T + ions - 1) / ions);
   const int nwork = nblk < G ? nblk : G;
   const double* part = w.part + (size_t)p * M * G * 5;
   const double* spec = w.spec + 2 * (size_t)p * M;
+  double* carry = w.carry + 4 * (size_t)p;
   if (tid == 0) {
-    s_carry[0] = st0.aver_x;
-    s_carry[1] = st0.aver_y;
+    s_carry[0] = ja == 0 ? st0.aver_x : carry[0];
+    s_carry[1] = ja == 0 ? st0.aver_y : carry[1];
   }
-  double last_rms_x = st0.rms_x, last_rms_y = st0.rms_y;
-  for (int j0 = 0; j0 < M; j0 += kFinishChunk) {
-    const int nj = min(kFinishChunk, M - j0);
+  for (int j0 = ja; j0 < jb; j0 += kFinishChunk) {
+    const int nj = min(kFinishChunk, jb - j0);
     __syncthreads();
     for (int jj = tid; jj < nj; jj += kFinishThreads) {
       const int j = j0 + jj;
@@ -342,6 +364,10 @@ __global__ void __launch_bounds__(kFinishThreads) k_ion_finish(ChainParams cp, I
       r.rms_y = ry;
       r.count = n;
       rec[(size_t)j * P + p] = r;  // centroid filled below
+      if (j == M - 1) {
+        carry[2] = rx;
+        carry[3] = ry;
+      }
     }
     __syncthreads();
     if (tid == 0) {  // the stale-centroid carry is sequential
@@ -364,14 +390,28 @@ __global__ void __launch_bounds__(kFinishThreads) k_ion_finish(ChainParams cp, I
       r->aver_x = s_ax[jj];
       r->aver_y = s_ay[jj];
     }
-    if (j0 + nj == M) {
-      const CloudRec* r = rec + (size_t)(M - 1) * P + p;
-      __syncthreads();
-      last_rms_x = r->rms_x;
-      last_rms_y = r->rms_y;
-    }
   }
-  // survivors in trajectory order -> cloud buffer 0
+  __syncthreads();
+  if (tid == 0) {
+    carry[0] = s_carry[0];
+    carry[1] = s_carry[1];
+  }
+}
+
+// After the last walk segment and the last records: the surviving ions in
+// trajectory order (birth order, as the reference's erase keeps it) into
+// cloud buffer 0, and the cloud state.  One CTA per species.
+__global__ void __launch_bounds__(kFinishThreads) k_ion_compact(ChainParams cp, IonWalk w,
+                                                              CloudDev* clouds, CloudState* cst,
+                                                              int* status) {
+  __shared__ int s_wsum[kFinishThreads / 32];
+  __shared__ int s_base;
+  const int p = blockIdx.x, tid = threadIdx.x;
+  const int M = cp.n_bunches, NM = cp.macro_per_ip;
+  const CloudState st0 = cst[p];
+  const int64_t T = (int64_t)st0.n + (int64_t)M * NM;
+  const double* spec = w.spec + 2 * (size_t)p * M;
+  const double* carry = w.carry + 4 * (size_t)p;
   CloudDev cd = clouds[p];
   const double* traj = w.traj + (size_t)p * 4 * w.tcap;
   const uint8_t* al = w.alive + (size_t)p * w.tcap;
@@ -405,16 +445,16 @@ __global__ void __launch_bounds__(kFinishThreads) k_ion_finish(ChainParams cp, I
     st.n = s_base < cd.cap ? s_base : cd.cap;
     if (s_base > cd.cap) atomicOr(status, kStatusIonOverflow);
     st.cur = 0;
-    st.aver_x = s_carry[0];
-    st.aver_y = s_carry[1];
-    st.rms_x = last_rms_x;
-    st.rms_y = last_rms_y;
+    st.aver_x = carry[0];
+    st.aver_y = carry[1];
+    st.rms_x = carry[2];
+    st.rms_y = carry[3];
     st.macro_charge = spec[2 * (M - 1)];
     cst[p] = st;
   }
 }
 
-cudaError_t launch_ion_chain(Handle& h, int k) {
+static ChainSection chain_section(const Handle& h, int k) {
   ChainSection cs;
   const cg_section& s = h.sections[k];
   cs.pressure = s.pressure;
@@ -422,24 +462,54 @@ cudaError_t launch_ion_chain(Handle& h, int k) {
   cs.length = s.length;
   cs.aperture_x = s.aperture_x;
   cs.aperture_y = s.aperture_y;
-  const int M = h.M;
-  k_ion_prep<<<(M + kPrepThreads - 1) / kPrepThreads, kPrepThreads, 0, h.stream>>>(
-      h.chain, cs, h.d.bunch, h.d.mom, h.d.iw, h.d.status, h.d.turn, k);
-  dim3 grid(h.d.iw.grid, h.P);
-  k_ion_walk<<<grid, kWalkThreads, 0, h.stream>>>(h.chain, h.d.iw, h.d.clouds + (size_t)k * h.P,
-                                                  h.d.cloud_state + (size_t)k * h.P);
-  k_ion_finish<<<h.P, kFinishThreads, 0, h.stream>>>(
-      h.chain, h.d.iw, h.d.clouds + (size_t)k * h.P, h.d.cloud_state + (size_t)k * h.P,
-      h.d.rec + (size_t)k * h.M * h.P, h.d.status, h.d.iw.grid);
+  return cs;
+}
+
+cudaError_t launch_ion_prep(Handle& h, int k) {
+  k_ion_prep<<<(h.M + kPrepThreads - 1) / kPrepThreads, kPrepThreads, 0, h.stream>>>(
+      h.chain, chain_section(h, k), h.d.bunch, h.d.mom, h.d.iw, h.d.status, h.d.turn, k);
   return cudaGetLastError();
+}
+
+cudaError_t launch_ion_walk(Handle& h, int k, int ja, int jb, cudaStream_t s) {
+  const int ions = h.walk_ions;
+  const dim3 grid(ion_walk_grid(h.d.iw.tcap, ions), h.P);
+  const CloudDev* cl = h.d.clouds + (size_t)k * h.P;
+  const CloudState* cs = h.d.cloud_state + (size_t)k * h.P;
+  if (ions == 16) k_ion_walk<16><<<grid, 64, 0, s>>>(h.chain, h.d.iw, cl, cs, ja, jb);
+  else if (ions == 32) k_ion_walk<32><<<grid, 128, 0, s>>>(h.chain, h.d.iw, cl, cs, ja, jb);
+  else k_ion_walk<64><<<grid, 256, 0, s>>>(h.chain, h.d.iw, cl, cs, ja, jb);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ion_records(Handle& h, int k, int ja, int jb, cudaStream_t s) {
+  k_ion_records<<<h.P, kFinishThreads, 0, s>>>(h.chain, h.d.iw, h.d.cloud_state + (size_t)k * h.P,
+                                               h.d.rec + (size_t)k * h.M * h.P, h.d.status,
+                                               ion_walk_grid(h.d.iw.tcap, h.walk_ions),
+                                               h.walk_ions, ja, jb);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ion_compact(Handle& h, int k, cudaStream_t s) {
+  k_ion_compact<<<h.P, kFinishThreads, 0, s>>>(h.chain, h.d.iw, h.d.clouds + (size_t)k * h.P,
+                                               h.d.cloud_state + (size_t)k * h.P, h.d.status);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ion_chain(Handle& h, int k) {
+  cudaError_t e = launch_ion_prep(h, k);
+  if (e == cudaSuccess) e = launch_ion_walk(h, k, 0, h.M, h.stream);
+  if (e == cudaSuccess) e = launch_ion_records(h, k, 0, h.M, h.stream);
+  if (e == cudaSuccess) e = launch_ion_compact(h, k, h.stream);
+  return e;
 }
 
 cudaError_t upload_weideman_table_ion() {
   return cudaMemcpyToSymbol(c_weideman, &h_weideman, sizeof(WeidemanTable));
 }
 
-int ion_walk_grid(int64_t tcap) {
-  const int64_t blocks = (tcap + kWalkIons - 1) / kWalkIons;
+int ion_walk_grid(int64_t tcap, int ions) {
+  const int64_t blocks = (tcap + ions - 1) / ions;
   return (int)std::max<int64_t>(1, std::min<int64_t>(blocks, 148 * 4));
 }
 

@@ -474,7 +474,7 @@ __global__ void __launch_bounds__(kSurRows, 3) k_ion_kick_sur(double* __restrict
                                                            const BunchDev* __restrict__ bunch,
                                                            const CloudRec* __restrict__ rec, int P,
                                                            const float* __restrict__ w,
-                                                           int n_half, int* status) {
+                                                           int ht_a, int ht_b, int* status) {
   extern __shared__ unsigned char dyn[];
   __shared__ SurSmall sm;
   __shared__ uint32_t s_tmem;
@@ -485,7 +485,7 @@ __global__ void __launch_bounds__(kSurRows, 3) k_ion_kick_sur(double* __restrict
   const uint32_t tmem = s_tmem, bar = umma::smem_addr(&s_bar);
   uint32_t phase = 0;
   bool ok = true;
-  for (int ht = blockIdx.x; ht < n_half; ht += gridDim.x) {
+  for (int ht = ht_a + blockIdx.x; ht < ht_b; ht += gridDim.x) {
     const int tile = ht >> 1, b = tile_bunch[tile];
     const BunchDev B = bunch[b];
     const int i = (tile - B.tile_off) * kTile + (ht & 1) * kSurRows + threadIdx.x;
@@ -620,11 +620,14 @@ cudaError_t launch_sur_step(const float* w, const float* xin, const float* tin, 
   return cudaGetLastError();
 }
 
-cudaError_t launch_ion_kick_sur(Handle& h, int k) {
-  const int n_half = 2 * h.n_tiles;
-  k_ion_kick_sur<<<sur_grid(n_half), kSurRows, kSmFwdBytes, h.stream>>>(
+cudaError_t launch_ion_kick_sur(Handle& h, int k, int tile_a, int tile_b, cudaStream_t s) {
+  if (tile_b < 0) tile_b = h.n_tiles;
+  if (!s) s = h.stream;
+  const int n_half = 2 * (tile_b - tile_a);
+  if (n_half <= 0) return cudaSuccess;
+  k_ion_kick_sur<<<sur_grid(n_half), kSurRows, kSmFwdBytes, s>>>(
       h.d.c, h.npad, h.d.surv, h.d.tile_bunch, h.d.bunch, h.d.rec + (size_t)k * h.M * h.P, h.P,
-      h.d.sur_w, n_half, h.d.status);
+      h.d.sur_w, 2 * tile_a, 2 * tile_b, h.d.status);
   return cudaGetLastError();
 }
 

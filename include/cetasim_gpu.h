@@ -344,6 +344,24 @@ int cg_set_kick_variant(cg_handle* h, int v);
  * the kick (ms holds n + 2 values). */
 int cg_autotune(cg_handle* h, int k, int reps, int* choice, double* ms);
 
+/* Pipelined turn: the ion walk of each IP runs in `groups` segments of
+ * bunches, and the records, kicks and maps of a segment run alongside the next
+ * segment's walk (1 = one segment, no overlap; default 4; at most 16); results
+ * do not depend on `groups`.  walk_ions: trajectories per walk CTA, 16, 32 or
+ * 64 (0 keeps the current shape); the shape sets the summation order of the
+ * cloud moments, so results agree to rounding across shapes. */
+int cg_set_pipeline(cg_handle* h, int groups, int walk_ions);
+
+/* Times whole turns (turn0 to warm up the turn graph, then `reps` turns, CUDA
+ * events on h's stream) with each of the CG_PIPE_SHAPES pipeline shapes
+ * (segments x walk ions: 1, 2, 3, 4, 6 segments with 64, then with 16
+ * trajectories per walk CTA), puts the beam and the ion clouds back from a
+ * host checkpoint after every trial, and keeps the fastest: *groups,
+ * *walk_ions, ms[CG_PIPE_SHAPES] per turn (either may be NULL). */
+#define CG_PIPE_SHAPES 10
+int cg_autotune_pipeline(cg_handle* h, int turn0, int reps, int* groups, int* walk_ions,
+                         double* ms);
+
 /* ---- bunch-sharded runs over several GPUs (no counterpart in the reference,
  * which is single-threaded) ---- */
 

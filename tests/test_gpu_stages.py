@@ -236,3 +236,86 @@ def test_kick_inside_the_map_pass_repeats_the_separate_kernels():
     worst = max(np.max(np.abs(a - b) / (np.abs(b).max(axis=1, keepdims=True) + 1e-300))
                 for a, b in zip(*runs))
     assert worst <= 1e-14
+
+
+@pytest.mark.parametrize("groups", [3, 4, 16])
+def test_pipelined_turn_repeats_the_unpipelined_turn(groups):
+    """The ion walk in segments with records, kicks and maps overlapping the
+    next segment gives the same turn bit for bit."""
+    wl = small("fast_ion", 0.01, bunch_current=TRAPPED)
+    parts = particles(wl, seed=9)
+    runs = []
+    for gcount in (1, groups):
+        g, _ = pair(wl, parts)
+        g.set_pipeline(gcount)
+        g.Run(0, 4)
+        runs.append(([g.download(j) for j in range(wl.n_bunches)],
+                     [g.ions(k) for k in (0, wl.cfg.n_sections - 1)],
+                     g.cloud_record(wl.cfg.n_sections - 1)))
+    (ca, ia, ra), (cb, ib, rb) = runs
+    for (x, s), (y, t) in zip(ca, cb):
+        assert np.array_equal(x, y) and np.array_equal(s, t)
+    for u, v in zip(ia, ib):
+        for p, q in zip(u, v):
+            assert np.array_equal(p, q)
+    assert np.array_equal(ra, rb)
+
+
+def _stage(g, stage, k, reps=1):
+    import ctypes as C
+    t = C.c_double()
+    g._check(g.lib.cg_time_stage(g.h, stage, k, reps, C.byref(t)))
+
+
+@pytest.mark.parametrize("name,scale,kick", [("batched_uneven", 0.05, False),
+                                             ("fast_ion", 0.15, False),
+                                             ("fast_ion", 0.15, True)])
+def test_streamed_map_pass_repeats_the_register_pass(name, scale, kick):
+    """The map pass fed by bulk copies into shared memory (stages 8, 9) gives
+    the coordinates and moments of the register pass (stages 5, 7) bit for
+    bit, on ragged bunches (partial chunks and tiles) with lost particles."""
+    wl = small(name, scale, bunch_current=TRAPPED if kick else None)
+    parts = particles(wl, seed=11, spread=3.0 if kick else 1.0)
+    rng = np.random.default_rng(12)
+    surv = [(rng.random(len(c[0])) < 0.1).astype(np.uint8) for c in parts]
+    runs = []
+    for stage in ((7, 9) if kick else (5, 8)):
+        g, _ = pair(wl, parts, surv)
+        g.MPBeamRMSCal(0)
+        if kick:
+            g.SSBeamIonEffectOneInteractionPoint(0, 0)
+        _stage(g, stage, 0, reps=3)  # three passes: the per-bunch counters rearm
+        runs.append(([g.download(j) for j in range(wl.n_bunches)], g.moments()))
+    (ca, ma), (cb, mb) = runs
+    for (x, s), (y, t) in zip(ca, cb):
+        assert np.array_equal(x, y) and np.array_equal(s, t)
+    assert bytes(ma) == bytes(mb)
+
+
+def test_pipeline_autotuner_restores_the_beam_and_shapes_agree():
+    """The pipeline autotuner runs whole turns with every shape and puts the
+    beam and the clouds back; the walk CTA size changes only the summation
+    order of the cloud moments."""
+    wl = small("fast_ion", 0.01, bunch_current=TRAPPED)
+    parts = particles(wl, seed=13)
+    g, _ = pair(wl, parts)
+    g.Run(0, 2)
+    before = ([g.download(j) for j in range(wl.n_bunches)], g.ions(0))
+    (groups, ions), ms = g.autotune_pipeline(2, reps=1)
+    assert (groups, ions) in [(1, 64), (2, 64), (3, 64), (4, 64), (6, 64),
+                              (1, 16), (2, 16), (3, 16), (4, 16), (6, 16)]
+    assert np.all(ms > 0)
+    after = ([g.download(j) for j in range(wl.n_bunches)], g.ions(0))
+    for (a, s), (b, t) in zip(before[0], after[0]):
+        assert np.array_equal(a, b) and np.array_equal(s, t)
+    for p, q in zip(before[1], after[1]):
+        assert np.array_equal(p, q)
+    runs = []
+    for ions in (16, 64):
+        h, _ = pair(wl, parts)
+        h.set_pipeline(3, ions)
+        h.Run(0, 4)
+        runs.append([h.download(j)[0] for j in range(wl.n_bunches)])
+    worst = max(np.max(np.abs(a - b) / (np.abs(b).max(axis=1, keepdims=True) + 1e-300))
+                for a, b in zip(*runs))
+    assert worst <= 1e-12
