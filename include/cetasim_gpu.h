@@ -282,7 +282,9 @@ int cg_run_turns(cg_handle* h, int turn0, int n_turns);
 /* Page-locked host buffer for fast uploads/downloads (cudaMallocHost). */
 void* cg_host_alloc(size_t bytes);
 void cg_host_free(void* p);
-/* The CUDA stream (cudaStream_t) all kernels of h run on. */
+/* The CUDA stream (cudaStream_t) h's work is ordered on: every call and every
+ * turn graph launch runs on it (the turn graph's branches join it before the
+ * turn ends). */
 void* cg_stream(cg_handle* h);
 /* Kernel launches one cg_run_turns turn issues. */
 int cg_turn_launches(cg_handle* h, int* launches);
@@ -291,7 +293,9 @@ int cg_turn_launches(cg_handle* h, int* launches);
  * field kick (k, uses the records of the last cg_beam_ion_ip at k), 2 ion
  * chain (k), 3 moments (k), 4 longitudinal turn tail, 5 the map + moments
  * pass of the turn graph (section k), 6 the surrogate field kick (k, after
- * cg_set_surrogate). The beam state is advanced by these launches. */
+ * cg_set_surrogate), 7 the map + moments pass with the ion kick inside, 8 and
+ * 9 the passes 5 and 7 streamed through shared memory by bulk copies
+ * (persistent grid).  The beam state is advanced by these launches. */
 int cg_time_stage(cg_handle* h, int stage, int k, int reps, double* ms);
 /* FP64 FMA throughput of this device measured by a register-resident FMA
  * chain kernel, in FLOP/s (2 per FMA). */
