@@ -591,7 +591,7 @@ int cg_set_beam(cg_handle* H, int M, const int* n_macro, const int* harm, const 
     IonWalk& w = d.iw;
     const size_t NM = (size_t)h.cfg.ion.macro_ions_per_ip, P = (size_t)h.P;
     w.tcap = (int64_t)h.ion_cap + (int64_t)M * (int64_t)NM;
-    w.grid = ion_walk_grid(w.tcap, 16);  // the most walk CTAs of any shape
+    w.grid = ion_walk_grid(w.tcap, 8);  // the most walk CTAs of any shape
     if (dalloc(&w.births, P * M * NM * 2) || dalloc(&w.prep, (size_t)M) ||
         dalloc(&w.bunch, 3 * (size_t)M) || dalloc(&w.spec, P * M * 2) || dalloc(&w.bound, 2) ||
         dalloc(&w.part, P * M * (size_t)w.grid * 5) || dalloc(&w.traj, P * 4 * (size_t)w.tcap) ||
@@ -1293,8 +1293,8 @@ int cg_set_pipeline(cg_handle* H, int groups, int walk_ions) {
   if (groups < 1 || groups > kMaxPipeGroups)
     return fail(&h, CG_ERR_INVALID, "pipeline groups must be 1 .. 16");
   if (walk_ions == 0) walk_ions = h.walk_ions;
-  if (walk_ions != 16 && walk_ions != 32 && walk_ions != 64)
-    return fail(&h, CG_ERR_INVALID, "walk_ions must be 16, 32 or 64 (0: keep)");
+  if (walk_ions != 8 && walk_ions != 16 && walk_ions != 32 && walk_ions != 64)
+    return fail(&h, CG_ERR_INVALID, "walk_ions must be 8, 16, 32 or 64 (0: keep)");
   if ((h.pipe_groups != groups || h.walk_ions != walk_ions) && h.turn_graph) {
     cudaGraphExecDestroy(h.turn_graph);
     h.turn_graph = nullptr;

@@ -136,8 +136,9 @@ struct Handle {
   // records, kicks and maps of a segment run on `side` while the next segment
   // walks
   int pipe_groups = 4;
-  // trajectories per walk CTA (16, 32, 64): a smaller CTA finds room on an
-  // SM sooner while the kicks and maps of earlier segments fill the GPU
+  // trajectories per walk CTA (8, 16, 32, 64): smaller CTAs spread the
+  // walk's FP64 work over more SMs and find room sooner while the kicks and
+  // maps of earlier segments fill the GPU
   int walk_ions = 64;
   cudaStream_t side = nullptr;   // records and kicks of the segments
   cudaStream_t side2 = nullptr;  // maps of the segments (kick g + 1 overlaps map g)

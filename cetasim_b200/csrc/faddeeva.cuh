@@ -246,7 +246,10 @@ CG_HD cplx weideman_half(double x, double y, double L, const double* a, bool upp
   cplx s1 = cmuladd(r[2], r[3], Z4);  // Z^8 .. Z^15 (over Z^8)
   cplx t = cmuladd(s0, s1, Z8);       // Z^0 .. Z^15
   cplx p = cmuladd(t, r[4], Z16);     // + Z^16 .. Z^19
-  if (upper) p = cmul(p, cmul(Z16, Z4));
+  // the upper half times Z^20, the lower times 1 (exact): no divergence
+  // between the two lanes of a w(z)
+  const cplx Z20 = cmul(Z16, Z4);
+  p = cmul(p, upper ? Z20 : cplx{1.0, 0.0});
   *rden = {den.re * inv, -den.im * inv};
   return p;
 }

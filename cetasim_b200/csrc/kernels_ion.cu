@@ -38,7 +38,7 @@ namespace cg {
 
 #define FULL_MASK 0xffffffffu
 
-// The walk's CTA shape: IONS trajectories per block (16, 32 or 64), four
+// The walk's CTA shape: IONS trajectories per block (8, 16, 32 or 64), four
 // lanes per ion; per step the block's ions are summed in groups of 4 (in
 // trajectory order), then the groups in order.
 constexpr int kWin = 16;                       // steps per shared-memory window
@@ -55,7 +55,8 @@ __device__ __forceinline__ void warp_max2(double& a, double& b) {
   }
 }
 
-// Loss bounds, births and per-bunch constants for one IP.
+// Loss bounds, births and per-bunch constants for one IP: block 0 also takes
+// the loss bounds; one warp per (species, bunch) the rest.
 __global__ void __launch_bounds__(kPrepThreads) k_ion_prep(ChainParams cp, ChainSection cs,
                                                          const BunchDev* __restrict__ bunch,
                                                          const BunchMomDev* __restrict__ mom,
@@ -87,19 +88,22 @@ __global__ void __launch_bounds__(kPrepThreads) k_ion_prep(ChainParams cp, Chain
       w.bound[1] = cs.aperture_y > lby ? lby : cs.aperture_y;
     }
   }
-  const int j = blockIdx.x * kPrepThreads + tid;
-  if (j >= M) return;
+  // one warp per (species, bunch): w = p * M + j
+  const int lane = tid & 31;
+  const int wid = (int)(blockIdx.x * (kPrepThreads / 32)) + (tid >> 5);
+  if (wid >= M * P) return;
+  const int j = wid % M, p = wid / M;
   const double mx = mom[j].mean[0], my = mom[j].mean[2];
   const double sx = mom[j].rms_x, sy = mom[j].rms_y;
   const double ne = bunch[j].ne;
-  w.prep[j] = field_prep(sx, sy);
-  w.bunch[3 * j + 0] = mx;
-  w.bunch[3 * j + 1] = my;
-  // drift time to the next bunch: gap * C/h / c (LIP.cpp:1172-1173)
-  w.bunch[3 * j + 2] = cp.circ_ring / cp.harmonics * bunch[j].gap / kCLight;
-  const uint32_t turn = (uint32_t)(*d_turn);
-  const uint32_t k0 = (uint32_t)cp.seed, k1 = (uint32_t)(cp.seed >> 32) ^ kStreamIonBirth;
-  for (int p = 0; p < P; ++p) {
+  if (p == 0 && lane == 0) {
+    w.prep[j] = field_prep(sx, sy);
+    w.bunch[3 * j + 0] = mx;
+    w.bunch[3 * j + 1] = my;
+    // drift time to the next bunch: gap * C/h / c (LIP.cpp:1172-1173)
+    w.bunch[3 * j + 2] = cp.circ_ring / cp.harmonics * bunch[j].gap / kCLight;
+  }
+  if (lane == 0) {
     // LIP::GetIonNumberPerInterAction (LIP.cpp:974-982) and the macro-ion
     // charge of IonGenerator (LIP.cpp:985-995)
     const double press_p = cp.gas_percent[p] * cs.pressure;
@@ -109,27 +113,35 @@ __global__ void __launch_bounds__(kPrepThreads) k_ion_prep(ChainParams cp, Chain
     // ion-side coefficient 2 N_e r_e (m_e / m_ion A) c (MPBunch.cpp:1117)
     w.spec[2 * ((size_t)p * M + j) + 1] =
         2.0 * ne * kElecClassicRadius * kElectronMassEV / kIonMassEV / cp.mass_number[p] * kCLight;
-    // births: Gaussian around the bunch centroid with the bunch sizes,
-    // rejected beyond r^2 > 4 (LIP.cpp:1000-1016); attempt a of bunch j, IP k,
-    // species p draws Philox({a, j, turn, 8k + p})
-    double* out = w.births + 2 * ((size_t)p * M + j) * NM;
-    int got = 0;
-    for (uint32_t a = 0; got < NM; ++a) {
-      if (a >= (1u << 20)) {  // a degenerate bunch size would reject forever
-        atomicOr(status, kStatusIonBirth);
-        for (; got < NM; ++got) out[2 * got] = out[2 * got + 1] = 0.0;
-        break;
-      }
-      u32x4 ctr = {{a, (uint32_t)j, turn, (uint32_t)(k * CG_MAX_SPECIES + p)}};
-      double g0, g1;
-      normal2(philox4x32_10(ctr, k0, k1), &g0, &g1);
-      const double tx = mx + sx * g0, ty = my + sy * g1;
-      const double ax = (tx - mx) / sx, ay = (ty - my) / sy;
-      if (ax * ax + ay * ay > 4.E0) continue;
-      out[2 * got] = tx;
-      out[2 * got + 1] = ty;
-      got++;
+  }
+  // births: Gaussian around the bunch centroid with the bunch sizes,
+  // rejected beyond r^2 > 4 (LIP.cpp:1000-1016); attempt a of bunch j, IP k,
+  // species p draws Philox({a, j, turn, 8k + p}).  The warp tries 32
+  // attempts at once and keeps the accepted ones in attempt order, which are
+  // the births the sequential loop makes.
+  const uint32_t turn = (uint32_t)(*d_turn);
+  const uint32_t k0 = (uint32_t)cp.seed, k1 = (uint32_t)(cp.seed >> 32) ^ kStreamIonBirth;
+  double* out = w.births + 2 * ((size_t)p * M + j) * NM;
+  int got = 0;
+  for (uint32_t a0 = 0; got < NM; a0 += 32) {
+    if (a0 >= (1u << 20)) {  // a degenerate bunch size would reject forever
+      if (lane == 0) atomicOr(status, kStatusIonBirth);
+      for (int q = got + lane; q < NM; q += 32) out[2 * q] = out[2 * q + 1] = 0.0;
+      break;
     }
+    u32x4 ctr = {{a0 + (uint32_t)lane, (uint32_t)j, turn, (uint32_t)(k * CG_MAX_SPECIES + p)}};
+    double g0, g1;
+    normal2(philox4x32_10(ctr, k0, k1), &g0, &g1);
+    const double tx = mx + sx * g0, ty = my + sy * g1;
+    const double ax = (tx - mx) / sx, ay = (ty - my) / sy;
+    const bool ok = !(ax * ax + ay * ay > 4.E0);
+    const unsigned acc = __ballot_sync(FULL_MASK, ok);
+    const int slot = got + __popc(acc & ((1u << lane) - 1u));
+    if (ok && slot < NM) {
+      out[2 * slot] = tx;
+      out[2 * slot + 1] = ty;
+    }
+    got += __popc(acc);
   }
 }
 
@@ -239,7 +251,10 @@ __global__ void __launch_bounds__(4 * IONS, 1) k_ion_walk(ChainParams cp, IonWal
           // lanes 0, 1 of the quad: w(z1); lanes 2, 3: w(z2), which also
           // evaluate the Gaussian factor alongside the series
           const double zr = second ? z2r : z1r, zi = second ? z2i : z1i;
-          const double g = (active && second && fp.mode != 2) ? field_gauss(fp, dx, dy) : 0.0;
+          // every lane evaluates the factor (a per-lane branch would make the
+          // series lanes wait for the exp); lanes 2, 3 keep it
+          const double gall = field_gauss(fp, dx, dy);
+          const double g = (active && second && fp.mode != 2) ? gall : 0.0;
           cplx wv;
           if (__all_sync(FULL_MASK, fp.mode == 2 || fma(zr, zr, zi * zi) < 900.0)) {
             // each w(z) over two lanes: lower and upper halves of the series
@@ -466,7 +481,8 @@ static ChainSection chain_section(const Handle& h, int k) {
 }
 
 cudaError_t launch_ion_prep(Handle& h, int k) {
-  k_ion_prep<<<(h.M + kPrepThreads - 1) / kPrepThreads, kPrepThreads, 0, h.stream>>>(
+  constexpr int kWarps = kPrepThreads / 32;
+  k_ion_prep<<<(h.M * h.P + kWarps - 1) / kWarps, kPrepThreads, 0, h.stream>>>(
       h.chain, chain_section(h, k), h.d.bunch, h.d.mom, h.d.iw, h.d.status, h.d.turn, k);
   return cudaGetLastError();
 }
@@ -476,7 +492,8 @@ cudaError_t launch_ion_walk(Handle& h, int k, int ja, int jb, cudaStream_t s) {
   const dim3 grid(ion_walk_grid(h.d.iw.tcap, ions), h.P);
   const CloudDev* cl = h.d.clouds + (size_t)k * h.P;
   const CloudState* cs = h.d.cloud_state + (size_t)k * h.P;
-  if (ions == 16) k_ion_walk<16><<<grid, 64, 0, s>>>(h.chain, h.d.iw, cl, cs, ja, jb);
+  if (ions == 8) k_ion_walk<8><<<grid, 32, 0, s>>>(h.chain, h.d.iw, cl, cs, ja, jb);
+  else if (ions == 16) k_ion_walk<16><<<grid, 64, 0, s>>>(h.chain, h.d.iw, cl, cs, ja, jb);
   else if (ions == 32) k_ion_walk<32><<<grid, 128, 0, s>>>(h.chain, h.d.iw, cl, cs, ja, jb);
   else k_ion_walk<64><<<grid, 256, 0, s>>>(h.chain, h.d.iw, cl, cs, ja, jb);
   return cudaGetLastError();

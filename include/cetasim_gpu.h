@@ -351,9 +351,9 @@ int cg_autotune(cg_handle* h, int k, int reps, int* choice, double* ms);
 /* Pipelined turn: the ion walk of each IP runs in `groups` segments of
  * bunches, and the records, kicks and maps of a segment run alongside the next
  * segment's walk (1 = one segment, no overlap; default 4; at most 16); results
- * do not depend on `groups`.  walk_ions: trajectories per walk CTA, 16, 32 or
- * 64 (0 keeps the current shape); the shape sets the summation order of the
- * cloud moments, so results agree to rounding across shapes. */
+ * do not depend on `groups`.  walk_ions: trajectories per walk CTA, 8, 16, 32
+ * or 64 (0 keeps the current shape); the shape sets the summation order of
+ * the cloud moments, so results agree to rounding across shapes. */
 int cg_set_pipeline(cg_handle* h, int groups, int walk_ions);
 
 /* Times whole turns (turn0 to warm up the turn graph, then `reps` turns, CUDA

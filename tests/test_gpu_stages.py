@@ -311,11 +311,12 @@ def test_pipeline_autotuner_restores_the_beam_and_shapes_agree():
     for p, q in zip(before[1], after[1]):
         assert np.array_equal(p, q)
     runs = []
-    for ions in (16, 64):
+    for ions in (64, 16, 8):
         h, _ = pair(wl, parts)
         h.set_pipeline(3, ions)
         h.Run(0, 4)
         runs.append([h.download(j)[0] for j in range(wl.n_bunches)])
-    worst = max(np.max(np.abs(a - b) / (np.abs(b).max(axis=1, keepdims=True) + 1e-300))
-                for a, b in zip(*runs))
-    assert worst <= 1e-12
+    for other in runs[1:]:
+        worst = max(np.max(np.abs(a - b) / (np.abs(b).max(axis=1, keepdims=True) + 1e-300))
+                    for a, b in zip(other, runs[0]))
+        assert worst <= 1e-12
