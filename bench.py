@@ -362,9 +362,12 @@ def main():
 
 
 # FP64 operations of one electron-side kick (two w(z) through the Weideman
-# series, the exp of the Gaussian factor counted as one operation, and the
-# field algebra), counted from be_field.cuh / faddeeva.cuh: 2 x 307 + 32.
-FLOPS_PER_KICK = 646
+# series evaluated by Knuth's real recurrence, the exp of the Gaussian factor
+# counted as one operation, and the field algebra), counted from
+# be_field.cuh / faddeeva.cuh: per w(z) 3 (branch test) + 24 (Z and the Newton
+# reciprocal) + 4 (r, s) + 150 (38 recurrence steps) + 5 (p) + 20 (w from p);
+# 2 x 203 + 32.
+FLOPS_PER_KICK = 438
 
 
 def surrogate_leg(args, beam, lib, stream, flush, exact_kick_ms, exact_turn_ms):
