@@ -157,6 +157,7 @@ SectionDev make_section_dev(const cg_section& s, const cg_ring& r) {
   std::memcpy(d.b1h1, s.map_b1h1, sizeof d.b1h1);
   std::memcpy(d.h1b1, s.map_h1b1, sizeof d.h1b1);
   std::memcpy(d.h2b2, s.map_h2b2, sizeof d.h2b2);
+  d.twiss_form = fits_twiss_form(d.b1h1) && fits_twiss_form(d.h1b1) && fits_twiss_form(d.h2b2);
   return d;
 }
 
