@@ -344,9 +344,9 @@ def main():
                                     "128 thr x6/SM"],
                          "pipeline": None if pipe is None else {
                              "segments": pipe[0][0], "walk_ions": pipe[0][1],
-                             "turn_ms": {f"{g}x{w}": round(float(m), 4) for (g, w), m in zip(
-                                 [(1, 64), (2, 64), (3, 64), (4, 64), (6, 64),
-                                  (1, 16), (2, 16), (3, 16), (4, 16), (6, 16)], pipe[1])}}},
+                             "ramp": bool(pipe[0][2]),
+                             "turn_ms": {f"{g}x{w}{'r' if r else ''}": round(float(m), 4)
+                                         for (g, w, r), m in zip(_abi.PIPE_SHAPES, pipe[1])}}},
             "surrogate": sur,
             "e2e": {"value": e2e_value, "unit": "macroparticle-turns/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},

@@ -98,6 +98,19 @@ PF = C.POINTER(C.c_float)
 PU8 = C.POINTER(C.c_uint8)
 PI = C.POINTER(C.c_int)
 
+class TraceRecord(C.Structure):
+    _fields_ = [("kind", C.c_int), ("stream", C.c_int), ("ip", C.c_int), ("segment", C.c_int),
+                ("t_end_us", C.c_double)]
+
+
+PIPE_SHAPES = [(1, 64, 0), (1, 16, 0), (2, 64, 0), (2, 64, 1), (3, 64, 0), (3, 64, 1),
+               (4, 64, 0), (4, 64, 1), (3, 16, 1), (6, 64, 1)]
+
+TRACE_KINDS = ["start", "moments", "ion_prep", "ion_walk", "ion_records", "ion_compact",
+               "ion_chain", "ion_kick", "map_pass", "exchange", "lr_wake", "long", "sr_wake",
+               "fir", "mark_lost"]
+
+
 class SurTrainParams(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("n_train", C.c_int64), ("n_holdout", C.c_int64),
                 ("epochs", C.c_int), ("batch", C.c_int), ("lr", C.c_double)]
@@ -148,8 +161,9 @@ EXPORTS = [
     ("cg_faddeeva_w_q1", I, [PD, PD, PD, PD, C.c_int64]),
     ("cg_gaussian_field", I, [PD, PD, PD, PD, PD, PD, C.c_int64]),
     ("cg_kick_variants", I, [PI]),
-    ("cg_set_pipeline", I, [C.c_void_p, I, I]),
-    ("cg_autotune_pipeline", I, [C.c_void_p, I, I, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p]),
+    ("cg_set_pipeline", I, [C.c_void_p, I, I, I]),
+    ("cg_trace_turn", I, [C.c_void_p, I, C.c_void_p, I, C.POINTER(C.c_int)]),
+    ("cg_autotune_pipeline", I, [C.c_void_p, I, I, C.c_void_p, C.c_void_p]),
     ("cg_set_kick_variant", I, [C.c_void_p, I]),
     ("cg_autotune", I, [C.c_void_p, I, I, PI, PD]),
     ("cg_shard_plan", I, [PI, I, I, PI, PI]),

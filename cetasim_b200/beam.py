@@ -145,17 +145,26 @@ class MPBeam:
     def set_kick_variant(self, v: int):
         self._check(self.lib.cg_set_kick_variant(self.h, v))
 
-    def set_pipeline(self, groups: int, walk_ions: int = 0):
-        self._check(self.lib.cg_set_pipeline(self.h, groups, walk_ions))
+    def set_pipeline(self, groups: int, walk_ions: int = 0, ramp: bool = False):
+        self._check(self.lib.cg_set_pipeline(self.h, groups, walk_ions, int(ramp)))
+
+    def trace_turn(self, turn0: int, cap: int = 4096):
+        """One turn as direct launches with a timing event after each: a list
+        of (kind, stream, ip, segment, t_end_us) in launch order."""
+        recs = (_abi.TraceRecord * cap)()
+        n = C.c_int()
+        self._check(self.lib.cg_trace_turn(self.h, turn0, recs, cap, C.byref(n)))
+        return [(_abi.TRACE_KINDS[r.kind], r.stream, r.ip, r.segment, r.t_end_us)
+                for r in recs[:n.value]]
 
     def autotune_pipeline(self, turn0: int, reps: int = 5):
         """Times whole turns with each pipeline shape, restores the beam and
-        keeps the fastest; returns ((groups, walk_ions), ms per shape)."""
-        ms = np.zeros(10)
-        g, w = C.c_int(), C.c_int()
-        self._check(self.lib.cg_autotune_pipeline(self.h, turn0, reps, C.byref(g), C.byref(w),
-                                                  _abi.ptr(ms)))
-        return (g.value, w.value), ms
+        keeps the fastest; returns ((groups, walk_ions, ramp), ms per shape
+        in the order of _abi.PIPE_SHAPES)."""
+        ms = np.zeros(len(_abi.PIPE_SHAPES))
+        shape = (C.c_int * 3)()
+        self._check(self.lib.cg_autotune_pipeline(self.h, turn0, reps, shape, _abi.ptr(ms)))
+        return tuple(shape), ms
 
     # -- checkpoint / resume ------------------------------------------------------
     def checkpoint(self) -> bytes:

@@ -476,7 +476,7 @@ int cg_destroy(cg_handle* H) {
   if (h.stream) cudaStreamDestroy(h.stream);
   if (h.side) cudaStreamDestroy(h.side);
   if (h.side2) cudaStreamDestroy(h.side2);
-  for (auto* evs : {&h.pipe_ev, &h.kick_ev})
+  for (auto* evs : {&h.pipe_ev, &h.kick_ev, &h.trace_ev})
     for (auto ev : *evs)
       if (ev) cudaEventDestroy(ev);
   delete H;
@@ -823,6 +823,38 @@ int cg_mark_lost(cg_handle* H, double* trans) {
   return st;
 }
 
+// First bunch of walk segment g of G (g = G: M).  Uniform segments, or with
+// pipe_ramp the last segment half as long as the others: what follows the
+// end of the walk (the last segment's records, kick and map) is shorter.
+static int seg_begin(const Handle& h, int g, int G) {
+  if (g <= 0) return 0;
+  if (g >= G) return h.M;
+  if (!h.pipe_ramp) return (int)((int64_t)h.M * g / G);
+  return (int)((int64_t)h.M * 2 * g / (2 * G - 1));
+}
+
+// Turn trace (cg_trace_turn): when h.trace is set, a timing event is recorded
+// on the launching stream after every launch of the turn.
+static cudaError_t trace_mark(Handle& h, cudaStream_t s, int kind, int ip, int seg) {
+  if (!h.trace) return cudaSuccess;
+  const size_t i = h.trace->size();
+  if (i >= h.trace_ev.size()) {
+    cudaEvent_t ev;
+    cudaError_t e = cudaEventCreate(&ev);
+    if (e != cudaSuccess) return e;
+    h.trace_ev.push_back(ev);
+  }
+  TraceMark m;
+  m.kind = kind;
+  m.stream = s == h.side ? 1 : s == h.side2 ? 2 : 0;
+  m.ip = ip;
+  m.seg = seg;
+  h.trace->push_back(m);
+  return cudaEventRecord(h.trace_ev[i], s);
+}
+#define TRACE(s, kind, ip, seg) \
+  if ((e = trace_mark(h, s, kind, ip, seg))) return e
+
 // One turn of MPBeam::Run (MPBeam.cpp:1010-1102) as a kernel sequence on
 // h.stream.  The turn-start and post-map moment calls whose results no stage
 // reads are skipped (the per-turn output writer is not part of this path).
@@ -833,7 +865,11 @@ static cudaError_t enqueue_turn(Handle& h) {
   // and the moments the next stage reads (those of IP k+1 for its ion chain;
   // after the last IP those of section K-1 for the wakes, MPBeam.cpp:1069)
   const bool post = c.flag_lr_wake || c.flag_sr_wake;
-  if (c.flag_beam_ion && ((e = launch_moments(h, 0)) || (e = exchange_moments(h)))) return e;
+  TRACE(h.stream, CG_TRACE_START, -1, -1);
+  if (c.flag_beam_ion) {
+    if ((e = launch_moments(h, 0)) || (e = exchange_moments(h))) return e;
+    TRACE(h.stream, CG_TRACE_MOMENTS, 0, -1);
+  }
   const int G = std::max(1, std::min(h.pipe_groups, h.M));
   for (int k = 0; k < h.K; ++k) {
     const bool fused = c.flag_beam_ion && !h.d.sur_w && h.fuse_kick;
@@ -846,26 +882,33 @@ static cudaError_t enqueue_turn(Handle& h) {
       // the next IP's moments) on `side2`, so that the walk of segment g + 1,
       // the kick of g + 1 and the map of g run at the same time
       if ((e = launch_ion_prep(h, k))) return e;
+      TRACE(h.stream, CG_TRACE_ION_PREP, k, -1);
       for (int g = 0; g < G; ++g) {
-        const int ja = (int)((int64_t)h.M * g / G), jb = (int)((int64_t)h.M * (g + 1) / G);
+        const int ja = seg_begin(h, g, G), jb = seg_begin(h, g + 1, G);
         if ((e = launch_ion_walk(h, k, ja, jb, h.stream))) return e;
+        TRACE(h.stream, CG_TRACE_ION_WALK, k, g);
         if ((e = cudaEventRecord(h.pipe_ev[g], h.stream))) return e;
         if ((e = cudaStreamWaitEvent(h.side, h.pipe_ev[g], 0))) return e;
         if ((e = launch_ion_records(h, k, ja, jb, h.side))) return e;
+        TRACE(h.side, CG_TRACE_ION_RECORDS, k, g);
         const int ta = h.tile_off[ja], tb = h.tile_off[jb];
         const int ca = h.chunk_off[ja], cb = h.chunk_off[jb];
         if (fused) {
           if ((e = launch_map_pass(h, k, mom, true, ca, cb, h.side))) return e;
+          TRACE(h.side, CG_TRACE_MAP_PASS, k, g);
           continue;
         }
         e = h.d.sur_w ? launch_ion_kick_sur(h, k, ta, tb, h.side)
                       : launch_ion_kick_variant(h, k, h.kick_variant, ta, tb, h.side);
         if (e) return e;
+        TRACE(h.side, CG_TRACE_ION_KICK, k, g);
         if ((e = cudaEventRecord(h.kick_ev[g], h.side))) return e;
         if ((e = cudaStreamWaitEvent(h.side2, h.kick_ev[g], 0))) return e;
         if ((e = launch_map_pass(h, k, mom, false, ca, cb, h.side2))) return e;
+        TRACE(h.side2, CG_TRACE_MAP_PASS, k, g);
       }
       if ((e = launch_ion_compact(h, k, h.side))) return e;
+      TRACE(h.side, CG_TRACE_ION_COMPACT, k, -1);
       if ((e = cudaEventRecord(h.pipe_ev[kMaxPipeGroups], h.side))) return e;
       if ((e = cudaStreamWaitEvent(h.stream, h.pipe_ev[kMaxPipeGroups], 0))) return e;
       if (!fused) {
@@ -875,27 +918,45 @@ static cudaError_t enqueue_turn(Handle& h) {
     } else {
       if (c.flag_beam_ion) {
         if ((e = launch_ion_chain(h, k))) return e;
-        if (!fused && (e = h.d.sur_w ? launch_ion_kick_sur(h, k) : launch_ion_kick(h, k)))
-          return e;
+        TRACE(h.stream, CG_TRACE_ION_CHAIN, k, -1);
+        if (!fused) {
+          if ((e = h.d.sur_w ? launch_ion_kick_sur(h, k) : launch_ion_kick(h, k))) return e;
+          TRACE(h.stream, CG_TRACE_ION_KICK, k, -1);
+        }
       }
       if ((e = launch_map_pass(h, k, mom, fused))) return e;
+      TRACE(h.stream, CG_TRACE_MAP_PASS, k, -1);
     }
-    if (mom >= 0 && (e = exchange_moments(h))) return e;
+    if (mom >= 0) {
+      if ((e = exchange_moments(h))) return e;
+      if (h.sh_world > 1) TRACE(h.stream, CG_TRACE_EXCHANGE, k, -1);
+    }
   }
-  if (c.flag_lr_wake && (e = launch_lr_compute(h))) return e;
+  if (c.flag_lr_wake) {
+    if ((e = launch_lr_compute(h))) return e;
+    TRACE(h.stream, CG_TRACE_LR_WAKE, -1, -1);
+  }
   unsigned fl = kLongRF | kLongDrift | kLongLoss;
   if (c.flag_synrad) fl |= kLongSynrad;
   if (c.flag_lr_wake) fl |= kLongLR;
   if ((e = launch_long(h, fl))) return e;
-  if (c.flag_sr_wake && (e = launch_sr_wake(h))) return e;
+  TRACE(h.stream, CG_TRACE_LONG, -1, -1);
+  if (c.flag_sr_wake) {
+    if ((e = launch_sr_wake(h))) return e;
+    TRACE(h.stream, CG_TRACE_SR_WAKE, -1, -1);
+  }
   if (c.flag_fir) {
     if ((e = launch_moments(h, 0))) return e;
     if ((e = exchange_moments(h))) return e;
     if ((e = launch_fir_compute(h))) return e;
+    TRACE(h.stream, CG_TRACE_FIR, -1, -1);
   }
   if ((e = launch_mark_lost(h, c.flag_fir != 0, true))) return e;
-  return launch_turn_advance(h);
+  if ((e = launch_turn_advance(h))) return e;
+  TRACE(h.stream, CG_TRACE_MARK_LOST, -1, -1);
+  return cudaSuccess;
 }
+#undef TRACE
 
 int cg_run_turns(cg_handle* H, int turn0, int n_turns) {
   STAGE_PROLOGUE
@@ -931,7 +992,32 @@ int cg_run_turns(cg_handle* H, int turn0, int n_turns) {
   return check_status(h);
 }
 
-// ---- measurement and host memory ----
+int cg_trace_turn(cg_handle* H, int turn0, cg_trace_record* out, int cap, int* n) {
+  STAGE_PROLOGUE
+  if (!out || !n || cap < 1) return fail(&h, CG_ERR_INVALID, "bad arguments");
+  int st = set_turn(h, turn0);
+  if (st) return st;
+  std::vector<TraceMark> marks;
+  h.trace = &marks;
+  cudaError_t e = enqueue_turn(h);
+  h.trace = nullptr;
+  if (e != cudaSuccess) return cuda_fail(&h, e, "traced turn");
+  CG_CUDA(&h, cudaStreamSynchronize(h.stream));
+  if ((int)marks.size() > cap) return fail(&h, CG_ERR_INVALID, "trace buffer too small");
+  for (size_t i = 0; i < marks.size(); ++i) {
+    float t = 0;
+    CG_CUDA(&h, cudaEventElapsedTime(&t, h.trace_ev[0], h.trace_ev[i]));
+    out[i].kind = marks[i].kind;
+    out[i].stream = marks[i].stream;
+    out[i].ip = marks[i].ip;
+    out[i].segment = marks[i].seg;
+    out[i].t_end_us = 1e3 * (double)t;
+  }
+  *n = (int)marks.size();
+  return check_status(h);
+}
+
+// ---- measurement and host memory ----// ---- measurement and host memory ----
 
 void* cg_host_alloc(size_t bytes) {
   void* p = nullptr;
@@ -1288,7 +1374,7 @@ int cg_autotune(cg_handle* H, int k, int reps, int* choice, double* ms) {
   return st;
 }
 
-int cg_set_pipeline(cg_handle* H, int groups, int walk_ions) {
+int cg_set_pipeline(cg_handle* H, int groups, int walk_ions, int ramp) {
   if (!H) return CG_ERR_INVALID;
   Handle& h = H->h;
   if (groups < 1 || groups > kMaxPipeGroups)
@@ -1296,12 +1382,15 @@ int cg_set_pipeline(cg_handle* H, int groups, int walk_ions) {
   if (walk_ions == 0) walk_ions = h.walk_ions;
   if (walk_ions != 8 && walk_ions != 16 && walk_ions != 32 && walk_ions != 64)
     return fail(&h, CG_ERR_INVALID, "walk_ions must be 8, 16, 32 or 64 (0: keep)");
-  if ((h.pipe_groups != groups || h.walk_ions != walk_ions) && h.turn_graph) {
+  const bool rp = ramp != 0;
+  if ((h.pipe_groups != groups || h.walk_ions != walk_ions || h.pipe_ramp != rp) &&
+      h.turn_graph) {
     cudaGraphExecDestroy(h.turn_graph);
     h.turn_graph = nullptr;
   }
   h.pipe_groups = groups;
   h.walk_ions = walk_ions;
+  h.pipe_ramp = rp;
   return CG_OK;
 }
 
@@ -1519,12 +1608,13 @@ int cg_checkpoint_load(cg_handle* H, const void* buf, size_t bytes) {
   return CG_OK;
 }
 
-// The pipeline shapes cg_autotune_pipeline tries, in order: (segments, walk ions).
-static const int kPipeShapes[CG_PIPE_SHAPES][2] = {{1, 64}, {2, 64}, {3, 64}, {4, 64}, {6, 64},
-                                                   {1, 16}, {2, 16}, {3, 16}, {4, 16}, {6, 16}};
+// The pipeline shapes cg_autotune_pipeline tries, in order: (segments, walk
+// ions, ramp).
+static const int kPipeShapes[CG_PIPE_SHAPES][3] = {
+    {1, 64, 0}, {1, 16, 0}, {2, 64, 0}, {2, 64, 1}, {3, 64, 0},
+    {3, 64, 1}, {4, 64, 0}, {4, 64, 1}, {3, 16, 1}, {6, 64, 1}};
 
-int cg_autotune_pipeline(cg_handle* H, int turn0, int reps, int* groups, int* walk_ions,
-                         double* ms) {
+int cg_autotune_pipeline(cg_handle* H, int turn0, int reps, int* shape, double* ms) {
   STAGE_PROLOGUE
   if (!h.cfg.flag_beam_ion) return fail(&h, CG_ERR_NOT_READY, "runBeamIonFlag is off");
   if (reps < 1 || turn0 < 0) return fail(&h, CG_ERR_INVALID, "bad arguments");
@@ -1541,7 +1631,8 @@ int cg_autotune_pipeline(cg_handle* H, int turn0, int reps, int* groups, int* wa
   int best = -1;
   double best_ms = 0;
   for (int v = 0; v < CG_PIPE_SHAPES && !st; ++v) {
-    if ((st = cg_set_pipeline(H, kPipeShapes[v][0], kPipeShapes[v][1]))) break;
+    if ((st = cg_set_pipeline(H, kPipeShapes[v][0], kPipeShapes[v][1], kPipeShapes[v][2])))
+      break;
     if ((st = cg_run_turns(H, turn0, 1))) break;  // captures the turn graph
     cudaEventRecord(e0, h.stream);
     if ((st = cg_run_turns(H, turn0 + 1, reps))) break;
@@ -1560,9 +1651,12 @@ int cg_autotune_pipeline(cg_handle* H, int turn0, int reps, int* groups, int* wa
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (st) return st;
-  if (groups) *groups = kPipeShapes[best][0];
-  if (walk_ions) *walk_ions = kPipeShapes[best][1];
-  return cg_set_pipeline(H, kPipeShapes[best][0], kPipeShapes[best][1]);
+  if (shape) {
+    shape[0] = kPipeShapes[best][0];
+    shape[1] = kPipeShapes[best][1];
+    shape[2] = kPipeShapes[best][2];
+  }
+  return cg_set_pipeline(H, kPipeShapes[best][0], kPipeShapes[best][1], kPipeShapes[best][2]);
 }
 
 // ---- field surrogate ----

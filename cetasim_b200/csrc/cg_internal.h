@@ -118,6 +118,10 @@ struct DeviceBufs {
   size_t scratch_bytes = 0;
 };
 
+struct TraceMark {
+  int kind, stream, ip, seg;
+};
+
 struct Handle {
   cg_config cfg;
   std::vector<cg_section> sections;
@@ -140,6 +144,10 @@ struct Handle {
   // walk's FP64 work over more SMs and find room sooner while the kicks and
   // maps of earlier segments fill the GPU
   int walk_ions = 64;
+  bool pipe_ramp = false;  // last walk segment half as long as the others
+  // turn trace (cg_trace_turn): marks and their timing events
+  std::vector<TraceMark>* trace = nullptr;
+  std::vector<cudaEvent_t> trace_ev;
   cudaStream_t side = nullptr;   // records and kicks of the segments
   cudaStream_t side2 = nullptr;  // maps of the segments (kick g + 1 overlaps map g)
   std::vector<cudaEvent_t> pipe_ev;  // kMaxPipeGroups + 1: walked segments, then the join

@@ -349,22 +349,59 @@ int cg_set_kick_variant(cg_handle* h, int v);
 int cg_autotune(cg_handle* h, int k, int reps, int* choice, double* ms);
 
 /* Pipelined turn: the ion walk of each IP runs in `groups` segments of
- * bunches, and the records, kicks and maps of a segment run alongside the next
- * segment's walk (1 = one segment, no overlap; default 4; at most 16); results
- * do not depend on `groups`.  walk_ions: trajectories per walk CTA, 8, 16, 32
- * or 64 (0 keeps the current shape); the shape sets the summation order of
+ * bunches, and the kicks and maps of a walked segment run alongside the next
+ * segment's walk (1 = one segment, no overlap; default 4; at most 16); ramp
+ * != 0 makes the last segment half as long as the others.  Results do not
+ * depend on `groups` or `ramp`.  walk_ions: trajectories per walk CTA, 8, 16,
+ * 32 or 64 (0 keeps the current shape); the shape sets the summation order of
  * the cloud moments, so results agree to rounding across shapes. */
-int cg_set_pipeline(cg_handle* h, int groups, int walk_ions);
+int cg_set_pipeline(cg_handle* h, int groups, int walk_ions, int ramp);
 
 /* Times whole turns (turn0 to warm up the turn graph, then `reps` turns, CUDA
  * events on h's stream) with each of the CG_PIPE_SHAPES pipeline shapes
- * (segments x walk ions: 1, 2, 3, 4, 6 segments with 64, then with 16
- * trajectories per walk CTA), puts the beam and the ion clouds back from a
- * host checkpoint after every trial, and keeps the fastest: *groups,
- * *walk_ions, ms[CG_PIPE_SHAPES] per turn (either may be NULL). */
+ * (segments, walk ions, ramp): (1,64,0) (1,16,0) (2,64,0) (2,64,1) (3,64,0)
+ * (3,64,1) (4,64,0) (4,64,1) (3,16,1) (6,64,1); puts the beam and the ion
+ * clouds back from a host checkpoint after every trial and keeps the
+ * fastest: shape[0..2] (may be NULL), ms[CG_PIPE_SHAPES] per turn (may be
+ * NULL). */
 #define CG_PIPE_SHAPES 10
-int cg_autotune_pipeline(cg_handle* h, int turn0, int reps, int* groups, int* walk_ions,
-                         double* ms);
+int cg_autotune_pipeline(cg_handle* h, int turn0, int reps, int* shape, double* ms);
+
+/* ---- turn trace (no counterpart in the reference) ---- */
+
+/* Launch kinds of a traced turn. */
+enum {
+  CG_TRACE_START = 0,        /* the turn's start on the handle's stream */
+  CG_TRACE_MOMENTS = 1,      /* turn-start moments (and their exchange) */
+  CG_TRACE_ION_PREP = 2,
+  CG_TRACE_ION_WALK = 3,     /* one walk segment */
+  CG_TRACE_ION_RECORDS = 4,  /* the cloud records of one segment */
+  CG_TRACE_ION_COMPACT = 5,
+  CG_TRACE_ION_CHAIN = 6,    /* prep + walk + records + compact, unpipelined */
+  CG_TRACE_ION_KICK = 7,     /* electron-side kick (of one segment, pipelined) */
+  CG_TRACE_MAP_PASS = 8,     /* map + next moments (of one segment, pipelined) */
+  CG_TRACE_EXCHANGE = 9,     /* moment all-gather over the ranks (sharded runs) */
+  CG_TRACE_LR_WAKE = 10,
+  CG_TRACE_LONG = 11,        /* RF, drift, energy loss, synchrotron radiation */
+  CG_TRACE_SR_WAKE = 12,
+  CG_TRACE_FIR = 13,
+  CG_TRACE_MARK_LOST = 14    /* loss marking and the turn counter */
+};
+
+typedef struct {
+  int kind;         /* CG_TRACE_* */
+  int stream;       /* 0 the handle's stream, 1 and 2 the pipelined turn's side streams */
+  int ip;           /* interaction point / section, or -1 */
+  int segment;      /* walk segment of the pipelined turn, or -1 */
+  double t_end_us;  /* completion after the turn's start (CUDA events), microseconds */
+} cg_trace_record;
+
+/* Runs turn `turn0` as direct launches (not the turn graph) with a timing
+ * event after every launch on its stream, and returns the timeline in launch
+ * order: out[0 .. *n - 1] (at most `cap`; CG_ERR_INVALID if the turn has
+ * more).  The turn advances the beam as cg_run_turns(h, turn0, 1) does; the
+ * events add a little time to each launch. */
+int cg_trace_turn(cg_handle* h, int turn0, cg_trace_record* out, int cap, int* n);
 
 /* ---- bunch-sharded runs over several GPUs (no counterpart in the reference,
  * which is single-threaded) ---- */

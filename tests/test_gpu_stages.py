@@ -238,8 +238,8 @@ def test_kick_inside_the_map_pass_repeats_the_separate_kernels():
     assert worst <= 1e-14
 
 
-@pytest.mark.parametrize("groups", [3, 4, 16])
-def test_pipelined_turn_repeats_the_unpipelined_turn(groups):
+@pytest.mark.parametrize("groups,ramp", [(3, False), (4, True), (16, False), (2, True)])
+def test_pipelined_turn_repeats_the_unpipelined_turn(groups, ramp):
     """The ion walk in segments with records, kicks and maps overlapping the
     next segment gives the same turn bit for bit."""
     wl = small("fast_ion", 0.01, bunch_current=TRAPPED)
@@ -247,7 +247,7 @@ def test_pipelined_turn_repeats_the_unpipelined_turn(groups):
     runs = []
     for gcount in (1, groups):
         g, _ = pair(wl, parts)
-        g.set_pipeline(gcount)
+        g.set_pipeline(gcount, 0, ramp)
         g.Run(0, 4)
         runs.append(([g.download(j) for j in range(wl.n_bunches)],
                      [g.ions(k) for k in (0, wl.cfg.n_sections - 1)],
@@ -301,9 +301,9 @@ def test_pipeline_autotuner_restores_the_beam_and_shapes_agree():
     g, _ = pair(wl, parts)
     g.Run(0, 2)
     before = ([g.download(j) for j in range(wl.n_bunches)], g.ions(0))
-    (groups, ions), ms = g.autotune_pipeline(2, reps=1)
-    assert (groups, ions) in [(1, 64), (2, 64), (3, 64), (4, 64), (6, 64),
-                              (1, 16), (2, 16), (3, 16), (4, 16), (6, 16)]
+    from cetasim_b200 import _abi
+    shape, ms = g.autotune_pipeline(2, reps=1)
+    assert shape in _abi.PIPE_SHAPES
     assert np.all(ms > 0)
     after = ([g.download(j) for j in range(wl.n_bunches)], g.ions(0))
     for (a, s), (b, t) in zip(before[0], after[0]):
@@ -320,3 +320,29 @@ def test_pipeline_autotuner_restores_the_beam_and_shapes_agree():
         worst = max(np.max(np.abs(a - b) / (np.abs(b).max(axis=1, keepdims=True) + 1e-300))
                     for a, b in zip(other, runs[0]))
         assert worst <= 1e-12
+
+
+@pytest.mark.parametrize("groups", [1, 3])
+def test_traced_turn_equals_the_graph_turn(groups):
+    """cg_trace_turn runs the turn's launches directly with timing events: the
+    same beam as the turn graph, and a timeline that grows on every stream."""
+    wl = small("fast_ion", 0.01, bunch_current=TRAPPED)
+    parts = particles(wl, seed=17)
+    a, _ = pair(wl, parts)
+    b, _ = pair(wl, parts)
+    for g in (a, b):
+        g.set_pipeline(groups, 64)
+    a.Run(0, 2)
+    b.Run(0, 1)
+    tr = b.trace_turn(1)
+    for j in range(wl.n_bunches):
+        (x, s), (y, t) = a.download(j), b.download(j)
+        assert np.array_equal(x, y) and np.array_equal(s, t)
+    assert tr[0][0] == "start" and tr[-1][0] == "mark_lost"
+    kinds = {r[0] for r in tr}
+    assert {"ion_kick", "map_pass", "long"} <= kinds
+    assert ("ion_walk" in kinds) == (groups > 1) and ("ion_chain" in kinds) == (groups == 1)
+    for st in (0, 1, 2):
+        ts = [r[4] for r in tr if r[1] == st]
+        assert all(u <= v for u, v in zip(ts, ts[1:]))
+    assert tr[-1][4] >= max(r[4] for r in tr) - 1e-9
