@@ -242,6 +242,10 @@ def main():
         c, _ = beam.download(j)
         arr[:] = c
         hbufs.append((p, arr))
+    table = (C.c_void_p * (6 * wl.n_bunches))()
+    for j, (p, arr) in zip(beam.local, hbufs):
+        for d in range(6):
+            table[6 * j + d] = arr[d].ctypes.data
     mom = (_abi.BunchMoments * wl.n_bunches)()
     e2e_steps = max(3, args.steps // 2)
     barrier()
@@ -250,8 +254,7 @@ def main():
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for j, (p, arr) in zip(beam.local, hbufs):
-            beam._check(lib.cg_upload_bunch(beam.h, j, *[_abi.ptr(arr[d]) for d in range(6)], None))
+        beam._check(lib.cg_upload_beam(beam.h, table, None))
         beam.Run(t_first + args.warmup + args.steps + s, 1)
         beam._check(lib.cg_beam_rms(beam.h, 0))
         beam._check(lib.cg_get_moments(beam.h, mom))

@@ -130,6 +130,7 @@ EXPORTS = [
     ("cg_last_error", C.c_char_p, [C.c_void_p]),
     ("cg_set_beam", I, [C.c_void_p, I, PI, PI, PD]),
     ("cg_upload_bunch", I, [C.c_void_p, I, PD, PD, PD, PD, PD, PD, PU8]),
+    ("cg_upload_beam", I, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("cg_download_bunch", I, [C.c_void_p, I, PD, PD, PD, PD, PD, PD, PU8]),
     ("cg_generate_gaussian", I, [C.c_void_p, D, D, D, D, C.c_uint64]),
     ("cg_beam_rms", I, [C.c_void_p, I]),

@@ -80,6 +80,20 @@ class MPBeam:
         s = None if surv is None else np.ascontiguousarray(surv, dtype=np.uint8)
         self._check(self.lib.cg_upload_bunch(self.h, j, *[_abi.ptr(a) for a in c], _abi.ptr(s)))
 
+    def upload_beam(self, parts, surv=None):
+        """Every local bunch at once (cg_upload_beam): parts[j] = (6, n_j)
+        coordinates, surv[j] survival bytes or None."""
+        keep = [np.ascontiguousarray(parts[j], dtype=np.float64) for j in range(self.wl.n_bunches)]
+        table = (C.c_void_p * (6 * self.wl.n_bunches))()
+        for j, a in enumerate(keep):
+            for d in range(6):
+                table[6 * j + d] = a[d].ctypes.data
+        st = None
+        if surv is not None:
+            sk = [np.ascontiguousarray(x, dtype=np.uint8) for x in surv]
+            st = (C.c_void_p * self.wl.n_bunches)(*[x.ctypes.data for x in sk])
+        self._check(self.lib.cg_upload_beam(self.h, table, st))
+
     def download(self, j: int):
         n = int(self.wl.n_macro[j])
         c = np.empty((6, n))

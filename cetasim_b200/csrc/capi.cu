@@ -636,6 +636,31 @@ int cg_set_beam(cg_handle* H, int M, const int* n_macro, const int* harm, const 
   return CG_OK;
 }
 
+// Enqueues the copies of bunch j's coordinates and survival flags: the six
+// rows in one 2D copy when they are equally spaced in host memory (a (6, n)
+// array), else one copy each.
+static int enqueue_upload(Handle& h, int j, const double* const src[6], const uint8_t* surv) {
+  for (int d = 0; d < 6; ++d)
+    if (!src[d]) return fail(&h, CG_ERR_INVALID, "NULL coordinate array");
+  const int64_t off = (int64_t)h.tile_off[j] * kTile;
+  const size_t n = h.n_macro[j];
+  const ptrdiff_t pitch = src[1] - src[0];
+  bool even = pitch >= (ptrdiff_t)n;
+  for (int d = 2; d < 6 && even; ++d) even = src[d] - src[d - 1] == pitch;
+  if (even && n > 0) {
+    CG_CUDA(&h, cudaMemcpy2DAsync(h.d.c + off, h.npad * sizeof(double), src[0],
+                                  pitch * sizeof(double), n * sizeof(double), 6,
+                                  cudaMemcpyHostToDevice, h.stream));
+  } else {
+    for (int d = 0; d < 6; ++d)
+      CG_CUDA(&h, cudaMemcpyAsync(h.d.c + d * h.npad + off, src[d], n * sizeof(double),
+                                  cudaMemcpyHostToDevice, h.stream));
+  }
+  if (surv) CG_CUDA(&h, cudaMemcpyAsync(h.d.surv + off, surv, n, cudaMemcpyHostToDevice, h.stream));
+  else CG_CUDA(&h, cudaMemsetAsync(h.d.surv + off, 0, n, h.stream));
+  return CG_OK;
+}
+
 int cg_upload_bunch(cg_handle* H, int j, const double* x, const double* px, const double* y,
                     const double* py, const double* z, const double* dp, const uint8_t* surv) {
   if (!H) return CG_ERR_INVALID;
@@ -645,15 +670,22 @@ int cg_upload_bunch(cg_handle* H, int j, const double* x, const double* px, cons
   if (j < h.sh_j0 || j >= h.sh_j1) return fail(&h, CG_ERR_INVALID, "bunch held by another rank");
   cudaSetDevice(h.device);
   const double* src[6] = {x, px, y, py, z, dp};
-  int64_t off = (int64_t)h.tile_off[j] * kTile;
-  size_t n = h.n_macro[j];
-  for (int d = 0; d < 6; ++d) {
-    if (!src[d]) return fail(&h, CG_ERR_INVALID, "NULL coordinate array");
-    CG_CUDA(&h, cudaMemcpyAsync(h.d.c + d * h.npad + off, src[d], n * sizeof(double),
-                                cudaMemcpyHostToDevice, h.stream));
+  int st = enqueue_upload(h, j, src, surv);
+  if (st) return st;
+  CG_CUDA(&h, cudaStreamSynchronize(h.stream));
+  return CG_OK;
+}
+
+int cg_upload_beam(cg_handle* H, const double* const* coords, const uint8_t* const* surv) {
+  if (!H) return CG_ERR_INVALID;
+  Handle& h = H->h;
+  if (!h.beam_set) return fail(&h, CG_ERR_NOT_READY, "cg_set_beam first");
+  if (!coords) return fail(&h, CG_ERR_INVALID, "NULL coordinate table");
+  cudaSetDevice(h.device);
+  for (int j = h.sh_j0; j < h.sh_j1; ++j) {
+    int st = enqueue_upload(h, j, coords + 6 * (size_t)j, surv ? surv[j] : nullptr);
+    if (st) return st;
   }
-  if (surv) CG_CUDA(&h, cudaMemcpyAsync(h.d.surv + off, surv, n, cudaMemcpyHostToDevice, h.stream));
-  else CG_CUDA(&h, cudaMemsetAsync(h.d.surv + off, 0, n, h.stream));
   CG_CUDA(&h, cudaStreamSynchronize(h.stream));
   return CG_OK;
 }

@@ -224,6 +224,13 @@ int cg_set_beam(cg_handle* h, int n_bunches, const int* n_macro,
 int cg_upload_bunch(cg_handle* h, int j, const double* x, const double* px,
                     const double* y, const double* py, const double* z,
                     const double* dp, const uint8_t* surv);
+
+/* Uploads every bunch this handle holds (all of them unless sharded) with one
+ * synchronisation at the end: coords[6 j + d] is coordinate d (x, px, y, py,
+ * z, dp) of bunch j, n_macro[j] doubles; surv[j] its survival bytes (surv or
+ * surv[j] NULL: all alive).  Six equally spaced rows (a (6, n) array) go in
+ * one 2D copy.  Host buffers in pinned memory (cg_host_alloc) copy fastest. */
+int cg_upload_beam(cg_handle* h, const double* const* coords, const uint8_t* const* surv);
 int cg_download_bunch(cg_handle* h, int j, double* x, double* px, double* y,
                       double* py, double* z, double* dp, uint8_t* surv);
 

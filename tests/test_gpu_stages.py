@@ -346,3 +346,41 @@ def test_traced_turn_equals_the_graph_turn(groups):
         ts = [r[4] for r in tr if r[1] == st]
         assert all(u <= v for u, v in zip(ts, ts[1:]))
     assert tr[-1][4] >= max(r[4] for r in tr) - 1e-9
+
+
+def test_upload_beam_matches_per_bunch_uploads():
+    """cg_upload_beam: (6, n) rows in one 2D copy, padded rows (pitch > n) and
+    scattered rows (six separate arrays) give the bunches cg_upload_bunch
+    gives, survival bytes included."""
+    import ctypes as C
+    wl = small("batched_uneven", 0.01)
+    parts = particles(wl, seed=21)
+    rng = np.random.default_rng(22)
+    surv = [(rng.random(len(c[0])) < 0.2).astype(np.uint8) for c in parts]
+    g, _ = pair(wl, parts, surv)
+    want = [g.download(j) for j in range(wl.n_bunches)]
+    h, _ = pair(wl, [np.zeros_like(c) for c in parts])
+    keep = []
+    table = (C.c_void_p * (6 * wl.n_bunches))()
+    for j, c in enumerate(parts):
+        n = c.shape[1]
+        if j % 3 == 0:      # contiguous (6, n)
+            a = np.ascontiguousarray(c)
+            rows = [a[d] for d in range(6)]
+        elif j % 3 == 1:    # padded rows: pitch n + 7
+            big = np.zeros((6, n + 7))
+            big[:, :n] = c
+            a = big
+            rows = [big[d, :n] for d in range(6)]
+        else:               # six separate arrays
+            rows = [np.array(c[d]) for d in range(6)]
+            a = rows
+        keep.append(a)
+        for d in range(6):
+            table[6 * j + d] = rows[d].ctypes.data
+    sv = [np.ascontiguousarray(x) for x in surv]
+    st = (C.c_void_p * wl.n_bunches)(*[x.ctypes.data for x in sv])
+    h._check(h.lib.cg_upload_beam(h.h, table, st))
+    for j in range(wl.n_bunches):
+        (x, s), (y, t) = want[j], h.download(j)
+        assert np.array_equal(x, y) and np.array_equal(s, t)
