@@ -95,7 +95,7 @@ void free_beam(Handle& h) {
   dfree(d.c); dfree(d.surv); dfree(d.tile_bunch); dfree(d.chunk_bunch); dfree(d.bunch);
   dfree(d.partials);
   dfree(d.counters); dfree(d.mom); dfree(d.loss_count); dfree(d.scratch);
-  dfree(d.rec); dfree(d.lr_hist); dfree(d.lr_force); dfree(d.fir_hist); dfree(d.fir_kick);
+  dfree(d.rec); dfree(d.rec_prep); dfree(d.lr_hist); dfree(d.lr_force); dfree(d.fir_hist); dfree(d.fir_kick);
   dfree(d.sr_geom); dfree(d.sr_counts); dfree(d.sr_sumx); dfree(d.sr_sumy); dfree(d.sr_lag);
   dfree(d.sr_pot);
   dfree(d.mom_send); dfree(d.mom_all); dfree(d.sh_off); dfree(d.sh_cnt);
@@ -107,7 +107,7 @@ void free_beam(Handle& h) {
   d.c = nullptr; d.surv = nullptr; d.tile_bunch = nullptr; d.chunk_bunch = nullptr;
   d.bunch = nullptr; d.partials = nullptr;
   d.counters = nullptr; d.mom = nullptr; d.loss_count = nullptr; d.scratch = nullptr;
-  d.rec = nullptr; d.lr_hist = nullptr; d.lr_force = nullptr; d.fir_hist = nullptr;
+  d.rec = nullptr; d.rec_prep = nullptr; d.lr_hist = nullptr; d.lr_force = nullptr; d.fir_hist = nullptr;
   d.fir_kick = nullptr; d.sr_geom = nullptr; d.sr_counts = nullptr; d.sr_sumx = nullptr;
   d.sr_sumy = nullptr; d.sr_lag = nullptr; d.sr_pot = nullptr;
   if (h.turn_graph) {
@@ -583,11 +583,12 @@ int cg_set_beam(cg_handle* H, int M, const int* n_macro, const int* harm, const 
   for (auto& m : m0) m.transmission = 1.0;
   cudaMemcpy(d.mom, m0.data(), sizeof(BunchMomDev) * M, cudaMemcpyHostToDevice);
   if (h.cfg.flag_beam_ion) {
-    if (dalloc(&d.rec, (size_t)h.K * M * h.P)) {
+    if (dalloc(&d.rec, (size_t)h.K * M * h.P) || dalloc(&d.rec_prep, (size_t)h.K * M * h.P)) {
       free_beam(h);
       return fail(&h, CG_ERR_OOM, "ion records");
     }
     cudaMemset(d.rec, 0, sizeof(CloudRec) * h.K * M * h.P);
+    cudaMemset(d.rec_prep, 0, sizeof(FieldPrep) * h.K * M * h.P);
     // ion-chain scratch: trajectories = the cloud's capacity + the births of one walk
     IonWalk& w = d.iw;
     const size_t NM = (size_t)h.cfg.ion.macro_ions_per_ip, P = (size_t)h.P;

@@ -85,6 +85,7 @@ struct DeviceBufs {
   CloudDev* clouds = nullptr;      // K x P (device array of buffer pointers)
   CloudState* cloud_state = nullptr;  // K x P
   CloudRec* rec = nullptr;         // K x M x P
+  FieldPrep* rec_prep = nullptr;   // K x M x P: field constants of each record's Gaussian
   double* ion_totals = nullptr;    // K (charge), used by cg_ion_totals
   IonWalk iw;
   // bunch-sharded runs: moments of the local bunches out, of all bunches in

@@ -389,27 +389,26 @@ __global__ void __launch_bounds__(NT, MINB) k_ion_kick(double* __restrict__ c, i
                                                       const uint8_t* __restrict__ surv,
                                                       const int* __restrict__ tile_bunch,
                                                       const BunchDev* __restrict__ bunch,
-                                                      const CloudRec* __restrict__ rec, int P,
-                                                      int tile_base) {
-  // the field constants of the bunch's records, once per CTA (a tile holds
-  // particles of one bunch)
-  __shared__ FieldPrep s_prep[CG_MAX_SPECIES];
+                                                      const CloudRec* __restrict__ rec,
+                                                      const FieldPrep* __restrict__ rec_prep,
+                                                      int P, int tile_base) {
   constexpr int kSub = kTile / NT;
   const int tile = tile_base + (int)(blockIdx.x / kSub);
   const int b = tile_bunch[tile];
-  const BunchDev& B = bunch[b];
   const int lane = (blockIdx.x % kSub) * NT + threadIdx.x;
-  const int i = (tile - B.tile_off) * kTile + lane;
+  const int i = (tile - bunch[b].tile_off) * kTile + lane;
   const int64_t g = (int64_t)tile * kTile + lane;
-  const CloudRec* rb = rec + (size_t)b * P;
-  if ((int)threadIdx.x < P) s_prep[threadIdx.x] = field_prep(rb[threadIdx.x].rms_x, rb[threadIdx.x].rms_y);
-  __syncthreads();
-  if (i >= B.n || surv[g] != kAlive) return;
-  double x = c[0 * npad + g], y = c[2 * npad + g];
+  if (i >= bunch[b].n) return;
+  // every load of the particle at once (one memory round trip); the field
+  // constants of the bunch's records come precomputed with the records
+  const uint8_t alive = surv[g];
+  const double x = c[0 * npad + g], y = c[2 * npad + g];
+  const double px = c[1 * npad + g], py = c[3 * npad + g];
+  if (alive != kAlive) return;
   double dpx, dpy;
-  ion_kick_particle_prep(rb, s_prep, P, x, y, &dpx, &dpy);
-  c[1 * npad + g] += dpx;
-  c[3 * npad + g] += dpy;
+  ion_kick_particle_prep(rec + (size_t)b * P, rec_prep + (size_t)b * P, P, x, y, &dpx, &dpy);
+  c[1 * npad + g] = px + dpx;
+  c[3 * npad + g] = py + dpy;
 }
 
 // The kick shapes (threads per CTA, minimum CTAs per SM) of autotune choice v.
@@ -419,6 +418,7 @@ constexpr int kKickVariants = 4;
 cudaError_t launch_ion_kick_variant(Handle& h, int k, int v, int tile_a, int tile_b,
                                     cudaStream_t s) {
   const CloudRec* rec = h.d.rec + (size_t)k * h.M * h.P;
+  const FieldPrep* rp = h.d.rec_prep + (size_t)k * h.M * h.P;
   if (tile_b < 0) tile_b = h.n_tiles;
   if (!s) s = h.stream;
   const int nt = tile_b - tile_a;
@@ -426,19 +426,19 @@ cudaError_t launch_ion_kick_variant(Handle& h, int k, int v, int tile_a, int til
   switch (v) {
     case 1:
       k_ion_kick<256, 4><<<nt, 256, 0, s>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch, h.d.bunch,
-                                            rec, h.P, tile_a);
+                                            rec, rp, h.P, tile_a);
       break;
     case 2:
       k_ion_kick<128, 4><<<2 * nt, 128, 0, s>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch,
-                                                h.d.bunch, rec, h.P, tile_a);
+                                                h.d.bunch, rec, rp, h.P, tile_a);
       break;
     case 3:
       k_ion_kick<128, 6><<<2 * nt, 128, 0, s>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch,
-                                                h.d.bunch, rec, h.P, tile_a);
+                                                h.d.bunch, rec, rp, h.P, tile_a);
       break;
     default:
       k_ion_kick<256, 3><<<nt, 256, 0, s>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch, h.d.bunch,
-                                            rec, h.P, tile_a);
+                                            rec, rp, h.P, tile_a);
   }
   return cudaGetLastError();
 }

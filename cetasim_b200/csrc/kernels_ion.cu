@@ -330,8 +330,9 @@ __global__ void __launch_bounds__(4 * IONS, 1) k_ion_walk(ChainParams cp, IonWal
 // kept there too, for the cloud state.
 __global__ void __launch_bounds__(kFinishThreads) k_ion_records(ChainParams cp, IonWalk w,
                                                               const CloudState* __restrict__ cst,
-                                                              CloudRec* rec, int* status, int G,
-                                                              int ions, int ja, int jb) {
+                                                              CloudRec* rec, FieldPrep* rec_prep,
+                                                              int* status, int G, int ions,
+                                                              int ja, int jb) {
   __shared__ double s_ax[kFinishChunk], s_ay[kFinishChunk];
   __shared__ int s_n[kFinishChunk];
   __shared__ double s_carry[2];
@@ -379,6 +380,8 @@ __global__ void __launch_bounds__(kFinishThreads) k_ion_records(ChainParams cp, 
       r.rms_y = ry;
       r.count = n;
       rec[(size_t)j * P + p] = r;  // centroid filled below
+      // the field constants of this Gaussian, once for all the kicks that read it
+      rec_prep[(size_t)j * P + p] = field_prep(rx, ry);
       if (j == M - 1) {
         carry[2] = rx;
         carry[3] = ry;
@@ -501,7 +504,8 @@ cudaError_t launch_ion_walk(Handle& h, int k, int ja, int jb, cudaStream_t s) {
 
 cudaError_t launch_ion_records(Handle& h, int k, int ja, int jb, cudaStream_t s) {
   k_ion_records<<<h.P, kFinishThreads, 0, s>>>(h.chain, h.d.iw, h.d.cloud_state + (size_t)k * h.P,
-                                               h.d.rec + (size_t)k * h.M * h.P, h.d.status,
+                                               h.d.rec + (size_t)k * h.M * h.P,
+                                               h.d.rec_prep + (size_t)k * h.M * h.P, h.d.status,
                                                ion_walk_grid(h.d.iw.tcap, h.walk_ions),
                                                h.walk_ions, ja, jb);
   return cudaGetLastError();
