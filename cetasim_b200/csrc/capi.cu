@@ -93,7 +93,7 @@ int launch_ok(Handle& h, cudaError_t e, const char* what) {
 void free_beam(Handle& h) {
   DeviceBufs& d = h.d;
   dfree(d.c); dfree(d.surv); dfree(d.tile_bunch); dfree(d.chunk_bunch); dfree(d.bunch);
-  dfree(d.partials);
+  dfree(d.wpartials);
   dfree(d.counters); dfree(d.mom); dfree(d.loss_count); dfree(d.scratch);
   dfree(d.rec); dfree(d.rec_prep); dfree(d.lr_hist); dfree(d.lr_force); dfree(d.fir_hist); dfree(d.fir_kick);
   dfree(d.sr_geom); dfree(d.sr_counts); dfree(d.sr_sumx); dfree(d.sr_sumy); dfree(d.sr_lag);
@@ -105,7 +105,7 @@ void free_beam(Handle& h) {
   dfree(w.traj); dfree(w.alive); dfree(w.carry);
   w = IonWalk();
   d.c = nullptr; d.surv = nullptr; d.tile_bunch = nullptr; d.chunk_bunch = nullptr;
-  d.bunch = nullptr; d.partials = nullptr;
+  d.bunch = nullptr; d.wpartials = nullptr;
   d.counters = nullptr; d.mom = nullptr; d.loss_count = nullptr; d.scratch = nullptr;
   d.rec = nullptr; d.rec_prep = nullptr; d.lr_hist = nullptr; d.lr_force = nullptr; d.fir_hist = nullptr;
   d.fir_kick = nullptr; d.sr_geom = nullptr; d.sr_counts = nullptr; d.sr_sumx = nullptr;
@@ -548,7 +548,7 @@ int cg_set_beam(cg_handle* H, int M, const int* n_macro, const int* harm, const 
   DeviceBufs& d = h.d;
   if (dalloc(&d.c, 6 * (size_t)h.npad) || dalloc(&d.surv, (size_t)h.npad) ||
       dalloc(&d.tile_bunch, tiles) || dalloc(&d.chunk_bunch, chunks) || dalloc(&d.bunch, M) ||
-      dalloc(&d.partials, chunks) ||
+      dalloc(&d.wpartials, 8 * (size_t)chunks) ||
       dalloc(&d.counters, M + 1) || dalloc(&d.mom, M) || dalloc(&d.loss_count, M + 1)) {
     free_beam(h);
     return fail(&h, CG_ERR_OOM, "beam allocation failed");

@@ -75,7 +75,7 @@ struct DeviceBufs {
   int* tile_bunch = nullptr;    // n_tiles
   int* chunk_bunch = nullptr;   // n_chunks: bunch of each moments chunk
   BunchDev* bunch = nullptr;    // M
-  MomPartial* partials = nullptr;  // n_chunks
+  MomPartial* wpartials = nullptr; // n_chunks x 8: per-warp moment partials
   unsigned* counters = nullptr;    // M (+ spare)
   BunchMomDev* mom = nullptr;      // M
   int* loss_count = nullptr;       // M

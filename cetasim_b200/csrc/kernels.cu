@@ -271,6 +271,11 @@ __device__ void chunk_moment_partial(const double (&v)[kMomChunkTiles][6],
   chunk_moment_reduce(s, mn, mx, alive, [&](int u, int d) { return v[u][d]; }, smem, out);
 }
 
+__device__ __noinline__ void merge_partials_warp(int b, int part_off, int n_parts,
+                                                 const MomPartial* partials, unsigned* counters,
+                                                 BunchMomDev* mom, double beta_x, double beta_y,
+                                                 const double* z0);
+
 // Called by all threads of every CTA after its partial is stored: the last of
 // the n_parts CTAs of bunch b merges partials [part_off, part_off + n_parts)
 // and finalises.  z0 = z of the bunch's first particle (GetZMinMax seeds the
@@ -288,10 +293,18 @@ __device__ __noinline__ void bunch_moment_finish(int b, int part_off, int n_part
   __syncthreads();
   if (!last || threadIdx.x >= 32) return;
   __threadfence();
-  // warp 0: lane l merges partials l, l + 32, ... in order, then a fixed
-  // shuffle tree (lane i absorbs lane i + o) leaves the bunch total in lane 0
+  merge_partials_warp(b, part_off, n_parts, partials, counters, mom, beta_x, beta_y, z0);
+}
+
+// One full warp: lane l merges partials part_off + l, + l + 32, ... in order,
+// then a fixed shuffle tree (lane i absorbs lane i + o) leaves the bunch total
+// in lane 0, which finalises it and rearms the bunch's counter.
+__device__ __noinline__ void merge_partials_warp(int b, int part_off, int n_parts,
+                                                 const MomPartial* partials, unsigned* counters,
+                                                 BunchMomDev* mom, double beta_x, double beta_y,
+                                                 const double* z0) {
   constexpr int ND = (int)(sizeof(MomPartial) / sizeof(double));
-  const int lane = threadIdx.x;
+  const int lane = threadIdx.x & 31;
   MomPartial acc;
   mom_clear(acc);
   for (int t = lane; t < n_parts; t += 32) {
@@ -321,13 +334,87 @@ __device__ __noinline__ void bunch_moment_finish(int b, int part_off, int n_part
   }
 }
 
+// Warp-level moments for the map passes: each warp makes the two-pass partial
+// of its kMomChunkTiles x 32 particles of the chunk with shuffles only (no
+// block barrier), and the last warp of each bunch merges the bunch's warp
+// partials, index 8 x chunk + warp, in index order (deterministic).
+constexpr int kWarpsPerChunk = kTile / 32;
+
+__device__ __forceinline__ void warp_moment_partial(const double (&v)[kMomChunkTiles][6],
+                                                    const bool (&alive)[kMomChunkTiles],
+                                                    MomPartial* out) {
+  const int lane = threadIdx.x & 31;
+  double s[7] = {0, 0, 0, 0, 0, 0, 0};
+  double mn = INFINITY, mx = -INFINITY;
+#pragma unroll
+  for (int u = 0; u < kMomChunkTiles; ++u)
+    if (alive[u]) chunk_sums_add(v[u], s, mn, mx);
+  {  // warp totals to every lane: lanes 4 i hold total i after the transposed butterfly
+    const double s8[8] = {s[0], s[1], s[2], s[3], s[4], s[5], s[6], 0.0};
+    const double t = warp_sum8_t(s8);
+#pragma unroll
+    for (int k = 0; k < 7; ++k) s[k] = __shfl_sync(FULL_MASK, t, 4 * k);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    mn = fmin(mn, __shfl_xor_sync(FULL_MASK, mn, o));
+    mx = fmax(mx, __shfl_xor_sync(FULL_MASK, mx, o));
+  }
+  const double n = s[6];
+  double mean[6];
+#pragma unroll
+  for (int d = 0; d < 6; ++d) mean[d] = n > 0 ? s[d] / n : 0.0;
+  double q[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+  for (int u = 0; u < kMomChunkTiles; ++u) {
+    double dv[6];
+#pragma unroll
+    for (int d = 0; d < 6; ++d) dv[d] = alive[u] ? v[u][d] - mean[d] : 0.0;
+#pragma unroll
+    for (int d = 0; d < 6; ++d) q[d] = fma(dv[d], dv[d], q[d]);
+    q[6] = fma(dv[0], dv[1], q[6]);
+    q[7] = fma(dv[2], dv[3], q[7]);
+    q[8] = fma(dv[4], dv[5], q[8]);
+  }
+  const double q8[8] = {q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7]};
+  const double t = warp_sum8_t(q8);
+  double q9 = q[8];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) q9 += __shfl_xor_sync(FULL_MASK, q9, o);
+  if ((lane & 3) == 0) out->c[warp_sum8_index(lane)] = t;
+  if (lane == 0) {
+    out->n = n;
+#pragma unroll
+    for (int d = 0; d < 6; ++d) out->mean[d] = mean[d];
+    out->c[8] = q9;
+    out->zmin = mn;
+    out->zmax = mx;
+  }
+}
+
+// After the warp's partial is stored: the last of the bunch's n_parts warps
+// merges them.
+__device__ __forceinline__ void warp_moment_finish(int b, int part_off, int n_parts,
+                                                   const MomPartial* partials,
+                                                   unsigned* counters, BunchMomDev* mom,
+                                                   double beta_x, double beta_y,
+                                                   const double* z0) {
+  __threadfence();
+  __syncwarp();
+  unsigned prev = 0;
+  if ((threadIdx.x & 31) == 0) prev = atomicAdd(&counters[b], 1u);
+  prev = __shfl_sync(FULL_MASK, prev, 0);
+  if (prev != (unsigned)(n_parts - 1)) return;
+  __threadfence();
+  merge_partials_warp(b, part_off, n_parts, partials, counters, mom, beta_x, beta_y, z0);
+}
+
 __global__ void __launch_bounds__(kTile, 2) k_moments(const double* __restrict__ c, int64_t npad,
                                                    const uint8_t* __restrict__ surv,
                                                    const int* __restrict__ chunk_bunch,
                                                    const BunchDev* __restrict__ bunch,
                                                    MomPartial* partials, unsigned* counters,
                                                    BunchMomDev* mom, double beta_x, double beta_y) {
-  __shared__ double smem[18 * 32];
   const int b = chunk_bunch[blockIdx.x];
   const BunchDev B = bunch[b];
   const int tile0 = B.tile_off + (blockIdx.x - B.chunk_off) * kMomChunkTiles;
@@ -342,15 +429,17 @@ __global__ void __launch_bounds__(kTile, 2) k_moments(const double* __restrict__
 #pragma unroll
     for (int d = 0; d < 6; ++d) v[u][d] = valid ? c[d * npad + g] : 0.0;
   }
-  chunk_moment_partial(v, alive, smem, &partials[blockIdx.x]);
-  bunch_moment_finish(b, B.chunk_off, B.n_chunks, partials, counters, mom, beta_x, beta_y,
-                      c + 4 * npad + (int64_t)B.tile_off * kTile);
+  // the same warp partials and merge as the map passes (bitwise the same moments)
+  const int warp = threadIdx.x >> 5;
+  warp_moment_partial(v, alive, &partials[(size_t)blockIdx.x * kWarpsPerChunk + warp]);
+  warp_moment_finish(b, B.chunk_off * kWarpsPerChunk, B.n_chunks * kWarpsPerChunk, partials,
+                     counters, mom, beta_x, beta_y, c + 4 * npad + (int64_t)B.tile_off * kTile);
 }
 
 cudaError_t launch_moments(Handle& h, int k) {
   const SectionDev& s = h.sec_dev_host[k];
   k_moments<<<h.n_chunks, kTile, 0, h.stream>>>(h.d.c, h.npad, h.d.surv, h.d.chunk_bunch, h.d.bunch,
-                                                h.d.partials, h.d.counters, h.d.mom, s.beta_x,
+                                                h.d.wpartials, h.d.counters, h.d.mom, s.beta_x,
                                                 s.beta_y);
   return cudaGetLastError();
 }
@@ -466,7 +555,6 @@ __global__ void __launch_bounds__(kTile, 2) k_map_pass(double* __restrict__ c, i
                                                     BunchMomDev* mom, double beta_x, double beta_y,
                                                     const CloudRec* __restrict__ rec, int P,
                                                     int chunk_base) {
-  __shared__ double smem[18 * 32];
   __shared__ FieldPrep s_prep[CG_MAX_SPECIES];
   const int chunk = chunk_base + (int)blockIdx.x;
   const int b = chunk_bunch[chunk];
@@ -502,9 +590,10 @@ __global__ void __launch_bounds__(kTile, 2) k_map_pass(double* __restrict__ c, i
     store6(c, npad, (int64_t)(tile0 + u) * kTile + threadIdx.x, v[u]);
   }
   if (MOM) {
-    chunk_moment_partial(v, alive, smem, &partials[chunk]);
-    bunch_moment_finish(b, B.chunk_off, B.n_chunks, partials, counters, mom, beta_x, beta_y,
-                        c + 4 * npad + (int64_t)B.tile_off * kTile);
+    const int warp = threadIdx.x >> 5;
+    warp_moment_partial(v, alive, &partials[(size_t)chunk * kWarpsPerChunk + warp]);
+    warp_moment_finish(b, B.chunk_off * kWarpsPerChunk, B.n_chunks * kWarpsPerChunk, partials,
+                       counters, mom, beta_x, beta_y, c + 4 * npad + (int64_t)B.tile_off * kTile);
   }
 }
 
@@ -520,7 +609,7 @@ cudaError_t launch_map_pass(Handle& h, int k, int mom_section, bool kick, int ch
   auto kern = m ? (kick ? k_map_pass<true, true> : k_map_pass<true, false>)
                 : (kick ? k_map_pass<false, true> : k_map_pass<false, false>);
   kern<<<chunk_b - chunk_a, kTile, 0, s>>>(h.d.c, h.npad, h.d.surv, h.d.chunk_bunch, h.d.bunch,
-                                           h.sec_dev_host[k], h.ring, h.d.partials,
+                                           h.sec_dev_host[k], h.ring, h.d.wpartials,
                                            h.d.counters, h.d.mom, bx, by, rec, h.P, chunk_a);
   return cudaGetLastError();
 }
@@ -575,7 +664,6 @@ __global__ void __launch_bounds__(kTile, 2) k_map_stream(double* __restrict__ c,
   extern __shared__ __align__(128) unsigned char dyn_smem[];
   StreamBuf* buf = reinterpret_cast<StreamBuf*>(dyn_smem);
   __shared__ __align__(8) uint64_t s_bar[kStreamStages];
-  __shared__ double smem[18 * 32];
   __shared__ FieldPrep s_prep[CG_MAX_SPECIES];
   const int tid = threadIdx.x;
   const int nmine = (chunk_b - chunk_a - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
@@ -646,12 +734,13 @@ __global__ void __launch_bounds__(kTile, 2) k_map_stream(double* __restrict__ c,
       store6(c, npad, (int64_t)(l.tile0 + u) * kTile + tid, v[u]);
     }
     if (MOM) {
-      chunk_moment_partial(v, alive, smem, &partials[chunk]);
-      bunch_moment_finish(l.b, B.chunk_off, B.n_chunks, partials, counters, mom, beta_x, beta_y,
-                          c + 4 * npad + (int64_t)B.tile_off * kTile);
-    } else if (KICK) {
-      __syncthreads();  // s_prep is rewritten for the next chunk
+      const int warp = tid >> 5;
+      warp_moment_partial(v, alive, &partials[(size_t)chunk * kWarpsPerChunk + warp]);
+      warp_moment_finish(l.b, B.chunk_off * kWarpsPerChunk, B.n_chunks * kWarpsPerChunk,
+                         partials, counters, mom, beta_x, beta_y,
+                         c + 4 * npad + (int64_t)B.tile_off * kTile);
     }
+    if (KICK) __syncthreads();  // s_prep is rewritten for the next chunk
   }
 }
 
@@ -668,7 +757,7 @@ static cudaError_t map_stream_kernel(int grid, cudaStream_t s, Handle& h, int k,
   }
   k_map_stream<MOM, KICK><<<grid, kTile, kStreamSmem, s>>>(
       h.d.c, h.npad, h.d.surv, h.d.chunk_bunch, h.d.bunch, h.sec_dev_host[k], h.ring,
-      h.d.partials, h.d.counters, h.d.mom, bx, by, rec, h.P, chunk_a, chunk_b, h.d.status);
+      h.d.wpartials, h.d.counters, h.d.mom, bx, by, rec, h.P, chunk_a, chunk_b, h.d.status);
   return cudaGetLastError();
 }
 
