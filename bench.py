@@ -157,6 +157,12 @@ def main():
                          "moments all-gathered over NCCL) instead of N replicas")
     ap.add_argument("--no-surrogate", action="store_true",
                     help="skip the surrogate measurement (training + surrogate turns)")
+    ap.add_argument("--kick-variant", type=int, default=None, metavar="V",
+                    help="kick shape V (0-3; 4-7: the same inside the map pass) instead of "
+                         "the kick autotuner")
+    ap.add_argument("--pipeline", default=None, metavar="G:IONS:RAMP",
+                    help="pipeline shape (walk segments, ions per walk CTA, ramp 0/1) instead "
+                         "of the whole-turn pipeline autotuner")
     ap.add_argument("--workload", default="fast_ion", choices=["fast_ion", "batched_uneven"],
                     help="batched_uneven: 900 bunches of 5e3-5e4, 50 IPs, LR wake + FIR")
     args = ap.parse_args()
@@ -189,8 +195,6 @@ def main():
     beam.generate(seed=99 if shard else 99 + rank)
     copies = 1 if shard else world  # independent beams the ranks advance
     stream = torch.cuda.ExternalStream(lib.cg_stream(beam.h))
-    launches = C.c_int()
-    lib.cg_turn_launches(beam.h, C.byref(launches))
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     def barrier():
@@ -203,11 +207,23 @@ def main():
     # (it leaves the beam as it was), then the warm-up turns (the first one
     # instantiates the turn graph with the chosen shape)
     beam.Run(0, 1)
-    tune = beam.autotune(0, reps=10)
+    if args.kick_variant is not None:
+        beam.set_kick_variant(args.kick_variant)
+        tune = (args.kick_variant, None)
+    else:
+        tune = beam.autotune(0, reps=10)
     t_first = 1
     # pipeline shape (walk segments x walk CTA size) over whole turns; the
     # beam is restored after each trial
-    pipe = beam.autotune_pipeline(t_first, reps=3) if wl.cfg.flag_beam_ion else None
+    pipe = None
+    if args.pipeline:
+        g_, w_, r_ = (int(x) for x in args.pipeline.split(":"))
+        beam.set_pipeline(g_, w_, bool(r_))
+        pipe = ((g_, w_, r_), None)  # given, not tuned
+    elif wl.cfg.flag_beam_ion:
+        pipe = beam.autotune_pipeline(t_first, reps=3)
+    launches = C.c_int()  # of the turn graph as tuned
+    lib.cg_turn_launches(beam.h, C.byref(launches))
     beam.Run(t_first, args.warmup)
     barrier()
     times = []
@@ -333,23 +349,26 @@ def main():
                          "frac": achieved / peak.value if peak.value else None,
                          "peak_source": "measured FP64 FMA throughput (cg_fp64_peak)",
                          "algorithmic_flops_per_kick": flops_per_kick, "traffic": traffic,
-                         "traffic_source": "profiles/k_ion_kick_fast_ion.md (ncu, one launch)"},
+                         "traffic_source": "profiles/k_ion_kick_fast_ion.md (ncu, one segment launch scaled to the full beam by tiles)"},
             "ion_chain": {"us_per_ip": 1e3 * chain_ms.value,
                           "us_per_bunch_step": 1e3 * chain_ms.value / wl.n_bunches,
                           "bound": "latency (one field evaluation per bunch step)"},
             "cpu_baseline": cpu,
-            "autotune": {"kick_shapes_ms": [round(float(x), 5) for x in tune[1][:-2]],
-                         "map_pass_ms": round(float(tune[1][-2]), 5),
-                         "map_pass_with_kick_ms": round(float(tune[1][-1]), 5),
-                         "chosen_shape": int(tune[0]) % (len(tune[1]) - 2),
-                         "kick_in_map_pass": bool(tune[0] >= len(tune[1]) - 2),
+            "autotune": {"kick_shapes_ms": None if tune[1] is None else
+                         [round(float(x), 5) for x in tune[1][:-2]],
+                         "map_pass_ms": None if tune[1] is None else round(float(tune[1][-2]), 5),
+                         "map_pass_with_kick_ms": None if tune[1] is None else
+                         round(float(tune[1][-1]), 5),
+                         "chosen_shape": int(tune[0]) % 4,
+                         "kick_in_map_pass": bool(tune[0] >= 4),
                          "shapes": ["256 thr x3/SM", "256 thr x4/SM", "128 thr x4/SM",
                                     "128 thr x6/SM"],
                          "pipeline": None if pipe is None else {
                              "segments": pipe[0][0], "walk_ions": pipe[0][1],
                              "ramp": bool(pipe[0][2]),
-                             "turn_ms": {f"{g}x{w}{'r' if r else ''}": round(float(m), 4)
-                                         for (g, w, r), m in zip(_abi.PIPE_SHAPES, pipe[1])}}},
+                             "turn_ms": None if pipe[1] is None else {
+                                 f"{g}x{w}{'r' if r else ''}": round(float(m), 4)
+                                 for (g, w, r), m in zip(_abi.PIPE_SHAPES, pipe[1])}}},
             "surrogate": sur,
             "e2e": {"value": e2e_value, "unit": "macroparticle-turns/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
@@ -417,8 +436,9 @@ def kick_traffic():
         txt = open(os.path.join(ROOT, "profiles", "k_ion_kick_fast_ion.md")).read()
     except OSError:
         return None
-    m = re.search(r"dram bytes read / written per launch \| ([\d.]+) MB / ([\d.]+) MB", txt)
-    return (float(m.group(1)) + float(m.group(2))) * 1e6 if m else None
+    # the full-beam line (the last one of the summary)
+    m = re.findall(r"dram bytes read / written per launch \| ([\d.]+) MB / ([\d.]+) MB", txt)
+    return (float(m[-1][0]) + float(m[-1][1])) * 1e6 if m else None
 
 if __name__ == "__main__":
     main()
