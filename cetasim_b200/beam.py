@@ -171,6 +171,28 @@ class MPBeam:
         return [(_abi.TRACE_KINDS[r.kind], r.stream, r.ip, r.segment, r.t_end_us)
                 for r in recs[:n.value]]
 
+    # -- coupled-bunch mode history (MPBeam::GetCBMGR) -----------------------------
+    def cbm_init(self, capacity: int):
+        self._check(self.lib.cg_cbm_init(self.h, capacity))
+
+    def cbm_record(self):
+        self._check(self.lib.cg_cbm_record(self.h))
+
+    def cbm_history(self):
+        """(amp, arg, aver), each records x 3 planes x M."""
+        n = C.c_int()
+        self._check(self.lib.cg_cbm_count(self.h, C.byref(n)))
+        M = self.wl.n_bunches
+        out = [np.zeros((n.value, 3, M)) for _ in range(3)]
+        if n.value:
+            self._check(self.lib.cg_cbm_history(self.h, 0, n.value, *[_abi.ptr(a) for a in out]))
+        return tuple(out)
+
+    def cbm_growth(self, first: int, last: int, interval: float):
+        rate = np.zeros((3, self.wl.n_bunches))
+        self._check(self.lib.cg_cbm_growth(self.h, first, last, float(interval), _abi.ptr(rate)))
+        return rate
+
     def autotune_pipeline(self, turn0: int, reps: int = 5):
         """Times whole turns with each pipeline shape, restores the beam and
         keeps the fastest; returns ((groups, walk_ions, ramp), ms per shape

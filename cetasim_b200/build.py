@@ -15,7 +15,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libcetagpu.so")
 
-SOURCES = ["capi.cu", "kernels.cu", "kernels_sr.cu", "kernels_ion.cu", "surrogate.cu", "shard.cu", "faddeeva_table.cpp", "input_settings.cpp"]
+SOURCES = ["capi.cu", "kernels.cu", "kernels_sr.cu", "kernels_ion.cu", "surrogate.cu", "shard.cu",
+           "cbm.cu", "faddeeva_table.cpp", "input_settings.cpp"]
 HEADERS = ["cg_common.cuh", "faddeeva.cuh", "be_field.cuh", "track_math.cuh", "cg_internal.h",
            "kernels.cuh", "umma.cuh", "surrogate.cuh"]
 

@@ -100,6 +100,9 @@ void free_beam(Handle& h) {
   dfree(d.sr_pot);
   dfree(d.mom_send); dfree(d.mom_all); dfree(d.sh_off); dfree(d.sh_cnt);
   d.mom_send = nullptr; d.mom_all = nullptr; d.sh_off = nullptr; d.sh_cnt = nullptr;
+  dfree(d.cbm);  // sized by the bunch count
+  d.cbm = nullptr;
+  h.cbm_cap = h.cbm_n = 0;
   IonWalk& w = d.iw;
   dfree(w.births); dfree(w.prep); dfree(w.bunch); dfree(w.spec); dfree(w.bound); dfree(w.part);
   dfree(w.traj); dfree(w.alive); dfree(w.carry);
@@ -1050,7 +1053,91 @@ int cg_trace_turn(cg_handle* H, int turn0, cg_trace_record* out, int cap, int* n
   return check_status(h);
 }
 
-// ---- measurement and host memory ----// ---- measurement and host memory ----
+// ---- coupled-bunch mode history and growth rates (MPBeam::GetCBMGR) ----
+
+int cg_cbm_init(cg_handle* H, int capacity) {
+  STAGE_PROLOGUE
+  if (capacity < 1) return fail(&h, CG_ERR_INVALID, "capacity < 1");
+  dfree(h.d.cbm);
+  h.d.cbm = nullptr;
+  h.cbm_cap = h.cbm_n = 0;
+  if (dalloc(&h.d.cbm, (size_t)capacity * 9 * h.M)) return fail(&h, CG_ERR_OOM, "CBM history");
+  h.cbm_cap = capacity;
+  return CG_OK;
+}
+
+int cg_cbm_record(cg_handle* H) {
+  STAGE_PROLOGUE
+  if (!h.d.cbm) return fail(&h, CG_ERR_NOT_READY, "cg_cbm_init first");
+  if (h.cbm_n >= h.cbm_cap) return fail(&h, CG_ERR_INVALID, "CBM history full");
+  const SectionDev& s0 = h.sec_dev_host[0];
+  const cg_config& c = h.cfg;
+  CbmParams p;
+  // GetCBMGR: rmsBunchLength / rmsEnergySpread of the bunch settings; the
+  // ring's natural beta_z when those are unset
+  const double bz = c.bunch_sigma_z > 0 && c.bunch_sigma_dp > 0
+                        ? c.bunch_sigma_z / c.bunch_sigma_dp
+                        : c.ring.beta_z;
+  p.sqrt_beta[0] = std::sqrt(s0.beta_x);
+  p.sqrt_beta[1] = std::sqrt(s0.beta_y);
+  p.sqrt_beta[2] = std::sqrt(bz);
+  p.alpha_sqrt[0] = s0.alpha_x / std::sqrt(s0.beta_x);
+  p.alpha_sqrt[1] = s0.alpha_y / std::sqrt(s0.beta_y);
+  p.alpha_sqrt[2] = 0.0;
+  p.tune[0] = c.ring.work_qx;
+  p.tune[1] = c.ring.work_qy;
+  p.tune[2] = c.ring.work_qz;
+  p.H = c.ring.harmonics;
+  p.M = h.M;
+  // the moments at section 0, as the reference's print turn holds them
+  cudaError_t e = launch_moments(h, 0);
+  if (e == cudaSuccess) e = exchange_moments(h);
+  if (e == cudaSuccess) e = launch_cbm_record(h, p, h.cbm_n);
+  if (e != cudaSuccess) return cuda_fail(&h, e, "CBM record");
+  h.cbm_n++;
+  return CG_OK;
+}
+
+int cg_cbm_count(cg_handle* H, int* n) {
+  STAGE_PROLOGUE
+  if (!n) return fail(&h, CG_ERR_INVALID, "n is NULL");
+  *n = h.cbm_n;
+  return CG_OK;
+}
+
+int cg_cbm_history(cg_handle* H, int first, int count, double* amp, double* arg, double* aver) {
+  STAGE_PROLOGUE
+  if (first < 0 || count < 0 || first + count > h.cbm_n)
+    return fail(&h, CG_ERR_INVALID, "records outside the history");
+  const size_t per = (size_t)3 * h.M;
+  for (int r = 0; r < count; ++r) {
+    const double* src = h.d.cbm + (size_t)(first + r) * 3 * per;
+    double* dst[3] = {amp, arg, aver};
+    for (int q = 0; q < 3; ++q)
+      if (dst[q])
+        CG_CUDA(&h, cudaMemcpyAsync(dst[q] + r * per, src + q * per, per * sizeof(double),
+                                    cudaMemcpyDeviceToHost, h.stream));
+  }
+  CG_CUDA(&h, cudaStreamSynchronize(h.stream));
+  return check_status(h);
+}
+
+int cg_cbm_growth(cg_handle* H, int first, int last, double interval, double* rate) {
+  STAGE_PROLOGUE
+  if (!rate || first < 0 || last > h.cbm_n || last - first < 2 || !(interval > 0))
+    return fail(&h, CG_ERR_INVALID, "bad fit range");
+  double* d_rate = nullptr;
+  if (dalloc(&d_rate, (size_t)3 * h.M)) return fail(&h, CG_ERR_OOM, "fit result");
+  cudaError_t e = launch_cbm_fit(h, h.M, first, last - first, interval, h.cfg.ring.t0, d_rate);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(rate, d_rate, sizeof(double) * 3 * h.M, cudaMemcpyDeviceToHost, h.stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h.stream);
+  dfree(d_rate);
+  if (e != cudaSuccess) return cuda_fail(&h, e, "CBM fit");
+  return check_status(h);
+}
+
+// ---- measurement and host memory ----
 
 void* cg_host_alloc(size_t bytes) {
   void* p = nullptr;

@@ -1,0 +1,97 @@
+// Coupled-bunch mode analysis on the device: the "ideal" method of
+// MPBeam::GetCBMGR (MPBeam.cpp:1496-1575) and its growth-rate fit
+// (MPBeam.cpp:1781-1830 with FittingGSL::FitALinear, FittingGSL.cpp:231-243).
+//
+// A record takes the bunch centroids at section 0 (the moments the
+// reference's print turn holds after MPBeamRMSCal(0)), forms per plane the
+// normalised complex amplitude of every bunch
+//     x: (x / sqrt(b) - i (sqrt(b) x' + a / sqrt(b) x)) exp(i phi_j)
+//     y: the same with the y Twiss parameters
+//     z: (z / sqrt(b_z) + i sqrt(b_z) dp) exp(i phi_j),   b_z = sigma_z / sigma_dp
+// with phi_j = -2 pi Q h_j / H (h_j the bunch's harmonic number), and its
+// forward DFT over the M bunches, X_k = sum_j z_j exp(-2 pi i j k / M) (the
+// convention of the reference's GSL complex FFT).  |X_k| and atan2(Re, Im)
+// (the reference's argument order) go into a device history with the
+// centroids, so a run records every print interval without a host round
+// trip.  The fit is a least-squares line through log |X_k| against the turn
+// with unit weights; the growth rate is its slope / t0.
+#include <cuda_runtime.h>
+#include "kernels.cuh"
+
+namespace cg {
+
+// One thread per (mode k, plane): the DFT over bunches in bunch order
+// (deterministic).  Block 0 of each plane also stores the centroids.
+__global__ void k_cbm_record(const BunchMomDev* __restrict__ mom,
+                             const BunchDev* __restrict__ bunch, CbmParams p, double* amp,
+                             double* arg, double* aver) {
+  const int pl = blockIdx.y, M = p.M;
+  const int iu = 2 * pl;  // u, u' = mean[2 pl], mean[2 pl + 1]
+  const double sb = p.sqrt_beta[pl], ab = p.alpha_sqrt[pl], q = p.tune[pl];
+  const double sgn = pl == 2 ? 1.0 : -1.0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < M; k += gridDim.x * blockDim.x) {
+    double re = 0.0, im = 0.0;
+    for (int j = 0; j < M; ++j) {
+      const double u = mom[j].mean[iu], up = mom[j].mean[iu + 1];
+      const double a = u / sb, b = sgn * (sb * up + ab * u);
+      double sp, cp;
+      sincospi(-2.0 * q * (double)bunch[j].harm / (double)p.H, &sp, &cp);
+      const double zr = a * cp - b * sp, zi = a * sp + b * cp;
+      double st, ct;
+      sincospi(-2.0 * (double)(((int64_t)j * k) % M) / (double)M, &st, &ct);
+      re += zr * ct - zi * st;
+      im += zr * st + zi * ct;
+    }
+    amp[pl * M + k] = sqrt(re * re + im * im);
+    arg[pl * M + k] = atan2(re, im);
+  }
+  if (blockIdx.x == 0)
+    for (int j = threadIdx.x; j < M; j += blockDim.x) aver[pl * M + j] = mom[j].mean[iu];
+}
+
+// One thread per (plane, mode): the weighted linear fit of GSL's
+// gsl_fit_wlinear (running weighted means, then running second moments;
+// GSL 2.7, fit/linear.c) with unit weights, x_n = n * interval, y_n = log
+// |X_k| of record first + n.  rate = slope / t0.
+__global__ void k_cbm_fit(const double* __restrict__ hist, int M, int first, int dim,
+                          double interval, double t0, double* rate) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= 3 * M) return;
+  const size_t stride = (size_t)3 * M * 3;  // one record: amp, arg, aver of 3 planes
+  double W = 0, wm_x = 0, wm_y = 0;
+  for (int n = 0; n < dim; ++n) {
+    const double x = n * interval, y = log(hist[(size_t)(first + n) * stride + e]);
+    W += 1.0;
+    wm_x += (x - wm_x) * (1.0 / W);
+    wm_y += (y - wm_y) * (1.0 / W);
+  }
+  W = 0;
+  double wm_dx2 = 0, wm_dxdy = 0;
+  for (int n = 0; n < dim; ++n) {
+    const double x = n * interval, y = log(hist[(size_t)(first + n) * stride + e]);
+    const double dx = x - wm_x, dy = y - wm_y;
+    W += 1.0;
+    wm_dx2 += (dx * dx - wm_dx2) * (1.0 / W);
+    wm_dxdy += (dx * dy - wm_dxdy) * (1.0 / W);
+  }
+  rate[e] = wm_dxdy / wm_dx2 / t0;
+}
+
+cudaError_t launch_cbm_record(Handle& h, const CbmParams& p, int rec) {
+  double* base = h.d.cbm + (size_t)rec * 9 * p.M;
+  const int threads = 128;
+  dim3 grid((p.M + threads - 1) / threads, 3);
+  k_cbm_record<<<grid, threads, 0, h.stream>>>(h.d.mom, h.d.bunch, p, base, base + 3 * p.M,
+                                               base + 6 * p.M);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cbm_fit(Handle& h, int M, int first, int dim, double interval, double t0,
+                           double* rate) {
+  const int threads = 128;
+  k_cbm_fit<<<(3 * M + threads - 1) / threads, threads, 0, h.stream>>>(h.d.cbm, M, first, dim,
+                                                                       interval, t0, rate);
+  return cudaGetLastError();
+}
+
+}  // namespace cg

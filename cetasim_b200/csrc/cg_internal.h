@@ -114,9 +114,18 @@ struct DeviceBufs {
   double* sr_lag = nullptr;        // M x (2B-1)
   double* sr_pot = nullptr;        // M x B (z plane, persistent)
   double* sr_green = nullptr;      // resonators x 1000 (u-independent factors)
+  // coupled-bunch mode history (cg_cbm_*): records x (amp, arg, aver) x 3 planes x M
+  double* cbm = nullptr;
   // scratch
   double* scratch = nullptr;
   size_t scratch_bytes = 0;
+};
+
+// Coupled-bunch mode record constants (cbm.cu): per plane x, y, z
+struct CbmParams {
+  double sqrt_beta[3], alpha_sqrt[3];  // sqrt(beta), alpha / sqrt(beta) at section 0 (z: alpha 0)
+  double tune[3];
+  int H, M;
 };
 
 struct TraceMark {
@@ -140,6 +149,7 @@ struct Handle {
   // pipelined turn: the ion walk of an IP in `pipe_groups` segments of bunches;
   // records, kicks and maps of a segment run on `side` while the next segment
   // walks
+  int cbm_cap = 0, cbm_n = 0;  // coupled-bunch mode history: capacity, records made
   int pipe_groups = 4;
   // trajectories per walk CTA (8, 16, 32, 64): smaller CTAs spread the
   // walk's FP64 work over more SMs and find room sooner while the kicks and

@@ -70,6 +70,11 @@ void nccl_comm_destroy(void* comm);
 std::string nccl_error(int r);
 bool nccl_available();
 
+// coupled-bunch mode history and growth-rate fit (cbm.cu)
+cudaError_t launch_cbm_record(Handle& h, const CbmParams& p, int rec);
+cudaError_t launch_cbm_fit(Handle& h, int M, int first, int dim, double interval, double t0,
+                           double* rate);
+
 // field surrogate (surrogate.cu)
 cudaError_t prepare_surrogate();
 cudaError_t launch_sur_data(uint64_t seed, int64_t n, float* xin, float* tout, cudaStream_t s);

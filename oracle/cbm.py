@@ -1,0 +1,75 @@
+"""Coupled-bunch mode analysis: CPU restatement for the parity tests.
+
+Test infrastructure only (the library never imports it).  It restates the
+"ideal" method of MPBeam::GetCBMGR (MPBeam.cpp:1496-1575: per plane the
+normalised complex amplitude of each bunch, turned by its betatron phase
+-2 pi Q h_j / H, then GSL's forward complex FFT over the bunches, whose
+convention is X_k = sum_j z_j exp(-2 pi i j k / M)) and the growth-rate fit of
+MPBeam.cpp:1781-1830 (FittingGSL::FitALinear, FittingGSL.cpp:231-243, which
+calls gsl_fit_wlinear of GSL >= 2.7: weighted means accumulated as running
+means, then the running weighted second moments; slope = cov / var).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def cbm_record(mean, harm, H, beta, alpha, tunes, beta_z):
+    """mean: (M, 6) bunch centroids (x, x', y, y', z, dp); harm: (M,) bunch
+    harmonic numbers; beta, alpha: Twiss (x, y) at section 0; tunes (Qx, Qy,
+    Qz).  Returns amp, arg, aver, each (3, M): |X_k|, atan2(Re X_k, Im X_k)
+    (the reference's argument order, MPBeam.cpp:1567-1569) and the centroids."""
+    mean = np.asarray(mean, dtype=np.float64)
+    harm = np.asarray(harm, dtype=np.float64)
+    M = len(harm)
+    amp = np.zeros((3, M))
+    arg = np.zeros((3, M))
+    aver = np.zeros((3, M))
+    for pl in range(3):
+        u, up = mean[:, 2 * pl], mean[:, 2 * pl + 1]
+        if pl < 2:  # MPBeam.cpp:1536-1537
+            sb = np.sqrt(beta[pl])
+            z = u / sb - 1j * (sb * up + alpha[pl] / sb * u)
+        else:       # MPBeam.cpp:1538 (alpha_z = 0)
+            sb = np.sqrt(beta_z)
+            z = u / sb + 1j * (sb * up)
+        z = z * np.exp(1j * (-2.0 * np.pi * tunes[pl] * harm / H))
+        X = np.fft.fft(z)
+        amp[pl] = np.sqrt(X.real ** 2 + X.imag ** 2)
+        arg[pl] = np.arctan2(X.real, X.imag)
+        aver[pl] = u
+    return amp, arg, aver
+
+
+def wlinear_slope(x, y, w=None):
+    """gsl_fit_wlinear's slope (running weighted means, GSL 2.7 fit/linear.c)."""
+    x = np.asarray(x, dtype=np.float64)
+    y = np.asarray(y, dtype=np.float64)
+    w = np.ones_like(x) if w is None else np.asarray(w, dtype=np.float64)
+    W = wm_x = wm_y = 0.0
+    for xi, yi, wi in zip(x, y, w):
+        if wi > 0:
+            W += wi
+            wm_x += (xi - wm_x) * (wi / W)
+            wm_y += (yi - wm_y) * (wi / W)
+    W = wm_dx2 = wm_dxdy = 0.0
+    for xi, yi, wi in zip(x, y, w):
+        if wi > 0:
+            dx, dy = xi - wm_x, yi - wm_y
+            W += wi
+            wm_dx2 += (dx * dx - wm_dx2) * (wi / W)
+            wm_dxdy += (dx * dy - wm_dxdy) * (wi / W)
+    return wm_dxdy / wm_dx2
+
+
+def cbm_growth(amp_hist, first, last, interval, t0):
+    """Growth rates (3, M) in 1/s: the fit of log |X_k| over records
+    [first, last) against n x interval turns, slope / t0 (MPBeam.cpp:1781-1830)."""
+    amp_hist = np.asarray(amp_hist, dtype=np.float64)
+    x = np.arange(last - first) * float(interval)
+    _, P, M = amp_hist.shape
+    rate = np.zeros((P, M))
+    for pl in range(P):
+        for k in range(M):
+            rate[pl, k] = wlinear_slope(x, np.log(amp_hist[first:last, pl, k])) / t0
+    return rate

@@ -1,0 +1,71 @@
+"""Coupled-bunch mode history and growth rates on the GPU (cg_cbm_*) against
+the oracle (oracle/cbm.py) on the same bunch moments."""
+import numpy as np
+import pytest
+
+from helpers import pair, particles, small
+from oracle import cbm
+
+pytestmark = pytest.mark.gpu
+
+
+def _oracle_record(wl, g):
+    s0 = wl.sections[0]
+    r = wl.cfg.ring
+    mean = np.array([list(m.mean) for m in g.moments()])
+    return cbm.cbm_record(mean, wl.harm, r.harmonics, (s0.beta_x, s0.beta_y),
+                          (s0.alpha_x, s0.alpha_y), (r.work_qx, r.work_qy, r.work_qz), r.beta_z)
+
+
+def _with_mode(parts, mu, amp, n_bunch):
+    """Bunch centroids displaced by a travelling x and y pattern of mode mu."""
+    out = []
+    for j, c in enumerate(parts):
+        c = c.copy()
+        ph = 2 * np.pi * mu * j / n_bunch
+        c[0] += amp * np.cos(ph)
+        c[1] += 1e-2 * amp * np.sin(ph)
+        c[2] += 0.5 * amp * np.sin(ph)
+        c[4] += 1e-3 * np.cos(ph)
+        out.append(c)
+    return out
+
+
+def test_record_matches_the_oracle():
+    wl = small("fast_ion", 0.05)
+    parts = _with_mode(particles(wl, seed=31), 7, 2e-5, wl.n_bunches)
+    g, _ = pair(wl, parts)
+    g.cbm_init(4)
+    g.cbm_record()
+    amp, arg, aver = g.cbm_history()
+    assert amp.shape == (1, 3, wl.n_bunches)
+    oa, og, ov = _oracle_record(wl, g)
+    scale = oa.max(axis=1, keepdims=True)
+    assert np.max(np.abs(amp[0] - oa) / scale) < 1e-11
+    big = oa > 1e-6 * scale  # phases of the modes that carry the signal
+    dphi = np.angle(np.exp(1j * (arg[0] - og)))
+    assert np.max(np.abs(dphi[big])) < 1e-9
+    assert np.array_equal(aver[0], ov)
+
+
+def test_growth_of_a_synthetic_mode():
+    """Records of a mode whose amplitude grows as exp(g t): the device fit
+    returns g for that mode, and the oracle's fit of the device history."""
+    wl = small("fast_ion", 0.02)
+    # centred bunches: the centroids are the mode pattern alone
+    base = [c - c.mean(axis=1, keepdims=True) for c in particles(wl, seed=32)]
+    g, _ = pair(wl, base)
+    t0, interval, rate = wl.cfg.ring.t0, 50, 400.0
+    n_rec = 12
+    g.cbm_init(n_rec)
+    for n in range(n_rec):
+        a = 1e-6 * np.exp(rate * t0 * interval * n)
+        g.upload_beam(_with_mode(base, 3, a, wl.n_bunches))
+        g.cbm_record()
+    amp, _, _ = g.cbm_history()
+    dev = g.cbm_growth(2, n_rec, interval)
+    ora = cbm.cbm_growth(amp, 2, n_rec, interval, t0)
+    assert np.allclose(dev, ora, rtol=1e-9, atol=1e-6, equal_nan=True)
+    # the x mode the centroids carry (bin M - 3 after the -i rotation) grows at the set rate
+    k = int(np.argmax(amp[-1, 0]))
+    assert abs(dev[0, k] / rate - 1) < 1e-3

@@ -1,0 +1,36 @@
+"""The coupled-bunch mode oracle (oracle/cbm.py) against closed forms: a pure
+mode lands in its DFT bin, and the GSL-form fit is the least-squares slope."""
+import numpy as np
+
+from oracle import cbm
+
+
+def test_pure_mode_lands_in_its_bin():
+    M, H, mu = 16, 16, 5
+    harm = np.arange(M)
+    beta, alpha, tunes = (4.0, 2.5), (0.0, 0.0), (0.0, 0.0, 0.0)
+    j = np.arange(M)
+    mean = np.zeros((M, 6))
+    # alpha = 0, x / sqrt(b) = cos and sqrt(b) x' = sin: z_j = cos - i sin
+    mean[:, 0] = np.sqrt(beta[0]) * np.cos(2 * np.pi * mu * j / M)
+    mean[:, 1] = np.sin(2 * np.pi * mu * j / M) / np.sqrt(beta[0])
+    amp, arg, aver = cbm.cbm_record(mean, harm, H, beta, alpha, tunes, 1.0)
+    # z_j = cos - i sin = exp(-2 pi i mu j / M): all weight in bin M - mu
+    assert abs(amp[0, M - mu] - M) < 1e-12
+    assert np.max(np.delete(amp[0], M - mu)) < 1e-12
+    assert np.array_equal(aver[0], mean[:, 0])
+
+
+def test_fit_is_the_least_squares_slope():
+    rng = np.random.default_rng(3)
+    x = np.arange(40) * 25.0
+    y = 1e-4 * x + 0.3 + rng.normal(0, 1e-3, len(x))
+    assert abs(cbm.wlinear_slope(x, y) - np.polyfit(x, y, 1)[0]) < 1e-15 * 1e3
+
+
+def test_growth_recovers_an_exponential():
+    t0, interval, g = 2.5e-6, 10, 120.0  # 1/s
+    n = np.arange(30)
+    amp = np.exp(g * t0 * interval * n)[:, None, None] * np.ones((1, 3, 4))
+    rate = cbm.cbm_growth(amp, 5, 30, interval, t0)
+    assert np.allclose(rate, g, rtol=1e-9)
