@@ -179,18 +179,20 @@ class MPBeam:
         self._check(self.lib.cg_cbm_record(self.h))
 
     def cbm_history(self):
-        """(amp, arg, aver), each records x 3 planes x M."""
+        """(amp, arg, aver, iq_amp, iq_arg), each records x 3 planes x M."""
         n = C.c_int()
         self._check(self.lib.cg_cbm_count(self.h, C.byref(n)))
         M = self.wl.n_bunches
-        out = [np.zeros((n.value, 3, M)) for _ in range(3)]
+        out = [np.zeros((n.value, 3, M)) for _ in range(5)]
         if n.value:
             self._check(self.lib.cg_cbm_history(self.h, 0, n.value, *[_abi.ptr(a) for a in out]))
         return tuple(out)
 
-    def cbm_growth(self, first: int, last: int, interval: float):
+    def cbm_growth(self, first: int, last: int, interval: float, method: int = 0):
+        """Growth rates (3, M) in 1/s: method 0 the DFT modes, 1 the IQ scan."""
         rate = np.zeros((3, self.wl.n_bunches))
-        self._check(self.lib.cg_cbm_growth(self.h, first, last, float(interval), _abi.ptr(rate)))
+        self._check(self.lib.cg_cbm_growth(self.h, method, first, last, float(interval),
+                                           _abi.ptr(rate)))
         return rate
 
     def autotune_pipeline(self, turn0: int, reps: int = 5):

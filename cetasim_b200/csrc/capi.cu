@@ -1061,7 +1061,8 @@ int cg_cbm_init(cg_handle* H, int capacity) {
   dfree(h.d.cbm);
   h.d.cbm = nullptr;
   h.cbm_cap = h.cbm_n = 0;
-  if (dalloc(&h.d.cbm, (size_t)capacity * 9 * h.M)) return fail(&h, CG_ERR_OOM, "CBM history");
+  if (dalloc(&h.d.cbm, (size_t)capacity * kCbmRecord * h.M))
+    return fail(&h, CG_ERR_OOM, "CBM history");
   h.cbm_cap = capacity;
   return CG_OK;
 }
@@ -1105,15 +1106,16 @@ int cg_cbm_count(cg_handle* H, int* n) {
   return CG_OK;
 }
 
-int cg_cbm_history(cg_handle* H, int first, int count, double* amp, double* arg, double* aver) {
+int cg_cbm_history(cg_handle* H, int first, int count, double* amp, double* arg, double* aver,
+                   double* iq_amp, double* iq_arg) {
   STAGE_PROLOGUE
   if (first < 0 || count < 0 || first + count > h.cbm_n)
     return fail(&h, CG_ERR_INVALID, "records outside the history");
   const size_t per = (size_t)3 * h.M;
   for (int r = 0; r < count; ++r) {
-    const double* src = h.d.cbm + (size_t)(first + r) * 3 * per;
-    double* dst[3] = {amp, arg, aver};
-    for (int q = 0; q < 3; ++q)
+    const double* src = h.d.cbm + (size_t)(first + r) * kCbmRecord * h.M;
+    double* dst[5] = {amp, arg, aver, iq_amp, iq_arg};
+    for (int q = 0; q < 5; ++q)
       if (dst[q])
         CG_CUDA(&h, cudaMemcpyAsync(dst[q] + r * per, src + q * per, per * sizeof(double),
                                     cudaMemcpyDeviceToHost, h.stream));
@@ -1122,13 +1124,15 @@ int cg_cbm_history(cg_handle* H, int first, int count, double* amp, double* arg,
   return check_status(h);
 }
 
-int cg_cbm_growth(cg_handle* H, int first, int last, double interval, double* rate) {
+int cg_cbm_growth(cg_handle* H, int method, int first, int last, double interval, double* rate) {
   STAGE_PROLOGUE
   if (!rate || first < 0 || last > h.cbm_n || last - first < 2 || !(interval > 0))
     return fail(&h, CG_ERR_INVALID, "bad fit range");
+  if (method != 0 && method != 1) return fail(&h, CG_ERR_INVALID, "method must be 0 or 1");
   double* d_rate = nullptr;
   if (dalloc(&d_rate, (size_t)3 * h.M)) return fail(&h, CG_ERR_OOM, "fit result");
-  cudaError_t e = launch_cbm_fit(h, h.M, first, last - first, interval, h.cfg.ring.t0, d_rate);
+  cudaError_t e = launch_cbm_fit(h, method, h.M, first, last - first, interval, h.cfg.ring.t0,
+                                 d_rate);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(rate, d_rate, sizeof(double) * 3 * h.M, cudaMemcpyDeviceToHost, h.stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h.stream);

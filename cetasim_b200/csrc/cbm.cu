@@ -21,29 +21,44 @@
 namespace cg {
 
 // One thread per (mode k, plane): the DFT over bunches in bunch order
-// (deterministic).  Block 0 of each plane also stores the centroids.
+// (deterministic), and the IQ average at the scan frequency (k + Q) f0
+// (MPBeam.cpp:1586-1625, frequencies MPBeam.cpp:153-158):
+//     IQ_k = (1/M) sum_i u_i exp(-2 pi i (k + Q) f0 h_i t0 / H),
+// with f0 t0 = 1, stored as |IQ_k| and arg IQ_k.  A record holds kCbmRecord
+// x M doubles: DFT |X|, arg X, centroids, |IQ|, arg IQ, each 3 planes x M.
+// Block 0 of each plane also stores the centroids.
 __global__ void k_cbm_record(const BunchMomDev* __restrict__ mom,
                              const BunchDev* __restrict__ bunch, CbmParams p, double* amp,
-                             double* arg, double* aver) {
+                             double* arg, double* aver, double* iq_amp, double* iq_arg) {
   const int pl = blockIdx.y, M = p.M;
   const int iu = 2 * pl;  // u, u' = mean[2 pl], mean[2 pl + 1]
   const double sb = p.sqrt_beta[pl], ab = p.alpha_sqrt[pl], q = p.tune[pl];
   const double sgn = pl == 2 ? 1.0 : -1.0;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < M; k += gridDim.x * blockDim.x) {
-    double re = 0.0, im = 0.0;
+    double re = 0.0, im = 0.0, qre = 0.0, qim = 0.0;
+    const double fk = (double)k + q;
     for (int j = 0; j < M; ++j) {
       const double u = mom[j].mean[iu], up = mom[j].mean[iu + 1];
       const double a = u / sb, b = sgn * (sb * up + ab * u);
+      const double hj = (double)bunch[j].harm;
       double sp, cp;
-      sincospi(-2.0 * q * (double)bunch[j].harm / (double)p.H, &sp, &cp);
+      sincospi(-2.0 * q * hj / (double)p.H, &sp, &cp);
       const double zr = a * cp - b * sp, zi = a * sp + b * cp;
       double st, ct;
       sincospi(-2.0 * (double)(((int64_t)j * k) % M) / (double)M, &st, &ct);
       re += zr * ct - zi * st;
       im += zr * st + zi * ct;
+      double sq, cq;
+      sincospi(-2.0 * fk * hj / (double)p.H, &sq, &cq);
+      qre += u * cq;
+      qim += u * sq;
     }
     amp[pl * M + k] = sqrt(re * re + im * im);
     arg[pl * M + k] = atan2(re, im);
+    qre /= (double)M;
+    qim /= (double)M;
+    iq_amp[pl * M + k] = hypot(qre, qim);
+    iq_arg[pl * M + k] = atan2(qim, qre);
   }
   if (blockIdx.x == 0)
     for (int j = threadIdx.x; j < M; j += blockDim.x) aver[pl * M + j] = mom[j].mean[iu];
@@ -57,7 +72,7 @@ __global__ void k_cbm_fit(const double* __restrict__ hist, int M, int first, int
                           double interval, double t0, double* rate) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= 3 * M) return;
-  const size_t stride = (size_t)3 * M * 3;  // one record: amp, arg, aver of 3 planes
+  const size_t stride = (size_t)kCbmRecord * M;  // one record
   double W = 0, wm_x = 0, wm_y = 0;
   for (int n = 0; n < dim; ++n) {
     const double x = n * interval, y = log(hist[(size_t)(first + n) * stride + e]);
@@ -78,19 +93,21 @@ __global__ void k_cbm_fit(const double* __restrict__ hist, int M, int first, int
 }
 
 cudaError_t launch_cbm_record(Handle& h, const CbmParams& p, int rec) {
-  double* base = h.d.cbm + (size_t)rec * 9 * p.M;
+  double* base = h.d.cbm + (size_t)rec * kCbmRecord * p.M;
   const int threads = 128;
   dim3 grid((p.M + threads - 1) / threads, 3);
   k_cbm_record<<<grid, threads, 0, h.stream>>>(h.d.mom, h.d.bunch, p, base, base + 3 * p.M,
-                                               base + 6 * p.M);
+                                               base + 6 * p.M, base + 9 * p.M,
+                                               base + 12 * p.M);
   return cudaGetLastError();
 }
 
-cudaError_t launch_cbm_fit(Handle& h, int M, int first, int dim, double interval, double t0,
-                           double* rate) {
+// method 0: the DFT amplitudes, 1: the IQ amplitudes
+cudaError_t launch_cbm_fit(Handle& h, int method, int M, int first, int dim, double interval,
+                           double t0, double* rate) {
   const int threads = 128;
-  k_cbm_fit<<<(3 * M + threads - 1) / threads, threads, 0, h.stream>>>(h.d.cbm, M, first, dim,
-                                                                       interval, t0, rate);
+  k_cbm_fit<<<(3 * M + threads - 1) / threads, threads, 0, h.stream>>>(
+      h.d.cbm + (method ? 9 * (size_t)M : 0), M, first, dim, interval, t0, rate);
   return cudaGetLastError();
 }
 

@@ -114,12 +114,14 @@ struct DeviceBufs {
   double* sr_lag = nullptr;        // M x (2B-1)
   double* sr_pot = nullptr;        // M x B (z plane, persistent)
   double* sr_green = nullptr;      // resonators x 1000 (u-independent factors)
-  // coupled-bunch mode history (cg_cbm_*): records x (amp, arg, aver) x 3 planes x M
+  // coupled-bunch mode history (cg_cbm_*): records x kCbmRecord x M
   double* cbm = nullptr;
   // scratch
   double* scratch = nullptr;
   size_t scratch_bytes = 0;
 };
+
+constexpr int kCbmRecord = 15;  // doubles per bunch in one coupled-bunch mode record
 
 // Coupled-bunch mode record constants (cbm.cu): per plane x, y, z
 struct CbmParams {

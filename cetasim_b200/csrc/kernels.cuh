@@ -72,8 +72,8 @@ bool nccl_available();
 
 // coupled-bunch mode history and growth-rate fit (cbm.cu)
 cudaError_t launch_cbm_record(Handle& h, const CbmParams& p, int rec);
-cudaError_t launch_cbm_fit(Handle& h, int M, int first, int dim, double interval, double t0,
-                           double* rate);
+cudaError_t launch_cbm_fit(Handle& h, int method, int M, int first, int dim, double interval,
+                           double t0, double* rate);
 
 // field surrogate (surrogate.cu)
 cudaError_t prepare_surrogate();

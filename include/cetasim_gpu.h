@@ -377,8 +377,8 @@ int cg_autotune_pipeline(cg_handle* h, int turn0, int reps, int* shape, double* 
 /* ---- coupled-bunch mode history and growth rates (MPBeam::GetCBMGR,
  * MPBeam.cpp:1496-1575 "ideal" method, fit MPBeam.cpp:1781-1830) ---- */
 
-/* Device history for `capacity` records (3 x 3 x M doubles each); clears
- * any previous one.  Freed with the beam. */
+/* Device history for `capacity` records (15 x M doubles each); clears any
+ * previous one.  Freed with the beam. */
 int cg_cbm_init(cg_handle* h, int capacity);
 /* Appends one record (enqueued on h's stream, no host round trip): the bunch
  * moments at section 0 (as MPBeamRMSCal(0) leaves them at a print turn),
@@ -387,17 +387,21 @@ int cg_cbm_init(cg_handle* h, int capacity);
  * i sqrt(b_z) dp) exp(i phi) with b_z = bunch_sigma_z / bunch_sigma_dp (the
  * ring's beta_z when those are unset) and phi = -2 pi Q
  * h_j / H, its forward DFT over the M bunches X_k = sum_j z_j exp(-2 pi i j k
- * / M), and stores |X_k|, atan2(Re X_k, Im X_k) and the centroids. */
+ * / M), and stores |X_k|, atan2(Re X_k, Im X_k) and the centroids; also the
+ * IQ decomposition (MPBeam.cpp:1586-1625) at the scan frequencies (k + Q) f0,
+ * IQ_k = (1/M) sum_j u_j exp(-2 pi i (k + Q) h_j / H), as |IQ_k| and arg. */
 int cg_cbm_record(cg_handle* h);
 /* Records made since cg_cbm_init. */
 int cg_cbm_count(cg_handle* h, int* n);
-/* Records [first, first + count): amp, arg, aver each count x 3 x M (plane
- * major, then mode / bunch); any may be NULL. */
-int cg_cbm_history(cg_handle* h, int first, int count, double* amp, double* arg, double* aver);
+/* Records [first, first + count): amp, arg, aver, iq_amp, iq_arg each
+ * count x 3 x M (plane major, then mode / bunch); any may be NULL. */
+int cg_cbm_history(cg_handle* h, int first, int count, double* amp, double* arg, double* aver,
+                   double* iq_amp, double* iq_arg);
 /* Growth rates rate[3 x M] (1/s) per plane and mode: the least-squares line
- * through log |X_k| of records [first, last) against n x interval turns
- * (unit weights, GSL's gsl_fit_wlinear form), slope / t0. */
-int cg_cbm_growth(cg_handle* h, int first, int last, double interval, double* rate);
+ * through log |X_k| (method 0) or log |IQ_k| (method 1) of records
+ * [first, last) against n x interval turns (unit weights, GSL's
+ * gsl_fit_wlinear form), slope / t0. */
+int cg_cbm_growth(cg_handle* h, int method, int first, int last, double interval, double* rate);
 
 /* ---- turn trace (no counterpart in the reference) ---- */
 

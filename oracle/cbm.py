@@ -17,14 +17,19 @@ import numpy as np
 def cbm_record(mean, harm, H, beta, alpha, tunes, beta_z):
     """mean: (M, 6) bunch centroids (x, x', y, y', z, dp); harm: (M,) bunch
     harmonic numbers; beta, alpha: Twiss (x, y) at section 0; tunes (Qx, Qy,
-    Qz).  Returns amp, arg, aver, each (3, M): |X_k|, atan2(Re X_k, Im X_k)
-    (the reference's argument order, MPBeam.cpp:1567-1569) and the centroids."""
+    Qz).  Returns amp, arg, aver, iq_amp, iq_arg, each (3, M): |X_k|,
+    atan2(Re X_k, Im X_k) (the reference's argument order, MPBeam.cpp:1567-1569),
+    the centroids, and the IQ average at the scan frequency (k + Q) f0
+    (MPBeam.cpp:1586-1625 with the frequencies of MPBeam.cpp:153-158 and
+    f0 t0 = 1): |IQ_k| and arg IQ_k."""
     mean = np.asarray(mean, dtype=np.float64)
     harm = np.asarray(harm, dtype=np.float64)
     M = len(harm)
     amp = np.zeros((3, M))
     arg = np.zeros((3, M))
     aver = np.zeros((3, M))
+    iq_amp = np.zeros((3, M))
+    iq_arg = np.zeros((3, M))
     for pl in range(3):
         u, up = mean[:, 2 * pl], mean[:, 2 * pl + 1]
         if pl < 2:  # MPBeam.cpp:1536-1537
@@ -38,7 +43,11 @@ def cbm_record(mean, harm, H, beta, alpha, tunes, beta_z):
         amp[pl] = np.sqrt(X.real ** 2 + X.imag ** 2)
         arg[pl] = np.arctan2(X.real, X.imag)
         aver[pl] = u
-    return amp, arg, aver
+        f = np.arange(M)[:, None] + tunes[pl]
+        iq = (u[None, :] * np.exp(-2j * np.pi * f * harm[None, :] / H)).sum(axis=1) / M
+        iq_amp[pl] = np.abs(iq)
+        iq_arg[pl] = np.angle(iq)
+    return amp, arg, aver, iq_amp, iq_arg
 
 
 def wlinear_slope(x, y, w=None):

@@ -37,14 +37,15 @@ def test_record_matches_the_oracle():
     g, _ = pair(wl, parts)
     g.cbm_init(4)
     g.cbm_record()
-    amp, arg, aver = g.cbm_history()
+    amp, arg, aver, iqa, iqg = g.cbm_history()
     assert amp.shape == (1, 3, wl.n_bunches)
-    oa, og, ov = _oracle_record(wl, g)
-    scale = oa.max(axis=1, keepdims=True)
-    assert np.max(np.abs(amp[0] - oa) / scale) < 1e-11
-    big = oa > 1e-6 * scale  # phases of the modes that carry the signal
-    dphi = np.angle(np.exp(1j * (arg[0] - og)))
-    assert np.max(np.abs(dphi[big])) < 1e-9
+    oa, og, ov, oqa, oqg = _oracle_record(wl, g)
+    for dev_a, dev_g, ora_a, ora_g in ((amp[0], arg[0], oa, og), (iqa[0], iqg[0], oqa, oqg)):
+        scale = ora_a.max(axis=1, keepdims=True)
+        assert np.max(np.abs(dev_a - ora_a) / scale) < 1e-11
+        big = ora_a > 1e-6 * scale  # phases of the modes that carry the signal
+        dphi = np.angle(np.exp(1j * (dev_g - ora_g)))
+        assert np.max(np.abs(dphi[big])) < 1e-9
     assert np.array_equal(aver[0], ov)
 
 
@@ -62,10 +63,11 @@ def test_growth_of_a_synthetic_mode():
         a = 1e-6 * np.exp(rate * t0 * interval * n)
         g.upload_beam(_with_mode(base, 3, a, wl.n_bunches))
         g.cbm_record()
-    amp, _, _ = g.cbm_history()
-    dev = g.cbm_growth(2, n_rec, interval)
-    ora = cbm.cbm_growth(amp, 2, n_rec, interval, t0)
-    assert np.allclose(dev, ora, rtol=1e-9, atol=1e-6, equal_nan=True)
-    # the x mode the centroids carry (bin M - 3 after the -i rotation) grows at the set rate
-    k = int(np.argmax(amp[-1, 0]))
-    assert abs(dev[0, k] / rate - 1) < 1e-3
+    amp, _, _, iqa, _ = g.cbm_history()
+    for method, hist in ((0, amp), (1, iqa)):
+        dev = g.cbm_growth(2, n_rec, interval, method)
+        ora = cbm.cbm_growth(hist, 2, n_rec, interval, t0)
+        assert np.allclose(dev, ora, rtol=1e-9, atol=1e-6, equal_nan=True)
+        # the x mode the centroids carry grows at the set rate
+        k = int(np.argmax(hist[-1, 0]))
+        assert abs(dev[0, k] / rate - 1) < 1e-3

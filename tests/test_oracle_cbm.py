@@ -14,11 +14,14 @@ def test_pure_mode_lands_in_its_bin():
     # alpha = 0, x / sqrt(b) = cos and sqrt(b) x' = sin: z_j = cos - i sin
     mean[:, 0] = np.sqrt(beta[0]) * np.cos(2 * np.pi * mu * j / M)
     mean[:, 1] = np.sin(2 * np.pi * mu * j / M) / np.sqrt(beta[0])
-    amp, arg, aver = cbm.cbm_record(mean, harm, H, beta, alpha, tunes, 1.0)
+    amp, arg, aver, iq_amp, _ = cbm.cbm_record(mean, harm, H, beta, alpha, tunes, 1.0)
     # z_j = cos - i sin = exp(-2 pi i mu j / M): all weight in bin M - mu
     assert abs(amp[0, M - mu] - M) < 1e-12
     assert np.max(np.delete(amp[0], M - mu)) < 1e-12
     assert np.array_equal(aver[0], mean[:, 0])
+    # the IQ scan at (k + 0) f0 over uniform bunches sees the cos pattern in bins mu, M - mu
+    half = np.sqrt(beta[0]) / 2
+    assert abs(iq_amp[0, mu] - half) < 1e-12 and abs(iq_amp[0, M - mu] - half) < 1e-12
 
 
 def test_fit_is_the_least_squares_slope():
