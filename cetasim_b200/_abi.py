@@ -169,6 +169,7 @@ EXPORTS = [
     ("cg_cbm_count", I, [C.c_void_p, C.POINTER(C.c_int)]),
     ("cg_cbm_history", I, [C.c_void_p, I, I] + [C.c_void_p] * 5),
     ("cg_cbm_growth", I, [C.c_void_p, I, I, I, C.c_double, C.c_void_p]),
+    ("cg_cbm_hilbert", I, [C.c_void_p, I, I, C.c_double] + [C.c_void_p] * 4),
     ("cg_autotune_pipeline", I, [C.c_void_p, I, I, C.c_void_p, C.c_void_p]),
     ("cg_set_kick_variant", I, [C.c_void_p, I]),
     ("cg_autotune", I, [C.c_void_p, I, I, PI, PD]),

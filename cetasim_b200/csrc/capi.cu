@@ -1067,10 +1067,7 @@ int cg_cbm_init(cg_handle* H, int capacity) {
   return CG_OK;
 }
 
-int cg_cbm_record(cg_handle* H) {
-  STAGE_PROLOGUE
-  if (!h.d.cbm) return fail(&h, CG_ERR_NOT_READY, "cg_cbm_init first");
-  if (h.cbm_n >= h.cbm_cap) return fail(&h, CG_ERR_INVALID, "CBM history full");
+static CbmParams cbm_params(const Handle& h) {
   const SectionDev& s0 = h.sec_dev_host[0];
   const cg_config& c = h.cfg;
   CbmParams p;
@@ -1090,6 +1087,14 @@ int cg_cbm_record(cg_handle* H) {
   p.tune[2] = c.ring.work_qz;
   p.H = c.ring.harmonics;
   p.M = h.M;
+  return p;
+}
+
+int cg_cbm_record(cg_handle* H) {
+  STAGE_PROLOGUE
+  if (!h.d.cbm) return fail(&h, CG_ERR_NOT_READY, "cg_cbm_init first");
+  if (h.cbm_n >= h.cbm_cap) return fail(&h, CG_ERR_INVALID, "CBM history full");
+  const CbmParams p = cbm_params(h);
   // the moments at section 0, as the reference's print turn holds them
   cudaError_t e = launch_moments(h, 0);
   if (e == cudaSuccess) e = exchange_moments(h);
@@ -1138,6 +1143,45 @@ int cg_cbm_growth(cg_handle* H, int method, int first, int last, double interval
   if (e == cudaSuccess) e = cudaStreamSynchronize(h.stream);
   dfree(d_rate);
   if (e != cudaSuccess) return cuda_fail(&h, e, "CBM fit");
+  return check_status(h);
+}
+
+int cg_cbm_hilbert(cg_handle* H, int first, int last, double interval, double* mode_rate,
+                   double* bunch_rate, double* hamp, double* ana) {
+  STAGE_PROLOGUE
+  const int N = h.cbm_n;
+  if (N < 2 || first < 0 || last > N || last - first < 2 || !(interval > 0))
+    return fail(&h, CG_ERR_INVALID, "bad fit range");
+  if (N > 65535) return fail(&h, CG_ERR_INVALID, "more than 65535 records");
+  const size_t per = (size_t)3 * h.M * N;
+  double2 *d_spec = nullptr, *d_ana = nullptr;
+  double *d_hamp = nullptr, *d_babs = nullptr, *d_rate = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (dalloc(&d_spec, per) || dalloc(&d_ana, per) || dalloc(&d_hamp, per) ||
+      dalloc(&d_babs, per) || dalloc(&d_rate, (size_t)6 * h.M)) {
+    dfree(d_spec); dfree(d_ana); dfree(d_hamp); dfree(d_babs); dfree(d_rate);
+    return fail(&h, CG_ERR_OOM, "Hilbert scratch");
+  }
+  const CbmParams p = cbm_params(h);
+  const double t0 = h.cfg.ring.t0;
+  e = launch_cbm_hilbert(h, p, N, d_spec, d_ana, d_hamp, d_babs);
+  if (e == cudaSuccess)
+    e = launch_cbm_fit_plain(h, d_hamp, h.M, first, last - first, interval, t0, d_rate);
+  if (e == cudaSuccess)
+    e = launch_cbm_fit_plain(h, d_babs, h.M, first, last - first, interval, t0,
+                             d_rate + 3 * h.M);
+  const size_t rb = sizeof(double) * 3 * h.M;
+  if (e == cudaSuccess && mode_rate)
+    e = cudaMemcpyAsync(mode_rate, d_rate, rb, cudaMemcpyDeviceToHost, h.stream);
+  if (e == cudaSuccess && bunch_rate)
+    e = cudaMemcpyAsync(bunch_rate, d_rate + 3 * h.M, rb, cudaMemcpyDeviceToHost, h.stream);
+  if (e == cudaSuccess && hamp)
+    e = cudaMemcpyAsync(hamp, d_hamp, sizeof(double) * per, cudaMemcpyDeviceToHost, h.stream);
+  if (e == cudaSuccess && ana)
+    e = cudaMemcpyAsync(ana, d_ana, 2 * sizeof(double) * per, cudaMemcpyDeviceToHost, h.stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h.stream);
+  dfree(d_spec); dfree(d_ana); dfree(d_hamp); dfree(d_babs); dfree(d_rate);
+  if (e != cudaSuccess) return cuda_fail(&h, e, "Hilbert method");
   return check_status(h);
 }
 

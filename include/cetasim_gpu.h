@@ -402,6 +402,18 @@ int cg_cbm_history(cg_handle* h, int first, int count, double* amp, double* arg,
  * [first, last) against n x interval turns (unit weights, GSL's
  * gsl_fit_wlinear form), slope / t0. */
 int cg_cbm_growth(cg_handle* h, int method, int first, int last, double interval, double* rate);
+/* The Hilbert method (GetAnalyticalWithFilter / GetHilbertAnalytical,
+ * MPBeam.cpp:1892-1989, modes :1680-1725) over all N records made: per bunch
+ * and plane the analytic signal a_n of the centroid history (forward DFT over
+ * the records, positive frequencies doubled, the even-N Nyquist term kept
+ * single, negative ones zeroed, inverse DFT / N), the modes of each record
+ * from x = Re a, x' = -Im a as in cg_cbm_record, and the fits over records
+ * [first, last): mode_rate[3 x M] of log |X_k| (CBMHTGR*), bunch_rate[3 x M]
+ * of log |a_n| per bunch (BGR*), 1/s.  hamp (N x 3 x M) and ana (N x 3 x M
+ * complex, re/im interleaved) are optional outputs.  The DFTs are direct
+ * (N^2 per bunch and plane): at most 65535 records. */
+int cg_cbm_hilbert(cg_handle* h, int first, int last, double interval, double* mode_rate,
+                   double* bunch_rate, double* hamp, double* ana);
 
 /* ---- turn trace (no counterpart in the reference) ---- */
 

@@ -82,3 +82,39 @@ def cbm_growth(amp_hist, first, last, interval, t0):
         for k in range(M):
             rate[pl, k] = wlinear_slope(x, np.log(amp_hist[first:last, pl, k])) / t0
     return rate
+
+
+def analytic(u):
+    """GetHilbertAnalytical (MPBeam.cpp:1937-1989) without the Gaussian filter,
+    which the reference builds but does not apply: forward FFT, terms
+    1 .. N/2 doubled (the N/2 term of an even N kept single), terms above N/2
+    zeroed, inverse FFT with 1/N."""
+    u = np.asarray(u, dtype=np.float64)
+    N = len(u)
+    w = np.zeros(N)
+    w[0] = 1.0
+    w[1:N // 2 + 1] = 2.0
+    if N % 2 == 0:
+        w[N // 2] = 1.0
+    return np.fft.ifft(np.fft.fft(u) * w)
+
+
+def cbm_hilbert(aver_hist, harm, H, beta, alpha, tunes, beta_z, first, last, interval, t0):
+    """The Hilbert method of GetCBMGR (MPBeam.cpp:1680-1725, 1781-1830):
+    aver_hist (N, 3, M) centroid records.  Returns mode rates (3, M), bunch
+    rates (3, M), mode amplitudes (N, 3, M), analytic signals (N, 3, M)."""
+    aver_hist = np.asarray(aver_hist, dtype=np.float64)
+    N, _, M = aver_hist.shape
+    ana = np.zeros((N, 3, M), dtype=np.complex128)
+    for pl in range(3):
+        for j in range(M):
+            ana[:, pl, j] = analytic(aver_hist[:, pl, j])
+    hamp = np.zeros((N, 3, M))
+    for n in range(N):
+        mean = np.zeros((M, 6))
+        for pl in range(3):
+            mean[:, 2 * pl] = ana[n, pl].real
+            mean[:, 2 * pl + 1] = -ana[n, pl].imag
+        hamp[n] = cbm_record(mean, harm, H, beta, alpha, tunes, beta_z)[0]
+    return (cbm_growth(hamp, first, last, interval, t0),
+            cbm_growth(np.abs(ana), first, last, interval, t0), hamp, ana)

@@ -71,3 +71,42 @@ def test_growth_of_a_synthetic_mode():
         # the x mode the centroids carry grows at the set rate
         k = int(np.argmax(hist[-1, 0]))
         assert abs(dev[0, k] / rate - 1) < 1e-3
+
+
+def test_hilbert_method_matches_the_oracle():
+    """Records of betatron-like turn-by-turn centroids: the device's analytic
+    signals, mode amplitudes and both fits against the oracle on the same
+    centroid history."""
+    wl = small("fast_ion", 0.02)
+    base = [c - c.mean(axis=1, keepdims=True) for c in particles(wl, seed=33)]
+    g, _ = pair(wl, base)
+    r = wl.cfg.ring
+    t0, interval, n_rec = r.t0, 1, 40
+    g.cbm_init(n_rec)
+    M = wl.n_bunches
+    for n in range(n_rec):
+        parts = []
+        for j, c in enumerate(base):
+            c = c.copy()
+            ph = 2 * np.pi * (r.work_qx * n + 3 * j / M)
+            c[0] += 1e-6 * np.exp(2e-2 * n) * np.cos(ph)
+            c[2] += 5e-7 * np.sin(ph + 0.2 * j)
+            c[4] += 1e-4 * np.cos(2 * np.pi * r.work_qz * n + j)
+            parts.append(c)
+        g.upload_beam(parts)
+        g.cbm_record()
+    _, _, aver, _, _ = g.cbm_history()
+    mr, br, hamp, ana = g.cbm_hilbert(5, n_rec - 5, interval)
+    s0 = wl.sections[0]
+    omr, obr, ohamp, oana = cbm.cbm_hilbert(
+        aver, wl.harm, r.harmonics, (s0.beta_x, s0.beta_y), (s0.alpha_x, s0.alpha_y),
+        (r.work_qx, r.work_qy, r.work_qz), r.beta_z, 5, n_rec - 5, interval, t0)
+    scale = np.abs(oana).max(axis=0, keepdims=True)
+    assert np.max(np.abs(ana - oana) / scale) < 1e-10
+    assert np.max(np.abs(hamp - ohamp) / ohamp.max(axis=(0, 2), keepdims=True)) < 1e-10
+    # rates of the modes that carry signal through the fit window (the others
+    # fit the logarithm of rounding noise)
+    live = ohamp[5:n_rec - 5].min(axis=0) > 1e-6 * ohamp.max(axis=(0, 2))[:, None]
+    assert live.sum() > 10
+    assert np.allclose(mr[live], omr[live], rtol=1e-7, atol=1e-3)
+    assert np.allclose(br, obr, rtol=1e-7, atol=1e-3)

@@ -37,3 +37,9 @@ def test_growth_recovers_an_exponential():
     amp = np.exp(g * t0 * interval * n)[:, None, None] * np.ones((1, 3, 4))
     rate = cbm.cbm_growth(amp, 5, 30, interval, t0)
     assert np.allclose(rate, g, rtol=1e-9)
+
+
+def test_analytic_signal_of_a_sinusoid():
+    n = np.arange(64)
+    a = cbm.analytic(np.cos(2 * np.pi * 5 * n / 64 + 0.3))
+    assert np.allclose(a, np.exp(1j * (2 * np.pi * 5 * n / 64 + 0.3)), atol=1e-12)
