@@ -82,6 +82,7 @@ class Config(C.Structure):
         ("flag_fir", I), ("seed", C.c_uint64),
         ("n_turns", I), ("bunch_info_print_interval", I), ("bunch_emit_x", D), ("bunch_emit_y", D),
         ("bunch_sigma_z", D), ("bunch_sigma_dp", D),
+        ("growth_fit_start", I), ("growth_fit_end", I), ("run_cbmgr", C.c_char * 256),
     ]
 
 
@@ -169,7 +170,7 @@ EXPORTS = [
     ("cg_cbm_count", I, [C.c_void_p, C.POINTER(C.c_int)]),
     ("cg_cbm_history", I, [C.c_void_p, I, I] + [C.c_void_p] * 5),
     ("cg_cbm_growth", I, [C.c_void_p, I, I, I, C.c_double, C.c_void_p]),
-    ("cg_cbm_hilbert", I, [C.c_void_p, I, I, C.c_double] + [C.c_void_p] * 4),
+    ("cg_cbm_hilbert", I, [C.c_void_p, I, I, C.c_double] + [C.c_void_p] * 5),
     ("cg_autotune_pipeline", I, [C.c_void_p, I, I, C.c_void_p, C.c_void_p]),
     ("cg_set_kick_variant", I, [C.c_void_p, I]),
     ("cg_autotune", I, [C.c_void_p, I, I, PI, PD]),

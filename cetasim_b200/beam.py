@@ -197,17 +197,18 @@ class MPBeam:
 
     def cbm_hilbert(self, first: int, last: int, interval: float):
         """The Hilbert method over all records: (mode rates (3, M), bunch
-        rates (3, M), mode amplitudes (N, 3, M), analytic signals (N, 3, M))."""
+        rates (3, M), mode amplitudes and phases (N, 3, M), analytic signals
+        (N, 3, M))."""
         n = C.c_int()
         self._check(self.lib.cg_cbm_count(self.h, C.byref(n)))
         M = self.wl.n_bunches
         mr, br = np.zeros((3, M)), np.zeros((3, M))
-        hamp = np.zeros((n.value, 3, M))
+        hamp, harg = np.zeros((n.value, 3, M)), np.zeros((n.value, 3, M))
         ana = np.zeros((n.value, 3, M), dtype=np.complex128)
         self._check(self.lib.cg_cbm_hilbert(self.h, first, last, float(interval), _abi.ptr(mr),
-                                            _abi.ptr(br), _abi.ptr(hamp),
+                                            _abi.ptr(br), _abi.ptr(hamp), _abi.ptr(harg),
                                             ana.ctypes.data_as(C.c_void_p)))
-        return mr, br, hamp, ana
+        return mr, br, hamp, harg, ana
 
     def autotune_pipeline(self, turn0: int, reps: int = 5):
         """Times whole turns with each pipeline shape, restores the beam and

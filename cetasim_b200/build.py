@@ -72,14 +72,14 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
 
 
 CLI = os.path.join(HERE, "cetasim_mp")
-HOST_SOURCES = ["mpbeam.cpp", "cetasim_mp.cpp"]
+HOST_SOURCES = ["mpbeam.cpp", "cbm_writer.cpp", "cetasim_mp.cpp"]
 
 
 def build_host(force: bool = False, verbose: bool = False) -> str:
     """The C++ host layer (MPBeam-named wrapper) and the cetasim_mp driver,
     linked against the in-tree libcetagpu.so."""
     hdir = os.path.join(HERE, "host")
-    deps = [os.path.join(hdir, s) for s in HOST_SOURCES + ["mpbeam.hpp"]] + [LIB]
+    deps = [os.path.join(hdir, s) for s in HOST_SOURCES + ["mpbeam.hpp", "cbm_writer.hpp"]] + [LIB]
     if not force and not _stale(CLI, deps):
         return CLI
     cmd = ["g++", "-O2", "-std=c++17", "-o", CLI + ".tmp",

@@ -1147,7 +1147,7 @@ int cg_cbm_growth(cg_handle* H, int method, int first, int last, double interval
 }
 
 int cg_cbm_hilbert(cg_handle* H, int first, int last, double interval, double* mode_rate,
-                   double* bunch_rate, double* hamp, double* ana) {
+                   double* bunch_rate, double* hamp, double* harg, double* ana) {
   STAGE_PROLOGUE
   const int N = h.cbm_n;
   if (N < 2 || first < 0 || last > N || last - first < 2 || !(interval > 0))
@@ -1155,16 +1155,16 @@ int cg_cbm_hilbert(cg_handle* H, int first, int last, double interval, double* m
   if (N > 65535) return fail(&h, CG_ERR_INVALID, "more than 65535 records");
   const size_t per = (size_t)3 * h.M * N;
   double2 *d_spec = nullptr, *d_ana = nullptr;
-  double *d_hamp = nullptr, *d_babs = nullptr, *d_rate = nullptr;
+  double *d_hamp = nullptr, *d_harg = nullptr, *d_babs = nullptr, *d_rate = nullptr;
   cudaError_t e = cudaSuccess;
   if (dalloc(&d_spec, per) || dalloc(&d_ana, per) || dalloc(&d_hamp, per) ||
-      dalloc(&d_babs, per) || dalloc(&d_rate, (size_t)6 * h.M)) {
-    dfree(d_spec); dfree(d_ana); dfree(d_hamp); dfree(d_babs); dfree(d_rate);
+      dalloc(&d_harg, per) || dalloc(&d_babs, per) || dalloc(&d_rate, (size_t)6 * h.M)) {
+    dfree(d_spec); dfree(d_ana); dfree(d_hamp); dfree(d_harg); dfree(d_babs); dfree(d_rate);
     return fail(&h, CG_ERR_OOM, "Hilbert scratch");
   }
   const CbmParams p = cbm_params(h);
   const double t0 = h.cfg.ring.t0;
-  e = launch_cbm_hilbert(h, p, N, d_spec, d_ana, d_hamp, d_babs);
+  e = launch_cbm_hilbert(h, p, N, d_spec, d_ana, d_hamp, d_harg, d_babs);
   if (e == cudaSuccess)
     e = launch_cbm_fit_plain(h, d_hamp, h.M, first, last - first, interval, t0, d_rate);
   if (e == cudaSuccess)
@@ -1177,10 +1177,12 @@ int cg_cbm_hilbert(cg_handle* H, int first, int last, double interval, double* m
     e = cudaMemcpyAsync(bunch_rate, d_rate + 3 * h.M, rb, cudaMemcpyDeviceToHost, h.stream);
   if (e == cudaSuccess && hamp)
     e = cudaMemcpyAsync(hamp, d_hamp, sizeof(double) * per, cudaMemcpyDeviceToHost, h.stream);
+  if (e == cudaSuccess && harg)
+    e = cudaMemcpyAsync(harg, d_harg, sizeof(double) * per, cudaMemcpyDeviceToHost, h.stream);
   if (e == cudaSuccess && ana)
     e = cudaMemcpyAsync(ana, d_ana, 2 * sizeof(double) * per, cudaMemcpyDeviceToHost, h.stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h.stream);
-  dfree(d_spec); dfree(d_ana); dfree(d_hamp); dfree(d_babs); dfree(d_rate);
+  dfree(d_spec); dfree(d_ana); dfree(d_hamp); dfree(d_harg); dfree(d_babs); dfree(d_rate);
   if (e != cudaSuccess) return cuda_fail(&h, e, "Hilbert method");
   return check_status(h);
 }

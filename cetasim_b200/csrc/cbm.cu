@@ -136,11 +136,12 @@ __global__ void k_cbm_analytic(const double* __restrict__ hist, int M, int N, do
   }
 }
 
-// One thread per (mode k, plane, record n = blockIdx.z): |X_k| of the
-// analytic amplitudes; also |a_n| of bunch k for the bunch growth rates.
+// One thread per (mode k, plane, record n = blockIdx.z): |X_k| and
+// atan2(Re, Im) of the analytic amplitudes; also |a_n| of bunch k for the
+// bunch growth rates.
 __global__ void k_cbm_hilbert_modes(const double2* __restrict__ ana,
                                     const BunchDev* __restrict__ bunch, CbmParams p,
-                                    double* hamp, double* babs) {
+                                    double* hamp, double* harg, double* babs) {
   const int pl = blockIdx.y, M = p.M, n = blockIdx.z;
   const double sb = p.sqrt_beta[pl], ab = p.alpha_sqrt[pl], q = p.tune[pl];
   const double sgn = pl == 2 ? 1.0 : -1.0;
@@ -159,6 +160,7 @@ __global__ void k_cbm_hilbert_modes(const double2* __restrict__ ana,
       im += zr * st + zi * ct;
     }
     hamp[((size_t)n * 3 + pl) * M + k] = sqrt(re * re + im * im);
+    harg[((size_t)n * 3 + pl) * M + k] = atan2(re, im);
     babs[((size_t)n * 3 + pl) * M + k] = hypot(an[k].x, an[k].y);
   }
 }
@@ -189,13 +191,13 @@ __global__ void k_cbm_fit_plain(const double* __restrict__ a, int M, int first, 
 }
 
 cudaError_t launch_cbm_hilbert(Handle& h, const CbmParams& p, int N, double2* spec, double2* ana,
-                               double* hamp, double* babs) {
+                               double* hamp, double* harg, double* babs) {
   k_cbm_analytic<<<dim3(p.M, 3), 256, 0, h.stream>>>(h.d.cbm, p.M, N, spec, ana);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   const int threads = 128;
   k_cbm_hilbert_modes<<<dim3((p.M + threads - 1) / threads, 3, N), threads, 0, h.stream>>>(
-      ana, h.d.bunch, p, hamp, babs);
+      ana, h.d.bunch, p, hamp, harg, babs);
   return cudaGetLastError();
 }
 

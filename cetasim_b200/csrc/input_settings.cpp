@@ -9,6 +9,7 @@
 // lower-cased with blanks removed, lines without '=' ignored, a leading '!'
 // makes the key unmatched (a comment), later duplicates win, trailing tokens
 // (e.g. "// comment") are ignored once the expected count is read.
+#include <cstdio>
 #include <algorithm>
 #include <cctype>
 #include <cmath>
@@ -221,6 +222,22 @@ extern "C" int cg_config_from_input(const char* path, cg_config* cfg, int* n_bun
     cfg->flag_fir = flag("runfirbunchbybunchfeedbackflag");
     cfg->n_turns = flag("runnturns");
     cfg->bunch_info_print_interval = flag("runbunchinfoprintinterval");
+    cfg->growth_fit_start = flag("rungrowthratefittingstart");
+    cfg->growth_fit_end = flag("rungrowthratefittingend");
+    if (has("runcbmgr") && !get("runcbmgr").v.empty()) {
+      // the output base name, as given (ReadInputSettings.cpp:865-868)
+      const std::string& name = get("runcbmgr").v.at(0);
+      std::snprintf(cfg->run_cbmgr, sizeof cfg->run_cbmgr, "%s", name.c_str());
+      // the fit window checks of ReadInputSettings.cpp:946-956
+      if (cfg->growth_fit_start >= cfg->growth_fit_end) {
+        g_parse_error = "wrong settings: growthRateFittingEnd is smaller growthRateFittingStart";
+        return CG_ERR_INVALID;
+      }
+      if (cfg->growth_fit_end > cfg->n_turns) {
+        g_parse_error = "wrong settings: nTurns small than growthRateFittingEnd";
+        return CG_ERR_INVALID;
+      }
+    }
     cfg->seed = has("runrandomseed") ? (uint64_t)std::stoull(get("runrandomseed").v.at(0)) : 20240101ull;
     // bunch
     double kappa = D(get("bunchkappa"), 0);

@@ -77,7 +77,7 @@ cudaError_t launch_cbm_fit(Handle& h, int method, int M, int first, int dim, dou
 // the Hilbert method over records [0, N): spec N x 3 x M scratch, ana the
 // analytic signals, hamp the modes' amplitudes, babs |a| per bunch (N x 3 x M)
 cudaError_t launch_cbm_hilbert(Handle& h, const CbmParams& p, int N, double2* spec, double2* ana,
-                               double* hamp, double* babs);
+                               double* hamp, double* harg, double* babs);
 cudaError_t launch_cbm_fit_plain(Handle& h, const double* a, int M, int first, int dim,
                                  double interval, double t0, double* rate);
 

@@ -4,7 +4,8 @@
 // reads input.dat (and the twiss/BBR files it names), generates the bunches,
 // runs runNTurns turns on the GPU and writes result.sdds with the per-turn
 // beam averages of MPBeam::Run (MPBeam.cpp:902-991, 1107-1158: the column
-// subset this library computes).
+// subset this library computes) and, when runCBMGR names a file, the
+// coupled-bunch growth rates of MPBeam::GetCBMGR.
 #include <sys/time.h>
 
 #include <cmath>
@@ -16,6 +17,7 @@
 #include <iostream>
 #include <string>
 
+#include "cbm_writer.hpp"
 #include "mpbeam.hpp"
 
 static double wall() {
@@ -49,9 +51,21 @@ int main(int argc, char** argv) {
       fout << "&column name=" << c << (std::strcmp(c, "Turns") ? ", type=float, &end\n" : ", type=long, &end\n");
     fout << "&data mode=ascii, &end\n! page number 1\n" << in.cfg.n_turns << "\n";
     const int M = beam.n_bunches();
+    // coupled-bunch growth rates (MPBeam::GetCBMGR at every print turn, the
+    // file after the last one, MPBeam.cpp:1161-1171)
+    const int interval = in.cfg.bunch_info_print_interval;
+    const bool cbm = in.cfg.run_cbmgr[0] != 0 && interval > 0;
+    if (cbm) {
+      const int rc = cg_cbm_init(beam.handle(), in.cfg.n_turns / interval + 1);
+      if (rc) throw cetasim::Error(rc, cg_last_error(beam.handle()));
+    }
     for (int n = 0; n < in.cfg.n_turns; ++n) {
       beam.RunTurns(n, 1);
       beam.MPBeamRMSCal(0);
+      if (cbm && n % interval == 0) {
+        const int rc = cg_cbm_record(beam.handle());
+        if (rc) throw cetasim::Error(rc, cg_last_error(beam.handle()));
+      }
       auto m = beam.Moments();
       if (n % 10 == 0) std::cout << n << "  turns, bunch_0 transmission: " << m[0].transmission << "\n";
       double q = 0;
@@ -75,6 +89,9 @@ int main(int argc, char** argv) {
       for (int d : ord) fout << std::setw(15) << std::sqrt(rm[d] / M);
       fout << "\n";
     }
+    if (cbm)
+      cetasim::write_cbmgr(beam.handle(), in.cfg.run_cbmgr, M, in.bunch_harm, interval,
+                           in.cfg.growth_fit_start, in.cfg.growth_fit_end);
     std::cout << "End of Tracking " << in.cfg.n_turns << "Turns\n";
     std::cout << "total time " << wall() - t0 << " s\n";
   } catch (const cetasim::Error& e) {

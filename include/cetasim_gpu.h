@@ -150,6 +150,10 @@ typedef struct cg_config {
   double bunch_emit_x, bunch_emit_y; /* bunchEmittance/(1+kappa), x kappa (ReadInputSettings.cpp:1012-1016) */
   double bunch_sigma_z;          /* bunchRmsBunchLength */
   double bunch_sigma_dp;         /* bunchRmsEnergySpread */
+  int growth_fit_start;          /* runGrowthRateFittingStart (turns) */
+  int growth_fit_end;            /* runGrowthRateFittingEnd (turns) */
+  char run_cbmgr[256];           /* runCBMGR: base name of the coupled-bunch growth-rate
+                                    file ("" off) */
 } cg_config;
 
 /* Per-bunch moments, the fields MPBunch::GetMPBunchRMS sets
@@ -409,11 +413,12 @@ int cg_cbm_growth(cg_handle* h, int method, int first, int last, double interval
  * single, negative ones zeroed, inverse DFT / N), the modes of each record
  * from x = Re a, x' = -Im a as in cg_cbm_record, and the fits over records
  * [first, last): mode_rate[3 x M] of log |X_k| (CBMHTGR*), bunch_rate[3 x M]
- * of log |a_n| per bunch (BGR*), 1/s.  hamp (N x 3 x M) and ana (N x 3 x M
- * complex, re/im interleaved) are optional outputs.  The DFTs are direct
- * (N^2 per bunch and plane): at most 65535 records. */
+ * of log |a_n| per bunch (BGR*), 1/s.  hamp, harg (N x 3 x M: |X_k| and
+ * atan2(Re X_k, Im X_k)) and ana (N x 3 x M complex, re/im interleaved) are
+ * optional outputs.  The DFTs are direct (N^2 per bunch and plane): at most
+ * 65535 records. */
 int cg_cbm_hilbert(cg_handle* h, int first, int last, double interval, double* mode_rate,
-                   double* bunch_rate, double* hamp, double* ana);
+                   double* bunch_rate, double* hamp, double* harg, double* ana);
 
 /* ---- turn trace (no counterpart in the reference) ---- */
 

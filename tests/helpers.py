@@ -92,3 +92,39 @@ def moments_close(mg, mo, rtol):
             if not e <= rtol:
                 bad.append((j, f, e))
     return bad
+
+
+def write_input(d, n_turns=60, interval=5, cbmgr="cbmgr", fit=(10, 50), bunches=40,
+                macro=200):
+    """A small MP-model input.dat (the reference's key = value format) and its
+    twiss file in directory d: one train of `bunches` bunches every second
+    bucket of a 480-bucket ring, two sections, no ions or wakes."""
+    import os
+    harm = 480
+    gap = harm - 2 * bunches
+    lines = [
+        "runCalSetting = 2", f"runNTurns = {n_turns}", f"runBunchInfoPrintInterval = {interval}",
+        "runSynRadDampingFlag = 1", "runBeamIonFlag = 0", "runLongRangeWake = 0",
+        "runShortRangeWake = 0", "runFIRBunchByBunchFeedbackFlag = 0", "runRandomSeed = 7",
+        f"runGrowthRateFittingStart = {fit[0]}", f"runGrowthRateFittingEnd = {fit[1]}",
+        "ringCircRing = 288.0", "ringWorkQ = 18.21 10.17", "ringChrom = 1.0 1.0",
+        "ringSynchRadDampTime = 0.02 0.02 0.01", "ringPipeAperatureX = 0.02",
+        "ringPipeAperatureY = 0.01", "ringElectronBeamEnergy = 3.0e9",
+        "ringAlphac = 3.0e-4 0 0", "ringU0 = 1.0e6", "ringSdelta0 = 1.0e-3",
+        "ringNaturalEmit = 2.0e-9", "ringCoupling = 0.01", "ringCurrent = 0.1",
+        "ringSectNum = 2", "ringTwiss = twiss.dat",
+        f"rfRingHarm = {harm}", "rfResNum = 1", f"rfResHarm = 1", "rfResVol = 2.0e6",
+        "bunchKappa = 0.01", "bunchEmittance = 2.0e-9", "bunchRmsBunchLength = 3.0e-3",
+        "bunchRmsEnergySpread = 1.0e-3", f"bunchMacroEleNumPerBunch = {macro}",
+        f"fpTotBunchNumber = {bunches}", "fpTrainNumber = 1",
+        f"fpBunchNumberPerTrain = {bunches}", f"fpTrainGaps = {gap}", "fpBunchGaps = 1",
+    ]
+    if cbmgr:
+        lines.append(f"runCBMGR = {cbmgr}")
+    with open(os.path.join(d, "input.dat"), "w") as f:
+        f.write("\n".join(lines) + "\n")
+    rows = ["0.0 10.0 0.5 0.0 0.1 0.0 0.02 5.0 -0.3 0.0 0.0 0.0 0.01 144.0 1.0 300",
+            "144.0 8.0 -0.4 3.1 0.2 0.01 0.02 6.0 0.2 2.9 0.0 0.0 0.01 144.0 1.0 300"]
+    with open(os.path.join(d, "twiss.dat"), "w") as f:
+        f.write("header\n" * 5 + "\n".join(rows) + "\n")
+    return os.path.join(d, "input.dat")

@@ -96,7 +96,7 @@ def test_hilbert_method_matches_the_oracle():
         g.upload_beam(parts)
         g.cbm_record()
     _, _, aver, _, _ = g.cbm_history()
-    mr, br, hamp, ana = g.cbm_hilbert(5, n_rec - 5, interval)
+    mr, br, hamp, harg, ana = g.cbm_hilbert(5, n_rec - 5, interval)
     s0 = wl.sections[0]
     omr, obr, ohamp, oana = cbm.cbm_hilbert(
         aver, wl.harm, r.harmonics, (s0.beta_x, s0.beta_y), (s0.alpha_x, s0.alpha_y),
