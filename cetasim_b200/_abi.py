@@ -74,6 +74,14 @@ class FirParams(C.Structure):
     ]
 
 
+MAX_RW = 32
+
+
+class RwSectors(C.Structure):
+    _fields_ = [("n", I)] + [(f, D * MAX_RW) for f in ("radius_x", "radius_y", "length",
+                                                        "beta_x", "beta_y", "num", "sigma")]
+
+
 class Config(C.Structure):
     _fields_ = [
         ("ring", Ring), ("n_sections", I), ("sections", C.POINTER(Section)), ("ion", IonParams),
@@ -83,6 +91,7 @@ class Config(C.Structure):
         ("n_turns", I), ("bunch_info_print_interval", I), ("bunch_emit_x", D), ("bunch_emit_y", D),
         ("bunch_sigma_z", D), ("bunch_sigma_dp", D),
         ("growth_fit_start", I), ("growth_fit_end", I), ("run_cbmgr", C.c_char * 256),
+        ("lr_rw", RwSectors),
     ]
 
 
@@ -165,6 +174,8 @@ EXPORTS = [
     ("cg_kick_variants", I, [PI]),
     ("cg_set_pipeline", I, [C.c_void_p, I, I, I]),
     ("cg_trace_turn", I, [C.c_void_p, I, C.c_void_p, I, C.POINTER(C.c_int)]),
+    ("cg_yokoya_factors", I, [C.c_double, C.c_double, PD]),
+    ("cg_rw_lr_wake", I, [C.c_void_p, C.c_double, C.c_double, C.c_double, PD]),
     ("cg_cbm_init", I, [C.c_void_p, I]),
     ("cg_cbm_record", I, [C.c_void_p]),
     ("cg_cbm_count", I, [C.c_void_p, C.POINTER(C.c_int)]),

@@ -9,6 +9,7 @@
 #include <string>
 #include <vector>
 #include "kernels.cuh"
+#include "rw_wake.h"
 #include "surrogate.cuh"
 
 using namespace cg;
@@ -400,10 +401,15 @@ int cg_create(const cg_config* cfg, int device, cg_handle** out) {
     double dt = trf / 2;
     int np = int(turns * cfg->ring.harmonics * trf / dt) + 2;
     std::vector<double> tab(3 * (size_t)np);
+    // resistive-wall sectors (WakeFunction.cpp:124-131): the total is BBR + RW
+    double yok[CG_MAX_RW_SECTORS][5];
+    if (cfg->lr_rw.n > 0) rw_sector_factors(cfg->lr_rw, yok);
     for (int i = 0; i < np; ++i) {
-      double w[3];
+      double w[3], rw[3] = {0, 0, 0};
       bbr_wake(cfg->lr_bbr, h.sections[0].beta_x, h.sections[0].beta_y, -i * dt, w);
-      for (int d = 0; d < 3; ++d) tab[(size_t)d * np + i] = w[d];
+      if (cfg->lr_rw.n > 0)
+        rw_lr_wake(cfg->lr_rw, yok, h.sections[0].beta_x, h.sections[0].beta_y, -i * dt, rw);
+      for (int d = 0; d < 3; ++d) tab[(size_t)d * np + i] = w[d] + rw[d];
     }
     h.lr_np = np;
     h.lr_dt = (1 * dt) - (0 * dt);

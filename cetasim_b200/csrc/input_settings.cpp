@@ -139,6 +139,37 @@ int read_bbr(const std::string& path, cg_bbr* b) {
   return CG_OK;
 }
 
+// WakeFunction::RWWakeParaReadIn (WakeFunction.cpp:292-328): a header line,
+// then per sector radius x, radius y, length, beta x, beta y, count, sigma.
+int read_rw_sectors(const std::string& path, cg_rw_sectors* s) {
+  std::ifstream fin(path);
+  if (!fin.is_open()) {
+    g_parse_error = "Error opening file: " + path;
+    return CG_ERR_INVALID;
+  }
+  std::string str;
+  std::getline(fin, str);  // the header line
+  s->n = 0;
+  while (std::getline(fin, str)) {
+    std::istringstream iss(str);
+    std::vector<double> v;
+    for (std::string w; iss >> w;) v.push_back(std::stod(w));
+    if (v.empty()) continue;
+    if (v.size() < 7) {
+      g_parse_error = "pipe sector line with fewer than 7 columns in " + path;
+      return CG_ERR_INVALID;
+    }
+    if (s->n >= CG_MAX_RW_SECTORS) {
+      g_parse_error = "more than 32 resistive-wall sectors in " + path;
+      return CG_ERR_INVALID;
+    }
+    const int i = s->n++;
+    s->radius_x[i] = v[0]; s->radius_y[i] = v[1]; s->length[i] = v[2];
+    s->beta_x[i] = v[3]; s->beta_y[i] = v[4]; s->num[i] = v[5]; s->sigma[i] = v[6];
+  }
+  return CG_OK;
+}
+
 }  // namespace
 
 extern "C" int cg_config_derive(cg_config* cfg);
@@ -311,12 +342,15 @@ extern "C" int cg_config_from_input(const char* path, cg_config* cfg, int* n_bun
     std::string base = dir_of(path);
     if (cfg->flag_lr_wake) {
       cfg->lr_turns = has("lrwnturnswaketrunction") ? Ii(get("lrwnturnswaketrunction"), 0) + 1 : 10;
+      // resistive-wall sectors and / or resonators (WakeFunction.cpp:82-89)
       if (has("lrwpipegeoinput")) {
-        g_parse_error = "resistive-wall wakes are outside the tracking path of this library";
-        return CG_ERR_UNSUPPORTED;
+        int st = read_rw_sectors(resolve(base, get("lrwpipegeoinput").v.at(0)), &cfg->lr_rw);
+        if (st) return st;
       }
-      int st = read_bbr(resolve(base, get("lrwbbrinput").v.at(0)), &cfg->lr_bbr);
-      if (st) return st;
+      if (has("lrwbbrinput")) {
+        int st = read_bbr(resolve(base, get("lrwbbrinput").v.at(0)), &cfg->lr_bbr);
+        if (st) return st;
+      }
     }
     if (cfg->flag_sr_wake) {
       cfg->sr_bins = has("srwbunchbinnum") ? (int)D(get("srwbunchbinnum"), 0) : 100;

@@ -108,6 +108,19 @@ typedef struct cg_ion_params {
 
 /* Broadband resonators (BBR input file, WakeFunction.cpp:251-290); omegas are
  * angular frequencies (file value x 2 pi). */
+/* Resistive-wall pipe sectors (LRWPipeGeoInput, WakeFunction.cpp:292-364):
+ * per sector the half apertures, length, average betas, count and
+ * conductivity. */
+#define CG_MAX_RW_SECTORS 32
+typedef struct cg_rw_sectors {
+  int n;
+  double radius_x[CG_MAX_RW_SECTORS], radius_y[CG_MAX_RW_SECTORS];
+  double length[CG_MAX_RW_SECTORS];
+  double beta_x[CG_MAX_RW_SECTORS], beta_y[CG_MAX_RW_SECTORS];
+  double num[CG_MAX_RW_SECTORS];
+  double sigma[CG_MAX_RW_SECTORS];  /* [S/m] */
+} cg_rw_sectors;
+
 typedef struct cg_bbr {
   int n;
   double l_rs[CG_MAX_RESONATORS], l_q[CG_MAX_RESONATORS], l_omega[CG_MAX_RESONATORS];
@@ -154,6 +167,8 @@ typedef struct cg_config {
   int growth_fit_end;            /* runGrowthRateFittingEnd (turns) */
   char run_cbmgr[256];           /* runCBMGR: base name of the coupled-bunch growth-rate
                                     file ("" off) */
+  cg_rw_sectors lr_rw;           /* LRWPipeGeoInput: resistive-wall sectors of the
+                                    long-range wake (n = 0: none) */
 } cg_config;
 
 /* Per-bunch moments, the fields MPBunch::GetMPBunchRMS sets
@@ -377,6 +392,20 @@ int cg_set_pipeline(cg_handle* h, int groups, int walk_ions, int ramp);
  * NULL). */
 #define CG_PIPE_SHAPES 10
 int cg_autotune_pipeline(cg_handle* h, int turn0, int reps, int* shape, double* ms);
+
+/* ---- resistive-wall wake functions (host, stateless) ---- */
+
+/* Yokoya factors of an elliptical pipe with half apertures a >= b > 0
+ * (WakeFunction::GetyokoyaFactor, WakeFunction.cpp:723-787): out[0]
+ * longitudinal, out[1], out[2] dipolar x, y, out[3], out[4] quadrupolar. */
+int cg_yokoya_factors(double a, double b, double out[5]);
+/* Long-range resistive-wall wake function of the sectors at tau <= 0
+ * (WakeFunction::GetRWLRWakeFun, WakeFunction.cpp:499-552): out[0], out[1]
+ * transverse [V/C/m] at the betas beta_ip_x, beta_ip_y of the kick point,
+ * out[2] longitudinal [V/C]; tau = 0 gives zeros.  The sectors' Yokoya
+ * factors follow RWWakeParaReadIn (WakeFunction.cpp:332-361). */
+int cg_rw_lr_wake(const cg_rw_sectors* s, double beta_ip_x, double beta_ip_y, double tau,
+                  double out[3]);
 
 /* ---- coupled-bunch mode history and growth rates (MPBeam::GetCBMGR,
  * MPBeam.cpp:1496-1575 "ideal" method, fit MPBeam.cpp:1781-1830) ---- */

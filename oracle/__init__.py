@@ -92,6 +92,15 @@ class OracleBeam:
         if not self.s:
             raise RuntimeError("or_create failed")
         self.s = C.c_void_p(self.s)
+        rws = wl.cfg.lr_rw
+        if wl.cfg.flag_lr_wake and rws.n > 0:
+            # the resistive-wall term of the long-range table, with Yokoya
+            # factors from the mpmath restatement (oracle/rw.py)
+            from . import rw
+            yok = rw.sector_factors(list(rws.radius_x[:rws.n]), list(rws.radius_y[:rws.n]))
+            flat = (C.c_double * (5 * rws.n))(*[v for f in yok for v in f])
+            if self.lib.or_lr_add_rw(self.s, flat):
+                raise RuntimeError("or_lr_add_rw failed")
 
     def close(self):
         if self.s:

@@ -690,6 +690,34 @@ int or_synrad(or_state* s, int turn) {
 /* Long-range wake: MPBeam::LRWakeBeamIntaction (MPBeam.cpp:3232-3349) with  */
 /* WakeFunction::GetTotLRWakeLinearFit (WakeFunction.cpp:204-230) and        */
 /* Bunch::BunchTransferDueToWake (Bunch.cpp:1091-1103).                      */
+/* WakeFunction::GetRWLRWakeFun (WakeFunction.cpp:499-552) added to the
+   long-range table (the total is BBR + RW, WakeFunction.cpp:124-137), with the
+   sectors' Yokoya factors yok[n][5] given by the caller (the special
+   functions are not restated in C). */
+int or_lr_add_rw(or_state* s, const double* yok) {
+  const cg_rw_sectors* w = &s->cfg.lr_rw;
+  if (!s->lr_tab || w->n < 1) return 1;
+  const double PI = 4 * atan(1.E0), CL = 299792458.0;
+  const double fgs = 120 * PI * CL / (4 * PI);
+  const double trf = s->cfg.ring.t0 / s->cfg.ring.harmonics, dt = trf / 2;
+  for (int i = 1; i < s->lr_np; ++i) {
+    const double tau = -i * dt;
+    double r[3] = {0, 0, 0};
+    for (int k = 0; k < w->n; ++k) {
+      double radius = w->radius_x[k] >= w->radius_y[k] ? w->radius_y[k] : w->radius_x[k];
+      double sig = w->sigma[k] * fgs;
+      r[0] += 1. / pow(radius, 3) * sqrt(1.E0 / sig) * w->length[k] * w->num[k] * yok[5 * k + 1] * w->beta_x[k];
+      r[1] += 1. / pow(radius, 3) * sqrt(1.E0 / sig) * w->length[k] * w->num[k] * yok[5 * k + 2] * w->beta_y[k];
+      r[2] += 1. / radius * sqrt(1.E0 / sig) * w->length[k] * w->num[k] * yok[5 * k + 0];
+    }
+    r[0] = r[0] * (-2.) / PI / pow(fabs(tau), 0.5) * fgs / s->sec[0].beta_x;
+    r[1] = r[1] * (-2.) / PI / pow(fabs(tau), 0.5) * fgs / s->sec[0].beta_y;
+    r[2] = r[2] / (2.) / PI / CL / pow(fabs(tau), 1.5) * fgs;
+    for (int d = 0; d < 3; ++d) s->lr_tab[(size_t)d * s->lr_np + i] += r[d];
+  }
+  return 0;
+}
+
 int or_lr_table(or_state* s, double* out, int capacity, int* np) {
   *np = s->lr_np;
   if (out) for (int i = 0; i < 3 * s->lr_np && i < capacity; ++i) out[i] = s->lr_tab[i];

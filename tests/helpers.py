@@ -95,7 +95,7 @@ def moments_close(mg, mo, rtol):
 
 
 def write_input(d, n_turns=60, interval=5, cbmgr="cbmgr", fit=(10, 50), bunches=40,
-                macro=200):
+                macro=200, extra=()):
     """A small MP-model input.dat (the reference's key = value format) and its
     twiss file in directory d: one train of `bunches` bunches every second
     bucket of a 480-bucket ring, two sections, no ions or wakes."""
@@ -121,6 +121,7 @@ def write_input(d, n_turns=60, interval=5, cbmgr="cbmgr", fit=(10, 50), bunches=
     ]
     if cbmgr:
         lines.append(f"runCBMGR = {cbmgr}")
+    lines += list(extra)
     with open(os.path.join(d, "input.dat"), "w") as f:
         f.write("\n".join(lines) + "\n")
     rows = ["0.0 10.0 0.5 0.0 0.1 0.0 0.02 5.0 -0.3 0.0 0.0 0.0 0.01 144.0 1.0 300",

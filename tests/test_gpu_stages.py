@@ -384,3 +384,31 @@ def test_upload_beam_matches_per_bunch_uploads():
     for j in range(wl.n_bunches):
         (x, s), (y, t) = want[j], h.download(j)
         assert np.array_equal(x, y) and np.array_equal(s, t)
+
+
+def test_lr_wake_with_resistive_wall_over_turns():
+    """Long-range wake of resonators plus resistive-wall sectors (round,
+    elliptical both ways, and a round one after an elliptical one)."""
+    wl = small("batched_uneven", 0.004)
+    rws = wl.cfg.lr_rw
+    sec = [(0.02, 0.02, 100.0, 8.0, 9.0, 2, 5.8e7), (0.03, 0.01, 20.0, 10.0, 7.0, 3, 1.4e6),
+           (0.01, 0.02, 10.0, 4.0, 5.0, 1, 3.7e7), (0.015, 0.015, 5.0, 6.0, 3.0, 4, 5.8e7)]
+    rws.n = len(sec)
+    for i, (rx, ry, ln, bx, by, num, sig) in enumerate(sec):
+        rws.radius_x[i], rws.radius_y[i], rws.length[i] = rx, ry, ln
+        rws.beta_x[i], rws.beta_y[i], rws.num[i], rws.sigma[i] = bx, by, num, sig
+    parts = particles(wl, seed=19, spread=5.0)
+    g, o = pair(wl, parts)
+    for turn in range(4):
+        g.MPBeamRMSCal(wl.cfg.n_sections - 1)
+        o.MPBeamRMSCal(wl.cfg.n_sections - 1)
+        g.LRWakeBeamIntaction()
+        o.LRWakeBeamIntaction()
+    assert coord_err(g, o, wl, alive_only=False).max() <= 1e-11
+    # the sectors matter: without them the kicks differ
+    rws.n = 0
+    g0, _ = pair(wl, parts)
+    for turn in range(4):
+        g0.MPBeamRMSCal(wl.cfg.n_sections - 1)
+        g0.LRWakeBeamIntaction()
+    assert coord_err(g0, o, wl, alive_only=False).max() > 1e-9

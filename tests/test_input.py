@@ -40,3 +40,19 @@ def test_fit_window_checks(tmp_path, lib, fit, msg):
     rc, *_ = parse(write_input(str(tmp_path), fit=fit), lib)
     assert rc == 1  # CG_ERR_INVALID
     assert msg in lib.cg_parse_error()
+
+
+def test_resistive_wall_sectors_are_read(tmp_path, lib):
+    d = str(tmp_path)
+    with open(d + "/pipe.dat", "w") as f:
+        f.write("radiusX radiusY length betaX betaY number sigma\n"
+                "0.02 0.02 100.0 8.0 9.0 2 5.8e7\n\n0.03 0.01 20.0 10.0 7.0 3 1.4e6\n")
+    path = write_input(d, extra=["runLongRangeWake = 1", "lrwNTurnsWakeTrunction = 5",
+                                 "lrwPipeGeoInput = pipe.dat"])
+    rc, cfg, _, arrays = parse(path, lib)
+    assert rc == 0, lib.cg_parse_error()
+    w = cfg.lr_rw
+    assert w.n == 2 and cfg.lr_turns == 6 and cfg.lr_bbr.n == 0
+    assert (w.radius_x[1], w.radius_y[1], w.length[1], w.num[1], w.sigma[1]) == \
+        (0.03, 0.01, 20.0, 3.0, 1.4e6)
+    lib.cg_config_free(C.byref(cfg), *arrays)
