@@ -91,7 +91,7 @@ class Config(C.Structure):
         ("n_turns", I), ("bunch_info_print_interval", I), ("bunch_emit_x", D), ("bunch_emit_y", D),
         ("bunch_sigma_z", D), ("bunch_sigma_dp", D),
         ("growth_fit_start", I), ("growth_fit_end", I), ("run_cbmgr", C.c_char * 256),
-        ("lr_rw", RwSectors),
+        ("lr_rw", RwSectors), ("sr_rw", RwSectors),
     ]
 
 

@@ -311,10 +311,20 @@ int cg_create(const cg_config* cfg, int device, cg_handle** out) {
       (cfg->ion.n_species < 1 || cfg->ion.n_species > CG_MAX_SPECIES || cfg->ion.max_ions < 1 ||
        cfg->ion.macro_ions_per_ip < 1))
     return fail(nullptr, CG_ERR_INVALID, "bad ion settings");
-  if (cfg->flag_sr_wake && (cfg->sr_bins < 1 || cfg->sr_bins > 2048 || cfg->sr_bbr.n < 1))
-    return fail(nullptr, CG_ERR_INVALID, "SRWBunchBinNum must be in [1, 2048] with resonators");
-  if (cfg->flag_lr_wake && (cfg->lr_turns < 2 || cfg->lr_bbr.n < 1))
-    return fail(nullptr, CG_ERR_INVALID, "LR wake needs >= 1 truncation turn and resonators");
+  if (cfg->flag_sr_wake && (cfg->sr_bins < 1 || cfg->sr_bins > 2048 ||
+                            (cfg->sr_bbr.n < 1 && cfg->sr_rw.n < 1)))
+    return fail(nullptr, CG_ERR_INVALID,
+                "SRWBunchBinNum must be in [1, 2048] with resonators or resistive-wall sectors");
+  for (const cg_rw_sectors* w : {&cfg->lr_rw, &cfg->sr_rw}) {
+    if (w->n < 0 || w->n > CG_MAX_RW_SECTORS)
+      return fail(nullptr, CG_ERR_INVALID, "resistive-wall sectors must number 0 .. 32");
+    for (int i = 0; i < w->n; ++i)
+      if (!(w->radius_x[i] > 0) || !(w->radius_y[i] > 0) || !(w->sigma[i] > 0))
+        return fail(nullptr, CG_ERR_INVALID, "resistive-wall sector radii and sigma must be > 0");
+  }
+  if (cfg->flag_lr_wake && (cfg->lr_turns < 2 || (cfg->lr_bbr.n < 1 && cfg->lr_rw.n < 1)))
+    return fail(nullptr, CG_ERR_INVALID,
+                "LR wake needs >= 1 truncation turn and resonators or resistive-wall sectors");
   if (cfg->flag_fir && cfg->fir.mode != 0 &&
       (cfg->fir.delay + cfg->fir.taps < 1 || cfg->fir.delay + cfg->fir.taps > CG_MAX_FIR))
     return fail(nullptr, CG_ERR_INVALID, "fbDelay + fbTaps must be in [1, 64]");
@@ -434,7 +444,13 @@ int cg_create(const cg_config* cfg, int device, cg_handle** out) {
     cudaMemset(h.d.fir_head, 0, sizeof(int));
   }
   // short-range wake: per-resonator constants and u-independent factors
-  // (GetBBRPusdoWakeFun, WakeFunction.cpp:573-601)
+  // (GetBBRPusdoWakeFun, WakeFunction.cpp:573-601), and the resistive-wall
+  // sectors' coefficient
+  if (cfg->flag_sr_wake && cfg->sr_rw.n > 0) {
+    double yok[CG_MAX_RW_SECTORS][5];
+    rw_sector_factors(cfg->sr_rw, yok);
+    h.sr_rw_coeff = rw_sr_coeff(cfg->sr_rw, yok);
+  }
   if (cfg->flag_sr_wake) {
     const int NZ = 1000;
     const cg_bbr& w = cfg->sr_bbr;

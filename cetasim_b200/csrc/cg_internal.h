@@ -152,6 +152,7 @@ struct Handle {
   // records, kicks and maps of a segment run on `side` while the next segment
   // walks
   int cbm_cap = 0, cbm_n = 0;  // coupled-bunch mode history: capacity, records made
+  double sr_rw_coeff = 0.0;    // short-range resistive-wall coefficient (0: no sectors)
   int pipe_groups = 4;
   // trajectories per walk CTA (8, 16, 32, 64): smaller CTAs spread the
   // walk's FP64 work over more SMs and find room sooner while the kicks and

@@ -354,12 +354,15 @@ extern "C" int cg_config_from_input(const char* path, cg_config* cfg, int* n_bun
     }
     if (cfg->flag_sr_wake) {
       cfg->sr_bins = has("srwbunchbinnum") ? (int)D(get("srwbunchbinnum"), 0) : 100;
+      // resistive-wall sectors and / or resonators (WakeFunction.cpp:240-247)
       if (has("srwpipegeoinput")) {
-        g_parse_error = "resistive-wall wakes are outside the tracking path of this library";
-        return CG_ERR_UNSUPPORTED;
+        int st = read_rw_sectors(resolve(base, get("srwpipegeoinput").v.at(0)), &cfg->sr_rw);
+        if (st) return st;
       }
-      int st = read_bbr(resolve(base, get("srwbbrinput").v.at(0)), &cfg->sr_bbr);
-      if (st) return st;
+      if (has("srwbbrinput")) {
+        int st = read_bbr(resolve(base, get("srwbbrinput").v.at(0)), &cfg->sr_bbr);
+        if (st) return st;
+      }
     }
     // derived constants, then the lattice
     int st = cg_config_derive(cfg);

@@ -163,17 +163,71 @@ __global__ void __launch_bounds__(kTile) k_sr_hist(const double* __restrict__ c,
 }
 
 // One CTA per (bunch, lag): W_z(tau) summed over resonators.
+// e^{-x} I_nu(x) for nu = 1/4, 5/4, 3/4, 7/4 (in that order), over the 256
+// threads of the CTA: the power series sum_k (x/2)^{2k+nu} / (k! Gamma(k+nu+1)),
+// each term formed in logarithms (so e^{-x} and the peak near k = x/2 stay in
+// range) and summed up to 12 standard widths past the peak.  Thread 0 gets
+// the four sums.
+__device__ void scaled_bessel_i4(double x, double (&out)[4], double (*sw4)[8]) {
+  const double nu[4] = {0.25, 1.25, 0.75, 1.75};
+  const int K = (int)(0.5 * x + 12.0 * sqrt(0.5 * x + 1.0) + 40.0);
+  const double lx = log(0.5 * x);
+  double s[4] = {0, 0, 0, 0};
+  for (int k = threadIdx.x; k <= K; k += blockDim.x) {
+    const double lk = lgamma(k + 1.0);
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      s[q] += exp((2 * k + nu[q]) * lx - lk - lgamma(k + nu[q] + 1.0) - x);
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const double v = warp_sum1(s[q]);
+    if ((threadIdx.x & 31) == 0) sw4[q][threadIdx.x >> 5] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int q = 0; q < 4; ++q) {
+      double a = 0.0;
+      for (int w = 0; w < 8; ++w) a += sw4[q][w];
+      out[q] = a;
+    }
+  __syncthreads();
+}
+
+// GetRWPusdoWakeFun's longitudinal function fu_z(u) (WakeFunction.cpp:
+// 387-444), zero outside 1e-2 <= |u| <= 40; valid in thread 0.
+__device__ double rw_pseudo_fz(double u, double (*sw4)[8]) {
+  if (fabs(u) < 1.e-2 || fabs(u) > 40) return 0.0;
+  const double x = u * u / 4.0;
+  double bi[4];
+  scaled_bessel_i4(x, bi, sw4);
+  // I_{-3/4} = (2 (1/4) / x) I_{1/4} + I_{5/4};  I_{-1/4} = (2 (3/4) / x) I_{3/4} + I_{7/4}
+  const double p025 = bi[0], m075 = 2.0 * 0.25 / x * bi[0] + bi[1];
+  const double p075 = bi[2], m025 = 2.0 * 0.75 / x * bi[2] + bi[3];
+  const double c1 = pow(fabs(u), 1.5);  // times e^{-x}, already in the scaled sums
+  const double c2 = u > 0 ? 1 : -1;
+  return c1 * (c2 * (m025 - p075) + (-p025 + m075));
+}
+
 __global__ void __launch_bounds__(256) k_sr_lag(const double* __restrict__ geom,
                                                 const SrResonator* __restrict__ res,
                                                 const double* __restrict__ green, int n_res,
-                                                int B, double sigmat, double* lag) {
+                                                int B, double sigmat, double rw_coeff,
+                                                double* lag) {
   __shared__ double sw[8];
+  __shared__ double sw4[4][8];
   const int b = blockIdx.y;
   const int m = (int)blockIdx.x - (B - 1);  // i - j
   const double dtBin = geom[2 * b + 1] / kCLight;
   const double tau = m * dtBin;
   const double u = tau / sigmat;
   double total = 0.0;
+  // resistive-wall sectors (GetRWSRWakeFun, WakeFunction.cpp:446-497; the
+  // reference adds them before the resonators, MPBunch.cpp:1968-1978)
+  if (rw_coeff != 0.0) {
+    const double fz = rw_pseudo_fz(u, sw4);
+    if (threadIdx.x == 0) total += rw_coeff * fz;
+  }
   for (int r = 0; r < n_res; ++r) {
     const SrResonator R = res[r];
     double s = 0.0;
@@ -238,7 +292,7 @@ cudaError_t launch_sr_wake(Handle& h) {
   const double sigmat = 1.e-3 / kCLight;
   k_sr_lag<<<lg, 256, 0, h.stream>>>(h.d.sr_geom, reinterpret_cast<const SrResonator*>(h.d.sr_green),
                                      h.d.sr_green + 3 * CG_MAX_RESONATORS, h.cfg.sr_bbr.n, B,
-                                     sigmat, h.d.sr_lag);
+                                     sigmat, h.sr_rw_coeff, h.d.sr_lag);
   k_sr_pot<<<h.M, 128, 0, h.stream>>>(h.d.bunch, h.d.sr_counts, h.d.sr_lag, h.d.sr_pot, B,
                                       h.cfg.ring.electron_energy);
   k_sr_kick<<<h.n_tiles, kTile, 0, h.stream>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch, h.d.bunch,

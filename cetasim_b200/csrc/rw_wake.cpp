@@ -129,6 +129,20 @@ void rw_lr_wake(const cg_rw_sectors& s, const double (*yok)[5], double beta_ip_x
   out[2] = out[2] / (2.) / kPi / kCLight / std::pow(std::fabs(tau), 1.5) * factor_gauss_si;
 }
 
+double rw_sr_coeff(const cg_rw_sectors& s, const double (*yok)[5]) {
+  const double factor_gauss_si = 120 * kPi * kCLight / (4 * kPi);
+  const double sigmat = 1.e-3 / kCLight;  // the 1 mm pseudo wake of GetRWSRWakeFun
+  double c = 0.0;
+  for (int i = 0; i < s.n; ++i) {
+    const double radius = s.radius_x[i] >= s.radius_y[i] ? s.radius_y[i] : s.radius_x[i];
+    const double sig = s.sigma[i] * factor_gauss_si;
+    const double coeff_l = 1.0 / (4 * radius) / std::pow(sigmat * kCLight, 1.5) *
+                           std::sqrt(kCLight / (2 * kPi * sig));
+    c += coeff_l * s.length[i] * s.num[i] * yok[i][0] * factor_gauss_si;
+  }
+  return c;
+}
+
 }  // namespace cg
 
 extern "C" {

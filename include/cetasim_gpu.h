@@ -169,6 +169,8 @@ typedef struct cg_config {
                                     file ("" off) */
   cg_rw_sectors lr_rw;           /* LRWPipeGeoInput: resistive-wall sectors of the
                                     long-range wake (n = 0: none) */
+  cg_rw_sectors sr_rw;           /* SRWPipeGeoInput: resistive-wall sectors of the
+                                    short-range wake (n = 0: none) */
 } cg_config;
 
 /* Per-bunch moments, the fields MPBunch::GetMPBunchRMS sets

@@ -27,6 +27,8 @@ def load():
         _lib = C.CDLL(LIB)
         _lib.or_create.restype = C.c_void_p
         _lib.or_last_error.restype = C.c_char_p
+        _lib.or_rw_fz.restype = C.c_double
+        _lib.or_rw_fz.argtypes = [C.c_double]
         for n in ("or_destroy",):
             getattr(_lib, n).restype = None
     return _lib
@@ -101,6 +103,13 @@ class OracleBeam:
             flat = (C.c_double * (5 * rws.n))(*[v for f in yok for v in f])
             if self.lib.or_lr_add_rw(self.s, flat):
                 raise RuntimeError("or_lr_add_rw failed")
+        srw = wl.cfg.sr_rw
+        if wl.cfg.flag_sr_wake and srw.n > 0:
+            from . import rw
+            yok = rw.sector_factors(list(srw.radius_x[:srw.n]), list(srw.radius_y[:srw.n]))
+            flat = (C.c_double * (5 * srw.n))(*[v for f in yok for v in f])
+            if self.lib.or_sr_set_rw(self.s, flat):
+                raise RuntimeError("or_sr_set_rw failed")
 
     def close(self):
         if self.s:

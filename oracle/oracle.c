@@ -221,6 +221,8 @@ typedef struct {
 
 struct or_state {
   cg_config cfg;
+  double sr_rw_yok[5 * CG_MAX_RW_SECTORS]; /* Yokoya factors of the SR sectors */
+  int sr_rw_on;
   cg_section* sec;
   int K, M, P;
   or_bunch* b;
@@ -817,6 +819,51 @@ static void bbr_pseudo(const cg_bbr* w, double tau, double out[3]) {
     out[0] += wx; out[1] += wy; out[2] += wz;
   }
 }
+/* GetRWPusdoWakeFun's fu[2] (WakeFunction.cpp:387-444): the Bessel I of
+   orders 1/4, 5/4, 3/4, 7/4 by their power series, each term formed in
+   logarithms (the reference takes gsl_sf_bessel_Inu). */
+static double scaled_inu(double nu, double x) {
+  int K = (int)(0.5 * x + 12.0 * sqrt(0.5 * x + 1.0) + 40.0);
+  double lx = log(0.5 * x), sum = 0;
+  for (int k = 0; k <= K; ++k) sum += exp((2 * k + nu) * lx - lgamma(k + 1.0) - lgamma(k + nu + 1.0) - x);
+  return sum; /* e^{-x} I_nu(x) */
+}
+double or_rw_fz(double u) {
+  if (fabs(u) < 1.e-2 || fabs(u) > 40) return 0.0;
+  double x = pow(u, 2) / 4.0;
+  double a = 0.25;
+  double fa = scaled_inu(a, x), fap1 = scaled_inu(1 + a, x);
+  double fam1 = 2.0 * a / x * fa + fap1;
+  double besselP025 = fa, besselM075 = fam1;
+  a = 0.75;
+  fa = scaled_inu(a, x); fap1 = scaled_inu(1 + a, x);
+  fam1 = 2.0 * a / x * fa + fap1;
+  double besselP075 = fa, besselM025 = fam1;
+  double coeff1 = pow(fabs(u), 1.5); /* exp(-x) is in the scaled values */
+  double coeff2 = u > 0 ? 1 : -1;
+  return coeff1 * (coeff2 * (besselM025 - besselP075) + (-besselP025 + besselM075));
+}
+/* GetRWSRWakeFun's longitudinal term (WakeFunction.cpp:446-497) with the
+   sectors' Yokoya factors from the caller (or_sr_set_rw). */
+static double rw_sr_wz(const or_state* s, double tau) {
+  const cg_rw_sectors* w = &s->cfg.sr_rw;
+  double PI = PI_REF(), fgs = 120 * PI * C_LIGHT / (4 * PI);
+  double sigmat = 1.e-3 / C_LIGHT, u = tau / sigmat, fz = or_rw_fz(u), wz = 0;
+  for (int i = 0; i < w->n; i++) {
+    double radius = w->radius_x[i] >= w->radius_y[i] ? w->radius_y[i] : w->radius_x[i];
+    double sig = w->sigma[i] * fgs;
+    double coeffL = 1.0 / (4 * radius) / pow(sigmat * C_LIGHT, 1.5) * sqrt(C_LIGHT / (2 * PI * sig));
+    wz += coeffL * fz * w->length[i] * w->num[i] * s->sr_rw_yok[5 * i] * fgs;
+  }
+  return wz;
+}
+int or_sr_set_rw(or_state* s, const double* yok) {
+  if (s->cfg.sr_rw.n < 1 || s->cfg.sr_rw.n > CG_MAX_RW_SECTORS) return 1;
+  for (int i = 0; i < 5 * s->cfg.sr_rw.n; ++i) s->sr_rw_yok[i] = yok[i];
+  s->sr_rw_on = 1;
+  return 0;
+}
+
 int or_sr_wake(or_state* s, int turn) {
   (void)turn;
   int B = s->cfg.sr_bins;
@@ -853,6 +900,8 @@ int or_sr_wake(or_state* s, int turn) {
     double* pot = b->sr_pot;
 #pragma omp parallel for schedule(static)
     for (int i = 0; i < B; i++) {
+      if (s->sr_rw_on) /* resistive wall first (MPBunch.cpp:1968-1978) */
+        for (int jj = 0; jj < B; jj++) pot[2 * B + i] += rw_sr_wz(s, (i - jj) * dtBin) * cnt[jj];
       for (int jj = 0; jj < B; jj++) {
         double tau = (i - jj) * dtBin;
         double w[3];

@@ -52,6 +52,8 @@ int or_ion_upload(or_state* s, int k, int p, const double* x, const double* y,
 int or_ion_cloud_record(or_state* s, int k, double* out);
 int or_sr_bins(or_state* s, int j, double* zlo, double* dz, int* counts);
 int or_lr_add_rw(or_state* s, const double* yok);
+int or_sr_set_rw(or_state* s, const double* yok);
+double or_rw_fz(double u);
 int or_lr_table(or_state* s, double* out, int capacity, int* np);
 /* counter-based normals shared with the device code (test helper) */
 void or_philox_normals(uint64_t seed, uint32_t stream, uint32_t c0, uint32_t c1, uint32_t c2,

@@ -412,3 +412,27 @@ def test_lr_wake_with_resistive_wall_over_turns():
         g0.MPBeamRMSCal(wl.cfg.n_sections - 1)
         g0.LRWakeBeamIntaction()
     assert coord_err(g0, o, wl, alive_only=False).max() > 1e-9
+
+
+def test_sr_wake_with_resistive_wall():
+    """Short-range wake of resistive-wall sectors (and no resonators): the
+    longitudinal kicks against the oracle."""
+    wl = small("plain_single", 0.05)
+    wl.cfg.sr_bbr.n = 0
+    rws = wl.cfg.sr_rw
+    sec = [(0.012, 0.012, 200.0, 8.0, 9.0, 1, 5.8e7), (0.03, 0.01, 50.0, 10.0, 7.0, 2, 1.4e6)]
+    rws.n = len(sec)
+    for i, (rx, ry, ln, bx, by, num, sig) in enumerate(sec):
+        rws.radius_x[i], rws.radius_y[i], rws.length[i] = rx, ry, ln
+        rws.beta_x[i], rws.beta_y[i], rws.num[i], rws.sigma[i] = bx, by, num, sig
+    g, o = pair(wl, particles(wl))
+    g.MPBeamRMSCal(0)
+    o.MPBeamRMSCal(0)
+    dp0 = g.download(0)[0][5].copy()
+    for turn in range(2):
+        g.SRWakeBeamIntaction(turn)
+        o.SRWakeBeamIntaction(turn)
+    kick_g = g.download(0)[0][5] - dp0
+    kick_o = o.download(0)[0][5] - dp0
+    assert np.max(np.abs(kick_o)) > 0
+    assert np.max(np.abs(kick_g - kick_o)) <= 1e-10 * np.max(np.abs(kick_o))

@@ -44,3 +44,18 @@ def test_rw_lr_wake_matches_the_oracle(lib):
         assert lib.cg_rw_lr_wake(C.byref(s), 7.0, 6.0, tau, _abi.ptr(out)) == 0
         ref = rw.rw_lr_wake(sec, yok, 7.0, 6.0, tau)
         assert np.allclose(out, ref, rtol=1e-11, atol=0)
+
+
+def test_rw_pseudo_wake_matches_scipy():
+    """The oracle's fu_z of GetRWPusdoWakeFun (Bessel I by its series) against
+    scipy's exponentially scaled Bessel I of the four orders directly."""
+    from scipy.special import ive
+    import oracle
+    lib = oracle.load()
+    for u in (0.05, -0.05, 0.5, -0.5, 3.0, -3.0, 10.0, -10.0, 30.0, -39.0):
+        x = u * u / 4
+        ref = abs(u) ** 1.5 * (np.sign(u) * (ive(-0.25, x) - ive(0.75, x))
+                               + (-ive(0.25, x) + ive(-0.75, x)))
+        scale = abs(u) ** 1.5 * (ive(-0.25, x) + ive(0.75, x) + ive(0.25, x) + ive(-0.75, x))
+        assert abs(lib.or_rw_fz(u) - ref) <= 1e-12 * scale  # the terms cancel for u > 0
+    assert lib.or_rw_fz(0.005) == 0.0 and lib.or_rw_fz(41.0) == 0.0
