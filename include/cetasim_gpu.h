@@ -207,8 +207,10 @@ int cg_lattice_init(const cg_ring* ring, cg_section* sections, int n_sections);
 
 /* Parses an input.dat (ReadInputSettings::ParamRead, ReadInputSettings.cpp:
  * 46-1085) plus the twiss file (LIP::InitialLattice, LIP.cpp:181-290) and the
- * BBR files (WakeFunction::BBRWakeParaReadIn, WakeFunction.cpp:251-290) it
- * names, relative paths resolved against the input file's directory first.
+ * BBR files (WakeFunction::BBRWakeParaReadIn, WakeFunction.cpp:251-290) and
+ * resistive-wall pipe files (LRWPipeGeoInput, SRWPipeGeoInput;
+ * RWWakeParaReadIn, WakeFunction.cpp:292-328) it names, relative paths
+ * resolved against the input file's directory first.
  * Fills cfg (derived fields and lattice maps included) and the bunch train
  * (Train::Initial, Train.cpp:38-104; MPBeam::Initial, MPBeam.cpp:64-106):
  * per-bunch macroparticle counts, harmonic numbers and electrons per bunch.
@@ -216,8 +218,10 @@ int cg_lattice_init(const cg_ring* ring, cg_section* sections, int n_sections);
  * with cg_config_free.  Keys outside the MP tracking path are accepted and
  * ignored, except settings this library does not implement (rfMode 1,
  * runBBIFlag, runSpaceCharge, ionCalSCMethod 2, driveModeOn, runRamping),
- * which return CG_ERR_UNSUPPORTED.  Optional keys beyond the reference:
- * bunchMacroEleNumPerBunchList (one count per bunch) and runRandomSeed. */
+ * which return CG_ERR_UNSUPPORTED.  runCBMGR with runGrowthRateFittingStart /
+ * End fills run_cbmgr and the fit window (checked as ReadInputSettings.cpp:
+ * 946-956).  Optional keys beyond the reference: bunchMacroEleNumPerBunchList
+ * (one count per bunch) and runRandomSeed. */
 int cg_config_from_input(const char* path, cg_config* cfg, int* n_bunches, int** n_macro,
                          int** bunch_harm, double** bunch_ne);
 void cg_config_free(cg_config* cfg, int* n_macro, int* bunch_harm, double* bunch_ne);
