@@ -25,7 +25,6 @@ namespace cg {
 #define FULL_MASK 0xffffffffu
 
 constexpr int kSrGreenN = 1000;  // nz of GetBBRPusdoWakeFun
-constexpr int kSrMaxBins = 2048;
 
 struct SrResonator {
   double dz;       // zMax / nz
