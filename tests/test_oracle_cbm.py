@@ -43,3 +43,9 @@ def test_analytic_signal_of_a_sinusoid():
     n = np.arange(64)
     a = cbm.analytic(np.cos(2 * np.pi * 5 * n / 64 + 0.3))
     assert np.allclose(a, np.exp(1j * (2 * np.pi * 5 * n / 64 + 0.3)), atol=1e-12)
+
+
+def test_analytic_signal_of_an_odd_length_record():
+    n = np.arange(63)
+    a = cbm.analytic(np.sin(2 * np.pi * 4 * n / 63))
+    assert np.allclose(a, -1j * np.exp(1j * 2 * np.pi * 4 * n / 63), atol=1e-12)
