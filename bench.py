@@ -45,7 +45,9 @@ WORKLOAD_DESC = ("fast_ion: 80 bunches x 2e4 FP64 macroparticles, 2 ns spacing, 
 
 
 class ClockSampler:
-    """nvidia-smi clock/throttle samples while the timed region runs."""
+    """Clock and throttle-reason samples while the timed region runs: NVML
+    polled every 5 ms (read-only), or nvidia-smi every 200 ms where NVML is
+    not available."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -54,10 +56,48 @@ class ClockSampler:
     def __init__(self, index: int):
         self.index = index
         self.samples = []
+        self.source = "nvidia-smi"
         self._stop = threading.Event()
         self._t = None
 
+    def _nvml(self):
+        """The NVML handle of this process's CUDA device, or None."""
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            try:  # the CUDA device by its PCI address (NVML's indices may differ)
+                import torch
+                pr = torch.cuda.get_device_properties(self.index)
+                bus = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+                return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
+            except Exception:
+                return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
+        except Exception:
+            return None
+
+    def _run_nvml(self, nv, h):
+        bits = [getattr(nv, "nvmlClocksEventReason" + n) for n in
+                ("HwSlowdown", "HwThermalSlowdown", "SwThermalSlowdown", "SwPowerCap")]
+        reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons",
+                          getattr(nv, "nvmlDeviceGetCurrentClocksThrottleReasons", None))
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self._stop.is_set():
+            sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+            r = reasons(h)
+            flags = ["Active" if r & b else "Not Active" for b in bits]
+            self.samples.append([str(self.index), str(sm), str(mx), "", hex(r)] + flags)
+            self._stop.wait(0.005)
+
     def _run(self):
+        got = self._nvml()
+        if got is not None:
+            try:
+                self.source = "nvml"
+                self._run_nvml(*got)
+                return
+            except Exception:
+                self.samples.clear()
+                self.source = "nvidia-smi"
         while not self._stop.is_set():
             try:
                 out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
@@ -89,7 +129,7 @@ class ClockSampler:
                           if len(s) > 5 + i and s[5 + i].lower() == "active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(self.samples)}
+                "samples": len(self.samples), "source": self.source}
 
 
 def dist_env():
