@@ -1825,9 +1825,15 @@ int cg_autotune_pipeline(cg_handle* H, int turn0, int reps, int* shape, double* 
   for (int v = 0; v < CG_PIPE_SHAPES && !st; ++v) {
     if ((st = cg_set_pipeline(H, kPipeShapes[v][0], kPipeShapes[v][1], kPipeShapes[v][2])))
       break;
-    if ((st = cg_run_turns(H, turn0, 1))) break;  // captures the turn graph
+    if ((st = cg_run_turns(H, turn0, 1))) {  // captures the turn graph
+      cg_checkpoint_load(H, keep.data(), n);  // the beam as it was, whatever failed
+      break;
+    }
     cudaEventRecord(e0, h.stream);
-    if ((st = cg_run_turns(H, turn0 + 1, reps))) break;
+    if ((st = cg_run_turns(H, turn0 + 1, reps))) {
+      cg_checkpoint_load(H, keep.data(), n);
+      break;
+    }
     cudaEventRecord(e1, h.stream);
     cudaEventSynchronize(e1);
     float t = 0;
