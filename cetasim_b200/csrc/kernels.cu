@@ -747,14 +747,12 @@ __global__ void __launch_bounds__(kTile, 2) k_map_stream(double* __restrict__ c,
 template <bool MOM, bool KICK>
 static cudaError_t map_stream_kernel(int grid, cudaStream_t s, Handle& h, int k, double bx,
                                      double by, const CloudRec* rec, int chunk_a, int chunk_b) {
-  static bool attr = false;  // once per instantiation
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(k_map_stream<MOM, KICK>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)kStreamSmem);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
+  // the attribute belongs to the current device's context: set it there
+  // (cheap; the pass is a measurement stage, not in the turn graph)
+  cudaError_t e = cudaFuncSetAttribute(k_map_stream<MOM, KICK>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kStreamSmem);
+  if (e != cudaSuccess) return e;
   k_map_stream<MOM, KICK><<<grid, kTile, kStreamSmem, s>>>(
       h.d.c, h.npad, h.d.surv, h.d.chunk_bunch, h.d.bunch, h.sec_dev_host[k], h.ring,
       h.d.wpartials, h.d.counters, h.d.mom, bx, by, rec, h.P, chunk_a, chunk_b, h.d.status);
