@@ -49,3 +49,23 @@ def test_analytic_signal_of_an_odd_length_record():
     n = np.arange(63)
     a = cbm.analytic(np.sin(2 * np.pi * 4 * n / 63))
     assert np.allclose(a, -1j * np.exp(1j * 2 * np.pi * 4 * n / 63), atol=1e-12)
+
+
+def test_iq_scan_phase_form_equals_the_reference_form():
+    """The IQ average with the phase (k + Q) h / H (f0 t0 = 1) against the
+    reference's form exp(-i 2 pi f t) with f = (k + Q) f0 and t = h t0 / H
+    evaluated in floating point (MPBeam.cpp:153-158, 1597-1611)."""
+    rng = np.random.default_rng(4)
+    M, H, Q = 80, 3840, 18.213
+    harm = np.sort(rng.choice(H, M, replace=False))
+    t0 = 2.3057e-6
+    f0 = 1.0 / t0
+    u = rng.normal(0, 1e-5, M)
+    mean = np.zeros((M, 6))
+    mean[:, 0] = u
+    _, _, _, iq_amp, iq_arg = cbm.cbm_record(mean, harm, H, (10.0, 5.0), (0.0, 0.0),
+                                            (Q, 10.1, 0.01), 1.0)
+    t = harm * (t0 / H)
+    for k in range(M):
+        ref = np.mean(u * np.exp(-1j * 2.0 * np.pi * ((k + Q) * f0) * t))
+        assert abs(iq_amp[0, k] - abs(ref)) <= 1e-11 * np.abs(u).max()
