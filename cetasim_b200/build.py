@@ -18,7 +18,7 @@ LIB = os.path.join(HERE, "libcetagpu.so")
 SOURCES = ["capi.cu", "kernels.cu", "kernels_sr.cu", "kernels_ion.cu", "surrogate.cu", "shard.cu",
            "cbm.cu", "faddeeva_table.cpp", "input_settings.cpp", "rw_wake.cpp"]
 HEADERS = ["cg_common.cuh", "faddeeva.cuh", "be_field.cuh", "track_math.cuh", "cg_internal.h",
-           "kernels.cuh", "umma.cuh", "surrogate.cuh"]
+           "kernels.cuh", "umma.cuh", "surrogate.cuh", "bulk.cuh", "rw_wake.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -51,7 +51,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
         return LIB
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
-    objs = []
+    cmds, objs = [], []
     for src in SOURCES:
         obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
         cmd = [nvcc(), *NVCC_FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
@@ -59,8 +59,14 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
             cmd += ["-Xptxas", "-v"]
         if verbose:
             print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
+        cmds.append(cmd)
         objs.append(obj)
+    # the translation units compile independently: one nvcc per source at once
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for r in list(ex.map(lambda c: subprocess.run(c), cmds)):
+            if r.returncode != 0:
+                raise subprocess.CalledProcessError(r.returncode, r.args)
     tmp = LIB + ".tmp"
     cmd = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp, *objs,
            "-lcudart_static", "-lrt", "-ldl", "-lpthread"]
