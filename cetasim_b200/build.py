@@ -99,16 +99,25 @@ def build_host(force: bool = False, verbose: bool = False) -> str:
 
 
 def build_oracle(verbose: bool = False) -> None:
-    """Builds the CPU oracle (test infrastructure) and, when the reference
-    sources are present, its compiled w(z) under oracle/_ref."""
+    """Builds the CPU oracle (test infrastructure).  With the CETASim source
+    tree named by the environment variable CETASIM_REFERENCE, also builds
+    the reference's own sources into oracle/_ref (its compiled w(z), and its
+    multi-particle path with the harness: see oracle/Makefile); without it,
+    oracle/_ref keeps whatever an earlier build left there."""
     odir = os.path.join(ROOT, "oracle")
     subprocess.run(["make", "-s", "-C", odir, "CC=gcc", "CXX=g++"], check=True,
                    stdout=None if verbose else subprocess.DEVNULL)
-    ref_src = os.environ.get("CETASIM_REFERENCE", "/root/reference")
-    if os.path.exists(os.path.join(ref_src, "src", "Faddeeva.cpp")):
-        subprocess.run(["make", "-s", "-C", odir, "ref", f"REF={ref_src}", "CC=gcc", "CXX=g++"],
-                       check=True, stdout=None if verbose else subprocess.DEVNULL,
-                       stderr=subprocess.DEVNULL)
+    ref_src = os.environ.get("CETASIM_REFERENCE")
+    if not ref_src:
+        if verbose:
+            print("CETASIM_REFERENCE not set: oracle/_ref not rebuilt", flush=True)
+        return
+    if not os.path.exists(os.path.join(ref_src, "src", "MPBeam.cpp")):
+        raise RuntimeError(f"CETASIM_REFERENCE={ref_src} holds no src/MPBeam.cpp")
+    subprocess.run(["make", "-s", f"-j{os.cpu_count() or 1}", "-C", odir, "ref", f"REF={ref_src}",
+                    "CC=gcc", "CXX=g++"], check=True,
+                   stdout=None if verbose else subprocess.DEVNULL,
+                   stderr=None if verbose else subprocess.DEVNULL)
 
 
 if __name__ == "__main__":

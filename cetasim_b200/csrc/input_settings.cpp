@@ -332,11 +332,14 @@ extern "C" int cg_config_from_input(const char* path, cg_config* cfg, int* n_bun
         g_parse_error = "fbDelay + fbTaps must be in [1, 64]";
         return CG_ERR_INVALID;
       }
+      // tap i >= delay is the (i - delay)-th value after '=' (the reference
+      // indexes strVec[i - delay + 1] with the key at strVec[0],
+      // ReadInputSettings.cpp:630-642)
       const char* names[3] = {"fbfircoeffx", "fbfircoeffy", "fbfircoeffz"};
       double* dst[3] = {f.coeff_x, f.coeff_y, f.coeff_z};
       for (int c = 0; c < 3; ++c)
         if (has(names[c]))
-          for (int i = 0; i < order; ++i) dst[c][i] = i < f.delay ? 0 : D(get(names[c]), i - f.delay + 1);
+          for (int i = 0; i < order; ++i) dst[c][i] = i < f.delay ? 0 : D(get(names[c]), i - f.delay);
     }
     // wakes
     std::string base = dir_of(path);

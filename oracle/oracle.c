@@ -19,6 +19,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include "philox.h"
 
 /* include/Global.h:26-40 */
 #define C_LIGHT 299792458.0
@@ -30,35 +31,14 @@
 static double PI_REF(void) { return 4 * atan(1.E0); }
 
 /* ------------------------------------------------------------------------ */
-/* Philox4x32-10 (Salmon et al., SC'11) and Box-Muller, identical to the     */
-/* device code's stream definitions.                                         */
-static void philox(uint32_t c[4], uint32_t k0, uint32_t k1) {
-  for (int r = 0; r < 10; ++r) {
-    uint64_t p0 = (uint64_t)0xD2511F53u * c[0];
-    uint64_t p1 = (uint64_t)0xCD9E8D57u * c[2];
-    uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
-    uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
-    uint32_t o0 = hi1 ^ c[1] ^ k0, o1 = lo1, o2 = hi0 ^ c[3] ^ k1, o3 = lo0;
-    c[0] = o0; c[1] = o1; c[2] = o2; c[3] = o3;
-    k0 += 0x9E3779B9u;
-    k1 += 0xBB67AE85u;
-  }
-}
+/* Philox4x32-10 and Box-Muller, identical to the device code's stream       */
+/* definitions (philox.h, shared with the harness of the reference build).   */
 void or_philox_normals(uint64_t seed, uint32_t stream, uint32_t c0, uint32_t c1, uint32_t c2,
                        uint32_t c3, double* out2) {
-  uint32_t c[4] = {c0, c1, c2, c3};
-  philox(c, (uint32_t)seed, (uint32_t)(seed >> 32) ^ stream);
-  uint64_t m1 = ((uint64_t)(c[0] >> 6) << 27) | (uint64_t)(c[1] >> 5);
-  uint64_t m2 = ((uint64_t)(c[2] >> 6) << 27) | (uint64_t)(c[3] >> 5);
-  double u1 = ((double)m1 + 1.0) * (1.0 / 9007199254740992.0);
-  double u2 = (double)m2 * (1.0 / 9007199254740992.0);
-  double rad = sqrt(-2.0 * log(u1));
-  const double pi = 3.141592653589793115997963468544185161590576171875;
-  out2[0] = rad * cos(2.0 * pi * u2);
-  out2[1] = rad * sin(2.0 * pi * u2);
+  cg_philox_normals(seed, stream, c0, c1, c2, c3, out2);
 }
-#define STREAM_SYNRAD 0x5359u
-#define STREAM_IONBIRTH 0x494Fu
+#define STREAM_SYNRAD CG_STREAM_SYNRAD
+#define STREAM_IONBIRTH CG_STREAM_IONBIRTH
 
 /* ------------------------------------------------------------------------ */
 /* Gaussian field: Bunch::BassettiErskine1 (Bunch.cpp:119-170),              */

@@ -6,8 +6,8 @@ from the reference source, plus seeded dense grids.  Outputs: the reference's
 own Faddeeva::w at every point, computed by oracle/_ref/libfaddeeva_ref.so,
 which oracle/Makefile compiles from the reference's src/Faddeeva.cpp.
 
-Run in a checkout where the reference is present:
-    make -C oracle ref && python tests/golden/make_faddeeva_golden.py
+Run with the CETASim source tree named by CETASIM_REFERENCE:
+    make -C oracle ref REF=$CETASIM_REFERENCE && python tests/golden/make_faddeeva_golden.py
 """
 import ctypes
 import os
@@ -18,7 +18,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("CETASIM_REFERENCE", "/root/reference")
+REF = os.environ.get("CETASIM_REFERENCE")
+if not REF:
+    sys.exit("set CETASIM_REFERENCE to the CETASim source tree (src/, include/)")
 
 
 def kat_points():
