@@ -259,6 +259,11 @@ class MPBeam:
         self._check(self.lib.cg_ion_download(self.h, k, p, *[_abi.ptr(x) for x in a], cap, C.byref(n)))
         return [x[: n.value] for x in a]
 
+    def upload_ions(self, k: int, p: int, x, y, vx, vy):
+        """Replaces the accumulated cloud of section k, species p."""
+        a = [np.ascontiguousarray(v, dtype=np.float64) for v in (x, y, vx, vy)]
+        self._check(self.lib.cg_ion_upload(self.h, k, p, *[_abi.ptr(v) for v in a], len(a[0])))
+
     def cloud_record(self, k: int):
         out = np.empty((self.wl.n_bunches, max(1, self.wl.cfg.ion.n_species), 6))
         self._check(self.lib.cg_ion_cloud_record(self.h, k, _abi.ptr(out)))

@@ -18,6 +18,12 @@ coupling 0.2 (eps_x = 20 pm, eps_y = 4 pm), sigma_z = 2.5 mm, sigma_dp = 9e-4.
   batched_uneven 900 bunches in 1000 buckets, macroparticles log-uniform in
                  [5e3, 5e4], 50 sections, long-range HOM (1.2 GHz, 1 MOhm/m,
                  Q = 1e4), 9-tap FIR feedback.
+  large_trapping 1000 uniformly filled bunches x 5e4: h = 4000 with a bunch
+                 in every 4th bucket (8 ns), V_RF re-solved so that the
+                 reference's formula still gives nu_s = 0.0049; 50 sections,
+                 clouds of 2e5 macro-ions per section pre-loaded
+                 (preload_clouds), short-range wake as plain_single, HOM and
+                 FIR as batched_uneven.
 
 Beam current is not part of those shapes: 1 mA for the single bunch and
 0.125 mA per bunch in the trains are used.
@@ -36,6 +42,18 @@ E_CHARGE = 1.602017733e-19
 # 9-tap FIR filter of the reference's example input (fbFircoeffx / y)
 FIR9_X = [0.5865, 0.5254, -0.0959, -0.3964, -0.2094, -0.0695, -0.2310, -0.2686, 0.1589]
 FIR9_Y = [0.7383, -0.2091, -0.4253, 0.1469, 0.1190, 0.0087, 0.0508, -0.3009, -0.1284]
+
+
+def rf_voltage_for_nus(nus: float, harmonics: int, energy: float = 6.0e9, u0: float = 4.166343e6,
+                       alphac1: float = 3.3e-5) -> float:
+    """V_RF that gives synchrotron tune nus through the reference's formula
+    nu_s^2 = -eta h V cos(phi_s) / (2 pi beta E) with phi_s = pi - asin(U0/V)
+    (ReadInputSettings.cpp:1024-1027): V^2 = (2 pi beta E nu_s^2 / (eta h))^2 + U0^2."""
+    gamma = energy / 0.51099906e6
+    beta = math.sqrt(1.0 - gamma ** -2)
+    eta = alphac1 - 1.0 / gamma ** 2
+    a = 2 * math.pi * beta * energy * nus ** 2 / (eta * harmonics)
+    return math.sqrt(a * a + u0 * u0)
 
 
 def base_ring(n_sections: int) -> _abi.Ring:
@@ -136,10 +154,17 @@ def make(name: str, n_scale: float = 1.0, turns_lr: int = 10, lib=None, seed: in
         rng = np.random.default_rng(seed)
         n_macro = [max(1, int(v * n_scale)) for v in np.exp(rng.uniform(math.log(5e3), math.log(5e4), M))]
         harm = list(range(M))
+    elif name == "large_trapping":
+        K, M = 50, 1000
+        n_macro = [max(1, int(5e4 * n_scale))] * M
+        harm = [4 * j for j in range(M)]
     else:
         raise KeyError(name)
     cfg = _abi.Config()
     cfg.ring = base_ring(K)
+    if name == "large_trapping":
+        cfg.ring.harmonics = 4000
+        cfg.ring.cav_vol[0] = rf_voltage_for_nus(0.0049, 4000)
     if derive(cfg) != 0:
         raise RuntimeError("cg_config_derive failed")
     secs = ring_sections(cfg.ring, K)
@@ -149,11 +174,11 @@ def make(name: str, n_scale: float = 1.0, turns_lr: int = 10, lib=None, seed: in
     cfg.sections = C_cast(secs)
     cfg.flag_synrad = 1
     cfg.seed = seed
-    if name == "plain_single":
+    if name in ("plain_single", "large_trapping"):
         cfg.flag_sr_wake = 1
         cfg.sr_bins = 100
         cfg.sr_bbr = bbr([(5e3, 1.0, 30e9, 2e6, 1.0, 30e9, 2e6, 1.0, 30e9)])
-    if name in ("fast_ion", "batched_uneven"):
+    if name in ("fast_ion", "batched_uneven", "large_trapping"):
         cfg.flag_beam_ion = 1
         ion = cfg.ion
         ion.n_species = 1
@@ -161,9 +186,9 @@ def make(name: str, n_scale: float = 1.0, turns_lr: int = 10, lib=None, seed: in
         ion.cross_section[0] = 2.0e-22
         ion.gas_percent[0] = 1.0
         ion.loss_boundary = 10.0
-        ion.max_ions = 100000
+        ion.max_ions = 100000 if name != "large_trapping" else 400000
         ion.macro_ions_per_ip = 1
-    if name == "batched_uneven":
+    if name in ("batched_uneven", "large_trapping"):
         cfg.flag_lr_wake = 1
         cfg.lr_turns = turns_lr + 1
         cfg.lr_bbr = bbr([(0.0, 1.0, 1.2e9, 1e6, 1e4, 1.2e9, 1e6, 1e4, 1.2e9)])
@@ -192,6 +217,22 @@ def make(name: str, n_scale: float = 1.0, turns_lr: int = 10, lib=None, seed: in
     eps_x = cfg.ring.natural_emit / (1 + cfg.ring.coupling)
     eps_y = eps_x * cfg.ring.coupling
     return Workload(name, cfg, secs, n_macro, harm, ne, (eps_x, eps_y, 2.5e-3, 9.0e-4))
+
+
+def preload_clouds(wl: Workload, n_ions: int = 200000, seed: int = 4321):
+    """Accumulated clouds for every section (species 0): n_ions macro-ions at
+    rest, Gaussian with the beam's transverse sizes at the section
+    (sqrt(eps beta)) about the axis, from a seeded generator.  Returns a list
+    of (x, y, vx, vy) per section."""
+    rng = np.random.default_rng(seed)
+    ex, ey = wl.gen[0], wl.gen[1]
+    out = []
+    for k in range(wl.cfg.n_sections):
+        s = wl.sections[k]
+        x = rng.normal(0.0, math.sqrt(ex * s.beta_x), n_ions)
+        y = rng.normal(0.0, math.sqrt(ey * s.beta_y), n_ions)
+        out.append((x, y, np.zeros(n_ions), np.zeros(n_ions)))
+    return out
 
 
 def C_ref(x):

@@ -190,6 +190,10 @@ class OracleBeam:
         self._check(self.lib.or_ion_download(self.s, k, p, *[_p(x) for x in a], cap, C.byref(n)))
         return [x[: n.value] for x in a]
 
+    def upload_ions(self, k, p, x, y, vx, vy):
+        a = [np.ascontiguousarray(v, dtype=np.float64) for v in (x, y, vx, vy)]
+        self._check(self.lib.or_ion_upload(self.s, k, p, *[_p(v) for v in a], len(a[0])))
+
     def cloud_record(self, k):
         out = np.empty((self.wl.n_bunches, max(1, self.wl.cfg.ion.n_species), 6))
         self._check(self.lib.or_ion_cloud_record(self.s, k, _p(out)))

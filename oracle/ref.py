@@ -156,6 +156,9 @@ class RefBeam:
         self._check(self.lib.ref_ion_get(self.h, k, p, *[_dp(x) for x in a], max(n, 1)))
         return [x[:n] for x in a]
 
+    def upload_ions(self, k, p, x, y, vx, vy):
+        self.set_ions(k, p, x, y, vx, vy)
+
     def set_ions(self, k, p, x, y, vx, vy):
         a = [np.ascontiguousarray(v, dtype=np.float64) for v in (x, y, vx, vy)]
         self._check(self.lib.ref_ion_set(self.h, k, p, *[_dp(v) for v in a], len(a[0])))

@@ -1,0 +1,88 @@
+"""The CUDA path against the reference's own compiled code.
+
+Each case of tests/refcases.py is written as the reference's input files,
+read by the library's parser, and tracked on the GPU from the same seeded
+particles the reference tracked when it wrote tests/golden/ref_tracking.npz
+(quantum excitation off; ion births from the shared counter-based stream).
+Where oracle/_ref is present (it ships with the build), further cases run
+the reference beside the GPU in the same test.
+"""
+import numpy as np
+import pytest
+
+import refcases
+from cetasim_b200.beam import MPBeam
+from oracle import ref
+
+pytestmark = pytest.mark.gpu
+
+# GPU vs reference, max |delta| / rms of each coordinate over alive particles.
+# The GPU's transcendentals, fused multiply-adds and w(z) differ from the
+# host's by ulps; 1000 turns of the linear map grow that to ~1e-12.
+TOL = {"plain_sr": 1e-10, "plain_1000": 1e-10, "fast_ion": 1e-10, "batched_lr_fir": 1e-10}
+
+
+def run_gpu(case, d):
+    wl, path, parts = refcases.build(case, d)
+    g = MPBeam(wl)
+    for j, c in enumerate(parts):
+        g.upload(j, c)
+    g.Run(0, refcases.CASES[case][2])
+    g.MPBeamRMSCal(0)
+    return wl, parts, g
+
+
+@pytest.mark.parametrize("case", list(refcases.CASES))
+def test_gpu_reproduces_reference_fixture(case, tmp_path):
+    gold = refcases.golden()
+    wl, parts, g = run_gpu(case, str(tmp_path))
+    assert refcases.parts_digest(parts) == bytes(gold[f"{case}/digest"]).hex()
+    worst = 0.0
+    for j in gold[f"{case}/bunches"]:
+        c, s = g.download(int(j))
+        want, ws = gold[f"{case}/coords/{j}"], gold[f"{case}/surv/{j}"]
+        assert np.array_equal(s, ws), f"bunch {j}: survival flags differ"
+        worst = max(worst, refcases.coord_rel_err(c, want, s == 0).max())
+    assert worst <= TOL[case], f"{case}: {worst:.3e}"
+    got = refcases.moments_array(g.moments())
+    want = gold[f"{case}/moments"]
+    assert np.array_equal(got[:, 0], want[:, 0])  # survivors per bunch
+    # centroids and z extremes against the bunch sizes, the rest relatively
+    # (columns of refcases.moments_array)
+    bx, by = wl.sections[0].beta_x, wl.sections[0].beta_y
+    scale = np.abs(want).copy()
+    scale[:, 1] = want[:, 13]
+    scale[:, 2] = np.sqrt(want[:, 7] / bx)
+    scale[:, 3] = want[:, 14]
+    scale[:, 4] = np.sqrt(want[:, 8] / by)
+    scale[:, 5] = scale[:, 19] = scale[:, 20] = want[:, 17]
+    scale[:, 6] = want[:, 18]
+    rel = np.abs(got[:, 1:] - want[:, 1:]) / np.maximum(scale[:, 1:], 1e-300)
+    assert np.max(rel) <= 1e-8, f"{case}: moments {np.max(rel):.3e}"
+
+
+@pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
+def test_gpu_and_reference_side_by_side_fast_ion_ip_records(tmp_path):
+    """One turn of the trapped fast-ion train: the electrons after every IP
+    against the reference run stage by stage."""
+    wl, path, parts = refcases.build("fast_ion", str(tmp_path))
+    r = ref.RefBeam(path, seed=wl.cfg.seed)
+    r.set_emit_nat([0.0, 0.0, 0.0])
+    g = MPBeam(wl)
+    for j, c in enumerate(parts):
+        r.upload(j, c)
+        g.upload(j, c)
+    for b in (r, g):
+        b.MPBeamRMSCal(0)
+    for k in range(wl.cfg.n_sections):
+        for b in (r, g):
+            b.MPBeamRMSCal(k)
+            b.SSBeamIonEffectOneInteractionPoint(0, k)
+            b.BeamTransferPerInteractionPointDueToLatticeT(k)
+        worst = 0.0
+        for j in range(0, wl.n_bunches, 7):
+            cr, sr = r.download(j)
+            cg, sg = g.download(j)
+            assert np.array_equal(sr, sg)
+            worst = max(worst, refcases.coord_rel_err(cg, cr, sr == 0).max())
+        assert worst <= 1e-11, f"IP {k}: {worst:.3e}"
