@@ -1,24 +1,37 @@
-"""Benchmark: fast-ion multi-particle tracking turns on B200.
+"""Benchmark: multi-particle tracking turns (MPBeam::Run order,
+MPBeam.cpp:1010-1102) on B200.  One step = one full turn of the workload.
 
-Workload (one step = one full turn of MPBeam::Run order, MPBeam.cpp:1010-1102):
-80 bunches x 2e4 FP64 macroparticles in consecutive 2 ns buckets, 20
-interaction points (beta = 10 m), CO ions at 1e-9 Pa with one macro-ion per
-bunch passage per IP, exact Bassetti-Erskine kicks both ways through the
-FP64 Faddeeva kernel, synchrotron radiation with quantum excitation.
+Workloads (--workload; default batched_uneven, the shape the surrogate
+target is stated on):
+  plain_single    config 0: 1 bunch x 1e5, 1 IP, short-range BBR wake (100
+                  bins), synchrotron radiation with quantum excitation
+  fast_ion        config 1: 80 bunches x 2e4, 20 IPs, CO ions, exact
+                  Bassetti-Erskine kicks both ways
+  batched_uneven  config 3: 900 of 1000 buckets filled, 5e3-5e4 macroparticles
+                  per bunch (log-uniform), 50 IPs, CO ions, long-range HOM
+                  wake, 9-tap FIR; the learned-field arm ("surrogate") beside
+                  the exact path
+  large_trapping  config 4: 1000 bunches x 5e4 (every 4th bucket of h = 4000),
+                  clouds of 2e5 macro-ions per IP pre-loaded, 50 IPs, short-
+                  range wake, HOM, FIR
 
-  value  macroparticle-turns/s with the beam resident in HBM (device time of
-         K turns by CUDA events on the library's stream, L2 flushed between
-         turns: the 77 MB state would otherwise stay in the 126 MB L2)
-  e2e    the same through the C ABI with the beam uploaded from pinned host
-         memory and the per-bunch moments read back every turn
-  roofline  the electron-side field-kick kernel (the largest FP64 kernel of
-         the turn) against the FP64 FMA throughput measured on this GPU
-  cpu_baseline  the CPU oracle (OpenMP over particles) on a bounded sample
+  value     macroparticle-turns/s of the exact path with the beam resident in
+            HBM (device time of K turns by CUDA events on the library's
+            stream, L2 flushed before every turn)
+  e2e       the same through the C ABI with the beam uploaded from pinned host
+            memory and the per-bunch moments read back every turn
+  roofline  every kernel of the turn with its own bound; the one with the
+            largest share of the turn first
+  cpu_baseline  the reference's own build (oracle/_ref) on the host cores
 
---impl reference times the reference algorithm on the host cores (the oracle
-restatement; the reference's own tracking sources do not build here).
-Multi-GPU: one process per GPU (torchrun), each an independent replica of the
-workload (weak scaling); timing is the max over ranks.
+--impl reference times the reference's own CPU code (its src/*.cpp built in
+oracle/_ref) on the same workload at full particle counts, one process per
+host core, each holding a contiguous slice of the train: a step is one
+interaction point of the turn loop over the whole train, and a turn is
+extrapolated as (IPs x step) + the once-per-turn stages, both measured.
+Multi-GPU: one process per GPU (torchrun), each an independent replica
+(weak scaling) or, with --shard, one beam split by bunches; timing is the
+max over ranks.
 """
 from __future__ import annotations
 
@@ -36,12 +49,23 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-BATCHED_DESC = ("batched_uneven: 900 of 1000 buckets filled, 5e3-5e4 FP64 macroparticles "
-                "per bunch (log-uniform), 50 IPs, CO ions, exact Bassetti-Erskine both ways, "
-                "long-range HOM wake, 9-tap FIR, synchrotron radiation with quantum excitation")
-WORKLOAD_DESC = ("fast_ion: 80 bunches x 2e4 FP64 macroparticles, 2 ns spacing, 20 IPs, "
+DESC = {
+    "plain_single": ("config 0 plain_single: 1 bunch x 1e5 FP64 macroparticles, 1 IP, short-range "
+                     "BBR wake (5 kOhm / 2 MOhm/m, 30 GHz, Q = 1, 100 bins), synchrotron radiation "
+                     "with quantum excitation"),
+    "fast_ion": ("config 1 fast_ion: 80 bunches x 2e4 FP64 macroparticles, 2 ns spacing, 20 IPs, "
                  "CO at 1e-9 Pa, 1 macro-ion/bunch/IP, exact Bassetti-Erskine both ways, "
-                 "synchrotron radiation with quantum excitation")
+                 "synchrotron radiation with quantum excitation"),
+    "batched_uneven": ("config 3 batched_uneven: 900 of 1000 buckets filled, 5e3-5e4 FP64 "
+                       "macroparticles per bunch (log-uniform), 50 IPs, CO ions, long-range HOM "
+                       "wake (1.2 GHz, 1 MOhm/m, Q = 1e4), 9-tap FIR, synchrotron radiation with "
+                       "quantum excitation; value = exact Bassetti-Erskine path, learned-field arm "
+                       "in 'surrogate'"),
+    "large_trapping": ("config 4 large_trapping: 1000 bunches x 5e4 FP64 macroparticles (every 4th "
+                       "bucket of h = 4000), 2e5 pre-loaded macro-ions per IP, 50 IPs, short-range "
+                       "wake, long-range HOM wake, 9-tap FIR, synchrotron radiation with quantum "
+                       "excitation, exact Bassetti-Erskine both ways"),
+}
 
 
 class ClockSampler:
@@ -139,46 +163,137 @@ def dist_env():
     return rank, world, local
 
 
-def cpu_sample(turns: int = 1, n_scale: float = 0.025, threads: int | None = None):
-    """Oracle timing on a bounded sample of the workload: 80 bunches x 500
-    macroparticles, all 20 IPs, `turns` turns.  Returns (value, seconds, n)."""
-    os.environ.setdefault("OMP_NUM_THREADS", str(threads or os.cpu_count() or 1))
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
+def _ref_gen(wl, j, seed):
+    """Seeded Gaussian macroparticles of bunch j (the same for any slicing)."""
+    rng = np.random.default_rng([seed, j])
+    ex, ey, sz, sdp = wl.gen
+    s0 = wl.sections[0]
+    n = int(wl.n_macro[j])
+    c = np.empty((6, n))
+    for d, sig in enumerate((np.sqrt(ex * s0.beta_x), np.sqrt(ex / s0.beta_x), np.sqrt(ey * s0.beta_y),
+                             np.sqrt(ey / s0.beta_y), sz, sdp)):
+        c[d] = rng.normal(0.0, sig, n)
+    return c
+
+
+def _ref_slice(spec):
+    """One worker of the reference arm: the reference's own MP code
+    (oracle/_ref/libcetasim_ref.so) on bunches [a, b) of the workload at full
+    particle counts.  Times `nsteps` IP sections of the turn loop
+    (MPBeam.cpp:1059-1070: moments, ion chain, map, moments) and once the
+    per-turn stages (RF, drift, energy loss, damping, wakes, FIR, losses)."""
+    import tempfile
+    sys.path.insert(0, ROOT)
     import oracle
-    from helpers import particles, small
-    wl = small("fast_ion", n_scale)
-    o = oracle.OracleBeam(wl)
-    for j, c in enumerate(particles(wl, seed=3, spread=2.0)):
-        o.upload(j, c)
-    t = time.perf_counter()
-    o.Run(0, turns)
-    dt = time.perf_counter() - t
-    return wl.n_particles * turns / dt, dt, wl.n_particles
+    from cetasim_b200 import configs, input_dat
+    from oracle import ref
+    name, n_scale, a, b, nsteps, seed = spec
+    wl = configs.make(name, n_scale=n_scale, derive=oracle.config_derive,
+                      lattice_init=oracle.lattice_init)
+    cl = configs.preload_clouds(wl) if name == "large_trapping" else None
+    parts = [_ref_gen(wl, j, seed) for j in range(a, b)]
+    wl.n_macro, wl.harm, wl.ne = wl.n_macro[a:b].copy(), wl.harm[a:b].copy(), wl.ne[a:b].copy()
+    with tempfile.TemporaryDirectory() as d:
+        path = input_dat.write_case(d, wl, n_turns=1)
+        r = ref.RefBeam(path, seed=seed)
+        for j, c in enumerate(parts):
+            r.upload(j, c)
+        del parts
+        if cl is not None:
+            for k, (x, y, vx, vy) in enumerate(cl):
+                r.upload_ions(k, 0, x, y, vx, vy)
+        K = wl.cfg.n_sections
+        times = []
+        for s in range(nsteps):
+            k = s % K
+            t = time.perf_counter()
+            r.MPBeamRMSCal(k)
+            if wl.cfg.flag_beam_ion:
+                r.SSBeamIonEffectOneInteractionPoint(0, k)
+            r.BeamTransferPerInteractionPointDueToLatticeT(k)
+            r.stage(ref.ST_RMS_ONLY, 0, k)
+            times.append(time.perf_counter() - t)
+        t = time.perf_counter()
+        r.BeamMomtumUpdateDueToRFTest()
+        r.BeamLongiPosTransferOneTurn()
+        r.BeamEnergyLossOneTurn()
+        if wl.cfg.flag_synrad:
+            r.BeamSynRadDamping(0)
+        if wl.cfg.flag_lr_wake:
+            r.LRWakeBeamIntaction()
+        if wl.cfg.flag_sr_wake:
+            r.SRWakeBeamIntaction(1)
+        r.stage(ref.ST_RMS_ONLY, 0, 0)
+        if wl.cfg.flag_fir:
+            r.FIRBunchByBunchFeedback(0)
+        r.MarkParticleLostInBunch()
+        tail = time.perf_counter() - t
+        r.close()
+    return times, tail, int(wl.n_macro.sum())
+
+
+def reference_cpu(workload, n_scale, nsteps, workers=None, seed=7):
+    """The reference's own CPU code on the workload: P processes (one per
+    host core, at most one per bunch), slices balanced by macroparticle
+    count.  Returns a dict with the extrapolated turn time and
+    macroparticle-turns/s (total particles / turn), or None when the
+    reference build is absent."""
+    import multiprocessing as mp
+    from oracle import ref
+    if not ref.available():
+        return None
+    sys.path.insert(0, ROOT)
+    from cetasim_b200 import configs
+    import oracle
+    wl = configs.make(workload, n_scale=n_scale, derive=oracle.config_derive,
+                      lattice_init=oracle.lattice_init)
+    M, K = wl.n_bunches, wl.cfg.n_sections
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    P = max(1, min(workers or cores, M))
+    cum = np.concatenate([[0], np.cumsum(wl.n_macro)])
+    cuts = [0] + [int(np.searchsorted(cum, cum[-1] * i / P)) for i in range(1, P)] + [M]
+    cuts = sorted(set(cuts))
+    specs = [(workload, n_scale, cuts[i], cuts[i + 1], nsteps, seed) for i in range(len(cuts) - 1)]
+    t0 = time.perf_counter()
+    with mp.get_context("spawn").Pool(len(specs)) as pool:
+        res = pool.map(_ref_slice, specs)
+    wall = time.perf_counter() - t0
+    step = np.max(np.array([r[0] for r in res]), axis=0)  # the slowest slice of each step
+    tail = max(r[1] for r in res)
+    n = sum(r[2] for r in res)
+    turn_s = K * float(np.mean(step)) + tail
+    return {"value": n / turn_s, "turn_s": turn_s, "step_s": [float(x) for x in step],
+            "tail_s": tail, "processes": len(specs), "particles": n, "wall_s": wall,
+            "sample": (f"reference build (its src/*.cpp, oracle/_ref) on all {M} bunches at full "
+                       f"particle counts in {len(specs)} processes (contiguous bunch slices); "
+                       f"{nsteps} IP sections of the turn loop timed (slowest slice each), turn = "
+                       f"{K} x mean IP section + the once-per-turn stages, measured")}
 
 
 def run_reference(args, rank):
     if rank != 0:
         return
-    from cetasim_b200 import build
-    build.build_oracle()
-    vals = []
-    n = 0
-    for s in range(args.warmup + args.steps):
-        v, dt, n = cpu_sample(turns=1)
-        if s >= args.warmup:
-            vals.append(dt)
-    tot = sum(vals)
-    value = n * len(vals) / tot
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    sample = (f"80 bunches x {n // 80} macroparticles (of 2e4), 20 IPs, 1 turn per step; "
-              "oracle restatement in C with OpenMP over particles")
+    r = reference_cpu(args.workload, args.n_scale, args.warmup + args.steps)
+    if r is None:
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/libcetasim_ref.so (the reference's own "
+                                         "sources) is not built"}), flush=True)
+        return
+    # the turn from the timed steps only (the warm-up steps are dropped)
+    steps = r["step_s"][args.warmup:]
+    K = {"plain_single": 1, "fast_ion": 20}.get(args.workload, 50)
+    turn_s = K * float(np.mean(steps)) + r["tail_s"]
+    value = r["particles"] / turn_s
     line = {"impl": "reference", "metric": "macroparticle-turns/s", "value": value,
             "unit": "macroparticle-turns/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(vals), "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(steps)),
+            "ms_per_turn": 1e3 * turn_s, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD_DESC, "sample": sample},
-            "cpu_baseline": {"value": value, "unit": "macroparticle-turns/s", "cores": cores,
-                             "kind": "port", "sample": sample},
+            "config": {"workload": DESC[args.workload], "macroparticles": r["particles"],
+                       "turns_per_step": "one IP section of the turn per step (extrapolated turn in "
+                                         "ms_per_turn)", "sample": r["sample"]},
+            "cpu_baseline": {"value": value, "unit": "macroparticle-turns/s", "cores": r["processes"],
+                             "kind": "reference", "sample": r["sample"]},
             "e2e": {"value": value, "unit": "macroparticle-turns/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -203,8 +318,8 @@ def main():
     ap.add_argument("--pipeline", default=None, metavar="G:IONS:RAMP",
                     help="pipeline shape (walk segments, ions per walk CTA, ramp 0/1) instead "
                          "of the whole-turn pipeline autotuner")
-    ap.add_argument("--workload", default="fast_ion", choices=["fast_ion", "batched_uneven"],
-                    help="batched_uneven: 900 bunches of 5e3-5e4, 50 IPs, LR wake + FIR")
+    ap.add_argument("--workload", default="batched_uneven", choices=list(DESC),
+                    help="; ".join(f"{k}: {v}" for k, v in DESC.items()))
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.impl == "reference":
@@ -233,6 +348,9 @@ def main():
         wl = configs.make(args.workload, n_scale=args.n_scale, seed=1234)  # one beam
     beam = MPBeam(wl, device=local, shard=shard)
     beam.generate(seed=99 if shard else 99 + rank)
+    if args.workload == "large_trapping":
+        for k, (x, y, vx, vy) in enumerate(configs.preload_clouds(wl)):
+            beam.upload_ions(k, 0, x, y, vx, vy)
     copies = 1 if shard else world  # independent beams the ranks advance
     stream = torch.cuda.ExternalStream(lib.cg_stream(beam.h))
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -247,11 +365,14 @@ def main():
     # (it leaves the beam as it was), then the warm-up turns (the first one
     # instantiates the turn graph with the chosen shape)
     beam.Run(0, 1)
+    ions = bool(wl.cfg.flag_beam_ion)
     if args.kick_variant is not None:
         beam.set_kick_variant(args.kick_variant)
         tune = (args.kick_variant, None)
-    else:
+    elif ions:
         tune = beam.autotune(0, reps=10)
+    else:
+        tune = (0, None)
     t_first = 1
     # pipeline shape (walk segments x walk CTA size) over whole turns; the
     # beam is restored after each trial
@@ -287,7 +408,6 @@ def main():
         tot_ms = float(t.item())
     n_part = wl.n_particles
     value = copies * n_part * args.steps / (tot_ms * 1e-3)
-    ion_kicks_turn = n_part * wl.cfg.n_sections  # electron-side kicks (dominant)
 
     # e2e through the C ABI: pinned host beam uploaded every turn, moments read back
     hbufs = []
@@ -329,70 +449,97 @@ def main():
     for p, _ in hbufs:
         lib.cg_host_free(p)
 
-    # dominant FP64 kernel: electron-side ion kick at IP 0, timed alone
+    # per-kernel device times on the live beam (cg_time_stage: one stage
+    # launched `reps` times on the library stream, CUDA events around it)
+    def stage_ms(st, reps):
+        v = C.c_double()
+        beam._check(lib.cg_time_stage(beam.h, st, 0, reps, C.byref(v)))
+        return v.value
+    K = wl.cfg.n_sections
     beam.MPBeamRMSCal(0)
-    beam.SSBeamIonEffectOneInteractionPoint(10**6, 0)
-    kick_ms = C.c_double()
-    beam._check(lib.cg_time_stage(beam.h, 1, 0, 20, C.byref(kick_ms)))
-    map_ms = C.c_double()
-    beam._check(lib.cg_time_stage(beam.h, 0, 0, 20, C.byref(map_ms)))
-    chain_ms = C.c_double()
-    beam._check(lib.cg_time_stage(beam.h, 2, 0, 5, C.byref(chain_ms)))
-    mom_ms = C.c_double()
-    beam._check(lib.cg_time_stage(beam.h, 3, 0, 20, C.byref(mom_ms)))
-    pass_ms = C.c_double()
-    beam._check(lib.cg_time_stage(beam.h, 5, 0, 20, C.byref(pass_ms)))
-    tail_ms = C.c_double()
-    beam._check(lib.cg_time_stage(beam.h, 4, 0, 5, C.byref(tail_ms)))
-    peak = C.c_double()
-    lib.cg_fp64_peak(C.byref(peak))
-    flops_per_kick = FLOPS_PER_KICK
-    achieved = n_part * flops_per_kick / (kick_ms.value * 1e-3)
-    traffic = kick_traffic() if args.workload == "fast_ion" else None
+    if ions:
+        beam.SSBeamIonEffectOneInteractionPoint(10 ** 6, 0)
+    kms = {"map_moments_pass": stage_ms(5, 20), "moments": stage_ms(3, 20),
+           "section_map": stage_ms(0, 20), "longitudinal_tail": stage_ms(4, 5)}
+    if ions:
+        kms["ion_field_kick"] = stage_ms(1, 20)
+        kms["ion_chain"] = stage_ms(2, 5)
+    peak64 = C.c_double()
+    lib.cg_fp64_peak(C.byref(peak64))
+    hbm = measured_peak("hbm_gbs")
+    n_part = wl.n_particles
+    kernels = []
+    # the map + moments pass: 6 FP64 read + written and the survival byte
+    # read once per particle (97 B), HBM-bound
+    mp_bytes = 97.0 * n_part
+    kernels.append({"kernel": "k_map_pass (section map + next IP's moments)", "bound": "hbm",
+                    "per_turn_ms": K * kms["map_moments_pass"],
+                    "achieved": mp_bytes / (kms["map_moments_pass"] * 1e-3) / 1e9,
+                    "peak": hbm[0], "unit": "GB/s", "peak_source": hbm[1],
+                    "algorithmic_bytes": mp_bytes})
+    if ions:
+        fl = FLOPS_PER_KICK * n_part
+        kernels.append({"kernel": "k_ion_kick (electron-side Bassetti-Erskine)", "bound": "fp64",
+                        "per_turn_ms": K * kms["ion_field_kick"],
+                        "achieved": fl / (kms["ion_field_kick"] * 1e-3) / 1e12,
+                        "peak": peak64.value / 1e12, "unit": "TFLOP/s",
+                        "peak_source": "FP64 FMA throughput measured by cg_fp64_peak",
+                        "algorithmic_flops": fl})
+        lat = C.c_double()
+        beam._check(lib.cg_field_chain_latency(C.byref(lat)))
+        steps = wl.n_bunches
+        kernels.append({"kernel": "ion chain (k_ion_prep/walk/records/compact)", "bound": "latency",
+                        "per_turn_ms": K * kms["ion_chain"],
+                        "achieved": 1e3 * kms["ion_chain"] / steps, "peak": lat.value,
+                        "unit": "us per bunch step (lower is better)",
+                        "peak_source": "one thread's dependent chain of field evaluations, "
+                                       "measured by cg_field_chain_latency",
+                        "algorithmic_steps": steps})
+    # the once-per-turn longitudinal tail: RF, drift, loss, damping, wakes,
+    # FIR, losses; one read and write of the state
+    kernels.append({"kernel": "longitudinal tail (k_long, wakes, FIR, k_mark_lost)", "bound": "hbm",
+                    "per_turn_ms": kms["longitudinal_tail"],
+                    "achieved": mp_bytes / (kms["longitudinal_tail"] * 1e-3) / 1e9,
+                    "peak": hbm[0], "unit": "GB/s", "peak_source": hbm[1],
+                    "algorithmic_bytes": mp_bytes})
+    for kk in kernels:
+        a_, p_ = kk["achieved"], kk["peak"]
+        kk["frac"] = (p_ / a_ if kk["bound"] == "latency" else a_ / p_) if a_ and p_ else None
+    kernels.sort(key=lambda kk: -kk["per_turn_ms"])
+    top = dict(kernels[0])
+    top["traffic"] = kernel_traffic(args.workload, top["kernel"])
+    top["kernels"] = kernels
     sur = None
-    if world == 1 and not args.no_surrogate:
-        sur = surrogate_leg(args, beam, lib, stream, flush, kick_ms.value, tot_ms / args.steps)
+    if world == 1 and ions and not args.no_surrogate:
+        sur = surrogate_leg(args, beam, lib, stream, flush, kms["ion_field_kick"], tot_ms / args.steps)
 
     result = None
     if rank == 0:
         cpu = None
-        if not args.no_cpu and world == 1 and args.workload == "fast_ion":
+        if not args.no_cpu and world == 1:
             try:
-                v, dt, n = cpu_sample(turns=1)
-                cpu = {"value": v, "unit": "macroparticle-turns/s",
-                       "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)),
-                       "kind": "port",
-                       "sample": f"80 bunches x {n // 80} macroparticles, 20 IPs, 1 turn "
-                                 f"({dt:.1f} s); C oracle, OpenMP over particles"}
+                r = reference_cpu(args.workload, args.n_scale, 4)
+                if r is not None:
+                    cpu = {"value": r["value"], "unit": "macroparticle-turns/s",
+                           "cores": r["processes"], "kind": "reference",
+                           "sample": r["sample"] + f"; {r['wall_s']:.1f} s wall"}
             except Exception as e:  # the baseline is reported, never required
-                cpu = {"value": None, "unit": "macroparticle-turns/s", "cores": 0, "kind": "port",
-                       "sample": f"failed: {e}"}
+                cpu = {"value": None, "unit": "macroparticle-turns/s", "cores": 0,
+                       "kind": "reference", "sample": f"failed: {e}"}
         result = {
             "metric": "macroparticle-turns/s", "value": value, "unit": "macroparticle-turns/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
             "scaling": "strong" if shard else "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD_DESC if args.workload == "fast_ion" else
-                       BATCHED_DESC, "bunches": wl.n_bunches,
-                       "macroparticles": n_part, "interaction_points": wl.cfg.n_sections,
+            "config": {"workload": DESC[args.workload], "bunches": wl.n_bunches,
+                       "macroparticles": n_part, "interaction_points": K,
                        "turns_per_step": 1, "l2": "flushed between turns (512 MB write)",
                        "parallelism": (f"bunch-sharded x{world} (moments all-gathered per IP)"
                                        if shard else f"replica x{world}")},
-            "ion_kicks_per_s": copies * ion_kicks_turn * args.steps / (tot_ms * 1e-3),
-            "kernels_ms": {"ion_field_kick": kick_ms.value, "section_map": map_ms.value,
-                           "moments": mom_ms.value, "ion_chain": chain_ms.value,
-                           "map_moments_pass": pass_ms.value,
-                           "longitudinal_tail": tail_ms.value},
-            "roofline": {"bound": "fp64", "kernel": "k_ion_kick (electron-side Bassetti-Erskine)",
-                         "achieved": achieved / 1e12, "peak": peak.value / 1e12, "unit": "TFLOP/s",
-                         "frac": achieved / peak.value if peak.value else None,
-                         "peak_source": "measured FP64 FMA throughput (cg_fp64_peak)",
-                         "algorithmic_flops_per_kick": flops_per_kick, "traffic": traffic,
-                         "traffic_source": "profiles/k_ion_kick_fast_ion.md (ncu, one segment launch scaled to the full beam by tiles)"},
-            "ion_chain": {"us_per_ip": 1e3 * chain_ms.value,
-                          "us_per_bunch_step": 1e3 * chain_ms.value / wl.n_bunches,
-                          "bound": "latency (one field evaluation per bunch step)"},
+            "ion_kicks_per_s": (copies * n_part * K * args.steps / (tot_ms * 1e-3)) if ions else None,
+            "kernels_ms": kms,
+            "roofline": top,
             "cpu_baseline": cpu,
             "autotune": {"kick_shapes_ms": None if tune[1] is None else
                          [round(float(x), 5) for x in tune[1][:-2]],
@@ -432,10 +579,25 @@ def main():
 FLOPS_PER_KICK = 438
 
 
+def measured_peak(key):
+    """(value, source) of a peak from MEASURED_PEAKS.json beside this file,
+    else the pool's earlier measurement."""
+    fallback = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            v = json.load(f).get(key)
+        if v:
+            return float(v), f"measured ({key}, MEASURED_PEAKS.json)"
+    except (OSError, ValueError):
+        pass
+    return fallback[key], f"fallback ({key} of an earlier measurement on this pool)"
+
+
 def surrogate_leg(args, beam, lib, stream, flush, exact_kick_ms, exact_turn_ms):
     """The learned field in place of the exact one: trains the surrogate on the
     GPU (2^20 exact-field samples), then times its kick kernel and whole turns
-    with it, the same way as the exact path."""
+    with it, the same way as the exact path, and audits it against the exact
+    field on the live beam."""
     import torch
     from cetasim_b200 import surrogate as S
     w, st = S.train()
@@ -459,26 +621,40 @@ def surrogate_leg(args, beam, lib, stream, flush, exact_kick_ms, exact_turn_ms):
     audit = beam.surrogate_audit(beam.wl.cfg.n_sections - 1)
     beam.set_surrogate(None)
     n = beam.wl.n_particles
+    K = beam.wl.cfg.n_sections
+    peak = measured_peak("bf16_tflops")
+    bf16 = 17024.0 * n / (k_ms.value * 1e-3) / 1e12
     return {"network": "3-64-64-64-2 SiLU, BF16 weights, FP32 accumulation, tcgen05",
             "holdout_rms_rel": st[1], "holdout_max_rel": st[2], "train_s": st[3],
+            "field_error_target": 1e-3,
+            "audit_max_field_err_rel": audit[0] / audit[1] if audit[1] else None,
             "kick_ms": k_ms.value, "exact_kick_ms": exact_kick_ms,
-            "kick_speedup": exact_kick_ms / k_ms.value,
             "ion_kicks_per_s_kernel": n / (k_ms.value * 1e-3),
+            "exact_ion_kicks_per_s_kernel": n / (exact_kick_ms * 1e-3),
+            "kick_speedup": exact_kick_ms / k_ms.value,
+            "ion_kicks_per_s": n * K / (turn_ms * 1e-3),
+            "exact_ion_kicks_per_s": n * K / (exact_turn_ms * 1e-3),
             "ms_per_turn": turn_ms, "exact_ms_per_turn": exact_turn_ms,
-            "turn_speedup": exact_turn_ms / turn_ms,
-            "audit_max_field_err_rel": audit[0] / audit[1] if audit[1] else None}
+            "turn_speedup": exact_turn_ms / turn_ms, "target_speedup": 5.0,
+            "kick_bf16_tflops": bf16, "kick_bf16_frac": bf16 / peak[0],
+            "bf16_peak_source": peak[1]}
 
 
-def kick_traffic():
-    """DRAM bytes per k_ion_kick launch from the committed ncu summary."""
+def kernel_traffic(workload, kernel):
+    """DRAM bytes per launch of a kernel from the committed ncu summary of
+    that kernel on that workload (profiles/<kernel>_<workload>.md, the line
+    'dram bytes read / written per launch | R MB / W MB'), or None."""
     import re
+    name = kernel.split()[0]
+    if name == "ion":
+        name = "k_ion_walk"
     try:
-        txt = open(os.path.join(ROOT, "profiles", "k_ion_kick_fast_ion.md")).read()
+        txt = open(os.path.join(ROOT, "profiles", f"{name}_{workload}.md")).read()
     except OSError:
         return None
-    # the full-beam line (the last one of the summary)
     m = re.findall(r"dram bytes read / written per launch \| ([\d.]+) MB / ([\d.]+) MB", txt)
     return (float(m[-1][0]) + float(m[-1][1])) * 1e6 if m else None
+
 
 if __name__ == "__main__":
     main()

@@ -163,6 +163,8 @@ EXPORTS = [
     ("cg_turn_launches", I, [C.c_void_p, PI]),
     ("cg_time_stage", I, [C.c_void_p, I, I, I, PD]),
     ("cg_fp64_peak", I, [PD]),
+    ("cg_field_chain_latency", I, [PD]),
+    ("cg_eigen_emit", I, [C.c_void_p, I, PD]),
     ("cg_ion_count", I, [C.c_void_p, I, I, PI]),
     ("cg_ion_download", I, [C.c_void_p, I, I, PD, PD, PD, PD, I, PI]),
     ("cg_ion_upload", I, [C.c_void_p, I, I, PD, PD, PD, PD, I]),

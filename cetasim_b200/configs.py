@@ -135,12 +135,14 @@ class Workload:
 def make(name: str, n_scale: float = 1.0, turns_lr: int = 10, lib=None, seed: int = 1234,
          derive=None, lattice_init=None, bunch_current: float | None = None) -> Workload:
     """Builds a workload.  `n_scale` scales macroparticle counts (tests use
-    small values); `derive`/`lattice_init` default to the library's own
-    cg_config_derive / cg_lattice_init (tests may pass the oracle's)."""
+    small values); `derive(cfg_ref)` / `lattice_init(ring_ref, sections, n)`
+    default to the library's own cg_config_derive / cg_lattice_init (the
+    oracle's or_config_derive / or_lattice_init take the same arguments, so a
+    process that must not load the library passes those)."""
     if derive is None or lattice_init is None:
         L = lib or _abi.load()
-        derive = derive or (lambda c: L.cg_config_derive(C_ref(c)))
-        lattice_init = lattice_init or (lambda r, s, n: L.cg_lattice_init(C_ref(r), s, n))
+        derive = derive or L.cg_config_derive
+        lattice_init = lattice_init or L.cg_lattice_init
     if name == "plain_single":
         K, M = 1, 1
         n_macro = [max(1, int(1e5 * n_scale))]
@@ -165,10 +167,10 @@ def make(name: str, n_scale: float = 1.0, turns_lr: int = 10, lib=None, seed: in
     if name == "large_trapping":
         cfg.ring.harmonics = 4000
         cfg.ring.cav_vol[0] = rf_voltage_for_nus(0.0049, 4000)
-    if derive(cfg) != 0:
+    if derive(C_ref(cfg)) != 0:
         raise RuntimeError("cg_config_derive failed")
     secs = ring_sections(cfg.ring, K)
-    if lattice_init(cfg.ring, secs, K) != 0:
+    if lattice_init(C_ref(cfg.ring), secs, K) != 0:
         raise RuntimeError("cg_lattice_init failed")
     cfg.n_sections = K
     cfg.sections = C_cast(secs)

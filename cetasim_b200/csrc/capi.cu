@@ -83,6 +83,8 @@ int check_status(Handle& h) {
     return fail(&h, CG_ERR_INVALID, "long-range wake lag outside the wake table (tau > 0)");
   if (st & kStatusCopyWait)
     return fail(&h, CG_ERR_TIMEOUT, "a bulk-copy completion wait of the map pass gave up");
+  if (st & kStatusGaussCut)
+    return fail(&h, CG_ERR_INVALID, "an initial-distribution draw found no sample inside the 3-sigma cut");
   return fail(&h, CG_ERR_CUDA, "unknown device status");
 }
 
@@ -1307,6 +1309,76 @@ int cg_fp64_peak(double* flops) {
   return CG_OK;
 }
 
+// MPBunch::GetEigenEmit (MPBunch.cpp:500-658) for bunch j: the ten second
+// moments on the device (k_eigen_sums), the 4 x 4 algebra here: Sigma J4
+// squared, its trace, det(Sigma) by LU with partial pivoting, the two
+// eigen-emittances, the 4-D emittance and the x-y tilt of the beam ellipse.
+int cg_eigen_emit(cg_handle* H, int j, double* out4) {
+  STAGE_PROLOGUE
+  if (!out4) return fail(&h, CG_ERR_INVALID, "null output");
+  if (j < 0 || j >= h.M) return fail(&h, CG_ERR_INVALID, "bunch index out of range");
+  if (j < h.sh_j0 || j >= h.sh_j1) return fail(&h, CG_ERR_INVALID, "bunch held by another rank");
+  int st = launch_ok(h, launch_eigen_sums(h, j, h.d.scratch), "eigen sums");
+  if (st) return st;
+  double a[10];
+  CG_CUDA(&h, cudaMemcpyAsync(a, h.d.scratch, sizeof a, cudaMemcpyDeviceToHost, h.stream));
+  CG_CUDA(&h, cudaStreamSynchronize(h.stream));
+  const double n = (double)h.n_macro[j];
+  for (double& v : a) v /= n;
+  const double S[4][4] = {{a[0], a[1], a[2], a[3]}, {a[1], a[4], a[5], a[6]},
+                          {a[2], a[5], a[7], a[8]}, {a[3], a[6], a[8], a[9]}};
+  // J4 = [[0,1,0,0],[-1,0,0,0],[0,0,0,1],[0,0,-1,0]]: (S J4)[i][0] = -S[i][1],
+  // [i][1] = S[i][0], [i][2] = -S[i][3], [i][3] = S[i][2]
+  double CJ[4][4];
+  for (int i = 0; i < 4; ++i) {
+    CJ[i][0] = -S[i][1];
+    CJ[i][1] = S[i][0];
+    CJ[i][2] = -S[i][3];
+    CJ[i][3] = S[i][2];
+  }
+  double tr = 0;
+  for (int i = 0; i < 4; ++i)
+    for (int k = 0; k < 4; ++k) tr += CJ[i][k] * CJ[k][i];
+  double L[4][4];
+  std::memcpy(L, S, sizeof L);
+  double det = 1;
+  for (int c = 0; c < 4; ++c) {
+    int p = c;
+    for (int r = c + 1; r < 4; ++r)
+      if (std::fabs(L[r][c]) > std::fabs(L[p][c])) p = r;
+    if (p != c) {
+      for (int k = 0; k < 4; ++k) std::swap(L[c][k], L[p][k]);
+      det = -det;
+    }
+    det *= L[c][c];
+    if (L[c][c] == 0) break;
+    for (int r = c + 1; r < 4; ++r) {
+      const double f = L[r][c] / L[c][c];
+      for (int k = c + 1; k < 4; ++k) L[r][k] -= f * L[c][k];
+    }
+  }
+  const double disc = std::sqrt(tr * tr - 16 * det);
+  out4[0] = std::sqrt(-tr + disc) / 2;
+  out4[1] = std::sqrt(-tr - disc) / 2;
+  out4[2] = std::sqrt(std::sqrt(det));
+  const double A = a[0], B = a[2], Cc = a[7];
+  const double lambda = (A + Cc) / 2 + std::sqrt((A - Cc) * (A - Cc) / 4 + B * B);
+  out4[3] = B == 0 ? (A >= Cc ? 0.0 : 2 * std::atan(1.0)) : std::atan2(lambda - A, B);
+  return CG_OK;
+}
+
+int cg_field_chain_latency(double* us_per_step) {
+  if (!us_per_step) return CG_ERR_INVALID;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(nullptr, CG_ERR_CUDA, "no CUDA device available");
+  double v = 0;
+  cudaError_t e = measure_field_chain_latency(&v);
+  if (e != cudaSuccess) return fail(nullptr, CG_ERR_CUDA, cudaGetErrorString(e));
+  *us_per_step = v;
+  return CG_OK;
+}
+
 // ---- ion clouds ----
 
 static int cloud_index(Handle& h, int k, int p) { return k * h.P + p; }
@@ -1817,21 +1889,33 @@ int cg_autotune_pipeline(cg_handle* H, int turn0, int reps, int* shape, double* 
   if (st) return st;
   std::vector<char> keep(n);
   if ((st = cg_checkpoint_save(H, keep.data(), n))) return st;
+  // the shape in effect before the call, put back on every failure path
+  const int old_groups = h.pipe_groups, old_ions = h.walk_ions, old_ramp = h.pipe_ramp ? 1 : 0;
+  // a failed trial: the beam and clouds as they were and the old shape; a
+  // failed restore is reported (it means the handle holds the trial's state)
+  auto restore = [&](int trial_st) -> int {
+    const int ls = cg_checkpoint_load(H, keep.data(), n);
+    const int ps = cg_set_pipeline(H, old_groups, old_ions, old_ramp);
+    if (ls) return fail(&h, ls, "autotune trial failed and the beam could not be restored");
+    return trial_st ? trial_st : ps;
+  };
   cudaEvent_t e0, e1;
   CG_CUDA(&h, cudaEventCreate(&e0));
   CG_CUDA(&h, cudaEventCreate(&e1));
   int best = -1;
   double best_ms = 0;
   for (int v = 0; v < CG_PIPE_SHAPES && !st; ++v) {
-    if ((st = cg_set_pipeline(H, kPipeShapes[v][0], kPipeShapes[v][1], kPipeShapes[v][2])))
+    if ((st = cg_set_pipeline(H, kPipeShapes[v][0], kPipeShapes[v][1], kPipeShapes[v][2]))) {
+      st = restore(st);
       break;
+    }
     if ((st = cg_run_turns(H, turn0, 1))) {  // captures the turn graph
-      cg_checkpoint_load(H, keep.data(), n);  // the beam as it was, whatever failed
+      st = restore(st);
       break;
     }
     cudaEventRecord(e0, h.stream);
     if ((st = cg_run_turns(H, turn0 + 1, reps))) {
-      cg_checkpoint_load(H, keep.data(), n);
+      st = restore(st);
       break;
     }
     cudaEventRecord(e1, h.stream);
@@ -1844,7 +1928,10 @@ int cg_autotune_pipeline(cg_handle* H, int turn0, int reps, int* shape, double* 
       best = v;
       best_ms = per;
     }
-    st = cg_checkpoint_load(H, keep.data(), n);
+    if ((st = cg_checkpoint_load(H, keep.data(), n))) {
+      st = restore(st);
+      break;
+    }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);

@@ -1051,8 +1051,17 @@ cudaError_t launch_turn_advance(Handle& h) {
 // ---------------------------------------------------------------------------
 // Seeded initial distribution: MPBunch::DistriGenerator type 3
 // (MPBunch.cpp:134-277) with counter-based draws: (z, dp) Gaussian cut at
-// 3 sigma jointly, transverse Gaussian in action-angle cut at 3 sigma in
-// (x/rX)^2 + (y/rY)^2, plus dispersion (MPBunch.cpp:268-277).
+// 3 sigma jointly (MPBunch.cpp:134-152), transverse Gaussian cut at 3 sigma
+// in (x/rX)^2 + (y/rY)^2 (MPBunch.cpp:254-260), plus dispersion
+// (MPBunch.cpp:268-277).  The reference draws the 4-D action radially
+// (GSSlover) and splits it uniformly between the planes; for a Gaussian beam
+// that is the law of independent normals per plane, which is what is drawn
+// here.  As in the reference a rejected draw is drawn again until one is
+// accepted: each cut keeps 98.9 % of draws, so kGaussAttempts attempts all
+// fail with probability below 1e-1900; if that ever happens the particle
+// keeps the zero vector and the status word reports it (no draw outside the
+// cut is ever kept).
+constexpr uint32_t kGaussAttempts = 1024;
 
 __global__ void __launch_bounds__(kTile) k_gaussian(double* __restrict__ c, int64_t npad,
                                                     uint8_t* __restrict__ surv,
@@ -1060,7 +1069,8 @@ __global__ void __launch_bounds__(kTile) k_gaussian(double* __restrict__ c, int6
                                                     const BunchDev* __restrict__ bunch,
                                                     const SectionDev* __restrict__ sec0,
                                                     double emit_x, double emit_y, double sz,
-                                                    double sdp, double r_beta2, uint64_t seed) {
+                                                    double sdp, double r_beta2, uint64_t seed,
+                                                    int* __restrict__ status) {
   TileIdx t = tile_index(tile_bunch, bunch);
   if (!t.valid) {
     surv[t.g] = 0xFF;  // padding slot: never alive
@@ -1070,33 +1080,39 @@ __global__ void __launch_bounds__(kTile) k_gaussian(double* __restrict__ c, int6
   }
   const SectionDev& s = *sec0;
   const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32) ^ kStreamInitDist;
-  // both cuts keep ~99% of draws; at most 64 attempts (the last one is kept)
+  bool ok_l = false, ok_t = false;
   double z = 0, dp = 0;
-  for (uint32_t a = 0; a < 64; ++a) {
+  for (uint32_t a = 0; a < kGaussAttempts && !ok_l; ++a) {
     u32x4 ctr = {{(uint32_t)t.i, (uint32_t)t.b, a, 0u}};
     double g0, g1;
     normal2(philox4x32_10(ctr, k0, k1), &g0, &g1);
-    z = sz * g0;
-    dp = sdp * g1 / r_beta2;
-    if (g0 * g0 + g1 * g1 < 9.0) break;
+    if (g0 * g0 + g1 * g1 < 9.0) {
+      z = sz * g0;
+      dp = sdp * g1 / r_beta2;
+      ok_l = true;
+    }
   }
   double rx = sqrt(emit_x * s.beta_x), ry = sqrt(emit_y * s.beta_y);
   double x = 0, px = 0, y = 0, py = 0;
-  for (uint32_t a = 0; a < 64; ++a) {
+  for (uint32_t a = 0; a < kGaussAttempts && !ok_t; ++a) {
     u32x4 ctr = {{(uint32_t)t.i, (uint32_t)t.b, a, 1u}};
     double g0, g1, g2, g3;
     normal2(philox4x32_10(ctr, k0, k1), &g0, &g1);
     ctr.v[3] = 2u;
     normal2(philox4x32_10(ctr, k0, k1), &g2, &g3);
     // normalised phase space (u, u') ~ N(0, emit) per plane
-    double ux = sqrt(emit_x) * g0, upx = sqrt(emit_x) * g1;
-    double uy = sqrt(emit_y) * g2, upy = sqrt(emit_y) * g3;
-    x = sqrt(s.beta_x) * ux;
-    px = (upx - s.alpha_x * ux) / sqrt(s.beta_x);
-    y = sqrt(s.beta_y) * uy;
-    py = (upy - s.alpha_y * uy) / sqrt(s.beta_y);
-    if ((x / rx) * (x / rx) + (y / ry) * (y / ry) <= 9.0) break;
+    const double ux = sqrt(emit_x) * g0, upx = sqrt(emit_x) * g1;
+    const double uy = sqrt(emit_y) * g2, upy = sqrt(emit_y) * g3;
+    const double tx = sqrt(s.beta_x) * ux, ty = sqrt(s.beta_y) * uy;
+    if ((tx / rx) * (tx / rx) + (ty / ry) * (ty / ry) <= 9.0) {
+      x = tx;
+      px = (upx - s.alpha_x * ux) / sqrt(s.beta_x);
+      y = ty;
+      py = (upy - s.alpha_y * uy) / sqrt(s.beta_y);
+      ok_t = true;
+    }
   }
+  if (!(ok_l && ok_t)) atomicOr(status, kStatusGaussCut);
   x += s.eta_x * dp;
   y += s.eta_y * dp;
   px += s.etap_x * dp;
@@ -1111,7 +1127,50 @@ cudaError_t launch_gaussian(Handle& h, double emit_x, double emit_y, double sigm
   double rb2 = h.cfg.ring.r_beta * h.cfg.ring.r_beta;
   k_gaussian<<<h.n_tiles, kTile, 0, h.stream>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch,
                                                 h.d.bunch, h.sec_dev, emit_x, emit_y, sigma_z,
-                                                sigma_dp, rb2, seed);
+                                                sigma_dp, rb2, seed, h.d.status);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// The ten second moments of MPBunch::GetEigenEmit (MPBunch.cpp:500-560) for
+// one bunch: every particle (lost ones too), x, x', y, y' less the dispersion
+// of section 0 times dp, products taken about zero (the reference sums its
+// "means" with an int accumulator, MPBunch.cpp:516-519, so they stay zero),
+// not yet divided by n.  One CTA: per-thread sums in particle order, then a
+// fixed tree over the threads (deterministic).
+__global__ void __launch_bounds__(kTile) k_eigen_sums(const double* __restrict__ c, int64_t npad,
+                                                      const BunchDev* __restrict__ bunch, int j,
+                                                      const SectionDev* __restrict__ sec0,
+                                                      double* __restrict__ out) {
+  __shared__ double sh[10][kTile];
+  const BunchDev b = bunch[j];
+  const SectionDev& s = *sec0;
+  double a[10];
+#pragma unroll
+  for (int q = 0; q < 10; ++q) a[q] = 0.0;
+  const int64_t base = (int64_t)b.tile_off * kTile;
+  for (int i = threadIdx.x; i < b.n; i += kTile) {
+    const int64_t g = base + i;
+    const double dp = c[5 * npad + g];
+    const double x = c[g] - s.eta_x * dp, xp = c[npad + g] - s.etap_x * dp;
+    const double y = c[2 * npad + g] - s.eta_y * dp, yp = c[3 * npad + g] - s.etap_y * dp;
+    a[0] += x * x;   a[1] += x * xp;  a[2] += x * y;   a[3] += x * yp;  a[4] += xp * xp;
+    a[5] += xp * y;  a[6] += xp * yp; a[7] += y * y;   a[8] += y * yp;  a[9] += yp * yp;
+  }
+#pragma unroll
+  for (int q = 0; q < 10; ++q) sh[q][threadIdx.x] = a[q];
+  __syncthreads();
+  for (int w = kTile / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w)
+#pragma unroll
+      for (int q = 0; q < 10; ++q) sh[q][threadIdx.x] += sh[q][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x < 10) out[threadIdx.x] = sh[threadIdx.x][0];
+}
+
+cudaError_t launch_eigen_sums(Handle& h, int j, double* out) {
+  k_eigen_sums<<<1, kTile, 0, h.stream>>>(h.d.c, h.npad, h.d.bunch, j, h.sec_dev, out);
   return cudaGetLastError();
 }
 
@@ -1207,20 +1266,25 @@ cudaError_t upload_weideman_table() {
 // partials, the finished moments and the completion counter therefore live in
 // one file-scope device array of fixed size.
 //
-// Layout of the array (doubles): kNoAllocMaxTiles partials, then one
-// BunchMomDev slot (32 doubles), then the completion counter (32 doubles).
+// Layout of the array (doubles): one partial per CTA, i.e. per chunk of
+// kMomChunkTiles tiles (kNoAllocMaxChunks of them), then one BunchMomDev slot
+// (32 doubles), then the completion counter (32 doubles).
 // Only the counter must read zero when a call starts: it is zero at module
 // load, zeroed again when the address is first resolved on a device, and the
 // last CTA of every call puts it back to zero.  The partials and the moments
 // slot are written before they are read in every call.  Two calls that overlap
 // on one device (different streams, or different host threads without
 // ordering) share this array and race.
+constexpr int kNoAllocMaxChunks = kNoAllocMaxTiles / kMomChunkTiles;
 constexpr int kNoAllocPartialDoubles = (int)(sizeof(MomPartial) / sizeof(double));
-constexpr size_t kNoAllocMomOff = (size_t)kNoAllocMaxTiles * kNoAllocPartialDoubles;
+constexpr size_t kNoAllocMomOff = (size_t)kNoAllocMaxChunks * kNoAllocPartialDoubles;
 constexpr size_t kNoAllocCounterOff = kNoAllocMomOff + 32;
 constexpr size_t kNoAllocDoubles = kNoAllocCounterOff + 32;
 static_assert(sizeof(MomPartial) % sizeof(double) == 0, "partial is a whole number of doubles");
 static_assert(sizeof(BunchMomDev) <= 32 * sizeof(double), "moments slot holds a BunchMomDev");
+static_assert(kNoAllocMaxTiles % kMomChunkTiles == 0 &&
+                  (long long)kNoAllocMaxChunks * kMomChunkTiles * kTile >= CG_NOALLOC_MAX_PARTICLES,
+              "one partial per chunk covers the largest accepted call");
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
 
 cudaError_t noalloc_scratch_address(double** ptr) {
@@ -1281,6 +1345,7 @@ cudaError_t launch_moments_noalloc(const double* c, int64_t stride, const uint8_
                                    double beta_x, double beta_y, double* scratch,
                                    cg_bunch_moments* out, cudaStream_t s) {
   const int chunks = (n + kTile * kMomChunkTiles - 1) / (kTile * kMomChunkTiles);
+  if (n < 1 || chunks > kNoAllocMaxChunks) return cudaErrorInvalidValue;
   k_moments_noalloc<<<chunks, kTile, 0, s>>>(c, stride, surv, n, beta_x, beta_y, scratch);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;

@@ -12,6 +12,7 @@ enum : int {
   kStatusIonBirth = 8,
   kStatusSurrogateWait = 16,  // a tensor-core completion wait gave up
   kStatusCopyWait = 32,       // a bulk-copy completion wait gave up
+  kStatusGaussCut = 64,       // an initial-distribution draw found no accepted sample
 };
 
 cudaError_t launch_moments(Handle& h, int k);
@@ -107,5 +108,7 @@ cudaError_t launch_moments_noalloc(const double* c, int64_t stride, const uint8_
                                    double beta_x, double beta_y, double* scratch,
                                    cg_bunch_moments* out, cudaStream_t s);
 cudaError_t measure_fp64_peak(double* flops);
+cudaError_t measure_field_chain_latency(double* us_per_step);
+cudaError_t launch_eigen_sums(Handle& h, int j, double* out);
 
 }  // namespace cg

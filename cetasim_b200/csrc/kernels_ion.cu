@@ -529,6 +529,49 @@ cudaError_t upload_weideman_table_ion() {
   return cudaMemcpyToSymbol(c_weideman, &h_weideman, sizeof(WeidemanTable));
 }
 
+// Latency floor of the walk: one thread advances an ion through a dependent
+// chain of bunch passages (the walk's low-latency field, then the velocity
+// and position update), so each field evaluation waits for the previous one.
+// With c = 1e-13 the ion oscillates in the core of the Gaussian (period of
+// ~300 passages), where the walk spends its time (Weideman region of w(z)).
+__global__ void k_field_chain(double* out, int n) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double x = 3.0e-6, y = 2.0e-6, vx = 0.0, vy = 0.0;
+  const double sx = 1.4e-5, sy = 6.3e-6, c = 1.0e-13;
+  for (int i = 0; i < n; ++i) {
+    double fx, fy;
+    gaussian_field<true>(x, y, sx, sy, &fx, &fy);
+    vx += c * fx;
+    vy += c * fy;
+    x += vx;
+    y += vy;
+  }
+  out[0] = x + y;
+}
+
+cudaError_t measure_field_chain_latency(double* us_per_step) {
+  double* out = nullptr;
+  cudaError_t e = cudaMalloc(&out, sizeof(double));
+  if (e != cudaSuccess) return e;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int n = 4096;
+  k_field_chain<<<1, 32>>>(out, 64);  // warm-up
+  cudaEventRecord(e0);
+  k_field_chain<<<1, 32>>>(out, n);
+  cudaEventRecord(e1);
+  e = cudaEventSynchronize(e1);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  if (e != cudaSuccess) return e;
+  *us_per_step = 1e3 * (double)ms / n;
+  return cudaGetLastError();
+}
+
 int ion_walk_grid(int64_t tcap, int ions) {
   const int64_t blocks = (tcap + ions - 1) / ions;
   return (int)std::max<int64_t>(1, std::min<int64_t>(blocks, 148 * 4));

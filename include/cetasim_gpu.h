@@ -332,6 +332,18 @@ int cg_time_stage(cg_handle* h, int stage, int k, int reps, double* ms);
 /* FP64 FMA throughput of this device measured by a register-resident FMA
  * chain kernel, in FLOP/s (2 per FMA). */
 int cg_fp64_peak(double* flops);
+/* Latency of one bunch passage of the ion walk on this device, in us: one
+ * thread advances an ion through a dependent chain of Gaussian-field
+ * evaluations (the walk's low-latency w(z)) and velocity / position updates.
+ * The floor of the sequential ion chain, which needs one passage per bunch. */
+int cg_field_chain_latency(double* us_per_step);
+
+/* MPBunch::GetEigenEmit (MPBunch.cpp:500-658) of bunch j, the diagnostic
+ * result.sdds prints for the TBT bunches: out4 = {eigenEmitX, eigenEmitY,
+ * emitXY4D, xyCouplingAlpha}.  Second moments about zero (the reference's
+ * means are summed in an int and vanish) over every particle of the bunch,
+ * lost ones included, with section 0's dispersion removed; synchronous. */
+int cg_eigen_emit(cg_handle* h, int j, double* out4);
 
 /* ---- ion clouds (LatticeInterActionPoint ion state) ---- */
 
@@ -579,17 +591,17 @@ int cg_surrogate_audit_stats(cg_handle* h, int* count, double* last, double* wor
 /* Largest n of one cg_bunch_moments_noalloc call (4096 tiles of 256). */
 #define CG_NOALLOC_MAX_PARTICLES 1048576
 
-/* No counterpart in the reference.  The moments MPBunch::GetMPBunchRMS sets
- * (MPBunch.cpp:342-498; the same kernels and merge order as cg_beam_rms) for
- * one bunch whose particles sit in the caller's DEVICE memory: d_coords holds
+/* No counterpart in the reference.  The moments of cg_beam_rms for one
+ * bunch whose particles sit in the caller's DEVICE memory: d_coords holds
  * x, px, y, py, z, dp as six rows of `stride` doubles, d_surv one flag per
  * particle (0 = alive), and the result is written to *d_out in device memory
  * (n_macro = n, transmission = n_alive / n).  Work is enqueued on `stream`
  * (a cudaStream_t; NULL = legacy default stream) of the current device and
  * the call returns without waiting.
  *
- * It never allocates: the partials live in a fixed static device array of
- * CG_NOALLOC_MAX_PARTICLES / 256 tiles (about 577 KB per device), and
+ * It never allocates: the partials live in a fixed static device array,
+ * one per CTA of 1024 particles (CG_NOALLOC_MAX_PARTICLES / 1024 of them,
+ * about 148 KB per device, held by every device that loads the library), and
  * n > CG_NOALLOC_MAX_PARTICLES is rejected with CG_ERR_INVALID.  The first
  * call on each device resolves that array's address and zeroes its
  * completion counter with a synchronous memset, so make it before any stream

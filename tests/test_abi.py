@@ -43,11 +43,11 @@ def test_struct_layouts_match_c(built):
     assert list(sizes) == py
 
 
-@pytest.mark.parametrize("name", ["plain_single", "fast_ion", "batched_uneven"])
+@pytest.mark.parametrize("name", ["plain_single", "fast_ion", "batched_uneven", "large_trapping"])
 def test_derivations_match_oracle_bitwise(lib, name):
     a = configs.make(name, n_scale=0.001)
-    b = configs.make(name, n_scale=0.001, derive=lambda c: oracle.config_derive(C.byref(c)),
-                     lattice_init=lambda r, s, n: oracle.lattice_init(C.byref(r), s, n))
+    b = configs.make(name, n_scale=0.001, derive=oracle.config_derive,
+                     lattice_init=oracle.lattice_init)
     ra, rb = a.cfg.ring, b.cfg.ring
     for f, _ in _abi.Ring._fields_:
         va, vb = getattr(ra, f), getattr(rb, f)

@@ -86,3 +86,39 @@ def test_gpu_and_reference_side_by_side_fast_ion_ip_records(tmp_path):
             assert np.array_equal(sr, sg)
             worst = max(worst, refcases.coord_rel_err(cg, cr, sr == 0).max())
         assert worst <= 1e-11, f"IP {k}: {worst:.3e}"
+
+
+@pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
+def test_initial_distribution_statistics_match_the_reference_generator(tmp_path):
+    """k_gaussian against the reference's own MPBunch::DistriGenerator
+    (type 3, MPBunch.cpp:98-298), which the reference build ran when it set
+    the beam up: 1e5 macroparticles each.  Both keep every draw inside the
+    3-sigma cuts; second moments agree within 5 sampling sigmas (2.5 %), and
+    the normalised transverse amplitude and longitudinal radius have the same
+    law (two-sample Kolmogorov-Smirnov)."""
+    from scipy import stats
+    from cetasim_b200 import configs, input_dat
+    wl = configs.make("plain_single", n_scale=1.0)
+    path = input_dat.write_case(str(tmp_path), wl, n_turns=1)
+    wl = input_dat.load_case(path)
+    r = ref.RefBeam(path, seed=11)
+    cr, _ = r.download(0)
+    g = MPBeam(wl)
+    g.generate(seed=11)
+    cg, sg = g.download(0)
+    assert (sg == 0).all()
+    s0 = wl.sections[0]
+    ex, ey, sz, sdp = wl.gen
+    rb2 = wl.cfg.ring.r_beta ** 2
+    for c in (cr, cg):
+        # the cuts of MPBunch.cpp:145 and :256
+        assert np.all((c[4] / sz) ** 2 + (c[5] * rb2 / sdp) ** 2 < 9.0)
+        assert np.all(c[0] ** 2 / (ex * s0.beta_x) + c[2] ** 2 / (ey * s0.beta_y) <= 9.0)
+    n = cr.shape[1]
+    for d in range(6):
+        vr, vg = np.var(cr[d]), np.var(cg[d])
+        assert abs(vg / vr - 1) <= 5 * np.sqrt(2 / n), (d, vg / vr)
+    ax = lambda c: c[0] ** 2 / (ex * s0.beta_x) + c[1] ** 2 * s0.beta_x / ex
+    lz = lambda c: (c[4] / sz) ** 2 + (c[5] * rb2 / sdp) ** 2
+    for f in (ax, lz):
+        assert stats.ks_2samp(f(cr), f(cg)).pvalue > 1e-4

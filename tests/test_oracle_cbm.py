@@ -54,18 +54,25 @@ def test_analytic_signal_of_an_odd_length_record():
 def test_iq_scan_phase_form_equals_the_reference_form():
     """The IQ average with the phase (k + Q) h / H (f0 t0 = 1) against the
     reference's form exp(-i 2 pi f t) with f = (k + Q) f0 and t = h t0 / H
-    evaluated in floating point (MPBeam.cpp:153-158, 1597-1611)."""
+    evaluated in floating point (MPBeam.cpp:153-158, 1597-1611): amplitude
+    and argument (arg of the average, MPBeam.cpp:1617-1619) in all three
+    planes."""
     rng = np.random.default_rng(4)
-    M, H, Q = 80, 3840, 18.213
+    M, H = 80, 3840
+    tunes = (18.213, 10.137, 0.0049)
     harm = np.sort(rng.choice(H, M, replace=False))
     t0 = 2.3057e-6
     f0 = 1.0 / t0
-    u = rng.normal(0, 1e-5, M)
     mean = np.zeros((M, 6))
-    mean[:, 0] = u
-    _, _, _, iq_amp, iq_arg = cbm.cbm_record(mean, harm, H, (10.0, 5.0), (0.0, 0.0),
-                                            (Q, 10.1, 0.01), 1.0)
+    for pl in range(3):
+        mean[:, 2 * pl] = rng.normal(0, 1e-5, M) * (1 + pl)
+    _, _, _, iq_amp, iq_arg = cbm.cbm_record(mean, harm, H, (10.0, 5.0), (0.0, 0.0), tunes, 1.0)
     t = harm * (t0 / H)
-    for k in range(M):
-        ref = np.mean(u * np.exp(-1j * 2.0 * np.pi * ((k + Q) * f0) * t))
-        assert abs(iq_amp[0, k] - abs(ref)) <= 1e-11 * np.abs(u).max()
+    for pl in range(3):
+        u = mean[:, 2 * pl]
+        for k in range(M):
+            ref = np.mean(u * np.exp(-1j * 2.0 * np.pi * ((k + tunes[pl]) * f0) * t))
+            assert abs(iq_amp[pl, k] - abs(ref)) <= 1e-11 * np.abs(u).max()
+            if abs(ref) > 1e-3 * np.abs(u).max():
+                d = np.angle(np.exp(1j * (iq_arg[pl, k] - np.angle(ref))))
+                assert abs(d) <= 1e-8, (pl, k, d)
