@@ -188,6 +188,9 @@ EXPORTS = [
     ("cg_set_kick_variant", I, [C.c_void_p, I]),
     ("cg_autotune", I, [C.c_void_p, I, I, PI, PD]),
     ("cg_shard_plan", I, [PI, I, I, PI, PI]),
+    ("cg_shard_exchange_size", I, [PI, I, I, PI]),
+    ("cg_shard_pack", I, [PI, I, I, I, C.c_void_p, C.c_size_t, C.c_void_p]),
+    ("cg_shard_unpack", I, [PI, I, I, C.c_void_p, C.c_size_t, C.c_void_p]),
     ("cg_nccl_unique_id", I, [C.c_void_p]),
     ("cg_set_shard", I, [C.c_void_p, I, I, C.c_void_p]),
     ("cg_shard_range", I, [C.c_void_p, PI, PI]),

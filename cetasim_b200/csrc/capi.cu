@@ -540,12 +540,10 @@ int cg_set_beam(cg_handle* H, int M, const int* n_macro, const int* harm, const 
   h.tile_off.assign(M + 1, 0);
   int tiles = 0, chunks = 0;
   // bunch sharding: this rank tracks the particles of bunches [j0, j1)
-  std::vector<int> sj0(h.sh_world, 0), sj1(h.sh_world, M);
-  if (h.sh_world > 1) shard_plan(n_macro, M, h.sh_world, sj0.data(), sj1.data());
-  h.sh_j0 = sj0[h.sh_rank];
-  h.sh_j1 = sj1[h.sh_rank];
-  h.sh_maxlocal = 0;
-  for (int r = 0; r < h.sh_world; ++r) h.sh_maxlocal = std::max(h.sh_maxlocal, sj1[r] - sj0[r]);
+  const ShardLayout lay = shard_layout(n_macro, M, h.sh_world);
+  h.sh_j0 = lay.j0[h.sh_rank];
+  h.sh_j1 = lay.j1[h.sh_rank];
+  h.sh_maxlocal = lay.max_local;
   for (int j = 0; j < M; ++j) {
     const bool local = j >= h.sh_j0 && j < h.sh_j1;
     int nt = local ? (n_macro[j] + kTile - 1) / kTile : 0;
@@ -596,10 +594,8 @@ int cg_set_beam(cg_handle* H, int M, const int* n_macro, const int* harm, const 
       free_beam(h);
       return fail(&h, CG_ERR_OOM, "shard exchange buffers");
     }
-    std::vector<int> cnt(W);
-    for (int r = 0; r < W; ++r) cnt[r] = sj1[r] - sj0[r];
-    cudaMemcpy(d.sh_off, sj0.data(), sizeof(int) * W, cudaMemcpyHostToDevice);
-    cudaMemcpy(d.sh_cnt, cnt.data(), sizeof(int) * W, cudaMemcpyHostToDevice);
+    cudaMemcpy(d.sh_off, lay.j0.data(), sizeof(int) * W, cudaMemcpyHostToDevice);
+    cudaMemcpy(d.sh_cnt, lay.cnt.data(), sizeof(int) * W, cudaMemcpyHostToDevice);
     cudaMemset(d.mom_send, 0, sizeof(BunchMomDev) * ml);
   }
   cudaMemcpy(d.bunch, bd.data(), sizeof(BunchDev) * M, cudaMemcpyHostToDevice);
@@ -1664,6 +1660,32 @@ int cg_shard_plan(const int* n_macro, int M, int world, int* j0, int* j1) {
   if (!n_macro || !j0 || !j1 || M < 1 || world < 1)
     return fail(nullptr, CG_ERR_INVALID, "bad shard plan arguments");
   shard_plan(n_macro, M, world, j0, j1);
+  return CG_OK;
+}
+
+int cg_shard_exchange_size(const int* n_macro, int M, int world, int* max_local) {
+  if (!n_macro || !max_local || M < 1 || world < 1 || world > M)
+    return fail(nullptr, CG_ERR_INVALID, "bad shard exchange arguments");
+  *max_local = shard_layout(n_macro, M, world).max_local;
+  return CG_OK;
+}
+
+int cg_shard_pack(const int* n_macro, int M, int world, int rank, const void* records,
+                  size_t rec_bytes, void* send) {
+  if (!n_macro || !records || !send || M < 1 || world < 1 || world > M || rank < 0 ||
+      rank >= world || rec_bytes == 0)
+    return fail(nullptr, CG_ERR_INVALID, "bad shard pack arguments");
+  shard_pack_host(shard_layout(n_macro, M, world), rank, (const unsigned char*)records, rec_bytes,
+                  (unsigned char*)send);
+  return CG_OK;
+}
+
+int cg_shard_unpack(const int* n_macro, int M, int world, const void* gathered, size_t rec_bytes,
+                    void* records) {
+  if (!n_macro || !gathered || !records || M < 1 || world < 1 || world > M || rec_bytes == 0)
+    return fail(nullptr, CG_ERR_INVALID, "bad shard unpack arguments");
+  shard_unpack_host(shard_layout(n_macro, M, world), (const unsigned char*)gathered, rec_bytes,
+                    (unsigned char*)records);
   return CG_OK;
 }
 

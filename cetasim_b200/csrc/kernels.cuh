@@ -64,6 +64,15 @@ cudaError_t launch_field(const double* x, const double* y, const double* sx, con
                          double* fx, double* fy, int64_t n, cudaStream_t s);
 // bunch sharding (shard.cu)
 void shard_plan(const int* n_macro, int M, int world, int* j0, int* j1);
+struct ShardLayout {
+  std::vector<int> j0, j1, cnt;  // bunch range and count of each rank
+  int max_local = 0;             // records per rank slot of the all-gather
+};
+ShardLayout shard_layout(const int* n_macro, int M, int world);
+void shard_pack_host(const ShardLayout& L, int rank, const unsigned char* records, size_t rec,
+                     unsigned char* send);
+void shard_unpack_host(const ShardLayout& L, const unsigned char* gathered, size_t rec,
+                       unsigned char* records);
 cudaError_t exchange_moments(Handle& h);
 int nccl_unique_id(void* out);
 int nccl_comm_init(void** comm, int world, const void* id, int rank);

@@ -80,6 +80,40 @@ void shard_plan(const int* n_macro, int M, int world, int* j0, int* j1) {
   }
 }
 
+// The exchange layout of a plan: rank r owns bunches [j0[r], j1[r]) and
+// sends its records as one slot of max_local records (padded), so the
+// all-gather output holds rank r's records at slot r; j0 / cnt place them.
+ShardLayout shard_layout(const int* n_macro, int M, int world) {
+  ShardLayout L;
+  L.j0.assign(world, 0);
+  L.j1.assign(world, M);
+  if (world > 1) shard_plan(n_macro, M, world, L.j0.data(), L.j1.data());
+  L.cnt.resize(world);
+  L.max_local = 0;
+  for (int r = 0; r < world; ++r) {
+    L.cnt[r] = L.j1[r] - L.j0[r];
+    L.max_local = std::max(L.max_local, L.cnt[r]);
+  }
+  return L;
+}
+
+// Host form of the exchange's two local steps (the device runs the same
+// layout with a copy and k_scatter_moments around the NCCL all-gather):
+// pack copies this rank's records into its send slot (zero padding), unpack
+// places every rank's slot of the gathered buffer at its bunches.
+void shard_pack_host(const ShardLayout& L, int rank, const unsigned char* records, size_t rec,
+                     unsigned char* send) {
+  std::memset(send, 0, (size_t)L.max_local * rec);
+  std::memcpy(send, records + (size_t)L.j0[rank] * rec, (size_t)L.cnt[rank] * rec);
+}
+
+void shard_unpack_host(const ShardLayout& L, const unsigned char* gathered, size_t rec,
+                       unsigned char* records) {
+  for (size_t r = 0; r < L.cnt.size(); ++r)
+    std::memcpy(records + (size_t)L.j0[r] * rec, gathered + r * (size_t)L.max_local * rec,
+                (size_t)L.cnt[r] * rec);
+}
+
 __global__ void k_scatter_moments(const BunchMomDev* __restrict__ all, BunchMomDev* mom,
                                   const int* __restrict__ off, const int* __restrict__ cnt,
                                   int world, int maxlocal) {

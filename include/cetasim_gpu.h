@@ -509,6 +509,19 @@ int cg_trace_turn(cg_handle* h, int turn0, cg_trace_record* out, int cap, int* n
 /* Contiguous bunch ranges [j0[r], j1[r]) of `world` ranks, balanced by
  * macroparticle count (host only). */
 int cg_shard_plan(const int* n_macro, int M, int world, int* j0, int* j1);
+/* The moments exchange of a bunch-sharded run with the transport left to the
+ * caller (host memory, no GPU): the same layout and the same pack / place
+ * steps as the device exchange around its NCCL all-gather.  Each rank packs
+ * its own bunches' records (records = M records of rec_bytes, only this
+ * rank's range read) into send (max_local records, zero padded); the
+ * caller all-gathers the world send buffers in rank order into gathered
+ * (world x max_local records); unpack writes every rank's records at their
+ * bunches of records. */
+int cg_shard_exchange_size(const int* n_macro, int M, int world, int* max_local);
+int cg_shard_pack(const int* n_macro, int M, int world, int rank, const void* records,
+                  size_t rec_bytes, void* send);
+int cg_shard_unpack(const int* n_macro, int M, int world, const void* gathered,
+                    size_t rec_bytes, void* records);
 /* An NCCL unique id (128 bytes) for cg_set_shard; rank 0 makes it, the
  * caller broadcasts it (e.g. with torch.distributed). */
 int cg_nccl_unique_id(void* id);
