@@ -141,12 +141,17 @@ __device__ bool sur_gemm(uint8_t* base, uint32_t b_off, uint32_t tmem, uint32_t 
   return ok;
 }
 
-// Network input normalisation: (a, b, r) -> [-1, 1]^3.
+// Network input normalisation: (a, b, r) -> [-1, 1]^3, the aspect ratio on a
+// logarithmic scale (flat beams get as much of the input range as round ones).
 __device__ __forceinline__ void sur_norm(float a, float b, float r, float (&x)[3]) {
   x[0] = fmaf(2.0f, a, -1.0f);
   x[1] = fmaf(2.0f, b, -1.0f);
-  x[2] = fmaf(2.0f / (1.0f - (float)kSurRmin), r - (float)kSurRmin, -1.0f);
+  x[2] = fmaf(kSurLogScale, logf(r) - kSurLogRmin, -1.0f);
 }
+
+// a and b back from the normalised inputs (the factors of the odd outputs)
+__device__ __forceinline__ float sur_a(const float (&x)[3]) { return 0.5f * (x[0] + 1.0f); }
+__device__ __forceinline__ float sur_b(const float (&x)[3]) { return 0.5f * (x[1] + 1.0f); }
 
 // Forward pass of this thread's row; z1/z2/z3 (row stride kZs) are saved
 // when non-null.
@@ -180,8 +185,11 @@ __device__ bool sur_forward(uint8_t* base, const SurSmall& sm, uint32_t tmem, ui
     o0 = fmaf(sm.w4[j], hj, o0);
     o1 = fmaf(sm.w4[kSurH + j], hj, o1);
   }
-  out[0] = o0;
-  out[1] = o1;
+  // G_x = a N_x, G_y = b N_y: the field is odd in x and in y, so the
+  // outputs vanish exactly on the axes (no jump across x = 0 or y = 0 once
+  // the signs are restored)
+  out[0] = sur_a(x) * o0;
+  out[1] = sur_b(x) * o1;
   return ok;
 }
 
@@ -201,8 +209,8 @@ __device__ __forceinline__ void sur_end(uint32_t tmem) {
 }
 
 // ---------------------------------------------------------------------------
-// Training data: (a, b, r) uniform (Philox stream kStreamSurrogate, counter
-// {i, 0, 0, 0}), target G = -sigma_x F at x = 8 a sigma_x, y = 8 b sigma_y
+// Training data: (a, b) uniform, r half uniform and half log-uniform
+// (Philox stream kStreamSurrogate, counter {i, 0, 0, 0}), target G = -sigma_x F at x = 8 a sigma_x, y = 8 b sigma_y
 // with sigma_x = 1, sigma_y = r, from the exact FP64 field with the
 // reference's dispatch (Bunch.cpp:119-211).
 
@@ -214,7 +222,11 @@ __global__ void k_sur_data(uint64_t seed, int64_t n, float* __restrict__ xin,
   const u32x4 q = philox4x32_10(ctr, (uint32_t)seed, (uint32_t)(seed >> 32) ^ kStreamSurrogate);
   const double a = (q.v[0] + 0.5) * (1.0 / 4294967296.0);
   const double b = (q.v[1] + 0.5) * (1.0 / 4294967296.0);
-  const double r = kSurRmin + (1.0 - kSurRmin) * ((q.v[2] + 0.5) * (1.0 / 4294967296.0));
+  // r: half the samples uniform in [rmin, 1], half log-uniform (flat beams,
+  // where the field bends fastest, get denser sampling)
+  const double ur = (q.v[2] + 0.5) * (1.0 / 4294967296.0);
+  const double r = (q.v[3] & 1u) ? exp(log(kSurRmin) * (1.0 - ur))
+                                 : kSurRmin + (1.0 - kSurRmin) * ur;
   double fx, fy;
   gaussian_field<false>(kSurRange * a, kSurRange * b * r, 1.0, r, &fx, &fy);
   xin[3 * i] = (float)a;
@@ -290,7 +302,8 @@ __global__ void __launch_bounds__(kSurRows) k_sur_train_tile(const float* __rest
   sur_norm(xin[3 * s], xin[3 * s + 1], xin[3 * s + 2], x);
   bool ok = sur_forward(base, sm, tmem, bar, phase, x, out, z1s, z2s, z3s);
   const float e0 = out[0] - tin[2 * s], e1 = out[1] - tin[2 * s + 1];
-  const float d0 = e0 * inv_batch, d1 = e1 * inv_batch;
+  // dL/d(layer-4 output): through the odd-output factors a, b
+  const float d0 = e0 * inv_batch * sur_a(x), d1 = e1 * inv_batch * sur_b(x);
   s_x[r][0] = x[0];
   s_x[r][1] = x[1];
   s_x[r][2] = x[2];

@@ -50,7 +50,7 @@ def gradient(weights, x, t):
     return loss.value, g
 
 
-def train(seed: int = 2024, n_train: int = 1 << 20, n_holdout: int = 1 << 16, epochs: int = 60,
+def train(seed: int = 2024, n_train: int = 1 << 20, n_holdout: int = 1 << 16, epochs: int = 150,
           batch: int = 2048, lr: float = 3e-3):
     """Trains on the GPU; returns (weights, stats) with stats = (final training
     loss per output, hold-out RMS error / peak |G|, hold-out max error / peak,

@@ -3,8 +3,9 @@
 FP64 restatement of the field surrogate (no reference counterpart: the MLP
 that replaces Bunch::BassettiErskine1 / GaussianField, Bunch.cpp:119-211, in
 the electron-ion kicks).  It follows the network definition of the library
-(cetasim_b200/csrc/surrogate.cu): inputs (a, b, r) normalised to [-1, 1]^3,
-three hidden layers of 64 SiLU units, two outputs; weights rounded to BF16
+(cetasim_b200/csrc/surrogate.cu): inputs (a, b, r) normalised to [-1, 1]^3
+(r on a log scale), three hidden layers of 64 SiLU units, two outputs
+multiplied by a and b (the field is odd in x and y); weights rounded to BF16
 (round to nearest even), biases FP32; loss L = sum (out - target)^2 / (2 n).
 Gradients are taken with respect to the BF16-rounded weights (the library
 applies them to its FP32 master copy).  The tests use it as the checker of
@@ -34,8 +35,18 @@ def unpack(w):
 
 
 def normalise(x):
-    x = np.asarray(x, dtype=np.float64).reshape(-1, 3)
-    return np.stack([2 * x[:, 0] - 1, 2 * x[:, 1] - 1, 2 * (x[:, 2] - RMIN) / (1 - RMIN) - 1], 1)
+    """(a, b, r) -> (2a - 1, 2b - 1, 2 ln(r / rmin) / ln(1 / rmin) - 1), in
+    the float32 steps of the device code."""
+    x = np.asarray(x, dtype=np.float32).reshape(-1, 3)
+    lr = np.log(x[:, 2]).astype(np.float32)
+    scale, lrmin = np.float32(0.6676164014), np.float32(-2.99573227355399)
+    return np.stack([2 * x[:, 0] - 1, 2 * x[:, 1] - 1, scale * (lr - lrmin) - 1], 1).astype(np.float64)
+
+
+def odd_factors(x0):
+    """(a, b) back from the normalised inputs: the factors of the outputs
+    G_x = a N_x, G_y = b N_y (the field is odd in x and in y)."""
+    return np.stack([0.5 * (x0[:, 0] + 1), 0.5 * (x0[:, 1] + 1)], 1)
 
 
 def silu(z):
@@ -53,7 +64,7 @@ def forward(w, x):
     z1 = x0 @ w1.T + b1
     z2 = silu(z1) @ w2.T + b2
     z3 = silu(z2) @ w3.T + b3
-    out = silu(z3) @ w4.T + b4
+    out = (silu(z3) @ w4.T + b4) * odd_factors(x0)
     return out, (x0, z1, z2, z3)
 
 
@@ -65,7 +76,7 @@ def loss_and_grad(w, x, t):
     n = len(t)
     e = out - t
     loss = float(np.sum(e * e) / (2 * n))
-    dout = e / n
+    dout = e / n * odd_factors(x0)  # through the odd-output factors
     g = np.zeros(P)
     h3, h2, h1 = silu(z3), silu(z2), silu(z1)
     g[W4:W4 + 128] = (dout.T @ h3).ravel()

@@ -7,6 +7,9 @@ particles the reference tracked when it wrote tests/golden/ref_tracking.npz
 Where oracle/_ref is present (it ships with the build), further cases run
 the reference beside the GPU in the same test.
 """
+import os
+import shutil
+
 import numpy as np
 import pytest
 
@@ -122,3 +125,51 @@ def test_initial_distribution_statistics_match_the_reference_generator(tmp_path)
     lz = lambda c: (c[4] / sz) ** 2 + (c[5] * rb2 / sdp) ** 2
     for f in (ax, lz):
         assert stats.ks_2samp(f(cr), f(cg)).pvalue > 1e-4
+
+
+@pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
+def test_quantum_excitation_statistics_over_seeds(tmp_path):
+    """Radiation damping with quantum excitation ON: the reference draws its
+    noise from mt19937 (Bunch.cpp:989-1023, seeded here per run through the
+    hooks), the CUDA path from Philox, so single runs differ.  From the same
+    initial beam (1.5x the matched size in all planes) 8 seeded runs on each
+    side over 400 turns: the seed-averaged emittances, bunch length and
+    energy spread agree within 4 standard errors of their difference, and
+    both sit between the initial and the equilibrium values."""
+    from cetasim_b200 import configs, input_dat
+    wl = configs.make("plain_single", n_scale=0.02)
+    wl.cfg.flag_sr_wake = 0
+    path = input_dat.write_case(str(tmp_path / "case"), wl, n_turns=400)
+    wl = input_dat.load_case(path)
+    turns, seeds = 400, 8
+    parts = [1.5 * c for c in refcases.particles(wl, seed=3)]
+
+    def fields(m):
+        return [m.emit[0], m.emit[1], m.bunch_length, m.energy_spread]
+
+    got = {"ref": [], "gpu": []}
+    for s in range(seeds):
+        # the reference writes .sdds files where it runs: a fresh copy per run
+        d = tmp_path / f"seed{s}"
+        shutil.copytree(os.path.dirname(path), d, ignore=shutil.ignore_patterns("*.sdds"))
+        r = ref.RefBeam(str(d / "input.dat"), seed=1000 + s)
+        r.upload(0, parts[0])
+        r.Run(0, turns)
+        r.MPBeamRMSCal(0)
+        got["ref"].append(fields(r.moments()[0]))
+        r.close()
+        wl.cfg.seed = 1000 + s
+        g = MPBeam(wl)
+        g.upload(0, parts[0])
+        g.Run(0, turns)
+        g.MPBeamRMSCal(0)
+        got["gpu"].append(fields(g.moments()[0]))
+        g.close()
+    a, b = np.array(got["ref"]), np.array(got["gpu"])
+    se = np.sqrt(a.var(0, ddof=1) / seeds + b.var(0, ddof=1) / seeds)
+    diff = np.abs(a.mean(0) - b.mean(0))
+    assert np.all(diff <= 4 * se + 1e-3 * np.abs(a.mean(0))), (a.mean(0), b.mean(0), se)
+    # the beam is damping towards equilibrium in both
+    init = [1.5 ** 2 * wl.gen[0], 1.5 ** 2 * wl.gen[1], 1.5 * wl.gen[2], 1.5 * wl.gen[3]]
+    for m in (a.mean(0), b.mean(0)):
+        assert m[0] < 0.95 * init[0] and m[2] < 0.99 * init[2]
