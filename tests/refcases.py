@@ -15,7 +15,8 @@ import numpy as np
 from cetasim_b200 import configs, input_dat
 from helpers import TRAPPED, particles
 
-# name -> (config, n_scale, turns, bunch current, cfg overrides)
+# name -> (config, n_scale, turns, bunch current, cfg overrides[, layout])
+# layout: {"bunches": first bunches kept, "clouds": macro-ions pre-loaded per IP}
 CASES = {
     # config 0's ring with the short-range wake (BBR, 100 bins)
     "plain_sr": ("plain_single", 0.005, 5, None, {}),
@@ -25,24 +26,51 @@ CASES = {
     "fast_ion": ("fast_ion", 0.00125, 4, TRAPPED, {}),
     # config 3's ragged 900-bunch train, 50 IPs, LR HOM wake and 9-tap FIR (no ions)
     "batched_lr_fir": ("batched_uneven", 0.001, 5, None, {"flag_beam_ion": 0}),
+    # config 4's ring (every 4th bucket of h = 4000, 50 IPs, SR + HOM + FIR,
+    # pre-loaded clouds): the first 150 bunches, 2000 macro-ions per IP, at a
+    # current low enough that the ions' motion stays regular over the slice
+    # (along the full 1000-bunch train rounding differences grow chaotically)
+    "trapping_slice": ("large_trapping", 0.0002, 1, 0.005e-3, {"sr_bins": 10},
+                       {"bunches": 150, "clouds": 2000}),
 }
 
 # bunches whose final coordinates the fixtures keep (all bunches' moments are kept)
 KEEP_BUNCHES = {"plain_sr": None, "plain_1000": None, "fast_ion": None,
-                "batched_lr_fir": list(range(0, 900, 30))}
+                "batched_lr_fir": list(range(0, 900, 30)), "trapping_slice": list(range(0, 150, 5))}
 
 
 def build(case, d):
     """(workload read back from the written input, input path, initial particles)."""
-    name, scale, turns, cur, over = CASES[case]
+    name, scale, turns, cur, over = CASES[case][:5]
+    lay = CASES[case][5] if len(CASES[case]) > 5 else {}
     wl = configs.make(name, n_scale=scale, bunch_current=cur)
     for k, v in over.items():
         setattr(wl.cfg, k, v)
+    if "bunches" in lay:
+        m = lay["bunches"]
+        wl.n_macro, wl.harm, wl.ne = wl.n_macro[:m].copy(), wl.harm[:m].copy(), wl.ne[:m].copy()
     path = input_dat.write_case(d, wl, n_turns=turns, qe=False)
     wl2 = input_dat.load_case(path, name=case)
     for i in range(3):
         wl2.cfg.ring.emit_nat[i] = 0.0
     return wl2, path, particles(wl2, seed=5, spread=2.0)
+
+
+def clouds(case, wl):
+    """The pre-loaded clouds of a case ((x, y, vx, vy) per IP) or None."""
+    lay = CASES[case][5] if len(CASES[case]) > 5 else {}
+    return configs.preload_clouds(wl, lay["clouds"]) if "clouds" in lay else None
+
+
+def start(case, beam, wl, parts):
+    """Uploads a case's particles and pre-loaded clouds into any of the three
+    beams (reference, oracle, CUDA path)."""
+    for j, c in enumerate(parts):
+        beam.upload(j, c)
+    cl = clouds(case, wl)
+    if cl is not None:
+        for k, (x, y, vx, vy) in enumerate(cl):
+            beam.upload_ions(k, 0, x, y, vx, vy)
 
 
 def parts_digest(parts):
@@ -58,8 +86,7 @@ def run_ref(case, d):
     wl, path, parts = build(case, d)
     r = ref.RefBeam(path, seed=wl.cfg.seed)
     r.set_emit_nat([0.0, 0.0, 0.0])
-    for j, c in enumerate(parts):
-        r.upload(j, c)
+    start(case, r, wl, parts)
     r.Run(0, CASES[case][2])
     return wl, parts, r
 

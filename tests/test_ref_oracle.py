@@ -15,7 +15,8 @@ from oracle import ref
 
 # oracle vs reference: identical arithmetic except w(z) (the oracle's own
 # evaluation, within ~1e-16 of Faddeeva::w), so bit-equal without ions
-TOL = {"plain_sr": 0.0, "plain_1000": 0.0, "batched_lr_fir": 0.0, "fast_ion": 1e-13}
+TOL = {"plain_sr": 0.0, "plain_1000": 0.0, "batched_lr_fir": 0.0, "fast_ion": 1e-13,
+       "trapping_slice": 1e-12}
 
 live = pytest.mark.skipif(not ref.available(), reason="oracle/_ref/libcetasim_ref.so not built")
 
@@ -27,8 +28,7 @@ def test_oracle_reproduces_reference_fixture(case, tmp_path):
     assert refcases.parts_digest(parts) == bytes(g[f"{case}/digest"]).hex(), \
         "the seeded initial particles changed"
     o = oracle.OracleBeam(wl)
-    for j, c in enumerate(parts):
-        o.upload(j, c)
+    refcases.start(case, o, wl, parts)
     o.Run(0, refcases.CASES[case][2])
     o.MPBeamRMSCal(0)
     worst = 0.0
