@@ -88,7 +88,7 @@ def build_host(force: bool = False, verbose: bool = False) -> str:
     deps = [os.path.join(hdir, s) for s in HOST_SOURCES + ["mpbeam.hpp", "cbm_writer.hpp"]] + [LIB]
     if not force and not _stale(CLI, deps):
         return CLI
-    cmd = ["g++", "-O2", "-std=c++17", "-o", CLI + ".tmp",
+    cmd = ["g++", "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), "-o", CLI + ".tmp",
            *[os.path.join(hdir, s) for s in HOST_SOURCES], "-L" + HERE, "-lcetagpu",
            "-Wl,-rpath,$ORIGIN"]
     if verbose:

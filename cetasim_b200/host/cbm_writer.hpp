@@ -4,7 +4,7 @@
 #pragma once
 #include <string>
 
-#include "../../include/cetasim_gpu.h"
+#include "cetasim_gpu.h"
 
 namespace cetasim {
 

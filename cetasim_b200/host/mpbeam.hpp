@@ -8,7 +8,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/cetasim_gpu.h"
+#include "cetasim_gpu.h"
 
 namespace cetasim {
 
