@@ -25,8 +25,13 @@ coupling 0.2 (eps_x = 20 pm, eps_y = 4 pm), sigma_z = 2.5 mm, sigma_dp = 9e-4.
                  (preload_clouds), short-range wake as plain_single, HOM and
                  FIR as batched_uneven.
 
-Beam current is not part of those shapes: 1 mA for the single bunch and
-0.125 mA per bunch in the trains are used.
+Beam current is not part of those shapes: 1 mA for the single bunch,
+0.125 mA per bunch in the 2 ns trains (fast_ion, batched_uneven) and 0.03 mA
+per bunch in large_trapping.  The last is the trapping regime the config is
+named for: with 8 ns spacing CO (A = 28) is trapped when the critical mass
+number N r_p L / (2 sigma_y (sigma_x + sigma_y)) is below 28, which needs
+N <~ 2e9 electrons per bunch (0.03 mA gives 21; at 0.125 mA it is 86 and the
+pre-loaded clouds are over-focused out of the beam within a few passages).
 """
 from __future__ import annotations
 
@@ -212,7 +217,7 @@ def make(name: str, n_scale: float = 1.0, turns_lr: int = 10, lib=None, seed: in
     # 1 mA for the single bunch; 0.125 mA per bunch in the trains (N_e = 6e9,
     # the regime where CO ions are trapped inside the train: critical mass
     # number ~23 < 28 for 2 ns spacing)
-    current = 1e-3 if name == "plain_single" else 0.125e-3
+    current = {"plain_single": 1e-3, "large_trapping": 0.03e-3}.get(name, 0.125e-3)
     if bunch_current is not None:
         current = bunch_current
     ne = [current / f0 / E_CHARGE] * M

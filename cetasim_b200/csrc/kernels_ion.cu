@@ -145,6 +145,14 @@ __global__ void __launch_bounds__(kPrepThreads) k_ion_prep(ChainParams cp, Chain
   }
 }
 
+// w(z) for a warp in which some lane has |z| >= 30 (an ion far from the
+// bunch), kept out of line: inlined, its continued fraction doubles the
+// walk's code and registers (214 -> 142) and lengthens every step's
+// instruction fetch, although the branch is rarely taken.
+__device__ __noinline__ cplx walk_w_wide(double zr, double zi) {
+  return w_quadrant1_wide_lowlat(zr, zi);
+}
+
 // One CTA block = IONS trajectories: index t < n0 is ion t of the cloud the
 // previous call left, t >= n0 the ion born as number (t - n0) % NM at bunch
 // (t - n0) / NM.  blockIdx.y = species.  The step loop has no block barrier:
@@ -265,7 +273,7 @@ __global__ void __launch_bounds__(4 * IONS, 1) k_ion_walk(ChainParams cp, IonWal
             const cplx lo = upper ? po : ph, hi = upper ? ph : po;
             wv = weideman_from_sum({lo.re + hi.re, lo.im + hi.im}, rden);
           } else {
-            wv = w_quadrant1_wide_lowlat(zr, zi);
+            wv = walk_w_wide(zr, zi);
           }
           const cplx wo = {__shfl_xor_sync(FULL_MASK, wv.re, 2),
                            __shfl_xor_sync(FULL_MASK, wv.im, 2)};
@@ -529,24 +537,44 @@ cudaError_t upload_weideman_table_ion() {
   return cudaMemcpyToSymbol(c_weideman, &h_weideman, sizeof(WeidemanTable));
 }
 
-// Latency floor of the walk: one thread advances an ion through a dependent
-// chain of bunch passages (the walk's low-latency field, then the velocity
-// and position update), so each field evaluation waits for the previous one.
-// With c = 1e-13 the ion oscillates in the core of the Gaussian (period of
+// Latency floor of the walk: one quad of lanes advances one ion through a
+// dependent chain of bunch passages with exactly the walk's step arithmetic
+// (the field arguments, w(z1) and w(z2) each split over two lanes, the
+// Gaussian factor beside them, the shuffles, the field and the velocity and
+// position update) and none of its window stores, barriers and sums.  With
+// coefficient 1e-13 the ion oscillates in the core of the Gaussian (period of
 // ~300 passages), where the walk spends its time (Weideman region of w(z)).
 __global__ void k_field_chain(double* out, int n) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  __shared__ double s_a[kWeidemanN];
+  const int lane = threadIdx.x & 31, sub = lane & 3;
+  for (int i = lane; i < kWeidemanN; i += 32) s_a[i] = weideman_table().a[i];
+  __syncwarp();
+  if (threadIdx.x >= 32) return;
+  const bool second = (sub >> 1) != 0, upper = (sub & 1) != 0;
+  const double L = weideman_table().L;
+  const FieldPrep fp = field_prep(1.4e-5, 6.3e-6);
   double x = 3.0e-6, y = 2.0e-6, vx = 0.0, vy = 0.0;
-  const double sx = 1.4e-5, sy = 6.3e-6, c = 1.0e-13;
+  const double c = 1.0e-13;
   for (int i = 0; i < n; ++i) {
+    double z1r, z1i, z2r, z2i;
+    field_zargs(fp, x, y, &z1r, &z1i, &z2r, &z2i);
+    const double zr = second ? z2r : z1r, zi = second ? z2i : z1i;
+    const double g = second ? field_gauss(fp, x, y) : 0.0;
+    cplx rden;
+    const cplx ph = weideman_half(zr, zi, L, s_a, upper, &rden);
+    const cplx po = {__shfl_xor_sync(FULL_MASK, ph.re, 1), __shfl_xor_sync(FULL_MASK, ph.im, 1)};
+    const cplx lo = upper ? po : ph, hi = upper ? ph : po;
+    const cplx wv = weideman_from_sum({lo.re + hi.re, lo.im + hi.im}, rden);
+    const cplx wo = {__shfl_xor_sync(FULL_MASK, wv.re, 2), __shfl_xor_sync(FULL_MASK, wv.im, 2)};
+    const double go = __shfl_xor_sync(FULL_MASK, g, 2);
     double fx, fy;
-    gaussian_field<true>(x, y, sx, sy, &fx, &fy);
+    field_finish_g(fp, x, y, second ? wo : wv, second ? wv : wo, second ? g : go, &fx, &fy);
     vx += c * fx;
     vy += c * fy;
     x += vx;
     y += vy;
   }
-  out[0] = x + y;
+  if (lane == 0) out[0] = x + y;
 }
 
 cudaError_t measure_field_chain_latency(double* us_per_step) {

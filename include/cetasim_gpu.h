@@ -333,9 +333,11 @@ int cg_time_stage(cg_handle* h, int stage, int k, int reps, double* ms);
  * chain kernel, in FLOP/s (2 per FMA). */
 int cg_fp64_peak(double* flops);
 /* Latency of one bunch passage of the ion walk on this device, in us: one
- * thread advances an ion through a dependent chain of Gaussian-field
- * evaluations (the walk's low-latency w(z)) and velocity / position updates.
- * The floor of the sequential ion chain, which needs one passage per bunch. */
+ * quad of lanes advances an ion through a dependent chain of passages with
+ * the walk's own step arithmetic (field arguments, w(z1) and w(z2) split over
+ * lanes, the Gaussian factor, field, velocity and position update), without
+ * the walk's window stores, barriers and sums.  The floor of the sequential
+ * ion chain, which needs one passage per bunch. */
 int cg_field_chain_latency(double* us_per_step);
 
 /* MPBunch::GetEigenEmit (MPBunch.cpp:500-658) of bunch j, the diagnostic

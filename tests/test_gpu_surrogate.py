@@ -20,7 +20,8 @@ pytestmark = pytest.mark.gpu
 TARGET = 1e-3
 MAX_NOT_MET = pytest.mark.xfail(
     strict=False, reason="the largest error of the 3-64-64-64-2 BF16 network is above the 1e-3 "
-                         "target (measured ~3e-3 on the hold-out); its RMS meets it")
+                         "target (measured 1.3e-3 on the hold-out after 150 epochs, 1.1e-3 "
+                         "after 300); its RMS (9.5e-5) meets it")
 
 
 @pytest.fixture(scope="module")
@@ -189,3 +190,37 @@ def test_turns_with_surrogate_and_periodic_audit(trained):
     n, last, worst = g.surrogate_audit_stats()
     # two audits made, each a positive error ratio, the worst one kept
     assert n == 2 and 0 < last <= worst < 1
+
+
+def test_coupled_bunch_growth_rate_with_the_surrogate(trained):
+    """The fast-ion instability of the 80-bunch train at 1e-8 Pa (ten times
+    the benchmark pressure, so that the vertical coupled-bunch mode grows by
+    about e^2 within 400 turns; radiation damping off): the growth rate of
+    the dominant vertical mode from the GetCBMGR-form estimator
+    (cg_cbm_growth, the DFT modes) with the surrogate in the electron-ion
+    kicks is within 5 % of the exact path's."""
+    from cetasim_b200 import configs
+    w, _ = trained
+    turns, rates = 400, {}
+    for arm in ("exact", "surrogate"):
+        wl = configs.make("fast_ion", n_scale=0.05)
+        for k in range(wl.cfg.n_sections):
+            wl.sections[k].pressure = 1e-8
+        wl.cfg.flag_synrad = 0
+        g = MPBeam(wl)
+        for j, c in enumerate(particles(wl, seed=5, spread=0.2)):
+            g.upload(j, c)
+        if arm == "surrogate":
+            g.set_surrogate(w)
+        g.cbm_init(turns + 1)
+        for n in range(turns):
+            g.Run(n, 1)
+            g.MPBeamRMSCal(0)
+            g.cbm_record()
+        amp = g.cbm_history()[0]
+        mode = int(np.argmax(amp[-1, 1, :]))
+        rates[arm] = (mode, g.cbm_growth(100, turns, 1.0, 0)[1, mode])
+        g.close()
+    (me, re), (ms, rs) = rates["exact"], rates["surrogate"]
+    assert me == ms and re > 100.0            # the same mode, growing (1/s)
+    assert abs(rs - re) <= 0.05 * re, rates
