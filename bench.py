@@ -68,6 +68,11 @@ DESC = {
 }
 
 
+# the kick kernel's shapes in the order of cg_autotune's timings
+KICK_SHAPES = ["256 thr x3/SM", "256 thr x4/SM", "128 thr x4/SM", "128 thr x6/SM",
+               "256 thr x3/SM, 4 tiles per CTA", "128 thr x6/SM, 2 tiles per CTA"]
+
+
 class ClockSampler:
     """Clock and throttle-reason samples while the timed region runs: NVML
     polled every 5 ms (read-only), or nvidia-smi every 200 ms where NVML is
@@ -315,6 +320,8 @@ def main():
     ap.add_argument("--kick-variant", type=int, default=None, metavar="V",
                     help="kick shape V (0-3; 4-7: the same inside the map pass) instead of "
                          "the kick autotuner")
+    ap.add_argument("--map-async", type=int, default=0, choices=[0, 1],
+                    help="with --kick-variant: the map-pass form (1 = next chunk in flight)")
     ap.add_argument("--pipeline", default=None, metavar="G:IONS:RAMP",
                     help="pipeline shape (walk segments, ions per walk CTA, ramp 0/1) instead "
                          "of the whole-turn pipeline autotuner")
@@ -368,6 +375,7 @@ def main():
     ions = bool(wl.cfg.flag_beam_ion)
     if args.kick_variant is not None:
         beam.set_kick_variant(args.kick_variant)
+        beam.set_map_async(args.map_async)
         tune = (args.kick_variant, None)
     elif ions:
         tune = beam.autotune(0, reps=10)
@@ -526,7 +534,8 @@ def main():
     top["kernels"] = kernels
     sur = None
     if world == 1 and ions and not args.no_surrogate:
-        sur = surrogate_leg(args, beam, lib, stream, flush, kms["ion_field_kick"], tot_ms / args.steps)
+        sur = surrogate_leg(args, beam, lib, stream, flush, kms["ion_field_kick"], tot_ms / args.steps,
+                            clk.summary().get("sm_max_mhz"))
 
     result = None
     if rank == 0:
@@ -557,14 +566,18 @@ def main():
             "roofline": top,
             "cpu_baseline": cpu,
             "autotune": {"kick_shapes_ms": None if tune[1] is None else
-                         [round(float(x), 5) for x in tune[1][:-2]],
-                         "map_pass_ms": None if tune[1] is None else round(float(tune[1][-2]), 5),
+                         [round(float(x), 5) for x in tune[1][:-4]],
+                         "map_pass_ms": None if tune[1] is None else round(float(tune[1][-4]), 5),
                          "map_pass_with_kick_ms": None if tune[1] is None else
+                         round(float(tune[1][-3]), 5),
+                         "map_pass_async_ms": None if tune[1] is None else
+                         round(float(tune[1][-2]), 5),
+                         "map_pass_async_with_kick_ms": None if tune[1] is None else
                          round(float(tune[1][-1]), 5),
-                         "chosen_shape": int(tune[0]) % 4,
-                         "kick_in_map_pass": bool(tune[0] >= 4),
-                         "shapes": ["256 thr x3/SM", "256 thr x4/SM", "128 thr x4/SM",
-                                    "128 thr x6/SM"],
+                         "map_async": beam.map_async(),
+                         "chosen_shape": int(tune[0]) % len(KICK_SHAPES),
+                         "kick_in_map_pass": bool(tune[0] >= len(KICK_SHAPES)),
+                         "shapes": KICK_SHAPES,
                          "pipeline": None if pipe is None else {
                              "segments": pipe[0][0], "walk_ions": pipe[0][1],
                              "ramp": bool(pipe[0][2]),
@@ -608,7 +621,7 @@ def measured_peak(key):
     return fallback[key], f"fallback ({key} of an earlier measurement on this pool)"
 
 
-def surrogate_leg(args, beam, lib, stream, flush, exact_kick_ms, exact_turn_ms):
+def surrogate_leg(args, beam, lib, stream, flush, exact_kick_ms, exact_turn_ms, sm_mhz):
     """The learned field in place of the exact one: trains the surrogate on the
     GPU (2^20 exact-field samples), then times its kick kernel and whole turns
     with it, the same way as the exact path, and audits it against the exact
@@ -639,6 +652,11 @@ def surrogate_leg(args, beam, lib, stream, flush, exact_kick_ms, exact_turn_ms):
     K = beam.wl.cfg.n_sections
     peak = measured_peak("bf16_tflops")
     bf16 = 17024.0 * n / (k_ms.value * 1e-3) / 1e12
+    # the unit that bounds the network: every SiLU takes an exponential and a
+    # reciprocal on the multi-function unit (16 results per clock per SM), 192
+    # SiLU per sample
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    mufu_ms = 384.0 * n / (16.0 * sms * (sm_mhz or 1965.0) * 1e6) * 1e3
     return {"network": "3-64-64-64-2 SiLU, BF16 weights, FP32 accumulation, tcgen05",
             "holdout_rms_rel": st[1], "holdout_max_rel": st[2], "train_s": st[3],
             "field_error_target": 1e-3,
@@ -652,7 +670,11 @@ def surrogate_leg(args, beam, lib, stream, flush, exact_kick_ms, exact_turn_ms):
             "ms_per_turn": turn_ms, "exact_ms_per_turn": exact_turn_ms,
             "turn_speedup": exact_turn_ms / turn_ms, "target_speedup": 5.0,
             "kick_bf16_tflops": bf16, "kick_bf16_frac": bf16 / peak[0],
-            "bf16_peak_source": peak[1]}
+            "bf16_peak_source": peak[1],
+            "roofline": {"bound": "mufu", "unit": "ms per kick launch (lower is better)",
+                         "achieved": k_ms.value, "peak": mufu_ms, "frac": mufu_ms / k_ms.value,
+                         "peak_source": "384 MUFU operations per sample (192 SiLU x (exp, rcp)) "
+                                        "at 16 per clock per SM, SM count and max SM clock"}}
 
 
 def kernel_traffic(workload, kernel):

@@ -114,7 +114,8 @@ class TraceRecord(C.Structure):
 
 
 PIPE_SHAPES = [(1, 64, 0), (1, 16, 0), (2, 64, 0), (2, 64, 1), (3, 64, 0), (3, 64, 1),
-               (4, 64, 0), (4, 64, 1), (3, 16, 1), (6, 64, 1)]
+               (4, 64, 0), (4, 64, 1), (3, 16, 1), (6, 64, 1), (8, 64, 1), (12, 64, 1),
+               (16, 64, 1), (8, 32, 1), (12, 32, 1), (16, 32, 1)]
 
 TRACE_KINDS = ["start", "moments", "ion_prep", "ion_walk", "ion_records", "ion_compact",
                "ion_chain", "ion_kick", "map_pass", "exchange", "lr_wake", "long", "sr_wake",
@@ -123,7 +124,8 @@ TRACE_KINDS = ["start", "moments", "ion_prep", "ion_walk", "ion_records", "ion_c
 
 class SurTrainParams(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("n_train", C.c_int64), ("n_holdout", C.c_int64),
-                ("epochs", C.c_int), ("batch", C.c_int), ("lr", C.c_double)]
+                ("epochs", C.c_int), ("batch", C.c_int), ("lr", C.c_double),
+                ("l4_from", C.c_double), ("l4_weight", C.c_double)]
 
 
 # (name, restype, argtypes) of every export declared in include/cetasim_gpu.h
@@ -187,6 +189,8 @@ EXPORTS = [
     ("cg_autotune_pipeline", I, [C.c_void_p, I, I, C.c_void_p, C.c_void_p]),
     ("cg_set_kick_variant", I, [C.c_void_p, I]),
     ("cg_autotune", I, [C.c_void_p, I, I, PI, PD]),
+    ("cg_set_map_async", I, [C.c_void_p, I]),
+    ("cg_map_async", I, [C.c_void_p, PI]),
     ("cg_shard_plan", I, [PI, I, I, PI, PI]),
     ("cg_shard_exchange_size", I, [PI, I, I, PI]),
     ("cg_shard_pack", I, [PI, I, I, I, C.c_void_p, C.c_size_t, C.c_void_p]),

@@ -148,16 +148,26 @@ class MPBeam:
 
     # -- autotuning ---------------------------------------------------------------
     def autotune(self, k: int = 0, reps: int = 10):
-        """Times the kick shapes on this beam at IP k; returns (choice, ms)."""
+        """Times the kick shapes and the map-pass forms on this beam at IP k;
+        returns (choice, ms) as cg_autotune fills them (n kick shapes, then
+        the map pass, with the kick, and both with the next chunk in flight)."""
         n = C.c_int()
         self._check(self.lib.cg_kick_variants(C.byref(n)))
-        ms = np.zeros(n.value + 2)
+        ms = np.zeros(n.value + 4)
         choice = C.c_int()
         self._check(self.lib.cg_autotune(self.h, k, reps, C.byref(choice), _abi.ptr(ms)))
         return choice.value, ms
 
     def set_kick_variant(self, v: int):
         self._check(self.lib.cg_set_kick_variant(self.h, v))
+
+    def set_map_async(self, on: bool):
+        self._check(self.lib.cg_set_map_async(self.h, int(bool(on))))
+
+    def map_async(self) -> bool:
+        v = C.c_int()
+        self._check(self.lib.cg_map_async(self.h, C.byref(v)))
+        return bool(v.value)
 
     def set_pipeline(self, groups: int, walk_ions: int = 0, ramp: bool = False):
         self._check(self.lib.cg_set_pipeline(self.h, groups, walk_ions, int(ramp)))

@@ -18,7 +18,7 @@ LIB = os.path.join(HERE, "libcetagpu.so")
 SOURCES = ["capi.cu", "kernels.cu", "kernels_sr.cu", "kernels_ion.cu", "surrogate.cu", "shard.cu",
            "cbm.cu", "faddeeva_table.cpp", "input_settings.cpp", "rw_wake.cpp"]
 HEADERS = ["cg_common.cuh", "faddeeva.cuh", "be_field.cuh", "track_math.cuh", "cg_internal.h",
-           "kernels.cuh", "umma.cuh", "surrogate.cuh", "bulk.cuh", "rw_wake.h"]
+           "kernels.cuh", "umma.cuh", "surrogate.cuh", "rw_wake.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

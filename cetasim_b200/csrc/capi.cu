@@ -81,8 +81,6 @@ int check_status(Handle& h) {
     return fail(&h, CG_ERR_TIMEOUT, "a tensor-core completion wait of the field surrogate gave up");
   if (st & kStatusLrRange)
     return fail(&h, CG_ERR_INVALID, "long-range wake lag outside the wake table (tau > 0)");
-  if (st & kStatusCopyWait)
-    return fail(&h, CG_ERR_TIMEOUT, "a bulk-copy completion wait of the map pass gave up");
   if (st & kStatusGaussCut)
     return fail(&h, CG_ERR_INVALID, "an initial-distribution draw found no sample inside the 3-sigma cut");
   return fail(&h, CG_ERR_CUDA, "unknown device status");
@@ -95,7 +93,8 @@ int launch_ok(Handle& h, cudaError_t e, const char* what) {
 
 void free_beam(Handle& h) {
   DeviceBufs& d = h.d;
-  dfree(d.c); dfree(d.surv); dfree(d.tile_bunch); dfree(d.chunk_bunch); dfree(d.bunch);
+  dfree(d.c); dfree(d.surv); dfree(d.tile_bunch); dfree(d.chunk_bunch); dfree(d.chunk_loc);
+  dfree(d.bunch);
   dfree(d.wpartials);
   dfree(d.counters); dfree(d.mom); dfree(d.loss_count); dfree(d.scratch);
   dfree(d.rec); dfree(d.rec_prep); dfree(d.lr_hist); dfree(d.lr_force); dfree(d.fir_hist); dfree(d.fir_kick);
@@ -111,6 +110,7 @@ void free_beam(Handle& h) {
   dfree(w.traj); dfree(w.alive); dfree(w.carry);
   w = IonWalk();
   d.c = nullptr; d.surv = nullptr; d.tile_bunch = nullptr; d.chunk_bunch = nullptr;
+  d.chunk_loc = nullptr;
   d.bunch = nullptr; d.wpartials = nullptr;
   d.counters = nullptr; d.mom = nullptr; d.loss_count = nullptr; d.scratch = nullptr;
   d.rec = nullptr; d.rec_prep = nullptr; d.lr_hist = nullptr; d.lr_force = nullptr; d.fir_hist = nullptr;
@@ -537,6 +537,7 @@ int cg_set_beam(cg_handle* H, int M, const int* n_macro, const int* harm, const 
   h.gap[M - 1] = Hh - harm[M - 1];
   std::vector<BunchDev> bd(M);
   std::vector<int> tb, cb;
+  std::vector<int4> cl;
   h.tile_off.assign(M + 1, 0);
   int tiles = 0, chunks = 0;
   // bunch sharding: this rank tracks the particles of bunches [j0, j1)
@@ -559,7 +560,11 @@ int cg_set_beam(cg_handle* H, int M, const int* n_macro, const int* harm, const 
     bd[j].q_macro = ne[j] / n_macro[j];
     h.tile_off[j] = tiles;
     for (int t = 0; t < nt; ++t) tb.push_back(j);
-    for (int t = 0; t < nc; ++t) cb.push_back(j);
+    for (int t = 0; t < nc; ++t) {
+      cb.push_back(j);
+      cl.push_back(make_int4(j, tiles + t * kMomChunkTiles, std::min(kMomChunkTiles, nt - t * kMomChunkTiles),
+                             bd[j].n - t * kMomChunkTiles * kTile));
+    }
     tiles += nt;
     chunks += nc;
   }
@@ -572,7 +577,8 @@ int cg_set_beam(cg_handle* H, int M, const int* n_macro, const int* harm, const 
   h.npad = (int64_t)tiles * kTile;
   DeviceBufs& d = h.d;
   if (dalloc(&d.c, 6 * (size_t)h.npad) || dalloc(&d.surv, (size_t)h.npad) ||
-      dalloc(&d.tile_bunch, tiles) || dalloc(&d.chunk_bunch, chunks) || dalloc(&d.bunch, M) ||
+      dalloc(&d.tile_bunch, tiles) || dalloc(&d.chunk_bunch, chunks) ||
+      dalloc(&d.chunk_loc, chunks) || dalloc(&d.bunch, M) ||
       dalloc(&d.wpartials, 8 * (size_t)chunks) ||
       dalloc(&d.counters, M + 1) || dalloc(&d.mom, M) || dalloc(&d.loss_count, M + 1)) {
     free_beam(h);
@@ -584,9 +590,10 @@ int cg_set_beam(cg_handle* H, int M, const int* n_macro, const int* harm, const 
     return fail(&h, CG_ERR_OOM, "scratch allocation failed");
   }
   cudaMemset(d.c, 0, sizeof(double) * 6 * h.npad);
-  cudaMemset(d.surv, 0xFF, h.npad);
+  cudaMemset(d.surv, kPadding, h.npad);
   cudaMemcpy(d.tile_bunch, tb.data(), sizeof(int) * tiles, cudaMemcpyHostToDevice);
   cudaMemcpy(d.chunk_bunch, cb.data(), sizeof(int) * chunks, cudaMemcpyHostToDevice);
+  cudaMemcpy(d.chunk_loc, cl.data(), sizeof(int4) * chunks, cudaMemcpyHostToDevice);
   if (h.nccl_comm) {
     const int W = h.sh_world, ml = std::max(1, h.sh_maxlocal);
     if (dalloc(&d.mom_send, (size_t)ml) || dalloc(&d.mom_all, (size_t)W * ml) ||
@@ -950,7 +957,7 @@ static cudaError_t enqueue_turn(Handle& h) {
         const int ta = h.tile_off[ja], tb = h.tile_off[jb];
         const int ca = h.chunk_off[ja], cb = h.chunk_off[jb];
         if (fused) {
-          if ((e = launch_map_pass(h, k, mom, true, ca, cb, h.side))) return e;
+          if ((e = launch_map_turn(h, k, mom, true, ca, cb, h.side))) return e;
           TRACE(h.side, CG_TRACE_MAP_PASS, k, g);
           continue;
         }
@@ -960,7 +967,7 @@ static cudaError_t enqueue_turn(Handle& h) {
         TRACE(h.side, CG_TRACE_ION_KICK, k, g);
         if ((e = cudaEventRecord(h.kick_ev[g], h.side))) return e;
         if ((e = cudaStreamWaitEvent(h.side2, h.kick_ev[g], 0))) return e;
-        if ((e = launch_map_pass(h, k, mom, false, ca, cb, h.side2))) return e;
+        if ((e = launch_map_turn(h, k, mom, false, ca, cb, h.side2))) return e;
         TRACE(h.side2, CG_TRACE_MAP_PASS, k, g);
       }
       if ((e = launch_ion_compact(h, k, h.side))) return e;
@@ -980,7 +987,7 @@ static cudaError_t enqueue_turn(Handle& h) {
           TRACE(h.stream, CG_TRACE_ION_KICK, k, -1);
         }
       }
-      if ((e = launch_map_pass(h, k, mom, fused))) return e;
+      if ((e = launch_map_turn(h, k, mom, fused))) return e;
       TRACE(h.stream, CG_TRACE_MAP_PASS, k, -1);
     }
     if (mom >= 0) {
@@ -1272,9 +1279,9 @@ int cg_time_stage(cg_handle* H, int stage, int k, int reps, double* ms) {
       case 7:
         e = h.cfg.flag_beam_ion ? launch_map_pass(h, k, k, true) : cudaErrorInvalidValue;
         break;
-      case 8: e = launch_map_stream(h, k, k); break;
+      case 8: e = launch_map_async(h, k, k); break;
       case 9:
-        e = h.cfg.flag_beam_ion ? launch_map_stream(h, k, k, true) : cudaErrorInvalidValue;
+        e = h.cfg.flag_beam_ion ? launch_map_async(h, k, k, true) : cudaErrorInvalidValue;
         break;
       case 6:
         e = h.d.sur_w ? launch_ion_kick_sur(h, k) : cudaErrorInvalidValue;
@@ -1608,14 +1615,19 @@ int cg_autotune(cg_handle* H, int k, int reps, int* choice, double* ms) {
       best_ms = per;
     }
   }
-  // the separate kick + map pass against the kick inside the map pass
+  // the separate kick + map pass against the kick inside the map pass, each
+  // pass in its register form and with the next chunk in flight
   const int mom = k + 1 < h.K ? k + 1 : k;
-  double map_ms = 0, fused_ms = 0;
+  double map_ms = 0, fused_ms = 0, amap_ms = 0, afused_ms = 0;
   if (e == cudaSuccess) e = time_it([&]() { return launch_map_pass(h, k, mom, false); }, &map_ms);
   if (e == cudaSuccess) e = time_it([&]() { return launch_map_pass(h, k, mom, true); }, &fused_ms);
+  if (e == cudaSuccess) e = time_it([&]() { return launch_map_async(h, k, mom, false); }, &amap_ms);
+  if (e == cudaSuccess) e = time_it([&]() { return launch_map_async(h, k, mom, true); }, &afused_ms);
   if (ms) {
     ms[nv] = map_ms;
     ms[nv + 1] = fused_ms;
+    ms[nv + 2] = amap_ms;
+    ms[nv + 3] = afused_ms;
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(h.stream);
   cudaEventDestroy(e0);
@@ -1623,15 +1635,35 @@ int cg_autotune(cg_handle* H, int k, int reps, int* choice, double* ms) {
   dfree(keep);
   dfree(keep_mom);
   if (e != cudaSuccess) return cuda_fail(&h, e, "autotune");
-  const bool fuse = fused_ms < best_ms + map_ms;
+  const double sep = best_ms + std::min(map_ms, amap_ms), fus = std::min(fused_ms, afused_ms);
+  const bool fuse = fus < sep;
+  const bool async = fuse ? afused_ms < fused_ms : amap_ms < map_ms;
   if (choice) *choice = best + (fuse ? nv : 0);
   int st = cg_set_kick_variant(H, best);
-  if (h.fuse_kick != fuse && h.turn_graph) {
+  if ((h.fuse_kick != fuse || h.map_async != async) && h.turn_graph) {
     cudaGraphExecDestroy(h.turn_graph);
     h.turn_graph = nullptr;
   }
   h.fuse_kick = fuse;
+  h.map_async = async;
   return st;
+}
+
+int cg_set_map_async(cg_handle* H, int on) {
+  if (!H) return CG_ERR_INVALID;
+  Handle& h = H->h;
+  if (h.map_async != (on != 0) && h.turn_graph) {
+    cudaGraphExecDestroy(h.turn_graph);
+    h.turn_graph = nullptr;
+  }
+  h.map_async = on != 0;
+  return CG_OK;
+}
+
+int cg_map_async(cg_handle* H, int* on) {
+  if (!H || !on) return CG_ERR_INVALID;
+  *on = H->h.map_async ? 1 : 0;
+  return CG_OK;
 }
 
 int cg_set_pipeline(cg_handle* H, int groups, int walk_ions, int ramp) {
@@ -1898,7 +1930,8 @@ int cg_checkpoint_load(cg_handle* H, const void* buf, size_t bytes) {
 // ions, ramp).
 static const int kPipeShapes[CG_PIPE_SHAPES][3] = {
     {1, 64, 0}, {1, 16, 0}, {2, 64, 0}, {2, 64, 1}, {3, 64, 0},
-    {3, 64, 1}, {4, 64, 0}, {4, 64, 1}, {3, 16, 1}, {6, 64, 1}};
+    {3, 64, 1}, {4, 64, 0}, {4, 64, 1}, {3, 16, 1}, {6, 64, 1}, {8, 64, 1}, {12, 64, 1},
+    {16, 64, 1}, {8, 32, 1}, {12, 32, 1}, {16, 32, 1}};
 
 int cg_autotune_pipeline(cg_handle* H, int turn0, int reps, int* shape, double* ms) {
   STAGE_PROLOGUE
@@ -2097,7 +2130,8 @@ int cg_surrogate_grad(const float* weights, const float* inputs, const float* ta
 
 int cg_surrogate_train(const cg_sur_train_params* p, float* weights, double* stats) {
   if (!p || !weights || p->batch <= 0 || p->batch % 128 != 0 || p->n_train < p->batch ||
-      p->n_train % p->batch != 0 || p->n_holdout < 1 || p->epochs < 1 || !(p->lr > 0))
+      p->n_train % p->batch != 0 || p->n_holdout < 1 || p->epochs < 1 || !(p->lr > 0) ||
+      !(p->l4_weight >= 0 && p->l4_weight <= 1) || !(p->l4_from >= 0))
     return fail(nullptr, CG_ERR_INVALID, "bad training parameters");
   int st = sur_device_ready();
   if (st) return st;
@@ -2115,7 +2149,8 @@ int cg_surrogate_train(const cg_sur_train_params* p, float* weights, double* sta
   float* part = b.get<float>((size_t)ncta * (CG_SUR_PARAMS + 1));
   double* l = b.get<double>(1);
   int* s = b.get<int>(1);
-  if (!x || !t || !xh || !th || !oh || !w || !m || !v || !part || !l || !s)
+  float* e2 = b.get<float>(1);
+  if (!x || !t || !xh || !th || !oh || !w || !m || !v || !part || !l || !s || !e2)
     return fail(nullptr, CG_ERR_OOM, "surrogate training buffers");
   // initial weights: uniform in +-1/sqrt(fan_in) (the common default of
   // linear layers), from the seeded host stream
@@ -2136,6 +2171,7 @@ int cg_surrogate_train(const cg_sur_train_params* p, float* weights, double* sta
   cudaMemset(m, 0, CG_SUR_PARAMS * sizeof(float));
   cudaMemset(v, 0, CG_SUR_PARAMS * sizeof(float));
   cudaMemset(s, 0, sizeof(int));
+  cudaMemset(e2, 0, sizeof(float));
   cudaError_t e = launch_sur_data(p->seed, n, x, t, 0);
   if (e == cudaSuccess) e = launch_sur_data(p->seed + 1, nh, xh, th, 0);
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
@@ -2157,6 +2193,8 @@ int cg_surrogate_train(const cg_sur_train_params* p, float* weights, double* sta
     mul %= (uint64_t)n;
     while (gcd(mul, (uint64_t)n) != 1) mul = (mul + 2) % (uint64_t)n;
     if (ep == p->epochs - 1) cudaMemsetAsync(l, 0, sizeof(double), 0);
+    // the fourth-power term from epoch l4_from * epochs on
+    const float l4w = (double)ep >= p->l4_from * p->epochs ? (float)p->l4_weight : 0.0f;
     for (int64_t q = 0; q < steps_per_epoch && e == cudaSuccess; ++q, ++step) {
       double lr = step < warm ? p->lr * (double)(step + 1) / warm
                               : p->lr * 0.5 * (1.0 + std::cos(3.14159265358979323846 *
@@ -2164,7 +2202,7 @@ int cg_surrogate_train(const cg_sur_train_params* p, float* weights, double* sta
       const float bc1 = (float)(1.0 - std::pow(0.9, (double)(step + 1)));
       const float bc2 = (float)(1.0 - std::pow(0.999, (double)(step + 1)));
       e = launch_sur_step(w, x, t, n, q * p->batch, p->batch, mul, add, part, m, v, w, (float)lr,
-                          bc1, bc2, ep == p->epochs - 1 ? l : nullptr, nullptr, s, 0);
+                          bc1, bc2, ep == p->epochs - 1 ? l : nullptr, nullptr, s, 0, l4w, e2);
     }
   }
   cudaEventRecord(e1, 0);

@@ -28,6 +28,8 @@ constexpr double kPi = 3.141592653589793115997963468544185161590576171875;
 // Survival codes of MPBunch::eSurive (Bunch.cpp:172-200): 0 alive,
 // 1 lost transversely, 2 lost longitudinally.
 constexpr uint8_t kAlive = 0;
+// Survival mark of the padding slots that fill each bunch's last tile.
+constexpr uint8_t kPadding = 0xFF;
 
 // ---------------------------------------------------------------------------
 // Philox4x32-10 counter-based generator (Salmon, Moraes, Dror, Shaw, "Parallel

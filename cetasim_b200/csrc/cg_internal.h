@@ -74,6 +74,7 @@ struct DeviceBufs {
   uint8_t* surv = nullptr;      // npad
   int* tile_bunch = nullptr;    // n_tiles
   int* chunk_bunch = nullptr;   // n_chunks: bunch of each moments chunk
+  int4* chunk_loc = nullptr;    // n_chunks: (bunch, first tile, tiles, valid slots)
   BunchDev* bunch = nullptr;    // M
   MomPartial* wpartials = nullptr; // n_chunks x 8: per-warp moment partials
   unsigned* counters = nullptr;    // M (+ spare)
@@ -177,6 +178,7 @@ struct Handle {
   cudaGraphExec_t turn_graph = nullptr;
   int kick_variant = 0;         // autotuned shape of the kick kernel
   bool fuse_kick = false;       // autotuned: kick inside the map pass
+  bool map_async = false;       // autotuned: the map pass with the next chunk in flight
   int sh_rank = 0, sh_world = 1;  // bunch sharding over ranks (cg_set_shard)
   int sh_j0 = 0, sh_j1 = 0, sh_maxlocal = 0;
   void* nccl_comm = nullptr;

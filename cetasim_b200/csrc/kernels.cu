@@ -10,7 +10,6 @@
 #include <cuda_runtime.h>
 #include <algorithm>
 #include "kernels.cuh"
-#include "bulk.cuh"
 
 namespace cg {
 
@@ -340,15 +339,12 @@ __device__ __noinline__ void merge_partials_warp(int b, int part_off, int n_part
 // partials, index 8 x chunk + warp, in index order (deterministic).
 constexpr int kWarpsPerChunk = kTile / 32;
 
-__device__ __forceinline__ void warp_moment_partial(const double (&v)[kMomChunkTiles][6],
-                                                    const bool (&alive)[kMomChunkTiles],
-                                                    MomPartial* out) {
+// From this thread's first-pass sums (chunk_sums_add over its alive slots in
+// tile order) and its particles v(u, d): the warp's two-pass partial.
+template <int UNROLL, class A, class V>
+__device__ __forceinline__ void warp_moment_reduce(double (&s)[7], double mn, double mx, A alive,
+                                                   V v, MomPartial* out) {
   const int lane = threadIdx.x & 31;
-  double s[7] = {0, 0, 0, 0, 0, 0, 0};
-  double mn = INFINITY, mx = -INFINITY;
-#pragma unroll
-  for (int u = 0; u < kMomChunkTiles; ++u)
-    if (alive[u]) chunk_sums_add(v[u], s, mn, mx);
   {  // warp totals to every lane: lanes 4 i hold total i after the transposed butterfly
     const double s8[8] = {s[0], s[1], s[2], s[3], s[4], s[5], s[6], 0.0};
     const double t = warp_sum8_t(s8);
@@ -365,11 +361,12 @@ __device__ __forceinline__ void warp_moment_partial(const double (&v)[kMomChunkT
 #pragma unroll
   for (int d = 0; d < 6; ++d) mean[d] = n > 0 ? s[d] / n : 0.0;
   double q[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-#pragma unroll
+#pragma unroll UNROLL
   for (int u = 0; u < kMomChunkTiles; ++u) {
     double dv[6];
+    const bool al = alive(u);
 #pragma unroll
-    for (int d = 0; d < 6; ++d) dv[d] = alive[u] ? v[u][d] - mean[d] : 0.0;
+    for (int d = 0; d < 6; ++d) dv[d] = al ? v(u, d) - mean[d] : 0.0;
 #pragma unroll
     for (int d = 0; d < 6; ++d) q[d] = fma(dv[d], dv[d], q[d]);
     q[6] = fma(dv[0], dv[1], q[6]);
@@ -390,6 +387,18 @@ __device__ __forceinline__ void warp_moment_partial(const double (&v)[kMomChunkT
     out->zmin = mn;
     out->zmax = mx;
   }
+}
+
+__device__ __forceinline__ void warp_moment_partial(const double (&v)[kMomChunkTiles][6],
+                                                    const bool (&alive)[kMomChunkTiles],
+                                                    MomPartial* out) {
+  double s[7] = {0, 0, 0, 0, 0, 0, 0};
+  double mn = INFINITY, mx = -INFINITY;
+#pragma unroll
+  for (int u = 0; u < kMomChunkTiles; ++u)
+    if (alive[u]) chunk_sums_add(v[u], s, mn, mx);
+  warp_moment_reduce<kMomChunkTiles>(s, mn, mx, [&](int u) { return alive[u]; },
+                                     [&](int u, int d) { return v[u][d]; }, out);
 }
 
 // After the warp's partial is stored: the last of the bunch's n_parts warps
@@ -500,9 +509,70 @@ __global__ void __launch_bounds__(NT, MINB) k_ion_kick(double* __restrict__ c, i
   c[3 * npad + g] = py + dpy;
 }
 
-// The kick shapes (threads per CTA, minimum CTAs per SM) of autotune choice v.
-static const int kKickShapes[][2] = {{256, 3}, {256, 4}, {128, 4}, {128, 6}};
-constexpr int kKickVariants = 4;
+// The same kick with IPC items per CTA (an item = the NT particles of one
+// tile that one CTA of k_ion_kick covers): the CTA issues the loads of its
+// next item before it evaluates the field of the current one, so after the
+// first item its warps find their coordinates loaded instead of waiting a
+// memory round trip at the start with nothing else to issue.  The padding
+// slots of a tile hold the survival mark kPadding, so the loads need no
+// bunch lookup first; results are bitwise those of k_ion_kick.
+template <int NT, int MINB, int IPC>
+__global__ void __launch_bounds__(NT, MINB) k_ion_kick_run(double* __restrict__ c, int64_t npad,
+                                                          const uint8_t* __restrict__ surv,
+                                                          const int* __restrict__ tile_bunch,
+                                                          const BunchDev* __restrict__ bunch,
+                                                          const CloudRec* __restrict__ rec,
+                                                          const FieldPrep* __restrict__ rec_prep,
+                                                          int P, int tile_base, int n_items) {
+  constexpr int kSub = kTile / NT;
+  const int it0 = blockIdx.x * IPC, it1 = min(it0 + IPC, n_items);
+  auto index = [&](int it) {
+    return (int64_t)(tile_base + it / kSub) * kTile + (it % kSub) * NT + threadIdx.x;
+  };
+  int64_t g = index(it0);
+  uint8_t alive = surv[g];
+  double x = c[0 * npad + g], y = c[2 * npad + g];
+  double px = c[1 * npad + g], py = c[3 * npad + g];
+  for (int it = it0; it < it1; ++it) {
+    // the next item's loads, in flight while this item's field is evaluated
+    int64_t gn = g;
+    uint8_t an = kPadding;
+    double xn = 0, yn = 0, pxn = 0, pyn = 0;
+    if (it + 1 < it1) {
+      gn = index(it + 1);
+      an = surv[gn];
+      xn = c[0 * npad + gn];
+      yn = c[2 * npad + gn];
+      pxn = c[1 * npad + gn];
+      pyn = c[3 * npad + gn];
+    }
+    if (alive == kAlive) {
+      const int tile = tile_base + it / kSub;
+      const int b = tile_bunch[tile];
+      const int i = (tile - bunch[b].tile_off) * kTile + (it % kSub) * NT + threadIdx.x;
+      if (i < bunch[b].n) {
+        double dpx, dpy;
+        ion_kick_particle_prep(rec + (size_t)b * P, rec_prep + (size_t)b * P, P, x, y, &dpx,
+                               &dpy);
+        c[1 * npad + g] = px + dpx;
+        c[3 * npad + g] = py + dpy;
+      }
+    }
+    g = gn;
+    alive = an;
+    x = xn;
+    y = yn;
+    px = pxn;
+    py = pyn;
+  }
+}
+
+// The kick shapes of autotune choice v: threads per CTA, minimum CTAs per SM
+// (the register budget) and items per CTA (1 = k_ion_kick, one tile or half
+// of one per CTA; more = k_ion_kick_run).
+static const int kKickShapes[][3] = {{256, 3, 1}, {256, 4, 1}, {128, 4, 1}, {128, 6, 1},
+                                     {256, 3, 4}, {128, 6, 4}};
+constexpr int kKickVariants = 6;
 
 cudaError_t launch_ion_kick_variant(Handle& h, int k, int v, int tile_a, int tile_b,
                                     cudaStream_t s) {
@@ -524,6 +594,14 @@ cudaError_t launch_ion_kick_variant(Handle& h, int k, int v, int tile_a, int til
     case 3:
       k_ion_kick<128, 6><<<2 * nt, 128, 0, s>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch,
                                                 h.d.bunch, rec, rp, h.P, tile_a);
+      break;
+    case 4:
+      k_ion_kick_run<256, 3, 4><<<(nt + 3) / 4, 256, 0, s>>>(
+          h.d.c, h.npad, h.d.surv, h.d.tile_bunch, h.d.bunch, rec, rp, h.P, tile_a, nt);
+      break;
+    case 5:
+      k_ion_kick_run<128, 6, 4><<<(2 * nt + 3) / 4, 128, 0, s>>>(
+          h.d.c, h.npad, h.d.surv, h.d.tile_bunch, h.d.bunch, rec, rp, h.P, tile_a, 2 * nt);
       break;
     default:
       k_ion_kick<256, 3><<<nt, 256, 0, s>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch, h.d.bunch,
@@ -615,172 +693,183 @@ cudaError_t launch_map_pass(Handle& h, int k, int mom_section, bool kick, int ch
 }
 
 // ---------------------------------------------------------------------------
-// The map pass with the chunks streamed through shared memory.  The register
-// pass above issues a chunk's loads, then computes and reduces with nothing in
-// flight, so DRAM idles while a CTA works.  Here a persistent grid of two CTAs
-// per SM walks the chunks [chunk_a, chunk_b) with stride gridDim.x; each CTA
-// has two chunk buffers, and one thread refills a buffer with the chunk two
-// ahead (seven bulk copies: six coordinate rows and the survival bytes of up
-// to kMomChunkTiles tiles, 2 KiB-aligned) as soon as the CTA has moved the
-// chunk into registers.  The arithmetic and the reductions are those of
-// k_map_pass, so the results are bitwise the same.
+// The map pass with the next chunk in flight.  k_map_pass issues a chunk's
+// loads, then maps, stores and reduces with nothing in flight, so at its two
+// CTAs per SM (128 registers) DRAM idles while a CTA computes.  Here a
+// persistent grid of two CTAs per SM walks the chunks [chunk_a, chunk_b) with
+// stride gridDim.x, and before it works on the current chunk every thread
+// copies its own slots of the CTA's next chunk into shared memory with
+// cp.async (8 bytes per coordinate).  A thread reads back only what it
+// copied, so cp.async.wait_group orders everything and no CTA barrier is
+// needed.  The chunk's place (bunch, first tile, tiles, valid slots) comes
+// from a per-chunk table, one load with no dependent lookup.  The arithmetic
+// and the reductions are those of k_map_pass (with the kick, the records'
+// precomputed field constants, as k_ion_kick reads them), so the results are
+// bitwise the same.
 
-constexpr int kStreamStages = 2;
-constexpr int kChunkParticles = kMomChunkTiles * kTile;
-constexpr uint32_t kCopyWaitLimit = 1u << 26;  // mbarrier polls before giving up
-struct StreamBuf {
-  double v[6][kChunkParticles];
-  uint8_t s[kChunkParticles];
+constexpr int kAsyncStages = 2;
+struct AsyncStage {
+  double v[kMomChunkTiles][6][kTile];  // [tile of the chunk][coordinate][thread]
+  uint32_t sw[kMomChunkTiles][kTile];  // the 4-byte word holding each slot's survival byte
 };
-static_assert(sizeof(StreamBuf) % 16 == 0, "buffers stay 16-byte aligned");
-constexpr size_t kStreamSmem = kStreamStages * sizeof(StreamBuf);
+constexpr size_t kAsyncSmem = kAsyncStages * sizeof(AsyncStage);
 
-struct ChunkLoc {
-  int b, tile0, nt;
-};
-__device__ __forceinline__ ChunkLoc chunk_loc(int chunk, const int* chunk_bunch,
-                                              const BunchDev* bunch) {
-  ChunkLoc l;
-  l.b = chunk_bunch[chunk];
-  const BunchDev& B = bunch[l.b];
-  const int q = chunk - B.chunk_off;
-  l.tile0 = B.tile_off + q * kMomChunkTiles;
-  l.nt = min(kMomChunkTiles, B.n_tiles - q * kMomChunkTiles);
-  return l;
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+// every group but the most recent one complete
+__device__ __forceinline__ void cp_async_wait_prior() {
+  asm volatile("cp.async.wait_group 1;\n" ::: "memory");
 }
 
 template <bool MOM, bool KICK>
-__global__ void __launch_bounds__(kTile, 2) k_map_stream(double* __restrict__ c, int64_t npad,
-                                                      const uint8_t* __restrict__ surv,
-                                                      const int* __restrict__ chunk_bunch,
-                                                      const BunchDev* __restrict__ bunch,
-                                                      const __grid_constant__ SectionDev sec,
-                                                      const __grid_constant__ RingDev r,
-                                                      MomPartial* partials, unsigned* counters,
-                                                      BunchMomDev* mom, double beta_x,
-                                                      double beta_y,
-                                                      const CloudRec* __restrict__ rec, int P,
-                                                      int chunk_a, int chunk_b, int* status) {
+__global__ void __launch_bounds__(kTile, 2) k_map_async(double* __restrict__ c, int64_t npad,
+                                                     const uint8_t* __restrict__ surv,
+                                                     const int4* __restrict__ chunk_loc,
+                                                     const BunchDev* __restrict__ bunch,
+                                                     const __grid_constant__ SectionDev sec,
+                                                     const __grid_constant__ RingDev r,
+                                                     MomPartial* partials, unsigned* counters,
+                                                     BunchMomDev* mom, double beta_x,
+                                                     double beta_y,
+                                                     const CloudRec* __restrict__ rec,
+                                                     const FieldPrep* __restrict__ rec_prep,
+                                                     int P, int chunk_a, int chunk_b) {
   extern __shared__ __align__(128) unsigned char dyn_smem[];
-  StreamBuf* buf = reinterpret_cast<StreamBuf*>(dyn_smem);
-  __shared__ __align__(8) uint64_t s_bar[kStreamStages];
-  __shared__ FieldPrep s_prep[CG_MAX_SPECIES];
-  const int tid = threadIdx.x;
-  const int nmine = (chunk_b - chunk_a - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
-  if (nmine <= 0) return;
-  if (tid == 0) {
-    for (int st = 0; st < kStreamStages; ++st) umma::mbar_init(umma::smem_addr(&s_bar[st]), 1);
-    bulk::fence_mbar_init();
-  }
-  __syncthreads();
-  // thread 0: chunk number `it` of this CTA into buffer it % kStreamStages
-  auto issue = [&](int it) {
-    const ChunkLoc l = chunk_loc(chunk_a + (int)blockIdx.x + it * (int)gridDim.x, chunk_bunch, bunch);
-    StreamBuf& sb = buf[it % kStreamStages];
-    const uint32_t bar = umma::smem_addr(&s_bar[it % kStreamStages]);
-    const uint32_t bc = (uint32_t)l.nt * kTile * sizeof(double), bs = (uint32_t)l.nt * kTile;
-    bulk::arrive_expect(bar, 6 * bc + bs);
-    const int64_t g0 = (int64_t)l.tile0 * kTile;
+  AsyncStage* stage = reinterpret_cast<AsyncStage*>(dyn_smem);
+  const int tid = threadIdx.x, G = (int)gridDim.x;
+  int chunk = chunk_a + (int)blockIdx.x;
+  if (chunk >= chunk_b) return;
+  // this thread's slots of the chunk at l (x bunch, y first tile, z tiles)
+  // into stage st: six coordinates and the aligned word holding the survival
+  // byte (the surv rows start 256-byte aligned)
+  auto issue = [&](const int4& l, int st) {
 #pragma unroll
-    for (int d = 0; d < 6; ++d) bulk::load(umma::smem_addr(&sb.v[d][0]), c + d * npad + g0, bc, bar);
-    bulk::load(umma::smem_addr(&sb.s[0]), surv + g0, bs, bar);
-  };
-  if (tid == 0)
-    for (int it = 0; it < kStreamStages && it < nmine; ++it) issue(it);
-  for (int it = 0; it < nmine; ++it) {
-    const int chunk = chunk_a + (int)blockIdx.x + it * (int)gridDim.x;
-    const ChunkLoc l = chunk_loc(chunk, chunk_bunch, bunch);
-    const BunchDev B = bunch[l.b];
-    const CloudRec* rb = rec + (size_t)l.b * P;
-    if (KICK && tid < P) s_prep[tid] = field_prep(rb[tid].rms_x, rb[tid].rms_y);
-    const int st = it % kStreamStages;
-    const bool ok = umma::mbar_wait(umma::smem_addr(&s_bar[st]), (uint32_t)(it / kStreamStages) & 1u,
-                                    kCopyWaitLimit);
-    if (__syncthreads_or(!ok)) {
-      // give up: record it, let the copies in flight land, leave
-      if (tid == 0) {
-        atomicOr(status, kStatusCopyWait);
-        for (int j = it; j < it + kStreamStages && j < nmine; ++j)
-          umma::mbar_wait(umma::smem_addr(&s_bar[j % kStreamStages]),
-                          (uint32_t)(j / kStreamStages) & 1u, kCopyWaitLimit);
+    for (int u = 0; u < kMomChunkTiles; ++u) {
+      if (u < l.z) {
+        const int64_t g = (int64_t)(l.y + u) * kTile + tid;
+#pragma unroll
+        for (int d = 0; d < 6; ++d) cp_async8(&stage[st].v[u][d][tid], c + d * npad + g);
+        cp_async4(&stage[st].sw[u][tid], surv + (g & ~(int64_t)3));
       }
-      return;
     }
-    StreamBuf& sb = buf[st];
-    const int i0 = (l.tile0 - B.tile_off) * kTile + tid;
-    double v[kMomChunkTiles][6];
-    bool alive[kMomChunkTiles];
-#pragma unroll
+  };
+  const int byte = 8 * (tid & 3);
+  int4 cur = chunk_loc[chunk];
+  issue(cur, 0);
+  cp_async_commit();
+  int4 nxt = chunk + G < chunk_b ? chunk_loc[chunk + G] : make_int4(0, 0, 0, 0);
+  for (int st = 0;; st ^= 1) {
+    const int cn = chunk + G;
+    if (cn < chunk_b) issue(nxt, st ^ 1);
+    cp_async_commit();  // (empty when there is no next chunk)
+    const int4 nn = cn + G < chunk_b ? chunk_loc[cn + G] : make_int4(0, 0, 0, 0);
+    cp_async_wait_prior();  // this chunk's copies have landed
+    AsyncStage& sb = stage[st];
+    // one tile at a time, not unrolled (the registers of one particle, not
+    // of four); the mapped particle goes back to this thread's slots of the
+    // stage for the second pass of the moments
+    uint32_t alive = 0;
+    double s[7] = {0, 0, 0, 0, 0, 0, 0};
+    double mn = INFINITY, mx = -INFINITY;
+#pragma unroll 1
     for (int u = 0; u < kMomChunkTiles; ++u) {
-      const int idx = u * kTile + tid;
-      const bool valid = i0 + u * kTile < B.n;
-      alive[u] = valid && sb.s[idx] == kAlive;
+      const bool valid = u * kTile + tid < cur.w;
+      if (!(valid && ((sb.sw[u][tid] >> byte) & 0xFFu) == kAlive)) continue;
+      alive |= 1u << u;
+      double v[6];
 #pragma unroll
-      for (int d = 0; d < 6; ++d) v[u][d] = valid ? sb.v[d][idx] : 0.0;
-    }
-    // buffer st is read: the copy two chunks ahead may refill it
-    __syncthreads();
-    if (tid == 0 && it + kStreamStages < nmine) issue(it + kStreamStages);
-#pragma unroll
-    for (int u = 0; u < kMomChunkTiles; ++u) {
-      if (!alive[u]) continue;
+      for (int d = 0; d < 6; ++d) v[d] = sb.v[u][d][tid];
       if (KICK) {
         double dpx, dpy;
-        ion_kick_particle_prep(rb, s_prep, P, v[u][0], v[u][2], &dpx, &dpy);
-        v[u][1] += dpx;
-        v[u][3] += dpy;
+        ion_kick_particle_prep(rec + (size_t)cur.x * P, rec_prep + (size_t)cur.x * P, P, v[0],
+                               v[2], &dpx, &dpy);
+        v[1] += dpx;
+        v[3] += dpy;
       }
-      section_map_particle(sec, r, v[u]);
-      store6(c, npad, (int64_t)(l.tile0 + u) * kTile + tid, v[u]);
+      section_map_particle(sec, r, v);
+      store6(c, npad, (int64_t)(cur.y + u) * kTile + tid, v);
+      if (MOM) {
+#pragma unroll
+        for (int d = 0; d < 6; ++d) sb.v[u][d][tid] = v[d];
+        chunk_sums_add(v, s, mn, mx);
+      }
     }
     if (MOM) {
       const int warp = tid >> 5;
-      warp_moment_partial(v, alive, &partials[(size_t)chunk * kWarpsPerChunk + warp]);
-      warp_moment_finish(l.b, B.chunk_off * kWarpsPerChunk, B.n_chunks * kWarpsPerChunk,
+      warp_moment_reduce<1>(s, mn, mx, [&](int u) { return ((alive >> u) & 1u) != 0; },
+                            [&](int u, int d) { return sb.v[u][d][tid]; },
+                            &partials[(size_t)chunk * kWarpsPerChunk + warp]);
+      const BunchDev& B = bunch[cur.x];
+      warp_moment_finish(cur.x, B.chunk_off * kWarpsPerChunk, B.n_chunks * kWarpsPerChunk,
                          partials, counters, mom, beta_x, beta_y,
                          c + 4 * npad + (int64_t)B.tile_off * kTile);
     }
-    if (KICK) __syncthreads();  // s_prep is rewritten for the next chunk
+    if (cn >= chunk_b) break;
+    chunk = cn;
+    cur = nxt;
+    nxt = nn;
   }
 }
 
-template <bool MOM, bool KICK>
-static cudaError_t map_stream_kernel(int grid, cudaStream_t s, Handle& h, int k, double bx,
-                                     double by, const CloudRec* rec, int chunk_a, int chunk_b) {
-  // the attribute belongs to the current device's context: set it there
-  // (cheap; the pass is a measurement stage, not in the turn graph)
-  cudaError_t e = cudaFuncSetAttribute(k_map_stream<MOM, KICK>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)kStreamSmem);
-  if (e != cudaSuccess) return e;
-  k_map_stream<MOM, KICK><<<grid, kTile, kStreamSmem, s>>>(
-      h.d.c, h.npad, h.d.surv, h.d.chunk_bunch, h.d.bunch, h.sec_dev_host[k], h.ring,
-      h.d.wpartials, h.d.counters, h.d.mom, bx, by, rec, h.P, chunk_a, chunk_b, h.d.status);
-  return cudaGetLastError();
+static int device_sms() {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms < 1 ? 1 : sms;
 }
 
-cudaError_t launch_map_stream(Handle& h, int k, int mom_section, bool kick, int chunk_a,
-                              int chunk_b, cudaStream_t s) {
+// Per device, once: the dynamic shared memory the asynchronous map pass asks
+// for (above the 48 KB default), and the largest shared-memory carveout, so
+// that two of its CTAs fit on an SM.
+cudaError_t prepare_map_async() {
+  const void* kerns[] = {(const void*)k_map_async<true, false>, (const void*)k_map_async<true, true>,
+                         (const void*)k_map_async<false, false>,
+                         (const void*)k_map_async<false, true>};
+  for (const void* f : kerns) {
+    cudaError_t e =
+        cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAsyncSmem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               (int)cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t launch_map_turn(Handle& h, int k, int mom_section, bool kick, int chunk_a,
+                            int chunk_b, cudaStream_t s) {
+  return h.map_async ? launch_map_async(h, k, mom_section, kick, chunk_a, chunk_b, s)
+                     : launch_map_pass(h, k, mom_section, kick, chunk_a, chunk_b, s);
+}
+
+cudaError_t launch_map_async(Handle& h, int k, int mom_section, bool kick, int chunk_a,
+                             int chunk_b, cudaStream_t s) {
   static int sms = 0;
-  if (!sms) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (sms < 1) sms = 1;
-  }
+  if (!sms) sms = device_sms();
   const bool m = mom_section >= 0;
   const double bx = m ? h.sec_dev_host[mom_section].beta_x : 0.0;
   const double by = m ? h.sec_dev_host[mom_section].beta_y : 0.0;
   const CloudRec* rec = kick ? h.d.rec + (size_t)k * h.M * h.P : nullptr;
+  const FieldPrep* rp = kick ? h.d.rec_prep + (size_t)k * h.M * h.P : nullptr;
   if (chunk_b < 0) chunk_b = h.n_chunks;
   if (!s) s = h.stream;
   if (chunk_b <= chunk_a) return cudaSuccess;
   const int grid = std::min(chunk_b - chunk_a, 2 * sms);
-  if (m)
-    return kick ? map_stream_kernel<true, true>(grid, s, h, k, bx, by, rec, chunk_a, chunk_b)
-                : map_stream_kernel<true, false>(grid, s, h, k, bx, by, rec, chunk_a, chunk_b);
-  return kick ? map_stream_kernel<false, true>(grid, s, h, k, bx, by, rec, chunk_a, chunk_b)
-              : map_stream_kernel<false, false>(grid, s, h, k, bx, by, rec, chunk_a, chunk_b);
+  auto kern = m ? (kick ? k_map_async<true, true> : k_map_async<true, false>)
+                : (kick ? k_map_async<false, true> : k_map_async<false, false>);
+  kern<<<grid, kTile, kAsyncSmem, s>>>(h.d.c, h.npad, h.d.surv, h.d.chunk_loc, h.d.bunch,
+                                       h.sec_dev_host[k], h.ring, h.d.wpartials, h.d.counters,
+                                       h.d.mom, bx, by, rec, rp, h.P, chunk_a, chunk_b);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_ion_kick(Handle& h, int k) { return launch_ion_kick_variant(h, k, h.kick_variant); }
@@ -1073,7 +1162,7 @@ __global__ void __launch_bounds__(kTile) k_gaussian(double* __restrict__ c, int6
                                                     int* __restrict__ status) {
   TileIdx t = tile_index(tile_bunch, bunch);
   if (!t.valid) {
-    surv[t.g] = 0xFF;  // padding slot: never alive
+    surv[t.g] = kPadding;  // padding slot: never alive
 #pragma unroll
     for (int d = 0; d < 6; ++d) c[d * npad + t.g] = 0.0;
     return;
@@ -1253,6 +1342,7 @@ cudaError_t measure_fp64_peak(double* flops) {
 
 cudaError_t upload_weideman_table() {
   cudaError_t e = cudaMemcpyToSymbol(c_weideman, &h_weideman, sizeof(WeidemanTable));
+  if (e == cudaSuccess) e = prepare_map_async();
   if (e == cudaSuccess) e = upload_weideman_table_ion();
   return e != cudaSuccess ? e : upload_weideman_table_sur();
 }

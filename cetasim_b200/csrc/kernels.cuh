@@ -11,7 +11,6 @@ enum : int {
   kStatusLrRange = 4,
   kStatusIonBirth = 8,
   kStatusSurrogateWait = 16,  // a tensor-core completion wait gave up
-  kStatusCopyWait = 32,       // a bulk-copy completion wait gave up
   kStatusGaussCut = 64,       // an initial-distribution draw found no accepted sample
 };
 
@@ -37,11 +36,16 @@ void kick_variant_shape(int v, int* threads, int* min_ctas);
 // (chunk_b < 0: all) on stream s (null: h.stream)
 cudaError_t launch_map_pass(Handle& h, int k, int mom_section, bool kick = false, int chunk_a = 0,
                             int chunk_b = -1, cudaStream_t s = nullptr);
-// The same pass with the chunks streamed through shared memory: a persistent
-// grid (two CTAs per SM), each CTA with two chunk buffers filled by bulk
-// asynchronous copies while it maps and reduces the previous chunk.
-cudaError_t launch_map_stream(Handle& h, int k, int mom_section, bool kick = false,
-                              int chunk_a = 0, int chunk_b = -1, cudaStream_t s = nullptr);
+// The same pass with the next chunk in flight: a persistent grid (two CTAs
+// per SM) in which every thread stages its slots of the CTA's next chunk in
+// shared memory by cp.async while it maps and reduces the current one.
+cudaError_t launch_map_async(Handle& h, int k, int mom_section, bool kick = false,
+                             int chunk_a = 0, int chunk_b = -1, cudaStream_t s = nullptr);
+// the map pass of the turn: the asynchronous form when h.map_async is set
+cudaError_t launch_map_turn(Handle& h, int k, int mom_section, bool kick = false,
+                            int chunk_a = 0, int chunk_b = -1, cudaStream_t s = nullptr);
+// per device, once: the dynamic shared memory of the asynchronous map pass
+cudaError_t prepare_map_async();
 enum LongFlags : unsigned {
   kLongRF = 1,
   kLongDrift = 2,
@@ -99,7 +103,8 @@ cudaError_t launch_sur_eval(const float* w, const float* xin, int64_t n, float* 
 cudaError_t launch_sur_step(const float* w, const float* xin, const float* tin, int64_t n,
                             int64_t row0, int batch, uint64_t mul, uint64_t add, float* part,
                             float* m, float* v, float* wmut, float lr, float bc1, float bc2,
-                            double* loss, float* grad_out, int* status, cudaStream_t s);
+                            double* loss, float* grad_out, int* status, cudaStream_t s,
+                            float l4w = 0.0f, float* e2_sum = nullptr);
 cudaError_t launch_ion_kick_sur(Handle& h, int k, int tile_a = 0, int tile_b = -1,
                                 cudaStream_t s = nullptr);
 cudaError_t launch_sur_audit(Handle& h, int k, unsigned long long* out);

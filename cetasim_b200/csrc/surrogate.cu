@@ -271,14 +271,17 @@ __global__ void __launch_bounds__(kSurRows) k_sur_eval(const float* __restrict__
 // ---------------------------------------------------------------------------
 // Training: one CTA = 128 samples of the batch (sample index (mul * j + add)
 // mod n for batch row j, an affine shuffle per epoch), gradients of
-// L = sum (out - t)^2 / (2 B) into a per-CTA slice of `part`
-// (kSurParams values + the tile's loss).
+// L = (1 - w) sum e^2 / (2 B) + w sum e^4 / (2 B m), e = out - t over both
+// outputs, into a per-CTA slice of `part` (kSurParams values + the tile's
+// sum of e^2).  m = mean e^2 of the previous step (*e2_prev = its sum, held
+// fixed in the derivative); w = 0 is the plain squared error.
 
 __global__ void __launch_bounds__(kSurRows) k_sur_train_tile(const float* __restrict__ w,
                                                              const float* __restrict__ xin,
                                                              const float* __restrict__ tin,
                                                              int64_t n, int64_t row0, uint64_t mul,
                                                              uint64_t add, float inv_batch,
+                                                             float l4w, const float* e2_prev,
                                                              float* __restrict__ part,
                                                              int* status) {
   extern __shared__ unsigned char dyn[];
@@ -302,8 +305,17 @@ __global__ void __launch_bounds__(kSurRows) k_sur_train_tile(const float* __rest
   sur_norm(xin[3 * s], xin[3 * s + 1], xin[3 * s + 2], x);
   bool ok = sur_forward(base, sm, tmem, bar, phase, x, out, z1s, z2s, z3s);
   const float e0 = out[0] - tin[2 * s], e1 = out[1] - tin[2 * s + 1];
+  // dL/de = (e / B) ((1 - w) + 2 w e^2 / m)
+  float g0 = 1.0f, g1 = 1.0f;
+  if (l4w > 0.0f && e2_prev) {
+    const float m = *e2_prev * inv_batch * 0.5f;
+    if (m > 0.0f) {
+      g0 = fmaf(2.0f * l4w, e0 * e0 / m, 1.0f - l4w);
+      g1 = fmaf(2.0f * l4w, e1 * e1 / m, 1.0f - l4w);
+    }
+  }
   // dL/d(layer-4 output): through the odd-output factors a, b
-  const float d0 = e0 * inv_batch * sur_a(x), d1 = e1 * inv_batch * sur_b(x);
+  const float d0 = e0 * inv_batch * g0 * sur_a(x), d1 = e1 * inv_batch * g1 * sur_b(x);
   s_x[r][0] = x[0];
   s_x[r][1] = x[1];
   s_x[r][2] = x[2];
@@ -418,17 +430,18 @@ __global__ void __launch_bounds__(kSurRows) k_sur_train_tile(const float* __rest
 }
 
 // Sum of the CTA slices in CTA order, then one Adam step (Kingma & Ba 2015)
-// on the FP32 master weights; the loss of the step is accumulated into
-// *loss.
+// on the FP32 master weights; the step's sum of e^2 is accumulated into
+// *loss and kept in *e2_sum (the next step's m).
 __global__ void k_sur_adam(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
                            const float* __restrict__ part, int ncta, float lr, float bc1,
-                           float bc2, double* loss, float* grad_out) {
+                           float bc2, double* loss, float* e2_sum, float* grad_out) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p > kSurParams) return;
   float gsum = 0.0f;
   for (int c = 0; c < ncta; ++c) gsum += part[(size_t)c * (kSurParams + 1) + p];
   if (p == kSurParams) {
     if (loss) *loss += (double)gsum;
+    if (e2_sum) *e2_sum = gsum;
     return;
   }
   if (grad_out) grad_out[p] = gsum;
@@ -622,14 +635,16 @@ cudaError_t launch_sur_eval(const float* w, const float* xin, int64_t n, float* 
 cudaError_t launch_sur_step(const float* w, const float* xin, const float* tin, int64_t n,
                             int64_t row0, int batch, uint64_t mul, uint64_t add, float* part,
                             float* m, float* v, float* wmut, float lr, float bc1, float bc2,
-                            double* loss, float* grad_out, int* status, cudaStream_t s) {
+                            double* loss, float* grad_out, int* status, cudaStream_t s,
+                            float l4w, float* e2_sum) {
   const int ncta = batch / kSurRows;
   k_sur_train_tile<<<ncta, kSurRows, kSmTrainBytes, s>>>(w, xin, tin, n, row0, mul, add,
-                                                         1.0f / (float)batch, part, status);
+                                                         1.0f / (float)batch, l4w, e2_sum, part,
+                                                         status);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   k_sur_adam<<<(kSurParams + 1 + 255) / 256, 256, 0, s>>>(wmut, m, v, part, ncta, lr, bc1, bc2,
-                                                          loss, grad_out);
+                                                          loss, e2_sum, grad_out);
   return cudaGetLastError();
 }
 

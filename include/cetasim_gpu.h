@@ -326,8 +326,9 @@ int cg_turn_launches(cg_handle* h, int* launches);
  * chain (k), 3 moments (k), 4 longitudinal turn tail, 5 the map + moments
  * pass of the turn graph (section k), 6 the surrogate field kick (k, after
  * cg_set_surrogate), 7 the map + moments pass with the ion kick inside, 8 and
- * 9 the passes 5 and 7 streamed through shared memory by bulk copies
- * (persistent grid).  The beam state is advanced by these launches. */
+ * 9 the passes 5 and 7 with each CTA's next chunk staged in shared memory by
+ * cp.async while it works on the current one (persistent grid).  The beam
+ * state is advanced by these launches. */
 int cg_time_stage(cg_handle* h, int stage, int k, int reps, double* ms);
 /* FP64 FMA throughput of this device measured by a register-resident FMA
  * chain kernel, in FLOP/s (2 per FMA). */
@@ -379,8 +380,8 @@ int cg_gaussian_field(const double* x, const double* y, const double* sx,
 
 /* ---- autotuning (no counterpart in the reference) ---- */
 
-/* Number n of shapes (threads per CTA, register budget) of the field-kick
- * kernel.  Choices 0 .. n-1 run the kick as its own kernel with that shape;
+/* Number n of shapes (threads per CTA, register budget, tiles per CTA) of
+ * the field-kick kernel.  Choices 0 .. n-1 run the kick as its own kernel with that shape;
  * n .. 2n-1 the same shape for the staged calls and, in the turn graph, the
  * kick inside the map pass (one particle pass for kick, map and moments). */
 int cg_kick_variants(int* n);
@@ -388,11 +389,19 @@ int cg_kick_variants(int* n);
 int cg_set_kick_variant(cg_handle* h, int v);
 /* Times every kick shape on h's own beam at IP k (reps launches each, after
  * a warm-up; the records of the last ion pass at k), then the map pass with
- * and without the kick inside; restores the beam after every trial and
- * selects the fastest combination: *choice (as cg_set_kick_variant takes it),
- * ms[0 .. n-1] per kick launch, ms[n] the map pass, ms[n+1] the map pass with
- * the kick (ms holds n + 2 values). */
+ * and without the kick inside, each in its register form and with the next
+ * chunk in flight; restores the beam after every trial and selects the
+ * fastest combination: *choice (as cg_set_kick_variant takes it), ms[0 .. n-1]
+ * per kick launch, ms[n] the map pass, ms[n+1] the map pass with the kick,
+ * ms[n+2] and ms[n+3] the same with the next chunk in flight (ms holds n + 4
+ * values); the map-pass form chosen is set as by cg_set_map_async. */
 int cg_autotune(cg_handle* h, int k, int reps, int* choice, double* ms);
+/* The map pass form of the turn graph: 0 one chunk per CTA with its loads in
+ * registers, 1 a persistent grid with each CTA's next chunk staged in shared
+ * memory by cp.async while it works on the current one (the turn graph is
+ * rebuilt).  Results are bitwise the same. */
+int cg_set_map_async(cg_handle* h, int on);
+int cg_map_async(cg_handle* h, int* on);
 
 /* Pipelined turn: the ion walk of each IP runs in `groups` segments of
  * bunches, and the kicks and maps of a walked segment run alongside the next
@@ -406,11 +415,11 @@ int cg_set_pipeline(cg_handle* h, int groups, int walk_ions, int ramp);
 /* Times whole turns (turn0 to warm up the turn graph, then `reps` turns, CUDA
  * events on h's stream) with each of the CG_PIPE_SHAPES pipeline shapes
  * (segments, walk ions, ramp): (1,64,0) (1,16,0) (2,64,0) (2,64,1) (3,64,0)
- * (3,64,1) (4,64,0) (4,64,1) (3,16,1) (6,64,1); puts the beam and the ion
- * clouds back from a host checkpoint after every trial and keeps the
- * fastest: shape[0..2] (may be NULL), ms[CG_PIPE_SHAPES] per turn (may be
- * NULL). */
-#define CG_PIPE_SHAPES 10
+ * (3,64,1) (4,64,0) (4,64,1) (3,16,1) (6,64,1) (8,64,1) (12,64,1) (16,64,1)
+ * (8,32,1) (12,32,1) (16,32,1); puts the beam and the ion clouds back from a
+ * host checkpoint after every trial and keeps the fastest: shape[0..2] (may
+ * be NULL), ms[CG_PIPE_SHAPES] per turn (may be NULL). */
+#define CG_PIPE_SHAPES 16
 int cg_autotune_pipeline(cg_handle* h, int turn0, int reps, int* shape, double* ms);
 
 /* ---- resistive-wall wake functions (host, stateless) ---- */
@@ -571,6 +580,10 @@ typedef struct cg_sur_train_params {
   int epochs;
   int batch;           /* a multiple of 128 */
   double lr;           /* peak Adam learning rate (30 % linear warm-up, cosine decay) */
+  double l4_from;      /* fraction of the epochs after which the loss mixes in the
+                          fourth power (1 or more: never) */
+  double l4_weight;    /* w of L = (1 - w) sum e^2 / (2B) + w sum e^4 / (2B m), m the
+                          previous step's mean e^2: weighs the largest errors */
 } cg_sur_train_params;
 
 /* n samples (a, b, r) of the exact FP64 field (Philox-seeded) -> inputs

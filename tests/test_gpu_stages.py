@@ -206,7 +206,7 @@ def test_kick_autotuner_keeps_the_beam_and_shapes_agree():
     g.SSBeamIonEffectOneInteractionPoint(0, 0)
     before = [g.download(j) for j in range(wl.n_bunches)]
     choice, ms = g.autotune(0, reps=3)
-    n = len(ms) - 2
+    n = len(ms) - 4
     assert 0 <= choice < 2 * n and np.all(ms > 0) and ms[choice % n] == ms[:n].min()
     after = [g.download(j) for j in range(wl.n_bunches)]
     for (a, s), (b, t) in zip(before, after):
@@ -227,8 +227,12 @@ def test_kick_autotuner_keeps_the_beam_and_shapes_agree():
 def test_kick_inside_the_map_pass_repeats_the_separate_kernels():
     wl = small("fast_ion", 0.01, bunch_current=TRAPPED)
     parts = particles(wl, seed=7)
+    import ctypes as C
+    from cetasim_b200 import _abi
+    nv = C.c_int()
+    _abi.load().cg_kick_variants(C.byref(nv))
     runs = []
-    for v in (0, 4):  # 4 = the first kick shape inside the map pass
+    for v in (0, nv.value):  # nv = the first kick shape inside the map pass
         g, _ = pair(wl, parts)
         g.set_kick_variant(v)
         g.Run(0, 4)
@@ -236,6 +240,33 @@ def test_kick_inside_the_map_pass_repeats_the_separate_kernels():
     worst = max(np.max(np.abs(a - b) / (np.abs(b).max(axis=1, keepdims=True) + 1e-300))
                 for a, b in zip(*runs))
     assert worst <= 1e-14
+
+
+@pytest.mark.parametrize("name,scale,groups", [("fast_ion", 0.01, 3), ("batched_uneven", 0.01, 6)])
+def test_turns_with_the_asynchronous_map_pass_repeat_the_register_pass(name, scale, groups):
+    """Whole turns (pipelined, with ions, wakes and feedback) with the map pass
+    that keeps each CTA's next chunk in flight give the coordinates, survival
+    flags and clouds of the register pass bit for bit."""
+    wl = small(name, scale, bunch_current=TRAPPED)
+    parts = particles(wl, seed=10)
+    runs = []
+    from cetasim_b200.beam import MPBeam
+    for on in (False, True):
+        g = MPBeam(wl)
+        for j, c in enumerate(parts):
+            g.upload(j, c)
+        g.set_pipeline(groups, 64, True)
+        g.set_map_async(on)
+        assert g.map_async() == on
+        g.Run(0, 3)
+        runs.append(([g.download(j) for j in range(wl.n_bunches)],
+                     [g.ions(k) for k in (0, wl.cfg.n_sections - 1)]))
+    (ca, ia), (cb, ib) = runs
+    for (x, s), (y, t) in zip(ca, cb):
+        assert np.array_equal(x, y) and np.array_equal(s, t)
+    for u, v in zip(ia, ib):
+        for p, q in zip(u, v):
+            assert np.array_equal(p, q)
 
 
 @pytest.mark.parametrize("groups,ramp", [(3, False), (4, True), (16, False), (2, True)])
@@ -271,9 +302,10 @@ def _stage(g, stage, k, reps=1):
                                              ("fast_ion", 0.15, False),
                                              ("fast_ion", 0.15, True)])
 def test_streamed_map_pass_repeats_the_register_pass(name, scale, kick):
-    """The map pass fed by bulk copies into shared memory (stages 8, 9) gives
-    the coordinates and moments of the register pass (stages 5, 7) bit for
-    bit, on ragged bunches (partial chunks and tiles) with lost particles."""
+    """The map pass with each CTA's next chunk staged in shared memory by
+    cp.async (stages 8, 9) gives the coordinates and moments of the register
+    pass (stages 5, 7) bit for bit, on ragged bunches (partial chunks and
+    tiles) with lost particles."""
     wl = small(name, scale, bunch_current=TRAPPED if kick else None)
     parts = particles(wl, seed=11, spread=3.0 if kick else 1.0)
     rng = np.random.default_rng(12)
