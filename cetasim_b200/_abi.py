@@ -38,6 +38,15 @@ class Ring(C.Structure):
         ("r_gamma", D), ("r_beta", D), ("t0", D), ("f0", D), ("eta", D), ("work_qz", D),
         ("natural_bunch_length", D), ("beta_z", D), ("emit_nat", D * 3),
         ("cav_vreq_re", D * MAX_CAVITIES), ("cav_vreq_im", D * MAX_CAVITIES),
+        ("rf_mode", I * MAX_CAVITIES), ("res_type", I * MAX_CAVITIES),
+        ("res_cold", I * MAX_CAVITIES), ("res_excite", I * MAX_CAVITIES),
+        ("res_dir_fb", I * MAX_CAVITIES), ("rf_bunch_bins", I),
+        ("res_rs", D * MAX_CAVITIES), ("res_q0", D * MAX_CAVITIES),
+        ("res_coupling", D * MAX_CAVITIES), ("res_detune", D * MAX_CAVITIES),
+        ("res_dir_fb_gain", D * MAX_CAVITIES), ("res_dir_fb_phase", D * MAX_CAVITIES),
+        ("res_dir_fb_delay", D * MAX_CAVITIES),
+        ("res_ql", D * MAX_CAVITIES), ("res_fre", D * MAX_CAVITIES),
+        ("res_psi", D * MAX_CAVITIES), ("res_tf", D * MAX_CAVITIES),
     ]
 
 
@@ -190,6 +199,10 @@ EXPORTS = [
     ("cg_set_kick_variant", I, [C.c_void_p, I]),
     ("cg_autotune", I, [C.c_void_p, I, I, PI, PD]),
     ("cg_set_map_async", I, [C.c_void_p, I]),
+    ("cg_resonator_state", I, [C.c_void_p, I, PD]),
+    ("cg_set_resonator_state", I, [C.c_void_p, I, PD]),
+    ("cg_rf_info", I, [C.c_void_p, I, I, PD]),
+    ("cg_set_walk_reserve", I, [C.c_void_p, I]),
     ("cg_map_async", I, [C.c_void_p, PI]),
     ("cg_shard_plan", I, [PI, I, I, PI, PI]),
     ("cg_shard_exchange_size", I, [PI, I, I, PI]),

@@ -161,6 +161,27 @@ class MPBeam:
     def set_kick_variant(self, v: int):
         self._check(self.lib.cg_set_kick_variant(self.h, v))
 
+    # -- cavities with beam loading (rfMode 1) -------------------------------------
+    def resonator(self, c: int):
+        """(vbAccum, resGenVol, resGenIg) of cavity c as complex numbers."""
+        out = np.empty(6)
+        self._check(self.lib.cg_resonator_state(self.h, c, _abi.ptr(out)))
+        return complex(out[0], out[1]), complex(out[2], out[3]), complex(out[4], out[5])
+
+    def set_resonator(self, c: int, vb: complex, gen: complex, ig: complex):
+        a = np.array([vb.real, vb.imag, gen.real, gen.imag, ig.real, ig.imag])
+        self._check(self.lib.cg_set_resonator_state(self.h, c, _abi.ptr(a)))
+
+    def rf_info(self, j: int, c: int):
+        """BunchRFModeInfo of bunch j, cavity c after the last RF step:
+        (cavity, generator, induced, self-loss) voltages as complex numbers."""
+        out = np.empty(8)
+        self._check(self.lib.cg_rf_info(self.h, j, c, _abi.ptr(out)))
+        return tuple(complex(out[2 * i], out[2 * i + 1]) for i in range(4))
+
+    def set_walk_reserve(self, on: bool):
+        self._check(self.lib.cg_set_walk_reserve(self.h, int(bool(on))))
+
     def set_map_async(self, on: bool):
         self._check(self.lib.cg_set_map_async(self.h, int(bool(on))))
 

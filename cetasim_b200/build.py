@@ -16,7 +16,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libcetagpu.so")
 
 SOURCES = ["capi.cu", "kernels.cu", "kernels_sr.cu", "kernels_ion.cu", "surrogate.cu", "shard.cu",
-           "cbm.cu", "faddeeva_table.cpp", "input_settings.cpp", "rw_wake.cpp"]
+           "cbm.cu", "beam_loading.cu", "faddeeva_table.cpp", "input_settings.cpp", "rw_wake.cpp"]
 HEADERS = ["cg_common.cuh", "faddeeva.cuh", "be_field.cuh", "track_math.cuh", "cg_internal.h",
            "kernels.cuh", "umma.cuh", "surrogate.cuh", "rw_wake.h"]
 
@@ -85,7 +85,8 @@ def build_host(force: bool = False, verbose: bool = False) -> str:
     """The C++ host layer (MPBeam-named wrapper) and the cetasim_mp driver,
     linked against the in-tree libcetagpu.so."""
     hdir = os.path.join(HERE, "host")
-    deps = [os.path.join(hdir, s) for s in HOST_SOURCES + ["mpbeam.hpp", "cbm_writer.hpp"]] + [LIB]
+    deps = [os.path.join(hdir, s) for s in HOST_SOURCES + ["mpbeam.hpp", "cbm_writer.hpp"]] + [
+        LIB, os.path.join(ROOT, "include", "cetasim_gpu.h")]
     if not force and not _stale(CLI, deps):
         return CLI
     cmd = ["g++", "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), "-o", CLI + ".tmp",

@@ -104,6 +104,10 @@ void free_beam(Handle& h) {
   d.mom_send = nullptr; d.mom_all = nullptr; d.sh_off = nullptr; d.sh_cnt = nullptr;
   dfree(d.cbm);  // sized by the bunch count
   d.cbm = nullptr;
+  dfree(d.res_state); dfree(d.rf_zr); dfree(d.rf_counts); dfree(d.rf_kick); dfree(d.rf_fbk);
+  dfree(d.rf_info); dfree(d.rf_work);
+  d.res_state = nullptr; d.rf_zr = nullptr; d.rf_counts = nullptr; d.rf_kick = nullptr;
+  d.rf_fbk = nullptr; d.rf_info = nullptr; d.rf_work = nullptr;
   h.cbm_cap = h.cbm_n = 0;
   IonWalk& w = d.iw;
   dfree(w.births); dfree(w.prep); dfree(w.bunch); dfree(w.spec); dfree(w.bound); dfree(w.part);
@@ -180,11 +184,16 @@ RingDev make_ring_dev(const cg_config& c, const cg_section& s0) {
   d.u0_term = r.u0 / r.electron_energy / std::pow(r.r_beta, 2);
   double fRF = r.f0 * r.harmonics;
   d.n_cav = r.n_cav;
+  int n_bl = 0;
   for (int i = 0; i < r.n_cav && i < 4; ++i) {
     d.rf_theta_coeff[i] = 1.0 / kCLight / r.r_beta * 2. * kPi * (double)r.cav_harm[i] * fRF;
     d.vreq_re[i] = r.cav_vreq_re[i];
     d.vreq_im[i] = r.cav_vreq_im[i];
+    d.bl_index[i] = r.rf_mode[i] == 1 ? n_bl++ : -1;
+    d.bl_fb[i] = r.rf_mode[i] == 1 && r.res_dir_fb[i] == 1;
   }
+  d.bl_any = n_bl > 0;
+  d.rf_bins = r.rf_bunch_bins;
   for (int i = 0; i < 3; ++i) d.lambda[i] = std::exp(-1.0 / r.synch_rad_damp_time[i]);
   d.qe_coeff[0] = std::sqrt(1 - std::pow(d.lambda[0], 2)) * std::sqrt(r.emit_nat[0]);
   d.qe_coeff[1] = std::sqrt(1 - std::pow(d.lambda[1], 2)) * std::sqrt(r.emit_nat[1]);
@@ -230,6 +239,16 @@ int cg_config_derive(cg_config* cfg) {
   for (int i = 0; i < r->n_cav; ++i) {
     r->cav_vreq_re[i] = r->cav_vol[i] * std::cos(ph[i]);
     r->cav_vreq_im[i] = r->cav_vol[i] * std::sin(ph[i]);
+  }
+  // the resonators' loaded Q, frequency, detuning angle and filling time
+  // (CavityResonator::Initial, CavityResonator.cpp:89-104)
+  for (int i = 0; i < r->n_cav; ++i) {
+    const double fh = (double)(r->cav_harm[i] * r->harmonics) * f0;
+    r->res_ql[i] = r->res_q0[i] / (1 + r->res_coupling[i]);
+    r->res_fre[i] = fh + r->res_detune[i];
+    const double tan_psi = r->res_ql[i] * (r->res_fre[i] / fh - fh / r->res_fre[i]);
+    r->res_psi[i] = std::atan(tan_psi);
+    r->res_tf[i] = 2 * r->res_ql[i] / (2 * PI * r->res_fre[i]);
   }
   return CG_OK;
 }
@@ -562,8 +581,7 @@ int cg_set_beam(cg_handle* H, int M, const int* n_macro, const int* harm, const 
     for (int t = 0; t < nt; ++t) tb.push_back(j);
     for (int t = 0; t < nc; ++t) {
       cb.push_back(j);
-      cl.push_back(make_int4(j, tiles + t * kMomChunkTiles, std::min(kMomChunkTiles, nt - t * kMomChunkTiles),
-                             bd[j].n - t * kMomChunkTiles * kTile));
+      cl.push_back(make_int4(j, tiles + t * kMomChunkTiles, t, bd[j].n - t * kMomChunkTiles * kTile));
     }
     tiles += nt;
     chunks += nc;
@@ -650,6 +668,34 @@ int cg_set_beam(cg_handle* H, int M, const int* n_macro, const int* harm, const 
     if (dalloc(&d.fir_hist, (size_t)h.fir_order * 3 * M)) { free_beam(h); return fail(&h, CG_ERR_OOM, "FIR history"); }
     cudaMemset(d.fir_hist, 0, sizeof(double) * h.fir_order * 3 * M);
     cudaMemset(h.d.fir_head, 0, sizeof(int));
+  }
+  if (h.ring.bl_any) {
+    // cavities with beam loading: the resonators' initial state from the fill
+    // pattern (MPBeam::InitialcavityResonator) and the per-bunch tables
+    if (h.sh_world > 1) {
+      free_beam(h);
+      return fail(&h, CG_ERR_UNSUPPORTED, "rfMode 1 with bunch sharding is not supported");
+    }
+    const int nb = h.cfg.ring.rf_bunch_bins;
+    if (nb < 1 || nb > 8192) {
+      free_beam(h);
+      return fail(&h, CG_ERR_INVALID, "rfBunchBinNum must be in [1, 8192] with rfMode 1");
+    }
+    int n_bl = 0;
+    for (int c = 0; c < h.cfg.ring.n_cav; ++c) n_bl += h.cfg.ring.rf_mode[c] == 1;
+    if (dalloc(&d.res_state, 6 * (size_t)CG_MAX_CAVITIES) || dalloc(&d.rf_zr, 2 * (size_t)M) ||
+        dalloc(&d.rf_counts, (size_t)M * nb) || dalloc(&d.rf_kick, (size_t)n_bl * M * nb * 2) ||
+        dalloc(&d.rf_fbk, (size_t)n_bl * M) || dalloc(&d.rf_work, rf_work_doubles(n_bl, M, nb)) ||
+        dalloc(&d.rf_info, (size_t)M * CG_MAX_CAVITIES * 8)) {
+      free_beam(h);
+      return fail(&h, CG_ERR_OOM, "beam-loading buffers");
+    }
+    std::vector<double> st(6 * CG_MAX_CAVITIES, 0.0), info((size_t)M * CG_MAX_CAVITIES * 8, 0.0);
+    std::vector<double> ne_all(h.ne.begin(), h.ne.end());
+    resonator_init(h.cfg, h.harm, ne_all, st.data(), info.data());
+    cudaMemcpy(d.res_state, st.data(), sizeof(double) * st.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(d.rf_info, info.data(), sizeof(double) * info.size(), cudaMemcpyHostToDevice);
+    cudaMemset(d.rf_fbk, 0, sizeof(double) * n_bl * M);
   }
   if (h.cfg.flag_sr_wake) {
     int B = h.cfg.sr_bins;
@@ -1649,6 +1695,46 @@ int cg_autotune(cg_handle* H, int k, int reps, int* choice, double* ms) {
   return st;
 }
 
+int cg_resonator_state(cg_handle* H, int c, double* out6) {
+  STAGE_PROLOGUE
+  if (!out6 || c < 0 || c >= h.cfg.ring.n_cav) return fail(&h, CG_ERR_INVALID, "bad cavity");
+  if (!h.ring.bl_any) return fail(&h, CG_ERR_NOT_READY, "no cavity with beam loading");
+  CG_CUDA(&h, cudaStreamSynchronize(h.stream));
+  CG_CUDA(&h, cudaMemcpy(out6, h.d.res_state + 6 * c, 6 * sizeof(double), cudaMemcpyDeviceToHost));
+  return CG_OK;
+}
+
+int cg_set_resonator_state(cg_handle* H, int c, const double* in6) {
+  STAGE_PROLOGUE
+  if (!in6 || c < 0 || c >= h.cfg.ring.n_cav) return fail(&h, CG_ERR_INVALID, "bad cavity");
+  if (!h.ring.bl_any) return fail(&h, CG_ERR_NOT_READY, "no cavity with beam loading");
+  CG_CUDA(&h, cudaStreamSynchronize(h.stream));
+  CG_CUDA(&h, cudaMemcpy(h.d.res_state + 6 * c, in6, 6 * sizeof(double), cudaMemcpyHostToDevice));
+  return CG_OK;
+}
+
+int cg_rf_info(cg_handle* H, int j, int c, double* out8) {
+  STAGE_PROLOGUE
+  if (!out8 || c < 0 || c >= h.cfg.ring.n_cav || j < 0 || j >= h.M)
+    return fail(&h, CG_ERR_INVALID, "bad bunch or cavity");
+  if (!h.ring.bl_any) return fail(&h, CG_ERR_NOT_READY, "no cavity with beam loading");
+  CG_CUDA(&h, cudaStreamSynchronize(h.stream));
+  CG_CUDA(&h, cudaMemcpy(out8, h.d.rf_info + ((size_t)j * CG_MAX_CAVITIES + c) * 8,
+                         8 * sizeof(double), cudaMemcpyDeviceToHost));
+  return CG_OK;
+}
+
+int cg_set_walk_reserve(cg_handle* H, int on) {
+  if (!H) return CG_ERR_INVALID;
+  Handle& h = H->h;
+  if (h.walk_reserve != (on != 0) && h.turn_graph) {
+    cudaGraphExecDestroy(h.turn_graph);
+    h.turn_graph = nullptr;
+  }
+  h.walk_reserve = on != 0;
+  return CG_OK;
+}
+
 int cg_set_map_async(cg_handle* H, int on) {
   if (!H) return CG_ERR_INVALID;
   Handle& h = H->h;
@@ -1795,6 +1881,8 @@ int ckpt_fixed(Handle& h, Op op) {
     if ((st = op(h.d.fir_head, sizeof(int)))) return st;
   }
   if (h.cfg.flag_sr_wake && (st = op(h.d.sr_pot, M * (size_t)h.cfg.sr_bins * sizeof(double))))
+    return st;
+  if (h.ring.bl_any && (st = op(h.d.res_state, 6 * (size_t)CG_MAX_CAVITIES * sizeof(double))))
     return st;
   return CG_OK;
 }

@@ -74,7 +74,7 @@ struct DeviceBufs {
   uint8_t* surv = nullptr;      // npad
   int* tile_bunch = nullptr;    // n_tiles
   int* chunk_bunch = nullptr;   // n_chunks: bunch of each moments chunk
-  int4* chunk_loc = nullptr;    // n_chunks: (bunch, first tile, tiles, valid slots)
+  int4* chunk_loc = nullptr;    // n_chunks: (bunch, first tile, chunk of the bunch, valid slots)
   BunchDev* bunch = nullptr;    // M
   MomPartial* wpartials = nullptr; // n_chunks x 8: per-warp moment partials
   unsigned* counters = nullptr;    // M (+ spare)
@@ -117,6 +117,14 @@ struct DeviceBufs {
   double* sr_green = nullptr;      // resonators x 1000 (u-independent factors)
   // coupled-bunch mode history (cg_cbm_*): records x kCbmRecord x M
   double* cbm = nullptr;
+  // cavities with beam loading (rfMode 1)
+  double* res_state = nullptr;     // CG_MAX_CAVITIES x 6: vbAccum, resGenVol, resGenIg
+  double* rf_zr = nullptr;         // M x 2: z range of the RF step
+  int* rf_counts = nullptr;        // M x bins
+  double* rf_kick = nullptr;       // loading cavities x M x bins x 2
+  double* rf_fbk = nullptr;        // loading cavities x M: direct-feedback kicks
+  double* rf_work = nullptr;       // work buffers of the cavities' recurrence
+  double* rf_info = nullptr;       // M x CG_MAX_CAVITIES x 8: BunchRFModeInfo
   // scratch
   double* scratch = nullptr;
   size_t scratch_bytes = 0;
@@ -160,6 +168,7 @@ struct Handle {
   // maps of earlier segments fill the GPU
   int walk_ions = 64;
   bool pipe_ramp = false;  // last walk segment half as long as the others
+  bool walk_reserve = false;  // walk CTAs take their SM's whole shared memory
   // turn trace (cg_trace_turn): marks and their timing events
   std::vector<TraceMark>* trace = nullptr;
   std::vector<cudaEvent_t> trace_ev;

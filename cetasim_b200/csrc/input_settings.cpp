@@ -225,14 +225,37 @@ extern "C" int cg_config_from_input(const char* path, cg_config* cfg, int* n_bun
       g_parse_error = "rfResNum must be in [1, 4]";
       return CG_ERR_INVALID;
     }
+    // per cavity (ReadInputSettings.cpp:192-362: the lists are sized by
+    // rfResNum and default to zero; the integer lists read through stod
+    // are truncated)
+    auto Dz = [&](const char* k, int i) { return has(k) ? D(get(k), i) : 0.0; };
+    bool loading = false;
     for (int i = 0; i < r.n_cav; ++i) {
       r.cav_harm[i] = Ii(get("rfresharm"), i);
       r.cav_vol[i] = D(get("rfresvol"), i);
-      r.cav_phase[i] = has("rfresphase") ? D(get("rfresphase"), i) : 0.0;
-      if (has("rfmode") && Ii(get("rfmode"), i) != 0) {
-        g_parse_error = "rfMode 1 (beam loading) is outside the tracking path of this library";
-        return CG_ERR_UNSUPPORTED;
+      r.cav_phase[i] = Dz("rfresphase", i);
+      r.rf_mode[i] = has("rfmode") ? Ii(get("rfmode"), i) : 0;
+      r.res_type[i] = has("rfrestype") ? Ii(get("rfrestype"), i) : 0;
+      r.res_cold[i] = has("rfrescold") ? Ii(get("rfrescold"), i) : 0;
+      r.res_excite[i] = (int)Dz("rfresexciteintability", i);
+      r.res_dir_fb[i] = (int)Dz("rfresdirfb", i);
+      r.res_rs[i] = Dz("rfresshuntimprs", i);
+      r.res_q0[i] = Dz("rfresqualityq0", i);
+      r.res_coupling[i] = Dz("rfrescouplingbeta", i);
+      r.res_detune[i] = Dz("rfresdetunefre", i);
+      r.res_dir_fb_gain[i] = Dz("rfresdirfbgain", i);
+      r.res_dir_fb_phase[i] = Dz("rfresdirfbphaseshift", i);
+      r.res_dir_fb_delay[i] = Dz("rfresdirfbdelay", i);
+      if (r.rf_mode[i] != 0 && r.rf_mode[i] != 1) {
+        g_parse_error = "rfMode must be 0 or 1";
+        return CG_ERR_INVALID;
       }
+      loading = loading || r.rf_mode[i] == 1;
+    }
+    r.rf_bunch_bins = has("rfbunchbinnum") ? (int)D(get("rfbunchbinnum"), 0) : 0;
+    if (loading && r.rf_bunch_bins < 1) {
+      g_parse_error = "rfMode 1 needs rfBunchBinNum >= 1";
+      return CG_ERR_INVALID;
     }
     // run flags
     auto flag = [&](const char* k) { return has(k) ? Ii(get(k), 0) : 0; };

@@ -401,19 +401,23 @@ __device__ __forceinline__ void warp_moment_partial(const double (&v)[kMomChunkT
                                      [&](int u, int d) { return v[u][d]; }, out);
 }
 
-// After the warp's partial is stored: the last of the bunch's n_parts warps
-// merges them.
-__device__ __forceinline__ void warp_moment_finish(int b, int part_off, int n_parts,
-                                                   const MomPartial* partials,
-                                                   unsigned* counters, BunchMomDev* mom,
-                                                   double beta_x, double beta_y,
-                                                   const double* z0) {
+// After the warp's partial is stored: whether this warp is the last of the
+// bunch's n_parts warps to arrive (it then merges them).
+__device__ __forceinline__ bool warp_moment_arrive(int b, int n_parts, unsigned* counters) {
   __threadfence();
   __syncwarp();
   unsigned prev = 0;
   if ((threadIdx.x & 31) == 0) prev = atomicAdd(&counters[b], 1u);
   prev = __shfl_sync(FULL_MASK, prev, 0);
-  if (prev != (unsigned)(n_parts - 1)) return;
+  return prev == (unsigned)(n_parts - 1);
+}
+
+__device__ __forceinline__ void warp_moment_finish(int b, int part_off, int n_parts,
+                                                   const MomPartial* partials,
+                                                   unsigned* counters, BunchMomDev* mom,
+                                                   double beta_x, double beta_y,
+                                                   const double* z0) {
+  if (!warp_moment_arrive(b, n_parts, counters)) return;
   __threadfence();
   merge_partials_warp(b, part_off, n_parts, partials, counters, mom, beta_x, beta_y, z0);
 }
@@ -625,7 +629,7 @@ void kick_variant_shape(int v, int* threads, int* min_ctas) {
 template <bool MOM, bool KICK>
 __global__ void __launch_bounds__(kTile, 2) k_map_pass(double* __restrict__ c, int64_t npad,
                                                     const uint8_t* __restrict__ surv,
-                                                    const int* __restrict__ chunk_bunch,
+                                                    const int4* __restrict__ chunk_loc,
                                                     const BunchDev* __restrict__ bunch,
                                                     const __grid_constant__ SectionDev sec,
                                                     const __grid_constant__ RingDev r,
@@ -635,25 +639,26 @@ __global__ void __launch_bounds__(kTile, 2) k_map_pass(double* __restrict__ c, i
                                                     int chunk_base) {
   __shared__ FieldPrep s_prep[CG_MAX_SPECIES];
   const int chunk = chunk_base + (int)blockIdx.x;
-  const int b = chunk_bunch[chunk];
-  const BunchDev B = bunch[b];
-  const CloudRec* rb = rec + (size_t)b * P;
-  if (KICK) {
-    if ((int)threadIdx.x < P)
-      s_prep[threadIdx.x] = field_prep(rb[threadIdx.x].rms_x, rb[threadIdx.x].rms_y);
-    __syncthreads();
-  }
-  const int tile0 = B.tile_off + (chunk - B.chunk_off) * kMomChunkTiles;
-  const int i0 = (tile0 - B.tile_off) * kTile + threadIdx.x;
+  // the chunk's place from one table load (x bunch, y first tile, z chunk of
+  // the bunch, w valid slots), so the coordinate loads wait for one round
+  // trip, not two
+  const int4 l = chunk_loc[chunk];
+  const int b = l.x, tile0 = l.y;
   double v[kMomChunkTiles][6];
   bool alive[kMomChunkTiles];
 #pragma unroll
   for (int u = 0; u < kMomChunkTiles; ++u) {
     const int64_t g = (int64_t)(tile0 + u) * kTile + threadIdx.x;
-    const bool valid = i0 + u * kTile < B.n;
+    const bool valid = u * kTile + (int)threadIdx.x < l.w;
     alive[u] = valid && surv[g] == kAlive;
 #pragma unroll
     for (int d = 0; d < 6; ++d) v[u][d] = valid ? c[d * npad + g] : 0.0;
+  }
+  const CloudRec* rb = rec + (size_t)b * P;
+  if (KICK) {
+    if ((int)threadIdx.x < P)
+      s_prep[threadIdx.x] = field_prep(rb[threadIdx.x].rms_x, rb[threadIdx.x].rms_y);
+    __syncthreads();
   }
 #pragma unroll
   for (int u = 0; u < kMomChunkTiles; ++u) {
@@ -668,6 +673,7 @@ __global__ void __launch_bounds__(kTile, 2) k_map_pass(double* __restrict__ c, i
     store6(c, npad, (int64_t)(tile0 + u) * kTile + threadIdx.x, v[u]);
   }
   if (MOM) {
+    const BunchDev& B = bunch[b];
     const int warp = threadIdx.x >> 5;
     warp_moment_partial(v, alive, &partials[(size_t)chunk * kWarpsPerChunk + warp]);
     warp_moment_finish(b, B.chunk_off * kWarpsPerChunk, B.n_chunks * kWarpsPerChunk, partials,
@@ -686,33 +692,35 @@ cudaError_t launch_map_pass(Handle& h, int k, int mom_section, bool kick, int ch
   if (chunk_b <= chunk_a) return cudaSuccess;
   auto kern = m ? (kick ? k_map_pass<true, true> : k_map_pass<true, false>)
                 : (kick ? k_map_pass<false, true> : k_map_pass<false, false>);
-  kern<<<chunk_b - chunk_a, kTile, 0, s>>>(h.d.c, h.npad, h.d.surv, h.d.chunk_bunch, h.d.bunch,
+  kern<<<chunk_b - chunk_a, kTile, 0, s>>>(h.d.c, h.npad, h.d.surv, h.d.chunk_loc, h.d.bunch,
                                            h.sec_dev_host[k], h.ring, h.d.wpartials,
                                            h.d.counters, h.d.mom, bx, by, rec, h.P, chunk_a);
   return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
-// The map pass with the next chunk in flight.  k_map_pass issues a chunk's
-// loads, then maps, stores and reduces with nothing in flight, so at its two
-// CTAs per SM (128 registers) DRAM idles while a CTA computes.  Here a
-// persistent grid of two CTAs per SM walks the chunks [chunk_a, chunk_b) with
-// stride gridDim.x, and before it works on the current chunk every thread
-// copies its own slots of the CTA's next chunk into shared memory with
-// cp.async (8 bytes per coordinate).  A thread reads back only what it
-// copied, so cp.async.wait_group orders everything and no CTA barrier is
-// needed.  The chunk's place (bunch, first tile, tiles, valid slots) comes
-// from a per-chunk table, one load with no dependent lookup.  The arithmetic
-// and the reductions are those of k_map_pass (with the kick, the records'
-// precomputed field constants, as k_ion_kick reads them), so the results are
-// bitwise the same.
+// The map pass with the chunk staged in shared memory.  k_map_pass holds the
+// 24 coordinates of its four particles per thread in registers while their
+// loads are in flight, which needs 128 registers and so allows two CTAs per
+// SM: at most two chunks per SM are loading at any time.  Here every thread
+// copies its slots of the chunk into shared memory with cp.async (8 bytes per
+// coordinate, the aligned 4-byte word holding each survival byte), waits for
+// its own copies (a thread reads back only what it copied, so no CTA barrier
+// is needed) and then maps one particle at a time, writing the mapped
+// particle back to its slots for the second pass of the moments.  The
+// registers of one particle instead of four let more CTAs, and so more
+// chunks in flight, share an SM.  The chunk's place (bunch, first tile,
+// tiles, valid slots) comes from a per-chunk table, one load with no
+// dependent lookup.  The arithmetic and the reductions are those of
+// k_map_pass (with the kick, the records' precomputed field constants, as
+// k_ion_kick reads them), so the results are bitwise the same.
 
-constexpr int kAsyncStages = 2;
-struct AsyncStage {
+struct ChunkStage {
   double v[kMomChunkTiles][6][kTile];  // [tile of the chunk][coordinate][thread]
   uint32_t sw[kMomChunkTiles][kTile];  // the 4-byte word holding each slot's survival byte
 };
-constexpr size_t kAsyncSmem = kAsyncStages * sizeof(AsyncStage);
+constexpr size_t kStageSmem = sizeof(ChunkStage);
+constexpr int kStagedCtasPerSm = 2;
 
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
   const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
@@ -722,124 +730,86 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
   const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
 }
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
-}
-// every group but the most recent one complete
-__device__ __forceinline__ void cp_async_wait_prior() {
-  asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
 template <bool MOM, bool KICK>
-__global__ void __launch_bounds__(kTile, 2) k_map_async(double* __restrict__ c, int64_t npad,
-                                                     const uint8_t* __restrict__ surv,
-                                                     const int4* __restrict__ chunk_loc,
-                                                     const BunchDev* __restrict__ bunch,
-                                                     const __grid_constant__ SectionDev sec,
-                                                     const __grid_constant__ RingDev r,
-                                                     MomPartial* partials, unsigned* counters,
-                                                     BunchMomDev* mom, double beta_x,
-                                                     double beta_y,
-                                                     const CloudRec* __restrict__ rec,
-                                                     const FieldPrep* __restrict__ rec_prep,
-                                                     int P, int chunk_a, int chunk_b) {
+__global__ void __launch_bounds__(kTile, kStagedCtasPerSm)
+    k_map_staged(double* __restrict__ c, int64_t npad, const uint8_t* __restrict__ surv,
+                 const int4* __restrict__ chunk_loc, const BunchDev* __restrict__ bunch,
+                 const __grid_constant__ SectionDev sec, const __grid_constant__ RingDev r,
+                 MomPartial* partials, unsigned* counters, BunchMomDev* mom, double beta_x,
+                 double beta_y, const CloudRec* __restrict__ rec,
+                 const FieldPrep* __restrict__ rec_prep, int P, int chunk_base) {
   extern __shared__ __align__(128) unsigned char dyn_smem[];
-  AsyncStage* stage = reinterpret_cast<AsyncStage*>(dyn_smem);
-  const int tid = threadIdx.x, G = (int)gridDim.x;
-  int chunk = chunk_a + (int)blockIdx.x;
-  if (chunk >= chunk_b) return;
-  // this thread's slots of the chunk at l (x bunch, y first tile, z tiles)
-  // into stage st: six coordinates and the aligned word holding the survival
-  // byte (the surv rows start 256-byte aligned)
-  auto issue = [&](const int4& l, int st) {
+  ChunkStage& sb = *reinterpret_cast<ChunkStage*>(dyn_smem);
+  const int tid = threadIdx.x;
+  const int chunk = chunk_base + (int)blockIdx.x;
+  const int4 l = chunk_loc[chunk];  // x bunch, y first tile, z chunk of the bunch, w valid slots
 #pragma unroll
-    for (int u = 0; u < kMomChunkTiles; ++u) {
-      if (u < l.z) {
-        const int64_t g = (int64_t)(l.y + u) * kTile + tid;
+  for (int u = 0; u < kMomChunkTiles; ++u) {
+    if (u * kTile < l.w) {  // a tile of this bunch
+      const int64_t g = (int64_t)(l.y + u) * kTile + tid;
 #pragma unroll
-        for (int d = 0; d < 6; ++d) cp_async8(&stage[st].v[u][d][tid], c + d * npad + g);
-        cp_async4(&stage[st].sw[u][tid], surv + (g & ~(int64_t)3));
-      }
+      for (int d = 0; d < 6; ++d) cp_async8(&sb.v[u][d][tid], c + d * npad + g);
+      cp_async4(&sb.sw[u][tid], surv + (g & ~(int64_t)3));  // surv rows are 256-byte aligned
     }
-  };
+  }
+  cp_async_wait_all();
   const int byte = 8 * (tid & 3);
-  int4 cur = chunk_loc[chunk];
-  issue(cur, 0);
-  cp_async_commit();
-  int4 nxt = chunk + G < chunk_b ? chunk_loc[chunk + G] : make_int4(0, 0, 0, 0);
-  for (int st = 0;; st ^= 1) {
-    const int cn = chunk + G;
-    if (cn < chunk_b) issue(nxt, st ^ 1);
-    cp_async_commit();  // (empty when there is no next chunk)
-    const int4 nn = cn + G < chunk_b ? chunk_loc[cn + G] : make_int4(0, 0, 0, 0);
-    cp_async_wait_prior();  // this chunk's copies have landed
-    AsyncStage& sb = stage[st];
-    // one tile at a time, not unrolled (the registers of one particle, not
-    // of four); the mapped particle goes back to this thread's slots of the
-    // stage for the second pass of the moments
-    uint32_t alive = 0;
-    double s[7] = {0, 0, 0, 0, 0, 0, 0};
-    double mn = INFINITY, mx = -INFINITY;
+  uint32_t alive = 0;
+  double s[7] = {0, 0, 0, 0, 0, 0, 0};
+  double mn = INFINITY, mx = -INFINITY;
 #pragma unroll 1
-    for (int u = 0; u < kMomChunkTiles; ++u) {
-      const bool valid = u * kTile + tid < cur.w;
-      if (!(valid && ((sb.sw[u][tid] >> byte) & 0xFFu) == kAlive)) continue;
-      alive |= 1u << u;
-      double v[6];
+  for (int u = 0; u < kMomChunkTiles; ++u) {
+    const bool valid = u * kTile + tid < l.w;
+    if (!(valid && ((sb.sw[u][tid] >> byte) & 0xFFu) == kAlive)) continue;
+    alive |= 1u << u;
+    double v[6];
 #pragma unroll
-      for (int d = 0; d < 6; ++d) v[d] = sb.v[u][d][tid];
-      if (KICK) {
-        double dpx, dpy;
-        ion_kick_particle_prep(rec + (size_t)cur.x * P, rec_prep + (size_t)cur.x * P, P, v[0],
-                               v[2], &dpx, &dpy);
-        v[1] += dpx;
-        v[3] += dpy;
-      }
-      section_map_particle(sec, r, v);
-      store6(c, npad, (int64_t)(cur.y + u) * kTile + tid, v);
-      if (MOM) {
-#pragma unroll
-        for (int d = 0; d < 6; ++d) sb.v[u][d][tid] = v[d];
-        chunk_sums_add(v, s, mn, mx);
-      }
+    for (int d = 0; d < 6; ++d) v[d] = sb.v[u][d][tid];
+    if (KICK) {
+      double dpx, dpy;
+      ion_kick_particle_prep(rec + (size_t)l.x * P, rec_prep + (size_t)l.x * P, P, v[0], v[2],
+                             &dpx, &dpy);
+      v[1] += dpx;
+      v[3] += dpy;
     }
+    section_map_particle(sec, r, v);
+    store6(c, npad, (int64_t)(l.y + u) * kTile + tid, v);
     if (MOM) {
-      const int warp = tid >> 5;
-      warp_moment_reduce<1>(s, mn, mx, [&](int u) { return ((alive >> u) & 1u) != 0; },
-                            [&](int u, int d) { return sb.v[u][d][tid]; },
-                            &partials[(size_t)chunk * kWarpsPerChunk + warp]);
-      const BunchDev& B = bunch[cur.x];
-      warp_moment_finish(cur.x, B.chunk_off * kWarpsPerChunk, B.n_chunks * kWarpsPerChunk,
-                         partials, counters, mom, beta_x, beta_y,
-                         c + 4 * npad + (int64_t)B.tile_off * kTile);
+#pragma unroll
+      for (int d = 0; d < 6; ++d) sb.v[u][d][tid] = v[d];
+      chunk_sums_add(v, s, mn, mx);
     }
-    if (cn >= chunk_b) break;
-    chunk = cn;
-    cur = nxt;
-    nxt = nn;
+  }
+  if (MOM) {
+    const int warp = tid >> 5;
+    warp_moment_reduce<1>(s, mn, mx, [&](int u) { return ((alive >> u) & 1u) != 0; },
+                          [&](int u, int d) { return sb.v[u][d][tid]; },
+                          &partials[(size_t)chunk * kWarpsPerChunk + warp]);
+    const BunchDev& B = bunch[l.x];
+    warp_moment_finish(l.x, B.chunk_off * kWarpsPerChunk, B.n_chunks * kWarpsPerChunk, partials,
+                       counters, mom, beta_x, beta_y, c + 4 * npad + (int64_t)B.tile_off * kTile);
   }
 }
 
-static int device_sms() {
-  int dev = 0, sms = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  return sms < 1 ? 1 : sms;
-}
-
-// Per device, once: the dynamic shared memory the asynchronous map pass asks
-// for (above the 48 KB default), and the largest shared-memory carveout, so
-// that two of its CTAs fit on an SM.
+// Per device, once: the dynamic shared memory the staged map pass asks for
+// (above the 48 KB default) and a shared-memory carveout that holds
+// kStagedCtasPerSm of its CTAs.
 cudaError_t prepare_map_async() {
-  const void* kerns[] = {(const void*)k_map_async<true, false>, (const void*)k_map_async<true, true>,
-                         (const void*)k_map_async<false, false>,
-                         (const void*)k_map_async<false, true>};
+  const void* kerns[] = {(const void*)k_map_staged<true, false>,
+                         (const void*)k_map_staged<true, true>,
+                         (const void*)k_map_staged<false, false>,
+                         (const void*)k_map_staged<false, true>};
+  const int carve = (int)std::min<size_t>(
+      100, (kStagedCtasPerSm * (kStageSmem + 1024) * 100 + 228 * 1024 - 1) / (228 * 1024));
   for (const void* f : kerns) {
     cudaError_t e =
-        cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAsyncSmem);
+        cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageSmem);
     if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout,
-                               (int)cudaSharedmemCarveoutMaxShared);
+      e = cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
@@ -853,8 +823,6 @@ cudaError_t launch_map_turn(Handle& h, int k, int mom_section, bool kick, int ch
 
 cudaError_t launch_map_async(Handle& h, int k, int mom_section, bool kick, int chunk_a,
                              int chunk_b, cudaStream_t s) {
-  static int sms = 0;
-  if (!sms) sms = device_sms();
   const bool m = mom_section >= 0;
   const double bx = m ? h.sec_dev_host[mom_section].beta_x : 0.0;
   const double by = m ? h.sec_dev_host[mom_section].beta_y : 0.0;
@@ -863,12 +831,11 @@ cudaError_t launch_map_async(Handle& h, int k, int mom_section, bool kick, int c
   if (chunk_b < 0) chunk_b = h.n_chunks;
   if (!s) s = h.stream;
   if (chunk_b <= chunk_a) return cudaSuccess;
-  const int grid = std::min(chunk_b - chunk_a, 2 * sms);
-  auto kern = m ? (kick ? k_map_async<true, true> : k_map_async<true, false>)
-                : (kick ? k_map_async<false, true> : k_map_async<false, false>);
-  kern<<<grid, kTile, kAsyncSmem, s>>>(h.d.c, h.npad, h.d.surv, h.d.chunk_loc, h.d.bunch,
-                                       h.sec_dev_host[k], h.ring, h.d.wpartials, h.d.counters,
-                                       h.d.mom, bx, by, rec, rp, h.P, chunk_a, chunk_b);
+  auto kern = m ? (kick ? k_map_staged<true, true> : k_map_staged<true, false>)
+                : (kick ? k_map_staged<false, true> : k_map_staged<false, false>);
+  kern<<<chunk_b - chunk_a, kTile, kStageSmem, s>>>(
+      h.d.c, h.npad, h.d.surv, h.d.chunk_loc, h.d.bunch, h.sec_dev_host[k], h.ring,
+      h.d.wpartials, h.d.counters, h.d.mom, bx, by, rec, rp, h.P, chunk_a);
   return cudaGetLastError();
 }
 
@@ -886,12 +853,21 @@ __global__ void __launch_bounds__(kTile) k_long(double* __restrict__ c, int64_t 
                                                 const __grid_constant__ RingDev r,
                                                 unsigned flags, uint64_t seed,
                                                 const int* __restrict__ d_turn,
-                                                const double* __restrict__ lr_force) {
+                                                const double* __restrict__ lr_force,
+                                                const double* __restrict__ rf_zr,
+                                                const double* __restrict__ rf_kick,
+                                                const double* __restrict__ rf_fbk, int M) {
   TileIdx t = tile_index(tile_bunch, bunch);
   if (!t.valid) return;
   double v[6];
   load6(c, npad, t.g, v);
-  if (flags & kLongRF) v[5] = rf_kick_dp(r, v[4], v[5]);
+  if (flags & kLongRF) {
+    if (r.bl_any)
+      v[5] = rf_kick_dp_loading(r, v[4], v[5], surv[t.g] == kAlive, t.b, M, rf_zr, rf_kick,
+                                rf_fbk);
+    else
+      v[5] = rf_kick_dp(r, v[4], v[5]);
+  }
   if (flags & kLongDrift) v[4] = drift_z(r, v[4], v[5]);
   if (flags & kLongLoss) v[5] -= r.u0_term;
   if ((flags & kLongSynrad) && surv[t.g] == kAlive) {
@@ -909,9 +885,14 @@ __global__ void __launch_bounds__(kTile) k_long(double* __restrict__ c, int64_t 
 }
 
 cudaError_t launch_long(Handle& h, unsigned flags) {
+  if ((flags & kLongRF) && h.ring.bl_any) {
+    // the cavities' recurrence over the train first: the kicks of each bin
+    cudaError_t e = launch_rf_beam_loading(h);
+    if (e != cudaSuccess) return e;
+  }
   k_long<<<h.n_tiles, kTile, 0, h.stream>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch, h.d.bunch,
                                             h.sec_dev_host[0], h.ring, flags, h.cfg.seed, h.d.turn,
-                                            h.d.lr_force);
+                                            h.d.lr_force, h.d.rf_zr, h.d.rf_kick, h.d.rf_fbk, h.M);
   return cudaGetLastError();
 }
 

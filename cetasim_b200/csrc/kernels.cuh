@@ -25,6 +25,8 @@ cudaError_t launch_ion_records(Handle& h, int k, int ja, int jb, cudaStream_t s)
 cudaError_t launch_ion_compact(Handle& h, int k, cudaStream_t s);
 // walk CTAs for `tcap` trajectory slots at `ions` trajectories per CTA
 int ion_walk_grid(int64_t tcap, int ions);
+// per device, once: the shared-memory reservation of each walk shape
+cudaError_t prepare_ion_walk();
 cudaError_t launch_ion_kick(Handle& h, int k);
 // the kick of the tiles [tile_a, tile_b) (tile_b < 0: all) on stream s (null: h.stream)
 cudaError_t launch_ion_kick_variant(Handle& h, int k, int v, int tile_a = 0, int tile_b = -1,
@@ -54,6 +56,13 @@ enum LongFlags : unsigned {
   kLongLR = 16,
 };
 cudaError_t launch_long(Handle& h, unsigned flags);
+// cavities with beam loading: z ranges and bins of the RF step, then the
+// cavities' recurrence over the train (beam_loading.cu); k_long applies the
+// kicks
+cudaError_t launch_rf_beam_loading(Handle& h);
+size_t rf_work_doubles(int n_bl, int M, int nb);
+void resonator_init(const cg_config& cfg, const std::vector<int>& harm,
+                    const std::vector<double>& ne, double* state, double* info);
 cudaError_t launch_lr_compute(Handle& h);
 cudaError_t launch_lr_kick(Handle& h);
 cudaError_t launch_fir_compute(Handle& h);

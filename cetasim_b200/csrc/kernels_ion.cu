@@ -498,15 +498,44 @@ cudaError_t launch_ion_prep(Handle& h, int k) {
   return cudaGetLastError();
 }
 
+// Shared memory a walk CTA of each shape asks for beyond its static arrays
+// when its SM is reserved: together with the static arrays and the 1 KB the
+// driver keeps per CTA, the whole 228 KB of the SM, so that no kick or map
+// CTA is scheduled beside the walk (their warps would take issue slots and
+// FP64 pipe cycles from the walk's latency-bound chain).  Set per device by
+// prepare_ion_walk; index 0..3 = 8, 16, 32, 64 ions per CTA.
+static int g_walk_reserve_dyn[4] = {0, 0, 0, 0};
+
+template <int IONS>
+static cudaError_t prepare_walk_shape(int slot) {
+  cudaFuncAttributes a;
+  cudaError_t e = cudaFuncGetAttributes(&a, k_ion_walk<IONS>);
+  if (e != cudaSuccess) return e;
+  const int dyn = 227 * 1024 - (int)a.sharedSizeBytes;
+  e = cudaFuncSetAttribute(k_ion_walk<IONS>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+  if (e == cudaSuccess) g_walk_reserve_dyn[slot] = dyn;
+  return e;
+}
+
+cudaError_t prepare_ion_walk() {
+  cudaError_t e = prepare_walk_shape<8>(0);
+  if (e == cudaSuccess) e = prepare_walk_shape<16>(1);
+  if (e == cudaSuccess) e = prepare_walk_shape<32>(2);
+  if (e == cudaSuccess) e = prepare_walk_shape<64>(3);
+  return e;
+}
+
 cudaError_t launch_ion_walk(Handle& h, int k, int ja, int jb, cudaStream_t s) {
   const int ions = h.walk_ions;
   const dim3 grid(ion_walk_grid(h.d.iw.tcap, ions), h.P);
   const CloudDev* cl = h.d.clouds + (size_t)k * h.P;
   const CloudState* cs = h.d.cloud_state + (size_t)k * h.P;
-  if (ions == 8) k_ion_walk<8><<<grid, 32, 0, s>>>(h.chain, h.d.iw, cl, cs, ja, jb);
-  else if (ions == 16) k_ion_walk<16><<<grid, 64, 0, s>>>(h.chain, h.d.iw, cl, cs, ja, jb);
-  else if (ions == 32) k_ion_walk<32><<<grid, 128, 0, s>>>(h.chain, h.d.iw, cl, cs, ja, jb);
-  else k_ion_walk<64><<<grid, 256, 0, s>>>(h.chain, h.d.iw, cl, cs, ja, jb);
+  const int slot = ions == 8 ? 0 : ions == 16 ? 1 : ions == 32 ? 2 : 3;
+  const size_t dyn = h.walk_reserve ? (size_t)g_walk_reserve_dyn[slot] : 0;
+  if (ions == 8) k_ion_walk<8><<<grid, 32, dyn, s>>>(h.chain, h.d.iw, cl, cs, ja, jb);
+  else if (ions == 16) k_ion_walk<16><<<grid, 64, dyn, s>>>(h.chain, h.d.iw, cl, cs, ja, jb);
+  else if (ions == 32) k_ion_walk<32><<<grid, 128, dyn, s>>>(h.chain, h.d.iw, cl, cs, ja, jb);
+  else k_ion_walk<64><<<grid, 256, dyn, s>>>(h.chain, h.d.iw, cl, cs, ja, jb);
   return cudaGetLastError();
 }
 
@@ -534,7 +563,8 @@ cudaError_t launch_ion_chain(Handle& h, int k) {
 }
 
 cudaError_t upload_weideman_table_ion() {
-  return cudaMemcpyToSymbol(c_weideman, &h_weideman, sizeof(WeidemanTable));
+  cudaError_t e = cudaMemcpyToSymbol(c_weideman, &h_weideman, sizeof(WeidemanTable));
+  return e != cudaSuccess ? e : prepare_ion_walk();
 }
 
 // Latency floor of the walk: one quad of lanes advances one ion through a

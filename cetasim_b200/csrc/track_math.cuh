@@ -33,6 +33,11 @@ struct RingDev {
   double rf_theta_coeff[4];          // 2 pi h_c f_RF / (c beta), Bunch.cpp:468
   double vreq_re[4], vreq_im[4];
   int n_cav;
+  // cavities with beam loading: per cavity its index among them (-1: an
+  // ideal cavity) and whether its direct feedback kicks; the bins per bunch
+  int bl_index[4];
+  int bl_fb[4];
+  int bl_any, rf_bins;
   double lambda[3], qe_coeff[3];     // synrad (Bunch.cpp:973-980)
   double z_loss;                     // t0 c / h / 2 (Bunch.cpp:181)
   double r_gamma;
@@ -146,6 +151,39 @@ CG_HD void section_map_particle(const SectionDev& s, const RingDev& r, double v[
 }
 
 // Bunch::BunchMomentumUpdateDueToRFCA (Bunch.cpp:466-472), every particle.
+// The RF step with cavities that load (MPBeam.cpp:2621-2704): per cavity in
+// order, the ideal cavity's kick or, for an alive particle, the two
+// increments of its bin from the recurrence's table (kick[((b M + j) nb +
+// bin) 2 ..]); then the direct-feedback kicks of the bunch, to every
+// particle.
+CG_HD double rf_kick_dp_loading(const RingDev& r, double z, double dp, bool alive, int j, int M,
+                                const double* zr, const double* kick, const double* fbk) {
+  int bin = -1;
+  if (alive) {
+    const double zmin = zr[2 * j], zmax = zr[2 * j + 1];
+    const double dz = (zmax - zmin) / r.rf_bins;
+    bin = (int)floor((zmax - z) / dz);
+    bin = bin < 0 ? 0 : (bin >= r.rf_bins ? r.rf_bins - 1 : bin);
+  }
+  for (int c = 0; c < r.n_cav; ++c) {
+    const int b = r.bl_index[c];
+    if (b < 0) {
+      double th = z * r.rf_theta_coeff[c];
+      double s, co;
+      sincos(th, &s, &co);
+      double re = fma(r.vreq_re[c], co, r.vreq_im[c] * s);
+      dp += re / r.energy / r.r_beta2;
+    } else if (bin >= 0) {
+      const double* k = kick + (((size_t)b * M + j) * r.rf_bins + bin) * 2;
+      dp += k[0];
+      dp += k[1];
+    }
+  }
+  for (int c = 0; c < r.n_cav; ++c)
+    if (r.bl_index[c] >= 0 && r.bl_fb[c]) dp += fbk[(size_t)r.bl_index[c] * M + j];
+  return dp;
+}
+
 CG_HD double rf_kick_dp(const RingDev& r, double z, double dp) {
   for (int c = 0; c < r.n_cav; ++c) {
     double th = z * r.rf_theta_coeff[c];

@@ -20,9 +20,10 @@
 // (transmission < 0.5 at Bunch.cpp:194-197, ion overflow at LIP.cpp:1043-1048).
 //
 // Not built here (paths outside the library's scope, kept as the reference's
-// declarations only): beam loading (rfMode = 1), broadband impedance, space
-// charge, ramping, drive mode, the per-bunch TBT and ion-dump writers
-// (MPBeamDataPrintPerTurn, SSIonDataPrint) and the Haissinski solver.
+// declarations only): broadband impedance, space charge, ramping, drive
+// mode, the per-bunch TBT and ion-dump writers (MPBeamDataPrintPerTurn,
+// SSIonDataPrint), the cavity transient printout of InitialcavityResonator
+// and the Haissinski solver.
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -137,15 +138,28 @@ void build_config(GpuBeam& g, const ReadInputSettings& in, const LatticeInterAct
     std::cerr << "rfResNum must be in [1, " << CG_MAX_CAVITIES << "]" << std::endl;
     exit(0);
   }
+  const auto* rf = in.ringParRf;
+  bool loading = false;
   for (int i = 0; i < r.n_cav; ++i) {
-    if (in.ringParRf->rfMode[i] != 0) {
-      std::cerr << "rfMode 1 (beam loading) is outside the GPU tracking path" << std::endl;
-      exit(0);
-    }
-    r.cav_harm[i] = in.ringParRf->resHarm[i];
-    r.cav_vol[i] = in.ringParRf->resVol[i];
-    r.cav_phase[i] = in.ringParRf->resPhase[i];
+    r.cav_harm[i] = rf->resHarm[i];
+    r.cav_vol[i] = rf->resVol[i];
+    r.cav_phase[i] = rf->resPhase[i];
+    // the resonator of a cavity with beam loading (CavityResonator.cpp:64-87)
+    r.rf_mode[i] = rf->rfMode[i];
+    r.res_type[i] = rf->resType[i];
+    r.res_cold[i] = rf->resCold[i];
+    r.res_excite[i] = (int)rf->resExciteIntability[i];
+    r.res_dir_fb[i] = (int)rf->resDirFB[i];
+    r.res_rs[i] = rf->resShuntImpRs[i];
+    r.res_q0[i] = rf->resQualityQ0[i];
+    r.res_coupling[i] = rf->resCouplingBeta[i];
+    r.res_detune[i] = rf->resDetuneFre[i];
+    r.res_dir_fb_gain[i] = rf->resDirFBGain[i];
+    r.res_dir_fb_phase[i] = rf->resDirFBPhase[i];
+    r.res_dir_fb_delay[i] = rf->resDirFBDelay[i];
+    loading = loading || r.rf_mode[i] == 1;
   }
+  if (loading) r.rf_bunch_bins = rf->rfBunchBinNum;
   check(g, cg_config_derive(&c), "cg_config_derive");
   const int K = in.ringParBasic->ringSectNum;
   g.secs.assign(K, cg_section());
@@ -390,15 +404,25 @@ void MPBeam::Initial(Train& train, LatticeInterActionPoint& latticeInterActionPo
   }
 }
 
-// Only the ideal cavity (rfMode = 0, RFCA) is on the GPU path; its kick needs
-// no transient pre-run.
+// The library set the cavities' state in cg_set_beam (Initial) as the
+// reference's InitialcavityResonator does: the steady-state beam-induced
+// voltage of the fill pattern, the generator voltage and current.  Here the
+// host resonators receive that state and their power figures (the
+// reference's own Resonator::GetInitialResonatorPower); the transient
+// printout of the reference's function (transResonParWriteTo) is not
+// written.
 void MPBeam::InitialcavityResonator(ReadInputSettings& inputParameter, CavityResonator& cavityResonator) {
-  for (int j = 0; j < inputParameter.ringParRf->resNum; ++j)
-    if (inputParameter.ringParRf->rfMode[j] != 0) {
-      std::cerr << "rfMode 1 (beam loading) is outside the GPU tracking path" << std::endl;
-      exit(0);
-    }
-  (void)cavityResonator;
+  GpuBeam& g = gpu(this);
+  for (int i = 0; i < inputParameter.ringParRf->resNum; ++i) {
+    if (inputParameter.ringParRf->rfMode[i] != 1) continue;
+    double st[6];
+    check(g, cg_resonator_state(g.h, i, st), "cg_resonator_state");
+    Resonator& R = cavityResonator.resonatorVec[i];
+    R.vbAccum = std::complex<double>(st[0], st[1]);
+    R.resGenVol = std::complex<double>(st[2], st[3]);
+    R.resGenIg = std::complex<double>(st[4], st[5]);
+    R.GetInitialResonatorPower(inputParameter);
+  }
 }
 
 void MPBeam::MPBeamRMSCal(LatticeInterActionPoint& latticeInterActionPoint, int k) {

@@ -129,23 +129,36 @@ def write_case(d: str, wl: Workload, n_turns: int = 1, print_interval: int | Non
         "ringTwiss = twiss.dat",
         f"ringSectNum = {K}",
         f"rfRingHarm = {int(r.harmonics)}", f"rfResNum = {n_cav}",
-        "rfMode = " + cav([0] * n_cav),
         "rfResHarm = " + " ".join(str(int(r.cav_harm[i])) for i in range(n_cav)),
-        "rfResType = " + cav([1] * n_cav),
         "rfResVol = " + cav(r.cav_vol[i] for i in range(n_cav)),
         "rfResPhase = " + cav(r.cav_phase[i] for i in range(n_cav)),
-        "rfResShuntImpRs = " + cav([0.0] * n_cav),
-        "rfResQualityQ0 = " + cav([1.0] * n_cav),
-        "rfResCouplingBeta = " + cav([0.0] * n_cav),
-        "rfResDetuneFre = " + cav([0.0] * n_cav),
-        "rfResCold = " + cav([0] * n_cav),
-        "rfResExciteIntability = " + cav([0] * n_cav),
-        "rfResDirFB = " + cav([0] * n_cav),
-        "rfResDirFBGain = " + cav([0.0] * n_cav),
-        "rfResDirFBPhaseShift = " + cav([0.0] * n_cav),
-        "rfResDirFBDelay = " + cav([0.0] * n_cav),
-        "rfBunchBinNum = 32",
     ]
+    if any(int(r.rf_mode[i]) == 1 for i in range(n_cav)):
+        # cavities with beam loading: their resonator parameters as given
+        ints = lambda f: " ".join(str(int(getattr(r, f)[i])) for i in range(n_cav))
+        reals = lambda f: cav(getattr(r, f)[i] for i in range(n_cav))
+        lines += [
+            "rfMode = " + ints("rf_mode"), "rfResType = " + ints("res_type"),
+            "rfResShuntImpRs = " + reals("res_rs"), "rfResQualityQ0 = " + reals("res_q0"),
+            "rfResCouplingBeta = " + reals("res_coupling"), "rfResDetuneFre = " + reals("res_detune"),
+            "rfResCold = " + ints("res_cold"), "rfResExciteIntability = " + ints("res_excite"),
+            "rfResDirFB = " + ints("res_dir_fb"), "rfResDirFBGain = " + reals("res_dir_fb_gain"),
+            "rfResDirFBPhaseShift = " + reals("res_dir_fb_phase"),
+            "rfResDirFBDelay = " + reals("res_dir_fb_delay"),
+            f"rfBunchBinNum = {int(r.rf_bunch_bins)}",
+        ]
+    else:
+        # ideal cavities: the resonator parameters are not read by the
+        # tracking; placeholders that keep the reference's set-up finite
+        lines += [
+            "rfMode = " + cav([0] * n_cav), "rfResType = " + cav([1] * n_cav),
+            "rfResShuntImpRs = " + cav([0.0] * n_cav), "rfResQualityQ0 = " + cav([1.0] * n_cav),
+            "rfResCouplingBeta = " + cav([0.0] * n_cav), "rfResDetuneFre = " + cav([0.0] * n_cav),
+            "rfResCold = " + cav([0] * n_cav), "rfResExciteIntability = " + cav([0] * n_cav),
+            "rfResDirFB = " + cav([0] * n_cav), "rfResDirFBGain = " + cav([0.0] * n_cav),
+            "rfResDirFBPhaseShift = " + cav([0.0] * n_cav), "rfResDirFBDelay = " + cav([0.0] * n_cav),
+            "rfBunchBinNum = 32",
+        ]
     if cfg.flag_lr_wake:
         lines.append(f"lrwNTurnsWakeTrunction = {int(cfg.lr_turns) - 1}")
         if cfg.lr_bbr.n:

@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define CG_ABI_VERSION 1
+#define CG_ABI_VERSION 2
 #define CG_MAX_SPECIES 8
 #define CG_MAX_CAVITIES 4
 #define CG_MAX_RESONATORS 16
@@ -68,7 +68,7 @@ typedef struct cg_ring {
   double u0;                   /* ringU0 [eV] */
   double skew_quad_k;          /* ringskewQuadK [1/m] */
   int harmonics;               /* rfRingHarm */
-  int n_cav;                   /* rfResNum (RFCA cavities; rfMode 0) */
+  int n_cav;                   /* rfResNum */
   int cav_harm[CG_MAX_CAVITIES];   /* rfResHarm */
   double cav_vol[CG_MAX_CAVITIES]; /* rfResVol [V] */
   double cav_phase[CG_MAX_CAVITIES]; /* rfResPhase [rad] (overridden for one cavity) */
@@ -77,6 +77,25 @@ typedef struct cg_ring {
   double natural_bunch_length, beta_z;
   double emit_nat[3];
   double cav_vreq_re[CG_MAX_CAVITIES], cav_vreq_im[CG_MAX_CAVITIES];
+  /* cavities with beam loading (CavityResonator::Initial,
+   * CavityResonator.cpp:36-176; ReadInputSettings.cpp:192-362) */
+  int rf_mode[CG_MAX_CAVITIES];        /* rfMode: 0 ideal cavity (RFCA), 1 beam loading */
+  int res_type[CG_MAX_CAVITIES];       /* rfResType: 0 passive, 1 active (generator) */
+  int res_cold[CG_MAX_CAVITIES];       /* rfResCold: starts without beam-induced voltage */
+  int res_excite[CG_MAX_CAVITIES];     /* rfResExciteIntability: 0 rigid bunch, 1 bin by bin */
+  int res_dir_fb[CG_MAX_CAVITIES];     /* rfResDirFB */
+  int rf_bunch_bins;                   /* rfBunchBinNum */
+  double res_rs[CG_MAX_CAVITIES];      /* rfResShuntImpRs [Ohm] */
+  double res_q0[CG_MAX_CAVITIES];      /* rfResQualityQ0 */
+  double res_coupling[CG_MAX_CAVITIES]; /* rfResCouplingBeta */
+  double res_detune[CG_MAX_CAVITIES];  /* rfResDetuneFre [Hz] */
+  double res_dir_fb_gain[CG_MAX_CAVITIES];  /* rfResDirFBGain */
+  double res_dir_fb_phase[CG_MAX_CAVITIES]; /* rfResDirFBPhaseShift [rad] */
+  double res_dir_fb_delay[CG_MAX_CAVITIES]; /* rfResDirFBDelay [s] */
+  /* derived (cg_config_derive): loaded Q, resonant frequency [Hz], detuning
+   * angle [rad], filling time [s] */
+  double res_ql[CG_MAX_CAVITIES], res_fre[CG_MAX_CAVITIES];
+  double res_psi[CG_MAX_CAVITIES], res_tf[CG_MAX_CAVITIES];
 } cg_ring;
 
 /* One lattice section / interaction point k (LatticeInterActionPoint.h:41-90;
@@ -216,8 +235,8 @@ int cg_lattice_init(const cg_ring* ring, cg_section* sections, int n_sections);
  * per-bunch macroparticle counts, harmonic numbers and electrons per bunch.
  * The arrays and cfg->sections are allocated by the library; release them
  * with cg_config_free.  Keys outside the MP tracking path are accepted and
- * ignored, except settings this library does not implement (rfMode 1,
- * runBBIFlag, runSpaceCharge, ionCalSCMethod 2, driveModeOn, runRamping),
+ * ignored, except settings this library does not implement (runBBIFlag,
+ * runSpaceCharge, ionCalSCMethod 2, driveModeOn, runRamping),
  * which return CG_ERR_UNSUPPORTED.  runCBMGR with runGrowthRateFittingStart /
  * End fills run_cbmgr and the fit window (checked as ReadInputSettings.cpp:
  * 946-956).  Optional keys beyond the reference: bunchMacroEleNumPerBunchList
@@ -281,6 +300,17 @@ int cg_section_map(cg_handle* h, int k);
 /* MPBeam::BeamMomtumUpdateDueToRFTest for RFCA cavities (MPBeam.cpp:2624-2706
  * -> Bunch::BunchMomentumUpdateDueToRFCA, Bunch.cpp:453-481). */
 int cg_rf_kick(cg_handle* h);
+/* Cavities with beam loading (rfMode 1).  cg_set_beam sets each cavity's
+ * state as MPBeam::InitialcavityResonator does (MPBeam.cpp:236-465): the
+ * steady-state beam-induced voltage of the fill pattern, the generator
+ * voltage and current (Resonator::GetInitialResonatorGenIg,
+ * Resonator.cpp:38-54); cg_rf_kick and the turn advance it bunch by bunch.
+ * out6 / in6 = (vbAccum, resGenVol, resGenIg) as (re, im) pairs. */
+int cg_resonator_state(cg_handle* h, int cavity, double* out6);
+int cg_set_resonator_state(cg_handle* h, int cavity, const double* in6);
+/* BunchRFModeInfo of bunch j and cavity c after the last RF step (Bunch.h:
+ * 109-118): cavity, generator, induced and self-loss voltages, (re, im). */
+int cg_rf_info(cg_handle* h, int j, int cavity, double* out8);
 /* MPBeam::BeamLongiPosTransferOneTurn (Bunch.cpp:494-501). */
 int cg_longi_drift(cg_handle* h);
 /* MPBeam::BeamEnergyLossOneTurn (Bunch.cpp:483-491). */
@@ -401,6 +431,11 @@ int cg_autotune(cg_handle* h, int k, int reps, int* choice, double* ms);
  * memory by cp.async while it works on the current one (the turn graph is
  * rebuilt).  Results are bitwise the same. */
 int cg_set_map_async(cg_handle* h, int on);
+/* 1: every walk CTA asks for its SM's whole shared memory, so that no other
+ * CTA (kick, map pass) runs on an SM while a walk CTA does; 0 (default):
+ * they share SMs.  Results are bitwise the same (the turn graph is
+ * rebuilt). */
+int cg_set_walk_reserve(cg_handle* h, int on);
 int cg_map_async(cg_handle* h, int* on);
 
 /* Pipelined turn: the ion walk of each IP runs in `groups` segments of

@@ -199,6 +199,23 @@ class OracleBeam:
         self._check(self.lib.or_ion_cloud_record(self.s, k, _p(out)))
         return out
 
+    def resonator(self, c):
+        """(vbAccum, resGenVol, resGenIg) of cavity c as complex numbers."""
+        out = np.empty(6)
+        self._check(self.lib.or_resonator_state(self.s, c, _p(out)))
+        return complex(out[0], out[1]), complex(out[2], out[3]), complex(out[4], out[5])
+
+    def set_resonator(self, c, vb, gen, ig):
+        a = np.array([vb.real, vb.imag, gen.real, gen.imag, ig.real, ig.imag])
+        self._check(self.lib.or_resonator_set(self.s, c, _p(a)))
+
+    def rf_info(self, j, c):
+        """BunchRFModeInfo of bunch j, cavity c: (cavity, generator, induced,
+        self-loss) voltages as complex numbers."""
+        out = np.empty(8)
+        self._check(self.lib.or_rf_info(self.s, j, c, _p(out)))
+        return tuple(complex(out[2 * i], out[2 * i + 1]) for i in range(4))
+
     def sr_bins(self, j):
         zlo, dz = C.c_double(), C.c_double()
         cnt = np.empty(int(self.wl.cfg.sr_bins), dtype=np.int32)

@@ -111,6 +111,15 @@ int or_config_derive(cg_config* cfg) {
     r->cav_vreq_re[i] = r->cav_vol[i] * cos(ph[i]);
     r->cav_vreq_im[i] = r->cav_vol[i] * sin(ph[i]);
   }
+  /* CavityResonator::Initial (CavityResonator.cpp:89-104) */
+  for (int i = 0; i < r->n_cav; ++i) {
+    double fh = (double)(r->cav_harm[i] * r->harmonics) * f0;
+    r->res_ql[i] = r->res_q0[i] / (1 + r->res_coupling[i]);
+    r->res_fre[i] = fh + r->res_detune[i];
+    double tan_psi = r->res_ql[i] * (r->res_fre[i] / fh - fh / r->res_fre[i]);
+    r->res_psi[i] = atan(tan_psi);
+    r->res_tf[i] = 2 * r->res_ql[i] / (2 * PI * r->res_fre[i]);
+  }
   return 0;
 }
 
@@ -217,10 +226,21 @@ struct or_state {
   /* FIR */
   double* fir_hist; /* [order][3][M] */
   double fir_limit;
+  /* cavities with beam loading (rfMode 1): Resonator::vbAccum, resGenVol,
+     resGenIg; per bunch the BunchRFModeInfo averages ([M][cav][8]: cavity,
+     generator, induced and self-loss voltages, re and im) and the
+     direct-feedback voltage sampled at the bunch's bucket ([cav][M][2]) */
+  double res_vb[CG_MAX_CAVITIES][2], res_gen[CG_MAX_CAVITIES][2], res_ig[CG_MAX_CAVITIES][2];
+  double* rf_info;
+  double* rf_fb;
+  double* rf_zmin; /* [M] zMinCurrentTurn, zMaxCurrentTurn of the RF step */
+  double* rf_zmax;
   char err[256];
 };
 
 const char* or_last_error(or_state* s) { return s->err; }
+
+static void res_init(or_state* s);
 
 /* WakeFunction::GetBBRWakeFun (WakeFunction.cpp:655-721) */
 static void bbr_wake(const cg_bbr* w, double beta_ip_x, double beta_ip_y, double tau, double out[3]) {
@@ -281,6 +301,11 @@ or_state* or_create(const cg_config* cfg, int M, const int* n_macro, const int* 
     c->fx = (double*)calloc(c->cap, sizeof(double)); c->fy = (double*)calloc(c->cap, sizeof(double));
   }
   s->rec = (double*)calloc((size_t)s->K * M * s->P * 6, sizeof(double));
+  s->rf_info = (double*)calloc((size_t)M * CG_MAX_CAVITIES * 8, sizeof(double));
+  s->rf_fb = (double*)calloc((size_t)CG_MAX_CAVITIES * M * 2, sizeof(double));
+  s->rf_zmin = (double*)calloc(M, sizeof(double));
+  s->rf_zmax = (double*)calloc(M, sizeof(double));
+  res_init(s);
   /* WakeFunction::InitialLRWake (WakeFunction.cpp:49-202) */
   if (cfg->flag_lr_wake) {
     int turns = cfg->lr_turns;
@@ -318,6 +343,7 @@ void or_destroy(or_state* s) {
   }
   free(s->cloud); free(s->b); free(s->sec); free(s->rec); free(s->lr_tab); free(s->lr_hist);
   free(s->fir_hist);
+  free(s->rf_info); free(s->rf_fb); free(s->rf_zmin); free(s->rf_zmax);
   free(s);
 }
 
@@ -592,25 +618,323 @@ int or_section_map(or_state* s, int k) {
 }
 
 /* MPBeam::BeamMomtumUpdateDueToRFTest, RFCA branch (MPBeam.cpp:2624-2652) -> */
-/* Bunch::BunchMomentumUpdateDueToRFCA (Bunch.cpp:453-481), all particles.    */
+/* ---- cavities with beam loading (rfMode 1) ------------------------------ */
+/* Complex values as two doubles, each operation in the order std::complex  */
+/* evaluates it (products a c - b d, a d + b c; real x complex scales both).  */
+typedef struct { double re, im; } cx;
+static cx cx_mul(cx a, cx b) { cx r = {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; return r; }
+static cx cx_add(cx a, cx b) { cx r = {a.re + b.re, a.im + b.im}; return r; }
+static cx cx_sub(cx a, cx b) { cx r = {a.re - b.re, a.im - b.im}; return r; }
+static cx cx_scale(cx a, double s) { cx r = {a.re * s, a.im * s}; return r; }
+static cx cx_div(cx a, double s) { cx r = {a.re / s, a.im / s}; return r; }
+static cx cx_expi(double th) { cx r = {cos(th), sin(th)}; return r; } /* exp(i th) */
+static double cx_abs(cx a) { return hypot(a.re, a.im); }
+static double cx_arg(cx a) { return atan2(a.im, a.re); }
+
+/* Resonator::GetInitialResonatorGenIg (Resonator.cpp:38-54) */
+static void res_gen_ig(or_state* s, int i) {
+  const cg_ring* r = &s->cfg.ring;
+  cx gen = {s->res_gen[i][0], s->res_gen[i][1]};
+  cx ig = {0.0, 0.0};
+  if (r->res_type[i] != 0) {
+    double argVgr = cx_arg(gen) - r->res_psi[i];
+    double absVgr = cx_abs(gen) / fabs(cos(r->res_psi[i]));
+    cx vgr = cx_scale(cx_expi(argVgr), absVgr);
+    ig = cx_div(cx_scale(vgr, 1.0 + r->res_coupling[i]), r->res_rs[i]);
+  }
+  s->res_ig[i][0] = ig.re;
+  s->res_ig[i][1] = ig.im;
+}
+
+/* MPBeam::InitialcavityResonator (MPBeam.cpp:236-465), the state it leaves:
+   the steady-state beam-induced voltage of the fill pattern after
+   ceil(100 tF f0) turns of bucket-by-bucket decay and rotation, the
+   generator voltage that completes the required cavity voltage (minus the
+   average self-loss kick for an active cavity), the generator current, and
+   the bunches' initial BunchRFModeInfo.  (The transient printout of that
+   function is host output and not restated.) */
+static void res_init(or_state* s) {
+  const cg_ring* r = &s->cfg.ring;
+  double PI = PI_REF();
+  int H = r->harmonics, M = s->M;
+  double f0 = r->f0;
+  cx kick_aver[CG_MAX_CAVITIES];
+  for (int i = 0; i < r->n_cav; ++i) {
+    double tF = r->res_tf[i];
+    int nTurns = (int)ceil(100 * tF * f0);
+    cx vb = {0, 0}, aver2 = {0, 0}, kick = {0, 0};
+    double tB = 1.0 / f0 / H;
+    double deltaL = tB / tF;
+    double cPsi = deltaL * tan(r->res_psi[i]);
+    double decay = exp(-deltaL);
+    cx rot = cx_expi(cPsi);
+    double vb0re = -1 * r->res_fre[i] * 2 * PI * r->res_rs[i] / r->res_q0[i];
+    for (int n = 0; n < nTurns; ++n) {
+      int k = 0;
+      for (int j = 0; j < H; ++j) {
+        cx vb0 = {0.0, 0.0};
+        if (k < M && s->b[k].harm_i == j) {
+          vb0.re = vb0re * s->b[k].ne * E_CHARGE;
+          vb0.im = 0.0 * s->b[k].ne * E_CHARGE;
+          k++;
+          if (n == nTurns - 1) kick = cx_add(kick, cx_div(vb0, 2.0));
+        }
+        vb = cx_add(vb, vb0);
+        vb = cx_mul(cx_scale(vb, decay), rot);
+        if (n == nTurns - 1) aver2 = cx_add(aver2, vb);
+      }
+    }
+    cx aver = cx_div(aver2, (double)H);
+    s->res_vb[i][0] = aver.re;
+    s->res_vb[i][1] = aver.im;
+    kick_aver[i] = cx_div(kick, (double)M);
+  }
+  for (int i = 0; i < r->n_cav; ++i) {
+    cx req = {r->cav_vreq_re[i], r->cav_vreq_im[i]};
+    cx vb = {s->res_vb[i][0], s->res_vb[i][1]};
+    cx gen = {0.0, 0.0};
+    if (r->res_type[i] != 0) gen = cx_sub(cx_sub(req, vb), kick_aver[i]);
+    s->res_gen[i][0] = gen.re;
+    s->res_gen[i][1] = gen.im;
+    if (r->res_cold[i] || r->rf_mode[i] == 0) s->res_vb[i][0] = s->res_vb[i][1] = 0.0;
+    res_gen_ig(s, i);
+    for (int j = 0; j < M; ++j) {
+      double* inf = s->rf_info + ((size_t)j * CG_MAX_CAVITIES + i) * 8;
+      inf[0] = req.re; inf[1] = req.im;
+      inf[2] = gen.re; inf[3] = gen.im;
+      inf[4] = s->res_vb[i][0]; inf[5] = s->res_vb[i][1];
+      inf[6] = kick_aver[i].re; inf[7] = kick_aver[i].im;
+    }
+  }
+}
+
+/* Resonator::ResonatorDynamics (Resonator.cpp:235-261): the generator-driven
+   cavity voltage over time tB with a constant generator current. */
+static void res_dynamics(or_state* s, int i, double tB) {
+  const cg_ring* r = &s->cfg.ring;
+  double PI = PI_REF();
+  double sigma = 2.0 * PI * r->res_fre[i] / (2.0 * r->res_ql[i]);
+  double deltaOmega = 2.0 * PI * r->res_detune[i];
+  cx ig = {s->res_ig[i][0], s->res_ig[i][1]};
+  cx gen = {s->res_gen[i][0], s->res_gen[i][1]};
+  gen = cx_mul(gen, cx_scale(cx_expi(deltaOmega * tB), exp(-sigma * tB)));
+  double alpha = deltaOmega * exp(-sigma * tB) * sin(deltaOmega * tB) -
+                 sigma * exp(-sigma * tB) * cos(deltaOmega * tB) + sigma;
+  double beta = sigma * exp(-sigma * tB) * sin(deltaOmega * tB) +
+                deltaOmega * exp(-sigma * tB) * cos(deltaOmega * tB) - deltaOmega;
+  double coefB = 2 * PI * r->res_fre[i] / 2.0 * r->res_rs[i] / r->res_q0[i] /
+                 (pow(sigma, 2) + pow(deltaOmega, 2));
+  gen.re += coefB * (alpha * ig.re + beta * ig.im);
+  gen.im += coefB * (-beta * ig.re + alpha * ig.im);
+  s->res_gen[i][0] = gen.re;
+  s->res_gen[i][1] = gen.im;
+}
+
+/* exp(-t/tF) exp(i 2 pi f t) applied to the beam-induced voltage
+   (Resonator::GetBeamInducedVol, Resonator.cpp:205-212) */
+static void res_decay(or_state* s, int i, double t) {
+  const cg_ring* r = &s->cfg.ring;
+  double PI = PI_REF();
+  double deltaL = t / r->res_tf[i];
+  double cPsi = 2.0 * PI * r->res_fre[i] * t;
+  cx vb = {s->res_vb[i][0], s->res_vb[i][1]};
+  vb = cx_mul(vb, cx_scale(cx_expi(cPsi), exp(-deltaL)));
+  s->res_vb[i][0] = vb.re;
+  s->res_vb[i][1] = vb.im;
+}
+
+/* MPBunch::BunchMomentumUpdateDueToRFModeStable (MPBunch.cpp:1323-1416,
+   resExciteIntability 0) and MPBunch::BunchMomentumUpdateDueToRFMode
+   (MPBunch.cpp:1419-1513, 1): the bunch in rfBunchBinNum bins from head
+   (zMax) to tail; every alive particle gains the cavity voltage at its bin
+   and half the voltage its own charge induces. */
+static void bunch_beam_loading(or_state* s, int j, int i) {
+  const cg_ring* r = &s->cfg.ring;
+  or_bunch* b = &s->b[j];
+  double PI = PI_REF();
+  int nb = r->rf_bunch_bins;
+  double fRF = r->f0 * r->harmonics;
+  double E = r->electron_energy, rBeta = r->r_beta;
+  double zMax = s->rf_zmax[j], zMin = s->rf_zmin[j];
+  double dzBin = (zMax - zMin) / nb;
+  double dtBin = dzBin / C_LIGHT / rBeta;
+  int* cnt = (int*)calloc(nb, sizeof(int));
+  int* bin = (int*)malloc(sizeof(int) * (b->n > 0 ? b->n : 1));
+  for (int p = 0; p < b->n; ++p) {
+    bin[p] = -1;
+    if (b->surv[p] != 0) continue;
+    int idx = (int)floor((zMax - b->c[4][p]) / dzBin);
+    bin[p] = idx;
+    cnt[idx]++;
+  }
+  double* kickA = (double*)malloc(sizeof(double) * nb);
+  double* kickB = (double*)malloc(sizeof(double) * nb);
+  double cavRe = 0, cavIm = 0, genRe = 0, genIm = 0, indRe = 0, indIm = 0;
+  cx selfLoss = {0, 0};
+  int inBunch = 0;
+  cx vbA = {s->res_vb[i][0], s->res_vb[i][1]};
+  cx gen0 = {s->res_gen[i][0], s->res_gen[i][1]};
+  if (r->res_excite[i] == 0) {
+    cx vb0 = {-1 * 2 * PI * r->res_fre[i] * r->res_rs[i] / r->res_q0[i], 0.0};
+    vb0 = cx_scale(cx_scale(vb0, b->ne), E_CHARGE);
+    cx cav = cx_add(vbA, gen0);
+    for (int k = 0; k < nb; ++k) {
+      double posZ = zMax - k * dzBin - dzBin / 2.0;
+      double th = -posZ / C_LIGHT / rBeta * 2. * PI * (double)r->cav_harm[i] * fRF;
+      kickA[k] = cx_mul(cav, cx_expi(th)).re / E / pow(rBeta, 2);
+      kickB[k] = vb0.re / 2.0 / E / pow(rBeta, 2);
+      double c = (double)cnt[k];
+      inBunch += cnt[k];
+      selfLoss = cx_add(selfLoss, cx_scale(cx_div(vb0, 2.0), c));
+      cavRe += cav.re * c; cavIm += cav.im * c;
+      genRe += gen0.re * c; genIm += gen0.im * c;
+      cx ind = cx_add(vbA, vb0);
+      indRe += ind.re * c; indIm += ind.im * c;
+    }
+    vbA = cx_add(vbA, vb0);
+  } else {
+    double deltaL = dtBin / r->res_tf[i];
+    double cPsi = 2.0 * PI * r->res_fre[i] * dtBin;
+    cx rot = cx_scale(cx_expi(cPsi), exp(-deltaL));
+    for (int k = 0; k < nb; ++k) {
+      double posZ = zMax - k * dzBin - dzBin / 2.0;
+      double th = -posZ / C_LIGHT / rBeta * 2. * PI * (double)r->cav_harm[i] * fRF;
+      cx gen = cx_mul(gen0, cx_expi(th));
+      cx cav = cx_add(vbA, gen);
+      cx vb0 = {-1 * 2 * PI * r->res_fre[i] * r->res_rs[i] / r->res_q0[i], 0.0};
+      vb0 = cx_scale(cx_scale(cx_scale(vb0, b->q_macro), (double)cnt[k]), E_CHARGE);
+      kickA[k] = cav.re / E / pow(rBeta, 2);
+      kickB[k] = vb0.re / 2.0 / E / pow(rBeta, 2);
+      double c = (double)cnt[k];
+      inBunch += cnt[k];
+      selfLoss = cx_add(selfLoss, cx_scale(cx_div(vb0, 2.0), c));
+      cavRe += cav.re * c; cavIm += cav.im * c;
+      genRe += gen.re * c; genIm += gen.im * c;
+      cx ind = cx_add(vbA, vb0);
+      indRe += ind.re * c; indIm += ind.im * c;
+      vbA = cx_add(vbA, vb0);
+      vbA = cx_mul(vbA, rot);
+    }
+  }
+  for (int p = 0; p < b->n; ++p) {
+    if (bin[p] < 0) continue;
+    b->c[5][p] += kickA[bin[p]];
+    b->c[5][p] += kickB[bin[p]];
+  }
+  double* inf = s->rf_info + ((size_t)j * CG_MAX_CAVITIES + i) * 8;
+  double nin = (double)inBunch;
+  inf[0] = cavRe / nin; inf[1] = cavIm / nin;
+  inf[2] = genRe / nin; inf[3] = genIm / nin;
+  if (r->res_excite[i] == 0) {
+    inf[4] = indRe / nin; inf[5] = indIm / nin;
+    inf[6] = selfLoss.re / nin; inf[7] = selfLoss.im / nin;
+  } else {
+    cx sl = cx_div(selfLoss, nin);
+    inf[4] = indRe / nin + sl.re; inf[5] = indIm / nin + sl.im;
+    inf[6] = sl.re; inf[7] = sl.im;
+  }
+  s->res_vb[i][0] = vbA.re;
+  s->res_vb[i][1] = vbA.im;
+  free(cnt); free(bin); free(kickA); free(kickB);
+}
+
+/* MPBeam::BeamMomtumUpdateDueToRFTest (MPBeam.cpp:2621-2704): per cavity in
+   order, the ideal cavity (Bunch::BunchMomentumUpdateDueToRFCA,
+   Bunch.cpp:453-480) or, with beam loading, bunch by bunch the kick above,
+   the bucket-by-bucket sampling and generator dynamics over the bunch's gap
+   and the decay of the induced voltage to the next bunch; then the direct
+   cavity feedback kicks (Bunch::GetLongiKickDueToCavFB, Bunch.cpp:431-451). */
 int or_rf_kick(or_state* s) {
   const cg_ring* r = &s->cfg.ring;
   double PI = PI_REF();
   double fRF = r->f0 * r->harmonics;
+  double tRF = r->t0 / r->harmonics;
+  int M = s->M;
+  /* MPBeam::GetTimeDisToNextBunch (MPBeam.cpp:2724-2763) */
+  double* tnext = (double*)malloc(sizeof(double) * M);
+  for (int j = 0; j < M; ++j) {
+    zminmax(&s->b[j]);
+    s->rf_zmin[j] = s->b[j].m.z_min;
+    s->rf_zmax[j] = s->b[j].m.z_max;
+  }
+  for (int j = 0; j < M; ++j) {
+    int nx = (j + 1) % M;
+    tnext[j] = s->b[j].gap_i * tRF + (s->rf_zmin[j] - s->rf_zmax[nx]) / C_LIGHT / r->r_beta;
+  }
   for (int c = 0; c < r->n_cav; ++c) {
-    for (int j = 0; j < s->M; ++j) {
-      or_bunch* b = &s->b[j];
+    if (r->rf_mode[c] == 0) {
+      for (int j = 0; j < M; ++j) {
+        or_bunch* b = &s->b[j];
 #pragma omp parallel for schedule(static)
-      for (int i = 0; i < b->n; i++) {
-        double th = b->c[4][i] / C_LIGHT / r->r_beta * 2. * PI * (double)r->cav_harm[c] * fRF;
-        /* Re(V exp(-i th)) as std::complex multiplies it: a c - b d, d = -sin */
-        double re = r->cav_vreq_re[c] * cos(-th) - r->cav_vreq_im[c] * sin(-th);
-        b->c[5][i] += re / r->electron_energy / pow(r->r_beta, 2);
+        for (int i = 0; i < b->n; i++) {
+          double th = b->c[4][i] / C_LIGHT / r->r_beta * 2. * PI * (double)r->cav_harm[c] * fRF;
+          /* Re(V exp(-i th)) as std::complex multiplies it: a c - b d, d = -sin */
+          double re = r->cav_vreq_re[c] * cos(-th) - r->cav_vreq_im[c] * sin(-th);
+          b->c[5][i] += re / r->electron_energy / pow(r->r_beta, 2);
+        }
       }
+      continue;
+    }
+    for (int j = 0; j < M; ++j) {
+      or_bunch* b = &s->b[j];
+      bunch_beam_loading(s, j, c);
+      for (int k = 0; k < b->gap_i; ++k) {
+        if (k == 0) {  /* Resonator::GetResonatorInfoAtNTrf (Resonator.cpp:263-274) */
+          double dt = k * tRF - s->rf_zmin[j] / C_LIGHT;
+          double deltaL = dt / r->res_tf[c];
+          double cPsi = 2.0 * PI * r->res_fre[c] * dt;
+          cx vb = {s->res_vb[c][0], s->res_vb[c][1]};
+          cx vbs = cx_mul(cx_scale(vb, exp(-deltaL)), cx_expi(cPsi));
+          cx gen = {s->res_gen[c][0], s->res_gen[c][1]};
+          cx req = {r->cav_vreq_re[c], r->cav_vreq_im[c]};
+          cx dv = cx_sub(cx_add(vbs, gen), req);
+          s->rf_fb[((size_t)c * M + j) * 2 + 0] = -dv.re;
+          s->rf_fb[((size_t)c * M + j) * 2 + 1] = -dv.im;
+        }
+        res_dynamics(s, c, tRF);
+      }
+      res_decay(s, c, r->res_excite[c] == 0 ? b->gap_i * tRF : tnext[j]);
     }
   }
+  for (int c = 0; c < r->n_cav; ++c) {
+    if (r->rf_mode[c] != 1 || r->res_dir_fb[c] != 1) continue;
+    for (int j = 0; j < M; ++j) {
+      or_bunch* b = &s->b[j];
+      cx fb = {s->rf_fb[((size_t)c * M + j) * 2 + 0], s->rf_fb[((size_t)c * M + j) * 2 + 1]};
+      double absFB = cx_abs(fb) * r->res_dir_fb_gain[c];
+      double argFB = cx_arg(fb) + r->res_dir_fb_phase[c] + r->res_dir_fb_delay[c] * r->res_fre[c] * 2 * PI;
+      cx k = cx_scale(cx_expi(argFB), absFB);
+      double dk = k.re / r->electron_energy / pow(r->r_beta, 2);
+      for (int p = 0; p < b->n; ++p) b->c[5][p] += dk;
+    }
+  }
+  free(tnext);
   return 0;
 }
+
+/* resonator state: vbAccum, resGenVol, resGenIg (re, im) */
+int or_resonator_state(or_state* s, int c, double* out) {
+  if (c < 0 || c >= s->cfg.ring.n_cav) return 1;
+  out[0] = s->res_vb[c][0]; out[1] = s->res_vb[c][1];
+  out[2] = s->res_gen[c][0]; out[3] = s->res_gen[c][1];
+  out[4] = s->res_ig[c][0]; out[5] = s->res_ig[c][1];
+  return 0;
+}
+int or_resonator_set(or_state* s, int c, const double* in) {
+  if (c < 0 || c >= s->cfg.ring.n_cav) return 1;
+  s->res_vb[c][0] = in[0]; s->res_vb[c][1] = in[1];
+  s->res_gen[c][0] = in[2]; s->res_gen[c][1] = in[3];
+  s->res_ig[c][0] = in[4]; s->res_ig[c][1] = in[5];
+  return 0;
+}
+/* BunchRFModeInfo of bunch j, cavity c: cavity, generator, induced and
+   self-loss voltages (re, im) */
+int or_rf_info(or_state* s, int j, int c, double* out) {
+  if (j < 0 || j >= s->M || c < 0 || c >= s->cfg.ring.n_cav) return 1;
+  memcpy(out, s->rf_info + ((size_t)j * CG_MAX_CAVITIES + c) * 8, 8 * sizeof(double));
+  return 0;
+}
+
 /* Bunch::BunchLongPosTransferOneTurn (Bunch.cpp:494-501) */
 int or_longi_drift(or_state* s) {
   const cg_ring* r = &s->cfg.ring;

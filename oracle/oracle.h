@@ -36,6 +36,9 @@ int or_get_moments(or_state* s, cg_bunch_moments* out);
 int or_beam_ion_ip(or_state* s, int turn, int k);
 int or_section_map(or_state* s, int k);
 int or_rf_kick(or_state* s);
+int or_resonator_state(or_state* s, int c, double* out);
+int or_resonator_set(or_state* s, int c, const double* in);
+int or_rf_info(or_state* s, int j, int c, double* out);
 int or_longi_drift(or_state* s);
 int or_energy_loss(or_state* s);
 int or_synrad(or_state* s, int turn);

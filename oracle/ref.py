@@ -47,7 +47,8 @@ def load():
         L.ref_close.restype = None
         for n in ("ref_info", "ref_bunch_info", "ref_set_emit_nat", "ref_bunch_size", "ref_set_bunch",
                   "ref_get_bunch", "ref_moments", "ref_beam_info", "ref_stage", "ref_run_turns",
-                  "ref_ion_count", "ref_ion_get", "ref_ion_set", "ref_sr_bins", "ref_ring"):
+                  "ref_ion_count", "ref_ion_get", "ref_ion_set", "ref_sr_bins", "ref_ring",
+                  "ref_resonator", "ref_rf_info"):
             getattr(L, n).restype = C.c_int
         L.cg_ref_seed.argtypes = [C.c_ulonglong, C.c_longlong]
         L.cg_ref_seed.restype = None
@@ -162,6 +163,21 @@ class RefBeam:
     def set_ions(self, k, p, x, y, vx, vy):
         a = [np.ascontiguousarray(v, dtype=np.float64) for v in (x, y, vx, vy)]
         self._check(self.lib.ref_ion_set(self.h, k, p, *[_dp(v) for v in a], len(a[0])))
+
+    def resonator(self, c):
+        """(vbAccum, resGenVol, resGenIg) as complex numbers and the derived
+        (resFre, resQualityQL, resDeTunePsi, tF) of cavity c."""
+        out = np.empty(10)
+        self._check(self.lib.ref_resonator(self.h, c, _dp(out)))
+        return (complex(out[0], out[1]), complex(out[2], out[3]), complex(out[4], out[5]),
+                tuple(out[6:10]))
+
+    def rf_info(self, j, c):
+        """BunchRFModeInfo of bunch j, cavity c: (cavity, generator, induced,
+        self-loss) voltages as complex numbers."""
+        out = np.empty(8)
+        self._check(self.lib.ref_rf_info(self.h, j, c, _dp(out)))
+        return tuple(complex(out[2 * i], out[2 * i + 1]) for i in range(4))
 
     def sr_bins(self, j, n_bins):
         zlo, dz = C.c_double(), C.c_double()

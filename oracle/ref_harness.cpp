@@ -457,6 +457,36 @@ int ref_sr_bins(void *h, int j, double *zlo, double *dz, int *counts) {
     return 0;
 }
 
+// Resonator c after the reference's set-up or its last RF step: vbAccum,
+// resGenVol, resGenIg (re, im), then resFre, resQualityQL, resDeTunePsi, tF
+// -> 10 doubles (Resonator.h)
+int ref_resonator(void *h, int c, double *out) {
+    RefRun *r = static_cast<RefRun *>(h);
+    if (c < 0 || c >= (int)r->cav.resonatorVec.size()) return 1;
+    const Resonator &R = r->cav.resonatorVec[c];
+    const double v[10] = {R.vbAccum.real(), R.vbAccum.imag(), R.resGenVol.real(),
+                          R.resGenVol.imag(), R.resGenIg.real(), R.resGenIg.imag(),
+                          R.resFre, R.resQualityQL, R.resDeTunePsi, R.tF};
+    std::memcpy(out, v, sizeof v);
+    return 0;
+}
+
+// BunchRFModeInfo of bunch j, cavity c (Bunch.h:109-118): cavity, generator,
+// induced and self-loss voltages (re, im) -> 8 doubles
+int ref_rf_info(void *h, int j, int c, double *out) {
+    RefRun *r = static_cast<RefRun *>(h);
+    if (j < 0 || j >= (int)r->beam.beamVec.size() || c < 0 ||
+        c >= (int)r->cav.resonatorVec.size())
+        return 1;
+    const auto *I = r->beam.beamVec[j].bunchRFModeInfo;
+    const double v[8] = {I->cavVolBunchCen[c].real(),      I->cavVolBunchCen[c].imag(),
+                         I->genVolBunchAver[c].real(),     I->genVolBunchAver[c].imag(),
+                         I->induceVolBunchCen[c].real(),   I->induceVolBunchCen[c].imag(),
+                         I->selfLossVolBunchCen[c].real(), I->selfLossVolBunchCen[c].imag()};
+    std::memcpy(out, v, sizeof v);
+    return 0;
+}
+
 // Derived ring constants after ParamRead (ReadInputSettings.cpp:986-1081):
 // rGamma, rBeta, t0, f0, workQz, emitNat[3], synchRadDampTime[3] (turns),
 // u0, sdelta0, ringHarm, 0  -> 16 doubles

@@ -269,6 +269,30 @@ def test_turns_with_the_asynchronous_map_pass_repeat_the_register_pass(name, sca
             assert np.array_equal(p, q)
 
 
+def test_turns_with_reserved_walk_sms_repeat_the_shared_ones():
+    """Walk CTAs that reserve their SM's shared memory (no kick or map CTA
+    beside them) give the same turns bit for bit."""
+    from cetasim_b200.beam import MPBeam
+    wl = small("batched_uneven", 0.01, bunch_current=TRAPPED)
+    parts = particles(wl, seed=13)
+    runs = []
+    for on in (False, True):
+        g = MPBeam(wl)
+        for j, c in enumerate(parts):
+            g.upload(j, c)
+        g.set_pipeline(8, 64, True)
+        g.set_walk_reserve(on)
+        g.Run(0, 3)
+        runs.append(([g.download(j) for j in range(wl.n_bunches)],
+                     [g.ions(k) for k in (0, wl.cfg.n_sections - 1)]))
+    (ca, ia), (cb, ib) = runs
+    for (x, s), (y, t) in zip(ca, cb):
+        assert np.array_equal(x, y) and np.array_equal(s, t)
+    for u, v in zip(ia, ib):
+        for p, q in zip(u, v):
+            assert np.array_equal(p, q)
+
+
 @pytest.mark.parametrize("groups,ramp", [(3, False), (4, True), (16, False), (2, True)])
 def test_pipelined_turn_repeats_the_unpipelined_turn(groups, ramp):
     """The ion walk in segments with records, kicks and maps overlapping the
