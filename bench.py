@@ -70,7 +70,8 @@ DESC = {
 
 # the kick kernel's shapes in the order of cg_autotune's timings
 KICK_SHAPES = ["256 thr x3/SM", "256 thr x4/SM", "128 thr x4/SM", "128 thr x6/SM",
-               "256 thr x3/SM, 4 tiles per CTA", "128 thr x6/SM, 2 tiles per CTA"]
+               "256 thr x3/SM, 4 tiles per CTA", "128 thr x6/SM, 2 tiles per CTA",
+               "128 thr x6/SM, 4 tiles per CTA", "256 thr x3/SM, 8 tiles per CTA"]
 
 
 class ClockSampler:

@@ -91,6 +91,14 @@ class RwSectors(C.Structure):
                                                         "beta_x", "beta_y", "num", "sigma")]
 
 
+class Bbi(C.Structure):
+    _fields_ = [("flag", I), ("time_domain", I), ("sim", I * 5), ("n_rows", I),
+                ("table", C.POINTER(D))]
+
+
+BBI_MAX_BINS = 4096
+
+
 class Config(C.Structure):
     _fields_ = [
         ("ring", Ring), ("n_sections", I), ("sections", C.POINTER(Section)), ("ion", IonParams),
@@ -100,7 +108,7 @@ class Config(C.Structure):
         ("n_turns", I), ("bunch_info_print_interval", I), ("bunch_emit_x", D), ("bunch_emit_y", D),
         ("bunch_sigma_z", D), ("bunch_sigma_dp", D),
         ("growth_fit_start", I), ("growth_fit_end", I), ("run_cbmgr", C.c_char * 256),
-        ("lr_rw", RwSectors), ("sr_rw", RwSectors),
+        ("lr_rw", RwSectors), ("sr_rw", RwSectors), ("bbi", Bbi),
     ]
 
 
@@ -164,6 +172,8 @@ EXPORTS = [
     ("cg_synrad", I, [C.c_void_p, I]),
     ("cg_lr_wake", I, [C.c_void_p]),
     ("cg_sr_wake", I, [C.c_void_p, I]),
+    ("cg_bbi_kick", I, [C.c_void_p]),
+    ("cg_bbi_profile", I, [C.c_void_p, I, PI, PI, PD, I]),
     ("cg_sr_bins", I, [C.c_void_p, I, PD, PD, PI]),
     ("cg_fir", I, [C.c_void_p, I]),
     ("cg_mark_lost", I, [C.c_void_p, PD]),

@@ -129,6 +129,21 @@ class MPBeam:
     def BeamSynRadDamping(self, turn: int):
         self._check(self.lib.cg_synrad(self.h, turn))
 
+    def BBImpBeamInteraction(self):
+        self._check(self.lib.cg_bbi_kick(self.h))
+
+    def bbi_profile(self, j: int):
+        """(first bin, 6 x n array) of bunch j after the last
+        BBImpBeamInteraction: the smoothed profile and the potentials of the
+        planes Z, Dx, Dy, Qx, Qy (zero at bins without particles)."""
+        lo, n = C.c_int(), C.c_int()
+        self._check(self.lib.cg_bbi_profile(self.h, j, C.byref(lo), C.byref(n), None, 0))
+        cap = max(1, n.value)
+        out = np.zeros((6, cap))
+        self._check(self.lib.cg_bbi_profile(self.h, j, C.byref(lo), C.byref(n),
+                                            out.ctypes.data_as(C.POINTER(C.c_double)), cap))
+        return lo.value, out[:, :n.value]
+
     def LRWakeBeamIntaction(self):
         self._check(self.lib.cg_lr_wake(self.h))
 

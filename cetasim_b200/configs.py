@@ -35,6 +35,7 @@ pre-loaded clouds are over-focused out of the beam within a few passages).
 """
 from __future__ import annotations
 
+import ctypes as C
 import math
 
 import numpy as np
@@ -127,6 +128,22 @@ class Workload:
         self.harm = np.ascontiguousarray(harm, dtype=np.int32)
         self.ne = np.ascontiguousarray(ne, dtype=np.float64)
         self.gen = gen  # (emit_x, emit_y, sigma_z, sigma_dp)
+        self.bbi_table = None
+
+    def set_bbi(self, table, time_domain: int, sim=(1, 1, 1, 1, 1)) -> None:
+        """Broadband impedance: `table` is the impedance file's rows (11
+        columns, time_domain 0) or the wake file's rows (6 columns,
+        time_domain 1); the array stays alive with the workload."""
+        cols = 6 if time_domain else 11
+        t = np.ascontiguousarray(table, dtype=np.float64).reshape(-1, cols)
+        self.bbi_table = t
+        b = self.cfg.bbi
+        b.flag = 1
+        b.time_domain = int(time_domain)
+        for i in range(5):
+            b.sim[i] = int(sim[i])
+        b.n_rows = t.shape[0]
+        b.table = t.ctypes.data_as(C.POINTER(C.c_double))
 
     @property
     def n_bunches(self) -> int:

@@ -2,6 +2,7 @@
 // include/cetasim_gpu.h).  Host-side orchestration: configuration, device
 // state, stage launches, the per-turn CUDA graph, status mapping.
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -83,6 +84,11 @@ int check_status(Handle& h) {
     return fail(&h, CG_ERR_INVALID, "long-range wake lag outside the wake table (tau > 0)");
   if (st & kStatusGaussCut)
     return fail(&h, CG_ERR_INVALID, "an initial-distribution draw found no sample inside the 3-sigma cut");
+  if (st & kStatusBbiRange)
+    return fail(&h, CG_ERR_INVALID,
+                "a particle lies outside the broadband-impedance profile bins");
+  if (st & kStatusBbiWide)
+    return fail(&h, CG_ERR_INVALID, "a bunch spans more than CG_BBI_MAX_BINS broadband-impedance bins");
   return fail(&h, CG_ERR_CUDA, "unknown device status");
 }
 
@@ -108,6 +114,10 @@ void free_beam(Handle& h) {
   dfree(d.rf_info); dfree(d.rf_work);
   d.res_state = nullptr; d.rf_zr = nullptr; d.rf_counts = nullptr; d.rf_kick = nullptr;
   d.rf_fbk = nullptr; d.rf_info = nullptr; d.rf_work = nullptr;
+  dfree(d.bbi_lo); dfree(d.bbi_hi); dfree(d.bbi_amax); dfree(d.bbi_cnt); dfree(d.bbi_sxy);
+  dfree(d.bbi_pot); dfree(d.bbi_win);
+  d.bbi_lo = nullptr; d.bbi_hi = nullptr; d.bbi_amax = nullptr; d.bbi_cnt = nullptr;
+  d.bbi_sxy = nullptr; d.bbi_pot = nullptr; d.bbi_win = nullptr;
   h.cbm_cap = h.cbm_n = 0;
   IonWalk& w = d.iw;
   dfree(w.births); dfree(w.prep); dfree(w.bunch); dfree(w.spec); dfree(w.bound); dfree(w.part);
@@ -319,6 +329,99 @@ int cg_lattice_init(const cg_ring* ring, cg_section* sec, int n) {
   return CG_OK;
 }
 
+// Broadband-impedance set-up from cfg.bbi (MPBeam.cpp:856-876).  Fills p and,
+// per plane Z, Dx, Dy, Qx, Qy, either the impedances times 1 / i
+// (frequency domain, data = 5 x n (re, im) pairs) or the wake samples (time
+// domain, data = 5 x nw).  Returns an error message or "".
+static std::string bbi_plan(const cg_config& cfg, BbiParams& p, std::vector<double>& data) {
+  const cg_bbi& b = cfg.bbi;
+  const cg_ring& r = cfg.ring;
+  if (b.time_domain != 0 && b.time_domain != 1) return "wrong setting in BoardBandImpedance namelist";
+  if (!b.table || b.n_rows < 2) return "the broadband-impedance table needs >= 2 rows";
+  p.td = b.time_domain;
+  for (int q = 0; q < 5; ++q) p.sim[q] = b.sim[q] != 0;
+  const double rfLen = r.t0 / r.harmonics * kCLight;  // MPBunch.cpp:2355, 2035
+  const int n = b.n_rows;
+  if (!p.td) {
+    // BoardBandImp::ReadInImp (BoardBandImp.cpp:64-115)
+    const double* t = b.table;
+    const double freqMax = t[(size_t)(n - 1) * 11];
+    if (!(freqMax > 0)) return "the impedance table's last frequency must be > 0";
+    const double dt = 1.0 / (2 * freqMax);
+    p.dz = dt * kCLight * r.r_beta;
+    const double zMax = p.dz * (n - 1);
+    p.nbins = 2 * n - 1;
+    p.nw = p.nbins;
+    p.zmin = -zMax;
+    // the filtered bins (MPBunch.cpp:2360-2361)
+    const double zMinBin = -zMax, dzBin = p.dz;
+    p.s0 = (int)((-rfLen / 2. - zMinBin + dzBin / 2) / dzBin);
+    p.s1 = (int)((rfLen / 2. - zMinBin + dzBin / 2) / dzBin);
+    if (p.s0 < 0 || p.s1 > p.nbins || p.s1 < p.s0)
+      return "the impedance table's bins (dz (n - 1) = zMax) must cover one RF bucket";
+    data.assign((size_t)5 * n * 2, 0.0);
+    for (int k = 0; k < n; ++k) {
+      const double* c = t + (size_t)k * 11;
+      // Alex Chao's convention (BoardBandImp.cpp:64-70); the transverse
+      // planes enter the spectrum product times i (MPBunch.cpp:2212 and after)
+      const double re[5] = {c[1], -c[7], -c[8], -c[9], -c[10]};
+      const double im[5] = {-c[6], -c[2], -c[3], -c[4], -c[5]};
+      for (int q = 0; q < 5; ++q) {
+        double* o = &data[((size_t)q * n + k) * 2];
+        if (q == 0) {
+          o[0] = re[q];
+          o[1] = im[q];
+        } else {
+          o[0] = -im[q];
+          o[1] = re[q];
+        }
+      }
+    }
+  } else {
+    // MPBeam::GetQuasiWakePoten (MPBeam.cpp:748-801) and
+    // MPBunch::BBImpBunchInteractionTD (MPBunch.cpp:2032-2041)
+    const double* t = b.table;
+    const double z0 = t[0];
+    int cen = 0;
+    for (int i = 0; i < n; ++i)
+      if (t[(size_t)i * 6] == 0) cen = i;
+    if (2 * cen > n) return "the wake table's z = 0 row must lie in its first half";
+    std::vector<double> wz(n);
+    for (int i = 0; i < n; ++i) wz[i] = -1 * t[(size_t)i * 6 + 1];
+    data.assign((size_t)5 * n, 0.0);
+    data[0] = wz[cen];
+    for (int i = 1; i < cen; ++i) data[i] = wz[cen + i] + wz[cen - i];
+    for (int i = cen; i < n - cen; ++i) data[i] = wz[cen + i];
+    for (int q = 1; q < 5; ++q)
+      for (int i = 0; i < n; ++i) data[(size_t)q * n + i] = -1 * t[(size_t)i * 6 + 1 + q];
+    const double z1 = t[6] - z0;
+    p.dz = std::fabs(z1 - 0.0);
+    if (!(p.dz > 0)) return "the wake table's first two z must differ";
+    p.zmin = -1 * rfLen / 2;
+    p.nbins = (int)(1 * rfLen / p.dz);
+    if (p.nbins < 1) return "the wake table's z step must be below the RF bucket length";
+    p.nw = n;
+    p.s0 = 0;
+    p.s1 = p.nbins;
+  }
+  p.wcap = std::min(CG_BBI_MAX_BINS, p.nbins) + 2 * kBbiHalf;
+  p.energy = r.electron_energy;
+  p.beta2 = std::pow(r.r_beta, 2);
+  p.beta_x = cfg.sections[0].beta_x;
+  p.beta_y = cfg.sections[0].beta_y;
+  // GSL's Gaussian filter kernel for K = 51, alpha = 10 (gsl_filter_gaussian,
+  // GSL 2.8: G(k) = exp(-(alpha k / H)^2 / 2), |k| <= H = (K - 1) / 2, unit sum)
+  const double alpha = 10.0;
+  double sum = 0;
+  for (int i = 0; i <= 2 * kBbiHalf; ++i) {
+    const double x = alpha * (double)(i - kBbiHalf) / (double)kBbiHalf;
+    p.g[i] = std::exp(-0.5 * x * x);
+    sum += p.g[i];
+  }
+  for (int i = 0; i <= 2 * kBbiHalf; ++i) p.g[i] /= sum;
+  return "";
+}
+
 int cg_create(const cg_config* cfg, int device, cg_handle** out) {
   if (!cfg || !out) return fail(nullptr, CG_ERR_INVALID, "NULL argument");
   *out = nullptr;
@@ -349,6 +452,12 @@ int cg_create(const cg_config* cfg, int device, cg_handle** out) {
   if (cfg->flag_fir && cfg->fir.mode != 0 &&
       (cfg->fir.delay + cfg->fir.taps < 1 || cfg->fir.delay + cfg->fir.taps > CG_MAX_FIR))
     return fail(nullptr, CG_ERR_INVALID, "fbDelay + fbTaps must be in [1, 64]");
+  BbiParams bbi_p;
+  std::vector<double> bbi_data;
+  if (cfg->bbi.flag) {
+    std::string m = bbi_plan(*cfg, bbi_p, bbi_data);
+    if (!m.empty()) return fail(nullptr, CG_ERR_INVALID, m);
+  }
   int ndev = 0;
   cudaError_t e = cudaGetDeviceCount(&ndev);
   if (e != cudaSuccess || ndev == 0)
@@ -366,6 +475,15 @@ int cg_create(const cg_config* cfg, int device, cg_handle** out) {
   h.P = cfg->ion.n_species > 0 ? cfg->ion.n_species : 1;
   h.sections.assign(cfg->sections, cfg->sections + h.K);
   h.cfg.sections = h.sections.data();
+  if (cfg->bbi.flag) {
+    h.bbi_table.assign(cfg->bbi.table,
+                       cfg->bbi.table + (size_t)cfg->bbi.n_rows * (cfg->bbi.time_domain ? 6 : 11));
+    h.cfg.bbi.table = h.bbi_table.data();
+    h.bbi = bbi_p;
+  } else {
+    h.cfg.bbi.table = nullptr;
+    h.cfg.bbi.n_rows = 0;
+  }
   for (int k = 0; k < h.K; ++k) h.sec_dev_host.push_back(make_section_dev(h.sections[k], cfg->ring));
   h.ring = make_ring_dev(*cfg, h.sections[0]);
   ChainParams& cp = h.chain;
@@ -496,6 +614,23 @@ int cg_create(const cg_config* cfg, int device, cg_handle** out) {
     if (dalloc(&h.d.sr_green, buf.size())) return bail(CG_ERR_OOM, "SR green");
     cudaMemcpy(h.d.sr_green, buf.data(), sizeof(double) * buf.size(), cudaMemcpyHostToDevice);
   }
+  if (h.cfg.bbi.flag) {
+    const BbiParams& p = h.bbi;
+    if (dalloc(&h.d.bbi_w, (size_t)5 * p.nw)) return bail(CG_ERR_OOM, "broadband-impedance wakes");
+    if (!p.td) {
+      double2* X = nullptr;
+      if (dalloc(&X, bbi_data.size() / 2)) return bail(CG_ERR_OOM, "broadband-impedance table");
+      cudaMemcpy(X, bbi_data.data(), sizeof(double) * bbi_data.size(), cudaMemcpyHostToDevice);
+      e = bbi_wake_fd(X, h.cfg.bbi.n_rows, h.d.bbi_w, h.stream);
+      cudaStreamSynchronize(h.stream);
+      dfree(X);
+      if (e != cudaSuccess) return bail(CG_ERR_CUDA, cudaGetErrorString(e));
+    } else {
+      cudaMemcpy(h.d.bbi_w, bbi_data.data(), sizeof(double) * bbi_data.size(),
+                 cudaMemcpyHostToDevice);
+    }
+    if ((e = prepare_bbi(p)) != cudaSuccess) return bail(CG_ERR_CUDA, cudaGetErrorString(e));
+  }
   if ((e = cudaDeviceSynchronize()) != cudaSuccess) return bail(CG_ERR_CUDA, cudaGetErrorString(e));
   *out = H;
   return CG_OK;
@@ -518,7 +653,7 @@ int cg_destroy(cg_handle* H) {
     dfree(h.d.clouds);
   }
   dfree(h.d.cloud_state); dfree(h.d.lr_tab); dfree(h.d.lr_head); dfree(h.d.fir_coeff);
-  dfree(h.d.fir_head); dfree(h.d.sr_green);
+  dfree(h.d.fir_head); dfree(h.d.sr_green); dfree(h.d.bbi_w);
   if (h.stream) cudaStreamDestroy(h.stream);
   if (h.side) cudaStreamDestroy(h.side);
   if (h.side2) cudaStreamDestroy(h.side2);
@@ -707,6 +842,23 @@ int cg_set_beam(cg_handle* H, int M, const int* n_macro, const int* harm, const 
     }
     cudaMemset(d.sr_pot, 0, sizeof(double) * M * B);
   }
+  if (h.cfg.bbi.flag) {
+    const size_t wc = h.bbi.wcap;
+    if (dalloc(&d.bbi_lo, (size_t)M) || dalloc(&d.bbi_hi, (size_t)M) ||
+        dalloc(&d.bbi_amax, 2 * (size_t)M) || dalloc(&d.bbi_cnt, (size_t)M * wc) ||
+        dalloc(&d.bbi_sxy, 2 * (size_t)M * wc) || dalloc(&d.bbi_pot, 6 * (size_t)M * wc) ||
+        dalloc(&d.bbi_win, (size_t)M)) {
+      free_beam(h);
+      return fail(&h, CG_ERR_OOM, "broadband-impedance buffers");
+    }
+    cudaMemset(d.bbi_lo, 0x7f, sizeof(int) * M);  // above every bin
+    cudaMemset(d.bbi_hi, 0xff, sizeof(int) * M);  // -1
+    cudaMemset(d.bbi_amax, 0, sizeof(unsigned long long) * 2 * M);
+    cudaMemset(d.bbi_cnt, 0, sizeof(int) * M * wc);
+    cudaMemset(d.bbi_sxy, 0, sizeof(unsigned long long) * 2 * M * wc);
+    cudaMemset(d.bbi_pot, 0, sizeof(double) * 6 * M * wc);
+    cudaMemset(d.bbi_win, 0, sizeof(int2) * M);
+  }
   cudaError_t e = cudaDeviceSynchronize();
   if (e != cudaSuccess) return cuda_fail(&h, e, "cg_set_beam");
   h.beam_set = true;
@@ -879,6 +1031,29 @@ int cg_synrad(cg_handle* H, int turn) {
   st = launch_ok(h, launch_long(h, kLongSynrad), "synrad");
   return st ? st : check_status(h);
 }
+int cg_bbi_kick(cg_handle* H) {
+  STAGE_PROLOGUE
+  if (!h.cfg.bbi.flag) return fail(&h, CG_ERR_NOT_READY, "runBBIFlag is off");
+  int st = launch_ok(h, launch_bbi(h), "bbi");
+  return st ? st : check_status(h);
+}
+int cg_bbi_profile(cg_handle* H, int j, int* lo, int* n, double* out, int cap) {
+  STAGE_PROLOGUE
+  if (!h.cfg.bbi.flag) return fail(&h, CG_ERR_NOT_READY, "runBBIFlag is off");
+  if (j < 0 || j >= h.M || !lo || !n) return fail(&h, CG_ERR_INVALID, "bad arguments");
+  CG_CUDA(&h, cudaStreamSynchronize(h.stream));
+  int2 w;
+  CG_CUDA(&h, cudaMemcpy(&w, h.d.bbi_win + j, sizeof w, cudaMemcpyDeviceToHost));
+  *lo = w.x;
+  *n = w.y;
+  if (!out) return CG_OK;
+  if (cap < w.y) return fail(&h, CG_ERR_INVALID, "cap below the bunch's bin count");
+  const size_t wc = h.bbi.wcap;
+  for (int q = 0; q < 6 && w.y > 0; ++q)
+    CG_CUDA(&h, cudaMemcpy(out + (size_t)q * cap, h.d.bbi_pot + ((size_t)j * 6 + q) * wc,
+                           sizeof(double) * w.y, cudaMemcpyDeviceToHost));
+  return CG_OK;
+}
 int cg_lr_wake(cg_handle* H) {
   STAGE_PROLOGUE
   if (!h.cfg.flag_lr_wake) return fail(&h, CG_ERR_NOT_READY, "runLongRangeWake is off");
@@ -1047,9 +1222,15 @@ static cudaError_t enqueue_turn(Handle& h) {
   }
   unsigned fl = kLongRF | kLongDrift | kLongLoss;
   if (c.flag_synrad) fl |= kLongSynrad;
-  if (c.flag_lr_wake) fl |= kLongLR;
+  // the LR kick joins the longitudinal kernel unless the broadband impedance
+  // kicks in between (MPBeam.cpp:1084-1085)
+  if (c.flag_lr_wake && !c.bbi.flag) fl |= kLongLR;
   if ((e = launch_long(h, fl))) return e;
   TRACE(h.stream, CG_TRACE_LONG, -1, -1);
+  if (c.bbi.flag) {
+    if ((e = launch_bbi(h))) return e;
+    if (c.flag_lr_wake && (e = launch_lr_kick(h))) return e;
+  }
   if (c.flag_sr_wake) {
     if ((e = launch_sr_wake(h))) return e;
     TRACE(h.stream, CG_TRACE_SR_WAKE, -1, -1);

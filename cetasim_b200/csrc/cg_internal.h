@@ -20,6 +20,21 @@ struct BunchDev {
   double ne, q_macro;
 };
 
+// Broadband impedance (cg_config::bbi), set up at cg_create.
+constexpr int kBbiHalf = 25;  // half width of the K = 51 Gaussian filter (MPBunch.cpp:2376)
+struct BbiParams {
+  int td = 0;                  // 1: time domain (wake table), 0: frequency domain
+  int sim[5] = {0, 0, 0, 0, 0};  // planes Z, Dx, Dy, Qx, Qy
+  int nbins = 0;               // profile bins: 2 n - 1 (frequency), int(rfLen / dz) (time)
+  int nw = 0;                  // wake samples per plane
+  int s0 = 0, s1 = 0;          // the filter runs over the bins [s0, s1)
+  int wcap = 0;                // bins kept per bunch: min(CG_BBI_MAX_BINS, nbins) + 2 kBbiHalf
+  double zmin = 0, dz = 0;     // left edge of bin 0 (frequency domain: its centre), width
+  double energy = 0, beta2 = 0;  // electronBeamEnergy, pow(rBeta, 2)
+  double beta_x = 0, beta_y = 0; // twissBetaX[0], twissBetaY[0]
+  double g[2 * kBbiHalf + 1];  // normalised Gaussian filter kernel
+};
+
 // Ion cloud of one (IP, species): ping-pong buffers of capacity `cap`.
 struct CloudDev {
   double* x[2];
@@ -125,6 +140,15 @@ struct DeviceBufs {
   double* rf_fbk = nullptr;        // loading cavities x M: direct-feedback kicks
   double* rf_work = nullptr;       // work buffers of the cavities' recurrence
   double* rf_info = nullptr;       // M x CG_MAX_CAVITIES x 8: BunchRFModeInfo
+  // broadband impedance
+  double* bbi_w = nullptr;         // 5 x nw wake samples (planes Z, Dx, Dy, Qx, Qy)
+  int* bbi_lo = nullptr;           // M: lowest bin holding a particle (INT_MAX between calls)
+  int* bbi_hi = nullptr;           // M: highest (-1 between calls)
+  unsigned long long* bbi_amax = nullptr;  // M x 2: largest |x|, |y| (bit patterns)
+  int* bbi_cnt = nullptr;          // M x wcap per-bin counts (zero between calls)
+  unsigned long long* bbi_sxy = nullptr;  // M x 2 x wcap fixed-point sums of x, y
+  double* bbi_pot = nullptr;       // M x 6 x wcap: profile and potentials of the last kick
+  int2* bbi_win = nullptr;         // M: first bin and bin count of bbi_pot
   // scratch
   double* scratch = nullptr;
   size_t scratch_bytes = 0;
@@ -162,6 +186,8 @@ struct Handle {
   // walks
   int cbm_cap = 0, cbm_n = 0;  // coupled-bunch mode history: capacity, records made
   double sr_rw_coeff = 0.0;    // short-range resistive-wall coefficient (0: no sectors)
+  BbiParams bbi;               // broadband impedance (cfg.bbi.flag)
+  std::vector<double> bbi_table;  // the copy of cfg.bbi.table
   int pipe_groups = 4;
   // trajectories per walk CTA (8, 16, 32, 64): smaller CTAs spread the
   // walk's FP64 work over more SMs and find room sooner while the kicks and

@@ -139,6 +139,41 @@ int read_bbr(const std::string& path, cg_bbr* b) {
   return CG_OK;
 }
 
+// The broadband-impedance tables (BoardBandImp::ReadInImp, BoardBandImp.cpp:
+// 42-71; MPBeam::GetQuasiWakePoten, MPBeam.cpp:748-775): 5 header lines, then
+// whitespace-separated rows of at least `cols` numbers; empty lines skipped.
+int read_bbi_table(const std::string& path, int cols, cg_bbi* b) {
+  std::ifstream fin(path);
+  if (!fin.is_open()) {
+    g_parse_error = "Error opening file: " + path;
+    return CG_ERR_INVALID;
+  }
+  std::string str;
+  std::vector<double> rows;
+  int line = 0;
+  while (std::getline(fin, str)) {
+    if (line++ < 5) continue;
+    std::istringstream iss(str);
+    std::vector<double> v;
+    for (std::string w; iss >> w;) v.push_back(std::stod(w));
+    if (v.empty()) continue;
+    if ((int)v.size() < cols) {
+      g_parse_error = "line with fewer than " + std::to_string(cols) + " columns in " + path;
+      return CG_ERR_INVALID;
+    }
+    rows.insert(rows.end(), v.begin(), v.begin() + cols);
+  }
+  if (rows.size() < 2 * (size_t)cols) {
+    g_parse_error = "fewer than 2 rows in " + path;
+    return CG_ERR_INVALID;
+  }
+  double* t = (double*)std::malloc(sizeof(double) * rows.size());
+  std::memcpy(t, rows.data(), sizeof(double) * rows.size());
+  b->n_rows = (int)(rows.size() / cols);
+  b->table = t;
+  return CG_OK;
+}
+
 // WakeFunction::RWWakeParaReadIn (WakeFunction.cpp:292-328): a header line,
 // then per sector radius x, radius y, length, beta x, beta y, count, sigma.
 int read_rw_sectors(const std::string& path, cg_rw_sectors* s) {
@@ -175,9 +210,8 @@ int read_rw_sectors(const std::string& path, cg_rw_sectors* s) {
 extern "C" int cg_config_derive(cg_config* cfg);
 extern "C" int cg_lattice_init(const cg_ring* ring, cg_section* sec, int n);
 
-extern "C" int cg_config_from_input(const char* path, cg_config* cfg, int* n_bunches,
-                                    int** n_macro, int** bunch_harm, double** bunch_ne) {
-  if (!path || !cfg || !n_bunches || !n_macro || !bunch_harm || !bunch_ne) return CG_ERR_INVALID;
+static int config_from_input(const char* path, cg_config* cfg, int* n_bunches, int** n_macro,
+                             int** bunch_harm, double** bunch_ne) {
   *n_macro = nullptr;
   *bunch_harm = nullptr;
   *bunch_ne = nullptr;
@@ -263,9 +297,9 @@ extern "C" int cg_config_from_input(const char* path, cg_config* cfg, int* n_bun
       g_parse_error = "runcalSetting must be 2 (MP model)";
       return CG_ERR_UNSUPPORTED;
     }
-    if (flag("runbbiflag") || flag("runspacecharge") || flag("runramping") || flag("drivemodeon") ||
+    if (flag("runspacecharge") || flag("runramping") || flag("drivemodeon") ||
         (has("ioncalscmethod") && flag("ioncalscmethod") == 2)) {
-      g_parse_error = "broadband impedance, space charge, ramping, drive mode and PIC beam-ion "
+      g_parse_error = "space charge, ramping, drive mode and PIC beam-ion "
                       "are outside the tracking path of this library";
       return CG_ERR_UNSUPPORTED;
     }
@@ -390,6 +424,27 @@ extern "C" int cg_config_from_input(const char* path, cg_config* cfg, int* n_bun
         if (st) return st;
       }
     }
+    // broadband impedance (ReadInputSettings.cpp:726-750, defaults of
+    // ReadInputSettings.h:209-214; MPBeam.cpp:856-876 reads the table the
+    // time / frequency flag names)
+    cfg->bbi.flag = flag("runbbiflag");
+    if (cfg->bbi.flag) {
+      cg_bbi& b = cfg->bbi;
+      b.time_domain = has("bbiimpedsimtimeorfreflag") ? flag("bbiimpedsimtimeorfreflag") : 1;
+      for (int i = 0; i < 5; ++i)
+        b.sim[i] = has("bbiimpedsimlandtflag") ? Ii(get("bbiimpedsimlandtflag"), i) : 1;
+      if (b.time_domain != 0 && b.time_domain != 1) {
+        g_parse_error = "wrong setting in BoardBandImpedance namelist";
+        return CG_ERR_INVALID;
+      }
+      const char* key = b.time_domain ? "bbiwakeinput" : "bbiimpedinput";
+      if (!has(key) || get(key).v.empty()) {
+        g_parse_error = std::string("runBBIFlag needs ") + (b.time_domain ? "BBIWakeInput" : "BBIImpedInput");
+        return CG_ERR_INVALID;
+      }
+      int st = read_bbi_table(resolve(base, get(key).v.at(0)), b.time_domain ? 6 : 11, &b);
+      if (st) return st;
+    }
     // derived constants, then the lattice
     int st = cg_config_derive(cfg);
     if (st) return st;
@@ -463,10 +518,26 @@ extern "C" int cg_config_from_input(const char* path, cg_config* cfg, int* n_bun
   return CG_OK;
 }
 
+extern "C" int cg_config_from_input(const char* path, cg_config* cfg, int* n_bunches,
+                                    int** n_macro, int** bunch_harm, double** bunch_ne) {
+  if (!path || !cfg || !n_bunches || !n_macro || !bunch_harm || !bunch_ne) return CG_ERR_INVALID;
+  std::memset(cfg, 0, sizeof *cfg);
+  int st = config_from_input(path, cfg, n_bunches, n_macro, bunch_harm, bunch_ne);
+  if (st != CG_OK && cfg->bbi.table) {
+    std::free((void*)cfg->bbi.table);
+    cfg->bbi.table = nullptr;
+  }
+  return st;
+}
+
 extern "C" void cg_config_free(cg_config* cfg, int* n_macro, int* bunch_harm, double* bunch_ne) {
   if (cfg && cfg->sections) {
     std::free((void*)cfg->sections);
     cfg->sections = nullptr;
+  }
+  if (cfg && cfg->bbi.table) {
+    std::free((void*)cfg->bbi.table);
+    cfg->bbi.table = nullptr;
   }
   std::free(n_macro);
   std::free(bunch_harm);

@@ -575,8 +575,8 @@ __global__ void __launch_bounds__(NT, MINB) k_ion_kick_run(double* __restrict__ 
 // (the register budget) and items per CTA (1 = k_ion_kick, one tile or half
 // of one per CTA; more = k_ion_kick_run).
 static const int kKickShapes[][3] = {{256, 3, 1}, {256, 4, 1}, {128, 4, 1}, {128, 6, 1},
-                                     {256, 3, 4}, {128, 6, 4}};
-constexpr int kKickVariants = 6;
+                                     {256, 3, 4}, {128, 6, 4}, {128, 6, 8}, {256, 3, 8}};
+constexpr int kKickVariants = 8;
 
 cudaError_t launch_ion_kick_variant(Handle& h, int k, int v, int tile_a, int tile_b,
                                     cudaStream_t s) {
@@ -606,6 +606,14 @@ cudaError_t launch_ion_kick_variant(Handle& h, int k, int v, int tile_a, int til
     case 5:
       k_ion_kick_run<128, 6, 4><<<(2 * nt + 3) / 4, 128, 0, s>>>(
           h.d.c, h.npad, h.d.surv, h.d.tile_bunch, h.d.bunch, rec, rp, h.P, tile_a, 2 * nt);
+      break;
+    case 6:
+      k_ion_kick_run<128, 6, 8><<<(2 * nt + 7) / 8, 128, 0, s>>>(
+          h.d.c, h.npad, h.d.surv, h.d.tile_bunch, h.d.bunch, rec, rp, h.P, tile_a, 2 * nt);
+      break;
+    case 7:
+      k_ion_kick_run<256, 3, 8><<<(nt + 7) / 8, 256, 0, s>>>(
+          h.d.c, h.npad, h.d.surv, h.d.tile_bunch, h.d.bunch, rec, rp, h.P, tile_a, nt);
       break;
     default:
       k_ion_kick<256, 3><<<nt, 256, 0, s>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch, h.d.bunch,

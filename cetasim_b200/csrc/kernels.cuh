@@ -12,7 +12,16 @@ enum : int {
   kStatusIonBirth = 8,
   kStatusSurrogateWait = 16,  // a tensor-core completion wait gave up
   kStatusGaussCut = 64,       // an initial-distribution draw found no accepted sample
+  kStatusBbiRange = 128,      // a particle outside the broadband-impedance profile
+  kStatusBbiWide = 256,       // a bunch over more than CG_BBI_MAX_BINS profile bins
 };
+
+// broadband impedance (bbi.cu)
+cudaError_t launch_bbi(Handle& h);
+size_t bbi_conv_smem(const BbiParams& p);
+cudaError_t prepare_bbi(const BbiParams& p);
+// w (5 x (2n - 1)) from the impedances X (5 x n, device) on stream st
+cudaError_t bbi_wake_fd(const double2* d_X, int n, double* d_w, cudaStream_t st);
 
 cudaError_t launch_moments(Handle& h, int k);
 cudaError_t launch_map(Handle& h, int k);

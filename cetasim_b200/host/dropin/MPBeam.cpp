@@ -20,10 +20,9 @@
 // (transmission < 0.5 at Bunch.cpp:194-197, ion overflow at LIP.cpp:1043-1048).
 //
 // Not built here (paths outside the library's scope, kept as the reference's
-// declarations only): broadband impedance, space charge, ramping, drive
-// mode, the per-bunch TBT and ion-dump writers (MPBeamDataPrintPerTurn,
-// SSIonDataPrint), the cavity transient printout of InitialcavityResonator
-// and the Haissinski solver.
+// declarations only): space charge, ramping, drive mode, the per-bunch TBT
+// and ion-dump writers (MPBeamDataPrintPerTurn, SSIonDataPrint), the cavity
+// transient printout of InitialcavityResonator and the Haissinski solver.
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -33,6 +32,7 @@
 #include <iomanip>
 #include <iostream>
 #include <map>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -50,6 +50,7 @@ struct GpuBeam {
   std::vector<int> n_macro, harm;
   std::vector<double> ne;
   std::vector<cg_bunch_moments> mom;
+  std::vector<double> bbi_table;  // the broadband-impedance table cfg.bbi points at
 };
 
 std::map<const MPBeam*, GpuBeam>& registry() {
@@ -192,11 +193,43 @@ void build_config(GpuBeam& g, const ReadInputSettings& in, const LatticeInterAct
   c.flag_lr_wake = run->lRWakeFlag;
   c.flag_sr_wake = run->sRWakeFlag;
   c.flag_fir = run->fIRBunchByBunchFeedbackFlag;
-  if (run->bBImpFlag || run->spaceChargeFlag || run->rampFlag || in.driveMode->driveModeOn ||
+  if (run->spaceChargeFlag || run->rampFlag || in.driveMode->driveModeOn ||
       (run->beamIonFlag && in.ringIonEffPara->ionCalSCMethod == 2)) {
-    std::cerr << "broadband impedance, space charge, ramping, drive mode and PIC beam-ion are "
-                 "outside the GPU tracking path" << std::endl;
+    std::cerr << "space charge, ramping, drive mode and PIC beam-ion are outside the GPU "
+                 "tracking path" << std::endl;
     exit(0);
+  }
+  if (run->bBImpFlag) {
+    // the table MPBeam::Run reads (MPBeam.cpp:856-876): the impedance file of
+    // BoardBandImp::ReadInImp (BoardBandImp.cpp:42-71) or the wake file of
+    // MPBeam::GetQuasiWakePoten (MPBeam.cpp:748-775); 5 header lines, then
+    // whitespace-separated rows
+    const auto* bb = in.ringBBImp;
+    c.bbi.flag = 1;
+    c.bbi.time_domain = bb->timeDomain;
+    for (int i = 0; i < 5; ++i) c.bbi.sim[i] = bb->impedSimFlag[i];
+    const std::string file = bb->timeDomain ? bb->wakeInput : bb->impedInput;
+    const size_t cols = bb->timeDomain ? 6 : 11;
+    std::ifstream fin(file);
+    if (!fin.is_open()) {
+      std::cerr << "Error opening file: " << file << std::endl;
+      exit(0);
+    }
+    std::string line;
+    for (int n = 0; std::getline(fin, line);) {
+      if (n++ < 5) continue;
+      std::istringstream iss(line);
+      std::vector<double> v;
+      for (std::string w; iss >> w;) v.push_back(std::stod(w));
+      if (v.empty()) continue;
+      if (v.size() < cols) {
+        std::cerr << "line with fewer than " << cols << " columns in " << file << std::endl;
+        exit(0);
+      }
+      g.bbi_table.insert(g.bbi_table.end(), v.begin(), v.begin() + cols);
+    }
+    c.bbi.n_rows = (int)(g.bbi_table.size() / cols);
+    c.bbi.table = g.bbi_table.data();
   }
   c.n_turns = run->nTurns;
   c.bunch_info_print_interval = run->bunchInfoPrintInterval;
@@ -540,6 +573,15 @@ void MPBeam::BeamSynRadDamping(const ReadInputSettings& inputParameter,
   (void)inputParameter;
   (void)latticeInterActionPoint;
   check(g, cg_synrad(g.h, currentTurnNum), "BeamSynRadDamping");
+}
+
+void MPBeam::BBImpBeamInteraction(const ReadInputSettings& inputParameter, const BoardBandImp& boardBandImp,
+                                  const LatticeInterActionPoint& latticeInterActionPoint) {
+  GpuBeam& g = gpu(this);
+  (void)inputParameter;
+  (void)boardBandImp;
+  (void)latticeInterActionPoint;
+  check(g, cg_bbi_kick(g.h), "BBImpBeamInteraction");
 }
 
 void MPBeam::LRWakeBeamIntaction(const ReadInputSettings& inputParameter, WakeFunction& wakefunction,

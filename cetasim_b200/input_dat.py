@@ -246,9 +246,24 @@ def write_case(d: str, wl: Workload, n_turns: int = 1, print_interval: int | Non
         f"runFIRBunchByBunchFeedbackFlag = {int(cfg.flag_fir)}",
         f"runLongRangeWake = {int(cfg.flag_lr_wake)}",
         f"runShortRangeWake = {int(cfg.flag_sr_wake)}",
-        "runBBIFlag = 0", "runRamping = 0", "runSpaceCharge = 0 32 32 33",
+        f"runBBIFlag = {int(cfg.bbi.flag)}", "runRamping = 0", "runSpaceCharge = 0 32 32 33",
         f"runRandomSeed = {int(cfg.seed if seed is None else seed)}",
     ]
+    if cfg.bbi.flag:
+        # the broadband-impedance table as the file the reference reads
+        # (5 header lines, BoardBandImp.cpp:53-58, MPBeam.cpp:762-767)
+        td = int(cfg.bbi.time_domain)
+        fname = "bbi_wake.dat" if td else "bbi_imped.dat"
+        with open(os.path.join(d, fname), "w") as fh:
+            fh.write("table\n" * 5)
+            for row in np.asarray(wl.bbi_table):
+                fh.write(" ".join(_fmt(v) for v in row) + "\n")
+        lines += [
+            f"bbiImpedSimTimeOrFreFlag = {td}",
+            "bbiImpedSimLandTFlag = " + " ".join(str(int(cfg.bbi.sim[i])) for i in range(5)),
+            "bbiBunchBinNumberZ = 100",
+            ("bbiWakeInput = " if td else "bbiImpedInput = ") + fname,
+        ]
     lines += list(extra)
     with open(os.path.join(d, "input.dat"), "w") as fh:
         fh.write("\n".join(lines) + "\n")
@@ -281,8 +296,16 @@ def load_case(path: str, name: str = "input", gen=None, lib=None) -> Workload:
     K = cfg.n_sections
     secs = (_abi.Section * K)()
     C.memmove(secs, cfg.sections, C.sizeof(_abi.Section) * K)
+    bbi = None
+    if cfg.bbi.flag:
+        cols = 6 if cfg.bbi.time_domain else 11
+        bbi = np.ctypeslib.as_array(cfg.bbi.table, shape=(cfg.bbi.n_rows * cols,)).copy()
+        sim = [cfg.bbi.sim[i] for i in range(5)]
     L.cg_config_free(C.byref(cfg), nm, hm, ne)  # the parser's arrays (sections copied above)
     cfg.sections = C.cast(secs, C.POINTER(_abi.Section))
     if gen is None:
         gen = (cfg.bunch_emit_x, cfg.bunch_emit_y, cfg.bunch_sigma_z, cfg.bunch_sigma_dp)
-    return Workload(name, cfg, secs, n_macro, harm, nev, gen)
+    wl = Workload(name, cfg, secs, n_macro, harm, nev, gen)
+    if bbi is not None:
+        wl.set_bbi(bbi, cfg.bbi.time_domain, sim)
+    return wl

@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define CG_ABI_VERSION 2
+#define CG_ABI_VERSION 3
 #define CG_MAX_SPECIES 8
 #define CG_MAX_CAVITIES 4
 #define CG_MAX_RESONATORS 16
@@ -140,6 +140,23 @@ typedef struct cg_rw_sectors {
   double sigma[CG_MAX_RW_SECTORS];  /* [S/m] */
 } cg_rw_sectors;
 
+/* Broadband impedance (ReadInputSettings.cpp:726-750, BoardBandImp::ReadInImp
+ * BoardBandImp.cpp:42-115, MPBeam::GetQuasiWakePoten MPBeam.cpp:748-823).
+ * time_domain 0 (bbiImpedSimTimeOrFreFlag 0): table holds the impedance file's
+ * rows after its 5 header lines, 11 columns each (f, then the real and
+ * imaginary columns of the five impedances as BoardBandImp.cpp:64-70 reads
+ * them).  time_domain 1: table holds the wake file's rows after its 5 header
+ * lines, 6 columns each (z, Wz, WDx, WDy, WQx, WQy as in the file, before the
+ * sign change and folding of MPBeam.cpp:772-801).  sim[] is
+ * bbiImpedSimLandTFlag (Z, Dx, Dy, Qx, Qy).  Row-major; cg_create copies it. */
+typedef struct cg_bbi {
+  int flag;                      /* runBBIFlag */
+  int time_domain;               /* bbiImpedSimTimeOrFreFlag */
+  int sim[5];                    /* bbiImpedSimLandTFlag */
+  int n_rows;
+  const double* table;           /* n_rows x (time_domain ? 6 : 11) */
+} cg_bbi;
+
 typedef struct cg_bbr {
   int n;
   double l_rs[CG_MAX_RESONATORS], l_q[CG_MAX_RESONATORS], l_omega[CG_MAX_RESONATORS];
@@ -190,6 +207,7 @@ typedef struct cg_config {
                                     long-range wake (n = 0: none) */
   cg_rw_sectors sr_rw;           /* SRWPipeGeoInput: resistive-wall sectors of the
                                     short-range wake (n = 0: none) */
+  cg_bbi bbi;                    /* broadband impedance (flag 0: off) */
 } cg_config;
 
 /* Per-bunch moments, the fields MPBunch::GetMPBunchRMS sets
@@ -235,8 +253,8 @@ int cg_lattice_init(const cg_ring* ring, cg_section* sections, int n_sections);
  * per-bunch macroparticle counts, harmonic numbers and electrons per bunch.
  * The arrays and cfg->sections are allocated by the library; release them
  * with cg_config_free.  Keys outside the MP tracking path are accepted and
- * ignored, except settings this library does not implement (runBBIFlag,
- * runSpaceCharge, ionCalSCMethod 2, driveModeOn, runRamping),
+ * ignored, except settings this library does not implement (runSpaceCharge,
+ * ionCalSCMethod 2, driveModeOn, runRamping),
  * which return CG_ERR_UNSUPPORTED.  runCBMGR with runGrowthRateFittingStart /
  * End fills run_cbmgr and the fit window (checked as ReadInputSettings.cpp:
  * 946-956).  Optional keys beyond the reference: bunchMacroEleNumPerBunchList
@@ -318,6 +336,21 @@ int cg_energy_loss(cg_handle* h);
 /* MPBeam::BeamSynRadDamping (Bunch.cpp:940-1044); the noise of turn `turn`
  * is Philox(seed, turn, particle). */
 int cg_synrad(cg_handle* h, int turn);
+/* MPBeam::BBImpBeamInteraction (MPBeam.cpp:1321-1346): the broadband
+ * impedance kick of every bunch with charge, in the frequency domain
+ * (MPBunch::BBImpBunchInteraction, MPBunch.cpp:2143-2346) or the time domain
+ * (MPBunch::BBImpBunchInteractionTD, MPBunch.cpp:2029-2141), with the
+ * smoothed profiles of MPBunch.cpp:2349-2414.  CG_ERR_INVALID when a
+ * particle falls outside the profile's bins or a bunch spans more than
+ * CG_BBI_MAX_BINS of them. */
+#define CG_BBI_MAX_BINS 4096
+int cg_bbi_kick(cg_handle* h);
+/* The longitudinal profile and the five wake potentials of bunch j from the
+ * last cg_bbi_kick over its bins [lo, lo + n): profile as the reference
+ * holds it after smoothing (profileForBunchBBImp / densityProfile) and the
+ * potentials (wakePotenFromBBI; in the time domain the five temp[] sums).
+ * out = 6 x cap doubles, row q at out + q * cap; n <= cap. */
+int cg_bbi_profile(cg_handle* h, int j, int* lo, int* n, double* out, int cap);
 /* MPBeam::LRWakeBeamIntaction (MPBeam.cpp:3232-3349). */
 int cg_lr_wake(cg_handle* h);
 /* MPBeam::SRWakeBeamIntaction (MPBeam.cpp:2117-2123 ->

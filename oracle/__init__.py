@@ -2,8 +2,9 @@
 the CPU restatement of the reference's MP tracking path (see oracle.c).
 
 Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg use this
-module, and only as the checker.  Parity unpinned except for w(z), which is
-pinned against the reference's compiled Faddeeva.cpp (tests/golden).
+module, and only as the checker.  The restatement is pinned against the
+reference's own sources built in oracle/_ref (oracle/ref.py) and against the
+fixtures they generated (tests/golden).
 """
 from __future__ import annotations
 
@@ -170,6 +171,19 @@ class OracleBeam:
 
     def SRWakeBeamIntaction(self, turn):
         self._check(self.lib.or_sr_wake(self.s, turn))
+
+    def BBImpBeamInteraction(self):
+        self._check(self.lib.or_bbi(self.s))
+
+    def bbi_profile(self, j):
+        """6 x nbins: bunch j's smoothed charge profile and the potentials of
+        the planes Z, Dx, Dy, Qx, Qy over all profile bins, from the last
+        BBImpBeamInteraction."""
+        nb = C.c_int()
+        self._check(self.lib.or_bbi_profile(self.s, j, C.byref(nb), None))
+        out = np.empty((6, nb.value))
+        self._check(self.lib.or_bbi_profile(self.s, j, C.byref(nb), _p(out)))
+        return out
 
     def FIRBunchByBunchFeedback(self, turn):
         self._check(self.lib.or_fir(self.s, turn))

@@ -11,8 +11,10 @@
  * draw (the reference itself seeds std::mt19937 from std::random_device, so
  * it is only reproducible statistically).
  *
- * Parity unpinned: the reference's tracking sources need GSL and FFTW and do
- * not build here; only w(z) (faddeeva_q.c) is pinned against the reference.
+ * Pinned against the reference itself: oracle/Makefile builds the
+ * reference's own sources (with a GSL / FFTW interface subset, oracle/
+ * ref_shim) into oracle/_ref, and the tests compare this restatement with it
+ * stage by stage and against fixtures it generated (tests/golden).
  */
 #include "oracle.h"
 #include <math.h>
@@ -235,12 +237,21 @@ struct or_state {
   double* rf_fb;
   double* rf_zmin; /* [M] zMinCurrentTurn, zMaxCurrentTurn of the RF step */
   double* rf_zmax;
+  /* broadband impedance (MPBeam.cpp:853-876) */
+  int bbi_n;        /* impedance samples (frequency domain) / wake samples (time domain) */
+  int bbi_nbins;    /* profile bins: 2 n - 1 / int(rfLen / dz) */
+  double bbi_dz, bbi_zmin;
+  int bbi_s0, bbi_s1; /* the filtered bins */
+  double* bbi_imp;  /* frequency domain [5][n][2]: Z, Dx, Dy, Qx, Qy (BoardBandImp.cpp:64-70) */
+  double* bbi_wake; /* time domain [5][n]: wz (folded), wDx, wDy, wQx, wQy */
+  double* bbi_out;  /* [M][6][nbins]: smoothed charge profile, then the five potentials */
   char err[256];
 };
 
 const char* or_last_error(or_state* s) { return s->err; }
 
 static void res_init(or_state* s);
+static int bbi_init(or_state* s);
 
 /* WakeFunction::GetBBRWakeFun (WakeFunction.cpp:655-721) */
 static void bbr_wake(const cg_bbr* w, double beta_ip_x, double beta_ip_y, double tau, double out[3]) {
@@ -306,6 +317,10 @@ or_state* or_create(const cg_config* cfg, int M, const int* n_macro, const int* 
   s->rf_zmin = (double*)calloc(M, sizeof(double));
   s->rf_zmax = (double*)calloc(M, sizeof(double));
   res_init(s);
+  if (cfg->bbi.flag && bbi_init(s)) {
+    or_destroy(s);
+    return NULL;
+  }
   /* WakeFunction::InitialLRWake (WakeFunction.cpp:49-202) */
   if (cfg->flag_lr_wake) {
     int turns = cfg->lr_turns;
@@ -344,6 +359,7 @@ void or_destroy(or_state* s) {
   free(s->cloud); free(s->b); free(s->sec); free(s->rec); free(s->lr_tab); free(s->lr_hist);
   free(s->fir_hist);
   free(s->rf_info); free(s->rf_fb); free(s->rf_zmin); free(s->rf_zmax);
+  free(s->bbi_imp); free(s->bbi_wake); free(s->bbi_out);
   free(s);
 }
 
@@ -1329,6 +1345,7 @@ int or_run_turns(or_state* s, int turn0, int n_turns) {
     or_longi_drift(s);
     or_energy_loss(s);
     if (c->flag_synrad) or_synrad(s, n);
+    if (c->bbi.flag && (st = or_bbi(s))) return st;
     if (c->flag_lr_wake && (st = or_lr_wake(s))) return st;
     if (c->flag_sr_wake) or_sr_wake(s, n);
     or_beam_rms(s, 0);
@@ -1336,6 +1353,285 @@ int or_run_turns(or_state* s, int turn0, int n_turns) {
     if ((st = or_mark_lost(s, NULL))) return st;
     or_beam_rms(s, 0);
   }
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Broadband impedance: MPBeam::BBImpBeamInteraction (MPBeam.cpp:1321-1346)   */
+
+/* BoardBandImp::ReadInImp (BoardBandImp.cpp:42-115) and
+   MPBeam::GetQuasiWakePoten (MPBeam.cpp:748-801): the set-up of the tables.
+   The table is borrowed from the caller; what is needed is copied. */
+static int bbi_init(or_state* s) {
+  const cg_bbi* b = &s->cfg.bbi;
+  const cg_ring* r = &s->cfg.ring;
+  const double* t = b->table;
+  int n = b->n_rows;
+  s->cfg.bbi.table = NULL;
+  if (n < 2 || !t) return 1;
+  double rfLen = r->t0 / r->harmonics * C_LIGHT; /* MPBunch.cpp:2355, 2035 */
+  s->bbi_n = n;
+  if (!b->time_domain) {
+    double freqMax = t[(size_t)(n - 1) * 11];
+    double dt = 1.0 / (2 * freqMax);
+    double dz = dt * C_LIGHT * r->r_beta;
+    double zMax = dz * (n - 1);
+    s->bbi_dz = dz;
+    s->bbi_zmin = -zMax;
+    s->bbi_nbins = 2 * n - 1;
+    /* MPBunch.cpp:2360-2361 */
+    double zMinBin = -zMax, dzBin = dz;
+    s->bbi_s0 = (int)((-rfLen / 2. - zMinBin + dzBin / 2) / dzBin);
+    s->bbi_s1 = (int)((rfLen / 2. - zMinBin + dzBin / 2) / dzBin);
+    if (s->bbi_s0 < 0 || s->bbi_s1 > s->bbi_nbins) return 1;
+    s->bbi_imp = (double*)malloc(sizeof(double) * 5 * n * 2);
+    for (int k = 0; k < n; ++k) {
+      const double* c = t + (size_t)k * 11;
+      double re[5] = {c[1], -c[7], -c[8], -c[9], -c[10]};
+      double im[5] = {-c[6], -c[2], -c[3], -c[4], -c[5]};
+      for (int q = 0; q < 5; ++q) {
+        s->bbi_imp[((size_t)q * n + k) * 2] = re[q];
+        s->bbi_imp[((size_t)q * n + k) * 2 + 1] = im[q];
+      }
+    }
+  } else {
+    int cen = 0;
+    for (int i = 0; i < n; ++i)
+      if (t[(size_t)i * 6] == 0) cen = i;
+    if (2 * cen > n) return 1;
+    double* w = (double*)calloc((size_t)5 * n, sizeof(double));
+    double* tmp = (double*)malloc(sizeof(double) * n);
+    for (int i = 0; i < n; ++i) tmp[i] = -1 * t[(size_t)i * 6 + 1];
+    w[0] = tmp[cen];
+    for (int i = 1; i < cen; i++) w[i] = tmp[cen + i] + tmp[cen - i];
+    for (int i = cen; i < n - cen; i++) w[i] = tmp[cen + i];
+    for (int i = n - cen; i < n; i++) w[i] = 0.0;
+    for (int q = 1; q < 5; ++q)
+      for (int i = 0; i < n; ++i) w[(size_t)q * n + i] = -1 * t[(size_t)i * 6 + 1 + q];
+    free(tmp);
+    s->bbi_wake = w;
+    double z0 = t[0];
+    double p0 = z0 - z0, p1 = t[6] - z0;
+    s->bbi_dz = fabs(p1 - p0);
+    if (!(s->bbi_dz > 0)) return 1;
+    s->bbi_zmin = -1 * rfLen / 2;
+    s->bbi_nbins = (int)(1 * rfLen / s->bbi_dz);
+    if (s->bbi_nbins < 1) return 1;
+    s->bbi_s0 = 0;
+    s->bbi_s1 = s->bbi_nbins;
+  }
+  s->bbi_out = (double*)calloc((size_t)s->M * 6 * s->bbi_nbins, sizeof(double));
+  return 0;
+}
+
+/* MPBunch::GetSmoothedBunchProfileGassionFilter (MPBunch.cpp:2373-2414) over
+   x[0..N): GSL's Gaussian filter (gsl_filter_gaussian, GSL 2.8; K = 51,
+   alpha = 10, end-value padding; kernel exp(-(alpha k / H)^2 / 2), |k| <= H =
+   25, normalised), then the filtered profile scaled to the raw one's sum. */
+static void bbi_gauss_filter(double* x, int N) {
+  const int H = 25;
+  const double alpha = 10.0;
+  double g[51], gs = 0;
+  for (int i = 0; i <= 2 * H; ++i) {
+    double a = alpha * (double)(i - H) / (double)H;
+    g[i] = exp(-0.5 * a * a);
+    gs += g[i];
+  }
+  for (int i = 0; i <= 2 * H; ++i) g[i] /= gs;
+  double* y = (double*)malloc(sizeof(double) * (N > 0 ? N : 1));
+  for (int i = 0; i < N; ++i) {
+    double acc = 0;
+    for (int k = -H; k <= H; ++k) {
+      int j = i + k;
+      j = j < 0 ? 0 : (j >= N ? N - 1 : j);
+      acc += g[k + H] * x[j];
+    }
+    y[i] = acc;
+  }
+  double sum0 = 0, sum1 = 0;
+  for (int i = 0; i < N; i++) {
+    sum0 += x[i];
+    sum1 += y[i];
+    x[i] = y[i];
+  }
+  sum0 = sum0 / sum1;
+  for (int i = 0; i < N; i++) x[i] *= sum0;
+  free(y);
+}
+
+/* FFTW's r2c of length N (out[0..N/2]) and c2r (unnormalised, Hermitian
+   input, imaginary parts of out[0] ignored), as direct sums. */
+static void bbi_r2c(const double* in, int N, double* out /* (N/2+1) x 2 */) {
+  for (int k = 0; k <= N / 2; ++k) {
+    double re = 0, im = 0;
+    long long r = 0;
+    for (int j = 0; j < N; ++j) {
+      double a = 2 * M_PI * (double)r / N;
+      re += in[j] * cos(a);
+      im -= in[j] * sin(a);
+      r += k;
+      if (r >= N) r -= N;
+    }
+    out[2 * k] = re;
+    out[2 * k + 1] = im;
+  }
+}
+static void bbi_c2r(const double* in /* (N/2+1) x 2 */, int N, double* out) {
+  for (int m = 0; m < N; ++m) {
+    double acc = in[0];
+    long long r = 0;
+    for (int k = 1; k <= (N - 1) / 2; ++k) {
+      r += m;
+      if (r >= N) r -= N;
+      double a = 2 * M_PI * (double)r / N;
+      acc += 2 * (in[2 * k] * cos(a) - in[2 * k + 1] * sin(a));
+    }
+    if (N % 2 == 0) acc += in[N] * ((m % 2) ? -1.0 : 1.0);
+    out[m] = acc;
+  }
+}
+
+/* MPBunch::BBImpBunchInteraction (MPBunch.cpp:2143-2346) */
+static int bbi_bunch_fd(or_state* s, int j) {
+  or_bunch* b = &s->b[j];
+  const cg_bbi* f = &s->cfg.bbi;
+  double E = s->cfg.ring.electron_energy, rBeta = s->cfg.ring.r_beta;
+  double zMinBin = s->bbi_zmin, dzBin = s->bbi_dz;
+  int N = s->bbi_nbins, n = s->bbi_n;
+  int any = 0;
+  for (int q = 0; q < 5; ++q) any = any || f->sim[q];
+  if (!any) return 0;
+  double* prof = (double*)calloc(N, sizeof(double));
+  double* spec = (double*)malloc(sizeof(double) * 2 * (N / 2 + 1));
+  double* c2r = (double*)malloc(sizeof(double) * 2 * (N / 2 + 1));
+  double* temp = (double*)malloc(sizeof(double) * N);
+  int* bin = (int*)malloc(sizeof(int) * (b->n > 0 ? b->n : 1));
+  double* out = s->bbi_out + (size_t)j * 6 * N;
+  int st = 0;
+  for (int i = 0; i < b->n; i++) {
+    double t = (b->c[4][i] - zMinBin + dzBin / 2) / dzBin;
+    if (!(t > -1.0 && t < (double)N)) { st = CG_ERR_INVALID; goto done; }
+    bin[i] = (int)t;
+    prof[bin[i]] += b->q_macro * E_CHARGE / dzBin * C_LIGHT;
+  }
+  bbi_gauss_filter(prof + s->bbi_s0, s->bbi_s1 - s->bbi_s0);
+  memcpy(out, prof, sizeof(double) * N);
+  bbi_r2c(prof, N, spec);
+  /* planes in the reference's order: Z (0), Qx (3), Qy (4), Dx (1), Dy (2) */
+  const int order[5] = {0, 3, 4, 1, 2};
+  for (int oi = 0; oi < 5; ++oi) {
+    int q = order[oi];
+    if (!f->sim[q]) continue;
+    if (q == 1 || q == 2) {
+      /* the dipole profiles (MPBunch.cpp:2259-2275) */
+      memset(prof, 0, sizeof(double) * N);
+      for (int i = 0; i < b->n; i++)
+        prof[bin[i]] += b->q_macro * E_CHARGE / dzBin * C_LIGHT * b->c[q == 1 ? 0 : 2][i];
+      bbi_gauss_filter(prof + s->bbi_s0, s->bbi_s1 - s->bbi_s0);
+      bbi_r2c(prof, N, spec);
+    }
+    for (int k = 0; k < n; ++k) {
+      double pr = spec[2 * k], pi = spec[2 * k + 1];
+      double zr = s->bbi_imp[((size_t)q * n + k) * 2], zi = s->bbi_imp[((size_t)q * n + k) * 2 + 1];
+      double vr = pr * zr - pi * zi, vi = pr * zi + pi * zr;
+      if (q != 0) { double tr = -vi; vi = vr; vr = tr; } /* times li */
+      c2r[2 * k] = vr;
+      c2r[2 * k + 1] = vi;
+    }
+    bbi_c2r(c2r, N, temp);
+    double* w = out + (size_t)(1 + q) * N;
+    for (int i = 0; i < N; i++) w[i] = (q == 0 ? -temp[i] : temp[i]) / N;
+    for (int i = 0; i < b->n; i++) {
+      double v = w[bin[i]];
+      switch (q) {
+        case 0: b->c[5][i] += v / E / pow(rBeta, 2); break;
+        case 3: b->c[1][i] += v / E / pow(rBeta, 2) * b->c[0][i] / s->sec[0].beta_x; break;
+        case 4: b->c[3][i] += v / E / pow(rBeta, 2) * b->c[2][i] / s->sec[0].beta_y; break;
+        case 1: b->c[1][i] += v / E / pow(rBeta, 2) / s->sec[0].beta_x; break;
+        case 2: b->c[3][i] += v / E / pow(rBeta, 2) / s->sec[0].beta_y; break;
+      }
+    }
+  }
+done:
+  free(prof); free(spec); free(c2r); free(temp); free(bin);
+  return st;
+}
+
+/* MPBunch::BBImpBunchInteractionTD (MPBunch.cpp:2029-2141).  The reference
+   reads the wake at tij = nBinWake as well (its break test is tij >
+   nBinWake, one past the table); the sum here stops at the table's end. */
+static int bbi_bunch_td(or_state* s, int j) {
+  or_bunch* b = &s->b[j];
+  const cg_bbi* f = &s->cfg.bbi;
+  double E = s->cfg.ring.electron_energy, rBeta = s->cfg.ring.r_beta;
+  double zMinBin = s->bbi_zmin, dzBin = s->bbi_dz;
+  int N = s->bbi_nbins, nw = s->bbi_n;
+  double* dens = (double*)calloc(N, sizeof(double));
+  int* cnt = (int*)calloc(N, sizeof(int));
+  double* ax = (double*)calloc(N, sizeof(double));
+  double* ay = (double*)calloc(N, sizeof(double));
+  int* bin = (int*)malloc(sizeof(int) * (b->n > 0 ? b->n : 1));
+  double* out = s->bbi_out + (size_t)j * 6 * N;
+  const double* w = s->bbi_wake;
+  int st = 0;
+  for (int i = 0; i < b->n; i++) {
+    double t = (b->c[4][i] - zMinBin) / dzBin;
+    if (!(t > -1.0 && t < (double)N)) { st = CG_ERR_INVALID; goto done; }
+    bin[i] = (int)t;
+    cnt[bin[i]]++;
+    dens[bin[i]] += b->q_macro * E_CHARGE;
+  }
+  bbi_gauss_filter(dens, N);
+  memcpy(out, dens, sizeof(double) * N);
+  for (int i = 0; i < b->n; i++) {
+    if (b->surv[i] != 0) continue;
+    ax[bin[i]] += b->c[0][i];
+    ay[bin[i]] += b->c[2][i];
+  }
+  for (int i = 0; i < N; i++) {
+    if (cnt[i] == 0) { ax[i] = 0; ay[i] = 0; }
+    else { ax[i] /= cnt[i]; ay[i] /= cnt[i]; }
+  }
+  for (int i = 0; i < N; i++) {
+    double tp[5] = {0, 0, 0, 0, 0};
+    for (int jj = i; jj < N; jj++) {
+      int tij = jj - i;
+      if (tij >= nw) break;
+      if (f->sim[0]) tp[0] -= w[tij] * dens[jj];
+      if (f->sim[1]) tp[1] -= w[nw + tij] * dens[jj] * ax[jj];
+      if (f->sim[2]) tp[2] -= w[2 * nw + tij] * dens[jj] * ay[jj];
+      if (f->sim[3]) tp[3] -= w[3 * nw + tij] * dens[jj];
+      if (f->sim[4]) tp[4] -= w[4 * nw + tij] * dens[jj];
+    }
+    for (int q = 0; q < 5; ++q) out[(size_t)(1 + q) * N + i] = tp[q];
+  }
+  for (int i = 0; i < b->n; i++) {
+    const double* tp = out + N + bin[i];
+    if (f->sim[0]) b->c[5][i] += tp[0] / E / pow(rBeta, 2);
+    if (f->sim[1]) b->c[1][i] += tp[N] / E / pow(rBeta, 2) / s->sec[0].beta_x;
+    if (f->sim[2]) b->c[3][i] += tp[2 * N] / E / pow(rBeta, 2) / s->sec[0].beta_y;
+    if (f->sim[3]) b->c[1][i] += tp[3 * N] / E / pow(rBeta, 2) / s->sec[0].beta_x * b->c[0][i];
+    if (f->sim[4]) b->c[3][i] += tp[4 * N] / E / pow(rBeta, 2) / s->sec[0].beta_y * b->c[2][i];
+  }
+done:
+  free(dens); free(cnt); free(ax); free(ay); free(bin);
+  return st;
+}
+
+int or_bbi(or_state* s) {
+  if (!s->cfg.bbi.flag) return CG_ERR_NOT_READY;
+  for (int j = 0; j < s->M; ++j) {
+    if (s->b[j].q_macro == 0) continue; /* MPBeam.cpp:1335 */
+    int st = s->cfg.bbi.time_domain ? bbi_bunch_td(s, j) : bbi_bunch_fd(s, j);
+    if (st) return st;
+  }
+  return 0;
+}
+
+int or_bbi_profile(or_state* s, int j, int* nbins, double* out) {
+  if (!s->cfg.bbi.flag) return CG_ERR_NOT_READY;
+  *nbins = s->bbi_nbins;
+  if (out) memcpy(out, s->bbi_out + (size_t)j * 6 * s->bbi_nbins, sizeof(double) * 6 * s->bbi_nbins);
   return 0;
 }
 

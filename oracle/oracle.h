@@ -44,6 +44,8 @@ int or_energy_loss(or_state* s);
 int or_synrad(or_state* s, int turn);
 int or_lr_wake(or_state* s);
 int or_sr_wake(or_state* s, int turn);
+int or_bbi(or_state* s);
+int or_bbi_profile(or_state* s, int j, int* nbins, double* out);
 int or_fir(or_state* s, int turn);
 int or_mark_lost(or_state* s, double* transmissions);
 int or_run_turns(or_state* s, int turn0, int n_turns);

@@ -36,6 +36,7 @@
 #include <string>
 #include <vector>
 
+#include "BoardBandImp.h"
 #include "CavityResonator.h"
 #include "FIRFeedBack.h"
 #include "LatticeInterActionPoint.h"
@@ -62,6 +63,7 @@ struct RefRun {
     MPBeam beam;
     WakeFunction lr, sr;
     FIRFeedBack fir;
+    BoardBandImp bbi;
     uint64_t birth_seed = 0;
 };
 
@@ -158,7 +160,8 @@ enum Stage {
     ST_SR = 9,        // SRWakeBeamIntaction(turn)
     ST_FIR = 10,      // FIRBunchByBunchFeedback(turn)
     ST_LOST = 11,     // MarkParticleLostInBunch
-    ST_RMS_ONLY = 12  // MPBeamRMSCal(k) alone
+    ST_RMS_ONLY = 12, // MPBeamRMSCal(k) alone
+    ST_BBI = 13       // BBImpBeamInteraction
 };
 
 void stage(RefRun *r, int s, int turn, int k) {
@@ -179,6 +182,7 @@ void stage(RefRun *r, int s, int turn, int k) {
         case ST_FIR: b.FIRBunchByBunchFeedback(in, r->fir, turn); break;
         case ST_LOST: b.MarkParticleLostInBunch(in, r->lat); break;
         case ST_RMS_ONLY: b.MPBeamRMSCal(r->lat, k); break;
+        case ST_BBI: b.BBImpBeamInteraction(in, r->bbi, r->lat); break;
         default: throw std::runtime_error("unknown stage");
     }
 }
@@ -199,6 +203,7 @@ void turn(RefRun *r, int n) {
     stage(r, ST_DRIFT, n, 0);
     stage(r, ST_ELOSS, n, 0);
     if (in.ringRun->synRadDampingFlag == 1) stage(r, ST_SYNRAD, n, 0);
+    if (in.ringRun->bBImpFlag) stage(r, ST_BBI, n, 0);
     if (in.ringRun->lRWakeFlag) stage(r, ST_LR, n, 0);
     if (in.ringRun->sRWakeFlag) stage(r, ST_SR, n, 0);
     stage(r, ST_RMS_ONLY, n, 0);
@@ -266,6 +271,24 @@ void *ref_open(const char *input_path, unsigned long long seed) {
         if (r->in.ringRun->lRWakeFlag) r->lr.InitialLRWake(r->in, r->lat);
         step = "WakeFunction::InitialSRWake";
         if (r->in.ringRun->sRWakeFlag) r->sr.InitialSRWake(r->in, r->lat);
+        // MPBeam.cpp:853-876
+        step = "BoardBandImp";
+        if (r->in.ringRun->bBImpFlag) {
+            if (r->in.ringBBImp->timeDomain == 0) {
+                r->bbi.ReadInImp(r->in);
+                for (auto &b : r->beam.beamVec) {
+                    const size_t n = r->bbi.nBins * 2 - 1;
+                    b.profileForBunchBBImp.resize(n, 0E0);
+                    b.wakePotenFromBBI->wakePotenZ.resize(n, 0E0);
+                    b.wakePotenFromBBI->wakePotenDx.resize(n, 0E0);
+                    b.wakePotenFromBBI->wakePotenDy.resize(n, 0E0);
+                    b.wakePotenFromBBI->wakePotenQx.resize(n, 0E0);
+                    b.wakePotenFromBBI->wakePotenQy.resize(n, 0E0);
+                }
+            } else {
+                r->beam.GetQuasiWakePoten(r->in);
+            }
+        }
     });
     if (st) g_err = std::string(step) + ": " + g_err;
     if (st) return nullptr;
@@ -490,6 +513,25 @@ int ref_rf_info(void *h, int j, int c, double *out) {
 // Derived ring constants after ParamRead (ReadInputSettings.cpp:986-1081):
 // rGamma, rBeta, t0, f0, workQz, emitNat[3], synchRadDampTime[3] (turns),
 // u0, sdelta0, ringHarm, 0  -> 16 doubles
+// Frequency-domain broadband impedance of bunch j after the last
+// BBImpBeamInteraction: profileForBunchBBImp (the last profile filtered,
+// MPBunch.cpp:2165-2316) and the five wakePotenFromBBI arrays, 6 x n.
+int ref_bbi_profile(void *h, int j, int *n, double *out) {
+    RefRun *r = static_cast<RefRun *>(h);
+    if (j < 0 || j >= (int)r->beam.beamVec.size()) return 1;
+    const MPBunch &b = r->beam.beamVec[j];
+    const std::vector<double> *rows[6] = {&b.profileForBunchBBImp, &b.wakePotenFromBBI->wakePotenZ,
+                                          &b.wakePotenFromBBI->wakePotenDx,
+                                          &b.wakePotenFromBBI->wakePotenDy,
+                                          &b.wakePotenFromBBI->wakePotenQx,
+                                          &b.wakePotenFromBBI->wakePotenQy};
+    *n = (int)rows[0]->size();
+    if (out)
+        for (int q = 0; q < 6; ++q)
+            for (int i = 0; i < *n; ++i) out[(size_t)q * *n + i] = i < (int)rows[q]->size() ? (*rows[q])[i] : 0.0;
+    return 0;
+}
+
 int ref_ring(void *h, double *out) {
     RefRun *r = static_cast<RefRun *>(h);
     const auto *b = r->in.ringParBasic;

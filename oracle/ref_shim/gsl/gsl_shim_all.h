@@ -167,7 +167,7 @@ void gsl_rng_set(const gsl_rng *r, unsigned long seed);
 double gsl_rng_uniform(const gsl_rng *r);
 double gsl_ran_gaussian(const gsl_rng *r, double sigma);
 
-/* ---- Gaussian filter (broadband-impedance profile smoothing: abort) --- */
+/* ---- Gaussian filter (broadband-impedance profile smoothing) --- */
 typedef enum { GSL_FILTER_END_PADZERO, GSL_FILTER_END_PADVALUE, GSL_FILTER_END_TRUNCATE }
     gsl_filter_end_t;
 typedef struct { size_t K; } gsl_filter_gaussian_workspace;

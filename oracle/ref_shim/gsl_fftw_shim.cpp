@@ -20,13 +20,18 @@
 //  * gsl_fit_wlinear: the weighted least-squares line through running
 //    weighted means (GSL's documented closed form, with its covariances and
 //    chi^2).
+//  * gsl_filter_gaussian (order 0, end-value padding): the Gaussian window
+//    G(k) = exp(-(alpha k / H)^2 / 2), |k| <= H = (K - 1) / 2, normalised to
+//    unit sum, applied as y_i = sum_k G(k) x_{i+k} with the end samples
+//    repeated beyond the ends (the broadband-impedance profiles,
+//    MPBunch.cpp:2373-2414).
 //  * gsl_sf_*: Gamma by std::tgamma, n! exactly, 2F1 by its power series,
 //    complete elliptic K by the arithmetic-geometric mean, I_nu by its power
 //    series (the resistive-wall wakes, WakeFunction.cpp:387-497, 787-941).
 //
-// Eigen-solvers, Gaussian filters and r2r/many-dimensional FFT plans are
-// reached only by paths outside the multi-particle tracking (one-turn-matrix
-// diagnostics, broadband impedance, PIC space charge): they abort.
+// Eigen-solvers and r2r/many-dimensional FFT plans are reached only by paths
+// outside the multi-particle tracking (one-turn-matrix diagnostics, PIC space
+// charge): they abort.
 #include "gsl/gsl_shim_all.h"
 #include "fftw3.h"
 
@@ -643,16 +648,51 @@ void gsl_rng_set(const gsl_rng *, unsigned long) { unreachable("gsl_rng_set"); }
 double gsl_rng_uniform(const gsl_rng *) { unreachable("gsl_rng_uniform"); }
 double gsl_ran_gaussian(const gsl_rng *, double) { unreachable("gsl_ran_gaussian"); }
 
-gsl_filter_gaussian_workspace *gsl_filter_gaussian_alloc(size_t) {
-    unreachable("gsl_filter_gaussian_alloc");
+gsl_filter_gaussian_workspace *gsl_filter_gaussian_alloc(size_t K) {
+    check(K % 2 == 1, "gsl_filter_gaussian_alloc: odd window length");
+    gsl_filter_gaussian_workspace *w =
+        static_cast<gsl_filter_gaussian_workspace *>(std::calloc(1, sizeof(*w)));
+    w->K = K;
+    return w;
 }
 void gsl_filter_gaussian_free(gsl_filter_gaussian_workspace *w) { std::free(w); }
-int gsl_filter_gaussian(gsl_filter_end_t, double, size_t, const gsl_vector *, gsl_vector *,
-                        gsl_filter_gaussian_workspace *) {
-    unreachable("gsl_filter_gaussian");
+// G(k) = exp(-(alpha k / H)^2 / 2), k = -H .. H, H = (K - 1) / 2 (order 0 only)
+int gsl_filter_gaussian_kernel(double alpha, size_t order, int normalize, gsl_vector *kernel) {
+    check(order == 0 && alpha > 0, "gsl_filter_gaussian_kernel: order 0, alpha > 0");
+    const size_t K = kernel->size;
+    const int H = (int)(K / 2);
+    double sum = 0;
+    for (size_t i = 0; i < K; ++i) {
+        const double x = H ? alpha * (double)((int)i - H) / (double)H : 0.0;
+        kernel->data[i * kernel->stride] = std::exp(-0.5 * x * x);
+        sum += kernel->data[i * kernel->stride];
+    }
+    if (normalize)
+        for (size_t i = 0; i < K; ++i) kernel->data[i * kernel->stride] /= sum;
+    return 0;
 }
-int gsl_filter_gaussian_kernel(double, size_t, int, gsl_vector *) {
-    unreachable("gsl_filter_gaussian_kernel");
+// y_i = sum_k G(k) x_{i+k} with the normalised kernel; samples beyond the
+// ends are the end values (GSL_FILTER_END_PADVALUE)
+int gsl_filter_gaussian(gsl_filter_end_t endtype, double alpha, size_t order, const gsl_vector *x,
+                        gsl_vector *y, gsl_filter_gaussian_workspace *w) {
+    check(endtype == GSL_FILTER_END_PADVALUE, "gsl_filter_gaussian: end-value padding only");
+    check(x->size == y->size, "gsl_filter_gaussian: sizes");
+    gsl_vector *k = gsl_vector_alloc(w->K);
+    gsl_filter_gaussian_kernel(alpha, order, 1, k);
+    const int N = (int)x->size, H = (int)(w->K / 2);
+    std::vector<double> out(N);
+    for (int i = 0; i < N; ++i) {
+        double acc = 0;
+        for (int q = -H; q <= H; ++q) {
+            int j = i + q;
+            j = j < 0 ? 0 : (j >= N ? N - 1 : j);
+            acc += k->data[(q + H) * k->stride] * x->data[j * x->stride];
+        }
+        out[i] = acc;
+    }
+    for (int i = 0; i < N; ++i) y->data[i * y->stride] = out[i];
+    gsl_vector_free(k);
+    return 0;
 }
 
 const char *gsl_strerror(int e) { return e == 0 ? "success" : "failure"; }

@@ -31,7 +31,7 @@ def test_library_exports_every_declared_symbol(lib):
 
 
 def test_abi_version(lib):
-    assert lib.cg_abi_version() == 2
+    assert lib.cg_abi_version() == 3
 
 
 def test_struct_layouts_match_c(built):

@@ -130,3 +130,33 @@ def test_dropin_with_beam_loading_matches_the_reference_program(tmp_path):
         rtol = 2e-4 if name.startswith(("eigenEmit", "xyCoupling")) else 2e-5
         bad = np.abs(a - b) > rtol * np.maximum(np.abs(a), 1e-3 * scale)
         assert not bad.any(), (name, a[bad][:3], b[bad][:3])
+
+
+@pytest.mark.parametrize("case_name", ["fd_train_lr", "td_train"])
+def test_dropin_with_broadband_impedance_matches_the_reference_program(tmp_path, case_name):
+    """The 80-bunch train with the broadband-impedance kick (frequency domain
+    with the long-range wake after it, and time domain; radiation off):
+    result.sdds of the drop-in against the reference program over 20 turns."""
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    import bbicases
+    wl, _, _ = bbicases.build(case_name, str(tmp_path / "base"))
+    wl.cfg.flag_synrad = 0
+    src = tmp_path / "src"
+    input_dat.write_case(str(src), wl, n_turns=20, qe=False)
+    dirs = []
+    for name in ("ref", "gpu"):
+        d = tmp_path / name
+        shutil.copytree(src, d)
+        dirs.append(str(d))
+    cols_r, rows_r = run(ref.EXE, dirs[0], teardown_may_crash=True)
+    cols_g, rows_g = run(DROPIN, dirs[1])
+    assert cols_r == cols_g and rows_r.shape == rows_g.shape == (20, len(cols_r))
+    for k, name in enumerate(cols_r):
+        if name == "IonCharge":
+            continue
+        a, b = rows_r[:, k], rows_g[:, k]
+        scale = np.max(np.abs(a)) + 1e-300
+        rtol = 2e-4 if name.startswith(("eigenEmit", "xyCoupling")) else 2e-5
+        bad = np.abs(a - b) > rtol * np.maximum(np.abs(a), 1e-3 * scale)
+        assert not bad.any(), (name, a[bad][:3], b[bad][:3])
