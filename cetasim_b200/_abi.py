@@ -109,6 +109,7 @@ class Config(C.Structure):
         ("bunch_sigma_z", D), ("bunch_sigma_dp", D),
         ("growth_fit_start", I), ("growth_fit_end", I), ("run_cbmgr", C.c_char * 256),
         ("lr_rw", RwSectors), ("sr_rw", RwSectors), ("bbi", Bbi),
+        ("flag_sc", I), ("sc_mesh", I * 3),
     ]
 
 
@@ -173,8 +174,13 @@ EXPORTS = [
     ("cg_lr_wake", I, [C.c_void_p]),
     ("cg_sr_wake", I, [C.c_void_p, I]),
     ("cg_bbi_kick", I, [C.c_void_p]),
+    ("cg_space_charge", I, [C.c_void_p, I]),
+    ("cg_bunch_ion_charge", I, [C.c_void_p, PD]),
+    ("cg_rf_profile", I, [C.c_void_p, I, PD, PD, PI]),
     ("cg_bbi_profile", I, [C.c_void_p, I, PI, PI, PD, I]),
     ("cg_sr_bins", I, [C.c_void_p, I, PD, PD, PI]),
+    ("cg_set_sr_potentials", I, [C.c_void_p, I]),
+    ("cg_sr_potentials", I, [C.c_void_p, I, PD]),
     ("cg_fir", I, [C.c_void_p, I]),
     ("cg_mark_lost", I, [C.c_void_p, PD]),
     ("cg_run_turns", I, [C.c_void_p, I, I]),

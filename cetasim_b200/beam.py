@@ -129,6 +129,11 @@ class MPBeam:
     def BeamSynRadDamping(self, turn: int):
         self._check(self.lib.cg_synrad(self.h, turn))
 
+    def BeamTransferDueToSpaceCharge(self, k: int):
+        """BeamTransferDueToSpaceChargePIC (runSpaceCharge 2) or
+        ...Analytical (1, 3) at section k."""
+        self._check(self.lib.cg_space_charge(self.h, k))
+
     def BBImpBeamInteraction(self):
         self._check(self.lib.cg_bbi_kick(self.h))
 
@@ -314,6 +319,16 @@ class MPBeam:
         out = np.empty((self.wl.n_bunches, max(1, self.wl.cfg.ion.n_species), 6))
         self._check(self.lib.cg_ion_cloud_record(self.h, k, _abi.ptr(out)))
         return out
+
+    def set_sr_potentials(self, on: bool):
+        self._check(self.lib.cg_set_sr_potentials(self.h, int(bool(on))))
+
+    def sr_potentials(self, j: int):
+        """Bunch j's short-range potentials x, y, z (3 x B) of the last SR step."""
+        B = int(self.wl.cfg.sr_bins)
+        out = np.empty(3 * B)
+        self._check(self.lib.cg_sr_potentials(self.h, j, _abi.ptr(out)))
+        return out.reshape(3, B)
 
     def sr_bins(self, j: int):
         zlo, dz = C.c_double(), C.c_double()

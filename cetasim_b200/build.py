@@ -16,7 +16,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libcetagpu.so")
 
 SOURCES = ["capi.cu", "kernels.cu", "kernels_sr.cu", "kernels_ion.cu", "surrogate.cu", "shard.cu",
-           "cbm.cu", "beam_loading.cu", "bbi.cu", "faddeeva_table.cpp", "input_settings.cpp", "rw_wake.cpp"]
+           "cbm.cu", "beam_loading.cu", "bbi.cu", "sc.cu", "faddeeva_table.cpp", "input_settings.cpp", "rw_wake.cpp"]
 HEADERS = ["cg_common.cuh", "faddeeva.cuh", "be_field.cuh", "track_math.cuh", "cg_internal.h",
            "kernels.cuh", "umma.cuh", "surrogate.cuh", "rw_wake.h"]
 

@@ -87,6 +87,8 @@ int check_status(Handle& h) {
   if (st & kStatusBbiRange)
     return fail(&h, CG_ERR_INVALID,
                 "a particle lies outside the broadband-impedance profile bins");
+  if (st & kStatusScMesh)
+    return fail(&h, CG_ERR_INVALID, "rms beam size is zero, not able to generate the space-charge mesh");
   if (st & kStatusBbiWide)
     return fail(&h, CG_ERR_INVALID, "a bunch spans more than CG_BBI_MAX_BINS broadband-impedance bins");
   return fail(&h, CG_ERR_CUDA, "unknown device status");
@@ -105,7 +107,8 @@ void free_beam(Handle& h) {
   dfree(d.counters); dfree(d.mom); dfree(d.loss_count); dfree(d.scratch);
   dfree(d.rec); dfree(d.rec_prep); dfree(d.lr_hist); dfree(d.lr_force); dfree(d.fir_hist); dfree(d.fir_kick);
   dfree(d.sr_geom); dfree(d.sr_counts); dfree(d.sr_sumx); dfree(d.sr_sumy); dfree(d.sr_lag);
-  dfree(d.sr_pot);
+  dfree(d.sr_pot); dfree(d.sr_potxy);
+  d.sr_potxy = nullptr;
   dfree(d.mom_send); dfree(d.mom_all); dfree(d.sh_off); dfree(d.sh_cnt);
   d.mom_send = nullptr; d.mom_all = nullptr; d.sh_off = nullptr; d.sh_cnt = nullptr;
   dfree(d.cbm);  // sized by the bunch count
@@ -118,6 +121,8 @@ void free_beam(Handle& h) {
   dfree(d.bbi_pot); dfree(d.bbi_win);
   d.bbi_lo = nullptr; d.bbi_hi = nullptr; d.bbi_amax = nullptr; d.bbi_cnt = nullptr;
   d.bbi_sxy = nullptr; d.bbi_pot = nullptr; d.bbi_win = nullptr;
+  dfree(d.sc_geom); dfree(d.sc_cnt); dfree(d.sc_acc); dfree(d.sc_field);
+  d.sc_geom = nullptr; d.sc_cnt = nullptr; d.sc_acc = nullptr; d.sc_field = nullptr;
   h.cbm_cap = h.cbm_n = 0;
   IonWalk& w = d.iw;
   dfree(w.births); dfree(w.prep); dfree(w.bunch); dfree(w.spec); dfree(w.bound); dfree(w.part);
@@ -452,6 +457,13 @@ int cg_create(const cg_config* cfg, int device, cg_handle** out) {
   if (cfg->flag_fir && cfg->fir.mode != 0 &&
       (cfg->fir.delay + cfg->fir.taps < 1 || cfg->fir.delay + cfg->fir.taps > CG_MAX_FIR))
     return fail(nullptr, CG_ERR_INVALID, "fbDelay + fbTaps must be in [1, 64]");
+  if (cfg->flag_sc < 0 || cfg->flag_sc > 3)
+    return fail(nullptr, CG_ERR_INVALID, "runSpaceCharge must be 0, 1, 2 or 3");
+  if (cfg->flag_sc && cfg->sc_mesh[2] < 2)
+    return fail(nullptr, CG_ERR_INVALID, "space charge needs >= 2 slices");
+  if (cfg->flag_sc == 2 && (cfg->sc_mesh[0] < 2 || cfg->sc_mesh[0] > 64 || cfg->sc_mesh[1] < 2 ||
+                            cfg->sc_mesh[1] > 64))
+    return fail(nullptr, CG_ERR_UNSUPPORTED, "the space-charge PIC mesh must be 2 .. 64 nodes per plane");
   BbiParams bbi_p;
   std::vector<double> bbi_data;
   if (cfg->bbi.flag) {
@@ -613,6 +625,54 @@ int cg_create(const cg_config* cfg, int device, cg_handle** out) {
     }
     if (dalloc(&h.d.sr_green, buf.size())) return bail(CG_ERR_OOM, "SR green");
     cudaMemcpy(h.d.sr_green, buf.data(), sizeof(double) * buf.size(), cudaMemcpyHostToDevice);
+    // the transverse planes (WakeFunction.cpp:596-629): per plane the
+    // resonators' dz, 2 Q / vz, sqrt(2 / pi) Rs c and sin(z a) / a
+    const size_t per = 3 * CG_MAX_RESONATORS + (size_t)w.n * NZ;
+    std::vector<double> bt(2 * per, 0.0);
+    for (int q = 0; q < 2; ++q)
+      for (int r = 0; r < w.n; ++r) {
+        const double Q = q ? w.ty_q[r] : w.tx_q[r];
+        const double om = q ? w.ty_omega[r] : w.tx_omega[r];
+        const double rs = q ? w.ty_rs[r] : w.tx_rs[r];
+        double vz = om * sigmaz / kCLight;
+        double zMax = 3 * vz / (2 * Q);
+        double dz = zMax / NZ;
+        double* o = bt.data() + q * per;
+        o[3 * r + 0] = dz;
+        o[3 * r + 1] = 2 * Q / vz;
+        o[3 * r + 2] = std::sqrt(2. / PI) * rs * kCLight;
+        double a = std::sqrt(4 * Q * Q - 1);
+        for (int j = 0; j < NZ; ++j) o[3 * CG_MAX_RESONATORS + (size_t)r * NZ + j] = std::sin(j * dz * a) / a;
+      }
+    if (dalloc(&h.d.sr_green_t, bt.size())) return bail(CG_ERR_OOM, "SR green");
+    cudaMemcpy(h.d.sr_green_t, bt.data(), sizeof(double) * bt.size(), cudaMemcpyHostToDevice);
+  }
+  if (h.cfg.flag_sc) {
+    ScParams& p = h.sc;
+    p.flag = h.cfg.flag_sc;
+    p.nx = h.cfg.sc_mesh[0];
+    p.ny = h.cfg.sc_mesh[1];
+    p.nz = h.cfg.sc_mesh[2];
+    p.acc_per_slice = p.flag == 2 ? p.nx * p.ny : 4;
+    // PIC2D::UpdateTransverseMomentum (PIC2D.cpp): the reference momentum
+    const double gamma0 = h.cfg.ring.electron_energy / 0.51099906e6;
+    const double beta0 = std::sqrt(1 - 1 / std::pow(gamma0, 2));
+    p.p0 = beta0 * gamma0;
+    if (p.flag == 2) {
+      // the DST-I matrices 2 sin(pi (i + 1)(k + 1) / (n + 1)), the argument
+      // reduced modulo 2 (n + 1) first
+      std::vector<double> sn((size_t)p.nx * p.nx + (size_t)p.ny * p.ny);
+      size_t o = 0;
+      for (int n : {p.nx, p.ny})
+        for (int k = 0; k < n; ++k)
+          for (int i = 0; i < n; ++i) {
+            const long r = (long)(i + 1) * (k + 1) % (2 * (n + 1));
+            sn[o++] = 2 * std::sin(kPi * (double)r / (n + 1));
+          }
+      if (dalloc(&h.d.sc_sin, sn.size())) return bail(CG_ERR_OOM, "space-charge tables");
+      cudaMemcpy(h.d.sc_sin, sn.data(), sizeof(double) * sn.size(), cudaMemcpyHostToDevice);
+    }
+    if ((e = prepare_sc(p)) != cudaSuccess) return bail(CG_ERR_CUDA, cudaGetErrorString(e));
   }
   if (h.cfg.bbi.flag) {
     const BbiParams& p = h.bbi;
@@ -653,7 +713,8 @@ int cg_destroy(cg_handle* H) {
     dfree(h.d.clouds);
   }
   dfree(h.d.cloud_state); dfree(h.d.lr_tab); dfree(h.d.lr_head); dfree(h.d.fir_coeff);
-  dfree(h.d.fir_head); dfree(h.d.sr_green); dfree(h.d.bbi_w);
+  dfree(h.d.fir_head); dfree(h.d.sr_green); dfree(h.d.sr_green_t); dfree(h.d.bbi_w);
+  dfree(h.d.sc_sin);
   if (h.stream) cudaStreamDestroy(h.stream);
   if (h.side) cudaStreamDestroy(h.side);
   if (h.side2) cudaStreamDestroy(h.side2);
@@ -804,6 +865,13 @@ int cg_set_beam(cg_handle* H, int M, const int* n_macro, const int* harm, const 
     cudaMemset(d.fir_hist, 0, sizeof(double) * h.fir_order * 3 * M);
     cudaMemset(h.d.fir_head, 0, sizeof(int));
   }
+  // BunchRFModeInfo of every bunch and cavity (Bunch.cpp:89-105: zero until
+  // the first RF step)
+  if (dalloc(&d.rf_info, (size_t)M * CG_MAX_CAVITIES * 8)) {
+    free_beam(h);
+    return fail(&h, CG_ERR_OOM, "RF info");
+  }
+  cudaMemset(d.rf_info, 0, sizeof(double) * M * CG_MAX_CAVITIES * 8);
   if (h.ring.bl_any) {
     // cavities with beam loading: the resonators' initial state from the fill
     // pattern (MPBeam::InitialcavityResonator) and the per-bunch tables
@@ -820,8 +888,7 @@ int cg_set_beam(cg_handle* H, int M, const int* n_macro, const int* harm, const 
     for (int c = 0; c < h.cfg.ring.n_cav; ++c) n_bl += h.cfg.ring.rf_mode[c] == 1;
     if (dalloc(&d.res_state, 6 * (size_t)CG_MAX_CAVITIES) || dalloc(&d.rf_zr, 2 * (size_t)M) ||
         dalloc(&d.rf_counts, (size_t)M * nb) || dalloc(&d.rf_kick, (size_t)n_bl * M * nb * 2) ||
-        dalloc(&d.rf_fbk, (size_t)n_bl * M) || dalloc(&d.rf_work, rf_work_doubles(n_bl, M, nb)) ||
-        dalloc(&d.rf_info, (size_t)M * CG_MAX_CAVITIES * 8)) {
+        dalloc(&d.rf_fbk, (size_t)n_bl * M) || dalloc(&d.rf_work, rf_work_doubles(n_bl, M, nb))) {
       free_beam(h);
       return fail(&h, CG_ERR_OOM, "beam-loading buffers");
     }
@@ -836,11 +903,29 @@ int cg_set_beam(cg_handle* H, int M, const int* n_macro, const int* harm, const 
     int B = h.cfg.sr_bins;
     if (dalloc(&d.sr_geom, 2 * (size_t)M) || dalloc(&d.sr_counts, (size_t)M * B) ||
         dalloc(&d.sr_sumx, (size_t)M * B) || dalloc(&d.sr_sumy, (size_t)M * B) ||
-        dalloc(&d.sr_lag, (size_t)M * (2 * B - 1)) || dalloc(&d.sr_pot, (size_t)M * B)) {
+        dalloc(&d.sr_lag, (size_t)M * 3 * (2 * B - 1)) || dalloc(&d.sr_pot, (size_t)M * B) ||
+        (h.sr_xy && dalloc(&d.sr_potxy, (size_t)M * 2 * B))) {
       free_beam(h);
       return fail(&h, CG_ERR_OOM, "SR buffers");
     }
     cudaMemset(d.sr_pot, 0, sizeof(double) * M * B);
+    if (d.sr_potxy) cudaMemset(d.sr_potxy, 0, sizeof(double) * M * 2 * B);
+  }
+  if (h.cfg.flag_sc) {
+    const ScParams& p = h.sc;
+    if (h.sh_world > 1) {
+      free_beam(h);
+      return fail(&h, CG_ERR_UNSUPPORTED, "space charge with bunch sharding is not supported");
+    }
+    const size_t slices = (size_t)M * p.nz;
+    if (dalloc(&d.sc_geom, (size_t)M * 11) || dalloc(&d.sc_cnt, slices) ||
+        dalloc(&d.sc_acc, slices * p.acc_per_slice) ||
+        (p.flag == 2 && dalloc(&d.sc_field, slices * 2 * p.nx * p.ny))) {
+      free_beam(h);
+      return fail(&h, CG_ERR_OOM, "space-charge buffers");
+    }
+    cudaMemset(d.sc_geom, 0, sizeof(double) * M * 11);
+    cudaMemset(d.sc_acc, 0, sizeof(unsigned long long) * slices * p.acc_per_slice);
   }
   if (h.cfg.bbi.flag) {
     const size_t wc = h.bbi.wcap;
@@ -1031,6 +1116,13 @@ int cg_synrad(cg_handle* H, int turn) {
   st = launch_ok(h, launch_long(h, kLongSynrad), "synrad");
   return st ? st : check_status(h);
 }
+int cg_space_charge(cg_handle* H, int k) {
+  STAGE_PROLOGUE
+  if (!h.cfg.flag_sc) return fail(&h, CG_ERR_NOT_READY, "runSpaceCharge is off");
+  if (k < 0 || k >= h.K) return fail(&h, CG_ERR_INVALID, "section index out of range");
+  int st = launch_ok(h, launch_space_charge(h, k), "space charge");
+  return st ? st : check_status(h);
+}
 int cg_bbi_kick(cg_handle* H) {
   STAGE_PROLOGUE
   if (!h.cfg.bbi.flag) return fail(&h, CG_ERR_NOT_READY, "runBBIFlag is off");
@@ -1067,6 +1159,42 @@ int cg_sr_wake(cg_handle* H, int turn) {
   if (!h.cfg.flag_sr_wake) return fail(&h, CG_ERR_NOT_READY, "runShortRangeWake is off");
   int st = launch_ok(h, launch_sr_wake(h), "sr");
   return st ? st : check_status(h);
+}
+int cg_set_sr_potentials(cg_handle* H, int on) {
+  if (!H) return CG_ERR_INVALID;
+  Handle& h = H->h;
+  if (!h.cfg.flag_sr_wake) return fail(&h, CG_ERR_NOT_READY, "runShortRangeWake is off");
+  if (on && h.cfg.sr_rw.n > 0)
+    return fail(&h, CG_ERR_UNSUPPORTED,
+                "the transverse resistive-wall pseudo-wakes of the potentials file are not built");
+  cudaSetDevice(h.device);
+  const bool want = on != 0;
+  if (want && h.beam_set && !h.d.sr_potxy) {
+    const size_t n = (size_t)h.M * 2 * h.cfg.sr_bins;
+    if (dalloc(&h.d.sr_potxy, n)) return fail(&h, CG_ERR_OOM, "SR potentials");
+    CG_CUDA(&h, cudaMemset(h.d.sr_potxy, 0, sizeof(double) * n));
+  }
+  if (want != h.sr_xy && h.turn_graph) {
+    cudaGraphExecDestroy(h.turn_graph);
+    h.turn_graph = nullptr;
+  }
+  h.sr_xy = want;
+  return CG_OK;
+}
+int cg_sr_potentials(cg_handle* H, int j, double* out) {
+  STAGE_PROLOGUE
+  if (!h.cfg.flag_sr_wake) return fail(&h, CG_ERR_NOT_READY, "runShortRangeWake is off");
+  if (j < 0 || j >= h.M || !out) return fail(&h, CG_ERR_INVALID, "bad arguments");
+  const int B = h.cfg.sr_bins;
+  CG_CUDA(&h, cudaStreamSynchronize(h.stream));
+  if (h.sr_xy && h.d.sr_potxy)
+    CG_CUDA(&h, cudaMemcpy(out, h.d.sr_potxy + (size_t)j * 2 * B, sizeof(double) * 2 * B,
+                           cudaMemcpyDeviceToHost));
+  else
+    std::fill(out, out + 2 * B, 0.0);
+  CG_CUDA(&h, cudaMemcpy(out + 2 * B, h.d.sr_pot + (size_t)j * B, sizeof(double) * B,
+                         cudaMemcpyDeviceToHost));
+  return CG_OK;
 }
 int cg_sr_bins(cg_handle* H, int j, double* zlo, double* dz, int* counts) {
   STAGE_PROLOGUE
@@ -1149,18 +1277,23 @@ static cudaError_t enqueue_turn(Handle& h) {
   // and the moments the next stage reads (those of IP k+1 for its ion chain;
   // after the last IP those of section K-1 for the wakes, MPBeam.cpp:1069)
   const bool post = c.flag_lr_wake || c.flag_sr_wake;
+  // the stages at each section that read that section's moments: the ion
+  // chain and the space charge (MPBeam.cpp:1059-1066)
+  const bool sec_mom = c.flag_beam_ion || c.flag_sc;
   TRACE(h.stream, CG_TRACE_START, -1, -1);
-  if (c.flag_beam_ion) {
+  if (sec_mom) {
     if ((e = launch_moments(h, 0)) || (e = exchange_moments(h))) return e;
     TRACE(h.stream, CG_TRACE_MOMENTS, 0, -1);
   }
   const int G = std::max(1, std::min(h.pipe_groups, h.M));
   for (int k = 0; k < h.K; ++k) {
-    const bool fused = c.flag_beam_ion && !h.d.sur_w && h.fuse_kick;
+    // the space charge kicks between the ion kick and the map, so neither
+    // the kick inside the map pass nor the segmented pipeline
+    const bool fused = c.flag_beam_ion && !h.d.sur_w && h.fuse_kick && !c.flag_sc;
     int mom = -1;
-    if (k + 1 < h.K) mom = c.flag_beam_ion ? k + 1 : -1;
+    if (k + 1 < h.K) mom = sec_mom ? k + 1 : -1;
     else mom = post ? h.K - 1 : -1;
-    if (c.flag_beam_ion && G > 1) {
+    if (c.flag_beam_ion && G > 1 && !c.flag_sc) {
       // the walk in G segments of bunches on the main stream; as soon as a
       // segment is walked, its records and kick on `side` and its map (with
       // the next IP's moments) on `side2`, so that the walk of segment g + 1,
@@ -1208,6 +1341,7 @@ static cudaError_t enqueue_turn(Handle& h) {
           TRACE(h.stream, CG_TRACE_ION_KICK, k, -1);
         }
       }
+      if (c.flag_sc && (e = launch_space_charge(h, k))) return e;
       if ((e = launch_map_turn(h, k, mom, fused))) return e;
       TRACE(h.stream, CG_TRACE_MAP_PASS, k, -1);
     }
@@ -1692,6 +1826,44 @@ int cg_ion_cloud_record(cg_handle* H, int k, double* out) {
   return CG_OK;
 }
 
+// MPBunch::totIonCharge after the last turn (MPBunch.cpp:1208-1209): the
+// total ion charge of every IP right after bunch j's interaction at the last
+// IP (LIP::GetTotIonCharge, LatticeInterActionPoint.cpp:1215-1225): the
+// clouds of the earlier IPs as the turn left them (their macro-ion charge
+// the last bunch's), the last IP's cloud as bunch j met it, at bunch j's
+// macro-ion charge.
+int cg_bunch_ion_charge(cg_handle* H, double* out) {
+  if (!H || !out) return CG_ERR_INVALID;
+  Handle& h = H->h;
+  if (!h.cfg.flag_beam_ion || !h.beam_set) return fail(&h, CG_ERR_NOT_READY, "no ion records");
+  if (h.sh_world > 1) return fail(&h, CG_ERR_UNSUPPORTED, "not with bunch sharding");
+  cudaSetDevice(h.device);
+  CG_CUDA(&h, cudaStreamSynchronize(h.stream));
+  std::vector<CloudState> st((size_t)h.K * h.P);
+  CG_CUDA(&h, cudaMemcpy(st.data(), h.d.cloud_state, sizeof(CloudState) * st.size(),
+                         cudaMemcpyDeviceToHost));
+  std::vector<CloudRec> rec((size_t)h.M * h.P);
+  CG_CUDA(&h, cudaMemcpy(rec.data(), h.d.rec + (size_t)(h.K - 1) * h.M * h.P,
+                         sizeof(CloudRec) * rec.size(), cudaMemcpyDeviceToHost));
+  std::vector<double> spec(2 * (size_t)h.P * h.M);
+  CG_CUDA(&h, cudaMemcpy(spec.data(), h.d.iw.spec, sizeof(double) * spec.size(),
+                         cudaMemcpyDeviceToHost));
+  for (int j = 0; j < h.M; ++j) {
+    double q = 0;
+    for (int k = 0; k < h.K; ++k)
+      for (int p = 0; p < h.P; ++p) {
+        if (k < h.K - 1) {
+          const CloudState& c = st[(size_t)k * h.P + p];
+          q += c.n * c.macro_charge;
+        } else {
+          q += rec[(size_t)j * h.P + p].count * spec[2 * ((size_t)p * h.M + j)];
+        }
+      }
+    out[j] = q;
+  }
+  return CG_OK;
+}
+
 int cg_ion_totals(cg_handle* H, double* tot_charge, int* tot_macro) {
   if (!H) return CG_ERR_INVALID;
   Handle& h = H->h;
@@ -1898,10 +2070,25 @@ int cg_rf_info(cg_handle* H, int j, int c, double* out8) {
   STAGE_PROLOGUE
   if (!out8 || c < 0 || c >= h.cfg.ring.n_cav || j < 0 || j >= h.M)
     return fail(&h, CG_ERR_INVALID, "bad bunch or cavity");
-  if (!h.ring.bl_any) return fail(&h, CG_ERR_NOT_READY, "no cavity with beam loading");
   CG_CUDA(&h, cudaStreamSynchronize(h.stream));
   CG_CUDA(&h, cudaMemcpy(out8, h.d.rf_info + ((size_t)j * CG_MAX_CAVITIES + c) * 8,
                          8 * sizeof(double), cudaMemcpyDeviceToHost));
+  return CG_OK;
+}
+
+int cg_rf_profile(cg_handle* H, int j, double* zmax, double* dz, int* counts) {
+  STAGE_PROLOGUE
+  if (!h.ring.bl_any) return fail(&h, CG_ERR_NOT_READY, "no cavity with beam loading");
+  if (j < 0 || j >= h.M || !zmax || !dz) return fail(&h, CG_ERR_INVALID, "bad arguments");
+  const int nb = h.cfg.ring.rf_bunch_bins;
+  CG_CUDA(&h, cudaStreamSynchronize(h.stream));
+  double zr[2];
+  CG_CUDA(&h, cudaMemcpy(zr, h.d.rf_zr + 2 * (size_t)j, sizeof zr, cudaMemcpyDeviceToHost));
+  *zmax = zr[1];
+  *dz = (zr[1] - zr[0]) / nb;
+  if (counts)
+    CG_CUDA(&h, cudaMemcpy(counts, h.d.rf_counts + (size_t)j * nb, sizeof(int) * nb,
+                           cudaMemcpyDeviceToHost));
   return CG_OK;
 }
 
@@ -2063,6 +2250,9 @@ int ckpt_fixed(Handle& h, Op op) {
   }
   if (h.cfg.flag_sr_wake && (st = op(h.d.sr_pot, M * (size_t)h.cfg.sr_bins * sizeof(double))))
     return st;
+  if (h.cfg.flag_sr_wake && h.sr_xy && h.d.sr_potxy &&
+      (st = op(h.d.sr_potxy, M * 2 * (size_t)h.cfg.sr_bins * sizeof(double))))
+    return st;
   if (h.ring.bl_any && (st = op(h.d.res_state, 6 * (size_t)CG_MAX_CAVITIES * sizeof(double))))
     return st;
   return CG_OK;
@@ -2081,7 +2271,8 @@ CkptHeader ckpt_header(const Handle& h) {
   c.fir_order = h.cfg.flag_fir ? h.fir_order : 0;
   c.sr_bins = h.cfg.flag_sr_wake ? h.cfg.sr_bins : 0;
   c.flags = (h.cfg.flag_beam_ion ? 1 : 0) | (h.cfg.flag_lr_wake ? 2 : 0) |
-            (h.cfg.flag_fir ? 4 : 0) | (h.cfg.flag_sr_wake ? 8 : 0);
+            (h.cfg.flag_fir ? 4 : 0) | (h.cfg.flag_sr_wake ? 8 : 0) |
+            (h.cfg.flag_sr_wake && h.sr_xy && h.d.sr_potxy ? 16 : 0);
   return c;
 }
 

@@ -35,6 +35,15 @@ struct BbiParams {
   double g[2 * kBbiHalf + 1];  // normalised Gaussian filter kernel
 };
 
+// Space charge (cg_config::flag_sc), set up at cg_create.
+struct ScParams {
+  int flag = 0;                // 1 Bassetti-Erskine slices, 2 2.5-D PIC, 3 linear
+  int nx = 0, ny = 0, nz = 0;  // mesh nodes (PIC) and slices
+  int acc_per_slice = 0;       // accumulators per slice: nx ny (PIC) or 4
+  double range = 10.0;         // mesh half-width in rms sizes (PIC3D.h:62, PIC3D.cpp:152)
+  double p0 = 0;               // beta0 gamma0 of the reference particle (PIC2D.cpp)
+};
+
 // Ion cloud of one (IP, species): ping-pong buffers of capacity `cap`.
 struct CloudDev {
   double* x[2];
@@ -130,6 +139,8 @@ struct DeviceBufs {
   double* sr_lag = nullptr;        // M x (2B-1)
   double* sr_pot = nullptr;        // M x B (z plane, persistent)
   double* sr_green = nullptr;      // resonators x 1000 (u-independent factors)
+  double* sr_green_t = nullptr;    // the same for the transverse planes x, y
+  double* sr_potxy = nullptr;      // M x 2 x B transverse potentials (persistent, cg_set_sr_potentials)
   // coupled-bunch mode history (cg_cbm_*): records x kCbmRecord x M
   double* cbm = nullptr;
   // cavities with beam loading (rfMode 1)
@@ -149,6 +160,12 @@ struct DeviceBufs {
   unsigned long long* bbi_sxy = nullptr;  // M x 2 x wcap fixed-point sums of x, y
   double* bbi_pot = nullptr;       // M x 6 x wcap: profile and potentials of the last kick
   int2* bbi_win = nullptr;         // M: first bin and bin count of bbi_pot
+  // space charge
+  double* sc_geom = nullptr;       // M x 11: slices, mesh, fixed-point scales
+  int* sc_cnt = nullptr;           // M x nz particles per slice
+  unsigned long long* sc_acc = nullptr;  // M x nz x acc_per_slice fixed-point sums
+  double* sc_field = nullptr;      // M x nz x 2 x nx x ny mesh field (PIC)
+  double* sc_sin = nullptr;        // nx x nx + ny x ny: 2 sin(pi (i + 1)(k + 1) / (n + 1))
   // scratch
   double* scratch = nullptr;
   size_t scratch_bytes = 0;
@@ -187,6 +204,8 @@ struct Handle {
   int cbm_cap = 0, cbm_n = 0;  // coupled-bunch mode history: capacity, records made
   double sr_rw_coeff = 0.0;    // short-range resistive-wall coefficient (0: no sectors)
   BbiParams bbi;               // broadband impedance (cfg.bbi.flag)
+  ScParams sc;                 // space charge (cfg.flag_sc)
+  bool sr_xy = false;          // SR wake: the transverse potentials too (the reference's file)
   std::vector<double> bbi_table;  // the copy of cfg.bbi.table
   int pipe_groups = 4;
   // trajectories per walk CTA (8, 16, 32, 64): smaller CTAs spread the

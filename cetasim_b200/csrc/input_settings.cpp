@@ -297,12 +297,20 @@ static int config_from_input(const char* path, cg_config* cfg, int* n_bunches, i
       g_parse_error = "runcalSetting must be 2 (MP model)";
       return CG_ERR_UNSUPPORTED;
     }
-    if (flag("runspacecharge") || flag("runramping") || flag("drivemodeon") ||
+    if (flag("runramping") || flag("drivemodeon") ||
         (has("ioncalscmethod") && flag("ioncalscmethod") == 2)) {
-      g_parse_error = "space charge, ramping, drive mode and PIC beam-ion "
+      g_parse_error = "ramping, drive mode and PIC beam-ion "
                       "are outside the tracking path of this library";
       return CG_ERR_UNSUPPORTED;
     }
+    // space charge: flag and mesh (ReadInputSettings.cpp:878-884; defaults
+    // ReadInputSettings.h:247-248)
+    cfg->flag_sc = flag("runspacecharge");
+    const int mesh0[3] = {32, 32, 33};
+    for (int i = 0; i < 3; ++i)
+      cfg->sc_mesh[i] = has("runspacecharge") && get("runspacecharge").v.size() > (size_t)(i + 1)
+                            ? Ii(get("runspacecharge"), i + 1)
+                            : mesh0[i];
     cfg->flag_synrad = flag("runsynraddampingflag");
     cfg->flag_beam_ion = flag("runbeamionflag");
     cfg->flag_lr_wake = flag("runlongrangewake");

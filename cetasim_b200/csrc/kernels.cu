@@ -864,11 +864,27 @@ __global__ void __launch_bounds__(kTile) k_long(double* __restrict__ c, int64_t 
                                                 const double* __restrict__ lr_force,
                                                 const double* __restrict__ rf_zr,
                                                 const double* __restrict__ rf_kick,
-                                                const double* __restrict__ rf_fbk, int M) {
+                                                const double* __restrict__ rf_fbk, int M,
+                                                double* rf_info) {
   TileIdx t = tile_index(tile_bunch, bunch);
   if (!t.valid) return;
   double v[6];
   load6(c, npad, t.g, v);
+  if ((flags & kLongRF) && t.i == bunch[t.b].n - 1) {
+    // the ideal cavities' BunchRFModeInfo: the voltage the bunch's last
+    // particle sees (Bunch.cpp:466-478; cavity = generator, no induced or
+    // self-loss voltage)
+    for (int q = 0; q < r.n_cav; ++q) {
+      if (r.bl_any && r.bl_index[q] >= 0) continue;
+      double sn, co;
+      sincos(v[4] * r.rf_theta_coeff[q], &sn, &co);
+      const double re = fma(r.vreq_re[q], co, r.vreq_im[q] * sn);
+      const double im = fma(r.vreq_im[q], co, -r.vreq_re[q] * sn);
+      double* o = rf_info + ((size_t)t.b * CG_MAX_CAVITIES + q) * 8;
+      o[0] = re; o[1] = im; o[2] = re; o[3] = im;
+      o[4] = 0.0; o[5] = 0.0; o[6] = 0.0; o[7] = 0.0;
+    }
+  }
   if (flags & kLongRF) {
     if (r.bl_any)
       v[5] = rf_kick_dp_loading(r, v[4], v[5], surv[t.g] == kAlive, t.b, M, rf_zr, rf_kick,
@@ -900,7 +916,8 @@ cudaError_t launch_long(Handle& h, unsigned flags) {
   }
   k_long<<<h.n_tiles, kTile, 0, h.stream>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch, h.d.bunch,
                                             h.sec_dev_host[0], h.ring, flags, h.cfg.seed, h.d.turn,
-                                            h.d.lr_force, h.d.rf_zr, h.d.rf_kick, h.d.rf_fbk, h.M);
+                                            h.d.lr_force, h.d.rf_zr, h.d.rf_kick, h.d.rf_fbk, h.M,
+                                            h.d.rf_info);
   return cudaGetLastError();
 }
 

@@ -14,7 +14,13 @@ enum : int {
   kStatusGaussCut = 64,       // an initial-distribution draw found no accepted sample
   kStatusBbiRange = 128,      // a particle outside the broadband-impedance profile
   kStatusBbiWide = 256,       // a bunch over more than CG_BBI_MAX_BINS profile bins
+  kStatusScMesh = 512,        // a space-charge mesh from a zero rms size
 };
+
+// space charge (sc.cu)
+cudaError_t launch_space_charge(Handle& h, int k);
+size_t sc_solve_smem(const ScParams& p);
+cudaError_t prepare_sc(const ScParams& p);
 
 // broadband impedance (bbi.cu)
 cudaError_t launch_bbi(Handle& h);

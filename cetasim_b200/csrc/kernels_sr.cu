@@ -212,7 +212,7 @@ __global__ void __launch_bounds__(256) k_sr_lag(const double* __restrict__ geom,
                                                 const SrResonator* __restrict__ res,
                                                 const double* __restrict__ green, int n_res,
                                                 int B, double sigmat, double rw_coeff,
-                                                double* lag) {
+                                                double* lag, const double* __restrict__ green_t) {
   __shared__ double sw[8];
   __shared__ double sw4[4][8];
   const int b = blockIdx.y;
@@ -246,19 +246,60 @@ __global__ void __launch_bounds__(256) k_sr_lag(const double* __restrict__ geom,
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0) lag[(size_t)b * (2 * B - 1) + blockIdx.x] = total;
+  if (threadIdx.x == 0) lag[(size_t)b * 3 * (2 * B - 1) + blockIdx.x] = total;
+  if (!green_t) return;
+  // the transverse pseudo-Green wakes of the resonators (GetBBRPusdoWakeFun,
+  // WakeFunction.cpp:596-629), for the potentials MPBunch.cpp:1981-1985
+  // accumulates: per plane a header of CG_MAX_RESONATORS x (dz, 2Q/vz,
+  // sqrt(2/pi) Rs c), then the resonators' sin(z a) / a tables
+  for (int q = 0; q < 2; ++q) {
+    const double* gt = green_t + (size_t)q * (3 * CG_MAX_RESONATORS + (size_t)n_res * kSrGreenN);
+    double tq = 0.0;
+    for (int r = 0; r < n_res; ++r) {
+      const double dz = gt[3 * r], c = gt[3 * r + 1], coeff = gt[3 * r + 2];
+      double s = 0.0;
+      for (int j = threadIdx.x; j < kSrGreenN; j += 256) {
+        double z = j * dz;
+        double a = u + c * z;
+        double t0 = -1 / 2.0 * (a * a) - z;
+        s = fma(exp(t0), gt[3 * CG_MAX_RESONATORS + (size_t)r * kSrGreenN + j], s);
+      }
+      s = warp_sum1(s);
+      if ((threadIdx.x & 31) == 0) sw[threadIdx.x >> 5] = s;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double acc = 0.0;
+        for (int w = 0; w < 8; ++w) acc += sw[w];
+        tq += c * acc * dz * coeff;
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) lag[((size_t)b * 3 + 1 + q) * (2 * B - 1) + blockIdx.x] = tq;
+  }
 }
 
 __global__ void k_sr_pot(const BunchDev* __restrict__ bunch, const int* __restrict__ counts,
-                         const double* __restrict__ lag, double* pot, int B, double energy) {
+                         const double* __restrict__ lag, double* pot, int B, double energy,
+                         const double* __restrict__ sumx, double* potxy) {
   const int b = blockIdx.x;
   const int* cnt = counts + (size_t)b * B;
-  const double* lg = lag + (size_t)b * (2 * B - 1);
+  const double* lg = lag + (size_t)b * 3 * (2 * B - 1);
   const double scale = (-1) * kElectronCharge * bunch[b].q_macro / energy;
   for (int i = threadIdx.x; i < B; i += blockDim.x) {
     double v = pot[(size_t)b * B + i];
     for (int j = 0; j < B; ++j) v += lg[i - j + B - 1] * cnt[j];
     pot[(size_t)b * B + i] = v * scale;
+    if (!potxy) continue;
+    // the transverse potentials, both from the horizontal centroids
+    // (averXAlongBunch in both lines, MPBunch.cpp:1981-1985)
+    double vx = potxy[(size_t)b * 2 * B + i], vy = potxy[((size_t)b * 2 + 1) * B + i];
+    for (int j = 0; j < B; ++j) {
+      const double ax = cnt[j] ? sumx[(size_t)b * B + j] / cnt[j] : 0.0;
+      vx += lg[(2 * B - 1) + i - j + B - 1] * cnt[j] * ax;
+      vy += lg[2 * (2 * B - 1) + i - j + B - 1] * cnt[j] * ax;
+    }
+    potxy[(size_t)b * 2 * B + i] = vx * scale;
+    potxy[((size_t)b * 2 + 1) * B + i] = vy * scale;
   }
 }
 
@@ -289,11 +330,13 @@ cudaError_t launch_sr_wake(Handle& h) {
                                                 h.d.sr_sumx, h.d.sr_sumy, B);
   dim3 lg(2 * B - 1, h.M);
   const double sigmat = 1.e-3 / kCLight;
+  const bool xy = h.sr_xy && h.d.sr_potxy;
   k_sr_lag<<<lg, 256, 0, h.stream>>>(h.d.sr_geom, reinterpret_cast<const SrResonator*>(h.d.sr_green),
                                      h.d.sr_green + 3 * CG_MAX_RESONATORS, h.cfg.sr_bbr.n, B,
-                                     sigmat, h.sr_rw_coeff, h.d.sr_lag);
+                                     sigmat, h.sr_rw_coeff, h.d.sr_lag, xy ? h.d.sr_green_t : nullptr);
   k_sr_pot<<<h.M, 128, 0, h.stream>>>(h.d.bunch, h.d.sr_counts, h.d.sr_lag, h.d.sr_pot, B,
-                                      h.cfg.ring.electron_energy);
+                                      h.cfg.ring.electron_energy, h.d.sr_sumx,
+                                      xy ? h.d.sr_potxy : nullptr);
   k_sr_kick<<<h.n_tiles, kTile, 0, h.stream>>>(h.d.c, h.npad, h.d.surv, h.d.tile_bunch, h.d.bunch,
                                                h.d.sr_geom, h.d.sr_pot, B);
   return cudaGetLastError();

@@ -20,10 +20,11 @@
 // (transmission < 0.5 at Bunch.cpp:194-197, ion overflow at LIP.cpp:1043-1048).
 //
 // Not built here (paths outside the library's scope, kept as the reference's
-// declarations only): space charge, ramping, drive mode, the per-bunch TBT
-// and ion-dump writers (MPBeamDataPrintPerTurn, SSIonDataPrint), the cavity
+// declarations only): PIC beam-ion, ramping, drive mode, the per-particle
+// dump of MPBeamDataPrintPerTurn, the ion dump (SSIonDataPrint), the cavity
 // transient printout of InitialcavityResonator and the Haissinski solver.
 #include <cmath>
+#include <complex>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -193,12 +194,14 @@ void build_config(GpuBeam& g, const ReadInputSettings& in, const LatticeInterAct
   c.flag_lr_wake = run->lRWakeFlag;
   c.flag_sr_wake = run->sRWakeFlag;
   c.flag_fir = run->fIRBunchByBunchFeedbackFlag;
-  if (run->spaceChargeFlag || run->rampFlag || in.driveMode->driveModeOn ||
+  if (run->rampFlag || in.driveMode->driveModeOn ||
       (run->beamIonFlag && in.ringIonEffPara->ionCalSCMethod == 2)) {
-    std::cerr << "space charge, ramping, drive mode and PIC beam-ion are outside the GPU "
-                 "tracking path" << std::endl;
+    std::cerr << "ramping, drive mode and PIC beam-ion are outside the GPU tracking path"
+              << std::endl;
     exit(0);
   }
+  c.flag_sc = run->spaceChargeFlag;
+  for (int i = 0; i < 3; ++i) c.sc_mesh[i] = run->scMeshNum[i];
   if (run->bBImpFlag) {
     // the table MPBeam::Run reads (MPBeam.cpp:856-876): the impedance file of
     // BoardBandImp::ReadInImp (BoardBandImp.cpp:42-71) or the wake file of
@@ -575,6 +578,22 @@ void MPBeam::BeamSynRadDamping(const ReadInputSettings& inputParameter,
   check(g, cg_synrad(g.h, currentTurnNum), "BeamSynRadDamping");
 }
 
+void MPBeam::BeamTransferDueToSpaceChargePIC(PIC3D& scBeam3D, LatticeInterActionPoint& latticeInterActionPoint,
+                                             int k) {
+  GpuBeam& g = gpu(this);
+  (void)scBeam3D;
+  (void)latticeInterActionPoint;
+  check(g, cg_space_charge(g.h, k), "BeamTransferDueToSpaceChargePIC");
+}
+
+void MPBeam::BeamTransferDueToSpaceChargeAnalytical(LatticeInterActionPoint& latticeInterActionPoint, int k,
+                                                    ReadInputSettings& inputParameter) {
+  GpuBeam& g = gpu(this);
+  (void)latticeInterActionPoint;
+  (void)inputParameter;
+  check(g, cg_space_charge(g.h, k), "BeamTransferDueToSpaceChargeAnalytical");
+}
+
 void MPBeam::BBImpBeamInteraction(const ReadInputSettings& inputParameter, const BoardBandImp& boardBandImp,
                                   const LatticeInterActionPoint& latticeInterActionPoint) {
   GpuBeam& g = gpu(this);
@@ -625,6 +644,151 @@ void MPBeam::MarkParticleLostInBunch(const ReadInputSettings& inputParameter,
     exit(0);
   }
   check(g, rc, "MarkParticleLostInBunch");
+}
+
+// The pages of the short-range potentials file that the turn's SR step
+// writes (MPBunch.cpp:1950-2001): per bunch, the header at turn 0 and, at the
+// print turns, the bins' z, counts and x, y, z potentials.
+static void write_sr_potentials(GpuBeam& g, const ReadInputSettings& in, int turns, int M) {
+  const int B = in.ringSRWake->SRWBunchBinNum;
+  const int every = in.ringRun->bunchInfoPrintInterval;
+  std::ofstream fout(in.ringSRWake->SRWWakePotenWriteTo + ".sdds", std::ios_base::app);
+  std::vector<int> cnt(B);
+  std::vector<double> pot(3 * (size_t)B);
+  for (int j = 0; j < M; ++j) {
+    if (turns == 0) {
+      fout << "SDDS1" << std::endl;
+      fout << "&column name=z,              units=m,              type=float,  &end" << std::endl;
+      fout << "&column name=profile,                              type=float,  &end" << std::endl;
+      fout << "&column name=wakePotenX,                        type=float,  &end" << std::endl;
+      fout << "&column name=wakePotenY,                        type=float,  &end" << std::endl;
+      fout << "&column name=wakePotenZ,                        type=float,  &end" << std::endl;
+      fout << "&data mode=ascii, &end" << std::endl;
+    }
+    if (every == 0 || turns % every != 0) continue;
+    double zlo = 0, dz = 0;
+    check(g, cg_sr_bins(g.h, j, &zlo, &dz, cnt.data()), "cg_sr_bins");
+    check(g, cg_sr_potentials(g.h, j, pot.data()), "cg_sr_potentials");
+    const double dtBin = dz / 299792458.0;
+    fout << "! page number " << int(turns / 100) + 1 << std::endl << B << std::endl;
+    for (int i = 0; i < B; ++i)
+      fout << std::setw(15) << std::left << i * dtBin * 299792458.0 + zlo << std::setw(15) << std::left
+           << cnt[i] << std::setw(15) << std::left << pot[i] << std::setw(15) << std::left << pot[B + i]
+           << std::setw(15) << std::left << pot[2 * B + i] << std::endl;
+  }
+}
+
+// MPBeam::MPBeamDataPrintPerTurn (MPBeam.cpp:2319-2563) for the files this
+// library writes: <TBTBunchAverData>.sdds (every bunch's averages, sizes and
+// the cavity voltages it saw, one page per print turn) and
+// <TBTBunchPro>_<i>.sdds (the longitudinal profile of the printed bunches
+// from the RF step's bins).  The bunch fields the reference reads are
+// refreshed from the device first: totIonCharge (cg_bunch_ion_charge) and
+// bunchRFModeInfo (cg_rf_info); the moments are current after Run's
+// moments call.  The per-particle dump <TBTBunchDisData>_<j>.sdds needs the
+// accumulated phase advance of every particle, which the device does not
+// track: it is not written.
+void MPBeam::MPBeamDataPrintPerTurn(int nTurns, LatticeInterActionPoint& latticeInterActionPoint,
+                                    ReadInputSettings& inputParameter) {
+  GpuBeam& g = gpu(this);
+  (void)latticeInterActionPoint;
+  const auto* run = inputParameter.ringRun;
+  const int nres = inputParameter.ringParRf->resNum;
+  if (run->beamIonFlag) {
+    std::vector<double> q(beamVec.size());
+    check(g, cg_bunch_ion_charge(g.h, q.data()), "cg_bunch_ion_charge");
+    for (size_t j = 0; j < beamVec.size(); ++j) beamVec[j].totIonCharge = q[j];
+  }
+  for (size_t j = 0; j < beamVec.size(); ++j)
+    for (int c = 0; c < nres; ++c) {
+      double v[8];
+      check(g, cg_rf_info(g.h, (int)j, c, v), "cg_rf_info");
+      auto* info = beamVec[j].bunchRFModeInfo;
+      info->cavVolBunchCen[c] = std::complex<double>(v[0], v[1]);
+      info->genVolBunchAver[c] = std::complex<double>(v[2], v[3]);
+      info->induceVolBunchCen[c] = std::complex<double>(v[4], v[5]);
+      info->selfLossVolBunchCen[c] = std::complex<double>(v[6], v[7]);
+    }
+  // the reference opens <TBTBunchAverData>.sdds even when the name is empty
+  { std::ofstream touch(run->TBTBunchAverData + ".sdds", std::ios_base::app); }
+  if (!run->TBTBunchAverData.empty()) {
+    std::ofstream fout(run->TBTBunchAverData + ".sdds", std::ios_base::app);
+    if (nTurns == 0) {
+      fout << "SDDS1" << std::endl;
+      const char* cols[][3] = {
+          {"Turns", "", "long"}, {"HarmIndex", "", "long"}, {"BunchIndex", "", "long"},
+          {"TotIonCharge", "e", "float"}, {"AverX", "m", "float"}, {"AverY", "m", "float"},
+          {"AverZ", "m", "float"}, {"AverXP", "rad", "float"}, {"AverYP", "rad", "float"},
+          {"AverZP", "rad", "float"}, {"RmsEmitX", "m*rad", "float"}, {"RmsEmitY", "m*rad", "float"},
+          {"RmsEmitZ", "m*rad", "float"}, {"RmsRX", "m*rad", "float"}, {"RmsRY", "m*rad", "float"},
+          {"RmsBunchLength", "m", "float"}, {"RmsBunchEnergySpread", "rad", "float"}};
+      for (auto& c : cols) {
+        fout << "&column name=" << c[0] << ", ";
+        if (c[1][0]) fout << "units=" << c[1] << ", ";
+        fout << "type=" << c[2] << ",  &end" << std::endl;
+      }
+      const char* per_cav[][2] = {{"cavAmp_", "V"}, {"cavPhase_", "rad"}, {"cavReal_", "V"},
+                                  {"genAmp_", "V"}, {"genPhase_", "rad"}, {"beamIndAmp_", "V"},
+                                  {"beamIndPhase_", "rad"}};
+      for (int c = 0; c < nres; ++c)
+        for (auto& q : per_cav)
+          fout << "&column name=" << q[0] << c << ", units=" << q[1] << ", type=float,  &end" << std::endl;
+      fout << "&data mode=ascii, &end" << std::endl;
+    }
+    fout << "! page number " << nTurns + 1 << std::endl << beamVec.size() << std::endl;
+    for (size_t i = 0; i < beamVec.size(); ++i) {
+      const MPBunch& b = beamVec[i];
+      auto col = [&](double v) { fout << std::setw(24) << std::left << std::setprecision(16) << v; };
+      fout << std::setw(24) << std::left << std::setprecision(16) << nTurns;
+      fout << std::setw(24) << std::left << std::setprecision(16) << b.bunchHarmNum;
+      fout << std::setw(24) << std::left << std::setprecision(16) << i;
+      for (double v : {b.totIonCharge, b.xAver, b.yAver, b.zAver, b.pxAver, b.pyAver, b.pzAver,
+                       b.emittanceX, b.emittanceY, b.emittanceZ, b.rmsRx, b.rmsRy, b.rmsBunchLength,
+                       b.rmsEnergySpread})
+        col(v);
+      for (int c = 0; c < nres; ++c) {
+        const auto* info = b.bunchRFModeInfo;
+        col(std::abs(info->cavVolBunchCen[c]));
+        col(std::arg(info->cavVolBunchCen[c]));
+        col(info->cavVolBunchCen[c].real());
+        col(std::abs(info->genVolBunchAver[c]));
+        col(std::arg(info->genVolBunchAver[c]));
+        col(std::abs(info->induceVolBunchCen[c]));
+        col(std::arg(info->induceVolBunchCen[c]));
+      }
+      fout << std::endl;
+    }
+  }
+  if (!run->TBTBunchPro.empty() && run->TBTBunchPrintNum != 0) {
+    const int nb = inputParameter.ringParRf->rfBunchBinNum;
+    bool loading = false;
+    for (int c = 0; c < nres; ++c) loading = loading || inputParameter.ringParRf->rfMode[c] == 1;
+    for (int i = 0; i < run->TBTBunchPrintNum; ++i) {
+      std::ofstream fout2(run->TBTBunchPro + "_" + std::to_string(i) + ".sdds", std::ios_base::app);
+      if (nTurns == 0) {
+        fout2 << "SDDS1" << std::endl;
+        fout2 << "&column name=z,              units=m,     type=float,  &end" << std::endl;
+        fout2 << "&column name=rho,            units=C/m,   type=float,  &end" << std::endl;
+        fout2 << "&data mode=ascii, &end" << std::endl;
+      }
+      MPBunch& b = beamVec[run->TBTBunchDisDataBunchIndex[i]];
+      if (loading) {
+        // posZBins and densProfVsBin of the last RF step (MPBunch.cpp:1340-1356)
+        double zmax = 0, dz = 0;
+        std::vector<int> cnt(nb);
+        check(g, cg_rf_profile(g.h, run->TBTBunchDisDataBunchIndex[i], &zmax, &dz, cnt.data()),
+              "cg_rf_profile");
+        for (int k = 0; k < nb && k < (int)b.posZBins.size(); ++k) {
+          b.posZBins[k] = zmax - k * dz - dz / 2.0;
+          b.densProfVsBin[k] = cnt[k] / double(b.macroEleNumPerBunch) / dz;
+        }
+      }
+      fout2 << "! page number " << nTurns + 1 << std::endl << nb << std::endl;
+      for (int k = 0; k < nb; ++k)
+        fout2 << std::setw(20) << std::left << -b.posZBins[k] + b.zMaxCurrentTurn << std::setw(20)
+              << std::left << b.densProfVsBin[k] << std::endl;
+    }
+  }
 }
 
 // MPBeam::Run (MPBeam.cpp:826-1173): result.sdds with the reference's header
@@ -696,10 +860,16 @@ void MPBeam::Run(Train& train, LatticeInterActionPoint& latticeInterActionPoint,
        << L.resDrivingTerms->linearCouplingFactor << std::endl;
   fout << "! page number " << 1 << std::endl << nTurns << std::endl;
 
+  // MPBunch::BunchTransferDueToSRWake writes the short-range potentials of
+  // every bunch to <SRWWakePotenWriteTo>.sdds at every print turn
+  // (MPBunch.cpp:1950-2001); the device accumulates the transverse ones too
+  const bool sr_file = inputParameter.ringRun->sRWakeFlag && inputParameter.ringSRWake->pipeGeoInput.empty();
+  if (sr_file) check(g, cg_set_sr_potentials(g.h, 1), "cg_set_sr_potentials");
   for (int n = 0; n < nTurns; n++) {
     if (n % 10 == 0) std::cout << n << "  turns, bunch_0 transmission: " << beamVec[0].transmission << std::endl;
     currentTurnNum = n;
     check(g, cg_run_turns(g.h, n, 1), "Run");
+    if (sr_file) write_sr_potentials(g, inputParameter, n, (int)beamVec.size());
     check(g, cg_beam_rms(g.h, 0), "MPBeamRMSCal");
     mirror_moments(*this, g, true);
     for (size_t j = 0; j < beamVec.size(); ++j) beamVec[j].transmission = g.mom[j].transmission;
@@ -742,6 +912,8 @@ void MPBeam::Run(Train& train, LatticeInterActionPoint& latticeInterActionPoint,
            << std::setw(15) << std::left << b.transmission << std::setw(15) << std::left << b.xyCouplingAlpha;
     }
     fout << std::endl;
+    if (bunchInfoPrintInterval && n % bunchInfoPrintInterval == 0)
+      MPBeamDataPrintPerTurn(n, latticeInterActionPoint, inputParameter);
     if (cbm && n % bunchInfoPrintInterval == 0) check(g, cg_cbm_record(g.h), "cg_cbm_record");
   }
   fout.close();

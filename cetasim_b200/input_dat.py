@@ -246,7 +246,9 @@ def write_case(d: str, wl: Workload, n_turns: int = 1, print_interval: int | Non
         f"runFIRBunchByBunchFeedbackFlag = {int(cfg.flag_fir)}",
         f"runLongRangeWake = {int(cfg.flag_lr_wake)}",
         f"runShortRangeWake = {int(cfg.flag_sr_wake)}",
-        f"runBBIFlag = {int(cfg.bbi.flag)}", "runRamping = 0", "runSpaceCharge = 0 32 32 33",
+        f"runBBIFlag = {int(cfg.bbi.flag)}", "runRamping = 0",
+        "runSpaceCharge = " + " ".join(str(int(v)) for v in (
+            cfg.flag_sc, *(cfg.sc_mesh[i] if cfg.flag_sc else (32, 32, 33)[i] for i in range(3)))),
         f"runRandomSeed = {int(cfg.seed if seed is None else seed)}",
     ]
     if cfg.bbi.flag:

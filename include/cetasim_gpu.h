@@ -208,6 +208,9 @@ typedef struct cg_config {
   cg_rw_sectors sr_rw;           /* SRWPipeGeoInput: resistive-wall sectors of the
                                     short-range wake (n = 0: none) */
   cg_bbi bbi;                    /* broadband impedance (flag 0: off) */
+  int flag_sc;                   /* runSpaceCharge: 0 off, 1 Bassetti-Erskine slices,
+                                    2 2.5-D PIC, 3 linear field (ReadInputSettings.cpp:878-884) */
+  int sc_mesh[3];                /* runSpaceCharge's mesh: nx, ny (PIC nodes), nz (slices) */
 } cg_config;
 
 /* Per-bunch moments, the fields MPBunch::GetMPBunchRMS sets
@@ -253,8 +256,8 @@ int cg_lattice_init(const cg_ring* ring, cg_section* sections, int n_sections);
  * per-bunch macroparticle counts, harmonic numbers and electrons per bunch.
  * The arrays and cfg->sections are allocated by the library; release them
  * with cg_config_free.  Keys outside the MP tracking path are accepted and
- * ignored, except settings this library does not implement (runSpaceCharge,
- * ionCalSCMethod 2, driveModeOn, runRamping),
+ * ignored, except settings this library does not implement (ionCalSCMethod
+ * 2, driveModeOn, runRamping),
  * which return CG_ERR_UNSUPPORTED.  runCBMGR with runGrowthRateFittingStart /
  * End fills run_cbmgr and the fit window (checked as ReadInputSettings.cpp:
  * 946-956).  Optional keys beyond the reference: bunchMacroEleNumPerBunchList
@@ -327,8 +330,18 @@ int cg_rf_kick(cg_handle* h);
 int cg_resonator_state(cg_handle* h, int cavity, double* out6);
 int cg_set_resonator_state(cg_handle* h, int cavity, const double* in6);
 /* BunchRFModeInfo of bunch j and cavity c after the last RF step (Bunch.h:
- * 109-118): cavity, generator, induced and self-loss voltages, (re, im). */
+ * 109-118): cavity, generator, induced and self-loss voltages, (re, im).  For
+ * an ideal cavity the voltage at the bunch's last particle (Bunch.cpp:
+ * 466-478); zero before the first RF step. */
 int cg_rf_info(cg_handle* h, int j, int cavity, double* out8);
+/* The longitudinal bins of bunch j's last RF step with beam loading
+ * (MPBunch.cpp:1332-1356): zMaxCurrentTurn, the bin width and the survivors
+ * per bin, head first (posZBins[i] = zmax - i dz - dz / 2). */
+int cg_rf_profile(cg_handle* h, int j, double* zmax, double* dz, int* counts /* [rfBunchBinNum] */);
+/* MPBunch::totIonCharge of every bunch after the last turn (MPBunch.cpp:
+ * 1208-1209): the ion charge of all IPs right after the bunch's interaction
+ * at the last IP [e].  out = M doubles. */
+int cg_bunch_ion_charge(cg_handle* h, double* out);
 /* MPBeam::BeamLongiPosTransferOneTurn (Bunch.cpp:494-501). */
 int cg_longi_drift(cg_handle* h);
 /* MPBeam::BeamEnergyLossOneTurn (Bunch.cpp:483-491). */
@@ -351,6 +364,12 @@ int cg_bbi_kick(cg_handle* h);
  * potentials (wakePotenFromBBI; in the time domain the five temp[] sums).
  * out = 6 x cap doubles, row q at out + q * cap; n <= cap. */
 int cg_bbi_profile(cg_handle* h, int j, int* lo, int* n, double* out, int cap);
+/* Space charge at section k: MPBeam::BeamTransferDueToSpaceChargePIC
+ * (flag_sc 2, MPBeam.cpp:2565-2572 -> MPBunch.cpp:887-931, PIC2D.cpp) or
+ * ...Analytical (flag_sc 1 and 3, MPBeam.cpp:2574-2581 -> MPBunch.cpp:
+ * 695-885), with the bunch moments of section k (cg_beam_rms(h, k) first).
+ * The PIC mesh is limited to 64 x 64 nodes. */
+int cg_space_charge(cg_handle* h, int k);
 /* MPBeam::LRWakeBeamIntaction (MPBeam.cpp:3232-3349). */
 int cg_lr_wake(cg_handle* h);
 /* MPBeam::SRWakeBeamIntaction (MPBeam.cpp:2117-2123 ->
@@ -360,6 +379,14 @@ int cg_sr_wake(cg_handle* h, int turn);
  * start zlo, the bin width dz and the B per-bin particle counts
  * (MPBunch.cpp:1900-1919: histoParIndex[i].size()). */
 int cg_sr_bins(cg_handle* h, int j, double* zlo, double* dz, int* counts /* [SRWBunchBinNum] */);
+/* The transverse short-range potentials the reference accumulates and
+ * writes to <SRWWakePotenWriteTo>.sdds (MPBunch.cpp:1950-2001): on = 1
+ * computes them at every cg_sr_wake (resonator wakes only;
+ * CG_ERR_UNSUPPORTED with resistive-wall sectors).  cg_sr_potentials
+ * returns bunch j's x, y and z potentials of the last cg_sr_wake, 3 x B
+ * (x and y zero while off). */
+int cg_set_sr_potentials(cg_handle* h, int on);
+int cg_sr_potentials(cg_handle* h, int j, double* out /* [3 * SRWBunchBinNum] */);
 /* MPBeam::FIRBunchByBunchFeedback (MPBeam.cpp:2978-3090). */
 int cg_fir(cg_handle* h, int turn);
 /* MPBeam::MarkParticleLostInBunch (MPBeam.cpp:1358-1364 -> Bunch.cpp:172-200);

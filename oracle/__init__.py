@@ -175,6 +175,9 @@ class OracleBeam:
     def BBImpBeamInteraction(self):
         self._check(self.lib.or_bbi(self.s))
 
+    def BeamTransferDueToSpaceCharge(self, k):
+        self._check(self.lib.or_space_charge(self.s, k))
+
     def bbi_profile(self, j):
         """6 x nbins: bunch j's smoothed charge profile and the potentials of
         the planes Z, Dx, Dy, Qx, Qy over all profile bins, from the last
@@ -229,6 +232,12 @@ class OracleBeam:
         out = np.empty(8)
         self._check(self.lib.or_rf_info(self.s, j, c, _p(out)))
         return tuple(complex(out[2 * i], out[2 * i + 1]) for i in range(4))
+
+    def sr_potentials(self, j):
+        """srWakePoten of bunch j: x, y, z rows (3 x B)."""
+        out = np.empty(3 * int(self.wl.cfg.sr_bins))
+        self._check(self.lib.or_sr_potentials(self.s, j, _p(out)))
+        return out.reshape(3, -1)
 
     def sr_bins(self, j):
         zlo, dz = C.c_double(), C.c_double()

@@ -888,6 +888,14 @@ int or_rf_kick(or_state* s) {
           double re = r->cav_vreq_re[c] * cos(-th) - r->cav_vreq_im[c] * sin(-th);
           b->c[5][i] += re / r->electron_energy / pow(r->r_beta, 2);
         }
+        /* the bunch's BunchRFModeInfo: the voltage at its last particle
+           (Bunch.cpp:466-478) */
+        double th = b->c[4][b->n - 1] / C_LIGHT / r->r_beta * 2. * PI * (double)r->cav_harm[c] * fRF;
+        double* inf = s->rf_info + ((size_t)j * CG_MAX_CAVITIES + c) * 8;
+        inf[0] = r->cav_vreq_re[c] * cos(-th) - r->cav_vreq_im[c] * sin(-th);
+        inf[1] = r->cav_vreq_re[c] * sin(-th) + r->cav_vreq_im[c] * cos(-th);
+        inf[2] = inf[0]; inf[3] = inf[1];
+        inf[4] = inf[5] = inf[6] = inf[7] = 0.0;
       }
       continue;
     }
@@ -1242,6 +1250,10 @@ int or_sr_wake(or_state* s, int turn) {
   }
   return 0;
 }
+int or_sr_potentials(or_state* s, int j, double* out) {
+  memcpy(out, s->b[j].sr_pot, sizeof(double) * 3 * s->cfg.sr_bins);
+  return 0;
+}
 int or_sr_bins(or_state* s, int j, double* zlo, double* dz, int* counts) {
   *zlo = s->b[j].sr_zlo; *dz = s->b[j].sr_dz;
   if (counts) memcpy(counts, s->b[j].sr_counts, sizeof(int) * s->cfg.sr_bins);
@@ -1338,6 +1350,7 @@ int or_run_turns(or_state* s, int turn0, int n_turns) {
     for (int k = 0; k < s->K; ++k) {
       or_beam_rms(s, k);
       if (c->flag_beam_ion && (st = or_beam_ion_ip(s, n, k))) return st;
+      if (c->flag_sc && (st = or_space_charge(s, k))) return st;
       or_section_map(s, k);
       or_beam_rms(s, k);
     }
@@ -1633,6 +1646,189 @@ int or_bbi_profile(or_state* s, int j, int* nbins, double* out) {
   *nbins = s->bbi_nbins;
   if (out) memcpy(out, s->bbi_out + (size_t)j * 6 * s->bbi_nbins, sizeof(double) * 6 * s->bbi_nbins);
   return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Space charge: MPBeam::BeamTransferDueToSpaceChargePIC / ...Analytical      */
+/* (MPBeam.cpp:2565-2583), flag 2 / flags 1 and 3.                           */
+
+#define SC_EPSILON 8.854187817E-12
+#define SC_E_MASS 9.10938215E-31
+
+/* PIC2D::UpdateTransverseMomentum (PIC2D.cpp) and the same update of
+   MPBunch.cpp:740-760 / 809-829: the total momentum from (delta, y, px) */
+static void sc_update(double* px, double* py, double y, double dp, double p0, double ex, double ey,
+                      double ds) {
+  double pz = (1 + dp) * p0;
+  double tpx = pz * y;
+  double tpy = pz * *px;
+  double p = sqrt(pow(pz, 2) + pow(tpx, 2) + pow(tpy, 2));
+  double gamma = sqrt(1 + pow(p, 2));
+  double beta = p / gamma;
+  double dpx = ex / pow(gamma, 2) * E_CHARGE * ds / (beta * C_LIGHT) / (SC_E_MASS * p * C_LIGHT);
+  double dpy = ey / pow(gamma, 2) * E_CHARGE * ds / (beta * C_LIGHT) / (SC_E_MASS * p * C_LIGHT);
+  *px += dpx;
+  *py += dpy;
+}
+
+/* 2-D DST-I (FFTW RODFT00 on both axes of a row-major nx x ny array) */
+static void sc_dst2(const double* in, double* out, int nx, int ny) {
+  double* t = (double*)malloc(sizeof(double) * nx * ny);
+  for (int k = 0; k < nx; ++k)
+    for (int j = 0; j < ny; ++j) {
+      double a = 0;
+      for (int i = 0; i < nx; ++i)
+        a += in[i * ny + j] * 2 * sin(PI_REF() * (double)(((long)(i + 1) * (k + 1)) % (2 * (nx + 1))) / (nx + 1));
+      t[k * ny + j] = a;
+    }
+  for (int k = 0; k < nx; ++k)
+    for (int l = 0; l < ny; ++l) {
+      double a = 0;
+      for (int j = 0; j < ny; ++j)
+        a += t[k * ny + j] * 2 * sin(PI_REF() * (double)(((long)(j + 1) * (l + 1)) % (2 * (ny + 1))) / (ny + 1));
+      out[k * ny + l] = a;
+    }
+  free(t);
+}
+
+/* PIC2D::Set2DRho's cell and weights; 0 outside the mesh */
+static int sc_cell(double x, double y, const double* mx, const double* my, double hx, double hy,
+                   double dv, int nx, int ny, int* ix, int* iy, double w[4]) {
+  double tx = floor((x - mx[0]) / hx), ty = floor((y - my[0]) / hy);
+  if (!(tx >= 0 && tx < nx - 1 && ty >= 0 && ty < ny - 1)) return 0;
+  *ix = (int)tx;
+  *iy = (int)ty;
+  for (int j = 0; j < 4; j++) {
+    int dx = (j % 2 == 0) ? 1 : 0, dy = (j % 4 < 2) ? 1 : 0;
+    w[j] = fabs(x - mx[*ix + dx]) * fabs(y - my[*iy + dy]) / dv;
+  }
+  return 1;
+}
+
+int or_space_charge(or_state* s, int k) {
+  const cg_config* c = &s->cfg;
+  int flag = c->flag_sc, nx = c->sc_mesh[0], ny = c->sc_mesh[1], nz = c->sc_mesh[2];
+  if (!flag) return CG_ERR_NOT_READY;
+  double ds = s->sec[k].length;
+  double gamma0 = c->ring.electron_energy / E_MASS_EV;
+  double beta0 = sqrt(1 - 1 / pow(gamma0, 2));
+  double p0 = beta0 * gamma0;
+  double* mx = (double*)malloc(sizeof(double) * (nx > 0 ? nx : 1));
+  double* my = (double*)malloc(sizeof(double) * (ny > 0 ? ny : 1));
+  double* rho = (double*)malloc(sizeof(double) * (flag == 2 ? nx * ny : 1));
+  double* phi = (double*)malloc(sizeof(double) * (flag == 2 ? nx * ny : 1));
+  double* ex = (double*)malloc(sizeof(double) * (flag == 2 ? nx * ny : 1));
+  double* ey = (double*)malloc(sizeof(double) * (flag == 2 ? nx * ny : 1));
+  int st = 0;
+  for (int jb = 0; jb < s->M && !st; ++jb) {
+    or_bunch* b = &s->b[jb];
+    double range = 10.0, dv = 1.0, hx = 0, hy = 0;
+    if (flag == 2) {
+      /* PIC2D::Set2DMesh(rmsXY, averXY) from the bunch's moments (MPBunch.cpp:890-904) */
+      double rms[2] = {b->m.rms_x, b->m.rms_y}, cen[2] = {b->m.mean[0], b->m.mean[2]};
+      if (rms[0] == 0 || rms[1] == 0) { st = CG_ERR_INVALID; break; }
+      double len[2] = {rms[0] * 2 * range, rms[1] * 2 * range};
+      double lmax = len[0] > len[1] ? len[0] : len[1];
+      hx = lmax / (nx - 1);
+      hy = lmax / (ny - 1);
+      dv *= hx;
+      dv *= hy;
+      for (int i = 0; i < nx; i++) mx[i] = (cen[0] - lmax / 2) + hx * i;
+      for (int i = 0; i < ny; i++) my[i] = (cen[1] - lmax / 2) + hy * i;
+    }
+    /* MPBunch::SetSlicedBunchInfo (MPBunch.cpp:660-693) */
+    zminmax(b);
+    double zMin = b->m.z_min, zMax = b->m.z_max;
+    double dz = (zMax - zMin) / (nz - 1);
+    int* sl = (int*)malloc(sizeof(int) * b->n);
+    int* cnt = (int*)calloc(nz, sizeof(int));
+    for (int i = 0; i < b->n; i++) {
+      double t = floor((b->c[4][i] - zMin) / dz);
+      sl[i] = t < 0 ? 0 : (t > nz - 1 ? nz - 1 : (int)t);
+      cnt[sl[i]]++;
+    }
+    double charge = b->q_macro * E_CHARGE / dz; /* [C/m] */
+    for (int q = 0; q < nz; ++q) {
+      if (cnt[q] < 2) continue; /* MPBunch.cpp:916 */
+      if (flag == 2) {
+        /* PIC2D::Set2DRho, Set2DPhi, Set2DEField (PIC2D.cpp) */
+        for (int t = 0; t < nx * ny; ++t) rho[t] = 0;
+        for (int i = 0; i < b->n; i++) {
+          if (sl[i] != q) continue;
+          int ix, iy;
+          double w[4];
+          if (!sc_cell(b->c[0][i], b->c[2][i], mx, my, hx, hy, dv, nx, ny, &ix, &iy, w)) continue;
+          rho[ix * ny + iy] += w[0] * charge / dv;
+          rho[(ix + 1) * ny + iy] += w[1] * charge / dv;
+          rho[ix * ny + iy + 1] += w[2] * charge / dv;
+          rho[(ix + 1) * ny + iy + 1] += w[3] * charge / dv;
+        }
+        sc_dst2(rho, phi, nx, ny);
+        for (int i = 0; i < nx; ++i)
+          for (int j = 0; j < ny; ++j) {
+            double knx = PI_REF() / 2 * (i + 1) / (nx + 1);
+            double kny = PI_REF() / 2 * (j + 1) / (ny + 1);
+            double K = pow(2 * sin(knx) / hx, 2) + pow(2 * sin(kny) / hy, 2);
+            phi[i * ny + j] = phi[i * ny + j] / K / SC_EPSILON;
+          }
+        sc_dst2(phi, rho, nx, ny);
+        for (int t = 0; t < nx * ny; ++t) phi[t] = rho[t] / (4 * (nx + 1) * (ny + 1));
+        for (int i = 0; i < nx; ++i)
+          for (int j = 0; j < ny; ++j) {
+            double x1 = i == 0 ? 0 : phi[(i - 1) * ny + j], x2 = i == nx - 1 ? 0 : phi[(i + 1) * ny + j];
+            double y1 = j == 0 ? 0 : phi[i * ny + j - 1], y2 = j == ny - 1 ? 0 : phi[i * ny + j + 1];
+            ex[i * ny + j] = -(x2 - x1) / (2 * hx);
+            ey[i * ny + j] = -(y2 - y1) / (2 * hy);
+          }
+        for (int i = 0; i < b->n; i++) {
+          if (sl[i] != q) continue;
+          int ix, iy;
+          double w[4], fx = 0, fy = 0;
+          if (sc_cell(b->c[0][i], b->c[2][i], mx, my, hx, hy, dv, nx, ny, &ix, &iy, w)) {
+            fx = ex[ix * ny + iy] * w[0] + ex[(ix + 1) * ny + iy] * w[1] + ex[ix * ny + iy + 1] * w[2] +
+                 ex[(ix + 1) * ny + iy + 1] * w[3];
+            fy = ey[ix * ny + iy] * w[0] + ey[(ix + 1) * ny + iy] * w[1] + ey[ix * ny + iy + 1] * w[2] +
+                 ey[(ix + 1) * ny + iy + 1] * w[3];
+          }
+          sc_update(&b->c[1][i], &b->c[3][i], b->c[2][i], b->c[5][i], p0, fx, fy, ds);
+        }
+      } else {
+        /* UpdateTransverseMomentumBEModel / ...Linear (MPBunch.cpp:695-831) */
+        double cen[2] = {0, 0}, rms[2] = {0, 0}, lambda = 0;
+        for (int d = 0; d < 2; ++d) {
+          for (int i = 0; i < b->n; i++)
+            if (sl[i] == q) cen[d] += b->c[2 * d][i];
+          cen[d] /= cnt[q];
+          for (int i = 0; i < b->n; i++)
+            if (sl[i] == q) rms[d] += pow(b->c[2 * d][i] - cen[d], 2);
+          rms[d] = sqrt(rms[d] / cnt[q]);
+        }
+        for (int i = 0; i < b->n; i++)
+          if (sl[i] == q) lambda += charge;
+        for (int i = 0; i < b->n; i++) {
+          if (sl[i] != q) continue;
+          double posx = b->c[0][i] - cen[0], posy = b->c[2][i] - cen[1], fx, fy, Ex, Ey;
+          if (flag == 1) {
+            if ((rms[0] - rms[1]) / rms[1] > 1.e-4) be1(posx, posy, rms[0], rms[1], &fx, &fy);
+            else if ((rms[0] - rms[1]) / rms[1] < -1.e-4) be1(posy, posx, rms[1], rms[0], &fy, &fx);
+            else round_field(posx, posy, rms[0], &fx, &fy);
+            Ex = -lambda / PI_REF() / 2.0 / SC_EPSILON * fx;
+            Ey = -lambda / PI_REF() / 2.0 / SC_EPSILON * fy;
+          } else {
+            fx = posx / (rms[0] * (rms[0] + rms[1]));
+            fy = posy / (rms[1] * (rms[0] + rms[1]));
+            Ex = lambda / PI_REF() / SC_EPSILON * fx;
+            Ey = lambda / PI_REF() / SC_EPSILON * fy;
+          }
+          sc_update(&b->c[1][i], &b->c[3][i], b->c[2][i], b->c[5][i], p0, Ex, Ey, ds);
+        }
+      }
+    }
+    free(sl);
+    free(cnt);
+  }
+  free(mx); free(my); free(rho); free(phi); free(ex); free(ey);
+  return st;
 }
 
 /* accessors for the ion clouds */

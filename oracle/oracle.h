@@ -45,6 +45,7 @@ int or_synrad(or_state* s, int turn);
 int or_lr_wake(or_state* s);
 int or_sr_wake(or_state* s, int turn);
 int or_bbi(or_state* s);
+int or_space_charge(or_state* s, int k);
 int or_bbi_profile(or_state* s, int j, int* nbins, double* out);
 int or_fir(or_state* s, int turn);
 int or_mark_lost(or_state* s, double* transmissions);
@@ -56,6 +57,7 @@ int or_ion_upload(or_state* s, int k, int p, const double* x, const double* y,
                   const double* vx, const double* vy, int count);
 int or_ion_cloud_record(or_state* s, int k, double* out);
 int or_sr_bins(or_state* s, int j, double* zlo, double* dz, int* counts);
+int or_sr_potentials(or_state* s, int j, double* out);
 int or_lr_add_rw(or_state* s, const double* yok);
 int or_sr_set_rw(or_state* s, const double* yok);
 double or_rw_fz(double u);

@@ -20,7 +20,7 @@ EXE = os.path.join(HERE, "_ref", "cetasim_ref")
 
 # stage numbers of ref_stage (ref_harness.cpp)
 ST_RMS, ST_ION, ST_MAP, ST_SKEW, ST_RF, ST_DRIFT, ST_ELOSS, ST_SYNRAD = range(8)
-ST_LR, ST_SR, ST_FIR, ST_LOST, ST_RMS_ONLY, ST_BBI = range(8, 14)
+ST_LR, ST_SR, ST_FIR, ST_LOST, ST_RMS_ONLY, ST_BBI, ST_SC = range(8, 15)
 
 MOMENT_FIELDS = ["n_alive", "n_macro", "mean", "emit", "eff_emit", "rms_x", "rms_y",
                  "eff_rms_x", "eff_rms_y", "bunch_length", "energy_spread", "z_min", "z_max",
@@ -48,7 +48,7 @@ def load():
         for n in ("ref_info", "ref_bunch_info", "ref_set_emit_nat", "ref_bunch_size", "ref_set_bunch",
                   "ref_get_bunch", "ref_moments", "ref_beam_info", "ref_stage", "ref_run_turns",
                   "ref_ion_count", "ref_ion_get", "ref_ion_set", "ref_sr_bins", "ref_ring",
-                  "ref_resonator", "ref_rf_info", "ref_bbi_profile"):
+                  "ref_resonator", "ref_rf_info", "ref_bbi_profile", "ref_bunch_ion_charge"):
             getattr(L, n).restype = C.c_int
         L.cg_ref_seed.argtypes = [C.c_ulonglong, C.c_longlong]
         L.cg_ref_seed.restype = None
@@ -131,6 +131,11 @@ class RefBeam:
         out = (C.c_double * 4)()
         self._check(self.lib.ref_bunch_info(self.h, j, out))
         return {"ne": out[0], "macro_charge": out[1], "harm": int(out[2]), "gap": int(out[3])}
+
+    def bunch_ion_charge(self, j):
+        out = C.c_double()
+        self._check(self.lib.ref_bunch_ion_charge(self.h, j, C.byref(out)))
+        return out.value
 
     def ring(self):
         out = np.empty(16)
@@ -218,6 +223,9 @@ class RefBeam:
 
     def BBImpBeamInteraction(self):
         self.stage(ST_BBI)
+
+    def BeamTransferDueToSpaceCharge(self, k):
+        self.stage(ST_SC, 0, k)
 
     def bbi_profile(self, j):
         """6 x (2n - 1): profileForBunchBBImp and the five wakePotenFromBBI

@@ -41,6 +41,7 @@
 #include "FIRFeedBack.h"
 #include "LatticeInterActionPoint.h"
 #include "MPBeam.h"
+#include "PIC3D.h"
 #include "ReadInputSettings.h"
 #include "Train.h"
 #include "WakeFunction.h"
@@ -64,6 +65,9 @@ struct RefRun {
     WakeFunction lr, sr;
     FIRFeedBack fir;
     BoardBandImp bbi;
+    // PIC3D's destructor frees members only InitialSC3D sets (PIC3D.cpp:
+    // 41-65), so the object exists only when the PIC space charge is on
+    std::unique_ptr<PIC3D> pic;
     uint64_t birth_seed = 0;
 };
 
@@ -161,7 +165,8 @@ enum Stage {
     ST_FIR = 10,      // FIRBunchByBunchFeedback(turn)
     ST_LOST = 11,     // MarkParticleLostInBunch
     ST_RMS_ONLY = 12, // MPBeamRMSCal(k) alone
-    ST_BBI = 13       // BBImpBeamInteraction
+    ST_BBI = 13,      // BBImpBeamInteraction
+    ST_SC = 14        // BeamTransferDueToSpaceChargePIC / ...Analytical(k)
 };
 
 void stage(RefRun *r, int s, int turn, int k) {
@@ -183,6 +188,11 @@ void stage(RefRun *r, int s, int turn, int k) {
         case ST_LOST: b.MarkParticleLostInBunch(in, r->lat); break;
         case ST_RMS_ONLY: b.MPBeamRMSCal(r->lat, k); break;
         case ST_BBI: b.BBImpBeamInteraction(in, r->bbi, r->lat); break;
+        case ST_SC:
+            if (in.ringRun->spaceChargeFlag == 2) b.BeamTransferDueToSpaceChargePIC(*r->pic, r->lat, k);
+            if (in.ringRun->spaceChargeFlag == 1 || in.ringRun->spaceChargeFlag == 3)
+                b.BeamTransferDueToSpaceChargeAnalytical(r->lat, k, in);
+            break;
         default: throw std::runtime_error("unknown stage");
     }
 }
@@ -195,6 +205,7 @@ void turn(RefRun *r, int n) {
     for (int k = 0; k < K; ++k) {
         stage(r, ST_RMS, n, k);
         if (in.ringRun->beamIonFlag) stage(r, ST_ION, n, k);
+        if (in.ringRun->spaceChargeFlag) stage(r, ST_SC, n, k);
         stage(r, ST_MAP, n, k);
         stage(r, ST_RMS_ONLY, n, k);
     }
@@ -271,6 +282,12 @@ void *ref_open(const char *input_path, unsigned long long seed) {
         if (r->in.ringRun->lRWakeFlag) r->lr.InitialLRWake(r->in, r->lat);
         step = "WakeFunction::InitialSRWake";
         if (r->in.ringRun->sRWakeFlag) r->sr.InitialSRWake(r->in, r->lat);
+        // MPBeam.cpp:894
+        step = "PIC3D::InitialSC3D";
+        if (r->in.ringRun->spaceChargeFlag == 2) {
+            r->pic.reset(new PIC3D());
+            r->pic->InitialSC3D(r->in);
+        }
         // MPBeam.cpp:853-876
         step = "BoardBandImp";
         if (r->in.ringRun->bBImpFlag) {
@@ -316,6 +333,14 @@ int ref_bunch_info(void *h, int j, double *out4) {
     out4[1] = B.macroEleCharge;
     out4[2] = B.bunchHarmNum;
     out4[3] = B.bunchGap;
+    return 0;
+}
+
+// MPBunch::totIonCharge of bunch j (MPBunch.cpp:1208-1209)
+int ref_bunch_ion_charge(void *h, int j, double *out) {
+    RefRun *r = static_cast<RefRun *>(h);
+    if (j < 0 || j >= (int)r->beam.beamVec.size()) return 1;
+    *out = r->beam.beamVec[j].totIonCharge;
     return 0;
 }
 

@@ -29,9 +29,11 @@
 //    complete elliptic K by the arithmetic-geometric mean, I_nu by its power
 //    series (the resistive-wall wakes, WakeFunction.cpp:387-497, 787-941).
 //
-// Eigen-solvers and r2r/many-dimensional FFT plans are reached only by paths
-// outside the multi-particle tracking (one-turn-matrix diagnostics, PIC space
-// charge): they abort.
+//  * FFTW's 2-D RODFT00 (DST-I on both axes of one contiguous array, the
+//    Poisson solve of the 2.5-D PIC space charge, PIC2D.cpp) as direct sums.
+//
+// Eigen-solvers and the other r2r / many-dimensional FFT plans (the 3-D
+// solver of PIC3D, not on the 2.5-D path) are planned but abort if executed.
 #include "gsl/gsl_shim_all.h"
 #include "fftw3.h"
 
@@ -701,11 +703,12 @@ const char *gsl_strerror(int e) { return e == 0 ? "success" : "failure"; }
 }  // extern "C"
 
 struct cg_fftw_plan_s {
-    int kind;  // 0 dft_1d, 1 r2c, 2 c2r, 3 unsupported
+    int kind;  // 0 dft_1d, 1 r2c, 2 c2r, 3 unsupported, 4 2-D RODFT00 (n x n2)
     int n;
     int sign;
     void *in;
     void *out;
+    int n2;
 };
 
 namespace {
@@ -713,8 +716,8 @@ std::mutex g_fftw_mu;
 std::set<void *> g_fftw_mem;
 std::set<void *> g_fftw_plans;
 
-fftw_plan make_plan(int kind, int n, int sign, void *in, void *out) {
-    fftw_plan p = new cg_fftw_plan_s{kind, n, sign, in, out};
+fftw_plan make_plan(int kind, int n, int sign, void *in, void *out, int n2 = 0) {
+    fftw_plan p = new cg_fftw_plan_s{kind, n, sign, in, out, n2};
     std::lock_guard<std::mutex> g(g_fftw_mu);
     g_fftw_plans.insert(p);
     return p;
@@ -754,8 +757,15 @@ fftw_plan fftw_plan_many_dft(int, const int *, int, fftw_complex *, const int *,
                              fftw_complex *, const int *, int, int, int, unsigned) {
     return make_plan(3, 0, 0, nullptr, nullptr);
 }
-fftw_plan fftw_plan_many_r2r(int, const int *, int, double *, const int *, int, int, double *,
-                             const int *, int, int, const fftw_r2r_kind *, unsigned) {
+// One contiguous 2-D array with FFTW_RODFT00 on both axes (the plan of
+// PIC2D::InitialPIC2D, PIC2D.cpp) is executed; other layouts are planned
+// (PIC3D::InitialSC3D makes them) but abort if executed.
+fftw_plan fftw_plan_many_r2r(int rank, const int *n, int howmany, double *in, const int *, int istride,
+                             int, double *out, const int *, int ostride, int,
+                             const fftw_r2r_kind *kind, unsigned) {
+    if (rank == 2 && howmany == 1 && istride == 1 && ostride == 1 && kind[0] == FFTW_RODFT00 &&
+        kind[1] == FFTW_RODFT00)
+        return make_plan(4, n[0], 0, in, out, n[1]);
     return make_plan(3, 0, 0, nullptr, nullptr);
 }
 fftw_plan fftw_plan_r2r(int, const int *, double *, double *, const fftw_r2r_kind *, unsigned) {
@@ -814,6 +824,28 @@ void fftw_execute(const fftw_plan p) {
             }
             y[j] = s;
         }
+        std::memcpy(p->out, y.data(), sizeof(double) * y.size());
+    } else if (p->kind == 4) {
+        // RODFT00 along both axes of a row-major n x n2 array:
+        // Y_k = 2 sum_j X_j sin(pi (j + 1)(k + 1) / (m + 1)) per axis
+        const int nx = p->n, ny = p->n2;
+        const double *x = static_cast<const double *>(p->in);
+        auto sn = [](long long a, long long b, int m) {
+            return 2.0 * std::sin(M_PI * static_cast<double>((a * b) % (2 * (m + 1))) / (m + 1));
+        };
+        std::vector<double> t(static_cast<size_t>(nx) * ny), y(t.size());
+        for (int k = 0; k < nx; ++k)
+            for (int j = 0; j < ny; ++j) {
+                double a = 0.0;
+                for (int i = 0; i < nx; ++i) a += x[i * ny + j] * sn(i + 1, k + 1, nx);
+                t[k * ny + j] = a;
+            }
+        for (int k = 0; k < nx; ++k)
+            for (int l = 0; l < ny; ++l) {
+                double a = 0.0;
+                for (int j = 0; j < ny; ++j) a += t[k * ny + j] * sn(j + 1, l + 1, ny);
+                y[k * ny + l] = a;
+            }
         std::memcpy(p->out, y.data(), sizeof(double) * y.size());
     } else {
         unreachable("an FFTW r2r / many-dimensional transform");

@@ -98,6 +98,31 @@ def test_dropin_result_sdds_matches_the_reference_program(tmp_path):
     # the run writes the files the reference writes besides result.sdds
     for f in ("elegant_filling_train_para.sdds",):
         assert open(os.path.join(dref, f)).read() == open(os.path.join(dgpu, f)).read()
+    # the short-range potentials of every bunch at the print turns
+    # (MPBunch.cpp:1950-2001): bins, counts and the x, y, z potentials
+    pr, pg = sr_pages(os.path.join(dref, "srw_poten.sdds")), sr_pages(os.path.join(dgpu, "srw_poten.sdds"))
+    assert len(pr) == len(pg) == 40
+    for a, b in zip(pr, pg):
+        assert a.shape == b.shape == (20, 5)
+        assert np.array_equal(a[:, 1], b[:, 1])
+        for k in (0, 2, 3, 4):
+            scale = np.max(np.abs(a[:, k])) + 1e-300
+            assert np.all(np.abs(a[:, k] - b[:, k]) <= 2e-5 * np.maximum(np.abs(a[:, k]), 1e-3 * scale)), k
+
+
+def sr_pages(path):
+    """The pages of a file with a header before each page group (the
+    reference writes one per bunch at turn 0)."""
+    lines = open(path).read().splitlines()
+    pages, i = [], 0
+    while i < len(lines):
+        if lines[i].startswith("! page number"):
+            n = int(lines[i + 1])
+            pages.append(np.array([[float(v) for v in ln.split()] for ln in lines[i + 2:i + 2 + n]]))
+            i += 2 + n
+        else:
+            i += 1
+    return pages
 
 
 def test_dropin_with_beam_loading_matches_the_reference_program(tmp_path):
@@ -160,3 +185,87 @@ def test_dropin_with_broadband_impedance_matches_the_reference_program(tmp_path,
         rtol = 2e-4 if name.startswith(("eigenEmit", "xyCoupling")) else 2e-5
         bad = np.abs(a - b) > rtol * np.maximum(np.abs(a), 1e-3 * scale)
         assert not bad.any(), (name, a[bad][:3], b[bad][:3])
+
+
+@pytest.mark.parametrize("case_name", ["pic_train", "linear_train"])
+def test_dropin_with_space_charge_matches_the_reference_program(tmp_path, case_name):
+    """8 bunches of the fast-ion ring with the space-charge kick at every
+    section (2.5-D PIC, and the linear model; radiation off): result.sdds of
+    the drop-in against the reference program over 20 turns."""
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    import sccases
+    wl, _, _ = sccases.build(case_name, str(tmp_path / "base"))
+    wl.cfg.flag_synrad = 0
+    src = tmp_path / "src"
+    input_dat.write_case(str(src), wl, n_turns=20, qe=False)
+    dirs = []
+    for name in ("ref", "gpu"):
+        d = tmp_path / name
+        shutil.copytree(src, d)
+        dirs.append(str(d))
+    cols_r, rows_r = run(ref.EXE, dirs[0], teardown_may_crash=True)
+    cols_g, rows_g = run(DROPIN, dirs[1])
+    assert cols_r == cols_g and rows_r.shape == rows_g.shape == (20, len(cols_r))
+    for k, name in enumerate(cols_r):
+        if name == "IonCharge":
+            continue
+        a, b = rows_r[:, k], rows_g[:, k]
+        scale = np.max(np.abs(a)) + 1e-300
+        rtol = 2e-4 if name.startswith(("eigenEmit", "xyCoupling")) else 2e-5
+        bad = np.abs(a - b) > rtol * np.maximum(np.abs(a), 1e-3 * scale)
+        assert not bad.any(), (name, a[bad][:3], b[bad][:3])
+
+
+def read_pages(path):
+    """Every page of a multi-page SDDS ASCII file: (column names, [rows per page])."""
+    lines = open(path).read().splitlines()
+    cols = [ln.split("name=")[1].split(",")[0] for ln in lines if ln.startswith("&column")]
+    pages = []
+    i = next(k for k, ln in enumerate(lines) if ln.startswith("&data")) + 1
+    while i < len(lines):
+        assert lines[i].startswith("! page number"), lines[i]
+        n = int(lines[i + 1])
+        pages.append(np.array([[float(v) for v in ln.split()] for ln in lines[i + 2:i + 2 + n]]))
+        i += 2 + n
+    return cols, pages
+
+
+def test_dropin_per_bunch_files_match_the_reference_program(tmp_path):
+    """<runTBTBunchAverData>.sdds (every bunch's averages and the voltages of
+    the loaded main cavity it saw) and <runTBTBunchProfile>_0.sdds (the
+    longitudinal profile of the RF step's bins) of the 80-bunch train with
+    bin-by-bin beam loading and direct feedback, every 5 turns over 20: the
+    drop-in's files against the reference program's."""
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    import blcases
+    wl, _, _ = blcases.build("train_binned_fb", str(tmp_path / "base"))
+    wl.cfg.flag_synrad = 0
+    src = tmp_path / "src"
+    input_dat.write_case(str(src), wl, n_turns=20, print_interval=5, qe=False,
+                         extra=["runTBTBunchAverData = tbt_aver", "runTBTBunchProfile = tbt_pro"])
+    dirs = []
+    for name in ("ref", "gpu"):
+        d = tmp_path / name
+        shutil.copytree(src, d)
+        dirs.append(str(d))
+    run(ref.EXE, dirs[0], teardown_may_crash=True)
+    run(DROPIN, dirs[1])
+    for f in ("tbt_aver.sdds", "tbt_pro_0.sdds"):
+        cr, pr = read_pages(os.path.join(dirs[0], f))
+        cg, pg = read_pages(os.path.join(dirs[1], f))
+        assert cr == cg and len(pr) == len(pg) == 4, f
+        for a, b in zip(pr, pg):
+            assert a.shape == b.shape
+            for k, name in enumerate(cr):
+                if name == "TotIonCharge":  # never set without ions
+                    continue
+                x, y = a[:, k], b[:, k]
+                scale = np.max(np.abs(x)) + 1e-300
+                if name.endswith(("Phase_0",)):
+                    # angles near +-pi: compare on the circle
+                    d = np.abs(np.angle(np.exp(1j * (x - y))))
+                else:
+                    d = np.abs(x - y)
+                assert np.all(d <= 1e-7 * np.maximum(np.abs(x), 1e-3 * scale) + 1e-300), (f, name)

@@ -89,6 +89,20 @@ def test_gpu_and_reference_side_by_side_fast_ion_ip_records(tmp_path):
             assert np.array_equal(sr, sg)
             worst = max(worst, refcases.coord_rel_err(cg, cr, sr == 0).max())
         assert worst <= 1e-11, f"IP {k}: {worst:.3e}"
+    # after the last IP: every bunch's totIonCharge (MPBunch.cpp:1208-1209)
+    import ctypes as C
+    q = np.empty(wl.n_bunches)
+    g._check(g.lib.cg_bunch_ion_charge(g.h, q.ctypes.data_as(C.POINTER(C.c_double))))
+    want = np.array([r.bunch_ion_charge(j) for j in range(wl.n_bunches)])
+    assert np.max(np.abs(q - want)) <= 1e-12 * np.max(np.abs(want))
+    # the ideal cavity's voltage at each bunch's last particle after an RF step
+    for b in (r, g):
+        b.BeamMomtumUpdateDueToRFTest()
+    for j in range(0, wl.n_bunches, 7):
+        want = r.rf_info(j, 0)
+        got = g.rf_info(j, 0)
+        for a, b_ in zip(got, want):
+            assert abs(a - b_) <= 1e-12 * abs(want[0])
 
 
 @pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")

@@ -111,6 +111,24 @@ def test_sr_wake_bins_bit_exact_and_kick():
     assert np.max(np.abs(kick_g - kick_o)) <= 1e-11 * np.max(np.abs(kick_o))
 
 
+def test_sr_wake_transverse_potentials_accumulate_as_the_oracle():
+    """The x, y potentials the reference accumulates for its potentials file
+    (MPBunch.cpp:1981-1993, both from the horizontal centroids), over turns
+    with the beam moving, against the oracle; the z row is the kick's."""
+    wl = small("plain_single", 0.05)
+    g, o = pair(wl, particles(wl))
+    g.set_sr_potentials(True)
+    for turn in range(3):
+        for b in (g, o):
+            b.MPBeamRMSCal(0)
+            b.SRWakeBeamIntaction(turn)
+            b.BeamTransferPerInteractionPointDueToLatticeT(0)
+        pg, po = g.sr_potentials(0), o.sr_potentials(0)
+        for q in range(3):
+            sc = np.max(np.abs(po[q]))
+            assert sc > 0 and np.max(np.abs(pg[q] - po[q])) <= 1e-11 * sc, (turn, q)
+
+
 def test_lr_wake_and_fir_over_turns():
     wl = small("batched_uneven", 0.004)  # 900 bunches x 20..200
     g, o = pair(wl, particles(wl, seed=9, spread=5.0))

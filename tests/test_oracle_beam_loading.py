@@ -87,3 +87,22 @@ def test_input_reads_the_cavity_settings():
     fh = float(r.cav_harm[0] * r.harmonics) * r.f0
     assert r.res_fre[0] == fh + r.res_detune[0]
     assert r.res_tf[0] == 2 * r.res_ql[0] / (2 * (4 * np.arctan(1.0)) * r.res_fre[0])
+
+
+@live
+def test_ideal_cavity_bunch_info_against_the_live_reference():
+    """BunchRFModeInfo of the ideal main cavity beside the loaded harmonic
+    one: the voltage at each bunch's last particle (Bunch.cpp:466-478)."""
+    with tempfile.TemporaryDirectory() as d:
+        wl, path, parts = blcases.build("ragged_harmonic", d)
+        r = ref.RefBeam(path, seed=wl.cfg.seed)
+        r.set_emit_nat([0.0, 0.0, 0.0])
+        o = oracle.OracleBeam(wl)
+        blcases.start(r, parts)
+        blcases.start(o, parts)
+        for b in (r, o):
+            b.MPBeamRMSCal(0)
+            b.BeamMomtumUpdateDueToRFTest()
+        for j in range(0, wl.n_bunches, 37):
+            assert o.rf_info(j, 0) == r.rf_info(j, 0)
+        r.close()
