@@ -310,6 +310,16 @@ class MPBeam:
         self._check(self.lib.cg_ion_download(self.h, k, p, *[_abi.ptr(x) for x in a], cap, C.byref(n)))
         return [x[: n.value] for x in a]
 
+    def ion_forces(self, k: int, p: int = 0):
+        """(fx, fy, macro-ion charge) of cloud (k, p): the last bunch's
+        velocity kick on each ion."""
+        cap = int(self.wl.cfg.ion.max_ions) + 8
+        fx, fy = np.empty(cap), np.empty(cap)
+        n, q = C.c_int(), C.c_double()
+        self._check(self.lib.cg_ion_forces(self.h, k, p, _abi.ptr(fx), _abi.ptr(fy), cap, C.byref(n),
+                                           C.byref(q)))
+        return fx[: n.value], fy[: n.value], q.value
+
     def upload_ions(self, k: int, p: int, x, y, vx, vy):
         """Replaces the accumulated cloud of section k, species p."""
         a = [np.ascontiguousarray(v, dtype=np.float64) for v in (x, y, vx, vy)]

@@ -549,6 +549,10 @@ int cg_create(const cg_config* cfg, int device, cg_handle** out) {
             dalloc(&c.vx[b], h.ion_cap) || dalloc(&c.vy[b], h.ion_cap))
           return bail(CG_ERR_OOM, "ion cloud buffers");
       }
+      if (dalloc(&c.fx, h.ion_cap) || dalloc(&c.fy, h.ion_cap))
+        return bail(CG_ERR_OOM, "ion cloud buffers");
+      cudaMemset(c.fx, 0, sizeof(double) * h.ion_cap);
+      cudaMemset(c.fy, 0, sizeof(double) * h.ion_cap);
     }
     if (dalloc(&h.d.clouds, cl.size())) return bail(CG_ERR_OOM, "clouds");
     cudaMemcpy(h.d.clouds, cl.data(), sizeof(CloudDev) * cl.size(), cudaMemcpyHostToDevice);
@@ -708,8 +712,10 @@ int cg_destroy(cg_handle* H) {
   if (h.d.clouds) {
     std::vector<CloudDev> cl(h.K * h.P);
     cudaMemcpy(cl.data(), h.d.clouds, sizeof(CloudDev) * cl.size(), cudaMemcpyDeviceToHost);
-    for (auto& c : cl)
+    for (auto& c : cl) {
       for (int b = 0; b < 2; ++b) { dfree(c.x[b]); dfree(c.y[b]); dfree(c.vx[b]); dfree(c.vy[b]); }
+      dfree(c.fx); dfree(c.fy);
+    }
     dfree(h.d.clouds);
   }
   dfree(h.d.cloud_state); dfree(h.d.lr_tab); dfree(h.d.lr_head); dfree(h.d.fir_coeff);
@@ -840,7 +846,7 @@ int cg_set_beam(cg_handle* H, int M, const int* n_macro, const int* harm, const 
     w.grid = ion_walk_grid(w.tcap, 8);  // the most walk CTAs of any shape
     if (dalloc(&w.births, P * M * NM * 2) || dalloc(&w.prep, (size_t)M) ||
         dalloc(&w.bunch, 3 * (size_t)M) || dalloc(&w.spec, P * M * 2) || dalloc(&w.bound, 2) ||
-        dalloc(&w.part, P * M * (size_t)w.grid * 5) || dalloc(&w.traj, P * 4 * (size_t)w.tcap) ||
+        dalloc(&w.part, P * M * (size_t)w.grid * 5) || dalloc(&w.traj, P * 6 * (size_t)w.tcap) ||
         dalloc(&w.alive, P * (size_t)w.tcap) || dalloc(&w.carry, 4 * P)) {
       free_beam(h);
       return fail(&h, CG_ERR_OOM, "ion chain scratch");
@@ -1784,6 +1790,29 @@ int cg_ion_download(cg_handle* H, int k, int p, double* x, double* y, double* vx
   return CG_OK;
 }
 
+int cg_ion_forces(cg_handle* H, int k, int p, double* fx, double* fy, int capacity, int* count,
+                  double* macro_charge) {
+  if (!H || !count) return CG_ERR_INVALID;
+  Handle& h = H->h;
+  if (!h.cfg.flag_beam_ion) return fail(&h, CG_ERR_NOT_READY, "runBeamIonFlag is off");
+  if (k < 0 || k >= h.K || p < 0 || p >= h.P) return fail(&h, CG_ERR_INVALID, "bad IP/species");
+  cudaSetDevice(h.device);
+  CG_CUDA(&h, cudaStreamSynchronize(h.stream));
+  CloudState s;
+  CloudDev cd;
+  int ci = cloud_index(h, k, p);
+  CG_CUDA(&h, cudaMemcpy(&s, h.d.cloud_state + ci, sizeof s, cudaMemcpyDeviceToHost));
+  CG_CUDA(&h, cudaMemcpy(&cd, h.d.clouds + ci, sizeof cd, cudaMemcpyDeviceToHost));
+  *count = s.n;
+  if (macro_charge) *macro_charge = s.macro_charge;
+  int n = s.n < capacity ? s.n : capacity;
+  if (n > 0) {
+    if (fx) CG_CUDA(&h, cudaMemcpy(fx, cd.fx, n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (fy) CG_CUDA(&h, cudaMemcpy(fy, cd.fy, n * sizeof(double), cudaMemcpyDeviceToHost));
+  }
+  return CG_OK;
+}
+
 int cg_ion_upload(cg_handle* H, int k, int p, const double* x, const double* y, const double* vx,
                   const double* vy, int count) {
   if (!H) return CG_ERR_INVALID;
@@ -1803,6 +1832,8 @@ int cg_ion_upload(cg_handle* H, int k, int p, const double* x, const double* y, 
     CG_CUDA(&h, cudaMemcpy(cd.y[s.cur], y, count * sizeof(double), cudaMemcpyHostToDevice));
     CG_CUDA(&h, cudaMemcpy(cd.vx[s.cur], vx, count * sizeof(double), cudaMemcpyHostToDevice));
     CG_CUDA(&h, cudaMemcpy(cd.vy[s.cur], vy, count * sizeof(double), cudaMemcpyHostToDevice));
+    CG_CUDA(&h, cudaMemset(cd.fx, 0, count * sizeof(double)));
+    CG_CUDA(&h, cudaMemset(cd.fy, 0, count * sizeof(double)));
   }
   s.n = count;
   CG_CUDA(&h, cudaMemcpy(h.d.cloud_state + ci, &s, sizeof s, cudaMemcpyHostToDevice));

@@ -50,6 +50,8 @@ struct CloudDev {
   double* y[2];
   double* vx[2];
   double* vy[2];
+  double* fx;  // velocity kick of the last bunch on each ion (ionAccumuFx, MPBunch.cpp:1149)
+  double* fy;
   int cap;
 };
 
@@ -86,7 +88,7 @@ struct IonWalk {
   double* spec = nullptr;     // P x M x (macro-ion charge, ion-side coefficient)
   double* bound = nullptr;    // loss bounds (x, y)
   double* part = nullptr;     // P x M x grid x (count, sum x, sum y, sum x^2, sum y^2)
-  double* traj = nullptr;     // P x 4 x tcap: x, y, vx, vy after the walk
+  double* traj = nullptr;     // P x 6 x tcap: x, y, vx, vy after the walk, last kick fx, fy
   uint8_t* alive = nullptr;   // P x tcap
   double* carry = nullptr;    // P x (centroid x, y carried between steps, last rms x, y)
   int64_t tcap = 0;           // trajectories per species: cloud capacity + M x NM

@@ -1350,6 +1350,7 @@ cudaError_t upload_weideman_table() {
   cudaError_t e = cudaMemcpyToSymbol(c_weideman, &h_weideman, sizeof(WeidemanTable));
   if (e == cudaSuccess) e = prepare_map_async();
   if (e == cudaSuccess) e = upload_weideman_table_ion();
+  if (e == cudaSuccess) e = upload_weideman_table_sc();
   return e != cudaSuccess ? e : upload_weideman_table_sur();
 }
 

@@ -136,6 +136,8 @@ cudaError_t upload_weideman_table_sur();
 
 cudaError_t upload_weideman_table();      // every translation unit that evaluates w(z)
 cudaError_t upload_weideman_table_ion();
+// the copy of the w(z) table in sc.cu (the Bassetti-Erskine slice model)
+cudaError_t upload_weideman_table_sc();
 
 // Moments of one bunch held in the caller's device buffers, with the partials
 // in a fixed file-scope device array (no allocation).  At most

@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(4 * IONS, 1) k_ion_walk(ChainParams cp, IonWal
   const double* births = w.births + 2 * (size_t)p * M * NM;
   const double* spec = w.spec + 2 * (size_t)p * M;
   double* part = w.part + (size_t)p * M * G * 5;
-  double* traj = w.traj + (size_t)p * 4 * w.tcap;
+  double* traj = w.traj + (size_t)p * 6 * w.tcap;
   uint8_t* alive_out = w.alive + (size_t)p * w.tcap;
   bool first = true;
   for (int blk = c; blk < nblk; blk += G, first = false) {
@@ -206,6 +206,7 @@ __global__ void __launch_bounds__(4 * IONS, 1) k_ion_walk(ChainParams cp, IonWal
     bool alive = t < T;
     int j0 = 0;
     double x = 0, y = 0, vx = 0, vy = 0;
+    double kx = 0, ky = 0;  // the last bunch's velocity kick (ionAccumuFx/Fy)
     if (alive) {
       const int start = t < n0 ? 0 : (int)((t - n0) / NM);
       if (t >= n0) j0 = start;
@@ -282,8 +283,10 @@ __global__ void __launch_bounds__(4 * IONS, 1) k_ion_walk(ChainParams cp, IonWal
             double fx, fy;
             field_finish_g(fp, dx, dy, second ? wo : wv, second ? wv : wo, second ? g : go, &fx,
                            &fy);
-            vx += coeffI * fx;
-            vy += coeffI * fy;
+            kx = coeffI * fx;
+            ky = coeffI * fy;
+            vx += kx;
+            vy += ky;
             x += vx * dt;
             y += vy * dt;
             alive = !(fabs(x) > bx || fabs(y) > by);
@@ -324,6 +327,8 @@ __global__ void __launch_bounds__(4 * IONS, 1) k_ion_walk(ChainParams cp, IonWal
       traj[w.tcap + t] = y;
       traj[2 * w.tcap + t] = vx;
       traj[3 * w.tcap + t] = vy;
+      traj[4 * w.tcap + t] = kx;
+      traj[5 * w.tcap + t] = ky;
       alive_out[t] = alive ? 1 : 0;
     }
     __syncthreads();  // shared windows reused by the next block of this CTA
@@ -439,7 +444,7 @@ __global__ void __launch_bounds__(kFinishThreads) k_ion_compact(ChainParams cp, 
   const double* spec = w.spec + 2 * (size_t)p * M;
   const double* carry = w.carry + 4 * (size_t)p;
   CloudDev cd = clouds[p];
-  const double* traj = w.traj + (size_t)p * 4 * w.tcap;
+  const double* traj = w.traj + (size_t)p * 6 * w.tcap;
   const uint8_t* al = w.alive + (size_t)p * w.tcap;
   if (tid == 0) s_base = 0;
   __syncthreads();
@@ -461,6 +466,8 @@ __global__ void __launch_bounds__(kFinishThreads) k_ion_compact(ChainParams cp, 
       cd.y[0][pre] = traj[w.tcap + t];
       cd.vx[0][pre] = traj[2 * w.tcap + t];
       cd.vy[0][pre] = traj[3 * w.tcap + t];
+      cd.fx[pre] = traj[4 * w.tcap + t];
+      cd.fy[pre] = traj[5 * w.tcap + t];
     }
     __syncthreads();
     if (tid == 0) s_base += tot;

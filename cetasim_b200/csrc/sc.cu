@@ -352,6 +352,12 @@ __global__ void __launch_bounds__(kTile) k_sc_kick(double* __restrict__ c, int64
   c[3 * npad + g] += dpy;
 }
 
+// this translation unit's copy of the w(z) table (faddeeva.cuh keeps one
+// __constant__ copy per unit)
+cudaError_t upload_weideman_table_sc() {
+  return cudaMemcpyToSymbol(c_weideman, &h_weideman, sizeof(WeidemanTable));
+}
+
 size_t sc_solve_smem(const ScParams& p) {
   return sizeof(double) * ((size_t)2 * p.nx * p.ny + p.nx * p.nx + p.ny * p.ny);
 }

@@ -21,8 +21,8 @@
 //
 // Not built here (paths outside the library's scope, kept as the reference's
 // declarations only): PIC beam-ion, ramping, drive mode, the per-particle
-// dump of MPBeamDataPrintPerTurn, the ion dump (SSIonDataPrint), the cavity
-// transient printout of InitialcavityResonator and the Haissinski solver.
+// dump of MPBeamDataPrintPerTurn, the cavity transient printout of
+// InitialcavityResonator and the Haissinski solver.
 #include <cmath>
 #include <complex>
 #include <cstdint>
@@ -678,6 +678,61 @@ static void write_sr_potentials(GpuBeam& g, const ReadInputSettings& in, int tur
   }
 }
 
+// MPBeam::SSIonDataPrint (MPBeam.cpp:2912-2976): per IP a page of every
+// accumulated macro-ion (mass number, macro-ion charge, position, velocity
+// and the last bunch's kick), after the turn's ion stages.
+void MPBeam::SSIonDataPrint(ReadInputSettings& inputParameter, LatticeInterActionPoint& latticeInterActionPoint,
+                            int nTurns) {
+  GpuBeam& g = gpu(this);
+  LatticeInterActionPoint& L = latticeInterActionPoint;
+  const int K = L.numberOfInteraction, P = L.gasSpec;
+  std::vector<double> q(beamVec.size());
+  check(g, cg_bunch_ion_charge(g.h, q.data()), "cg_bunch_ion_charge");
+  L.totIonCharge = q.back();  // LIP::GetTotIonCharge at the last bunch's interaction
+  std::ofstream fout(inputParameter.ringIonEffPara->ionDisWriteTo + ".sdds", std::ios_base::app);
+  const int cap = g.cfg.ion.max_ions + g.cfg.ion.macro_ions_per_ip + 1;
+  std::vector<double> x(cap), y(cap), vx(cap), vy(cap), fx(cap), fy(cap);
+  for (int k = 0; k < K; k++) {
+    if (nTurns == 0) {
+      fout << "SDDS1" << std::endl;
+      fout << "&parameter name=totIonCharge, units=e, type=float,  &end" << std::endl;
+      fout << "&parameter name=tunrs,                 type=long,   &end" << std::endl;
+      for (int p = 0; p < P; p++)
+        fout << "parameter name=numOfMacroIon_" << p << ",  type=long,  &end" << std::endl;
+      fout << "&column name=ionMass,                   type=float,  &end" << std::endl;
+      fout << "&column name=macroIonCharge,  units=e,   type=float,  &end" << std::endl;
+      fout << "&column name=x,  units=m,   type=float,  &end" << std::endl;
+      fout << "&column name=y,  units=m,   type=float,  &end" << std::endl;
+      fout << "&column name=xp, units=m/s, type=float,  &end" << std::endl;
+      fout << "&column name=yp, units=m/s, type=float,  &end" << std::endl;
+      fout << "&column name=Fx, units=m/s, type=float,  &end" << std::endl;
+      fout << "&column name=Fy, units=m/s, type=float,  &end" << std::endl;
+      fout << "&data mode=ascii, &end" << std::endl;
+    }
+    std::vector<int> cnt(P);
+    std::vector<double> mq(P);
+    int tot = 0;
+    for (int p = 0; p < P; p++) {
+      check(g, cg_ion_forces(g.h, k, p, nullptr, nullptr, 0, &cnt[p], &mq[p]), "cg_ion_forces");
+      tot += cnt[p];
+    }
+    fout << "! page number " << nTurns * K + k + 1 << std::endl;
+    fout << L.totIonCharge << std::endl << nTurns << std::endl;
+    for (int p = 0; p < P; p++) fout << cnt[p] << std::endl;
+    fout << tot << std::endl;
+    for (int p = 0; p < P; p++) {
+      int n = 0;
+      check(g, cg_ion_download(g.h, k, p, x.data(), y.data(), vx.data(), vy.data(), cap, &n), "cg_ion_download");
+      check(g, cg_ion_forces(g.h, k, p, fx.data(), fy.data(), cap, &n, nullptr), "cg_ion_forces");
+      for (int i = 0; i < n; i++)
+        fout << std::setw(15) << std::left << L.ionMassNumber[p] << std::setw(15) << std::left << mq[p]
+             << std::setw(15) << std::left << x[i] << std::setw(15) << std::left << y[i] << std::setw(15)
+             << std::left << vx[i] << std::setw(15) << std::left << vy[i] << std::setw(15) << std::left
+             << fx[i] << std::setw(15) << std::left << fy[i] << std::endl;
+    }
+  }
+}
+
 // MPBeam::MPBeamDataPrintPerTurn (MPBeam.cpp:2319-2563) for the files this
 // library writes: <TBTBunchAverData>.sdds (every bunch's averages, sizes and
 // the cavity voltages it saw, one page per print turn) and
@@ -875,8 +930,12 @@ void MPBeam::Run(Train& train, LatticeInterActionPoint& latticeInterActionPoint,
     for (size_t j = 0; j < beamVec.size(); ++j) beamVec[j].transmission = g.mom[j].transmission;
     MPGetBeamInfo();
     if (inputParameter.ringRun->beamIonFlag) {
-      int macro = 0;
-      check(g, cg_ion_totals(g.h, &latticeInterActionPoint.totIonCharge, &macro), "cg_ion_totals");
+      // LIP::totIonCharge as the last bunch's interaction at the last IP left it
+      std::vector<double> q(beamVec.size());
+      check(g, cg_bunch_ion_charge(g.h, q.data()), "cg_bunch_ion_charge");
+      latticeInterActionPoint.totIonCharge = q.back();
+      const int every = inputParameter.ringIonEffPara->ionInfoPrintInterval;
+      if (every && n % every == 0) SSIonDataPrint(inputParameter, latticeInterActionPoint, n);
     }
     const double nux = inputParameter.ringParBasic->workQx - std::floor(inputParameter.ringParBasic->workQx);
     const double nuy = inputParameter.ringParBasic->workQy - std::floor(inputParameter.ringParBasic->workQy);

@@ -446,6 +446,12 @@ int cg_ion_count(cg_handle* h, int k, int p, int* count);
 /* ionAccumuPosition{X,Y}, ionAccumuVelocity{X,Y} of IP k, species p. */
 int cg_ion_download(cg_handle* h, int k, int p, double* x, double* y,
                     double* vx, double* vy, int capacity, int* count);
+/* The velocity kick of the last bunch on each ion of cloud (k, p) (the
+ * reference's ionAccumuFx / ionAccumuFy, MPBunch.cpp:1149-1150; zero for
+ * uploaded ions until their next bunch), the cloud's count and its macro-ion
+ * charge (macroIonCharge[k][p], the last bunch's). */
+int cg_ion_forces(cg_handle* h, int k, int p, double* fx, double* fy, int capacity, int* count,
+                  double* macro_charge);
 int cg_ion_upload(cg_handle* h, int k, int p, const double* x, const double* y,
                   const double* vx, const double* vy, int count);
 /* Recorded per-bunch ion-cloud Gaussians of the last cg_beam_ion_ip at IP k

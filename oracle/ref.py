@@ -132,6 +132,14 @@ class RefBeam:
         self._check(self.lib.ref_bunch_info(self.h, j, out))
         return {"ne": out[0], "macro_charge": out[1], "harm": int(out[2]), "gap": int(out[3])}
 
+    def ion_forces(self, k, p=0):
+        cap = 1 << 20
+        fx, fy = np.empty(cap), np.empty(cap)
+        n = self.lib.ref_ion_forces(self.h, k, p, _dp(fx), _dp(fy), cap)
+        if n < 0:
+            raise RuntimeError("bad IP or species")
+        return fx[:n], fy[:n]
+
     def bunch_ion_charge(self, j):
         out = C.c_double()
         self._check(self.lib.ref_bunch_ion_charge(self.h, j, C.byref(out)))

@@ -336,6 +336,19 @@ int ref_bunch_info(void *h, int j, double *out4) {
     return 0;
 }
 
+// ionAccumuFx / ionAccumuFy of IP k, species p (MPBunch.cpp:1149-1150)
+int ref_ion_forces(void *h, int k, int p, double *fx, double *fy, int cap) {
+    RefRun *r = static_cast<RefRun *>(h);
+    const LatticeInterActionPoint &L = r->lat;
+    if (k < 0 || k >= L.numberOfInteraction || p < 0 || p >= L.gasSpec) return -1;
+    const int n = (int)L.ionAccumuFx[k][p].size();
+    for (int i = 0; i < n && i < cap; ++i) {
+        fx[i] = L.ionAccumuFx[k][p][i];
+        fy[i] = L.ionAccumuFy[k][p][i];
+    }
+    return n;
+}
+
 // MPBunch::totIonCharge of bunch j (MPBunch.cpp:1208-1209)
 int ref_bunch_ion_charge(void *h, int j, double *out) {
     RefRun *r = static_cast<RefRun *>(h);

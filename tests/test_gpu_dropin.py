@@ -269,3 +269,49 @@ def test_dropin_per_bunch_files_match_the_reference_program(tmp_path):
                 else:
                     d = np.abs(x - y)
                 assert np.all(d <= 1e-7 * np.maximum(np.abs(x), 1e-3 * scale) + 1e-300), (f, name)
+
+
+def test_dropin_ion_dump_has_the_reference_layout(tmp_path):
+    """<ionCalIonDisWriteTo>.sdds (MPBeam::SSIonDataPrint, MPBeam.cpp:
+    2912-2976) of the fast-ion train over 2 turns, printed every turn: the
+    drop-in's file has the reference program's header and page layout (the
+    two programs draw different ion births, so the values are compared on the
+    GPU against the reference harness instead, test_gpu_ref.py)."""
+    wl = configs.make("fast_ion", n_scale=0.002)
+    wl.cfg.flag_synrad = 0
+    src = tmp_path / "src"
+    input_dat.write_case(str(src), wl, n_turns=2, qe=False, extra=["ionCalIonInfoPrintInterval = 1"])
+    dirs = []
+    for name in ("ref", "gpu"):
+        d = tmp_path / name
+        shutil.copytree(src, d)
+        dirs.append(str(d))
+    run(ref.EXE, dirs[0], teardown_may_crash=True)
+    run(DROPIN, dirs[1])
+
+    def layout(path):
+        lines = open(path).read().splitlines()
+        heads, pages, i = [], [], 0
+        while i < len(lines):
+            if lines[i] == "SDDS1":
+                j = i
+                while not lines[j].startswith("&data"):
+                    j += 1
+                heads.append(lines[i:j + 1])
+                i = j + 1
+            elif lines[i].startswith("! page number"):
+                page = int(lines[i].split()[-1])
+                P = wl.cfg.ion.n_species
+                counts = [int(v) for v in lines[i + 3:i + 3 + P]]
+                tot = int(lines[i + 3 + P])
+                rows = lines[i + 4 + P:i + 4 + P + tot]
+                assert sum(counts) == tot and all(len(r.split()) == 8 for r in rows)
+                pages.append(page)
+                i += 4 + P + tot
+            else:
+                raise AssertionError(lines[i])
+        return heads, pages
+
+    hr, pr = layout(os.path.join(dirs[0], "ion_dis.sdds"))
+    hg, pg = layout(os.path.join(dirs[1], "ion_dis.sdds"))
+    assert hr == hg and pr == pg == list(range(1, 2 * wl.cfg.n_sections + 1))

@@ -89,6 +89,13 @@ def test_gpu_and_reference_side_by_side_fast_ion_ip_records(tmp_path):
             assert np.array_equal(sr, sg)
             worst = max(worst, refcases.coord_rel_err(cg, cr, sr == 0).max())
         assert worst <= 1e-11, f"IP {k}: {worst:.3e}"
+        if k % 5 == 0:
+            # the last bunch's kick on every ion of the cloud (ionAccumuFx/Fy)
+            fxr, fyr = r.ion_forces(k)
+            fxg, fyg, _ = g.ion_forces(k)
+            assert len(fxg) == len(fxr)
+            for a, b in ((fxg, fxr), (fyg, fyr)):
+                assert np.max(np.abs(a - b)) <= 1e-10 * np.max(np.abs(b)), k
     # after the last IP: every bunch's totIonCharge (MPBunch.cpp:1208-1209)
     import ctypes as C
     q = np.empty(wl.n_bunches)
