@@ -178,6 +178,8 @@ EXPORTS = [
     ("cg_bunch_ion_charge", I, [C.c_void_p, PD]),
     ("cg_rf_profile", I, [C.c_void_p, I, PD, PD, PI]),
     ("cg_ion_forces", I, [C.c_void_p, I, I, PD, PD, I, PI, PD]),
+    ("cg_set_phase_track", I, [C.c_void_p, I, PI]),
+    ("cg_phase_adv", I, [C.c_void_p, I, PD]),
     ("cg_bbi_profile", I, [C.c_void_p, I, PI, PI, PD, I]),
     ("cg_sr_bins", I, [C.c_void_p, I, PD, PD, PI]),
     ("cg_set_sr_potentials", I, [C.c_void_p, I]),

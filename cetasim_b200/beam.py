@@ -310,6 +310,19 @@ class MPBeam:
         self._check(self.lib.cg_ion_download(self.h, k, p, *[_abi.ptr(x) for x in a], cap, C.byref(n)))
         return [x[: n.value] for x in a]
 
+    def set_phase_track(self, bunches):
+        """Tracks the accumulated phase advance of every particle of these
+        bunches from now on (cg_set_phase_track)."""
+        b = np.ascontiguousarray(list(bunches), dtype=np.int32)
+        self._check(self.lib.cg_set_phase_track(self.h, len(b), _abi.ptr(b) if len(b) else None))
+
+    def phase_adv(self, j: int):
+        """Accumulated x, y, z phase advance of bunch j's particles (3 x n)."""
+        n = int(self.wl.n_macro[j])
+        out = np.empty(3 * n)
+        self._check(self.lib.cg_phase_adv(self.h, j, _abi.ptr(out)))
+        return out.reshape(3, n)
+
     def ion_forces(self, k: int, p: int = 0):
         """(fx, fy, macro-ion charge) of cloud (k, p): the last bunch's
         velocity kick on each ion."""

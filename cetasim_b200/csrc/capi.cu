@@ -121,6 +121,11 @@ void free_beam(Handle& h) {
   dfree(d.bbi_pot); dfree(d.bbi_win);
   d.bbi_lo = nullptr; d.bbi_hi = nullptr; d.bbi_amax = nullptr; d.bbi_cnt = nullptr;
   d.bbi_sxy = nullptr; d.bbi_pot = nullptr; d.bbi_win = nullptr;
+  for (double* b : h.phase_bufs) dfree(b);
+  h.phase_bufs.clear();
+  h.phase_bunches.clear();
+  dfree(d.phase_slot); dfree(d.phase_ptr);
+  d.phase_slot = nullptr; d.phase_ptr = nullptr;
   dfree(d.sc_geom); dfree(d.sc_cnt); dfree(d.sc_acc); dfree(d.sc_field);
   d.sc_geom = nullptr; d.sc_cnt = nullptr; d.sc_acc = nullptr; d.sc_field = nullptr;
   h.cbm_cap = h.cbm_n = 0;
@@ -1096,8 +1101,58 @@ int cg_beam_ion_ip(cg_handle* H, int turn, int k) {
 int cg_section_map(cg_handle* H, int k) {
   STAGE_PROLOGUE
   if (k < 0 || k >= h.K) return fail(&h, CG_ERR_INVALID, "section index out of range");
-  int st = launch_ok(h, launch_map(h, k), "map");
+  int st = 0;
+  if (k == h.K - 1) st = launch_ok(h, launch_phase_adv(h, 0, h.M), "phase advance");
+  if (!st) st = launch_ok(h, launch_map(h, k), "map");
   return st ? st : check_status(h);
+}
+
+int cg_set_phase_track(cg_handle* H, int n, const int* bunches) {
+  STAGE_PROLOGUE
+  if (n < 0 || (n > 0 && !bunches)) return fail(&h, CG_ERR_INVALID, "bad bunch list");
+  if (h.sh_world > 1) return fail(&h, CG_ERR_UNSUPPORTED, "not with bunch sharding");
+  for (int i = 0; i < n; ++i)
+    if (bunches[i] < 0 || bunches[i] >= h.M) return fail(&h, CG_ERR_INVALID, "bunch index out of range");
+  CG_CUDA(&h, cudaStreamSynchronize(h.stream));
+  for (double* b : h.phase_bufs) dfree(b);
+  h.phase_bufs.clear();
+  h.phase_bunches.clear();
+  if (h.turn_graph) {
+    cudaGraphExecDestroy(h.turn_graph);
+    h.turn_graph = nullptr;
+  }
+  if (n == 0) return CG_OK;
+  if (!h.d.phase_slot && (dalloc(&h.d.phase_slot, (size_t)h.M) || dalloc(&h.d.phase_ptr, (size_t)h.M)))
+    return fail(&h, CG_ERR_OOM, "phase-advance tables");
+  std::vector<int> slot(h.M, -1);
+  for (int i = 0; i < n; ++i) {
+    const int j = bunches[i];
+    if (slot[j] >= 0) continue;
+    double* b = nullptr;
+    if (dalloc(&b, 6 * (size_t)h.n_macro[j])) return fail(&h, CG_ERR_OOM, "phase-advance buffers");
+    slot[j] = (int)h.phase_bufs.size();
+    h.phase_bufs.push_back(b);
+    h.phase_bunches.push_back(j);
+  }
+  CG_CUDA(&h, cudaMemcpy(h.d.phase_slot, slot.data(), sizeof(int) * h.M, cudaMemcpyHostToDevice));
+  CG_CUDA(&h, cudaMemcpy(h.d.phase_ptr, h.phase_bufs.data(), sizeof(double*) * h.phase_bufs.size(),
+                         cudaMemcpyHostToDevice));
+  int st = launch_ok(h, launch_phase_init(h), "phase init");
+  return st ? st : check_status(h);
+}
+
+int cg_phase_adv(cg_handle* H, int j, double* out) {
+  STAGE_PROLOGUE
+  if (j < 0 || j >= h.M || !out) return fail(&h, CG_ERR_INVALID, "bad arguments");
+  for (size_t s = 0; s < h.phase_bunches.size(); ++s)
+    if (h.phase_bunches[s] == j) {
+      CG_CUDA(&h, cudaStreamSynchronize(h.stream));
+      const size_t n = h.n_macro[j];
+      CG_CUDA(&h, cudaMemcpy(out, h.phase_bufs[s] + 3 * n, sizeof(double) * 3 * n,
+                             cudaMemcpyDeviceToHost));
+      return CG_OK;
+    }
+  return fail(&h, CG_ERR_NOT_READY, "the bunch's phase advance is not tracked (cg_set_phase_track)");
 }
 
 int cg_rf_kick(cg_handle* H) {
@@ -1295,7 +1350,8 @@ static cudaError_t enqueue_turn(Handle& h) {
   for (int k = 0; k < h.K; ++k) {
     // the space charge kicks between the ion kick and the map, so neither
     // the kick inside the map pass nor the segmented pipeline
-    const bool fused = c.flag_beam_ion && !h.d.sur_w && h.fuse_kick && !c.flag_sc;
+    const bool fused = c.flag_beam_ion && !h.d.sur_w && h.fuse_kick && !c.flag_sc &&
+                       !(k == h.K - 1 && !h.phase_bunches.empty());
     int mom = -1;
     if (k + 1 < h.K) mom = sec_mom ? k + 1 : -1;
     else mom = post ? h.K - 1 : -1;
@@ -1327,6 +1383,7 @@ static cudaError_t enqueue_turn(Handle& h) {
         TRACE(h.side, CG_TRACE_ION_KICK, k, g);
         if ((e = cudaEventRecord(h.kick_ev[g], h.side))) return e;
         if ((e = cudaStreamWaitEvent(h.side2, h.kick_ev[g], 0))) return e;
+        if (k == h.K - 1 && (e = launch_phase_adv(h, ja, jb, h.side2))) return e;
         if ((e = launch_map_turn(h, k, mom, false, ca, cb, h.side2))) return e;
         TRACE(h.side2, CG_TRACE_MAP_PASS, k, g);
       }
@@ -1348,6 +1405,7 @@ static cudaError_t enqueue_turn(Handle& h) {
         }
       }
       if (c.flag_sc && (e = launch_space_charge(h, k))) return e;
+      if (k == h.K - 1 && (e = launch_phase_adv(h, 0, h.M))) return e;
       if ((e = launch_map_turn(h, k, mom, fused))) return e;
       TRACE(h.stream, CG_TRACE_MAP_PASS, k, -1);
     }

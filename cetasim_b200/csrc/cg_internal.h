@@ -168,6 +168,10 @@ struct DeviceBufs {
   unsigned long long* sc_acc = nullptr;  // M x nz x acc_per_slice fixed-point sums
   double* sc_field = nullptr;      // M x nz x 2 x nx x ny mesh field (PIC)
   double* sc_sin = nullptr;        // nx x nx + ny x ny: 2 sin(pi (i + 1)(k + 1) / (n + 1))
+  // phase advance of the tracked bunches: slot per bunch (-1 untracked),
+  // per slot 6 x n (previous angles x, y, z; accumulated x, y, z)
+  int* phase_slot = nullptr;
+  double** phase_ptr = nullptr;
   // scratch
   double* scratch = nullptr;
   size_t scratch_bytes = 0;
@@ -208,6 +212,8 @@ struct Handle {
   BbiParams bbi;               // broadband impedance (cfg.bbi.flag)
   ScParams sc;                 // space charge (cfg.flag_sc)
   bool sr_xy = false;          // SR wake: the transverse potentials too (the reference's file)
+  std::vector<int> phase_bunches;  // bunches whose particles' phase advance is tracked
+  std::vector<double*> phase_bufs; // their device buffers (6 x n each)
   std::vector<double> bbi_table;  // the copy of cfg.bbi.table
   int pipe_groups = 4;
   // trajectories per walk CTA (8, 16, 32, 64): smaller CTAs spread the

@@ -908,6 +908,79 @@ __global__ void __launch_bounds__(kTile) k_long(double* __restrict__ c, int64_t 
   store6(c, npad, t.g, v);
 }
 
+// The accumulated phase advance of the tracked bunches' particles
+// (Bunch.cpp:715-731), before the map of the ring's last section: per
+// particle the angles of the rotated normal-form vector, their decrease since
+// the last turn (plus 2 pi when negative) added up.  ph[slot] holds per
+// particle (previous x, y, z angles, accumulated x, y, z), 6 x n.
+__global__ void __launch_bounds__(kTile) k_phase_adv(const double* __restrict__ c, int64_t npad,
+                                                     const uint8_t* __restrict__ surv,
+                                                     const int* __restrict__ tile_bunch,
+                                                     const BunchDev* __restrict__ bunch,
+                                                     const __grid_constant__ SectionDev sec,
+                                                     const __grid_constant__ RingDev r,
+                                                     const int* __restrict__ slot_of,
+                                                     double* const* __restrict__ ph, int tile0) {
+  const int tile = tile0 + blockIdx.x;
+  const int b = tile_bunch[tile];
+  const BunchDev& B = bunch[b];
+  const int i = (tile - B.tile_off) * kTile + threadIdx.x;
+  const int64_t g = (int64_t)tile * kTile + threadIdx.x;
+  const int slot = slot_of[b];
+  if (i >= B.n || slot < 0 || surv[g] != kAlive) return;  // the map skips lost particles
+  double v[6], v2[6];
+  load6(c, npad, g, v);
+  section_map_rotated(sec, r, v, v2);
+  double* P = ph[slot];
+  const int n = B.n;
+  for (int q = 0; q < 3; ++q) {
+    const double cur = atan2(v2[2 * q + 1], v2[2 * q]);
+    const double tmp = P[(size_t)q * n + i] - cur;
+    P[(size_t)(3 + q) * n + i] += tmp >= 0 ? tmp : tmp + 2 * kPi;
+    P[(size_t)q * n + i] = cur;
+  }
+}
+
+// Bunch::InitialAccumPhaseAdV (Bunch.cpp:504-553): the angles of B1H1 . v at
+// section 0, accumulated phases zero.
+__global__ void __launch_bounds__(kTile) k_phase_init(const double* __restrict__ c, int64_t npad,
+                                                      const int* __restrict__ tile_bunch,
+                                                      const BunchDev* __restrict__ bunch,
+                                                      const __grid_constant__ SectionDev sec0,
+                                                      const int* __restrict__ slot_of,
+                                                      double* const* __restrict__ ph) {
+  TileIdx t = tile_index(tile_bunch, bunch);
+  if (!t.valid) return;
+  const int slot = slot_of[t.b];
+  if (slot < 0) return;
+  double v[6], v1[6];
+  load6(c, npad, t.g, v);
+  matvec6(sec0.b1h1, v, v1);
+  double* P = ph[slot];
+  const int n = bunch[t.b].n;
+  for (int q = 0; q < 3; ++q) {
+    P[(size_t)q * n + t.i] = atan2(v1[2 * q + 1], v1[2 * q]);
+    P[(size_t)(3 + q) * n + t.i] = 0.0;
+  }
+}
+
+cudaError_t launch_phase_init(Handle& h) {
+  k_phase_init<<<h.n_tiles, kTile, 0, h.stream>>>(h.d.c, h.npad, h.d.tile_bunch, h.d.bunch,
+                                                  h.sec_dev_host[0], h.d.phase_slot, h.d.phase_ptr);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_phase_adv(Handle& h, int ja, int jb, cudaStream_t s) {
+  bool any = false;
+  for (int j : h.phase_bunches) any = any || (j >= ja && j < jb);
+  if (!any) return cudaSuccess;
+  const int ta = h.tile_off[ja], tb = jb < h.M ? h.tile_off[jb] : h.n_tiles;
+  k_phase_adv<<<tb - ta, kTile, 0, s ? s : h.stream>>>(
+      h.d.c, h.npad, h.d.surv, h.d.tile_bunch, h.d.bunch, h.sec_dev_host[h.K - 1], h.ring,
+      h.d.phase_slot, h.d.phase_ptr, ta);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_long(Handle& h, unsigned flags) {
   if ((flags & kLongRF) && h.ring.bl_any) {
     // the cavities' recurrence over the train first: the kicks of each bin

@@ -17,6 +17,11 @@ enum : int {
   kStatusScMesh = 512,        // a space-charge mesh from a zero rms size
 };
 
+// per-particle phase advance of the tracked bunches (cg_set_phase_track)
+cudaError_t launch_phase_init(Handle& h);
+// before the last section's map, for the tracked bunches among [ja, jb)
+cudaError_t launch_phase_adv(Handle& h, int ja, int jb, cudaStream_t s = nullptr);
+
 // space charge (sc.cu)
 cudaError_t launch_space_charge(Handle& h, int k);
 size_t sc_solve_smem(const ScParams& p);

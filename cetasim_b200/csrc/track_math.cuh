@@ -113,8 +113,12 @@ CG_HD void sincos_shifted(double phi0, double c0, double s0, double d, double* s
 // v <- H2B2 . R(phi_x, phi_y) . B1H1 . v.  The phase phi = phaseAdv + 2 pi dnu
 // is rounded as in the reference and applied by angle addition
 // (sincos_shifted); the amplitude uses 1/beta.  Both differ from the
-// reference's direct forms by an ulp or so.
-CG_HD void section_map_particle(const SectionDev& s, const RingDev& r, double v[6]) {
+// reference's direct forms by an ulp or so.  section_map_rotated stops at
+// the rotated normal-form vector R(phi) . B1H1 . v (Bunch.cpp:706-712), whose
+// angles the reference accumulates as each particle's phase advance at the
+// ring's last section (Bunch.cpp:715-731).
+CG_HD void section_map_rotated(const SectionDev& s, const RingDev& r, const double v[6],
+                               double v2[6]) {
   const double dp = v[5];
   double x = v[0] - s.eta_x * dp;
   double px = v[1] - s.etap_x * dp;
@@ -140,13 +144,17 @@ CG_HD void section_map_particle(const SectionDev& s, const RingDev& r, double v[
   sincos_shifted(s.phase_adv_y, s.cos_y, s.sin_y, phiY - s.phase_adv_y, &sy, &cy);
   double v1[6];
   matvec6_section(s, s.b1h1, v, v1);
-  double v2[6];
   v2[0] = fma(cx, v1[0], sx * v1[1]);
   v2[1] = fma(-sx, v1[0], cx * v1[1]);
   v2[2] = fma(cy, v1[2], sy * v1[3]);
   v2[3] = fma(-sy, v1[2], cy * v1[3]);
   v2[4] = v1[4];
   v2[5] = v1[5];
+}
+
+CG_HD void section_map_particle(const SectionDev& s, const RingDev& r, double v[6]) {
+  double v2[6];
+  section_map_rotated(s, r, v, v2);
   matvec6_section(s, s.h2b2, v2, v);
 }
 

@@ -20,9 +20,8 @@
 // (transmission < 0.5 at Bunch.cpp:194-197, ion overflow at LIP.cpp:1043-1048).
 //
 // Not built here (paths outside the library's scope, kept as the reference's
-// declarations only): PIC beam-ion, ramping, drive mode, the per-particle
-// dump of MPBeamDataPrintPerTurn, the cavity transient printout of
-// InitialcavityResonator and the Haissinski solver.
+// declarations only): PIC beam-ion, ramping, drive mode, the cavity
+// transient printout of InitialcavityResonator and the Haissinski solver.
 #include <cmath>
 #include <complex>
 #include <cstdint>
@@ -438,6 +437,13 @@ void MPBeam::Initial(Train& train, LatticeInterActionPoint& latticeInterActionPo
                              B.eMomentumY.data(), B.ePositionZ.data(), B.eMomentumZ.data(), s.data()),
           "cg_upload_bunch");
   }
+  // the printed bunches' particle file needs every particle's accumulated
+  // phase advance (Bunch::InitialAccumPhaseAdV, MPBeam.cpp:115, and the map's
+  // update, Bunch.cpp:715-731): tracked on the device from here
+  const auto* run = inputParameter.ringRun;
+  if (!run->TBTBunchDisData.empty() && run->TBTBunchPrintNum > 0)
+    check(g, cg_set_phase_track(g.h, run->TBTBunchPrintNum, run->TBTBunchDisDataBunchIndex.data()),
+          "cg_set_phase_track");
 }
 
 // The library set the cavities' state in cg_set_beam (Initial) as the
@@ -741,8 +747,8 @@ void MPBeam::SSIonDataPrint(ReadInputSettings& inputParameter, LatticeInterActio
 // refreshed from the device first: totIonCharge (cg_bunch_ion_charge) and
 // bunchRFModeInfo (cg_rf_info); the moments are current after Run's
 // moments call.  The per-particle dump <TBTBunchDisData>_<j>.sdds needs the
-// accumulated phase advance of every particle, which the device does not
-// track: it is not written.
+// accumulated phase advance of every particle (cg_set_phase_track at
+// Initial, cg_phase_adv here).
 void MPBeam::MPBeamDataPrintPerTurn(int nTurns, LatticeInterActionPoint& latticeInterActionPoint,
                                     ReadInputSettings& inputParameter) {
   GpuBeam& g = gpu(this);
@@ -812,6 +818,58 @@ void MPBeam::MPBeamDataPrintPerTurn(int nTurns, LatticeInterActionPoint& lattice
         col(std::arg(info->induceVolBunchCen[c]));
       }
       fout << std::endl;
+    }
+  }
+  if (!run->TBTBunchDisData.empty() && run->TBTBunchPrintNum != 0) {
+    // the printed bunches' particles and their accumulated phase advances
+    // (MPBeam.cpp:2415-2491); the reference sizes each page by bunch i's
+    // count (beamVec[i], MPBeam.cpp:2475), the same for equal bunches
+    const double TWO_PI = 8 * std::atan(1.0);
+    for (int i = 0; i < run->TBTBunchPrintNum; ++i) {
+      const int j = run->TBTBunchDisDataBunchIndex[i];
+      MPBunch& b = beamVec[j];
+      const size_t n = b.macroEleNumPerBunch;
+      std::vector<uint8_t> sv(n);
+      check(g, cg_download_bunch(g.h, j, b.ePositionX.data(), b.eMomentumX.data(), b.ePositionY.data(),
+                                 b.eMomentumY.data(), b.ePositionZ.data(), b.eMomentumZ.data(), sv.data()),
+            "cg_download_bunch");
+      std::vector<double> ph(3 * n);
+      check(g, cg_phase_adv(g.h, j, ph.data()), "cg_phase_adv");
+      std::ofstream fout1(run->TBTBunchDisData + "_" + std::to_string(j) + ".sdds", std::ios_base::app);
+      if (nTurns == 0) {
+        fout1 << "SDDS1" << std::endl;
+        const char* pars[][2] = {{"BunchHarm", ""}, {"partNum", ""}, {"AverX", "m"}, {"AverY", "m"},
+                                 {"AverZ", "m"}, {"rmsEmitX", "m*rad"}, {"rmsEmitY", "m*rad"},
+                                 {"rmsEmitZ", "m*rad"}, {"rmsRx", "m"}, {"rmsRy", "m"},
+                                 {"rmsBunchLen", "m"}, {"rmsBunchEnergySpread", "rad"}};
+        for (auto& q : pars) {
+          fout1 << "&parameter name=" << q[0] << ", ";
+          if (q[1][0]) fout1 << "units=" << q[1] << ", ";
+          fout1 << "type=float,  &end" << std::endl;
+        }
+        const char* cols[][2] = {{"x", "m"}, {"y", "m"}, {"z", "m"}, {"xp", "rad"}, {"yp", "rad"},
+                                 {"zp", "rad"}, {"nux", ""}, {"nuy", ""}, {"nus", ""}};
+        for (auto& q : cols) {
+          fout1 << "&column name=" << q[0] << ", ";
+          if (q[1][0]) fout1 << "units=" << q[1] << ", ";
+          fout1 << "type=float,  &end" << std::endl;
+        }
+        fout1 << "&data mode=ascii, &end" << std::endl;
+      }
+      fout1 << "! page number " << nTurns * run->TBTBunchPrintNum + i + 1 << std::endl;
+      for (double v : {(double)b.bunchHarmNum, b.electronNumPerBunch, b.xAver, b.yAver, b.zAver,
+                       b.emittanceX, b.emittanceY, b.emittanceZ, b.rmsRx, b.rmsRy, b.rmsBunchLength,
+                       b.rmsEnergySpread})
+        fout1 << v << std::endl;
+      fout1 << b.macroEleNumPerBunch << std::endl;
+      for (size_t k = 0; k < n; ++k)
+        fout1 << std::setw(20) << std::left << b.ePositionX[k] << std::setw(20) << std::left
+              << b.ePositionY[k] << std::setw(20) << std::left << b.ePositionZ[k] << std::setw(20)
+              << std::left << b.eMomentumX[k] << std::setw(20) << std::left << b.eMomentumY[k]
+              << std::setw(20) << std::left << b.eMomentumZ[k] << std::setw(20) << std::left
+              << ph[k] / TWO_PI / (nTurns + 1) << std::setw(20) << std::left
+              << ph[n + k] / TWO_PI / (nTurns + 1) << std::setw(20) << std::left
+              << 1 - ph[2 * n + k] / TWO_PI / (nTurns + 1) << std::endl;
     }
   }
   if (!run->TBTBunchPro.empty() && run->TBTBunchPrintNum != 0) {

@@ -318,6 +318,14 @@ int cg_beam_ion_ip(cg_handle* h, int turn, int k);
  * -> Bunch::BunchTransferDueToLatticeTSymplectic, Bunch.cpp:625-755). */
 int cg_section_map(cg_handle* h, int k);
 
+/* The accumulated phase advance of every particle of the listed bunches
+ * (Bunch::accPhaseAdvX/Y/Z[i][2]: Bunch::InitialAccumPhaseAdV, Bunch.cpp:
+ * 504-553, from the current coordinates, then the update of the ring's last
+ * section map, Bunch.cpp:715-731), for the particle file of
+ * MPBeam::MPBeamDataPrintPerTurn (MPBeam.cpp:2439-2491).  n = 0 stops it.
+ * cg_phase_adv returns bunch j's accumulated x, y, z phases, 3 x n_macro. */
+int cg_set_phase_track(cg_handle* h, int n, const int* bunches);
+int cg_phase_adv(cg_handle* h, int j, double* out);
 /* MPBeam::BeamMomtumUpdateDueToRFTest for RFCA cavities (MPBeam.cpp:2624-2706
  * -> Bunch::BunchMomentumUpdateDueToRFCA, Bunch.cpp:453-481). */
 int cg_rf_kick(cg_handle* h);

@@ -48,7 +48,7 @@ def load():
         for n in ("ref_info", "ref_bunch_info", "ref_set_emit_nat", "ref_bunch_size", "ref_set_bunch",
                   "ref_get_bunch", "ref_moments", "ref_beam_info", "ref_stage", "ref_run_turns",
                   "ref_ion_count", "ref_ion_get", "ref_ion_set", "ref_sr_bins", "ref_ring",
-                  "ref_resonator", "ref_rf_info", "ref_bbi_profile", "ref_bunch_ion_charge"):
+                  "ref_resonator", "ref_rf_info", "ref_bbi_profile", "ref_bunch_ion_charge", "ref_phase_adv"):
             getattr(L, n).restype = C.c_int
         L.cg_ref_seed.argtypes = [C.c_ulonglong, C.c_longlong]
         L.cg_ref_seed.restype = None
@@ -139,6 +139,12 @@ class RefBeam:
         if n < 0:
             raise RuntimeError("bad IP or species")
         return fx[:n], fy[:n]
+
+    def phase_adv(self, j):
+        n = self.lib.ref_bunch_size(self.h, j)
+        out = np.empty(3 * n)
+        self._check(self.lib.ref_phase_adv(self.h, j, _dp(out)))
+        return out.reshape(3, n)
 
     def bunch_ion_charge(self, j):
         out = C.c_double()

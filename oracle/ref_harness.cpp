@@ -397,6 +397,23 @@ int ref_set_bunch(void *h, int j, int n, const double *x, const double *px, cons
         B.eMomentumZ[i] = dp[i];
         B.eSurive[i] = surv ? surv[i] : 0;
     }
+    // the particles' initial phase angles, as MPBeam::Initial sets them for
+    // the generated ones (MPBeam.cpp:115)
+    B.InitialAccumPhaseAdV(r->lat, r->in);
+    return 0;
+}
+
+// accPhaseAdvX/Y/Z[i][2] of bunch j (Bunch.cpp:715-731), 3 x n
+int ref_phase_adv(void *h, int j, double *out) {
+    RefRun *r = static_cast<RefRun *>(h);
+    if (j < 0 || j >= (int)r->beam.beamVec.size()) return 1;
+    const MPBunch &B = r->beam.beamVec[j];
+    const int n = B.macroEleNumPerBunch;
+    for (int i = 0; i < n; ++i) {
+        out[i] = B.accPhaseAdvX[i][2];
+        out[n + i] = B.accPhaseAdvY[i][2];
+        out[2 * n + i] = B.accPhaseAdvZ[i][2];
+    }
     return 0;
 }
 

@@ -218,16 +218,19 @@ def test_dropin_with_space_charge_matches_the_reference_program(tmp_path, case_n
 
 
 def read_pages(path):
-    """Every page of a multi-page SDDS ASCII file: (column names, [rows per page])."""
+    """Every page of a multi-page SDDS ASCII file: (column names, [rows per
+    page]); a page's parameter lines come before its row count."""
     lines = open(path).read().splitlines()
     cols = [ln.split("name=")[1].split(",")[0] for ln in lines if ln.startswith("&column")]
+    npar = sum(1 for ln in lines if ln.startswith("&parameter"))
     pages = []
     i = next(k for k, ln in enumerate(lines) if ln.startswith("&data")) + 1
     while i < len(lines):
         assert lines[i].startswith("! page number"), lines[i]
-        n = int(lines[i + 1])
-        pages.append(np.array([[float(v) for v in ln.split()] for ln in lines[i + 2:i + 2 + n]]))
-        i += 2 + n
+        i += 1 + npar
+        n = int(lines[i])
+        pages.append(np.array([[float(v) for v in ln.split()] for ln in lines[i + 1:i + 1 + n]]))
+        i += 1 + n
     return cols, pages
 
 
@@ -244,7 +247,8 @@ def test_dropin_per_bunch_files_match_the_reference_program(tmp_path):
     wl.cfg.flag_synrad = 0
     src = tmp_path / "src"
     input_dat.write_case(str(src), wl, n_turns=20, print_interval=5, qe=False,
-                         extra=["runTBTBunchAverData = tbt_aver", "runTBTBunchProfile = tbt_pro"])
+                         extra=["runTBTBunchAverData = tbt_aver", "runTBTBunchProfile = tbt_pro",
+                                "runTBTBunchDisData = tbt_dis"])
     dirs = []
     for name in ("ref", "gpu"):
         d = tmp_path / name
@@ -252,7 +256,7 @@ def test_dropin_per_bunch_files_match_the_reference_program(tmp_path):
         dirs.append(str(d))
     run(ref.EXE, dirs[0], teardown_may_crash=True)
     run(DROPIN, dirs[1])
-    for f in ("tbt_aver.sdds", "tbt_pro_0.sdds"):
+    for f in ("tbt_aver.sdds", "tbt_pro_0.sdds", "tbt_dis_0.sdds"):
         cr, pr = read_pages(os.path.join(dirs[0], f))
         cg, pg = read_pages(os.path.join(dirs[1], f))
         assert cr == cg and len(pr) == len(pg) == 4, f
@@ -268,7 +272,9 @@ def test_dropin_per_bunch_files_match_the_reference_program(tmp_path):
                     d = np.abs(np.angle(np.exp(1j * (x - y))))
                 else:
                     d = np.abs(x - y)
-                assert np.all(d <= 1e-7 * np.maximum(np.abs(x), 1e-3 * scale) + 1e-300), (f, name)
+                # tbt_aver prints 16 digits, the others the stream's 6
+                rtol = 1e-7 if f == "tbt_aver.sdds" else 2e-5
+                assert np.all(d <= rtol * np.maximum(np.abs(x), 1e-3 * scale) + 1e-300), (f, name)
 
 
 def test_dropin_ion_dump_has_the_reference_layout(tmp_path):

@@ -94,7 +94,7 @@ def test_gpu_and_reference_side_by_side_fast_ion_ip_records(tmp_path):
             fxr, fyr = r.ion_forces(k)
             fxg, fyg, _ = g.ion_forces(k)
             assert len(fxg) == len(fxr)
-            for a, b in ((fxg, fxr), (fyg, fyr)):
+            for a, b in ((fxg, fxr), (fyg, fyr)) if len(fxr) else ():
                 assert np.max(np.abs(a - b)) <= 1e-10 * np.max(np.abs(b)), k
     # after the last IP: every bunch's totIonCharge (MPBunch.cpp:1208-1209)
     import ctypes as C
@@ -194,3 +194,24 @@ def test_quantum_excitation_statistics_over_seeds(tmp_path):
     init = [1.5 ** 2 * wl.gen[0], 1.5 ** 2 * wl.gen[1], 1.5 * wl.gen[2], 1.5 * wl.gen[3]]
     for m in (a.mean(0), b.mean(0)):
         assert m[0] < 0.95 * init[0] and m[2] < 0.99 * init[2]
+
+
+@pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("case, bunches", [("batched_lr_fir", [0, 450]), ("fast_ion", [0, 79])])
+def test_particle_phase_advance_matches_the_reference(tmp_path, case, bunches):
+    """The accumulated phase advance of every particle of two bunches over
+    the case's turns (Bunch.cpp:715-731; the turn graph, with the segmented
+    maps of the ion train) against the reference."""
+    wl, path, parts = refcases.build(case, str(tmp_path))
+    r = ref.RefBeam(path, seed=wl.cfg.seed)
+    r.set_emit_nat([0.0, 0.0, 0.0])
+    g = MPBeam(wl)
+    refcases.start(case, r, wl, parts)
+    refcases.start(case, g, wl, parts)
+    g.set_phase_track(bunches)
+    turns = refcases.CASES[case][2]
+    r.Run(0, turns)
+    g.Run(0, turns)
+    for j in bunches:
+        a, b = g.phase_adv(j), r.phase_adv(j)
+        assert np.max(np.abs(a - b)) <= 1e-9 * np.max(np.abs(b)), j
