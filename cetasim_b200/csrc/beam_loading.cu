@@ -54,9 +54,6 @@ __device__ __forceinline__ Cx cx_sub(Cx a, Cx b) {
 __device__ __forceinline__ Cx cx_scale(Cx a, double s) {
   return {__dmul_rn(a.re, s), __dmul_rn(a.im, s)};
 }
-__device__ __forceinline__ Cx cx_div(Cx a, double s) {
-  return {__ddiv_rn(a.re, s), __ddiv_rn(a.im, s)};
-}
 __device__ __forceinline__ Cx cx_expi(double th) {
   double s, c;
   sincos(th, &s, &c);

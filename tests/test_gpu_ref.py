@@ -214,4 +214,10 @@ def test_particle_phase_advance_matches_the_reference(tmp_path, case, bunches):
     g.Run(0, turns)
     for j in bunches:
         a, b = g.phase_adv(j), r.phase_adv(j)
-        assert np.max(np.abs(a - b)) <= 1e-9 * np.max(np.abs(b)), j
+        # a particle whose turn-to-turn phase change lies within rounding of
+        # zero can take the other branch of the reference's rule (tmp >= 0 ?
+        # tmp : tmp + 2 pi, Bunch.cpp:725-727): then its sum differs by 2 pi
+        d = a - b
+        wraps = np.round(d / (2 * np.pi))
+        assert np.max(np.abs(d - 2 * np.pi * wraps)) <= 1e-9 * np.max(np.abs(b)), j
+        assert np.count_nonzero(wraps) <= max(1, 0.01 * wraps.size), (j, np.count_nonzero(wraps))
