@@ -8,7 +8,9 @@ keeps the digest of the initial particles, the final coordinates and
 survival flags (all bunches, or the listed ones), and every bunch's moments.
 
 Run from the repository root after building oracle/_ref:
-    python tests/golden/make_ref_golden.py
+    python tests/golden/make_ref_golden.py [case ...]
+With case names, only those cases are run and the other cases' entries of
+the existing fixture are kept.
 """
 import os
 import sys
@@ -28,8 +30,12 @@ from oracle import ref  # noqa: E402
 def main():
     if not ref.available():
         sys.exit("oracle/_ref/libcetasim_ref.so is not built")
+    only = sys.argv[1:]
     out = {}
-    for case in refcases.CASES:
+    if only and os.path.exists(refcases.GOLDEN):
+        old = np.load(refcases.GOLDEN)
+        out = {k: old[k] for k in old.files if k.split("/")[0] not in only}
+    for case in only or refcases.CASES:
         with tempfile.TemporaryDirectory() as d:
             wl, parts, r = refcases.run_ref(case, d)
             out[f"{case}/digest"] = np.frombuffer(bytes.fromhex(refcases.parts_digest(parts)),

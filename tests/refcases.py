@@ -22,6 +22,8 @@ CASES = {
     "plain_sr": ("plain_single", 0.005, 5, None, {}),
     # config 0's ring over 1000 turns (map, RF, drift, energy loss, damping)
     "plain_1000": ("plain_single", 0.01, 1000, None, {"flag_sr_wake": 0}),
+    # config 0 itself over 1000 turns: the short-range wake on, its 100 bins
+    "plain_sr_1000": ("plain_single", 0.005, 1000, None, {}),
     # config 1: 80 bunches x 25, 20 IPs, ions in the trapped regime
     "fast_ion": ("fast_ion", 0.00125, 4, TRAPPED, {}),
     # config 3's ragged 900-bunch train, 50 IPs, LR HOM wake and 9-tap FIR (no ions)
@@ -35,7 +37,7 @@ CASES = {
 }
 
 # bunches whose final coordinates the fixtures keep (all bunches' moments are kept)
-KEEP_BUNCHES = {"plain_sr": None, "plain_1000": None, "fast_ion": None,
+KEEP_BUNCHES = {"plain_sr": None, "plain_1000": None, "plain_sr_1000": None, "fast_ion": None,
                 "batched_lr_fir": list(range(0, 900, 30)), "trapping_slice": list(range(0, 150, 5))}
 
 

@@ -22,7 +22,7 @@ pytestmark = pytest.mark.gpu
 # GPU vs reference, max |delta| / rms of each coordinate over alive particles.
 # The GPU's transcendentals, fused multiply-adds and w(z) differ from the
 # host's by ulps; 1000 turns of the linear map grow that to ~1e-12.
-TOL = {"plain_sr": 1e-10, "plain_1000": 1e-10, "fast_ion": 1e-10, "batched_lr_fir": 1e-10,
+TOL = {"plain_sr": 1e-10, "plain_1000": 1e-10, "plain_sr_1000": 1e-10, "fast_ion": 1e-10, "batched_lr_fir": 1e-10,
        "trapping_slice": 1e-10}
 
 

@@ -21,7 +21,9 @@ TOL = {"plain_sr": 0.0, "plain_1000": 0.0, "batched_lr_fir": 0.0, "fast_ion": 1e
 live = pytest.mark.skipif(not ref.available(), reason="oracle/_ref/libcetasim_ref.so not built")
 
 
-@pytest.mark.parametrize("case", list(refcases.CASES))
+# plain_sr_1000's 1000 short-range-wake turns take the oracle minutes; the
+# CUDA path is checked against that fixture (test_gpu_ref.py)
+@pytest.mark.parametrize("case", [c for c in refcases.CASES if c != "plain_sr_1000"])
 def test_oracle_reproduces_reference_fixture(case, tmp_path):
     g = refcases.golden()
     wl, _, parts = refcases.build(case, str(tmp_path))
