@@ -20,8 +20,8 @@
 // (transmission < 0.5 at Bunch.cpp:194-197, ion overflow at LIP.cpp:1043-1048).
 //
 // Not built here (paths outside the library's scope, kept as the reference's
-// declarations only): PIC beam-ion, ramping, drive mode, the cavity
-// transient printout of InitialcavityResonator and the Haissinski solver.
+// declarations only): PIC beam-ion, ramping, drive mode and the Haissinski
+// solver.
 #include <cmath>
 #include <complex>
 #include <cstdint>
@@ -453,8 +453,109 @@ void MPBeam::Initial(Train& train, LatticeInterActionPoint& latticeInterActionPo
 // reference's own Resonator::GetInitialResonatorPower); the transient
 // printout of the reference's function (transResonParWriteTo) is not
 // written.
+// The printout of MPBeam::InitialcavityResonator (MPBeam.cpp:336-426): per
+// cavity the steady state of the fill pattern (the first pass of
+// MPBeam.cpp:262-334: induced voltage, generator voltage, current and powers
+// from the reference's own Resonator methods) and the induced voltage's
+// build-up from zero over 100 filling times, bunch by bunch, to
+// <rfTransientCavParWriteTo>.sdds.  Host arithmetic in std::complex, as
+// there; the tracking state is the library's.
+static void write_cavity_transient(const std::vector<MPBunch>& beamVec, ReadInputSettings& in,
+                                   const CavityResonator& cav) {
+  const int resNum = in.ringParRf->resNum, H = in.ringParBasic->harmonics;
+  const double f0 = in.ringParBasic->f0, PI = 4 * std::atan(1.E0), e = 1.602017733e-19;
+  const std::complex<double> li(0, 1);
+  std::ofstream fout(in.ringParRf->transResonParWriteTo + ".sdds");
+  fout << "SDDS1" << std::endl;
+  // the header lines as the reference prints them (MPBeam.cpp:342-368)
+  static const char* const head[] = {
+      "&parameter name=CavAmpIdeal,      units=V,   type=float,  &end",
+      "&parameter name=CavPhaseIdeal,    units=rad, type=float,  &end",
+      "&parameter name=CavFreq,          units=Hz,  type=float,  &end",
+      "&parameter name=GenAmp,           units=V,   type=float,  &end",
+      "&parameter name=GenPhase,         units=rad, type=float,  &end",
+      "&parameter name=beamIndAmp,       units=V,   type=float,  &end",
+      "&parameter name=beamIndPhase,     units=rad, type=float,  &end",
+      "&parameter name=CavDetunPsi,      units=rad, type=float,  &end",
+      "&parameter name=GenAmpIg,         units=Ampere, type=float,  &end",
+      "&parameter name=GenArgIg,         units=rad, type=float,  &end",
+      "&parameter name=LoadAnlge,        units=rad, type=float,  &end",
+      "&parameter name=BeamPower,        units=watt,type=float,  &end",
+      "&parameter name=GenPower,         units=watt,type=float,  &end",
+      "&parameter name=CavPower,         units=watt,type=float,  &end",
+      "&parameter name=GenReflectPower,  units=watt,type=float,  &end",
+      "",
+      "&column name=Turns,              units=s       type=float,  &end",
+      "&column name=CavAmpReq,          units=V,      type=float,  &end",
+      "&column name=CavPhaseReq,        units=rad,    type=float,  &end",
+      "&column name=CavAmp,             units=V,      type=float,  &end",
+      "&column name=CavPhase,           units=rad,    type=float,  &end",
+      "&column name=BeamIndAmp,         units=V,      type=float,  &end",
+      "&column name=BeamIndPhase,       units=rad,    type=float,  &end",
+      "&column name=GenAmp,             units=V,      type=float,  &end",
+      "&column name=GenPhase,           units=rad,    type=float,  &end"};
+  for (const char* l : head)
+    if (l[0]) fout << l << std::endl;
+  fout << "&data mode=ascii, &end" << std::endl;
+  for (int i = 0; i < resNum; i++) {
+    Resonator R = cav.resonatorVec[i];
+    const double tF = R.tF;
+    const int nTurns = std::ceil(100 * tF * f0);
+    // the first pass (MPBeam.cpp:262-330)
+    std::complex<double> vbAccum(0, 0), aver2(0, 0);
+    for (int n = 0; n < nTurns; n++) {
+      size_t k = 0;
+      for (int j = 0; j < H; j++) {
+        std::complex<double> vb0(0.E0, 0.E0);
+        if (k < beamVec.size() && beamVec[k].bunchHarmNum == j) {
+          vb0 = std::complex<double>(-1 * R.resFre * 2 * PI * R.resShuntImpRs / R.resQualityQ0, 0.E0) *
+                beamVec[k].electronNumPerBunch * e;
+          k++;
+        }
+        vbAccum += vb0;
+        const double tB = 1.0 / f0 / H, deltaL = tB / tF, cPsi = deltaL * std::tan(R.resDeTunePsi);
+        vbAccum = vbAccum * std::exp(-deltaL) * std::exp(li * cPsi);
+        if (n == nTurns - 1) aver2 += vbAccum;
+      }
+    }
+    R.vbAccum = aver2 / double(H);
+    R.resGenVol = R.resCavVolReq - R.vbAccum;
+    R.GetInitialResonatorGenIg(in);
+    R.GetInitialResonatorPower(in);
+    for (double v : {std::abs(R.resCavVolReq), std::arg(R.resCavVolReq), R.resFre, std::abs(R.resGenVol),
+                     std::arg(R.resGenVol), std::abs(R.vbAccum), std::arg(R.vbAccum), R.resDeTunePsi,
+                     std::abs(R.resGenIg), std::arg(R.resGenIg),
+                     std::arg(R.resGenIg) - std::arg(R.resCavVolReq), R.resBeamPower, R.resGenPower,
+                     R.resCavPower, R.resGenPowerReflect})
+      fout << v << std::endl;
+    fout << "! page number " << i + 1 << std::endl << nTurns * beamVec.size() << std::endl;
+    // the build-up from zero, generator off (MPBeam.cpp:400-424)
+    const std::complex<double> gen(0.E0, 0.E0);
+    std::complex<double> acc(0, 0);
+    double time = 0;
+    for (int n = 0; n < nTurns; n++)
+      for (size_t j = 0; j < beamVec.size(); j++) {
+        const std::complex<double> vb0 =
+            std::complex<double>(-1 * R.resFre * 2 * PI * R.resShuntImpRs / R.resQualityQ0, 0.E0) *
+            beamVec[j].electronNumPerBunch * e;
+        acc += vb0;
+        const double tB = beamVec[j].bunchGap * 1 / f0 / H;
+        time += tB;
+        const double deltaL = tB / tF, cPsi = deltaL * std::tan(R.resDeTunePsi);
+        fout << std::setw(15) << std::left << time * f0 << std::setw(15) << std::left
+             << std::abs(R.resCavVolReq) << std::setw(15) << std::left << std::arg(R.resCavVolReq)
+             << std::setw(15) << std::left << std::abs(acc + gen) << std::setw(15) << std::left
+             << std::arg(acc + gen) << std::setw(15) << std::left << std::abs(acc) << std::setw(15)
+             << std::left << std::arg(acc) << std::setw(15) << std::left << std::abs(gen)
+             << std::setw(15) << std::left << std::arg(gen) << std::endl;
+        acc = acc * std::exp(-deltaL) * std::exp(li * cPsi);
+      }
+  }
+}
+
 void MPBeam::InitialcavityResonator(ReadInputSettings& inputParameter, CavityResonator& cavityResonator) {
   GpuBeam& g = gpu(this);
+  write_cavity_transient(beamVec, inputParameter, cavityResonator);
   for (int i = 0; i < inputParameter.ringParRf->resNum; ++i) {
     if (inputParameter.ringParRf->rfMode[i] != 1) continue;
     double st[6];

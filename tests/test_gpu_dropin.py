@@ -155,6 +155,19 @@ def test_dropin_with_beam_loading_matches_the_reference_program(tmp_path):
         rtol = 2e-4 if name.startswith(("eigenEmit", "xyCoupling")) else 2e-5
         bad = np.abs(a - b) > rtol * np.maximum(np.abs(a), 1e-3 * scale)
         assert not bad.any(), (name, a[bad][:3], b[bad][:3])
+    # InitialcavityResonator's printout (MPBeam.cpp:336-426; no
+    # rfTransientCavParWriteTo given, so the file is ".sdds"): header lines
+    # equal, the parameters and the build-up rows to the printed digits
+    tr = open(os.path.join(dirs[0], ".sdds")).read().splitlines()
+    tg = open(os.path.join(dirs[1], ".sdds")).read().splitlines()
+    assert len(tr) == len(tg) and [l for l in tr if l.startswith(("SDDS", "&"))] == \
+        [l for l in tg if l.startswith(("SDDS", "&"))]
+    for a, b in zip(tr, tg):
+        if a.startswith(("SDDS", "&", "!")):
+            assert a == b
+            continue
+        va, vb = np.array(a.split(), float), np.array(b.split(), float)
+        assert np.all(np.abs(va - vb) <= 2e-5 * np.maximum(np.abs(va), 1e-300) + 1e-9), (a, b)
 
 
 @pytest.mark.parametrize("case_name", ["fd_train_lr", "td_train"])
