@@ -461,7 +461,7 @@ void MPBeam::Initial(Train& train, LatticeInterActionPoint& latticeInterActionPo
 // <rfTransientCavParWriteTo>.sdds.  Host arithmetic in std::complex, as
 // there; the tracking state is the library's.
 static void write_cavity_transient(const std::vector<MPBunch>& beamVec, ReadInputSettings& in,
-                                   const CavityResonator& cav) {
+                                   CavityResonator& cav) {
   const int resNum = in.ringParRf->resNum, H = in.ringParBasic->harmonics;
   const double f0 = in.ringParBasic->f0, PI = 4 * std::atan(1.E0), e = 1.602017733e-19;
   const std::complex<double> li(0, 1);
@@ -498,7 +498,11 @@ static void write_cavity_transient(const std::vector<MPBunch>& beamVec, ReadInpu
     if (l[0]) fout << l << std::endl;
   fout << "&data mode=ascii, &end" << std::endl;
   for (int i = 0; i < resNum; i++) {
-    Resonator R = cav.resonatorVec[i];
+    // the resonator itself (it owns its feedback objects, so no copy), its
+    // state put back after the printout
+    Resonator& R = cav.resonatorVec[i];
+    const std::complex<double> keep[4] = {R.vbAccum, R.resGenVol, R.resGenVgr, R.resGenIg};
+    const double keepP[4] = {R.resCavPower, R.resBeamPower, R.resGenPower, R.resGenPowerReflect};
     const double tF = R.tF;
     const int nTurns = std::ceil(100 * tF * f0);
     // the first pass (MPBeam.cpp:262-330)
@@ -550,6 +554,14 @@ static void write_cavity_transient(const std::vector<MPBunch>& beamVec, ReadInpu
              << std::setw(15) << std::left << std::arg(gen) << std::endl;
         acc = acc * std::exp(-deltaL) * std::exp(li * cPsi);
       }
+    R.vbAccum = keep[0];
+    R.resGenVol = keep[1];
+    R.resGenVgr = keep[2];
+    R.resGenIg = keep[3];
+    R.resCavPower = keepP[0];
+    R.resBeamPower = keepP[1];
+    R.resGenPower = keepP[2];
+    R.resGenPowerReflect = keepP[3];
   }
 }
 
