@@ -316,6 +316,8 @@ def main():
     ap.add_argument("--shard", action="store_true",
                     help="N > 1: one beam split by bunches over the ranks (strong scaling; "
                          "moments all-gathered over NCCL) instead of N replicas")
+    ap.add_argument("--no-widened", action="store_true",
+                    help="skip the broadband-impedance and space-charge stage timings")
     ap.add_argument("--no-surrogate", action="store_true",
                     help="skip the surrogate measurement (training + surrogate turns)")
     ap.add_argument("--kick-variant", type=int, default=None, metavar="V",
@@ -538,6 +540,13 @@ def main():
         sur = surrogate_leg(args, beam, lib, stream, flush, kms["ion_field_kick"], tot_ms / args.steps,
                             clk.summary().get("sm_max_mhz"))
 
+    widened = None
+    if world == 1 and not args.no_widened:
+        try:
+            widened = widened_leg(measured_peak("hbm_gbs"))
+        except Exception as e:  # reported, never required
+            widened = {"failed": str(e)}
+
     result = None
     if rank == 0:
         cpu = None
@@ -586,6 +595,7 @@ def main():
                                  f"{g}x{w}{'r' if r else ''}": round(float(m), 4)
                                  for (g, w, r), m in zip(_abi.PIPE_SHAPES, pipe[1])}}},
             "surrogate": sur,
+            "widened_stages": widened,
             "e2e": {"value": e2e_value, "unit": "macroparticle-turns/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches.value * args.steps,
@@ -620,6 +630,74 @@ def measured_peak(key):
     except (OSError, ValueError):
         pass
     return fallback[key], f"fallback ({key} of an earlier measurement on this pool)"
+
+
+def widened_leg(hbm):
+    """The stages beyond the ion hot path on the 80-bunch fast-ion train at
+    full size (80 x 2e4 macroparticles): the broadband-impedance kick
+    (frequency domain, 640 impedance samples to 300 GHz; time domain, a
+    400-sample wake table) and the space charge at one section (2.5-D PIC on
+    32 x 32 x 33, and the Bassetti-Erskine slices).  Each is the time of one
+    host-synchronous C-ABI call (launches and the status read included),
+    averaged over 20 after 3 warm-up calls; achieved = the stage's algorithmic
+    bytes (read z, x, y and read-write px, py, dp: 72 B per macroparticle)
+    over that time, against the measured copy bandwidth."""
+    from cetasim_b200 import configs
+    from cetasim_b200.beam import MPBeam
+
+    def resonators(n, fmax):
+        f = np.arange(n) * (fmax / (n - 1))
+        t = np.zeros((n, 11))
+        t[:, 0] = f
+        with np.errstate(divide="ignore", invalid="ignore"):
+            for p, (rs, fr) in enumerate(((2e4, 40e9), (4e5, 30e9), (4e5, 30e9), (1e5, 30e9), (1e5, 30e9))):
+                z = rs / (1 + 1j * (fr / f - f / fr)) * (fr / f if p else 1.0)
+                z[0] = 0
+                t[:, 1 + p], t[:, 6 + p] = z.real, z.imag
+        return t
+
+    def wake(nw, dzw, cen):
+        z = (np.arange(nw) - cen) * dzw
+        env = np.exp(-0.5 * (z / 1.5e-3) ** 2) + np.where(z > 0, np.exp(-z / 20e-3), 0.0)
+        t = np.zeros((nw, 6))
+        t[:, 0] = z
+        for p, a in enumerate((3e13, 2e15, 2e15, 5e14, 5e14)):
+            t[:, 1 + p] = a * env * np.cos(2 * np.pi * z / 6e-3 + 0.3 * p)
+        t[cen, 0] = 0.0
+        return t
+
+    def timed(fn, reps=20):
+        for _ in range(3):
+            fn()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        return (time.perf_counter() - t0) / reps * 1e3
+
+    out = {"workload": "fast_ion train at full size: 80 bunches x 2e4 macroparticles",
+           "timing": "host-synchronous C-ABI call, mean of 20 after 3 warm-up",
+           "peak_gbs": hbm[0], "peak_source": hbm[1]}
+    cases = [("bbi_frequency_domain", "bbi", 0, resonators(640, 300e9)),
+             ("bbi_time_domain", "bbi", 1, wake(400, 0.5e-3, 40)),
+             ("space_charge_pic_32x32x33", "sc", 2, None),
+             ("space_charge_bassetti_erskine", "sc", 1, None)]
+    for name, kind, mode, table in cases:
+        wl = configs.make("fast_ion", n_scale=1.0)
+        wl.cfg.flag_beam_ion = 0
+        if kind == "bbi":
+            wl.set_bbi(table, mode)
+        else:
+            wl.cfg.flag_sc = mode
+            for i, v in enumerate((32, 32, 33)):
+                wl.cfg.sc_mesh[i] = v
+        b = MPBeam(wl)
+        b.generate(seed=3)
+        b.MPBeamRMSCal(0)
+        ms = timed(b.BBImpBeamInteraction if kind == "bbi" else (lambda: b.BeamTransferDueToSpaceCharge(0)))
+        gbs = 72.0 * wl.n_particles / (ms * 1e-3) / 1e9
+        out[name] = {"ms": ms, "achieved_gbs": gbs, "frac": gbs / hbm[0] if hbm[0] else None}
+        b.close()
+    return out
 
 
 def surrogate_leg(args, beam, lib, stream, flush, exact_kick_ms, exact_turn_ms, sm_mhz):
