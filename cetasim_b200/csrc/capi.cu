@@ -127,7 +127,9 @@ void free_beam(Handle& h) {
   dfree(d.phase_slot); dfree(d.phase_ptr);
   d.phase_slot = nullptr; d.phase_ptr = nullptr;
   dfree(d.sc_geom); dfree(d.sc_cnt); dfree(d.sc_acc); dfree(d.sc_field);
+  dfree(d.sc_slice_of); dfree(d.sc_list); dfree(d.sc_start); dfree(d.sc_cursor);
   d.sc_geom = nullptr; d.sc_cnt = nullptr; d.sc_acc = nullptr; d.sc_field = nullptr;
+  d.sc_slice_of = nullptr; d.sc_list = nullptr; d.sc_start = nullptr; d.sc_cursor = nullptr;
   h.cbm_cap = h.cbm_n = 0;
   IonWalk& w = d.iw;
   dfree(w.births); dfree(w.prep); dfree(w.bunch); dfree(w.spec); dfree(w.bound); dfree(w.part);
@@ -930,13 +932,15 @@ int cg_set_beam(cg_handle* H, int M, const int* n_macro, const int* harm, const 
     }
     const size_t slices = (size_t)M * p.nz;
     if (dalloc(&d.sc_geom, (size_t)M * 11) || dalloc(&d.sc_cnt, slices) ||
-        dalloc(&d.sc_acc, slices * p.acc_per_slice) ||
-        (p.flag == 2 && dalloc(&d.sc_field, slices * 2 * p.nx * p.ny))) {
+        (p.flag != 2 && dalloc(&d.sc_acc, slices * p.acc_per_slice)) ||
+        (p.flag == 2 && (dalloc(&d.sc_field, slices * 2 * p.nx * p.ny) ||
+                         dalloc(&d.sc_slice_of, (size_t)h.npad) || dalloc(&d.sc_list, (size_t)h.npad) ||
+                         dalloc(&d.sc_start, slices) || dalloc(&d.sc_cursor, slices)))) {
       free_beam(h);
       return fail(&h, CG_ERR_OOM, "space-charge buffers");
     }
     cudaMemset(d.sc_geom, 0, sizeof(double) * M * 11);
-    cudaMemset(d.sc_acc, 0, sizeof(unsigned long long) * slices * p.acc_per_slice);
+    if (d.sc_acc) cudaMemset(d.sc_acc, 0, sizeof(unsigned long long) * slices * p.acc_per_slice);
   }
   if (h.cfg.bbi.flag) {
     const size_t wc = h.bbi.wcap;

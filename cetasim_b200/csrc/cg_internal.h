@@ -167,6 +167,10 @@ struct DeviceBufs {
   int* sc_cnt = nullptr;           // M x nz particles per slice
   unsigned long long* sc_acc = nullptr;  // M x nz x acc_per_slice fixed-point sums
   double* sc_field = nullptr;      // M x nz x 2 x nx x ny mesh field (PIC)
+  int* sc_slice_of = nullptr;      // npad: each particle's slice (PIC)
+  int* sc_list = nullptr;          // npad: particle indices grouped by bunch and slice (PIC)
+  int* sc_start = nullptr;         // M x nz: first list entry of each slice (PIC)
+  int* sc_cursor = nullptr;        // M x nz: fill cursors (PIC)
   double* sc_sin = nullptr;        // nx x nx + ny x ny: 2 sin(pi (i + 1)(k + 1) / (n + 1))
   // phase advance of the tracked bunches: slot per bunch (-1 untracked),
   // per slot 6 x n (previous angles x, y, z; accumulated x, y, z)

@@ -20,13 +20,15 @@
 //                seeded with particle 0), the slice width, the mesh
 //                (PIC2D::Set2DMesh(rms, centroid), PIC2D.cpp), the largest
 //                |x|, |y| for the fixed-point scales.
-//  k_sc_deposit  per tile: slice counts; PIC: cloud-in-cell charge in 64-bit
-//                fixed point (order-independent sums under atomics);
-//                analytic: per-slice sums of x and y.
+//  k_sc_deposit  per tile: slice counts; PIC: each particle's slice;
+//                analytic: per-slice sums of x and y in 64-bit fixed point
+//                (order-independent sums under atomics).
+//  k_sc_offsets, k_sc_scatter (PIC): the particles grouped by slice.
 //  k_sc_second   per tile (analytic): per-slice sums of (x - <x>)^2, (y - <y>)^2.
-//  k_sc_solve    one CTA per (bunch, slice) (PIC): the DST-I Poisson solve
-//                as two matrix products each way in shared memory, then the
-//                field on the mesh; resets the slice's charge accumulators.
+//  k_sc_solve    one CTA per (bunch, slice) (PIC): the slice's cloud-in-cell
+//                charge in shared memory (fixed point), the DST-I Poisson
+//                solve as two matrix products each way, then the field on
+//                the mesh.
 //  k_sc_kick     per tile: the field at each particle and the kick.
 #include <cuda_runtime.h>
 
@@ -155,7 +157,8 @@ __global__ void __launch_bounds__(kTile) k_sc_deposit(const double* __restrict__
                                                       const int* __restrict__ tile_bunch,
                                                       const BunchDev* __restrict__ bunch,
                                                       ScParams p, const double* __restrict__ geom,
-                                                      int* cnt, unsigned long long* acc) {
+                                                      int* cnt, unsigned long long* acc,
+                                                      int* slice_of) {
   const int b = tile_bunch[blockIdx.x];
   const BunchDev& Bd = bunch[b];
   const int i = (blockIdx.x - Bd.tile_off) * kTile + threadIdx.x;
@@ -166,21 +169,11 @@ __global__ void __launch_bounds__(kTile) k_sc_deposit(const double* __restrict__
   const int s = sc_slice(c[4 * npad + g], G, p.nz);
   const size_t bs = (size_t)b * p.nz + s;
   atomicAdd(&cnt[bs], 1);
-  const double x = c[g], y = c[2 * npad + g];
-  unsigned long long* A = acc + bs * p.acc_per_slice;
   if (p.flag == 2) {
-    int ix, iy;
-    double w[4];
-    if (!sc_cell(x, y, G, p, &ix, &iy, w)) return;
-    const double charge = Bd.q_macro * kElectronCharge / G[kGDz];
-    const int e = (int)G[kGExp0];
-    const int node[4] = {ix * p.ny + iy, (ix + 1) * p.ny + iy, ix * p.ny + iy + 1,
-                         (ix + 1) * p.ny + iy + 1};
-    for (int j = 0; j < 4; ++j) {
-      const double v = w[j] * charge / G[kGDv];  // [C/m^3], PIC2D.cpp rho +=
-      atomicAdd(&A[node[j]], (unsigned long long)__double2ll_rn(scalbn(v, e)));
-    }
+    slice_of[g] = s;  // the slice's CTA deposits its particles (k_sc_solve)
   } else {
+    const double x = c[g], y = c[2 * npad + g];
+    unsigned long long* A = acc + bs * p.acc_per_slice;
     atomicAdd(&A[0], (unsigned long long)__double2ll_rn(scalbn(x, (int)G[kGExp0])));
     atomicAdd(&A[1], (unsigned long long)__double2ll_rn(scalbn(y, (int)G[kGExp1])));
   }
@@ -188,6 +181,41 @@ __global__ void __launch_bounds__(kTile) k_sc_deposit(const double* __restrict__
 
 __device__ __forceinline__ double sc_fix(unsigned long long v, int e) {
   return scalbn((double)(long long)v, -e);
+}
+
+// PIC: each bunch's particles grouped by slice (a counting sort: the
+// slices' starts, then every particle's index at its slice's cursor), so
+// that one CTA per slice deposits its own particles in shared memory
+__global__ void k_sc_offsets(const BunchDev* __restrict__ bunch, int nz, const int* __restrict__ cnt,
+                             int* start, int* cursor, int M) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= M) return;
+  int pos = bunch[b].tile_off * kTile;
+  for (int s = 0; s < nz; ++s) {
+    start[(size_t)b * nz + s] = pos;
+    cursor[(size_t)b * nz + s] = pos;
+    pos += cnt[(size_t)b * nz + s];
+  }
+}
+
+__global__ void __launch_bounds__(kTile) k_sc_scatter(const int* __restrict__ tile_bunch,
+                                                      const BunchDev* __restrict__ bunch, int nz,
+                                                      const double* __restrict__ geom,
+                                                      const int* __restrict__ slice_of, int* cursor,
+                                                      int* list) {
+  const int b = tile_bunch[blockIdx.x];
+  const BunchDev& Bd = bunch[b];
+  const int i = (blockIdx.x - Bd.tile_off) * kTile + threadIdx.x;
+  const int64_t g = (int64_t)blockIdx.x * kTile + threadIdx.x;
+  const bool in = i < Bd.n && geom[(size_t)b * kScGeom + kGDv] != 0;
+  const int key = in ? b * nz + slice_of[g] : -1;
+  // one cursor increment per slice and warp
+  const unsigned peers = __match_any_sync(SC_FULL, key);
+  const int lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
+  int base = 0;
+  if (in && lane == leader) base = atomicAdd(&cursor[key], __popc(peers));
+  base = __shfl_sync(SC_FULL, base, leader);
+  if (in) list[base + __popc(peers & ((1u << lane) - 1u))] = (int)g;
 }
 
 // analytic models: second pass, (x - <x>)^2 and (y - <y>)^2 per slice
@@ -216,9 +244,13 @@ __global__ void __launch_bounds__(kTile) k_sc_second(const double* __restrict__ 
 // One CTA per (bunch, slice): PIC2D::Set2DPhi and Set2DEField (PIC2D.cpp).
 // The 2-D DST-I (RODFT00, Y_k = 2 sum_j X_j sin(pi (j + 1)(k + 1) / (n + 1))
 // along each axis) as S_x R S_y^T in shared memory; sx, sy hold 2 sin(...).
-__global__ void __launch_bounds__(kScThreads) k_sc_solve(ScParams p, const double* __restrict__ geom,
+__global__ void __launch_bounds__(kScThreads) k_sc_solve(ScParams p, const double* __restrict__ c,
+                                                         int64_t npad,
+                                                         const BunchDev* __restrict__ bunch,
+                                                         const double* __restrict__ geom,
                                                          const int* __restrict__ cnt,
-                                                         unsigned long long* acc,
+                                                         const int* __restrict__ start,
+                                                         const int* __restrict__ list,
                                                          const double* __restrict__ sxy,
                                                          double* field) {
   extern __shared__ double sm[];
@@ -226,21 +258,33 @@ __global__ void __launch_bounds__(kScThreads) k_sc_solve(ScParams p, const doubl
   const int b = blockIdx.x / p.nz;
   const size_t bs = blockIdx.x;
   const double* G = geom + (size_t)b * kScGeom;
-  unsigned long long* A = acc + bs * p.acc_per_slice;
-  if (cnt[bs] < 2 || G[kGDv] == 0) {
-    // a skipped slice (MPBunch.cpp:916) leaves its accumulators zero
-    for (int t = threadIdx.x; t < N; t += kScThreads) A[t] = 0ull;
-    return;
-  }
+  const int n = cnt[bs];
+  if (n < 2 || G[kGDv] == 0) return;  // a skipped slice (MPBunch.cpp:916)
   double* R = sm;
   double* T = sm + N;
   double* Sx = sm + 2 * N;
   double* Sy = Sx + nx * nx;
+  unsigned long long* S = reinterpret_cast<unsigned long long*>(Sy + ny * ny);
   const int e = (int)G[kGExp0];
-  for (int t = threadIdx.x; t < N; t += kScThreads) {
-    R[t] = sc_fix(A[t], e);
-    A[t] = 0ull;
+  for (int t = threadIdx.x; t < N; t += kScThreads) S[t] = 0ull;
+  __syncthreads();
+  // PIC2D::Set2DRho (PIC2D.cpp): cloud-in-cell charge [C/m^3] of the slice's
+  // particles, in 64-bit fixed point (order-independent)
+  const double charge = bunch[b].q_macro * kElectronCharge / G[kGDz];
+  const int* L = list + start[bs];
+  for (int t = threadIdx.x; t < n; t += kScThreads) {
+    const int64_t g = L[t];
+    int ix, iy;
+    double w[4];
+    if (!sc_cell(c[g], c[2 * npad + g], G, p, &ix, &iy, w)) continue;
+    const int node[4] = {ix * ny + iy, (ix + 1) * ny + iy, ix * ny + iy + 1, (ix + 1) * ny + iy + 1};
+    for (int j = 0; j < 4; ++j) {
+      const double v = w[j] * charge / G[kGDv];
+      atomicAdd(&S[node[j]], (unsigned long long)__double2ll_rn(scalbn(v, e)));
+    }
   }
+  __syncthreads();
+  for (int t = threadIdx.x; t < N; t += kScThreads) R[t] = sc_fix(S[t], e);
   for (int t = threadIdx.x; t < nx * nx; t += kScThreads) Sx[t] = sxy[t];
   for (int t = threadIdx.x; t < ny * ny; t += kScThreads) Sy[t] = sxy[nx * nx + t];
   __syncthreads();
@@ -359,7 +403,7 @@ cudaError_t upload_weideman_table_sc() {
 }
 
 size_t sc_solve_smem(const ScParams& p) {
-  return sizeof(double) * ((size_t)2 * p.nx * p.ny + p.nx * p.nx + p.ny * p.ny);
+  return sizeof(double) * ((size_t)3 * p.nx * p.ny + p.nx * p.nx + p.ny * p.ny);
 }
 
 cudaError_t prepare_sc(const ScParams& p) {
@@ -380,10 +424,16 @@ cudaError_t launch_space_charge(Handle& h, int k) {
   k_sc_geom<<<h.M, kScThreads, 0, h.stream>>>(h.d.c, h.npad, h.d.surv, h.d.bunch, h.d.mom, p,
                                              h.d.sc_geom, h.d.status);
   k_sc_deposit<<<h.n_tiles, kTile, 0, h.stream>>>(h.d.c, h.npad, h.d.tile_bunch, h.d.bunch, p,
-                                                  h.d.sc_geom, h.d.sc_cnt, h.d.sc_acc);
+                                                  h.d.sc_geom, h.d.sc_cnt, h.d.sc_acc,
+                                                  h.d.sc_slice_of);
   if (p.flag == 2) {
+    k_sc_offsets<<<(h.M + 127) / 128, 128, 0, h.stream>>>(h.d.bunch, p.nz, h.d.sc_cnt,
+                                                         h.d.sc_start, h.d.sc_cursor, h.M);
+    k_sc_scatter<<<h.n_tiles, kTile, 0, h.stream>>>(h.d.tile_bunch, h.d.bunch, p.nz, h.d.sc_geom,
+                                                    h.d.sc_slice_of, h.d.sc_cursor, h.d.sc_list);
     k_sc_solve<<<h.M * p.nz, kScThreads, sc_solve_smem(p), h.stream>>>(
-        p, h.d.sc_geom, h.d.sc_cnt, h.d.sc_acc, h.d.sc_sin, h.d.sc_field);
+        p, h.d.c, h.npad, h.d.bunch, h.d.sc_geom, h.d.sc_cnt, h.d.sc_start, h.d.sc_list, h.d.sc_sin,
+        h.d.sc_field);
   } else {
     k_sc_second<<<h.n_tiles, kTile, 0, h.stream>>>(h.d.c, h.npad, h.d.tile_bunch, h.d.bunch, p,
                                                    h.d.sc_geom, h.d.sc_cnt, h.d.sc_acc);
