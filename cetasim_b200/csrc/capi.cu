@@ -672,7 +672,7 @@ int cg_create(const cg_config* cfg, int device, cg_handle** out) {
     if (p.flag == 2) {
       // the DST-I matrices 2 sin(pi (i + 1)(k + 1) / (n + 1)), the argument
       // reduced modulo 2 (n + 1) first
-      std::vector<double> sn((size_t)p.nx * p.nx + (size_t)p.ny * p.ny);
+      std::vector<double> sn((size_t)p.nx * p.nx + (size_t)p.ny * p.ny + p.nx + p.ny);
       size_t o = 0;
       for (int n : {p.nx, p.ny})
         for (int k = 0; k < n; ++k)
@@ -680,6 +680,10 @@ int cg_create(const cg_config* cfg, int device, cg_handle** out) {
             const long r = (long)(i + 1) * (k + 1) % (2 * (n + 1));
             sn[o++] = 2 * std::sin(kPi * (double)r / (n + 1));
           }
+      // then the sines of the Laplacian's eigenvalues, sin(pi / 2 (k + 1) / (n + 1))
+      // as PIC2D::Set2DPhi forms them (PIC2D.cpp:303-307)
+      for (int n : {p.nx, p.ny})
+        for (int k = 0; k < n; ++k) sn[o++] = std::sin(kPi / 2 * (k + 1) / (n + 1));
       if (dalloc(&h.d.sc_sin, sn.size())) return bail(CG_ERR_OOM, "space-charge tables");
       cudaMemcpy(h.d.sc_sin, sn.data(), sizeof(double) * sn.size(), cudaMemcpyHostToDevice);
     }

@@ -289,6 +289,7 @@ __global__ void __launch_bounds__(kScThreads) k_sc_solve(ScParams p, const doubl
   for (int t = threadIdx.x; t < ny * ny; t += kScThreads) Sy[t] = sxy[nx * nx + t];
   __syncthreads();
   const double hx = G[kGHx], hy = G[kGHy];
+  const double* __restrict__ eig = sxy + nx * nx + ny * ny;
   for (int pass = 0; pass < 2; ++pass) {
     // T = Sx R (along x), then R = T Sy^T (along y)
     for (int t = threadIdx.x; t < N; t += kScThreads) {
@@ -301,11 +302,13 @@ __global__ void __launch_bounds__(kScThreads) k_sc_solve(ScParams p, const doubl
     for (int t = threadIdx.x; t < N; t += kScThreads) {
       const int k = t / ny, l = t % ny;
       double s = 0;
-      for (int j = 0; j < ny; ++j) s = fma(T[k * ny + j], Sy[l * ny + j], s);
+      // the DST-I matrix is symmetric: Sy[j][l] = Sy[l][j], read along the
+      // lanes' l so that the warp's loads fall in distinct banks
+      for (int j = 0; j < ny; ++j) s = fma(T[k * ny + j], Sy[j * ny + l], s);
       if (pass == 0) {
-        // the Laplacian's eigenvalue (PIC2D.cpp Set2DPhi): out / K / Epsilon
-        const double knx = kPi / 2 * (k + 1) / (nx + 1), kny = kPi / 2 * (l + 1) / (ny + 1);
-        const double ax = 2 * sin(knx) / hx, ay = 2 * sin(kny) / hy;
+        // the Laplacian's eigenvalue (PIC2D.cpp Set2DPhi): out / K / Epsilon,
+        // with the sines of pi / 2 (k + 1) / (n + 1) from the table
+        const double ax = 2 * eig[k] / hx, ay = 2 * eig[nx + l] / hy;
         const double K = ax * ax + ay * ay;
         R[t] = s / K / kEpsilon0;
       } else {
