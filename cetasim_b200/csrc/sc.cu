@@ -290,29 +290,54 @@ __global__ void __launch_bounds__(kScThreads) k_sc_solve(ScParams p, const doubl
   __syncthreads();
   const double hx = G[kGHx], hy = G[kGHy];
   const double* __restrict__ eig = sxy + nx * nx + ny * ny;
+  // A thread keeps four rows k0..k0+3 of one column: the column's element
+  // is loaded once for the four sums (rows past the mesh are clamped for the
+  // loads and not stored); every sum runs in the index order of a plain
+  // product, so the results do not depend on the grouping.
+  const int groups = ny * ((nx + 3) / 4);
   for (int pass = 0; pass < 2; ++pass) {
-    // T = Sx R (along x), then R = T Sy^T (along y)
-    for (int t = threadIdx.x; t < N; t += kScThreads) {
-      const int k = t / ny, j = t % ny;
-      double s = 0;
-      for (int i = 0; i < nx; ++i) s = fma(Sx[k * nx + i], R[i * ny + j], s);
-      T[t] = s;
+    // T = Sx R (along x)
+    for (int q = threadIdx.x; q < groups; q += kScThreads) {
+      const int j = q % ny, k0 = (q / ny) * 4;
+      const int k1 = min(k0 + 1, nx - 1), k2 = min(k0 + 2, nx - 1), k3 = min(k0 + 3, nx - 1);
+      double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+      for (int i = 0; i < nx; ++i) {
+        const double r = R[i * ny + j];
+        s0 = fma(Sx[k0 * nx + i], r, s0);
+        s1 = fma(Sx[k1 * nx + i], r, s1);
+        s2 = fma(Sx[k2 * nx + i], r, s2);
+        s3 = fma(Sx[k3 * nx + i], r, s3);
+      }
+      T[k0 * ny + j] = s0;
+      if (k0 + 1 < nx) T[k1 * ny + j] = s1;
+      if (k0 + 2 < nx) T[k2 * ny + j] = s2;
+      if (k0 + 3 < nx) T[k3 * ny + j] = s3;
     }
     __syncthreads();
-    for (int t = threadIdx.x; t < N; t += kScThreads) {
-      const int k = t / ny, l = t % ny;
-      double s = 0;
-      // the DST-I matrix is symmetric: Sy[j][l] = Sy[l][j], read along the
-      // lanes' l so that the warp's loads fall in distinct banks
-      for (int j = 0; j < ny; ++j) s = fma(T[k * ny + j], Sy[j * ny + l], s);
-      if (pass == 0) {
-        // the Laplacian's eigenvalue (PIC2D.cpp Set2DPhi): out / K / Epsilon,
-        // with the sines of pi / 2 (k + 1) / (n + 1) from the table
-        const double ax = 2 * eig[k] / hx, ay = 2 * eig[nx + l] / hy;
-        const double K = ax * ax + ay * ay;
-        R[t] = s / K / kEpsilon0;
-      } else {
-        R[t] = s / (4.0 * (nx + 1) * (ny + 1));  // phi [V]
+    // R = T Sy^T (along y); the DST-I matrix is symmetric, Sy[j][l] =
+    // Sy[l][j], so it is read along the lanes' l (distinct banks)
+    for (int q = threadIdx.x; q < groups; q += kScThreads) {
+      const int l = q % ny, k0 = (q / ny) * 4;
+      const int kk[4] = {k0, min(k0 + 1, nx - 1), min(k0 + 2, nx - 1), min(k0 + 3, nx - 1)};
+      double sum[4] = {0, 0, 0, 0};
+      for (int j = 0; j < ny; ++j) {
+        const double y = Sy[j * ny + l];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) sum[u] = fma(T[kk[u] * ny + j], y, sum[u]);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (k0 + u >= nx) break;
+        const int k = kk[u], t = k * ny + l;
+        if (pass == 0) {
+          // the Laplacian's eigenvalue (PIC2D.cpp Set2DPhi): out / K / Epsilon,
+          // with the sines of pi / 2 (k + 1) / (n + 1) from the table
+          const double ax = 2 * eig[k] / hx, ay = 2 * eig[nx + l] / hy;
+          const double K = ax * ax + ay * ay;
+          R[t] = sum[u] / K / kEpsilon0;
+        } else {
+          R[t] = sum[u] / (4.0 * (nx + 1) * (ny + 1));  // phi [V]
+        }
       }
     }
     __syncthreads();
